@@ -1,0 +1,58 @@
+/* C restatement of DG-Parallel's explicit DG right-hand side and SSP-RK3 step.
+ *
+ * TEST INFRASTRUCTURE ONLY.  This is the CPU oracle that the parity tests, the
+ * smoke check and the bench's cpu_baseline leg compare the CUDA path against;
+ * the product never links or calls it.  It restates, in plain FP64 C, the
+ * reference algorithm of DGCell::computeVolumeContribution (DGCell.cc:184-249),
+ * DGBoundaryCell::computeBoundaryContributions (DGCell.cc:639-732),
+ * RungeKuttaTVD3::advanceInTime (TimeIntegrator.cc:838-990) and the CFL rule
+ * of DGCell::adaptTimeStep (DGCell.cc:1155-1207), with DG-Parallel's face
+ * left/right convention (std::set order keyed by the sum of glibc rand() over
+ * vertex ids, mEntity.cc:173-200, Vertex.cc:26-31).  It also restates the
+ * features the reference lacks (Lax-Friedrichs fluxes, 3D Maxwell on tets, the
+ * isentropic vortex and TM110 cavity fields).
+ */
+#ifndef DG_ORACLE_H
+#define DG_ORACLE_H
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum { OR_SCALAR = 0, OR_BURGERS2D = 1, OR_EULER2D = 2, OR_EULER3D = 3, OR_MAXWELL3D = 4 };
+enum { OR_FLUX_UPWIND = 0, OR_FLUX_CENTRAL = 1, OR_FLUX_GODUNOV = 2, OR_FLUX_ROE = 3,
+       OR_FLUX_LLF = 4 };
+/* analytic fields used as initial condition, far field and exact solution */
+enum { OR_FIELD_GAUSS = 0, OR_FIELD_VORTEX = 1, OR_FIELD_PULSE3D = 2, OR_FIELD_SINE = 3,
+       OR_FIELD_GAUSS3D = 4, OR_FIELD_TM110 = 5 };
+
+/* field parameters (16 doubles):
+ *  [0..2] advection velocity a      [3..5] centre c       [6] width s
+ *  [7] gamma   [8] vortex beta   [9] amplitude A   [10] cavity side L */
+typedef struct or_solver or_solver;
+
+or_solver* or_create(const char* msh_path, int law, int flux, int order, int field,
+                     const double* params);
+void or_destroy(or_solver* s);
+int or_num_cells(const or_solver* s);
+int or_num_faces(const or_solver* s);
+int or_num_fields(const or_solver* s);
+int or_num_modes(const or_solver* s);
+/* per face: nfv vertex ids (file ids, sorted ascending), eL, eR, lfL, lfR, bid;
+ * nfv = 2 (edges) or 3 (tet faces); returns ints written. */
+int or_connectivity(const or_solver* s, int* out);
+void or_face_normals(const or_solver* s, double* out); /* per face n[3], measure */
+void or_get_state(const or_solver* s, double* out);    /* [E][m][Np] file order */
+void or_set_state(or_solver* s, const double* in);
+void or_project(or_solver* s, double t);                /* L2 projection of the field */
+void or_rhs(or_solver* s, double t, double* out);       /* assembled RHS, not scaled */
+double or_cfl_dt(const or_solver* s, double cfl);
+double or_step(or_solver* s, double t, double dt);      /* SSP-RK3, returns resid */
+double or_run(or_solver* s, double t0, double tend, double cfl, int nsteps, int* steps_done);
+double or_l2_error(const or_solver* s, double t, int field_index); /* vs exact field */
+void or_field_eval(const or_solver* s, const double* x, double t, double* q);
+unsigned int or_glibc_rand_first(unsigned int seed);   /* srand(seed); rand() */
+
+#ifdef __cplusplus
+}
+#endif
+#endif

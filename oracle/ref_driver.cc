@@ -1,0 +1,444 @@
+// Oracle driver around DG-Parallel's own C++ code (TEST INFRASTRUCTURE ONLY).
+//
+// This file is linked against objects compiled unchanged from the DG-Parallel
+// sources (see oracle/Makefile); it is never part of the product.  It rebuilds
+// the time loop that ships commented out in DGAnalysis::run
+// (DGAnalysis.cc:480-731) and dumps what the parity tests compare:
+//
+//   --conn FILE    one line per mesh face: sorted face vertex ids, left and
+//                  right cell (0-based file order of the cell elements, -1 for
+//                  none), local face index on each side, classification id,
+//                  the left-outward unit normal and the face measure.
+//   --rhs FILE     theRightHandSide of every cell after one assembly
+//                  (TimeIntegrator::assembleVolume + assembleBoundary) of the
+//                  projected initial state, in file order.
+//   --state FILE   coefficients of every cell ([field][mode], file order) of
+//                  the projected initial state and after every --every steps.
+//   --log FILE     per step: dt, time, residual returned by advanceInTime.
+//   --bench N      time N steps (CFL dt + RungeKuttaTVD3::advanceInTime)
+//                  with --threads workers of the reference pthreads path
+//                  (parallel.cc, chunked as main.cc) and print one "BENCH ..."
+//                  line.  Without --bench a single worker thread runs every
+//                  chunk, so results are deterministic and use the stage time.
+//
+// Cases (--case): the analytic fields below are this driver's own and are
+// restated identically by the C oracle and the product.
+//   gauss     scalar advection u_t + a.grad u = 0 (ScalarLaw), a = (ax, ay),
+//             u0 = exp(-((x-cx)^2+(y-cy)^2)/s), exact u0(x - a t) as far field.
+//   vortex    2D Euler isentropic vortex (Euler2d exact Godunov, or
+//             Euler2dRoe with --flux roe); exact solution as far field.
+//   pulse3d   3D Euler (Euler3d) density pulse advected by a uniform flow.
+//   sine      Burgers2D with u0 = 0.5 + A sin(2 pi (x+y)) as far field.
+//   gauss3d   scalar advection on tets, 3D Gaussian.
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <ctime>
+#include <map>
+#include <set>
+#include <string>
+#include <vector>
+#include <algorithm>
+#include <unistd.h>
+
+#include "mImportExport.h"
+#include "mDGMesh.h"
+#include "mEntity.h"
+#include "Vertex.h"
+#include "gEntity.h"
+#include "parallel.h"
+#include "DGCell.h"
+#include "FunctionSpace.h"
+#include "Mapping.h"
+#include "Integrator.h"
+#include "TimeIntegrator.h"
+#include "ScalarLaw.h"
+#include "EulerLaw.h"
+#include "Burgers.h"
+#include "FieldEvaluator.h"
+#include "mPoint.h"
+
+// Globals that the reference's threading code declares extern (main.cc owns
+// them in the shipped program).
+unsigned int numCPU = 1;
+unsigned int numThreads = 1;
+vector<infoWrapper> threadInfo[4];
+vector<infoWrapper> threadInfoBoundary[4];
+double timeRK = 0;
+
+static const double kPi = 3.14159265358979323846;
+
+struct Params {
+  std::string mesh, caseName = "gauss", flux = "exact", conn, rhs, state, log;
+  int order = 2, steps = 0, every = 1, threads = 1, bench = 0;
+  double cfl = 0.1, tend = -1.0;
+  // scalar
+  double ax = 1.0, ay = 0.5, az = 0.0, cx = 0.3, cy = 0.3, cz = 0.3, s = 0.01;
+  // vortex
+  double gamma = 1.4, beta = 5.0, vx0 = 5.0, vy0 = 5.0;
+  // burgers
+  double amp = 1.0;
+};
+static Params P;
+
+class ConstVelocity : public FieldEvaluator {
+ public:
+  void eval(const mPoint&, double, double* v) const { v[0] = P.ax; v[1] = P.ay; v[2] = P.az; }
+  int order() const { return 0; }
+};
+
+class GaussField : public FieldEvaluator {
+ public:
+  void eval(const mPoint& x, double t, double* v) const {
+    mPoint& p = const_cast<mPoint&>(x);
+    double dx = p(0) - P.ax * t - P.cx, dy = p(1) - P.ay * t - P.cy;
+    v[0] = exp(-(dx * dx + dy * dy) / P.s);
+  }
+  int order() const { return 0; }
+};
+
+class Gauss3DField : public FieldEvaluator {
+ public:
+  void eval(const mPoint& x, double t, double* v) const {
+    mPoint& p = const_cast<mPoint&>(x);
+    double dx = p(0) - P.ax * t - P.cx, dy = p(1) - P.ay * t - P.cy, dz = p(2) - P.az * t - P.cz;
+    v[0] = exp(-(dx * dx + dy * dy + dz * dz) / P.s);
+  }
+  int order() const { return 0; }
+};
+
+// Isentropic vortex (free stream rho=u=v=p=1) advected with velocity (1,1).
+class VortexField : public FieldEvaluator {
+ public:
+  void eval(const mPoint& x, double t, double* q) const {
+    mPoint& p = const_cast<mPoint&>(x);
+    const double g = P.gamma, b = P.beta;
+    double dx = p(0) - (P.vx0 + t), dy = p(1) - (P.vy0 + t);
+    double r2 = dx * dx + dy * dy;
+    double e = exp(0.5 * (1.0 - r2));
+    double u = 1.0 - b / (2.0 * kPi) * e * dy;
+    double v = 1.0 + b / (2.0 * kPi) * e * dx;
+    double T = 1.0 - (g - 1.0) * b * b / (8.0 * g * kPi * kPi) * e * e;
+    double rho = pow(T, 1.0 / (g - 1.0));
+    double pr = pow(rho, g);
+    q[0] = rho;
+    q[1] = rho * u;
+    q[2] = rho * v;
+    q[3] = pr / (g - 1.0) + 0.5 * rho * (u * u + v * v);
+  }
+  int order() const { return 0; }
+};
+
+// 3D Euler density pulse rho = 1 + 0.2 exp(-|x-c-Ut|^2/s), U = (ax,ay,az), p = 1.
+// Field order of Euler3d: (rho, rho u, rho v, E, rho w).
+class Pulse3DField : public FieldEvaluator {
+ public:
+  void eval(const mPoint& x, double t, double* q) const {
+    mPoint& p = const_cast<mPoint&>(x);
+    double dx = p(0) - P.ax * t - P.cx, dy = p(1) - P.ay * t - P.cy, dz = p(2) - P.az * t - P.cz;
+    double rho = 1.0 + 0.2 * exp(-(dx * dx + dy * dy + dz * dz) / P.s);
+    double pr = 1.0;
+    q[0] = rho;
+    q[1] = rho * P.ax;
+    q[2] = rho * P.ay;
+    q[4] = rho * P.az;
+    q[3] = pr / (P.gamma - 1.0) + 0.5 * rho * (P.ax * P.ax + P.ay * P.ay + P.az * P.az);
+  }
+  int order() const { return 0; }
+};
+
+class SineField : public FieldEvaluator {
+ public:
+  void eval(const mPoint& x, double, double* v) const {
+    mPoint& p = const_cast<mPoint&>(x);
+    v[0] = 0.5 + P.amp * sin(2.0 * kPi * (p(0) + p(1)));
+  }
+  int order() const { return 0; }
+};
+
+// ---- file-order bookkeeping -------------------------------------------------
+struct MshCells {
+  int dim = 0;
+  std::map<std::vector<int>, int> index;  // sorted vertex ids -> file order of the cell
+  std::vector<std::vector<int> > verts;    // file vertex order per cell
+};
+
+static MshCells readCells(const char* path) {
+  MshCells out;
+  FILE* f = fopen(path, "r");
+  if (!f) { fprintf(stderr, "cannot open %s\n", path); exit(2); }
+  char tok[256];
+  std::vector<std::vector<int> > tris, tets;
+  while (fscanf(f, "%255s", tok) == 1) {
+    if (!strcmp(tok, "$NOD")) {
+      int n; if (fscanf(f, "%d", &n) != 1) exit(2);
+      for (int i = 0; i < n; ++i) { int id; double x, y, z; if (fscanf(f, "%d %lf %lf %lf", &id, &x, &y, &z) != 4) exit(2); }
+    } else if (!strcmp(tok, "$ELM")) {
+      int n; if (fscanf(f, "%d", &n) != 1) exit(2);
+      for (int i = 0; i < n; ++i) {
+        int num, typ, phys, elem, nn;
+        if (fscanf(f, "%d %d %d %d %d", &num, &typ, &phys, &elem, &nn) != 5) exit(2);
+        std::vector<int> v(nn);
+        for (int k = 0; k < nn; ++k) if (fscanf(f, "%d", &v[k]) != 1) exit(2);
+        if (typ == 2) tris.push_back(v);
+        if (typ == 4) tets.push_back(v);
+      }
+    }
+  }
+  fclose(f);
+  out.dim = tets.empty() ? 2 : 3;
+  out.verts = tets.empty() ? tris : tets;
+  for (size_t i = 0; i < out.verts.size(); ++i) {
+    std::vector<int> k = out.verts[i];
+    std::sort(k.begin(), k.end());
+    out.index[k] = (int)i;
+  }
+  return out;
+}
+
+static int cellIndex(const MshCells& mc, mEntity* e) {
+  std::vector<int> k;
+  for (int i = 0; i < e->size(0); ++i) k.push_back(e->get(0, i)->getId());
+  std::sort(k.begin(), k.end());
+  std::map<std::vector<int>, int>::const_iterator it = mc.index.find(k);
+  if (it == mc.index.end()) { fprintf(stderr, "cell not found\n"); exit(3); }
+  return it->second;
+}
+
+// local face index of face entity f in cell c: triangle edge k = (v_k, v_{k+1});
+// tet faces {0,1,2},{0,1,3},{0,2,3},{1,2,3} (mTet.cc Tfv1).
+static int localFace(mEntity* c, mEntity* f) {
+  std::set<int> fv;
+  for (int i = 0; i < f->size(0); ++i) fv.insert(f->get(0, i)->getId());
+  int nv = c->size(0);
+  static const int tri[3][2] = {{0, 1}, {1, 2}, {2, 0}};
+  static const int tet[4][3] = {{0, 1, 2}, {0, 1, 3}, {0, 2, 3}, {1, 2, 3}};
+  if (nv == 3) {
+    for (int k = 0; k < 3; ++k) {
+      std::set<int> s;
+      s.insert(c->get(0, tri[k][0])->getId());
+      s.insert(c->get(0, tri[k][1])->getId());
+      if (s == fv) return k;
+    }
+  } else {
+    for (int k = 0; k < 4; ++k) {
+      std::set<int> s;
+      for (int j = 0; j < 3; ++j) s.insert(c->get(0, tet[k][j])->getId());
+      if (s == fv) return k;
+    }
+  }
+  return -1;
+}
+
+static double nowSec() {
+  timespec ts;
+  clock_gettime(CLOCK_MONOTONIC, &ts);
+  return ts.tv_sec + 1e-9 * ts.tv_nsec;
+}
+
+static void usage() {
+  fprintf(stderr, "usage: ref_driver --mesh F.msh [--case gauss|vortex|pulse3d|sine|gauss3d] "
+                  "[--flux exact|roe] [--order p] [--steps n | --tend T] [--cfl c] "
+                  "[--conn F] [--rhs F] [--state F --every k] [--log F] "
+                  "[--threads k --bench n]\n");
+  exit(1);
+}
+
+int main(int argc, char** argv) {
+  for (int i = 1; i < argc; ++i) {
+    std::string a = argv[i];
+    const char* v = (i + 1 < argc) ? argv[i + 1] : 0;
+    if (!v) usage();
+    if (a == "--mesh") P.mesh = v;
+    else if (a == "--case") P.caseName = v;
+    else if (a == "--flux") P.flux = v;
+    else if (a == "--order") P.order = atoi(v);
+    else if (a == "--steps") P.steps = atoi(v);
+    else if (a == "--tend") P.tend = atof(v);
+    else if (a == "--cfl") P.cfl = atof(v);
+    else if (a == "--every") P.every = atoi(v);
+    else if (a == "--threads") P.threads = atoi(v);
+    else if (a == "--bench") P.bench = atoi(v);
+    else if (a == "--conn") P.conn = v;
+    else if (a == "--rhs") P.rhs = v;
+    else if (a == "--state") P.state = v;
+    else if (a == "--log") P.log = v;
+    else if (a == "--ax") P.ax = atof(v);
+    else if (a == "--ay") P.ay = atof(v);
+    else if (a == "--az") P.az = atof(v);
+    else if (a == "--cx") P.cx = atof(v);
+    else if (a == "--cy") P.cy = atof(v);
+    else if (a == "--cz") P.cz = atof(v);
+    else if (a == "--s") P.s = atof(v);
+    else if (a == "--beta") P.beta = atof(v);
+    else if (a == "--x0") P.vx0 = atof(v);
+    else if (a == "--y0") P.vy0 = atof(v);
+    else if (a == "--amp") P.amp = atof(v);
+    else usage();
+    ++i;
+  }
+  if (P.mesh.empty()) usage();
+  numCPU = sysconf(_SC_NPROCESSORS_ONLN);
+  numThreads = P.threads > 0 ? P.threads : 1;
+
+  MshCells mc = readCells(P.mesh.c_str());
+  mImportExport io;
+  mDGMesh* mesh = new mDGMesh;
+  io.import((char*)P.mesh.c_str(), mesh);
+  const int dim = mesh->size(3) ? 3 : 2;
+  mesh->createCellBoundaries(dim, dim - 1);
+  mesh->createConnections(dim - 1, dim);
+  mesh->createConnections(0, dim - 1);
+  mesh->setPeriodicBC(dim);
+
+  // Thread chunks.  --bench uses the chunking of main.cc:137-159.  Otherwise
+  // (parity runs) one forked worker owns every entity and the master's chunk
+  // is empty: TimeIntegrator::assembleBoundary hands the master chunk
+  // info->_t, which it never updates (TimeIntegrator.cc:1366-1384), so with
+  // main.cc's chunking the master's faces see boundary data at t = 0.
+  if (P.bench <= 0) {
+    numThreads = 2;
+    for (int i = 0; i < 4; ++i) {
+      if (mesh->size(i) == 0) continue;
+      threadInfo[i].push_back(infoWrapper(mesh->begin(i), mesh->end(i), 0, 0));
+      threadInfo[i].push_back(infoWrapper(mesh->end(i), mesh->end(i), 0, 0));
+    }
+  }
+  for (int i = 0; i < 4 && P.bench > 0; ++i) {
+    if (mesh->size(i) == 0) continue;
+    int chunk = mesh->size(i) / numThreads;
+    mMesh::iter it = mesh->begin(i);
+    for (unsigned j = 0; j + 1 < numThreads; ++j) {
+      mMesh::iter head = it;
+      for (int k = 0; k < chunk; ++k) ++it;
+      threadInfo[i].push_back(infoWrapper(head, it, 0, 0));
+    }
+    threadInfo[i].push_back(infoWrapper(it, mesh->end(i), 0, 0));
+  }
+
+  ConstVelocity vel;
+  GaussField gauss;
+  Gauss3DField gauss3;
+  VortexField vortex;
+  Pulse3DField pulse;
+  SineField sine;
+  std::set<int> walls;
+  ConservationLaw* law = 0;
+  if (P.caseName == "gauss") law = new ScalarLaw(&gauss, &vel, &gauss);
+  else if (P.caseName == "gauss3d") law = new ScalarLaw(&gauss3, &vel, &gauss3);
+  else if (P.caseName == "vortex") {
+    if (P.flux == "roe") law = new Euler2dRoe(walls, &vortex, P.gamma);
+    else law = new Euler2d(walls, &vortex, P.gamma);
+  } else if (P.caseName == "pulse3d") law = new Euler3d(walls, &pulse, P.gamma);
+  else if (P.caseName == "sine") law = new Burgers2D(&sine, &sine);
+  else usage();
+  const int m = law->getNbFields();
+
+  GaussIntegrator gi;
+  int DOF = 0;
+  const int E = (int)mc.verts.size();
+  std::vector<DGCell*> byFile(E, (DGCell*)0);
+  for (mMesh::iter it = mesh->begin(dim); it != mesh->end(dim); ++it) {
+    mEntity* ent = *it;
+    FunctionSpace* fs;
+    if (dim == 2) fs = new OrthogonalTriangleFunctionSpace(P.order);
+    else fs = new OrthogonalTetFunctionSpace(P.order);
+    ConstantMeshMapping* map = new ConstantMeshMapping(ent);
+    DGCell* cell = new DGCell(law, ent, fs, 0, map, &gi);
+    ent->setCell(cell);
+    DOF += m * fs->size();
+    cell->L2ProjInitial(law->getFarField());
+    cell->computeMean();
+    cell->ZeroRHS();
+    byFile[cellIndex(mc, ent)] = cell;
+  }
+  for (mMesh::iter it = mesh->begin(dim - 1); it != mesh->end(dim - 1); ++it) {
+    mEntity* ent = *it;
+    DGBoundaryCell* bc = new DGBoundaryCell(ent, new MeshMapping(ent), &gi);
+    ent->setCell(bc);
+  }
+  const int Np = byFile[0]->fSize;
+
+  if (!P.conn.empty()) {
+    FILE* f = fopen(P.conn.c_str(), "w");
+    for (mMesh::iter it = mesh->begin(dim - 1); it != mesh->end(dim - 1); ++it) {
+      mEntity* ent = *it;
+      DGBoundaryCell* bc = (DGBoundaryCell*)ent->getCell();
+      std::vector<int> fv;
+      for (int i = 0; i < ent->size(0); ++i) fv.push_back(ent->get(0, i)->getId());
+      std::sort(fv.begin(), fv.end());
+      mEntity* L = bc->getLeft();
+      mEntity* R = bc->getRight();
+      int eL = cellIndex(mc, L), eR = R ? cellIndex(mc, R) : -1;
+      int lfL = localFace(L, ent), lfR = R ? localFace(R, ent) : -1;
+      double meas = 0;
+      for (int q = 0; q < bc->getNbPtGauss(); ++q) meas += bc->pt(q)->JacTimesWeight;
+      mVector& n = bc->pt(0)->n;
+      for (size_t i = 0; i < fv.size(); ++i) fprintf(f, "%d ", fv[i]);
+      fprintf(f, "%d %d %d %d %d %.17g %.17g %.17g %.17g\n", eL, eR, lfL, lfR,
+              ent->getClassification()->getId(), n(0), n(1), n(2), meas);
+    }
+    fclose(f);
+  }
+
+  RungeKuttaTVD3 rk(mesh, 0, m, DOF);
+
+  if (!P.rhs.empty()) {
+    rk.assembleVolume(0.0);
+    rk.assembleBoundary(0.0);
+    FILE* f = fopen(P.rhs.c_str(), "w");
+    fprintf(f, "%d %d %d\n", E, m, Np);
+    for (int e = 0; e < E; ++e) {
+      for (int j = 0; j < m * Np; ++j) fprintf(f, "%.17g ", byFile[e]->theRightHandSide[j]);
+      fprintf(f, "\n");
+    }
+    fclose(f);
+    for (int e = 0; e < E; ++e) byFile[e]->ZeroRHS();
+  }
+
+  FILE* fs = P.state.empty() ? 0 : fopen(P.state.c_str(), "w");
+  FILE* fl = P.log.empty() ? 0 : fopen(P.log.c_str(), "w");
+  if (fs) fprintf(fs, "%d %d %d\n", E, m, Np);
+  struct Dump {
+    static void state(FILE* f, int step, double t, std::vector<DGCell*>& cells, int m, int Np) {
+      fprintf(f, "step %d %.17g\n", step, t);
+      for (size_t e = 0; e < cells.size(); ++e) {
+        for (int i = 0; i < m; ++i)
+          for (int j = 0; j < Np; ++j) fprintf(f, "%.17g ", cells[e]->theFieldsCoefficients->get(i, j));
+        fprintf(f, "\n");
+      }
+    }
+  };
+  if (fs) Dump::state(fs, 0, 0.0, byFile, m, Np);
+
+  const int nsteps = P.bench > 0 ? P.bench : P.steps;
+  double TACT = 0.0;
+  double t0 = nowSec();
+  for (int step = 1; nsteps <= 0 || step <= nsteps; ++step) {
+    if (P.tend > 0 && TACT >= P.tend) break;
+    if (nsteps <= 0 && P.tend <= 0) break;
+    // CFL time step (DGAnalysis.cc:514-548, mode 0)
+    double dt = 500;
+    for (mMesh::iter it = mesh->begin(dim); it != mesh->end(dim); ++it)
+      ((DGCell*)(*it)->getCell())->adaptTimeStep(P.cfl, dt);
+    if (P.tend > 0) {
+      int N = (int)ceil((P.tend - TACT) / dt);
+      dt = (P.tend - TACT) / N;
+    }
+    for (mMesh::iter it = mesh->begin(dim); it != mesh->end(dim); ++it)
+      ((DGCell*)(*it)->getCell())->setTimeStep(dt);
+    double resid = rk.advanceInTime(TACT, dt);
+    TACT += dt;
+    if (fl) fprintf(fl, "%d %.17g %.17g %.17g\n", step, dt, TACT, resid);
+    if (fs && (step % P.every == 0)) Dump::state(fs, step, TACT, byFile, m, Np);
+  }
+  double elapsed = nowSec() - t0;
+  if (fs) fclose(fs);
+  if (fl) fclose(fl);
+  if (P.bench > 0)
+    printf("BENCH elements=%d fields=%d modes=%d steps=%d threads=%u seconds=%.6f "
+           "dof_stage_per_s=%.6e\n", E, m, Np, P.bench, numThreads, elapsed,
+           (double)E * m * Np * 3.0 * P.bench / elapsed);
+  return 0;
+}
