@@ -1,0 +1,337 @@
+#!/usr/bin/env python3
+"""Benchmark of the DG right-hand side + SSP-RK3 step on B200.
+
+Workload (N = 1): 2D Euler isentropic vortex (gamma 1.4, beta 5, free stream
+(1,1,1,1), centred at (5,5)) on [0,10]^2 cut into 256x256x2 = 131072 seeded
+jittered triangles (+-0.15h), P3 orthonormal basis (10 modes x 4 fields), 12-point
+volume / 4-point edge rules, Roe flux, exact-solution boundaries, CFL 0.1.
+A "step" is one SSP-RK3 step (three stages) over the whole mesh.
+
+Metric: DOF-stage updates/s = cells * fields * modes * 3 * steps / seconds.
+`value` times K device-resident steps (dgp_run, CUDA graphs) with CUDA events
+on the solver's stream; `e2e` times K steps through the C ABI with the state
+copied from pinned host memory before and back after every step.
+
+--gpus N > 1 (torchrun): N independent replicas (the north-star path is one
+GPU; there is no data-path collective); barrier + max over ranks of the timed
+region, value = total updates of all ranks / that time.
+
+--impl reference: DG-Parallel's own pthreads CPU path (oracle/_ref/ref_driver,
+built from the reference sources) on the same mesh and case, all host cores.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "dg-parallel_b200"))
+sys.path.insert(0, os.path.join(ROOT, "tests"))
+
+WORKLOAD = {"workload": "euler2d_isentropic_vortex_256x256x2_P3_roe", "cells": 131072, "order": 3,
+            "fields": 4, "modes": 10, "flux": "roe", "cfl": 0.1, "mesh": "tri 256x256x2 jitter 0.15h seed 2",
+            "rules": "12-pt volume, 4-pt Gauss-Legendre edges"}
+METRIC = "DOF-stage updates/s"
+REF_DRIVER = os.path.join(ROOT, "oracle", "_ref", "ref_driver")
+
+
+def load_peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as fh:
+            return json.load(fh), "measured"
+    except OSError:
+        return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0}, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled while the timed region runs."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+        self.out = tempfile.NamedTemporaryFile(prefix="clocks", suffix=".csv", delete=False)
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), "--query-gpu=" + self.FIELDS,
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                         stdout=self.out, stderr=subprocess.DEVNULL)
+            time.sleep(0.3)
+        except OSError:
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc:
+            time.sleep(0.2)
+            self.proc.terminate()
+            self.proc.wait(timeout=10)
+        self.out.close()
+
+    def summary(self):
+        rows = []
+        try:
+            for line in open(self.out.name):
+                parts = [p.strip() for p in line.split(",")]
+                if len(parts) >= 9:
+                    rows.append(parts)
+        finally:
+            os.unlink(self.out.name)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        sm = sorted(float(r[1]) for r in rows if r[1].replace(".", "").isdigit())
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({n for r in rows for n, v in zip(names, r[5:9]) if v.lower() == "active"})
+        return {"sm_mhz": sm[len(sm) // 2] if sm else None,
+                "sm_max_mhz": float(rows[0][2]) if rows[0][2].replace(".", "").isdigit() else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+def make_mesh():
+    from dgp import meshgen
+    return meshgen.tri_square(256, 256, 0.0, 10.0, 0.0, 10.0, jitter=0.15, seed=2)
+
+
+def vortex_params():
+    import dgp
+    return dgp.law_params(velocity=(1.0, 1.0, 0.0), center=(5.0, 5.0, 0.0), gamma=1.4, beta=5.0)
+
+
+def cpu_reference(mesh, steps: int, warmup: int, threads: int):
+    """DG-Parallel's pthreads path (parallel.cc) on this workload; None if not built."""
+    from dgp import meshgen
+    if not os.path.exists(REF_DRIVER):
+        return None
+    with tempfile.TemporaryDirectory() as td:
+        msh = os.path.join(td, "vortex256.msh")
+        meshgen.write_msh_v1(mesh, msh)
+        cmd = [REF_DRIVER, "--mesh", msh, "--case", "vortex", "--flux", "roe", "--order", "3",
+               "--cfl", "0.1", "--threads", str(threads), "--bench", str(steps), "--warmup", str(warmup)]
+        p = subprocess.run(cmd, capture_output=True, text=True, timeout=1800)
+    line = next((ln for ln in p.stdout.splitlines() if ln.startswith("BENCH")), None)
+    if p.returncode != 0 or line is None:
+        return None
+    kv = dict(tok.split("=") for tok in line.split()[1:])
+    return {"value": float(kv["dof_stage_per_s"]), "seconds": float(kv["seconds"]),
+            "steps": int(kv["steps"]), "threads": int(kv["threads"])}
+
+
+def cpu_model():
+    try:
+        for line in open("/proc/cpuinfo"):
+            if line.startswith("model name"):
+                return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
+
+
+def run_reference_arm(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    mesh = make_mesh()
+    threads = os.cpu_count() or 1
+    r = cpu_reference(mesh, args.steps, args.warmup, threads)
+    if r is None:
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/ref_driver not built "
+                          "(make -C oracle ref needs the DG-Parallel sources)"}))
+        return 0
+    line = {"impl": "reference", "metric": METRIC, "value": r["value"], "unit": "DOF-stage/s",
+            "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": 1e3 * r["seconds"] / r["steps"], "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": dict(WORKLOAD, threads=threads, cpu=cpu_model()),
+            "cpu_baseline": {"value": r["value"], "unit": "DOF-stage/s", "cores": threads,
+                             "kind": "reference",
+                             "sample": f"{args.steps} SSP-RK3 steps of the full workload after "
+                                       f"{args.warmup} warm-up steps, DG-Parallel pthreads path "
+                                       "(parallel.cc) built from source"},
+            "e2e": {"value": r["value"], "unit": "DOF-stage/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=300)
+    ap.add_argument("--warmup", type=int, default=10)
+    ap.add_argument("--impl", default="dgp", choices=["dgp", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--e2e-steps", type=int, default=20)
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        return run_reference_arm(args)
+
+    import numpy as np
+    import torch
+    import dgp
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300))
+
+    mesh_np = make_mesh()
+    prm = vortex_params()
+    mesh = dgp.Mesh.from_arrays(2, mesh_np.vertices, mesh_np.cells, 100, mesh_np.bfaces, mesh_np.btags)
+    law = dgp.Law(dgp.LAW_EULER2D, dgp.FLUX_ROE, dgp.FIELD_VORTEX, prm)
+    E = mesh.ncells
+    units_per_step = E * 4 * 10 * 3
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    def max_over_ranks(x):
+        if dist is None:
+            return x
+        t = torch.tensor([x], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    def timed_run(solver, steps, warmup, sampler=None):
+        solver.project(0.0)
+        t, _ = solver.run(0.0, 0.0, 0.1, warmup)
+        stream = torch.cuda.ExternalStream(solver.stream())
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        barrier()
+        ctx = sampler if sampler is not None else _Null()
+        with ctx:
+            ev0.record(stream)
+            t_end, n = solver.run(t, 0.0, 0.1, steps)
+            ev1.record(stream)
+            ev1.synchronize()
+        barrier()
+        return max_over_ranks(ev0.elapsed_time(ev1) / 1e3), t_end, n
+
+    results = {}
+    clocks = None
+    for name, prec in (("fp64", dgp.FP64), ("mixed", dgp.MIXED)):
+        s = dgp.Solver(mesh, law, 3, prec)
+        sampler = ClockSampler(local) if (name == "fp64" and rank == 0) else None
+        sec, t_end, n = timed_run(s, args.steps, args.warmup, sampler)
+        if sampler is not None:
+            clocks = sampler.summary()
+        assert n == args.steps
+        err = s.l2_error(t_end, 0)
+        kern = s.profile_kernels(20)
+        results[name] = {"seconds": sec, "value": units_per_step * args.steps * world / sec,
+                         "t_end": t_end, "density_l2_vs_exact": err, "kernel_ms": kern.tolist(),
+                         "solver": s}
+    fp64, mixed = results["fp64"], results["mixed"]
+    # mixed vs FP64 at the same time: density L2 difference
+    c64 = fp64["solver"].get_state()
+    c32 = mixed["solver"].get_state()
+    mixed["density_coeff_rel_diff_vs_fp64"] = float(np.abs(c32[:, 0] - c64[:, 0]).max() / np.abs(c64[:, 0]).max())
+
+    # end to end through the C ABI with host buffers: per step, state H2D from
+    # pinned memory, one SSP-RK3 step, state D2H
+    s = fp64["solver"]
+    host = torch.empty(s.shape, dtype=torch.float64, pin_memory=True).numpy()
+    host[...] = s.get_state()
+    nbytes = host.nbytes
+    t = fp64["t_end"]
+    barrier()
+    w0 = time.perf_counter()
+    for _ in range(args.e2e_steps):
+        s.set_state(host)
+        t, _ = s.run(t, 0.0, 0.1, 1)
+        s.get_state(out=host)
+    torch.cuda.synchronize()
+    e2e_sec = max_over_ranks(time.perf_counter() - w0)
+    e2e_value = units_per_step * args.e2e_steps * world / e2e_sec
+
+    if rank == 0:
+        peaks, peak_src = load_peaks()
+        # dominant kernel per stage and its algorithmic bytes per launch
+        face_ms, elem_ms, elem3_ms = fp64["kernel_ms"]
+        M, NP, NQF, NLF = 4, 10, 4, 3
+        F = mesh.nfaces
+        state_b = E * M * NP * 8
+        slot_b = E * NLF * NQF * M * 8
+        geo_e = E * (4 + 1) * 8
+        geo_f = F * (2 * 8 + 8 + 8 + 4)
+        elem_bytes = state_b * 3 + slot_b + geo_e     # read C, U0, slots, geometry; write C
+        face_bytes = state_b + geo_f + slot_b         # read C (each cell once), write slots
+        if elem_ms >= face_ms:
+            kname, kms, kbytes = "elem_kernel (volume + lift + RK3 stage)", elem_ms, elem_bytes
+        else:
+            kname, kms, kbytes = "face_kernel (traces + Roe flux + slot scatter)", face_ms, face_bytes
+        achieved = kbytes / (kms * 1e-3) / 1e9
+        traffic = None
+        tfile = os.path.join(ROOT, "profiles", "traffic.json")
+        if os.path.exists(tfile):
+            tr = json.load(open(tfile))
+            traffic = tr.get(kname.split()[0])
+        ms_per_step = fp64["seconds"] / args.steps * 1e3
+        cpu = None
+        if not args.no_cpu_baseline:
+            r = cpu_reference(mesh_np, 3, 1, os.cpu_count() or 1)
+            if r is not None:
+                cpu = {"value": r["value"], "unit": "DOF-stage/s", "cores": r["threads"], "kind": "reference",
+                       "sample": "3 SSP-RK3 steps (after 1 warm-up) of the full 131072-cell workload, "
+                                 "DG-Parallel pthreads path built from source, " + cpu_model()}
+        line = {
+            "metric": METRIC, "value": fp64["value"], "unit": "DOF-stage/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_per_step,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic",
+            "config": dict(WORKLOAD, parallelism=f"replicas{world}",
+                           l2="working set 150 MB > 126 MB L2; each step streams ~1 GB"),
+            "mixed": {"value": mixed["value"], "dtype": "f32 (f64 geometry, time, totals)",
+                      "speedup_vs_fp64": mixed["value"] / fp64["value"],
+                      "density_l2_vs_exact": mixed["density_l2_vs_exact"],
+                      "density_coeff_rel_diff_vs_fp64": mixed["density_coeff_rel_diff_vs_fp64"],
+                      "kernel_ms": mixed["kernel_ms"]},
+            "fp64_density_l2_vs_exact": fp64["density_l2_vs_exact"],
+            "kernel_ms": {"face": face_ms, "elem": elem_ms, "elem_last_stage_cfl": elem3_ms},
+            "roofline": {"kernel": kname, "bound": "hbm", "achieved": achieved,
+                         "peak": peaks.get("hbm_gbs"), "unit": "GB/s",
+                         "frac": achieved / peaks.get("hbm_gbs"), "traffic": traffic,
+                         "peak_source": peak_src, "algorithmic_bytes_per_launch": kbytes},
+            "cpu_baseline": cpu,
+            "e2e": {"value": e2e_value, "unit": "DOF-stage/s", "h2d_bytes_per_step": nbytes,
+                    "d2h_bytes_per_step": nbytes, "steps": args.e2e_steps,
+                    "timing": "host wall clock, synchronized, C ABI with pinned host state"},
+            "gpu_launches": 48 * ((args.steps + 7) // 8) + 1,  # graphs of 8 steps x 6 kernels + first CFL
+            "clocks": clocks,
+        }
+        print(json.dumps(line))
+    for r in results.values():
+        r["solver"].close()
+    if dist is not None:
+        dist.destroy_process_group()
+    return 0
+
+
+class _Null:
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        return False
+
+
+if __name__ == "__main__":
+    sys.exit(main())

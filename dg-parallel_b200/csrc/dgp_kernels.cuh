@@ -1,0 +1,516 @@
+// CUDA kernels of one explicit DG stage on sm_100a.
+//
+//   face_kernel  one thread per (face, face point): gathers the left and right
+//                traces from [cell][field][mode] coefficients, evaluates the
+//                law's numerical (or boundary) flux and writes -F|J|w into the
+//                left cell's face slot and +F|J|w into the right cell's slot
+//                (per-cell slots [cell][local face][point][field]; no atomics).
+//                Replaces DGBoundaryCell::computeBoundaryContributions
+//                (DGCell.cc:639-732).
+//   elem_kernel  one CTA per tile of TE cells staged in shared memory: volume
+//                term (DGCell::computeVolumeContribution, DGCell.cc:184-249) as
+//                interpolate -> flux -> contraction with the reference gradient
+//                table, plus the lift of the face slots, the diagonal inverse
+//                mass 1/|J| and the SSP-RK3 stage combination
+//                (RungeKuttaTVD3::advanceInTime, TimeIntegrator.cc:838-990).  The
+//                last stage also reduces the CFL time step of the next step
+//                (DGCell::adaptTimeStep, DGCell.cc:1155-1207) and the residual.
+//   cfl_kernel   the same CFL reduction for the first step.
+#pragma once
+
+#include <cstdint>
+
+#include "dgp_laws.cuh"
+
+namespace dgp {
+
+// ---- compile-time shape of one (law, flux, dim, order, precision) ----------
+constexpr int tri_vol_points(int p) { return p == 0 ? 1 : p == 1 ? 3 : p == 2 ? 6 : p == 3 ? 12 : 16; }
+constexpr int tet_vol_points(int p) { return p == 0 ? 1 : p == 1 ? 4 : p == 2 ? 14 : 24; }
+constexpr int tet_face_points(int p) { return p == 0 ? 1 : p == 1 ? 4 : p == 2 ? 7 : 13; }
+
+template <int LAW_, int FLUX_, int DIM_, int ORDER_, typename T_>
+struct Cfg {
+  using T = T_;
+  static constexpr int LAW = LAW_, FLUX = FLUX_, DIM = DIM_, ORDER = ORDER_;
+  static constexpr int M = LawTraits<LAW>::M;
+  static constexpr int NP = DIM == 2 ? (ORDER + 1) * (ORDER + 2) / 2
+                                     : (ORDER + 1) * (ORDER + 2) * (ORDER + 3) / 6;
+  static constexpr int NQ = DIM == 2 ? tri_vol_points(ORDER) : tet_vol_points(ORDER);
+  static constexpr int NQF = DIM == 2 ? ORDER + 1 : tet_face_points(ORDER);
+  static constexpr int NLF = DIM + 1;
+  static constexpr int NPERM = DIM == 2 ? 2 : 6;
+  static constexpr int MNP = M * NP;
+  static constexpr int BLOCK = 256;
+  static constexpr int TE_RAW = 1024 / MNP;
+  static constexpr int TE = TE_RAW < 4 ? 4 : (TE_RAW > 64 ? 64 : TE_RAW);
+  static constexpr int FACE_BLOCK = 128;
+};
+
+// time-step control that lives in device memory so that a whole run can be
+// captured in a CUDA graph without host round trips
+struct TimeCtl {
+  double t;          // time at the start of the current step
+  double dt;         // current step
+  double tend;       // <= 0: no end time
+  double cfl;
+  double resid;      // sum (u_new - u_n)^2 of the last step
+  int steps;         // steps completed
+  int max_steps;     // <= 0: unbounded
+  int done;          // set when tend or max_steps is reached
+  int pad;
+  unsigned long long dtmin_bits;  // atomicMin accumulator (positive double bits)
+  unsigned int blocks_done;       // completion counter of the reducing kernel
+  unsigned int pad2;
+};
+
+struct Status {
+  int nonphysical;
+  int first_bad;  // internal cell index, INT_MAX when none
+};
+
+// device views (internal cell order); T = arithmetic type of the hot path
+template <typename T>
+struct DevMesh {
+  int E, F, NB;
+  const T* jinv;      // E x DIM*DIM, [i][r] = d xi_r / d x_i
+  const T* detj;      // E, |det J|
+  const double* csize;// E, DGCell::computeCellSize
+  const double* x0;   // E x 3 affine origin (FP64)
+  const double* jac;  // E x 9 rows d x / d xi_r (FP64)
+  const int* fel;     // F x 2: eL, eR (eR < 0: boundary face -eR-1)
+  const int* fcode;   // F: lfL | lfR << 4 | perm << 8
+  const T* fnrm;      // F x DIM
+  const T* fj;        // F: |J_f|
+  const double* bpts; // NB x NQF x 3 physical points of boundary faces
+  const int* bbid;    // NB classification ids
+};
+
+template <typename T>
+struct DevTables {
+  const T* phi;     // NQ x NP
+  const T* dphi;    // NQ x DIM x NP
+  const T* qw;      // NQ
+  const T* phif;    // NLF x NQF x NP
+  const T* fqw;     // NQF
+  const int* qmap;  // NPERM x NQF
+  const double* phiv;  // (DIM+1) x NP  (FP64, CFL)
+  const double* phiq;  // NQ x NP (FP64, projection)
+  const double* qwd;   // NQ (FP64)
+  const double* qpd;   // NQ x 3 (FP64)
+  int nqe;             // error rule
+  const double* eqp;   // nqe x 3
+  const double* eqw;   // nqe
+  const double* ephi;  // nqe x NP
+  double phi0;
+};
+
+template <typename T>
+struct StageArgs {
+  DevMesh<T> mesh;
+  DevTables<T> tab;
+  LawParams law;
+  const T* C;      // state the stage reads
+  const T* U0;     // u_n (stages 2 and 3)
+  T* Cout;         // state the stage writes (or the RHS when stage == 0)
+  T* U0out;        // stage 1 copies u_n here
+  T* slots;        // E x NLF x NQF x M
+  TimeCtl* ctl;
+  Status* status;
+  double* partials;  // per-block residual partials (stage 3)
+  double stage_time_factor;  // 0, 1, 0.5: boundary time = t + factor * dt
+  int stage;       // 0: RHS only, 1..3: SSP-RK3 stages
+  int fuse_cfl;    // stage 3 reduces the next step's dt
+  int order;
+};
+
+__device__ __forceinline__ void flag_nonphysical(Status* st, int cell) {
+  atomicAdd(&st->nonphysical, 1);
+  atomicMin(&st->first_bad, cell);
+}
+
+// -----------------------------------------------------------------------------
+template <class K>
+__global__ void __launch_bounds__(K::FACE_BLOCK) face_kernel(StageArgs<typename K::T> a) {
+  using T = typename K::T;
+  constexpr int M = K::M, NP = K::NP, NQF = K::NQF, DIM = K::DIM;
+  if (a.ctl->done) return;
+  __shared__ T s_phif[K::NLF * NQF * NP];
+  __shared__ T s_fqw[NQF];
+  __shared__ int s_qmap[K::NPERM * NQF];
+  for (int i = threadIdx.x; i < K::NLF * NQF * NP; i += blockDim.x) s_phif[i] = a.tab.phif[i];
+  for (int i = threadIdx.x; i < NQF; i += blockDim.x) s_fqw[i] = a.tab.fqw[i];
+  for (int i = threadIdx.x; i < K::NPERM * NQF; i += blockDim.x) s_qmap[i] = a.tab.qmap[i];
+  __syncthreads();
+  const int gid = blockIdx.x * blockDim.x + threadIdx.x;
+  const int f = gid / NQF, q = gid - (gid / NQF) * NQF;
+  if (f >= a.mesh.F) return;
+  const int eL = a.mesh.fel[2 * f], eR = a.mesh.fel[2 * f + 1];
+  const int code = a.mesh.fcode[f];
+  const int lfL = code & 15, lfR = (code >> 4) & 15, perm = code >> 8;
+  T n[DIM];
+#pragma unroll
+  for (int i = 0; i < DIM; ++i) n[i] = a.mesh.fnrm[f * DIM + i];
+  const T jw = a.mesh.fj[f] * s_fqw[q];
+  T UL[M], UR[M], flux[M];
+  const T* cl = a.C + (size_t)eL * K::MNP;
+  const T* pl = s_phif + (lfL * NQF + q) * NP;
+#pragma unroll
+  for (int j = 0; j < M; ++j) {
+    T acc = 0;
+#pragma unroll
+    for (int k = 0; k < NP; ++k) acc += pl[k] * cl[j * NP + k];
+    UL[j] = acc;
+  }
+  if (!is_physical<K::LAW, T>(a.law, UL)) flag_nonphysical(a.status, eL);
+  int qR = 0;
+  if (eR >= 0) {
+    qR = s_qmap[perm * NQF + q];
+    const T* cr = a.C + (size_t)eR * K::MNP;
+    const T* pr = s_phif + (lfR * NQF + qR) * NP;
+#pragma unroll
+    for (int j = 0; j < M; ++j) {
+      T acc = 0;
+#pragma unroll
+      for (int k = 0; k < NP; ++k) acc += pr[k] * cr[j * NP + k];
+      UR[j] = acc;
+    }
+    if (!is_physical<K::LAW, T>(a.law, UR)) flag_nonphysical(a.status, eR);
+    numerical_flux<K::LAW, K::FLUX, DIM, T>(a.law, n, UL, UR, flux);
+  } else {
+    const int b = -eR - 1;
+    const double* x = a.mesh.bpts + ((size_t)b * NQF + q) * 3;
+    const double time = a.ctl->t + a.stage_time_factor * a.ctl->dt;
+    boundary_flux<K::LAW, K::FLUX, DIM, T>(a.law, a.mesh.bbid[b], n, x, time, UL, flux);
+  }
+  T* sl = a.slots + (((size_t)eL * K::NLF + lfL) * NQF + q) * M;
+#pragma unroll
+  for (int j = 0; j < M; ++j) sl[j] = -flux[j] * jw;
+  if (eR >= 0) {
+    T* sr = a.slots + (((size_t)eR * K::NLF + lfR) * NQF + qR) * M;
+#pragma unroll
+    for (int j = 0; j < M; ++j) sr[j] = flux[j] * jw;
+  }
+}
+
+// -----------------------------------------------------------------------------
+// CFL time step of one cell: |cell| * cfl / (a (2p+1)), a = max eigenvalue at
+// the mean and (triangles) at the three reference vertices.
+template <class K>
+__device__ __forceinline__ double cell_dt(const StageArgs<typename K::T>& a, const typename K::T* c,
+                                          int e, double cfl) {
+  using T = typename K::T;
+  constexpr int M = K::M, NP = K::NP;
+  T mean[M];
+#pragma unroll
+  for (int j = 0; j < M; ++j) mean[j] = c[j * NP] * (T)a.tab.phi0;
+  T am = max_eigen<K::LAW, T>(a.law, mean);
+  if constexpr (K::DIM == 2) {
+#pragma unroll
+    for (int v = 0; v < 3; ++v) {
+      T val[M];
+#pragma unroll
+      for (int j = 0; j < M; ++j) {
+        T acc = 0;
+#pragma unroll
+        for (int k = 0; k < NP; ++k) acc += (T)a.tab.phiv[v * NP + k] * c[j * NP + k];
+        val[j] = acc;
+      }
+      T b = max_eigen<K::LAW, T>(a.law, val);
+      am = (b > am ? b : am);
+    }
+  }
+  return a.mesh.csize[e] * cfl / ((double)am * (2. * K::ORDER + 1.0));
+}
+
+__device__ __forceinline__ double ctl_finalize(TimeCtl* c, double dtmin) {
+  bool done = (c->max_steps > 0 && c->steps >= c->max_steps) || (c->tend > 0 && c->t >= c->tend);
+  double dt = dtmin;
+  if (c->tend > 0 && !done) {
+    int N = (int)ceil((c->tend - c->t) / dt);
+    dt = (c->tend - c->t) / N;
+  }
+  c->dt = dt;
+  c->done = done ? 1 : 0;
+  return dt;
+}
+
+// block-wide min of a double; thread 0 gets the result
+template <int BLOCK>
+__device__ __forceinline__ double block_min(double v, double* red) {
+  for (int o = 16; o > 0; o >>= 1) v = fmin(v, __shfl_xor_sync(0xffffffffu, v, o));
+  const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+  if (l == 0) red[w] = v;
+  __syncthreads();
+  if (w == 0) {
+    v = (l < BLOCK / 32) ? red[l] : 1e300;
+    for (int o = 16; o > 0; o >>= 1) v = fmin(v, __shfl_xor_sync(0xffffffffu, v, o));
+  }
+  __syncthreads();
+  return v;
+}
+
+template <int BLOCK>
+__device__ __forceinline__ double block_sum(double v, double* red) {
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+  if (l == 0) red[w] = v;
+  __syncthreads();
+  if (w == 0) {
+    v = (l < BLOCK / 32) ? red[l] : 0.0;
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  }
+  __syncthreads();
+  return v;
+}
+
+// -----------------------------------------------------------------------------
+template <class K>
+__global__ void __launch_bounds__(K::BLOCK) elem_kernel(StageArgs<typename K::T> a) {
+  using T = typename K::T;
+  constexpr int M = K::M, NP = K::NP, NQ = K::NQ, NQF = K::NQF, DIM = K::DIM, TE = K::TE;
+  constexpr int MNP = K::MNP, NS = K::NLF * NQF;
+  if (a.ctl->done) return;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  T* sC = reinterpret_cast<T*>(smem_raw);        // TE x MNP
+  T* sG = sC + TE * MNP;                          // TE x NQ x M x DIM
+  T* sS = sG + TE * NQ * M * DIM;                 // TE x NS x M
+  T* sPhi = sS + TE * NS * M;                     // NQ x NP
+  T* sDphi = sPhi + NQ * NP;                      // NQ x DIM x NP
+  T* sPhif = sDphi + NQ * DIM * NP;               // NS x NP
+  T* sQw = sPhif + NS * NP;                       // NQ
+  __shared__ double red[K::BLOCK / 32];
+  __shared__ bool amLast;
+
+  const int e0 = blockIdx.x * TE;
+  const int ne = min(TE, a.mesh.E - e0);
+  for (int i = threadIdx.x; i < NQ * NP; i += K::BLOCK) sPhi[i] = a.tab.phi[i];
+  for (int i = threadIdx.x; i < NQ * DIM * NP; i += K::BLOCK) sDphi[i] = a.tab.dphi[i];
+  for (int i = threadIdx.x; i < NS * NP; i += K::BLOCK) sPhif[i] = a.tab.phif[i];
+  for (int i = threadIdx.x; i < NQ; i += K::BLOCK) sQw[i] = a.tab.qw[i];
+  {
+    const T* src = a.C + (size_t)e0 * MNP;
+    for (int i = threadIdx.x; i < ne * MNP; i += K::BLOCK) sC[i] = src[i];
+    const T* ss = a.slots + (size_t)e0 * NS * M;
+    for (int i = threadIdx.x; i < ne * NS * M; i += K::BLOCK) sS[i] = ss[i];
+  }
+  __syncthreads();
+
+  // volume: per (cell, point) interpolate, flux, map to reference directions
+  for (int it = threadIdx.x; it < ne * NQ; it += K::BLOCK) {
+    const int e = it / NQ, q = it - (it / NQ) * NQ;
+    const T* c = sC + e * MNP;
+    T U[M];
+#pragma unroll
+    for (int j = 0; j < M; ++j) {
+      T acc = 0;
+#pragma unroll
+      for (int k = 0; k < NP; ++k) acc += sPhi[q * NP + k] * c[j * NP + k];
+      U[j] = acc;
+    }
+    if (!is_physical<K::LAW, T>(a.law, U)) flag_nonphysical(a.status, e0 + e);
+    T F[M][DIM];
+    volume_flux<K::LAW, DIM, T>(a.law, U, F);
+    const T* Ji = a.mesh.jinv + (size_t)(e0 + e) * DIM * DIM;
+    T J[DIM * DIM];
+#pragma unroll
+    for (int i = 0; i < DIM * DIM; ++i) J[i] = Ji[i];
+    const T jw = a.mesh.detj[e0 + e] * sQw[q];
+    T* g = sG + (e * NQ + q) * M * DIM;
+#pragma unroll
+    for (int j = 0; j < M; ++j)
+#pragma unroll
+      for (int r = 0; r < DIM; ++r) {
+        T acc = 0;
+#pragma unroll
+        for (int i = 0; i < DIM; ++i) acc += F[j][i] * J[i * DIM + r];
+        g[j * DIM + r] = acc * jw;
+      }
+  }
+  __syncthreads();
+
+  // contraction + lift + inverse mass + stage combination, one coefficient per item
+  double rsum = 0.0;
+  const double dt = a.ctl->dt;
+  for (int it = threadIdx.x; it < ne * MNP; it += K::BLOCK) {
+    const int e = it / MNP, jk = it - (it / MNP) * MNP;
+    const int j = jk / NP, k = jk - (jk / NP) * NP;
+    T acc = 0;
+    const T* g = sG + e * NQ * M * DIM + j * DIM;
+#pragma unroll
+    for (int q = 0; q < NQ; ++q)
+#pragma unroll
+      for (int r = 0; r < DIM; ++r) acc += g[q * M * DIM + r] * sDphi[(q * DIM + r) * NP + k];
+    const T* s = sS + e * NS * M + j;
+#pragma unroll
+    for (int p = 0; p < NS; ++p) acc += s[p * M] * sPhif[p * NP + k];
+    const size_t gi = (size_t)(e0 + e) * MNP + jk;
+    if (a.stage == 0) {
+      a.Cout[gi] = acc;
+      continue;
+    }
+    const T dtj = (T)(dt / (double)a.mesh.detj[e0 + e]);
+    const T c = sC[it];
+    T out;
+    if (a.stage == 1) {
+      a.U0out[gi] = c;
+      out = c + acc * dtj;
+    } else if (a.stage == 2) {
+      out = (T)0.25 * (c + acc * dtj + (T)3. * a.U0[gi]);
+    } else {
+      const T u0 = a.U0[gi];
+      out = ((T)2.0 * (c + acc * dtj) + u0) / (T)3.0;
+      const double d = (double)out - (double)u0;
+      rsum += d * d;
+    }
+    a.Cout[gi] = out;
+    sC[it] = out;
+  }
+  if (a.stage != 3) return;
+
+  // stage 3: residual partial, and the CFL step of the next step
+  rsum = block_sum<K::BLOCK>(rsum, red);
+  if (threadIdx.x == 0) a.partials[blockIdx.x] = rsum;
+  if (a.fuse_cfl) {
+    double dtl = 1e300;
+    if (threadIdx.x < ne) dtl = cell_dt<K>(a, sC + threadIdx.x * MNP, e0 + threadIdx.x, a.ctl->cfl);
+    dtl = block_min<K::BLOCK>(dtl, red);
+    if (threadIdx.x == 0) atomicMin(&a.ctl->dtmin_bits, (unsigned long long)__double_as_longlong(dtl));
+  }
+  if (threadIdx.x == 0) {
+    __threadfence();
+    unsigned v = atomicAdd(&a.ctl->blocks_done, 1u);
+    amLast = (v == gridDim.x - 1);
+  }
+  __syncthreads();
+  if (amLast && threadIdx.x == 0) {
+    __threadfence();
+    double r = 0.0;
+    for (unsigned b = 0; b < gridDim.x; ++b) r += ((volatile double*)a.partials)[b];
+    TimeCtl* c = a.ctl;
+    c->resid = r;
+    c->blocks_done = 0;
+    c->t = c->t + c->dt;
+    c->steps += 1;
+    if (a.fuse_cfl) {
+      unsigned long long bits = atomicExch(&c->dtmin_bits, 0x7FF0000000000000ull);
+      ctl_finalize(c, __longlong_as_double((long long)bits));
+    }
+  }
+}
+
+// -----------------------------------------------------------------------------
+template <class K>
+__global__ void __launch_bounds__(256) cfl_kernel(StageArgs<typename K::T> a) {
+  __shared__ double red[256 / 32];
+  __shared__ bool amLast;
+  if (a.ctl->done) return;
+  const int e = blockIdx.x * 256 + threadIdx.x;
+  double dtl = 1e300;
+  if (e < a.mesh.E) dtl = cell_dt<K>(a, a.C + (size_t)e * K::MNP, e, a.ctl->cfl);
+  dtl = block_min<256>(dtl, red);
+  if (threadIdx.x == 0) {
+    atomicMin(&a.ctl->dtmin_bits, (unsigned long long)__double_as_longlong(dtl));
+    __threadfence();
+    unsigned v = atomicAdd(&a.ctl->blocks_done, 1u);
+    amLast = (v == gridDim.x - 1);
+  }
+  __syncthreads();
+  if (amLast && threadIdx.x == 0) {
+    __threadfence();
+    TimeCtl* c = a.ctl;
+    c->blocks_done = 0;
+    unsigned long long bits = atomicExch(&c->dtmin_bits, 0x7FF0000000000000ull);
+    ctl_finalize(c, __longlong_as_double((long long)bits));
+  }
+}
+
+// -----------------------------------------------------------------------------
+// L2 projection of the law's field (DGCell::L2ProjInitial, DGCell.cc:1458-1483):
+// one thread per (cell, mode), FP64 accumulation in the reference's order.
+template <class K>
+__global__ void project_kernel(StageArgs<typename K::T> a, double t, typename K::T* out) {
+  using T = typename K::T;
+  constexpr int M = K::M, NP = K::NP, NQ = K::NQ;
+  const int gid = blockIdx.x * blockDim.x + threadIdx.x;
+  const int e = gid / NP, k = gid - (gid / NP) * NP;
+  if (e >= a.mesh.E) return;
+  const double* x0 = a.mesh.x0 + 3 * (size_t)e;
+  const double* J = a.mesh.jac + 9 * (size_t)e;
+  double proj[M];
+#pragma unroll
+  for (int j = 0; j < M; ++j) proj[j] = 0.0;
+  const double detj = (double)a.mesh.detj[e];
+  for (int q = 0; q < NQ; ++q) {
+    double x[3];
+    const double* xi = a.tab.qpd + 3 * q;
+    for (int c = 0; c < 3; ++c) {
+      x[c] = x0[c];
+      for (int r = 0; r < K::DIM; ++r) x[c] += xi[r] * J[r * 3 + c];
+    }
+    double val[M];
+    field_eval<double>(a.law, x, t, val);
+    const double jw = detj * a.tab.qwd[q];
+    for (int j = 0; j < M; ++j) proj[j] += val[j] * a.tab.phiq[q * NP + k] * jw;
+  }
+  const double inv = 1. / detj;
+  for (int j = 0; j < M; ++j) out[(size_t)e * K::MNP + j * NP + k] = (T)(proj[j] * inv);
+}
+
+// per-block partial sums of (u_h - u_exact)^2 |J| w of one field over the
+// error rule of degree 2(p+1) (DGCell::densityErrorL2, DGError.cc:805-826)
+template <class K>
+__global__ void __launch_bounds__(256) l2err_kernel(StageArgs<typename K::T> a, double t, int field,
+                                                     double* partials) {
+  constexpr int M = K::M, NP = K::NP;
+  __shared__ double red[256 / 32];
+  const int e = blockIdx.x * 256 + threadIdx.x;
+  double acc = 0.0;
+  if (e < a.mesh.E) {
+    const double* x0 = a.mesh.x0 + 3 * (size_t)e;
+    const double* J = a.mesh.jac + 9 * (size_t)e;
+    const auto* c = a.C + (size_t)e * K::MNP;
+    const double detj = (double)a.mesh.detj[e];
+    for (int q = 0; q < a.tab.nqe; ++q) {
+      double x[3];
+      const double* xi = a.tab.eqp + 3 * q;
+      for (int cc = 0; cc < 3; ++cc) {
+        x[cc] = x0[cc];
+        for (int r = 0; r < K::DIM; ++r) x[cc] += xi[r] * J[r * 3 + cc];
+      }
+      double uh = 0.0;
+      for (int k = 0; k < NP; ++k) uh += a.tab.ephi[q * NP + k] * (double)c[field * NP + k];
+      double ex[M];
+      field_eval<double>(a.law, x, t, ex);
+      const double d = uh - ex[field];
+      acc += d * d * detj * a.tab.eqw[q];
+    }
+  }
+  acc = block_sum<256>(acc, red);
+  if (threadIdx.x == 0) partials[blockIdx.x] = acc;
+}
+
+// per-block partial cell integrals of every field: |J| * |ref| * phi0 * c[j][0]
+template <class K>
+__global__ void __launch_bounds__(256) totals_kernel(StageArgs<typename K::T> a, double refm,
+                                                      double* partials) {
+  __shared__ double red[256 / 32];
+  const int e = blockIdx.x * 256 + threadIdx.x;
+  for (int j = 0; j < K::M; ++j) {
+    double v = 0.0;
+    if (e < a.mesh.E)
+      v = (double)a.mesh.detj[e] * refm * a.tab.phi0 * (double)a.C[(size_t)e * K::MNP + j * K::NP];
+    v = block_sum<256>(v, red);
+    if (threadIdx.x == 0) partials[(size_t)blockIdx.x * K::M + j] = v;
+  }
+}
+
+template <class K>
+constexpr size_t elem_smem_bytes() {
+  using T = typename K::T;
+  constexpr int NS = K::NLF * K::NQF;
+  return sizeof(T) * (size_t)(K::TE * K::MNP + K::TE * K::NQ * K::M * K::DIM + K::TE * NS * K::M +
+                              K::NQ * K::NP + K::NQ * K::DIM * K::NP + NS * K::NP + K::NQ);
+}
+
+}  // namespace dgp

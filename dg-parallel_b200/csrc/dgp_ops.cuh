@@ -1,0 +1,112 @@
+// Launchers of one kernel instantiation (included by the per-law
+// instantiation units).
+#pragma once
+
+#include "dgp_solver.h"
+
+namespace dgp {
+
+template <class K>
+cudaError_t ops_prepare() {
+  const size_t smem = elem_smem_bytes<K>();
+  if (smem > 48 * 1024)
+    return cudaFuncSetAttribute(elem_kernel<K>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                static_cast<int>(smem));
+  return cudaSuccess;
+}
+
+template <class K>
+int ops_grid_elem(int E) {
+  return (E + K::TE - 1) / K::TE;
+}
+
+template <class K>
+StageArgs<typename K::T> stage_args(const DeviceBuffers& b, int stage, double time_factor, int fuse_cfl) {
+  using T = typename K::T;
+  StageArgs<T> a = make_args<T>(b);
+  a.stage = stage;
+  a.stage_time_factor = time_factor;
+  a.fuse_cfl = fuse_cfl;
+  if (stage == 0) a.Cout = static_cast<T*>(b.rhs);
+  return a;
+}
+
+template <class K>
+void ops_face(const DeviceBuffers& b, int stage, double time_factor, cudaStream_t st) {
+  auto a = stage_args<K>(b, stage, time_factor, 0);
+  const long long nf = static_cast<long long>(b.F) * K::NQF;
+  const int fgrid = static_cast<int>((nf + K::FACE_BLOCK - 1) / K::FACE_BLOCK);
+  face_kernel<K><<<fgrid, K::FACE_BLOCK, 0, st>>>(a);
+}
+
+template <class K>
+void ops_elem(const DeviceBuffers& b, int stage, int fuse_cfl, cudaStream_t st) {
+  auto a = stage_args<K>(b, stage, 0.0, fuse_cfl);
+  elem_kernel<K><<<ops_grid_elem<K>(b.E), K::BLOCK, elem_smem_bytes<K>(), st>>>(a);
+}
+
+template <class K>
+void ops_stage(const DeviceBuffers& b, int stage, double time_factor, int fuse_cfl, cudaStream_t st) {
+  ops_face<K>(b, stage, time_factor, st);
+  ops_elem<K>(b, stage, fuse_cfl, st);
+}
+
+template <class K>
+void ops_cfl(const DeviceBuffers& b, cudaStream_t st) {
+  StageArgs<typename K::T> a = make_args<typename K::T>(b);
+  cfl_kernel<K><<<(b.E + 255) / 256, 256, 0, st>>>(a);
+}
+
+template <class K>
+void ops_project(const DeviceBuffers& b, double t, cudaStream_t st) {
+  using T = typename K::T;
+  StageArgs<T> a = make_args<T>(b);
+  const long long n = static_cast<long long>(b.E) * K::NP;
+  project_kernel<K><<<static_cast<int>((n + 127) / 128), 128, 0, st>>>(a, t, static_cast<T*>(b.C));
+}
+
+template <class K>
+void ops_l2err(const DeviceBuffers& b, double t, int field, cudaStream_t st) {
+  StageArgs<typename K::T> a = make_args<typename K::T>(b);
+  l2err_kernel<K><<<(b.E + 255) / 256, 256, 0, st>>>(a, t, field, b.partials);
+}
+
+template <class K>
+void ops_totals(const DeviceBuffers& b, double refm, cudaStream_t st) {
+  StageArgs<typename K::T> a = make_args<typename K::T>(b);
+  totals_kernel<K><<<(b.E + 255) / 256, 256, 0, st>>>(a, refm, b.partials);
+}
+
+template <class K>
+Ops make_ops() {
+  Ops o;
+  o.M = K::M;
+  o.NP = K::NP;
+  o.NQ = K::NQ;
+  o.NQF = K::NQF;
+  o.TE = K::TE;
+  o.elem_block = K::BLOCK;
+  o.elem_smem = elem_smem_bytes<K>();
+  o.tsize = sizeof(typename K::T);
+  o.precision = sizeof(typename K::T) == 8 ? DGP_PRECISION_FP64 : DGP_PRECISION_MIXED;
+  o.prepare = &ops_prepare<K>;
+  o.stage = &ops_stage<K>;
+  o.face = &ops_face<K>;
+  o.elem = &ops_elem<K>;
+  o.cfl = &ops_cfl<K>;
+  o.project = &ops_project<K>;
+  o.l2err = &ops_l2err<K>;
+  o.totals = &ops_totals<K>;
+  o.grid_elem = &ops_grid_elem<K>;
+  return o;
+}
+
+template <int LAW, int FLUX, int DIM, int ORDER>
+void add_ops() {
+  ops_registry()[OpsKey(LAW, FLUX, DIM, ORDER, DGP_PRECISION_FP64)] =
+      make_ops<Cfg<LAW, FLUX, DIM, ORDER, double>>();
+  ops_registry()[OpsKey(LAW, FLUX, DIM, ORDER, DGP_PRECISION_MIXED)] =
+      make_ops<Cfg<LAW, FLUX, DIM, ORDER, float>>();
+}
+
+}  // namespace dgp

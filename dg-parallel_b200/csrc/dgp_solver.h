@@ -1,0 +1,133 @@
+// Solver object behind the C ABI: device buffers in the internal (Morton)
+// cell order and the kernel set of one (law, flux, dim, order, precision).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <map>
+#include <string>
+#include <tuple>
+#include <vector>
+
+#include "dgp_host.h"
+#include "dgp_kernels.cuh"
+
+namespace dgp {
+
+// Device buffers; pointers typed as void* hold the hot-path precision T.
+struct DeviceBuffers {
+  int E = 0, F = 0, NB = 0, order = 0, dim = 0, M = 0, NP = 0;
+  void* jinv = nullptr;
+  void* detj = nullptr;
+  double* csize = nullptr;
+  double* x0 = nullptr;
+  double* jac = nullptr;
+  int* fel = nullptr;
+  int* fcode = nullptr;
+  void* fnrm = nullptr;
+  void* fj = nullptr;
+  double* bpts = nullptr;
+  int* bbid = nullptr;
+  void* phi = nullptr;
+  void* dphi = nullptr;
+  void* qw = nullptr;
+  void* phif = nullptr;
+  void* fqw = nullptr;
+  int* qmap = nullptr;
+  double* phiv = nullptr;
+  double* phiq = nullptr;
+  double* qwd = nullptr;
+  double* qpd = nullptr;
+  int nqe = 0;
+  double* eqp = nullptr;
+  double* eqw = nullptr;
+  double* ephi = nullptr;
+  double phi0 = 0.0;
+  void* C = nullptr;      // state [cell][field][mode], updated in place by the stages
+  void* U0 = nullptr;     // u_n of the current step
+  void* slots = nullptr;  // per-cell face slots
+  void* rhs = nullptr;    // assembled RHS for dgp_rhs
+  void* scratch = nullptr;// state-sized staging for device-side set/get
+  TimeCtl* ctl = nullptr;
+  Status* status = nullptr;
+  double* partials = nullptr;
+  int npartials = 0;
+  LawParams law{};
+};
+
+template <typename T>
+inline StageArgs<T> make_args(const DeviceBuffers& b) {
+  StageArgs<T> a{};
+  a.mesh.E = b.E;
+  a.mesh.F = b.F;
+  a.mesh.NB = b.NB;
+  a.mesh.jinv = static_cast<const T*>(b.jinv);
+  a.mesh.detj = static_cast<const T*>(b.detj);
+  a.mesh.csize = b.csize;
+  a.mesh.x0 = b.x0;
+  a.mesh.jac = b.jac;
+  a.mesh.fel = b.fel;
+  a.mesh.fcode = b.fcode;
+  a.mesh.fnrm = static_cast<const T*>(b.fnrm);
+  a.mesh.fj = static_cast<const T*>(b.fj);
+  a.mesh.bpts = b.bpts;
+  a.mesh.bbid = b.bbid;
+  a.tab.phi = static_cast<const T*>(b.phi);
+  a.tab.dphi = static_cast<const T*>(b.dphi);
+  a.tab.qw = static_cast<const T*>(b.qw);
+  a.tab.phif = static_cast<const T*>(b.phif);
+  a.tab.fqw = static_cast<const T*>(b.fqw);
+  a.tab.qmap = b.qmap;
+  a.tab.phiv = b.phiv;
+  a.tab.phiq = b.phiq;
+  a.tab.qwd = b.qwd;
+  a.tab.qpd = b.qpd;
+  a.tab.nqe = b.nqe;
+  a.tab.eqp = b.eqp;
+  a.tab.eqw = b.eqw;
+  a.tab.ephi = b.ephi;
+  a.tab.phi0 = b.phi0;
+  a.law = b.law;
+  a.C = static_cast<const T*>(b.C);
+  a.U0 = static_cast<const T*>(b.U0);
+  a.Cout = static_cast<T*>(b.C);
+  a.U0out = static_cast<T*>(b.U0);
+  a.slots = static_cast<T*>(b.slots);
+  a.ctl = b.ctl;
+  a.status = b.status;
+  a.partials = b.partials;
+  a.order = b.order;
+  return a;
+}
+
+// Kernel set of one instantiation.
+struct Ops {
+  int M = 0, NP = 0, NQ = 0, NQF = 0, TE = 0, elem_block = 0, precision = 0;
+  size_t elem_smem = 0;
+  size_t tsize = 8;
+  cudaError_t (*prepare)() = nullptr;
+  // one SSP-RK3 stage (face kernel + element kernel); stage 0 writes the RHS
+  void (*stage)(const DeviceBuffers&, int stage, double time_factor, int fuse_cfl, cudaStream_t) = nullptr;
+  void (*face)(const DeviceBuffers&, int stage, double time_factor, cudaStream_t) = nullptr;
+  void (*elem)(const DeviceBuffers&, int stage, int fuse_cfl, cudaStream_t) = nullptr;
+  void (*cfl)(const DeviceBuffers&, cudaStream_t) = nullptr;
+  void (*project)(const DeviceBuffers&, double t, cudaStream_t) = nullptr;
+  void (*l2err)(const DeviceBuffers&, double t, int field, cudaStream_t) = nullptr;
+  void (*totals)(const DeviceBuffers&, double refm, cudaStream_t) = nullptr;
+  int (*grid_elem)(int E) = nullptr;
+};
+
+using OpsKey = std::tuple<int, int, int, int, int>;  // law, flux, dim, order, precision
+std::map<OpsKey, Ops>& ops_registry();
+void register_scalar_ops();
+void register_burgers_ops();
+void register_euler2d_godunov_ops();
+void register_euler2d_roe_ops();
+void register_euler2d_llf_ops();
+void register_euler3d_ops();
+void register_maxwell3d_ops();
+
+template <class K>
+Ops make_ops();
+
+}  // namespace dgp

@@ -1,0 +1,279 @@
+"""ctypes binding of libdgp.so (the C ABI in include/dgp.h).
+
+This module only marshals arguments; every computation runs in the CUDA
+library.  Importing it loads ``dg-parallel_b200/lib/libdgp.so`` and raises if the
+library is missing -- there is no CPU fallback.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(os.path.dirname(_HERE), "lib", "libdgp.so")
+
+LAW_SCALAR, LAW_BURGERS2D, LAW_EULER2D, LAW_EULER3D, LAW_MAXWELL3D = range(5)
+FLUX_UPWIND, FLUX_CENTRAL, FLUX_GODUNOV, FLUX_ROE, FLUX_LLF = range(5)
+FIELD_GAUSS, FIELD_VORTEX, FIELD_PULSE3D, FIELD_SINE, FIELD_GAUSS3D, FIELD_TM110 = range(6)
+FP64, MIXED = 0, 1
+NPARAMS = 16
+
+ERRORS = {-1: "invalid argument", -2: "I/O", -3: "unsupported", -4: "CUDA", -5: "non-physical",
+          -6: "out of memory"}
+
+
+class DGPError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"dgp error {code} ({ERRORS.get(code, '?')}): {msg}")
+        self.code = code
+
+
+_lib = None
+
+
+def lib() -> ctypes.CDLL:
+    """Load libdgp.so once; raises FileNotFoundError when it was not built."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise FileNotFoundError(f"{LIB_PATH} is missing: run dg-parallel_b200/build.py")
+    L = ctypes.CDLL(LIB_PATH)
+    P, I, D = ctypes.c_void_p, ctypes.c_int, ctypes.c_double
+    pI = ctypes.POINTER(ctypes.c_int)
+    pD = ctypes.POINTER(ctypes.c_double)
+    pP = ctypes.POINTER(ctypes.c_void_p)
+    sig = {
+        "dgp_last_error": ([], ctypes.c_char_p),
+        "dgp_version": ([], I),
+        "dgp_mesh_from_msh": ([ctypes.c_char_p, pP], I),
+        "dgp_mesh_from_arrays": ([I, I, pD, pI, I, pI, I, I, pI, pI, pP], I),
+        "dgp_mesh_info": ([P, pI, pI, pI, pI], I),
+        "dgp_mesh_connectivity": ([P, pI], I),
+        "dgp_mesh_face_geometry": ([P, pD], I),
+        "dgp_mesh_destroy": ([P], I),
+        "dgp_law_create": ([I, I, I, pD, pP], I),
+        "dgp_law_destroy": ([P], I),
+        "dgp_solver_create": ([P, P, I, I, I, pP], I),
+        "dgp_solver_destroy": ([P], I),
+        "dgp_solver_info": ([P, pI, pI, pI, pI], I),
+        "dgp_project": ([P, D], I),
+        "dgp_set_state": ([P, pD], I),
+        "dgp_get_state": ([P, pD], I),
+        "dgp_set_state_device": ([P, P], I),
+        "dgp_get_state_device": ([P, P], I),
+        "dgp_rhs": ([P, D, pD], I),
+        "dgp_cfl_dt": ([P, D, pD], I),
+        "dgp_step": ([P, D, D, pD], I),
+        "dgp_run": ([P, D, D, D, I, pD, pI], I),
+        "dgp_status": ([P, pI, pI], I),
+        "dgp_l2_error": ([P, D, I, pD], I),
+        "dgp_totals": ([P, pD], I),
+        "dgp_synchronize": ([P], I),
+        "dgp_solver_stream": ([P, pP], I),
+        "dgp_profile_kernels": ([P, I, ctypes.POINTER(ctypes.c_float)], I),
+    }
+    for name, (args, res) in sig.items():
+        f = getattr(L, name)
+        f.argtypes = args
+        f.restype = res
+    _lib = L
+    return L
+
+
+def check(rc: int) -> None:
+    if rc != 0:
+        raise DGPError(rc, lib().dgp_last_error().decode())
+
+
+def _dp(a: np.ndarray):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+
+
+def _ip(a: np.ndarray):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_int))
+
+
+def law_params(velocity=(0.0, 0.0, 0.0), center=(0.0, 0.0, 0.0), width=1.0, gamma=1.4, beta=5.0,
+               amplitude=1.0, cavity=1.0) -> np.ndarray:
+    p = np.zeros(NPARAMS)
+    p[0:3] = velocity
+    p[3:6] = center
+    p[6] = width
+    p[7] = gamma
+    p[8] = beta
+    p[9] = amplitude
+    p[10] = cavity
+    return p
+
+
+class Mesh:
+    def __init__(self, handle):
+        self.h = handle
+        dim, e, f, v = (ctypes.c_int() for _ in range(4))
+        check(lib().dgp_mesh_info(self.h, ctypes.byref(dim), ctypes.byref(e), ctypes.byref(f),
+                                  ctypes.byref(v)))
+        self.dim, self.ncells, self.nfaces, self.nvertices = dim.value, e.value, f.value, v.value
+
+    @classmethod
+    def from_msh(cls, path: str) -> "Mesh":
+        h = ctypes.c_void_p()
+        check(lib().dgp_mesh_from_msh(path.encode(), ctypes.byref(h)))
+        return cls(h)
+
+    @classmethod
+    def from_arrays(cls, dim, xyz, cells, cell_tag=100, bfaces=None, btags=None,
+                    vertex_ids=None) -> "Mesh":
+        xyz = np.ascontiguousarray(xyz, dtype=np.float64)
+        cells = np.ascontiguousarray(cells, dtype=np.int32)
+        nb = 0 if bfaces is None else len(bfaces)
+        bf = np.ascontiguousarray(bfaces if nb else np.zeros((1, dim)), dtype=np.int32)
+        bt = np.ascontiguousarray(btags if nb else np.zeros(1), dtype=np.int32)
+        vids = None if vertex_ids is None else np.ascontiguousarray(vertex_ids, dtype=np.int32)
+        h = ctypes.c_void_p()
+        check(lib().dgp_mesh_from_arrays(dim, xyz.shape[0], _dp(xyz), _ip(vids) if vids is not None else None,
+                                         cells.shape[0], _ip(cells), cell_tag, nb, _ip(bf), _ip(bt),
+                                         ctypes.byref(h)))
+        return cls(h)
+
+    def connectivity(self) -> np.ndarray:
+        n = self.dim + 5
+        out = np.zeros(self.nfaces * n, dtype=np.int32)
+        check(lib().dgp_mesh_connectivity(self.h, _ip(out)))
+        return out.reshape(self.nfaces, n)
+
+    def face_geometry(self) -> np.ndarray:
+        out = np.zeros(self.nfaces * 4)
+        check(lib().dgp_mesh_face_geometry(self.h, _dp(out)))
+        return out.reshape(self.nfaces, 4)
+
+    def close(self):
+        if self.h:
+            lib().dgp_mesh_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Law:
+    def __init__(self, kind: int, flux: int, field: int, params=None):
+        p = np.ascontiguousarray(params if params is not None else np.zeros(NPARAMS), dtype=np.float64)
+        self.h = ctypes.c_void_p()
+        self.kind, self.flux, self.field = kind, flux, field
+        check(lib().dgp_law_create(kind, flux, field, _dp(p), ctypes.byref(self.h)))
+
+    def close(self):
+        if self.h:
+            lib().dgp_law_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Solver:
+    """TimeIntegrator-style driver of one mesh + law on the current CUDA device."""
+
+    def __init__(self, mesh: Mesh, law: Law, order: int, precision: int = FP64, limiter: int = 0):
+        self.mesh, self.law = mesh, law
+        self.h = ctypes.c_void_p()
+        check(lib().dgp_solver_create(mesh.h, law.h, order, precision, limiter, ctypes.byref(self.h)))
+        m, n, e, f = (ctypes.c_int() for _ in range(4))
+        check(lib().dgp_solver_info(self.h, ctypes.byref(m), ctypes.byref(n), ctypes.byref(e),
+                                    ctypes.byref(f)))
+        self.nfields, self.nmodes, self.ncells, self.nfaces = m.value, n.value, e.value, f.value
+        self.shape = (self.ncells, self.nfields, self.nmodes)
+
+    def project(self, t: float = 0.0):
+        check(lib().dgp_project(self.h, t))
+
+    def get_state(self, out: np.ndarray | None = None) -> np.ndarray:
+        """State [cell][field][mode] in file order; `out` (C-contiguous float64,
+        e.g. a pinned buffer) is filled in place when given."""
+        if out is None:
+            out = np.zeros(self.shape)
+        assert out.dtype == np.float64 and out.flags.c_contiguous and out.size == np.prod(self.shape)
+        check(lib().dgp_get_state(self.h, _dp(out)))
+        return out
+
+    def set_state(self, c: np.ndarray):
+        c = np.ascontiguousarray(c, dtype=np.float64).reshape(self.shape)
+        check(lib().dgp_set_state(self.h, _dp(c)))
+
+    def set_state_device(self, ptr: int):
+        check(lib().dgp_set_state_device(self.h, ctypes.c_void_p(ptr)))
+
+    def get_state_device(self, ptr: int):
+        check(lib().dgp_get_state_device(self.h, ctypes.c_void_p(ptr)))
+
+    def rhs(self, t: float) -> np.ndarray:
+        out = np.zeros(self.shape)
+        check(lib().dgp_rhs(self.h, t, _dp(out)))
+        return out
+
+    def cfl_dt(self, cfl: float) -> float:
+        dt = ctypes.c_double()
+        check(lib().dgp_cfl_dt(self.h, cfl, ctypes.byref(dt)))
+        return dt.value
+
+    def step(self, t: float, dt: float) -> float:
+        r = ctypes.c_double()
+        check(lib().dgp_step(self.h, t, dt, ctypes.byref(r)))
+        return r.value
+
+    def run(self, t0: float, tend: float, cfl: float, max_steps: int = 0) -> tuple[float, int]:
+        t = ctypes.c_double()
+        n = ctypes.c_int()
+        check(lib().dgp_run(self.h, t0, tend, cfl, max_steps, ctypes.byref(t), ctypes.byref(n)))
+        return t.value, n.value
+
+    def status(self) -> tuple[int, int]:
+        a, b = ctypes.c_int(), ctypes.c_int()
+        check(lib().dgp_status(self.h, ctypes.byref(a), ctypes.byref(b)))
+        return a.value, b.value
+
+    def l2_error(self, t: float, field: int = 0) -> float:
+        e = ctypes.c_double()
+        check(lib().dgp_l2_error(self.h, t, field, ctypes.byref(e)))
+        return e.value
+
+    def totals(self) -> np.ndarray:
+        out = np.zeros(self.nfields)
+        check(lib().dgp_totals(self.h, _dp(out)))
+        return out
+
+    def stream(self) -> int:
+        """cudaStream_t of the solver (for CUDA events recorded on it)."""
+        h = ctypes.c_void_p()
+        check(lib().dgp_solver_stream(self.h, ctypes.byref(h)))
+        return h.value or 0
+
+    def profile_kernels(self, iters: int = 20) -> np.ndarray:
+        """Mean ms of [face kernel, element kernel (inner stage), element kernel
+        (last stage with the fused CFL reduction)]."""
+        out = (ctypes.c_float * 3)()
+        check(lib().dgp_profile_kernels(self.h, iters, out))
+        return np.array(out[:], dtype=np.float64)
+
+    def synchronize(self):
+        check(lib().dgp_synchronize(self.h))
+
+    def close(self):
+        if self.h:
+            lib().dgp_solver_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -1,0 +1,138 @@
+/* dgp -- B200-native explicit DG right-hand side and SSP-RK3 stepping.
+ *
+ * C ABI of libdgp.so.  Every function returns an int status (DGP_OK = 0,
+ * negative on error; dgp_last_error() gives the message of the calling
+ * thread's last failure).  Handles are opaque; one host thread per solver
+ * handle; each solver owns one CUDA stream on the device that was current when
+ * it was created.  State arrays crossing the ABI are FP64 in DG-Parallel's
+ * layout: [cell][field][mode], cells in the order of the cell elements in the
+ * mesh file (or of the `cells` array passed to dgp_mesh_from_arrays).
+ *
+ * Each entry point names the DG-Parallel interface it replaces.
+ */
+#ifndef DGP_H
+#define DGP_H
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define DGP_OK 0
+#define DGP_ERR_INVALID (-1)     /* bad argument or handle */
+#define DGP_ERR_IO (-2)          /* mesh file missing or malformed */
+#define DGP_ERR_UNSUPPORTED (-3) /* law/flux/order/element combination not built */
+#define DGP_ERR_CUDA (-4)        /* CUDA runtime error (message in dgp_last_error) */
+#define DGP_ERR_NONPHYSICAL (-5) /* a stage produced a non-physical state */
+#define DGP_ERR_NOMEM (-6)
+
+/* conservation laws (ConservationLaw subclasses, ConservationLaw.h:12-60) */
+#define DGP_LAW_SCALAR 0    /* ScalarLaw (ScalarLaw.cc), constant velocity field */
+#define DGP_LAW_BURGERS2D 1 /* Burgers2D (Burgers2D.cc) */
+#define DGP_LAW_EULER2D 2   /* Euler2d / Euler2dRoe (EulerLaw.cc) */
+#define DGP_LAW_EULER3D 3   /* Euler3d (EulerLaw.cc) */
+#define DGP_LAW_MAXWELL3D 4 /* 3D Maxwell on tets (no counterpart; Maxwell2d is 2D only) */
+
+/* numerical fluxes (ConservationLaw::riemannSolver overrides) */
+#define DGP_FLUX_UPWIND 0  /* ScalarLaw::riemannSolver, Maxwell upwind */
+#define DGP_FLUX_CENTRAL 1 /* Burgers2D::riemannSolver (maxIV = 0) */
+#define DGP_FLUX_GODUNOV 2 /* Euler2d/Euler3d::riemannSolver: exact Riemann solver */
+#define DGP_FLUX_ROE 3     /* Euler2dRoe::riemannSolver */
+#define DGP_FLUX_LLF 4     /* local Lax-Friedrichs (no counterpart in DG-Parallel) */
+
+/* analytic FieldEvaluator functors (FieldEvaluator.h:9-15) used as initial
+ * condition, far field (ConservationLaw::getFarField) and exact solution.  A
+ * host callback cannot run per GPU quadrature point, so evaluators are chosen
+ * by id with parameters. */
+#define DGP_FIELD_GAUSS 0   /* exp(-|x - c - a t|^2 / s), 2D */
+#define DGP_FIELD_VORTEX 1  /* isentropic vortex, free stream (1,1,1,1), moving (1,1) */
+#define DGP_FIELD_PULSE3D 2 /* Euler3d density pulse advected by velocity a, p = 1 */
+#define DGP_FIELD_SINE 3    /* 0.5 + A sin(2 pi (x + y)) */
+#define DGP_FIELD_GAUSS3D 4 /* exp(-|x - c - a t|^2 / s), 3D */
+#define DGP_FIELD_TM110 5   /* TM110 mode of the PEC cube [0,L]^3 */
+
+/* law / field parameters: double[16]
+ *  [0..2] advection velocity a   [3..5] centre c   [6] width s
+ *  [7] gamma (default 1.4)       [8] vortex strength beta
+ *  [9] amplitude A               [10] cavity side L */
+#define DGP_NPARAMS 16
+
+#define DGP_PRECISION_FP64 0  /* plain FP64 drop-in form */
+#define DGP_PRECISION_MIXED 1 /* FP32 bulk arithmetic, FP64 geometry/totals/time */
+
+#define DGP_LIMITER_NONE 0
+#define DGP_LIMITER_MOMENT 1
+
+typedef struct dgp_mesh_s* dgp_mesh;
+typedef struct dgp_law_s* dgp_law;
+typedef struct dgp_solver_s* dgp_solver;
+
+const char* dgp_last_error(void);
+int dgp_version(void);
+
+/* ---- mesh: replaces mImportExport::import (mImportExport.cc:57-170) and
+ * mMesh::createCellBoundaries/createConnections (mMesh.cc:321-378) */
+int dgp_mesh_from_msh(const char* path, dgp_mesh* out);
+/* dim 2: cells are triangles (3 vertex indices), bfaces edges (2);
+ * dim 3: tets (4) and triangles (3).  Indices are 0-based into xyz (nv x 3);
+ * vertex_ids are the file ids used by DG-Parallel's entity ordering
+ * (NULL -> 1..nv). */
+int dgp_mesh_from_arrays(int dim, int nv, const double* xyz, const int* vertex_ids, int ncells,
+                         const int* cells, int cell_tag, int nbfaces, const int* bfaces,
+                         const int* btags, dgp_mesh* out);
+int dgp_mesh_info(dgp_mesh m, int* dim, int* ncells, int* nfaces, int* nvertices);
+/* per face: dim sorted vertex ids, left cell, right cell (-1: boundary),
+ * local face on each side (-1), classification id; (dim + 5) ints per face.
+ * Left/right follow DG-Parallel's upward-adjacency order
+ * (DGBoundaryCell::check, DGCell.cc:355-391). */
+int dgp_mesh_connectivity(dgp_mesh m, int* out);
+/* per face: unit normal (outward from the left cell, 3 doubles) and measure */
+int dgp_mesh_face_geometry(dgp_mesh m, double* out);
+int dgp_mesh_destroy(dgp_mesh m);
+
+/* ---- law: replaces the ConservationLaw + FieldEvaluator objects */
+int dgp_law_create(int kind, int flux, int field, const double* params, dgp_law* out);
+int dgp_law_destroy(dgp_law law);
+
+/* ---- solver: DGAnalysis setup (DGAnalysis.cc:133-302) + TimeIntegrator */
+int dgp_solver_create(dgp_mesh m, dgp_law law, int order, int precision, int limiter,
+                      dgp_solver* out);
+int dgp_solver_destroy(dgp_solver s);
+int dgp_solver_info(dgp_solver s, int* nfields, int* nmodes, int* ncells, int* nfaces);
+/* DGCell::L2ProjInitial (DGCell.cc:1458-1483) of the law's field at time t */
+int dgp_project(dgp_solver s, double t);
+int dgp_set_state(dgp_solver s, const double* host_state);
+int dgp_get_state(dgp_solver s, double* host_state);
+/* device-resident variants (pointer to [cell][field][mode] FP64 in file order) */
+int dgp_set_state_device(dgp_solver s, const double* dev_state);
+int dgp_get_state_device(dgp_solver s, double* dev_state);
+/* assembled theRightHandSide of every cell for the current state at time t:
+ * TimeIntegrator::assembleVolume + assembleBoundary (TimeIntegrator.cc:1332-1412) */
+int dgp_rhs(dgp_solver s, double t, double* host_rhs);
+/* min over cells of DGCell::adaptTimeStep (DGCell.cc:1155-1207) */
+int dgp_cfl_dt(dgp_solver s, double cfl, double* dt);
+/* RungeKuttaTVD3::advanceInTime(t, dt) (TimeIntegrator.cc:838-990); resid may be NULL */
+int dgp_step(dgp_solver s, double t, double dt, double* resid);
+/* time loop of DGAnalysis::run (DGAnalysis.cc:480-731): CFL dt every step,
+ * stretched to land on tend when tend > 0; at most max_steps when > 0.
+ * Runs device-resident (CUDA graphs), no host sync per step. */
+int dgp_run(dgp_solver s, double t0, double tend, double cfl, int max_steps, double* t_out,
+            int* steps_out);
+/* non-physical states seen since the last call (isPhysical, EulerLaw.cc:1398) */
+int dgp_status(dgp_solver s, int* nonphysical, int* first_bad_cell);
+/* L2 error of one field against the law's exact field (DGCell::densityErrorL2,
+ * DGError.cc:805-826), FP64 reduction */
+int dgp_l2_error(dgp_solver s, double t, int field, double* err);
+/* sum over cells of the cell integral of every field (conserved totals), FP64 */
+int dgp_totals(dgp_solver s, double* totals);
+int dgp_synchronize(dgp_solver s);
+/* the solver's CUDA stream (cudaStream_t) for callers that order their own
+ * work or record CUDA events against the solver's launches */
+int dgp_solver_stream(dgp_solver s, void** stream);
+/* mean device time (CUDA events on the solver's stream) of the face kernel,
+ * the element kernel of an inner stage and the element kernel of the last
+ * stage (with the fused CFL reduction), over `iters` launches each: ms[3] */
+int dgp_profile_kernels(dgp_solver s, int iters, float* ms);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -15,7 +15,7 @@
 //   --state FILE   coefficients of every cell ([field][mode], file order) of
 //                  the projected initial state and after every --every steps.
 //   --log FILE     per step: dt, time, residual returned by advanceInTime.
-//   --bench N      time N steps (CFL dt + RungeKuttaTVD3::advanceInTime)
+//   --bench N      time N steps (after --warmup W untimed ones) (CFL dt + RungeKuttaTVD3::advanceInTime)
 //                  with --threads workers of the reference pthreads path
 //                  (parallel.cc, chunked as main.cc) and print one "BENCH ..."
 //                  line.  Without --bench a single worker thread runs every
@@ -71,7 +71,7 @@ static const double kPi = 3.14159265358979323846;
 
 struct Params {
   std::string mesh, caseName = "gauss", flux = "exact", conn, rhs, state, log;
-  int order = 2, steps = 0, every = 1, threads = 1, bench = 0;
+  int order = 2, steps = 0, every = 1, threads = 1, bench = 0, warmup = 0;
   double cfl = 0.1, tend = -1.0;
   // scalar
   double ax = 1.0, ay = 0.5, az = 0.0, cx = 0.3, cy = 0.3, cz = 0.3, s = 0.01;
@@ -260,6 +260,7 @@ int main(int argc, char** argv) {
     else if (a == "--every") P.every = atoi(v);
     else if (a == "--threads") P.threads = atoi(v);
     else if (a == "--bench") P.bench = atoi(v);
+    else if (a == "--warmup") P.warmup = atoi(v);
     else if (a == "--conn") P.conn = v;
     else if (a == "--rhs") P.rhs = v;
     else if (a == "--state") P.state = v;
@@ -412,10 +413,11 @@ int main(int argc, char** argv) {
   };
   if (fs) Dump::state(fs, 0, 0.0, byFile, m, Np);
 
-  const int nsteps = P.bench > 0 ? P.bench : P.steps;
+  const int nsteps = P.bench > 0 ? P.bench + P.warmup : P.steps;
   double TACT = 0.0;
   double t0 = nowSec();
   for (int step = 1; nsteps <= 0 || step <= nsteps; ++step) {
+    if (P.bench > 0 && step == P.warmup + 1) t0 = nowSec();
     if (P.tend > 0 && TACT >= P.tend) break;
     if (nsteps <= 0 && P.tend <= 0) break;
     // CFL time step (DGAnalysis.cc:514-548, mode 0)

@@ -1,0 +1,94 @@
+#!/usr/bin/env python3
+"""Regenerate the golden fixtures of tests/golden/ from DG-Parallel itself.
+
+Runs oracle/_ref/ref_driver -- the reference's own C++ code compiled from its
+sources by ``make -C oracle ref`` -- on small seeded meshes and stores, per
+case, the mesh file and an .npz with:
+
+* ``conn``   faces as (sorted vertex ids, eL, eR, lfL, lfR, classification id)
+* ``geom``   left-outward unit normal and measure per face (same row order)
+* ``states`` coefficients [step][cell][field*mode] (file order), step 0 = the
+             L2 projection of the initial field, then after each RK3 step
+* ``rhs``    assembled right-hand side of the projected state at t = 0
+* ``log``    per step: dt, time, residual
+
+The reference run uses one worker thread so that stage times are honoured (see
+oracle/ref_driver.cc).  Usage: python tests/golden/make_golden.py
+"""
+from __future__ import annotations
+
+import os
+import subprocess
+import sys
+import tempfile
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, os.path.join(ROOT, "dg-parallel_b200"))
+from dgp import meshgen  # noqa: E402
+
+DRIVER = os.path.join(ROOT, "oracle", "_ref", "ref_driver")
+
+# name: (mesh builder, driver arguments, steps)
+SQUARE = dict(nx=4, ny=4, seed=1)
+VORTEX_BOX = dict(nx=4, ny=4, x0=0.0, x1=10.0, y0=0.0, y1=10.0, seed=2)
+CASES = {
+    "scalar_tri_p1": ("tri", SQUARE, ["--case", "gauss", "--order", "1"], 3),
+    "scalar_tri_p2": ("tri", SQUARE, ["--case", "gauss", "--order", "2"], 3),
+    "scalar_tri_p3": ("tri", SQUARE, ["--case", "gauss", "--order", "3"], 3),
+    "scalar_tri_p4": ("tri", SQUARE, ["--case", "gauss", "--order", "4"], 3),
+    "euler_godunov_p2": ("tri", VORTEX_BOX, ["--case", "vortex", "--flux", "exact", "--order", "2"], 3),
+    "euler_godunov_p3": ("tri", VORTEX_BOX, ["--case", "vortex", "--flux", "exact", "--order", "3"], 3),
+    "euler_roe_p1": ("tri", VORTEX_BOX, ["--case", "vortex", "--flux", "roe", "--order", "1"], 3),
+    "euler_roe_p3": ("tri", VORTEX_BOX, ["--case", "vortex", "--flux", "roe", "--order", "3"], 3),
+    "euler_roe_p4": ("tri", VORTEX_BOX, ["--case", "vortex", "--flux", "roe", "--order", "4"], 3),
+    "burgers_p2": ("tri", SQUARE, ["--case", "sine", "--order", "2", "--amp", "0.25"], 3),
+    "scalar_tet_p2": ("tet", dict(n=2, seed=3), ["--case", "gauss3d", "--order", "2", "--ax", "1",
+                                                  "--ay", "0.5", "--az", "0.25", "--cx", "0.5",
+                                                  "--cy", "0.5", "--cz", "0.5", "--s", "0.05"], 3),
+    "euler3d_p1": ("tet", dict(n=2, seed=3), ["--case", "pulse3d", "--order", "1", "--ax", "1",
+                                               "--ay", "0.5", "--az", "0.25", "--cx", "0.5",
+                                               "--cy", "0.5", "--cz", "0.5", "--s", "0.05"], 3),
+    "euler3d_p2": ("tet", dict(n=2, seed=3), ["--case", "pulse3d", "--order", "2", "--ax", "1",
+                                               "--ay", "0.5", "--az", "0.25", "--cx", "0.5",
+                                               "--cy", "0.5", "--cz", "0.5", "--s", "0.05"], 3),
+}
+
+
+def build_mesh(kind, args):
+    return meshgen.tri_square(**args) if kind == "tri" else meshgen.tet_cube(**args)
+
+
+def run_case(name, kind, margs, dargs, steps):
+    mesh = build_mesh(kind, margs)
+    msh = os.path.join(HERE, name + ".msh")
+    meshgen.write_msh_v1(mesh, msh)
+    with tempfile.TemporaryDirectory() as td:
+        conn, rhs, state, log = (os.path.join(td, f) for f in ("c", "r", "s", "l"))
+        cmd = [DRIVER, "--mesh", msh, "--steps", str(steps), "--cfl", "0.1", "--conn", conn,
+               "--rhs", rhs, "--state", state, "--log", log] + dargs
+        subprocess.run(cmd, check=True, capture_output=True)
+        c = np.loadtxt(conn)
+        nf = 5 + (2 if kind == "tri" else 3)
+        r = np.loadtxt(rhs, skiprows=1)
+        blocks = open(state).read().split("step ")[1:]
+        states = np.array([[list(map(float, ln.split())) for ln in b.split("\n")[1:] if ln.strip()]
+                           for b in blocks])
+        lg = np.loadtxt(log, ndmin=2)
+    np.savez_compressed(os.path.join(HERE, name + ".npz"), conn=c[:, :nf].astype(np.int64),
+                        geom=c[:, nf:], states=states, rhs=np.atleast_2d(r), log=lg,
+                        args=np.array(dargs), steps=steps)
+
+
+def main():
+    if not os.path.exists(DRIVER):
+        sys.exit("build the reference first: make -C oracle ref")
+    for name, (kind, margs, dargs, steps) in CASES.items():
+        run_case(name, kind, margs, dargs, steps)
+        print("wrote", name)
+
+
+if __name__ == "__main__":
+    main()

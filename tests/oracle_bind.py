@@ -1,0 +1,119 @@
+"""ctypes binding of the C oracle (oracle/_build/liboracle.so) for the tests.
+
+The oracle is the checker: it restates DG-Parallel's CPU algorithm in plain C
+(see oracle/dg_oracle.h).  Only tests, the smoke check and the bench's CPU
+baseline use it.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+ORACLE_SO = os.path.join(ROOT, "oracle", "_build", "liboracle.so")
+
+_lib = None
+
+
+def lib():
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(ORACLE_SO):
+        subprocess.run(["make", "-C", os.path.join(ROOT, "oracle"), "oracle"], check=True,
+                       capture_output=True)
+    L = ctypes.CDLL(ORACLE_SO)
+    P, I, D = ctypes.c_void_p, ctypes.c_int, ctypes.c_double
+    pD = ctypes.POINTER(ctypes.c_double)
+    pI = ctypes.POINTER(ctypes.c_int)
+    L.or_create.restype = P
+    L.or_create.argtypes = [ctypes.c_char_p, I, I, I, I, pD]
+    for f in ("or_num_cells", "or_num_faces", "or_num_fields", "or_num_modes"):
+        getattr(L, f).argtypes = [P]
+        getattr(L, f).restype = I
+    L.or_destroy.argtypes = [P]
+    L.or_connectivity.argtypes = [P, pI]
+    L.or_connectivity.restype = I
+    L.or_face_normals.argtypes = [P, pD]
+    L.or_get_state.argtypes = [P, pD]
+    L.or_set_state.argtypes = [P, pD]
+    L.or_project.argtypes = [P, D]
+    L.or_rhs.argtypes = [P, D, pD]
+    L.or_cfl_dt.argtypes = [P, D]
+    L.or_cfl_dt.restype = D
+    L.or_step.argtypes = [P, D, D]
+    L.or_step.restype = D
+    L.or_run.argtypes = [P, D, D, D, I, pI]
+    L.or_run.restype = D
+    L.or_l2_error.argtypes = [P, D, I]
+    L.or_l2_error.restype = D
+    L.or_glibc_rand_first.argtypes = [ctypes.c_uint]
+    L.or_glibc_rand_first.restype = ctypes.c_uint
+    _lib = L
+    return L
+
+
+def _dp(a):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+
+
+class Oracle:
+    def __init__(self, msh: str, law: int, flux: int, order: int, field: int, params):
+        p = np.ascontiguousarray(params, dtype=np.float64)
+        self.h = lib().or_create(msh.encode(), law, flux, order, field, _dp(p))
+        if not self.h:
+            raise RuntimeError(f"oracle could not load {msh}")
+        L = lib()
+        self.ncells = L.or_num_cells(self.h)
+        self.nfaces = L.or_num_faces(self.h)
+        self.nfields = L.or_num_fields(self.h)
+        self.nmodes = L.or_num_modes(self.h)
+        self.shape = (self.ncells, self.nfields, self.nmodes)
+
+    def connectivity(self, dim):
+        n = dim + 5
+        out = np.zeros(self.nfaces * n, dtype=np.int32)
+        lib().or_connectivity(self.h, out.ctypes.data_as(ctypes.POINTER(ctypes.c_int)))
+        return out.reshape(self.nfaces, n)
+
+    def state(self):
+        out = np.zeros(self.shape)
+        lib().or_get_state(self.h, _dp(out))
+        return out
+
+    def set_state(self, c):
+        c = np.ascontiguousarray(c, dtype=np.float64)
+        lib().or_set_state(self.h, _dp(c))
+
+    def rhs(self, t):
+        out = np.zeros(self.shape)
+        lib().or_rhs(self.h, t, _dp(out))
+        return out
+
+    def cfl_dt(self, cfl):
+        return lib().or_cfl_dt(self.h, cfl)
+
+    def step(self, t, dt):
+        return lib().or_step(self.h, t, dt)
+
+    def run(self, t0, tend, cfl, nsteps):
+        n = ctypes.c_int()
+        t = lib().or_run(self.h, t0, tend, cfl, nsteps, ctypes.byref(n))
+        return t, n.value
+
+    def l2_error(self, t, field=0):
+        return lib().or_l2_error(self.h, t, field)
+
+    def close(self):
+        if self.h:
+            lib().or_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -1,0 +1,176 @@
+"""GPU parity: the CUDA path through the C ABI against DG-Parallel's own output
+(golden fixtures) and against the C oracle on the same seeded meshes.
+
+Tolerances are relative (max |a - b| / max |b|):
+* FP64 vs the oracle: 1e-12 on states and on the assembled RHS (the two differ
+  only in summation order and FMA contraction).
+* FP64 vs DG-Parallel: the per-order REF_TOL of tests/cases.py (the reference's
+  truncated basis tables dominate).
+* mixed (FP32) vs the oracle: 2e-5 on states after the steps taken.
+"""
+import os
+
+import numpy as np
+import pytest
+
+import dgp
+from dgp import meshgen
+from cases import (GOLDEN_CASES, PULSE3D, REF_RHS_TOL, REF_TOL, SCALAR2D, SCALAR3D, SINE, TM110,
+                   VORTEX, golden, rel)
+from oracle_bind import Oracle
+
+pytestmark = pytest.mark.gpu
+
+FP64_TOL = 1e-12
+
+
+def solver_for(msh, law, flux, field, order, prm, precision=dgp.FP64):
+    mesh = dgp.Mesh.from_msh(msh)
+    lw = dgp.Law(law, flux, field, prm)
+    return dgp.Solver(mesh, lw, order, precision)
+
+
+@pytest.mark.parametrize("name", sorted(GOLDEN_CASES))
+def test_gpu_matches_reference_golden(name):
+    law, flux, field, order, prm = GOLDEN_CASES[name]
+    msh, g = golden(name)
+    s = solver_for(msh, law, flux, field, order, prm)
+    E = s.ncells
+    tol = REF_TOL[order]
+    assert rel(s.get_state().reshape(E, -1), g["states"][0]) < tol
+    assert rel(s.rhs(0.0).reshape(E, -1), g["rhs"]) < REF_RHS_TOL[order]
+    t = 0.0
+    for k in range(1, int(g["steps"]) + 1):
+        dt = s.cfl_dt(0.1)
+        assert abs(dt - g["log"][k - 1, 1]) <= max(1e-13, tol) * dt
+        resid = s.step(t, dt)
+        t += dt
+        assert rel(s.get_state().reshape(E, -1), g["states"][k]) < tol
+        assert abs(resid - g["log"][k - 1, 3]) <= 1e-8 * g["log"][k - 1, 3]
+
+
+def _tri(tmp_path, n, box=(0.0, 1.0), seed=1, tag=1):
+    m = meshgen.tri_square(n, n, box[0], box[1], box[0], box[1], seed=seed, boundary_tag=tag)
+    p = str(tmp_path / f"tri{n}_{seed}_{tag}.msh")
+    meshgen.write_msh_v1(m, p)
+    return p
+
+
+def _tet(tmp_path, n, seed=3, tag=1):
+    m = meshgen.tet_cube(n, seed=seed, boundary_tag=tag)
+    p = str(tmp_path / f"tet{n}_{seed}_{tag}.msh")
+    meshgen.write_msh_v1(m, p)
+    return p
+
+
+# (id, mesh kind, mesh size, law, flux, field, params, orders, boundary tag)
+ORACLE_CASES = [
+    ("scalar", "tri", 8, dgp.LAW_SCALAR, dgp.FLUX_UPWIND, dgp.FIELD_GAUSS, SCALAR2D, [0, 1, 2, 3, 4], 1),
+    ("euler_godunov", "trib", 8, dgp.LAW_EULER2D, dgp.FLUX_GODUNOV, dgp.FIELD_VORTEX, VORTEX, [1, 2, 3, 4], 1),
+    ("euler_roe", "trib", 8, dgp.LAW_EULER2D, dgp.FLUX_ROE, dgp.FIELD_VORTEX, VORTEX, [0, 1, 2, 3, 4], 1),
+    ("euler_llf", "trib", 8, dgp.LAW_EULER2D, dgp.FLUX_LLF, dgp.FIELD_VORTEX, VORTEX, [1, 2, 3, 4], 1),
+    ("euler_wall", "trib", 6, dgp.LAW_EULER2D, dgp.FLUX_ROE, dgp.FIELD_VORTEX, VORTEX, [2], 40000),
+    ("burgers_central", "tri", 8, dgp.LAW_BURGERS2D, dgp.FLUX_CENTRAL, dgp.FIELD_SINE, SINE, [1, 2, 3, 4], 1),
+    ("burgers_llf", "tri", 8, dgp.LAW_BURGERS2D, dgp.FLUX_LLF, dgp.FIELD_SINE, SINE, [1, 2, 3, 4], 1),
+    ("scalar3d", "tet", 3, dgp.LAW_SCALAR, dgp.FLUX_UPWIND, dgp.FIELD_GAUSS3D, SCALAR3D, [0, 1, 2, 3], 1),
+    ("euler3d", "tet", 3, dgp.LAW_EULER3D, dgp.FLUX_GODUNOV, dgp.FIELD_PULSE3D, PULSE3D, [1, 2, 3], 1),
+    ("maxwell3d_pec", "tet", 3, dgp.LAW_MAXWELL3D, dgp.FLUX_UPWIND, dgp.FIELD_TM110, TM110, [1, 2, 3], 40000),
+    ("maxwell3d_far", "tet", 3, dgp.LAW_MAXWELL3D, dgp.FLUX_UPWIND, dgp.FIELD_TM110, TM110, [2], 1),
+]
+PARAMS = [(c[0], o) for c in ORACLE_CASES for o in c[7]]
+
+
+@pytest.mark.parametrize("cid,order", PARAMS)
+def test_gpu_matches_oracle(tmp_path, cid, order):
+    case = next(c for c in ORACLE_CASES if c[0] == cid)
+    _, kind, n, law, flux, field, prm, _, tag = case
+    if kind == "tri":
+        msh = _tri(tmp_path, n, tag=tag)
+    elif kind == "trib":
+        msh = _tri(tmp_path, n, box=(0.0, 10.0), seed=2, tag=tag)
+    else:
+        msh = _tet(tmp_path, n, tag=tag)
+    o = Oracle(msh, law, flux, order, field, prm)
+    s = solver_for(msh, law, flux, field, order, prm)
+    E = s.ncells
+    assert rel(s.get_state(), o.state()) < FP64_TOL
+    assert rel(s.rhs(0.0), o.rhs(0.0)) < FP64_TOL
+    assert rel(s.rhs(0.37), o.rhs(0.37)) < FP64_TOL  # time-dependent boundary data
+    t = 0.0
+    for _ in range(4):
+        dt_g, dt_o = s.cfl_dt(0.1), o.cfl_dt(0.1)
+        assert abs(dt_g - dt_o) <= 1e-13 * dt_o
+        rg = s.step(t, dt_o)
+        ro = o.step(t, dt_o)
+        t += dt_o
+        assert rel(s.get_state(), o.state()) < FP64_TOL
+        assert abs(rg - ro) <= 1e-9 * ro + 1e-300
+    assert s.status()[0] == 0
+
+
+def test_run_device_loop_matches_oracle(tmp_path):
+    msh = _tri(tmp_path, 12, box=(0.0, 10.0), seed=2)
+    o = Oracle(msh, dgp.LAW_EULER2D, dgp.FLUX_ROE, 3, dgp.FIELD_VORTEX, VORTEX)
+    s = solver_for(msh, dgp.LAW_EULER2D, dgp.FLUX_ROE, dgp.FIELD_VORTEX, 3, VORTEX)
+    tg, ng = s.run(0.0, 0.05, 0.1)
+    to, no = o.run(0.0, 0.05, 0.1, 0)
+    assert ng == no and tg == to
+    assert rel(s.get_state(), o.state()) < 1e-11
+    # fixed step count, continuing from the current state and time
+    tg2, ng2 = s.run(tg, 0.0, 0.1, 7)
+    to2, no2 = o.run(to, 0.0, 0.1, 7)
+    assert ng2 == no2 == 7 and abs(tg2 - to2) <= 1e-15 * to2
+    assert rel(s.get_state(), o.state()) < 1e-11
+
+
+def test_mixed_precision_tracks_fp64(tmp_path):
+    msh = _tri(tmp_path, 8, box=(0.0, 10.0), seed=2)
+    o = Oracle(msh, dgp.LAW_EULER2D, dgp.FLUX_ROE, 3, dgp.FIELD_VORTEX, VORTEX)
+    s = solver_for(msh, dgp.LAW_EULER2D, dgp.FLUX_ROE, dgp.FIELD_VORTEX, 3, VORTEX, dgp.MIXED)
+    assert rel(s.get_state(), o.state()) < 1e-6
+    t = 0.0
+    for _ in range(5):
+        dt = o.cfl_dt(0.1)
+        s.step(t, dt)
+        o.step(t, dt)
+        t += dt
+    assert rel(s.get_state(), o.state()) < 2e-5
+
+
+def test_state_roundtrip_and_totals(tmp_path):
+    msh = _tri(tmp_path, 8, box=(0.0, 10.0), seed=2)
+    s = solver_for(msh, dgp.LAW_EULER2D, dgp.FLUX_ROE, dgp.FIELD_VORTEX, 2, VORTEX)
+    c = np.random.default_rng(0).standard_normal(s.shape)
+    s.set_state(c)
+    assert np.array_equal(s.get_state(), c)
+    s.project(0.0)
+    tot0 = s.totals()
+    # the vortex moves (1,1); mass changes only through the boundary fluxes
+    assert abs(tot0[0] - 100.0) < 0.1
+    o = Oracle(msh, dgp.LAW_EULER2D, dgp.FLUX_ROE, 2, dgp.FIELD_VORTEX, VORTEX)
+    assert abs(s.l2_error(0.0, 0) - o.l2_error(0.0, 0)) <= 1e-12 * o.l2_error(0.0, 0)
+
+
+def test_device_pointer_state(tmp_path):
+    torch = pytest.importorskip("torch")
+    msh = _tri(tmp_path, 6)
+    s = solver_for(msh, dgp.LAW_SCALAR, dgp.FLUX_UPWIND, dgp.FIELD_GAUSS, 2, SCALAR2D)
+    host = s.get_state()
+    buf = torch.zeros(host.size, dtype=torch.float64, device="cuda")
+    s.get_state_device(buf.data_ptr())
+    torch.cuda.synchronize()
+    assert np.array_equal(buf.cpu().numpy().reshape(s.shape), host)
+    buf2 = buf * 2.0
+    s.set_state_device(buf2.data_ptr())
+    assert np.array_equal(s.get_state(), 2.0 * host)
+
+
+def test_unsupported_and_invalid(tmp_path):
+    msh = _tri(tmp_path, 4)
+    mesh = dgp.Mesh.from_msh(msh)
+    with pytest.raises(dgp.DGPError) as e:
+        dgp.Solver(mesh, dgp.Law(dgp.LAW_EULER3D, dgp.FLUX_GODUNOV, dgp.FIELD_PULSE3D, PULSE3D), 2)
+    assert e.value.code == -3
+    with pytest.raises(dgp.DGPError) as e:
+        dgp.Solver(mesh, dgp.Law(dgp.LAW_SCALAR, dgp.FLUX_UPWIND, dgp.FIELD_GAUSS, SCALAR2D), 7)
+    assert e.value.code == -3
