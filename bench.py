@@ -171,11 +171,15 @@ def main():
     ap.add_argument("--impl", default="dgp", choices=["dgp", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--e2e-steps", type=int, default=20)
+    ap.add_argument("--profile-case", choices=["fp64", "mixed"], default=None,
+                    help="only set up the workload and run --warmup + --steps steps (for ncu)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
     if args.impl == "reference":
         return run_reference_arm(args)
+    if args.profile_case:
+        return profile_case(args)
 
     import numpy as np
     import torch
@@ -322,6 +326,20 @@ def main():
         r["solver"].close()
     if dist is not None:
         dist.destroy_process_group()
+    return 0
+
+
+def profile_case(args):
+    """The bench workload alone: setup, --warmup steps, then --steps steps."""
+    import dgp
+    m = make_mesh()
+    mesh = dgp.Mesh.from_arrays(2, m.vertices, m.cells, 100, m.bfaces, m.btags)
+    law = dgp.Law(dgp.LAW_EULER2D, dgp.FLUX_ROE, dgp.FIELD_VORTEX, vortex_params())
+    s = dgp.Solver(mesh, law, 3, dgp.FP64 if args.profile_case == "fp64" else dgp.MIXED)
+    t, _ = s.run(0.0, 0.0, 0.1, args.warmup)
+    t, n = s.run(t, 0.0, 0.1, args.steps)
+    s.synchronize()
+    print(f"profile case {args.profile_case}: {n} steps, t = {t:.6e}")
     return 0
 
 

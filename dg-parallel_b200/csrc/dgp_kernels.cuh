@@ -41,9 +41,20 @@ struct Cfg {
   static constexpr int NLF = DIM + 1;
   static constexpr int NPERM = DIM == 2 ? 2 : 6;
   static constexpr int MNP = M * NP;
-  static constexpr int BLOCK = 256;
-  static constexpr int TE_RAW = 1024 / MNP;
-  static constexpr int TE = TE_RAW < 4 ? 4 : (TE_RAW > 64 ? 64 : TE_RAW);
+  static constexpr int NS = NLF * NQF;   // face points of a cell (lift length)
+  static constexpr int KV = NQ * DIM;    // volume contraction length
+  // element kernel: one thread per (cell, field) row of the tile, all modes of
+  // the row in registers; TE cells per CTA, capped by a shared-memory budget
+  static constexpr int BLOCK = 128;
+  static constexpr int NV = DIM == 2 ? 4 : 1;  // states of the CFL (mean + vertices)
+  static constexpr int CELL_BYTES =
+      (int)sizeof(T) * (MNP + KV * M + NS * M) + 8 * (NV + DIM * DIM + 1);
+  static constexpr int TE_SMEM = (96 * 1024) / CELL_BYTES;
+  static constexpr int TE_ROWS = BLOCK / M;
+  static constexpr int TE = TE_SMEM < TE_ROWS ? (TE_SMEM < 1 ? 1 : TE_SMEM) : TE_ROWS;
+  static constexpr int ROWS = TE * M;
+  static constexpr int LDR = ROWS | 1;   // leading dimension of the [k][row] operands
+  static constexpr int EG = BLOCK / NQ;   // cells processed concurrently in the volume phase
   static constexpr int FACE_BLOCK = 128;
 };
 
@@ -265,140 +276,6 @@ __device__ __forceinline__ double block_sum(double v, double* red) {
 }
 
 // -----------------------------------------------------------------------------
-template <class K>
-__global__ void __launch_bounds__(K::BLOCK) elem_kernel(StageArgs<typename K::T> a) {
-  using T = typename K::T;
-  constexpr int M = K::M, NP = K::NP, NQ = K::NQ, NQF = K::NQF, DIM = K::DIM, TE = K::TE;
-  constexpr int MNP = K::MNP, NS = K::NLF * NQF;
-  if (a.ctl->done) return;
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  T* sC = reinterpret_cast<T*>(smem_raw);        // TE x MNP
-  T* sG = sC + TE * MNP;                          // TE x NQ x M x DIM
-  T* sS = sG + TE * NQ * M * DIM;                 // TE x NS x M
-  T* sPhi = sS + TE * NS * M;                     // NQ x NP
-  T* sDphi = sPhi + NQ * NP;                      // NQ x DIM x NP
-  T* sPhif = sDphi + NQ * DIM * NP;               // NS x NP
-  T* sQw = sPhif + NS * NP;                       // NQ
-  __shared__ double red[K::BLOCK / 32];
-  __shared__ bool amLast;
-
-  const int e0 = blockIdx.x * TE;
-  const int ne = min(TE, a.mesh.E - e0);
-  for (int i = threadIdx.x; i < NQ * NP; i += K::BLOCK) sPhi[i] = a.tab.phi[i];
-  for (int i = threadIdx.x; i < NQ * DIM * NP; i += K::BLOCK) sDphi[i] = a.tab.dphi[i];
-  for (int i = threadIdx.x; i < NS * NP; i += K::BLOCK) sPhif[i] = a.tab.phif[i];
-  for (int i = threadIdx.x; i < NQ; i += K::BLOCK) sQw[i] = a.tab.qw[i];
-  {
-    const T* src = a.C + (size_t)e0 * MNP;
-    for (int i = threadIdx.x; i < ne * MNP; i += K::BLOCK) sC[i] = src[i];
-    const T* ss = a.slots + (size_t)e0 * NS * M;
-    for (int i = threadIdx.x; i < ne * NS * M; i += K::BLOCK) sS[i] = ss[i];
-  }
-  __syncthreads();
-
-  // volume: per (cell, point) interpolate, flux, map to reference directions
-  for (int it = threadIdx.x; it < ne * NQ; it += K::BLOCK) {
-    const int e = it / NQ, q = it - (it / NQ) * NQ;
-    const T* c = sC + e * MNP;
-    T U[M];
-#pragma unroll
-    for (int j = 0; j < M; ++j) {
-      T acc = 0;
-#pragma unroll
-      for (int k = 0; k < NP; ++k) acc += sPhi[q * NP + k] * c[j * NP + k];
-      U[j] = acc;
-    }
-    if (!is_physical<K::LAW, T>(a.law, U)) flag_nonphysical(a.status, e0 + e);
-    T F[M][DIM];
-    volume_flux<K::LAW, DIM, T>(a.law, U, F);
-    const T* Ji = a.mesh.jinv + (size_t)(e0 + e) * DIM * DIM;
-    T J[DIM * DIM];
-#pragma unroll
-    for (int i = 0; i < DIM * DIM; ++i) J[i] = Ji[i];
-    const T jw = a.mesh.detj[e0 + e] * sQw[q];
-    T* g = sG + (e * NQ + q) * M * DIM;
-#pragma unroll
-    for (int j = 0; j < M; ++j)
-#pragma unroll
-      for (int r = 0; r < DIM; ++r) {
-        T acc = 0;
-#pragma unroll
-        for (int i = 0; i < DIM; ++i) acc += F[j][i] * J[i * DIM + r];
-        g[j * DIM + r] = acc * jw;
-      }
-  }
-  __syncthreads();
-
-  // contraction + lift + inverse mass + stage combination, one coefficient per item
-  double rsum = 0.0;
-  const double dt = a.ctl->dt;
-  for (int it = threadIdx.x; it < ne * MNP; it += K::BLOCK) {
-    const int e = it / MNP, jk = it - (it / MNP) * MNP;
-    const int j = jk / NP, k = jk - (jk / NP) * NP;
-    T acc = 0;
-    const T* g = sG + e * NQ * M * DIM + j * DIM;
-#pragma unroll
-    for (int q = 0; q < NQ; ++q)
-#pragma unroll
-      for (int r = 0; r < DIM; ++r) acc += g[q * M * DIM + r] * sDphi[(q * DIM + r) * NP + k];
-    const T* s = sS + e * NS * M + j;
-#pragma unroll
-    for (int p = 0; p < NS; ++p) acc += s[p * M] * sPhif[p * NP + k];
-    const size_t gi = (size_t)(e0 + e) * MNP + jk;
-    if (a.stage == 0) {
-      a.Cout[gi] = acc;
-      continue;
-    }
-    const T dtj = (T)(dt / (double)a.mesh.detj[e0 + e]);
-    const T c = sC[it];
-    T out;
-    if (a.stage == 1) {
-      a.U0out[gi] = c;
-      out = c + acc * dtj;
-    } else if (a.stage == 2) {
-      out = (T)0.25 * (c + acc * dtj + (T)3. * a.U0[gi]);
-    } else {
-      const T u0 = a.U0[gi];
-      out = ((T)2.0 * (c + acc * dtj) + u0) / (T)3.0;
-      const double d = (double)out - (double)u0;
-      rsum += d * d;
-    }
-    a.Cout[gi] = out;
-    sC[it] = out;
-  }
-  if (a.stage != 3) return;
-
-  // stage 3: residual partial, and the CFL step of the next step
-  rsum = block_sum<K::BLOCK>(rsum, red);
-  if (threadIdx.x == 0) a.partials[blockIdx.x] = rsum;
-  if (a.fuse_cfl) {
-    double dtl = 1e300;
-    if (threadIdx.x < ne) dtl = cell_dt<K>(a, sC + threadIdx.x * MNP, e0 + threadIdx.x, a.ctl->cfl);
-    dtl = block_min<K::BLOCK>(dtl, red);
-    if (threadIdx.x == 0) atomicMin(&a.ctl->dtmin_bits, (unsigned long long)__double_as_longlong(dtl));
-  }
-  if (threadIdx.x == 0) {
-    __threadfence();
-    unsigned v = atomicAdd(&a.ctl->blocks_done, 1u);
-    amLast = (v == gridDim.x - 1);
-  }
-  __syncthreads();
-  if (amLast && threadIdx.x == 0) {
-    __threadfence();
-    double r = 0.0;
-    for (unsigned b = 0; b < gridDim.x; ++b) r += ((volatile double*)a.partials)[b];
-    TimeCtl* c = a.ctl;
-    c->resid = r;
-    c->blocks_done = 0;
-    c->t = c->t + c->dt;
-    c->steps += 1;
-    if (a.fuse_cfl) {
-      unsigned long long bits = atomicExch(&c->dtmin_bits, 0x7FF0000000000000ull);
-      ctl_finalize(c, __longlong_as_double((long long)bits));
-    }
-  }
-}
-
 // -----------------------------------------------------------------------------
 template <class K>
 __global__ void __launch_bounds__(256) cfl_kernel(StageArgs<typename K::T> a) {
@@ -505,12 +382,5 @@ __global__ void __launch_bounds__(256) totals_kernel(StageArgs<typename K::T> a,
   }
 }
 
-template <class K>
-constexpr size_t elem_smem_bytes() {
-  using T = typename K::T;
-  constexpr int NS = K::NLF * K::NQF;
-  return sizeof(T) * (size_t)(K::TE * K::MNP + K::TE * K::NQ * K::M * K::DIM + K::TE * NS * K::M +
-                              K::NQ * K::NP + K::NQ * K::DIM * K::NP + NS * K::NP + K::NQ);
-}
 
 }  // namespace dgp

@@ -124,14 +124,15 @@ __device__ __forceinline__ void volume_flux(const LawParams& lp, const T* Q, T (
     F[4][0] = q14; F[4][1] = q24; F[4][2] = q44 + p;
     T qq = invrho * (Q[3] + p);
     F[3][0] = Q[1] * qq; F[3][1] = Q[2] * qq; F[3][2] = Q[4] * qq;
-  } else {  // 3D Maxwell, eps = mu = 1: F_E e_i = -(e_i x H), F_H e_i = e_i x E
+  } else {  // 3D Maxwell, eps = mu = 1: dE/dt = curl H, dH/dt = -curl E, so
+            // F_E e_i = -(e_i x H) and F_H e_i = e_i x E
     const T *E = Q, *H = Q + 3;
-    F[0][0] = 0;     F[0][1] = H[2];  F[0][2] = -H[1];
-    F[1][0] = -H[2]; F[1][1] = 0;     F[1][2] = H[0];
-    F[2][0] = H[1];  F[2][1] = -H[0]; F[2][2] = 0;
-    F[3][0] = 0;     F[3][1] = -E[2]; F[3][2] = E[1];
-    F[4][0] = E[2];  F[4][1] = 0;     F[4][2] = -E[0];
-    F[5][0] = -E[1]; F[5][1] = E[0];  F[5][2] = 0;
+    F[0][0] = 0;     F[0][1] = -H[2]; F[0][2] = H[1];
+    F[1][0] = H[2];  F[1][1] = 0;     F[1][2] = -H[0];
+    F[2][0] = -H[1]; F[2][1] = H[0];  F[2][2] = 0;
+    F[3][0] = 0;     F[3][1] = E[2];  F[3][2] = -E[1];
+    F[4][0] = -E[2]; F[4][1] = 0;     F[4][2] = E[0];
+    F[5][0] = E[1];  F[5][1] = -E[0]; F[5][2] = 0;
   }
 }
 

@@ -2,13 +2,14 @@
 // instantiation units).
 #pragma once
 
+#include "dgp_elem.cuh"
 #include "dgp_solver.h"
 
 namespace dgp {
 
 template <class K>
 cudaError_t ops_prepare() {
-  const size_t smem = elem_smem_bytes<K>();
+  const size_t smem = elem_kernel_smem<K>();
   if (smem > 48 * 1024)
     return cudaFuncSetAttribute(elem_kernel<K>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 static_cast<int>(smem));
@@ -42,7 +43,7 @@ void ops_face(const DeviceBuffers& b, int stage, double time_factor, cudaStream_
 template <class K>
 void ops_elem(const DeviceBuffers& b, int stage, int fuse_cfl, cudaStream_t st) {
   auto a = stage_args<K>(b, stage, 0.0, fuse_cfl);
-  elem_kernel<K><<<ops_grid_elem<K>(b.E), K::BLOCK, elem_smem_bytes<K>(), st>>>(a);
+  elem_kernel<K><<<ops_grid_elem<K>(b.E), K::BLOCK, elem_kernel_smem<K>(), st>>>(a);
 }
 
 template <class K>
@@ -86,7 +87,7 @@ Ops make_ops() {
   o.NQF = K::NQF;
   o.TE = K::TE;
   o.elem_block = K::BLOCK;
-  o.elem_smem = elem_smem_bytes<K>();
+  o.elem_smem = elem_kernel_smem<K>();
   o.tsize = sizeof(typename K::T);
   o.precision = sizeof(typename K::T) == 8 ? DGP_PRECISION_FP64 : DGP_PRECISION_MIXED;
   o.prepare = &ops_prepare<K>;

@@ -2,8 +2,9 @@
 (golden fixtures) and against the C oracle on the same seeded meshes.
 
 Tolerances are relative (max |a - b| / max |b|):
-* FP64 vs the oracle: 1e-12 on states and on the assembled RHS (the two differ
-  only in summation order and FMA contraction).
+* FP64 vs the oracle: 1e-12 on states, 1e-11 on the assembled RHS (whose
+  volume and face parts cancel); the two differ only in summation order and
+  FMA contraction.
 * FP64 vs DG-Parallel: the per-order REF_TOL of tests/cases.py (the reference's
   truncated basis tables dominate).
 * mixed (FP32) vs the oracle: 2e-5 on states after the steps taken.
@@ -22,6 +23,7 @@ from oracle_bind import Oracle
 pytestmark = pytest.mark.gpu
 
 FP64_TOL = 1e-12
+RHS_TOL = 1e-11
 
 
 def solver_for(msh, law, flux, field, order, prm, precision=dgp.FP64):
@@ -94,8 +96,8 @@ def test_gpu_matches_oracle(tmp_path, cid, order):
     s = solver_for(msh, law, flux, field, order, prm)
     E = s.ncells
     assert rel(s.get_state(), o.state()) < FP64_TOL
-    assert rel(s.rhs(0.0), o.rhs(0.0)) < FP64_TOL
-    assert rel(s.rhs(0.37), o.rhs(0.37)) < FP64_TOL  # time-dependent boundary data
+    assert rel(s.rhs(0.0), o.rhs(0.0)) < RHS_TOL
+    assert rel(s.rhs(0.37), o.rhs(0.37)) < RHS_TOL  # time-dependent boundary data
     t = 0.0
     for _ in range(4):
         dt_g, dt_o = s.cfl_dt(0.1), o.cfl_dt(0.1)
@@ -145,8 +147,15 @@ def test_state_roundtrip_and_totals(tmp_path):
     assert np.array_equal(s.get_state(), c)
     s.project(0.0)
     tot0 = s.totals()
-    # the vortex moves (1,1); mass changes only through the boundary fluxes
-    assert abs(tot0[0] - 100.0) < 0.1
+    # the projection conserves the cell integrals: total mass = integral of the
+    # vortex density over [0,10]^2 (free stream 1 minus the core deficit)
+    n = 2000
+    x = (np.arange(n) + 0.5) * (10.0 / n)
+    X, Y = np.meshgrid(x, x)
+    r2 = (X - 5.0) ** 2 + (Y - 5.0) ** 2
+    T = 1.0 - 0.4 * 25.0 / (8.0 * 1.4 * np.pi ** 2) * np.exp(1.0 - r2)
+    mass = float((T ** 2.5).sum() * (10.0 / n) ** 2)
+    assert abs(tot0[0] - mass) < 1e-4 * mass
     o = Oracle(msh, dgp.LAW_EULER2D, dgp.FLUX_ROE, 2, dgp.FIELD_VORTEX, VORTEX)
     assert abs(s.l2_error(0.0, 0) - o.l2_error(0.0, 0)) <= 1e-12 * o.l2_error(0.0, 0)
 
