@@ -15,6 +15,7 @@
 
 #include "../../include/dgp.h"
 #include "dgp_host.h"
+#include "dgp_handles.h"
 #include "dgp_solver.h"
 
 namespace dgp {
@@ -24,7 +25,6 @@ std::map<OpsKey, Ops>& ops_registry() {
   return r;
 }
 
-namespace {
 thread_local std::string g_err;
 
 int fail(int code, const std::string& msg) {
@@ -32,13 +32,7 @@ int fail(int code, const std::string& msg) {
   return code;
 }
 
-#define DGP_CUDA(call)                                                                    \
-  do {                                                                                    \
-    cudaError_t e_ = (call);                                                              \
-    if (e_ != cudaSuccess)                                                                \
-      return fail(DGP_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_));      \
-  } while (0)
-
+namespace {
 void ensure_registry() {
   static std::once_flag once;
   std::call_once(once, [] {
@@ -85,70 +79,6 @@ uint64_t spread3(uint32_t x) {
 
 using namespace dgp;
 
-struct dgp_mesh_s {
-  HostMesh m;
-};
-
-struct dgp_law_s {
-  int kind, flux, field;
-  double p[DGP_NPARAMS];
-};
-
-struct dgp_solver_s {
-  HostMesh mesh;
-  RefTables tab;
-  Ops ops;
-  DeviceBuffers b;
-  int law = 0, flux = 0, order = 0, precision = 0, limiter = 0, device = 0;
-  cudaStream_t stream = nullptr;
-  std::vector<int> i2f, f2i;  // internal <-> file cell order
-  int* d_i2f = nullptr;
-  int* d_f2i = nullptr;
-  std::vector<void*> allocs;
-  cudaGraphExec_t graph = nullptr;
-  int graph_steps = 0;
-  TimeCtl* h_ctl = nullptr;  // pinned, 2 entries
-  ~dgp_solver_s() {
-    if (graph) cudaGraphExecDestroy(graph);
-    for (void* p : allocs) cudaFree(p);
-    if (h_ctl) cudaFreeHost(h_ctl);
-    if (stream) cudaStreamDestroy(stream);
-  }
-  template <typename U>
-  int alloc(U** p, size_t count) {
-    void* v = nullptr;
-    if (count == 0) count = 1;
-    cudaError_t e = cudaMalloc(&v, count * sizeof(U));
-    if (e != cudaSuccess) return fail(DGP_ERR_NOMEM, std::string("cudaMalloc: ") + cudaGetErrorString(e));
-    allocs.push_back(v);
-    *p = static_cast<U*>(v);
-    return DGP_OK;
-  }
-  // upload FP64 host data as the hot-path type
-  int upload_t(void** dst, const std::vector<double>& src) {
-    const size_t n = src.size();
-    if (ops.tsize == 8) {
-      double* d;
-      if (int rc = alloc(&d, n)) return rc;
-      DGP_CUDA(cudaMemcpy(d, src.data(), n * 8, cudaMemcpyHostToDevice));
-      *dst = d;
-    } else {
-      std::vector<float> f(src.begin(), src.end());
-      float* d;
-      if (int rc = alloc(&d, n)) return rc;
-      DGP_CUDA(cudaMemcpy(d, f.data(), n * 4, cudaMemcpyHostToDevice));
-      *dst = d;
-    }
-    return DGP_OK;
-  }
-  template <typename U>
-  int upload(U** dst, const std::vector<U>& src) {
-    if (int rc = alloc(dst, src.size())) return rc;
-    DGP_CUDA(cudaMemcpy(*dst, src.data(), src.size() * sizeof(U), cudaMemcpyHostToDevice));
-    return DGP_OK;
-  }
-  size_t state_count() const { return static_cast<size_t>(b.E) * b.M * b.NP; }
-};
 
 extern "C" {
 

@@ -1,0 +1,91 @@
+// Opaque handle types behind the C ABI (include/dgp.h) and the error helpers
+// shared by the translation units that implement it.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <string>
+#include <vector>
+
+#include "../../include/dgp.h"
+#include "dgp_host.h"
+#include "dgp_solver.h"
+
+namespace dgp {
+// records `msg` as the calling thread's dgp_last_error() and returns `code`
+int fail(int code, const std::string& msg);
+}  // namespace dgp
+
+#define DGP_CUDA(call)                                                               \
+  do {                                                                               \
+    cudaError_t e_ = (call);                                                         \
+    if (e_ != cudaSuccess)                                                           \
+      return ::dgp::fail(DGP_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
+  } while (0)
+
+using dgp::fail;
+
+struct dgp_mesh_s {
+  dgp::HostMesh m;
+};
+
+struct dgp_law_s {
+  int kind, flux, field;
+  double p[DGP_NPARAMS];
+};
+
+struct dgp_solver_s {
+  dgp::HostMesh mesh;
+  dgp::RefTables tab;
+  dgp::Ops ops;
+  dgp::DeviceBuffers b;
+  int law = 0, flux = 0, order = 0, precision = 0, limiter = 0, device = 0;
+  cudaStream_t stream = nullptr;
+  std::vector<int> i2f, f2i;  // internal <-> file cell order
+  int* d_i2f = nullptr;
+  int* d_f2i = nullptr;
+  std::vector<void*> allocs;
+  cudaGraphExec_t graph = nullptr;
+  int graph_steps = 0;
+  dgp::TimeCtl* h_ctl = nullptr;  // pinned, 2 entries
+  ~dgp_solver_s() {
+    if (graph) cudaGraphExecDestroy(graph);
+    for (void* p : allocs) cudaFree(p);
+    if (h_ctl) cudaFreeHost(h_ctl);
+    if (stream) cudaStreamDestroy(stream);
+  }
+  template <typename U>
+  int alloc(U** p, size_t count) {
+    void* v = nullptr;
+    if (count == 0) count = 1;
+    cudaError_t e = cudaMalloc(&v, count * sizeof(U));
+    if (e != cudaSuccess) return fail(DGP_ERR_NOMEM, std::string("cudaMalloc: ") + cudaGetErrorString(e));
+    allocs.push_back(v);
+    *p = static_cast<U*>(v);
+    return DGP_OK;
+  }
+  // upload FP64 host data as the hot-path type
+  int upload_t(void** dst, const std::vector<double>& src) {
+    const size_t n = src.size();
+    if (ops.tsize == 8) {
+      double* d;
+      if (int rc = alloc(&d, n)) return rc;
+      DGP_CUDA(cudaMemcpy(d, src.data(), n * 8, cudaMemcpyHostToDevice));
+      *dst = d;
+    } else {
+      std::vector<float> f(src.begin(), src.end());
+      float* d;
+      if (int rc = alloc(&d, n)) return rc;
+      DGP_CUDA(cudaMemcpy(d, f.data(), n * 4, cudaMemcpyHostToDevice));
+      *dst = d;
+    }
+    return DGP_OK;
+  }
+  template <typename U>
+  int upload(U** dst, const std::vector<U>& src) {
+    if (int rc = alloc(dst, src.size())) return rc;
+    DGP_CUDA(cudaMemcpy(*dst, src.data(), src.size() * sizeof(U), cudaMemcpyHostToDevice));
+    return DGP_OK;
+  }
+  size_t state_count() const { return static_cast<size_t>(b.E) * b.M * b.NP; }
+};
