@@ -131,6 +131,17 @@ int dgp_solver_stream(dgp_solver s, void** stream);
  * the element kernel of an inner stage and the element kernel of the last
  * stage (with the fused CFL reduction), over `iters` launches each: ms[3] */
 int dgp_profile_kernels(dgp_solver s, int iters, float* ms);
+/* Assembled right-hand side that allocates no device memory; no counterpart in
+ * DG-Parallel.  For callers that cannot call cudaMalloc when they need a RHS
+ * (device memory owned by another allocator, or no tolerance for the
+ * synchronisation an allocation implies).  dev_state and dev_rhs are device
+ * buffers, FP64 [cell][field][mode] in file order, like dgp_rhs's output.  The
+ * intermediates live in a 32 MiB static device array that every GPU loading
+ * the library holds until exit; meshes that need more return DGP_ERR_INVALID.
+ * Calls share that array: calls that overlap on the GPU race.  The first call
+ * on a device looks up the array's device address (host-side setup), so make
+ * it before any stream capture.  Returns after the solver's stream is idle. */
+int dgp_rhs_noalloc(dgp_solver s, const double* dev_state, double t, double* dev_rhs);
 
 #ifdef __cplusplus
 }
