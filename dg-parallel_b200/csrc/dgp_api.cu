@@ -349,18 +349,27 @@ int dgp_solver_create(dgp_mesh mh, dgp_law law, int order, int precision, int li
       (rc = s->upload(&b.ephi, t.ephi)) || (rc = s->upload(&s->d_i2f, s->i2f)) ||
       (rc = s->upload(&s->d_f2i, s->f2i)))
     return bail(rc);
+  {
+    std::vector<double> blob(s->ops.blob_elems);
+    s->ops.fill_blob(t.dphi.data(), t.phif.data(), t.phi.data(), t.qw.data(), blob.data());
+    if ((rc = s->upload_t(&b.blob, blob))) return bail(rc);
+    b.blob_bytes = static_cast<int>(s->ops.blob_elems * s->ops.tsize);
+  }
   b.nqe = t.nqe;
   b.phi0 = t.phi0;
   b.law.field = law->field;
   for (int i = 0; i < DGP_NPARAMS; ++i) b.law.p[i] = law->p[i];
 
   const size_t nstate = s->state_count();
-  const size_t nslot = static_cast<size_t>(E) * t.nlf * t.nqf * b.M;
+  // slots are tile-transposed over whole tiles of TE cells; state buffers get
+  // 256 bytes of tail so the bulk copy of the last tile may round up to 16 bytes
+  const size_t ntiles = (static_cast<size_t>(E) + s->ops.TE - 1) / s->ops.TE;
+  const size_t nslot = ntiles * s->ops.TE * t.nlf * t.nqf * b.M;
   unsigned char *C, *U0, *slots, *rhs, *scratch;
   const size_t ts = s->ops.tsize;
-  if ((rc = s->alloc(&C, nstate * ts)) || (rc = s->alloc(&U0, nstate * ts)) ||
-      (rc = s->alloc(&slots, nslot * ts)) || (rc = s->alloc(&rhs, nstate * ts)) ||
-      (rc = s->alloc(&scratch, nstate * 8)))
+  if ((rc = s->alloc(&C, nstate * ts + 256)) || (rc = s->alloc(&U0, nstate * ts + 256)) ||
+      (rc = s->alloc(&slots, nslot * ts)) || (rc = s->alloc(&rhs, nstate * ts + 256)) ||
+      (rc = s->alloc(&scratch, nstate * 8 + 256)))
     return bail(rc);
   b.C = C;
   b.U0 = U0;
@@ -594,6 +603,9 @@ int dgp_status(dgp_solver s, int* nonphysical, int* first_bad_cell) {
   Status st;
   DGP_CUDA(cudaMemcpyAsync(&st, s->b.status, sizeof(Status), cudaMemcpyDeviceToHost, s->stream));
   DGP_CUDA(cudaStreamSynchronize(s->stream));
+  if (st.timeouts > 0)
+    return fail(DGP_ERR_CUDA, "a bounded wait on a bulk copy gave up in " + std::to_string(st.timeouts) +
+                                  " CTA(s); results of that launch are incomplete");
   if (nonphysical) *nonphysical = st.nonphysical;
   if (first_bad_cell) *first_bad_cell = st.nonphysical ? s->i2f[std::min(st.first_bad, s->b.E - 1)] : -1;
   Status st0{0, INT32_MAX};

@@ -2,23 +2,33 @@
 // slots + inverse mass + SSP-RK3 combination for a tile of TE cells, with the
 // last stage's CFL and residual reductions fused in.
 //
+// Staging: one elected thread issues two bulk (1D TMA) copies completed on an
+// mbarrier -- the reference tables (basis at the volume points, reference
+// gradients, face traces, weights: one blob already in shared-memory layout)
+// and the tile's coefficients (contiguous [cell][field][mode]).
+//
 // Work mapping (BLOCK = 128 threads):
 //   volume   thread (q, g) owns quadrature point q and keeps phi(q,:) in
 //            registers; it walks cells g, g+EG, ... of the tile: interpolate the
-//            state (DGCell::interpolate, DGCell.h:217-227), evaluate the flux
-//            (ConservationLaw::Fi) and map it to reference directions with the
-//            cell's J^{-1} |J| w, writing G[(q,r)][(cell,field)].
+//            state (DGCell::interpolate, DGCell.h:217-227) with 16-byte reads of
+//            the cell's rows, evaluate the flux (ConservationLaw::Fi) and map it
+//            to reference directions with the cell's J^{-1} |J| w, writing
+//            G[(cell,field)][(q,r)] (odd row stride).  (A thread-per-row
+//            interpolation with broadcast table rows measured slower: as many
+//            shared loads plus a round trip of the point states.)
 //   contract thread = one (cell, field) row; all modes of the row accumulate in
-//            registers: R[row][k] = sum_(q,r) G[(q,r)][row] dphi[(q,r)][k]
+//            registers: R[row][k] = sum_(q,r) G[row][(q,r)] dphi[(q,r)][k]
 //                                  + sum_s S[s][row] phi_face[s][k];
-//            every k-step reads one value of its own row and one table row that
-//            all lanes share (a broadcast), so shared-memory traffic per FMA is
-//            ~1/NP of a naive (row, mode) mapping.
+//            each k-step reads one value of the thread's own row and one table
+//            row all lanes share (a 16-byte broadcast); the face slots S come
+//            straight from global memory in their tile-transposed layout
+//            (row-coalesced), never staged.
 //   update   RungeKuttaTVD3::advanceInTime (TimeIntegrator.cc:838-990) for the
-//            row's modes, coalesced per row.
+//            row's modes in the reference's operation order.
 #pragma once
 
 #include "dgp_kernels.cuh"
+#include "dgp_tma.cuh"
 
 namespace dgp {
 
@@ -36,39 +46,60 @@ struct Padded {
   static constexpr int value = (N + V - 1) / V * V;
 };
 
+// N consecutive values from shared memory with the widest aligned vector
+// loads (p is aligned to N*sizeof(T) modulo 16)
 template <typename T, int N>
-__device__ __forceinline__ void load_row16(const T* __restrict__ p, T (&out)[N]) {
-  using V = typename Vec16<T>::type;
-  constexpr int W = Vec16<T>::N;
+__device__ __forceinline__ void load_vec(const T* __restrict__ p, T (&out)[N]) {
+  if constexpr ((N * sizeof(T)) % 16 == 0) {
+    using V = typename Vec16<T>::type;
+    constexpr int W = Vec16<T>::N;
 #pragma unroll
-  for (int i = 0; i < N / W; ++i) {
-    V v = reinterpret_cast<const V*>(p)[i];
-    if constexpr (W == 2) {
+    for (int i = 0; i < N / W; ++i) {
+      V v = reinterpret_cast<const V*>(p)[i];
+      if constexpr (W == 2) {
+        out[2 * i] = v.x;
+        out[2 * i + 1] = v.y;
+      } else {
+        out[4 * i] = v.x;
+        out[4 * i + 1] = v.y;
+        out[4 * i + 2] = v.z;
+        out[4 * i + 3] = v.w;
+      }
+    }
+  } else if constexpr (sizeof(T) == 4 && (N * sizeof(T)) % 8 == 0) {
+#pragma unroll
+    for (int i = 0; i < N / 2; ++i) {
+      float2 v = reinterpret_cast<const float2*>(p)[i];
       out[2 * i] = v.x;
       out[2 * i + 1] = v.y;
-    } else {
-      out[4 * i] = v.x;
-      out[4 * i + 1] = v.y;
-      out[4 * i + 2] = v.z;
-      out[4 * i + 3] = v.w;
     }
+  } else {
+#pragma unroll
+    for (int i = 0; i < N; ++i) out[i] = p[i];
   }
 }
 
 template <class K>
 struct ElemSmem {
   using T = typename K::T;
+  static constexpr int V = Vec16<T>::N;
   static constexpr int NPP = Padded<T, K::NP>::value;
   static constexpr int DD = K::DIM * K::DIM + 1;
-  static constexpr size_t oC = 0;                                         // [ROWS][NP]
-  static constexpr size_t oG = oC + (size_t)K::ROWS * K::NP;              // [KV][LDR]
-  static constexpr size_t oS = oG + (size_t)K::KV * K::LDR;               // [NS][LDR]
-  static constexpr size_t oDphi = (oS + (size_t)K::NS * K::LDR + 3) / 4 * 4;  // [KV][NPP]
-  static constexpr size_t oPhif = oDphi + (size_t)K::KV * NPP;            // [NS][NPP]
-  static constexpr size_t oPhi = oPhif + (size_t)K::NS * NPP;             // [NQ][NP]
-  static constexpr size_t oQw = oPhi + (size_t)K::NQ * K::NP;             // [NQ]
-  static constexpr size_t t_bytes = ((oQw + K::NQ) * sizeof(T) + 15) / 16 * 16;
+  // table blob (bulk copied as one piece, same layout in global memory)
+  static constexpr size_t oDphi = 0;                                   // [KV][NPP]
+  static constexpr size_t oPhif = oDphi + (size_t)K::KV * NPP;         // [NS][NPP]
+  static constexpr size_t oPhi = oPhif + (size_t)K::NS * NPP;          // [NQ][NPP]
+  static constexpr size_t oQw = oPhi + (size_t)K::NQ * NPP;            // [NQ] padded
+  static constexpr size_t blob_elems = oQw + (K::NQ + V - 1) / V * V;
+  static constexpr size_t blob_bytes = blob_elems * sizeof(T);
+  // tile
+  static constexpr size_t oC = blob_elems;                                     // [ROWS][NP]
+  static constexpr size_t oG = oC + ((size_t)K::ROWS * K::NP + V - 1) / V * V;  // [ROWS][LDK]
+  static constexpr size_t t_bytes = ((oG + (size_t)K::ROWS * K::LDK) * sizeof(T) + 15) / 16 * 16;
   static constexpr size_t bytes = t_bytes + 8 * ((size_t)K::TE * DD + (size_t)K::TE * K::NV);
+  // the tile's coefficients can be bulk copied when every tile starts on a
+  // 16-byte boundary
+  static constexpr bool bulk_c = ((size_t)K::TE * K::MNP * sizeof(T)) % 16 == 0;
 };
 
 template <class K>
@@ -76,76 +107,97 @@ constexpr size_t elem_kernel_smem() {
   return ElemSmem<K>::bytes;
 }
 
+// host-side layout of the table blob (FP64; converted to T on upload)
+template <class K>
+void fill_table_blob(const double* dphi, const double* phif, const double* phi, const double* qw,
+                     double* blob) {
+  using L = ElemSmem<K>;
+  constexpr int NP = K::NP, NPP = L::NPP;
+  for (size_t i = 0; i < L::blob_elems; ++i) blob[i] = 0.0;
+  for (int kk = 0; kk < K::KV; ++kk)
+    for (int k = 0; k < NP; ++k) blob[L::oDphi + (size_t)kk * NPP + k] = dphi[kk * NP + k];
+  for (int s = 0; s < K::NS; ++s)
+    for (int k = 0; k < NP; ++k) blob[L::oPhif + (size_t)s * NPP + k] = phif[s * NP + k];
+  for (int q = 0; q < K::NQ; ++q)
+    for (int k = 0; k < NP; ++k) blob[L::oPhi + (size_t)q * NPP + k] = phi[q * NP + k];
+  for (int q = 0; q < K::NQ; ++q) blob[L::oQw + q] = qw[q];
+}
+
+constexpr int kMbarPolls = 1 << 22;  // bound of the bulk-copy wait
+
 template <class K>
 __global__ void __launch_bounds__(K::BLOCK) elem_kernel(StageArgs<typename K::T> a) {
   using T = typename K::T;
   using L = ElemSmem<K>;
   constexpr int M = K::M, NP = K::NP, NQ = K::NQ, DIM = K::DIM, TE = K::TE, BLOCK = K::BLOCK;
-  constexpr int MNP = K::MNP, NS = K::NS, KV = K::KV, LDR = K::LDR, NV = K::NV;
+  constexpr int MNP = K::MNP, NS = K::NS, KV = K::KV, LDK = K::LDK, NV = K::NV, ROWS = K::ROWS;
   constexpr int NPP = L::NPP, DD = L::DD;
   if (a.ctl->done) return;
-  extern __shared__ __align__(16) unsigned char smem_raw[];
+  extern __shared__ __align__(128) unsigned char smem_raw[];
   T* sT = reinterpret_cast<T*>(smem_raw);
-  T* sC = sT + L::oC;
-  T* sG = sT + L::oG;
-  T* sS = sT + L::oS;
   T* sDphi = sT + L::oDphi;
   T* sPhif = sT + L::oPhif;
   T* sPhi = sT + L::oPhi;
   T* sQw = sT + L::oQw;
+  T* sC = sT + L::oC;
+  T* sG = sT + L::oG;
   double* sJ = reinterpret_cast<double*>(smem_raw + L::t_bytes);
   double* sEig = sJ + TE * DD;
+  __shared__ __align__(8) uint64_t bar;
   __shared__ double red[BLOCK / 32];
   __shared__ bool amLast;
+  __shared__ int s_fail;
 
   const int tid = threadIdx.x;
   const int e0 = blockIdx.x * TE;
   const int ne = min(TE, a.mesh.E - e0);
+  const uint32_t c_bytes = (uint32_t)(((size_t)ne * MNP * sizeof(T) + 15) / 16 * 16);
 
-  // stage tables (rows padded to 16 bytes), the state tile, the slots
-  // transposed to [point][row], and the cells' J^{-1} and |J|
-  for (int i = tid; i < KV * NPP; i += BLOCK) {
-    const int kk = i / NPP, k = i - (i / NPP) * NPP;
-    sDphi[i] = k < NP ? a.tab.dphi[kk * NP + k] : T(0);
-  }
-  for (int i = tid; i < NS * NPP; i += BLOCK) {
-    const int s = i / NPP, k = i - (i / NPP) * NPP;
-    sPhif[i] = k < NP ? a.tab.phif[s * NP + k] : T(0);
-  }
-  for (int i = tid; i < NQ * NP; i += BLOCK) sPhi[i] = a.tab.phi[i];
-  for (int i = tid; i < NQ; i += BLOCK) sQw[i] = a.tab.qw[i];
-  {
-    const T* src = a.C + (size_t)e0 * MNP;
-    for (int i = tid; i < ne * MNP; i += BLOCK) sC[i] = src[i];
-    const T* ss = a.slots + (size_t)e0 * NS * M;
-    for (int i = tid; i < ne * NS * M; i += BLOCK) {
-      const int e = i / (NS * M), rem = i - e * (NS * M);
-      const int s = rem / M, j = rem - (rem / M) * M;
-      sS[s * LDR + e * M + j] = ss[i];
-    }
-    for (int i = tid; i < ne * DD; i += BLOCK) {
-      const int e = i / DD, c = i - (i / DD) * DD;
-      sJ[i] = c < DIM * DIM ? (double)a.mesh.jinv[(size_t)(e0 + e) * DIM * DIM + c]
-                            : (double)a.mesh.detj[e0 + e];
-    }
+  if (tid == 0) {
+    s_fail = 0;
+    mbar_init(&bar, 1);
   }
   __syncthreads();
+  if (tid == 0) {
+    mbar_arrive_expect_tx(&bar, (uint32_t)L::blob_bytes + (L::bulk_c ? c_bytes : 0u));
+    bulk_g2s(sT, a.tab.blob, (uint32_t)L::blob_bytes, &bar);
+    if constexpr (L::bulk_c) bulk_g2s(sC, a.C + (size_t)e0 * MNP, c_bytes, &bar);
+  }
+  if constexpr (!L::bulk_c) {
+    const T* src = a.C + (size_t)e0 * MNP;
+    for (int i = tid; i < ne * MNP; i += BLOCK) sC[i] = src[i];
+  }
+  for (int i = tid; i < ne * DD; i += BLOCK) {
+    const int e = i / DD, c = i - (i / DD) * DD;
+    sJ[i] = c < DIM * DIM ? (double)a.mesh.jinv[(size_t)(e0 + e) * DIM * DIM + c]
+                          : (double)a.mesh.detj[e0 + e];
+  }
+  if (tid == 0 && !mbar_wait(&bar, 0, kMbarPolls)) {
+    // record the failure, then wait once more (bounded) for the copies this
+    // CTA issued before its shared memory is released
+    s_fail = 1;
+    atomicAdd(&a.status->timeouts, 1);
+    mbar_wait(&bar, 0, kMbarPolls);
+  }
+  __syncthreads();
+  if (s_fail) return;
 
   // volume: fixed quadrature point per thread
   if (tid < K::EG * NQ) {
     const int q = tid % NQ, g = tid / NQ;
     T phi[NP];
 #pragma unroll
-    for (int k = 0; k < NP; ++k) phi[k] = sPhi[q * NP + k];
+    for (int k = 0; k < NP; ++k) phi[k] = sPhi[q * NPP + k];
     const T w = sQw[q];
     for (int e = g; e < ne; e += K::EG) {
-      const T* c = sC + e * MNP;
       T U[M];
 #pragma unroll
       for (int j = 0; j < M; ++j) {
+        T c[NP];
+        load_vec<T, NP>(sC + (e * M + j) * NP, c);
         T acc = 0;
 #pragma unroll
-        for (int k = 0; k < NP; ++k) acc += phi[k] * c[j * NP + k];
+        for (int k = 0; k < NP; ++k) acc += phi[k] * c[k];
         U[j] = acc;
       }
       if (!is_physical<K::LAW, T>(a.law, U)) flag_nonphysical(a.status, e0 + e);
@@ -163,7 +215,7 @@ __global__ void __launch_bounds__(K::BLOCK) elem_kernel(StageArgs<typename K::T>
           T acc = 0;
 #pragma unroll
           for (int i = 0; i < DIM; ++i) acc += F[j][i] * J[i * DIM + r];
-          sG[(q * DIM + r) * LDR + e * M + j] = acc * jw;
+          sG[(e * M + j) * LDK + q * DIM + r] = acc * jw;
         }
     }
   }
@@ -176,19 +228,21 @@ __global__ void __launch_bounds__(K::BLOCK) elem_kernel(StageArgs<typename K::T>
     T acc[NPP];
 #pragma unroll
     for (int k = 0; k < NPP; ++k) acc[k] = 0;
+    const T* g = sG + row * LDK;
 #pragma unroll 4
     for (int kk = 0; kk < KV; ++kk) {
-      const T gv = sG[kk * LDR + row];
+      const T gv = g[kk];
       T d[NPP];
-      load_row16<T, NPP>(sDphi + kk * NPP, d);
+      load_vec<T, NPP>(sDphi + kk * NPP, d);
 #pragma unroll
       for (int k = 0; k < NPP; ++k) acc[k] += gv * d[k];
     }
+    const T* sl = a.slots + (size_t)blockIdx.x * NS * ROWS + row;
 #pragma unroll 4
     for (int s = 0; s < NS; ++s) {
-      const T sv = sS[s * LDR + row];
+      const T sv = __ldg(sl + (size_t)s * ROWS);
       T p[NPP];
-      load_row16<T, NPP>(sPhif + s * NPP, p);
+      load_vec<T, NPP>(sPhif + s * NPP, p);
 #pragma unroll
       for (int k = 0; k < NPP; ++k) acc[k] += sv * p[k];
     }
@@ -200,18 +254,19 @@ __global__ void __launch_bounds__(K::BLOCK) elem_kernel(StageArgs<typename K::T>
       const int e = row / M;
       const T dtj = (T)(a.ctl->dt / sJ[e * DD + DIM * DIM]);
       T* crow = sC + row * NP;
+      T c[NP];
+      load_vec<T, NP>(crow, c);
 #pragma unroll
       for (int k = 0; k < NP; ++k) {
-        const T c = crow[k];
         T out;
         if (a.stage == 1) {
-          a.U0out[gbase + k] = c;
-          out = c + acc[k] * dtj;
+          a.U0out[gbase + k] = c[k];
+          out = c[k] + acc[k] * dtj;
         } else if (a.stage == 2) {
-          out = (T)0.25 * (c + acc[k] * dtj + (T)3. * a.U0[gbase + k]);
+          out = (T)0.25 * (c[k] + acc[k] * dtj + (T)3. * a.U0[gbase + k]);
         } else {
           const T u0 = a.U0[gbase + k];
-          out = ((T)2.0 * (c + acc[k] * dtj) + u0) / (T)3.0;
+          out = ((T)2.0 * (c[k] + acc[k] * dtj) + u0) / (T)3.0;
           const double dd = (double)out - (double)u0;
           rsum += dd * dd;
         }

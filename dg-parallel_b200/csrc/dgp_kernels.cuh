@@ -47,16 +47,25 @@ struct Cfg {
   // the row in registers; TE cells per CTA, capped by a shared-memory budget
   static constexpr int BLOCK = 128;
   static constexpr int NV = DIM == 2 ? 4 : 1;  // states of the CFL (mean + vertices)
-  static constexpr int CELL_BYTES =
-      (int)sizeof(T) * (MNP + KV * M + NS * M) + 8 * (NV + DIM * DIM + 1);
-  static constexpr int TE_SMEM = (96 * 1024) / CELL_BYTES;
+  static constexpr int LDK = KV | 1;           // row stride of G (odd: conflict-free)
+  static constexpr int CELL_BYTES = (int)sizeof(T) * (MNP + M * LDK) + 8 * (NV + DIM * DIM + 1);
+  static constexpr int TE_SMEM = (64 * 1024) / CELL_BYTES;
   static constexpr int TE_ROWS = BLOCK / M;
   static constexpr int TE = TE_SMEM < TE_ROWS ? (TE_SMEM < 1 ? 1 : TE_SMEM) : TE_ROWS;
   static constexpr int ROWS = TE * M;
-  static constexpr int LDR = ROWS | 1;   // leading dimension of the [k][row] operands
   static constexpr int EG = BLOCK / NQ;   // cells processed concurrently in the volume phase
+  // face slots live tile-transposed, [tile][face point][row], so that the
+  // element kernel reads them row-coalesced: slot(e, s, j) =
+  // ((e / TE) * NS + s) * ROWS + (e % TE) * M + j
   static constexpr int FACE_BLOCK = 128;
+  static constexpr int FPB = FACE_BLOCK / NQF;  // faces per face-kernel CTA
+  static constexpr int LDM = MNP | 1;           // staged coefficient row stride
 };
+
+template <class K>
+__device__ __forceinline__ size_t slot_index(int e, int s, int j) {
+  return ((size_t)(e / K::TE) * K::NS + s) * K::ROWS + (size_t)(e % K::TE) * K::M + j;
+}
 
 // time-step control that lives in device memory so that a whole run can be
 // captured in a CUDA graph without host round trips
@@ -78,6 +87,8 @@ struct TimeCtl {
 struct Status {
   int nonphysical;
   int first_bad;  // internal cell index, INT_MAX when none
+  int timeouts;   // bounded waits on bulk copies that gave up (never expected)
+  int pad;
 };
 
 // device views (internal cell order); T = arithmetic type of the hot path
@@ -99,6 +110,8 @@ struct DevMesh {
 
 template <typename T>
 struct DevTables {
+  const T* blob;    // element-kernel tables in their shared-memory layout (bulk copied)
+  int blob_bytes;
   const T* phi;     // NQ x NP
   const T* dphi;    // NQ x DIM x NP
   const T* qw;      // NQ
@@ -141,21 +154,79 @@ __device__ __forceinline__ void flag_nonphysical(Status* st, int cell) {
 }
 
 // -----------------------------------------------------------------------------
+// largest power of two (<= 16) dividing n
+constexpr int pow2_div(int n) { return (n % 16 == 0) ? 16 : (n % 8 == 0) ? 8 : (n % 4 == 0) ? 4 : 1; }
+
+// N values through the read-only path with loads of ALIGN bytes (p is
+// ALIGN-aligned)
+template <typename T, int N, int ALIGN>
+__device__ __forceinline__ void ldg_vec(const T* __restrict__ p, T (&out)[N]) {
+  if constexpr (ALIGN == 16 && sizeof(T) == 8 && N % 2 == 0) {
+#pragma unroll
+    for (int i = 0; i < N / 2; ++i) {
+      const double2 v = __ldg(reinterpret_cast<const double2*>(p) + i);
+      out[2 * i] = v.x;
+      out[2 * i + 1] = v.y;
+    }
+  } else if constexpr (ALIGN == 16 && sizeof(T) == 4 && N % 4 == 0) {
+#pragma unroll
+    for (int i = 0; i < N / 4; ++i) {
+      const float4 v = __ldg(reinterpret_cast<const float4*>(p) + i);
+      out[4 * i] = v.x;
+      out[4 * i + 1] = v.y;
+      out[4 * i + 2] = v.z;
+      out[4 * i + 3] = v.w;
+    }
+  } else if constexpr (ALIGN >= 8 && sizeof(T) == 4 && N % 2 == 0) {
+#pragma unroll
+    for (int i = 0; i < N / 2; ++i) {
+      const float2 v = __ldg(reinterpret_cast<const float2*>(p) + i);
+      out[2 * i] = v.x;
+      out[2 * i + 1] = v.y;
+    }
+  } else {
+#pragma unroll
+    for (int i = 0; i < N; ++i) out[i] = __ldg(p + i);
+  }
+}
+
+// trace of a cell's state at one face point: U[j] = sum_k phi[k] C[j][k],
+// streamed field by field
+template <class K>
+__device__ __forceinline__ void cell_trace(const typename K::T* __restrict__ c, const typename K::T* phi,
+                                           typename K::T* U) {
+  using T = typename K::T;
+  constexpr int NP = K::NP;
+  constexpr int ALIGN = pow2_div(NP * (int)sizeof(T)) < pow2_div(K::MNP * (int)sizeof(T))
+                            ? pow2_div(NP * (int)sizeof(T))
+                            : pow2_div(K::MNP * (int)sizeof(T));
+#pragma unroll
+  for (int j = 0; j < K::M; ++j) {
+    T cj[NP];
+    ldg_vec<T, NP, ALIGN>(c + j * NP, cj);
+    T acc = 0;
+#pragma unroll
+    for (int k = 0; k < NP; ++k) acc += phi[k] * cj[k];
+    U[j] = acc;
+  }
+}
+
 template <class K>
 __global__ void __launch_bounds__(K::FACE_BLOCK) face_kernel(StageArgs<typename K::T> a) {
   using T = typename K::T;
-  constexpr int M = K::M, NP = K::NP, NQF = K::NQF, DIM = K::DIM;
+  constexpr int M = K::M, NP = K::NP, NQF = K::NQF, DIM = K::DIM, MNP = K::MNP;
   if (a.ctl->done) return;
   __shared__ T s_phif[K::NLF * NQF * NP];
   __shared__ T s_fqw[NQF];
   __shared__ int s_qmap[K::NPERM * NQF];
-  for (int i = threadIdx.x; i < K::NLF * NQF * NP; i += blockDim.x) s_phif[i] = a.tab.phif[i];
-  for (int i = threadIdx.x; i < NQF; i += blockDim.x) s_fqw[i] = a.tab.fqw[i];
-  for (int i = threadIdx.x; i < K::NPERM * NQF; i += blockDim.x) s_qmap[i] = a.tab.qmap[i];
+  const int tid = threadIdx.x;
+  for (int i = tid; i < K::NLF * NQF * NP; i += blockDim.x) s_phif[i] = a.tab.phif[i];
+  for (int i = tid; i < NQF; i += blockDim.x) s_fqw[i] = a.tab.fqw[i];
+  for (int i = tid; i < K::NPERM * NQF; i += blockDim.x) s_qmap[i] = a.tab.qmap[i];
   __syncthreads();
-  const int gid = blockIdx.x * blockDim.x + threadIdx.x;
-  const int f = gid / NQF, q = gid - (gid / NQF) * NQF;
-  if (f >= a.mesh.F) return;
+  const int fl = tid / NQF, q = tid - (tid / NQF) * NQF;
+  const int f = blockIdx.x * K::FPB + fl;
+  if (fl >= K::FPB || f >= a.mesh.F) return;
   const int eL = a.mesh.fel[2 * f], eR = a.mesh.fel[2 * f + 1];
   const int code = a.mesh.fcode[f];
   const int lfL = code & 15, lfR = (code >> 4) & 15, perm = code >> 8;
@@ -164,28 +235,12 @@ __global__ void __launch_bounds__(K::FACE_BLOCK) face_kernel(StageArgs<typename 
   for (int i = 0; i < DIM; ++i) n[i] = a.mesh.fnrm[f * DIM + i];
   const T jw = a.mesh.fj[f] * s_fqw[q];
   T UL[M], UR[M], flux[M];
-  const T* cl = a.C + (size_t)eL * K::MNP;
-  const T* pl = s_phif + (lfL * NQF + q) * NP;
-#pragma unroll
-  for (int j = 0; j < M; ++j) {
-    T acc = 0;
-#pragma unroll
-    for (int k = 0; k < NP; ++k) acc += pl[k] * cl[j * NP + k];
-    UL[j] = acc;
-  }
+  cell_trace<K>(a.C + (size_t)eL * MNP, s_phif + (lfL * NQF + q) * NP, UL);
   if (!is_physical<K::LAW, T>(a.law, UL)) flag_nonphysical(a.status, eL);
   int qR = 0;
   if (eR >= 0) {
     qR = s_qmap[perm * NQF + q];
-    const T* cr = a.C + (size_t)eR * K::MNP;
-    const T* pr = s_phif + (lfR * NQF + qR) * NP;
-#pragma unroll
-    for (int j = 0; j < M; ++j) {
-      T acc = 0;
-#pragma unroll
-      for (int k = 0; k < NP; ++k) acc += pr[k] * cr[j * NP + k];
-      UR[j] = acc;
-    }
+    cell_trace<K>(a.C + (size_t)eR * MNP, s_phif + (lfR * NQF + qR) * NP, UR);
     if (!is_physical<K::LAW, T>(a.law, UR)) flag_nonphysical(a.status, eR);
     numerical_flux<K::LAW, K::FLUX, DIM, T>(a.law, n, UL, UR, flux);
   } else {
@@ -194,11 +249,11 @@ __global__ void __launch_bounds__(K::FACE_BLOCK) face_kernel(StageArgs<typename 
     const double time = a.ctl->t + a.stage_time_factor * a.ctl->dt;
     boundary_flux<K::LAW, K::FLUX, DIM, T>(a.law, a.mesh.bbid[b], n, x, time, UL, flux);
   }
-  T* sl = a.slots + (((size_t)eL * K::NLF + lfL) * NQF + q) * M;
+  T* sl = a.slots + slot_index<K>(eL, lfL * NQF + q, 0);
 #pragma unroll
   for (int j = 0; j < M; ++j) sl[j] = -flux[j] * jw;
   if (eR >= 0) {
-    T* sr = a.slots + (((size_t)eR * K::NLF + lfR) * NQF + qR) * M;
+    T* sr = a.slots + slot_index<K>(eR, lfR * NQF + qR, 0);
 #pragma unroll
     for (int j = 0; j < M; ++j) sr[j] = flux[j] * jw;
   }

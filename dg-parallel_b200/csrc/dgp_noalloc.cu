@@ -77,7 +77,8 @@ extern "C" int dgp_rhs_noalloc(dgp_solver s, const double* dev_state, double t, 
   const size_t tsize = s->ops.tsize;
   const int E = s->b.E, mnp = s->b.M * s->b.NP;
   const size_t state_b = round256(s->state_count() * tsize);
-  const size_t slot_b = round256(static_cast<size_t>(E) * s->tab.nlf * s->tab.nqf * s->b.M * tsize);
+  const size_t ntiles = (static_cast<size_t>(E) + s->ops.TE - 1) / s->ops.TE;
+  const size_t slot_b = round256(ntiles * s->ops.TE * s->tab.nlf * s->tab.nqf * s->b.M * tsize);
   const size_t need = 2 * state_b + slot_b;
   if (need > kScratchBytes)
     return fail(DGP_ERR_INVALID, "dgp_rhs_noalloc: this mesh needs " + std::to_string(need) +

@@ -35,8 +35,7 @@ StageArgs<typename K::T> stage_args(const DeviceBuffers& b, int stage, double ti
 template <class K>
 void ops_face(const DeviceBuffers& b, int stage, double time_factor, cudaStream_t st) {
   auto a = stage_args<K>(b, stage, time_factor, 0);
-  const long long nf = static_cast<long long>(b.F) * K::NQF;
-  const int fgrid = static_cast<int>((nf + K::FACE_BLOCK - 1) / K::FACE_BLOCK);
+  const int fgrid = (b.F + K::FPB - 1) / K::FPB;
   face_kernel<K><<<fgrid, K::FACE_BLOCK, 0, st>>>(a);
 }
 
@@ -89,6 +88,8 @@ Ops make_ops() {
   o.elem_block = K::BLOCK;
   o.elem_smem = elem_kernel_smem<K>();
   o.tsize = sizeof(typename K::T);
+  o.blob_elems = ElemSmem<K>::blob_elems;
+  o.fill_blob = &fill_table_blob<K>;
   o.precision = sizeof(typename K::T) == 8 ? DGP_PRECISION_FP64 : DGP_PRECISION_MIXED;
   o.prepare = &ops_prepare<K>;
   o.stage = &ops_stage<K>;

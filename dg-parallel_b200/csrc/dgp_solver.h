@@ -28,6 +28,8 @@ struct DeviceBuffers {
   void* fj = nullptr;
   double* bpts = nullptr;
   int* bbid = nullptr;
+  void* blob = nullptr;   // element-kernel tables in shared-memory layout
+  int blob_bytes = 0;
   void* phi = nullptr;
   void* dphi = nullptr;
   void* qw = nullptr;
@@ -72,6 +74,8 @@ inline StageArgs<T> make_args(const DeviceBuffers& b) {
   a.mesh.fj = static_cast<const T*>(b.fj);
   a.mesh.bpts = b.bpts;
   a.mesh.bbid = b.bbid;
+  a.tab.blob = static_cast<const T*>(b.blob);
+  a.tab.blob_bytes = b.blob_bytes;
   a.tab.phi = static_cast<const T*>(b.phi);
   a.tab.dphi = static_cast<const T*>(b.dphi);
   a.tab.qw = static_cast<const T*>(b.qw);
@@ -105,6 +109,10 @@ struct Ops {
   int M = 0, NP = 0, NQ = 0, NQF = 0, TE = 0, elem_block = 0, precision = 0;
   size_t elem_smem = 0;
   size_t tsize = 8;
+  size_t blob_elems = 0;
+  // writes the element-kernel table blob (FP64) from dphi [KV][NP], phif [NS][NP],
+  // phi [NQ][NP], qw [NQ]
+  void (*fill_blob)(const double*, const double*, const double*, const double*, double*) = nullptr;
   cudaError_t (*prepare)() = nullptr;
   // one SSP-RK3 stage (face kernel + element kernel); stage 0 writes the RHS
   void (*stage)(const DeviceBuffers&, int stage, double time_factor, int fuse_cfl, cudaStream_t) = nullptr;
