@@ -171,6 +171,8 @@ def main():
     ap.add_argument("--impl", default="dgp", choices=["dgp", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--e2e-steps", type=int, default=20)
+    ap.add_argument("--no-accuracy", action="store_true",
+                    help="skip the untimed runs to t = 2 that state the density L2 errors")
     ap.add_argument("--profile-case", choices=["fp64", "mixed"], default=None,
                     help="only set up the workload and run --warmup + --steps steps (for ncu)")
     args = ap.parse_args()
@@ -248,6 +250,24 @@ def main():
     c64 = fp64["solver"].get_state()
     c32 = mixed["solver"].get_state()
     mixed["density_coeff_rel_diff_vs_fp64"] = float(np.abs(c32[:, 0] - c64[:, 0]).max() / np.abs(c64[:, 0]).max())
+    # the workload's full run (isentropic vortex to t = 2, CFL 0.1), untimed:
+    # density L2 error against the exact solution for both forms
+    accuracy = None
+    if not args.no_accuracy:
+        accuracy = {}
+        for name in ("fp64", "mixed"):
+            s = results[name]["solver"]
+            s.project(0.0)
+            w0 = time.perf_counter()
+            t_end, n = s.run(0.0, 2.0, 0.1)
+            accuracy[name] = {"t": t_end, "steps": n, "density_l2_vs_exact": s.l2_error(t_end, 0),
+                              "wall_s": time.perf_counter() - w0}
+        accuracy["mixed_over_fp64_l2"] = (accuracy["mixed"]["density_l2_vs_exact"] /
+                                          accuracy["fp64"]["density_l2_vs_exact"])
+        c64 = results["fp64"]["solver"].get_state()
+        c32 = results["mixed"]["solver"].get_state()
+        accuracy["mixed_density_coeff_rel_diff_vs_fp64"] = float(
+            np.abs(c32[:, 0] - c64[:, 0]).max() / np.abs(c64[:, 0]).max())
 
     # end to end through the C ABI with host buffers: per step, state H2D from
     # pinned memory, one SSP-RK3 step, state D2H
@@ -303,12 +323,15 @@ def main():
             "data": "synthetic",
             "config": dict(WORKLOAD, parallelism=f"replicas{world}",
                            l2="working set 150 MB > 126 MB L2; each step streams ~1 GB"),
-            "mixed": {"value": mixed["value"], "dtype": "f32 (f64 geometry, time, totals)",
+            "mixed": {"value": mixed["value"],
+                      "dtype": "f32 RHS (traces, fluxes, contractions, face slots); f64 state, "
+                               "RK update, inverse mass, time, totals",
                       "speedup_vs_fp64": mixed["value"] / fp64["value"],
                       "density_l2_vs_exact": mixed["density_l2_vs_exact"],
                       "density_coeff_rel_diff_vs_fp64": mixed["density_coeff_rel_diff_vs_fp64"],
                       "kernel_ms": mixed["kernel_ms"]},
             "fp64_density_l2_vs_exact": fp64["density_l2_vs_exact"],
+            "accuracy_t2": accuracy,
             "kernel_ms": {"face": face_ms, "elem": elem_ms, "elem_last_stage_cfl": elem3_ms},
             "roofline": {"kernel": kname, "bound": "hbm", "achieved": achieved,
                          "peak": peaks.get("hbm_gbs"), "unit": "GB/s",

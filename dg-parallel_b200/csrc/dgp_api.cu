@@ -335,6 +335,7 @@ int dgp_solver_create(dgp_mesh mh, dgp_law law, int order, int precision, int li
     for (int c = 0; c < 3; ++c) qpd[3 * q + c] = t.qp[3 * q + c];
   int rc = DGP_OK;
   if ((rc = s->upload_t(&b.jinv, jinv)) || (rc = s->upload_t(&b.detj, detj)) ||
+      (rc = s->upload(&b.detjd, detj)) ||
       (rc = s->upload(&b.csize, csize)) || (rc = s->upload(&b.x0, x0)) || (rc = s->upload(&b.jac, jac)) ||
       (rc = s->upload(&b.fel, fel)) || (rc = s->upload(&b.fcode, fcode)) ||
       (rc = s->upload_t(&b.fnrm, fnrm)) || (rc = s->upload_t(&b.fj, fj)) ||
@@ -366,9 +367,9 @@ int dgp_solver_create(dgp_mesh mh, dgp_law law, int order, int precision, int li
   const size_t ntiles = (static_cast<size_t>(E) + s->ops.TE - 1) / s->ops.TE;
   const size_t nslot = ntiles * s->ops.TE * t.nlf * t.nqf * b.M;
   unsigned char *C, *U0, *slots, *rhs, *scratch;
-  const size_t ts = s->ops.tsize;
-  if ((rc = s->alloc(&C, nstate * ts + 256)) || (rc = s->alloc(&U0, nstate * ts + 256)) ||
-      (rc = s->alloc(&slots, nslot * ts)) || (rc = s->alloc(&rhs, nstate * ts + 256)) ||
+  const size_t ts = s->ops.tsize;  // slots hold the RHS arithmetic type; the state is FP64
+  if ((rc = s->alloc(&C, nstate * 8 + 256)) || (rc = s->alloc(&U0, nstate * 8 + 256)) ||
+      (rc = s->alloc(&slots, nslot * ts)) || (rc = s->alloc(&rhs, nstate * 8 + 256)) ||
       (rc = s->alloc(&scratch, nstate * 8 + 256)))
     return bail(rc);
   b.C = C;
@@ -448,25 +449,14 @@ static int host_to_state(dgp_solver s, const double* in, void* dst) {
   std::vector<double> tmp(n);
   for (int i = 0; i < s->b.E; ++i)
     std::memcpy(&tmp[i * mnp], &in[static_cast<size_t>(s->i2f[i]) * mnp], mnp * 8);
-  if (s->ops.tsize == 8) {
-    DGP_CUDA(cudaMemcpy(dst, tmp.data(), n * 8, cudaMemcpyHostToDevice));
-  } else {
-    std::vector<float> f(tmp.begin(), tmp.end());
-    DGP_CUDA(cudaMemcpy(dst, f.data(), n * 4, cudaMemcpyHostToDevice));
-  }
+  DGP_CUDA(cudaMemcpy(dst, tmp.data(), n * 8, cudaMemcpyHostToDevice));
   return DGP_OK;
 }
 
 static int state_to_host(dgp_solver s, const void* src, double* out) {
   const size_t mnp = static_cast<size_t>(s->b.M) * s->b.NP, n = s->state_count();
   std::vector<double> tmp(n);
-  if (s->ops.tsize == 8) {
-    DGP_CUDA(cudaMemcpy(tmp.data(), src, n * 8, cudaMemcpyDeviceToHost));
-  } else {
-    std::vector<float> f(n);
-    DGP_CUDA(cudaMemcpy(f.data(), src, n * 4, cudaMemcpyDeviceToHost));
-    std::copy(f.begin(), f.end(), tmp.begin());
-  }
+  DGP_CUDA(cudaMemcpy(tmp.data(), src, n * 8, cudaMemcpyDeviceToHost));
   for (int i = 0; i < s->b.E; ++i)
     std::memcpy(&out[static_cast<size_t>(s->i2f[i]) * mnp], &tmp[i * mnp], mnp * 8);
   return DGP_OK;
@@ -492,12 +482,8 @@ int dgp_set_state_device(dgp_solver s, const double* dev_state) {
   const int mnp = s->b.M * s->b.NP;
   const long long n = static_cast<long long>(s->b.E) * mnp;
   const int grid = static_cast<int>((n + 255) / 256);
-  if (s->ops.tsize == 8)
-    gather_cells<double, double><<<grid, 256, 0, s->stream>>>(dev_state, static_cast<double*>(s->b.C),
-                                                              s->d_i2f, s->b.E, mnp);
-  else
-    gather_cells<double, float><<<grid, 256, 0, s->stream>>>(dev_state, static_cast<float*>(s->b.C),
-                                                             s->d_i2f, s->b.E, mnp);
+  gather_cells<double, double><<<grid, 256, 0, s->stream>>>(dev_state, static_cast<double*>(s->b.C),
+                                                            s->d_i2f, s->b.E, mnp);
   DGP_CUDA(cudaGetLastError());
   DGP_CUDA(cudaStreamSynchronize(s->stream));
   return DGP_OK;
@@ -509,12 +495,8 @@ int dgp_get_state_device(dgp_solver s, double* dev_state) {
   const int mnp = s->b.M * s->b.NP;
   const long long n = static_cast<long long>(s->b.E) * mnp;
   const int grid = static_cast<int>((n + 255) / 256);
-  if (s->ops.tsize == 8)
-    gather_cells<double, double><<<grid, 256, 0, s->stream>>>(static_cast<const double*>(s->b.C),
-                                                              dev_state, s->d_f2i, s->b.E, mnp);
-  else
-    gather_cells<float, double><<<grid, 256, 0, s->stream>>>(static_cast<const float*>(s->b.C), dev_state,
-                                                             s->d_f2i, s->b.E, mnp);
+  gather_cells<double, double><<<grid, 256, 0, s->stream>>>(static_cast<const double*>(s->b.C), dev_state,
+                                                            s->d_f2i, s->b.E, mnp);
   DGP_CUDA(cudaGetLastError());
   DGP_CUDA(cudaStreamSynchronize(s->stream));
   return DGP_OK;
@@ -655,7 +637,7 @@ int dgp_solver_stream(dgp_solver s, void** stream) {
 int dgp_profile_kernels(dgp_solver s, int iters, float* ms) {
   if (!s || !ms || iters <= 0) return fail(DGP_ERR_INVALID, "bad argument");
   DGP_CUDA(cudaSetDevice(s->device));
-  const size_t bytes = s->state_count() * s->ops.tsize;
+  const size_t bytes = s->state_count() * 8;
   // the element kernel updates the state in place: run it with dt = 0 and
   // u_n = u so every launch leaves the state as it found it, then restore it
   DGP_CUDA(cudaMemcpyAsync(s->b.scratch, s->b.C, bytes, cudaMemcpyDeviceToDevice, s->stream));

@@ -92,14 +92,16 @@ struct ElemSmem {
   static constexpr size_t oQw = oPhi + (size_t)K::NQ * NPP;            // [NQ] padded
   static constexpr size_t blob_elems = oQw + (K::NQ + V - 1) / V * V;
   static constexpr size_t blob_bytes = blob_elems * sizeof(T);
-  // tile
-  static constexpr size_t oC = blob_elems;                                     // [ROWS][NP]
-  static constexpr size_t oG = oC + ((size_t)K::ROWS * K::NP + V - 1) / V * V;  // [ROWS][LDK]
-  static constexpr size_t t_bytes = ((oG + (size_t)K::ROWS * K::LDK) * sizeof(T) + 15) / 16 * 16;
-  static constexpr size_t bytes = t_bytes + 8 * ((size_t)K::TE * DD + (size_t)K::TE * K::NV);
+  // tile, byte offsets: FP64 coefficients [ROWS][NP], G [ROWS][LDK] (T),
+  // then FP64 J^{-1}, |J| [TE][DD] and CFL eigenvalues [TE][NV]
+  static constexpr size_t r16(size_t n) { return (n + 15) / 16 * 16; }
+  static constexpr size_t oCB = r16(blob_bytes);
+  static constexpr size_t oGB = oCB + r16((size_t)K::ROWS * K::NP * 8);
+  static constexpr size_t oJB = oGB + r16((size_t)K::ROWS * K::LDK * sizeof(T));
+  static constexpr size_t bytes = oJB + 8 * ((size_t)K::TE * DD + (size_t)K::TE * K::NV);
   // the tile's coefficients can be bulk copied when every tile starts on a
   // 16-byte boundary
-  static constexpr bool bulk_c = ((size_t)K::TE * K::MNP * sizeof(T)) % 16 == 0;
+  static constexpr bool bulk_c = ((size_t)K::TE * K::MNP * 8) % 16 == 0;
 };
 
 template <class K>
@@ -139,9 +141,9 @@ __global__ void __launch_bounds__(K::BLOCK) elem_kernel(StageArgs<typename K::T>
   T* sPhif = sT + L::oPhif;
   T* sPhi = sT + L::oPhi;
   T* sQw = sT + L::oQw;
-  T* sC = sT + L::oC;
-  T* sG = sT + L::oG;
-  double* sJ = reinterpret_cast<double*>(smem_raw + L::t_bytes);
+  double* sC = reinterpret_cast<double*>(smem_raw + L::oCB);
+  T* sG = reinterpret_cast<T*>(smem_raw + L::oGB);
+  double* sJ = reinterpret_cast<double*>(smem_raw + L::oJB);
   double* sEig = sJ + TE * DD;
   __shared__ __align__(8) uint64_t bar;
   __shared__ double red[BLOCK / 32];
@@ -151,7 +153,7 @@ __global__ void __launch_bounds__(K::BLOCK) elem_kernel(StageArgs<typename K::T>
   const int tid = threadIdx.x;
   const int e0 = blockIdx.x * TE;
   const int ne = min(TE, a.mesh.E - e0);
-  const uint32_t c_bytes = (uint32_t)(((size_t)ne * MNP * sizeof(T) + 15) / 16 * 16);
+  const uint32_t c_bytes = (uint32_t)(((size_t)ne * MNP * 8 + 15) / 16 * 16);
 
   if (tid == 0) {
     s_fail = 0;
@@ -164,13 +166,12 @@ __global__ void __launch_bounds__(K::BLOCK) elem_kernel(StageArgs<typename K::T>
     if constexpr (L::bulk_c) bulk_g2s(sC, a.C + (size_t)e0 * MNP, c_bytes, &bar);
   }
   if constexpr (!L::bulk_c) {
-    const T* src = a.C + (size_t)e0 * MNP;
+    const double* src = a.C + (size_t)e0 * MNP;
     for (int i = tid; i < ne * MNP; i += BLOCK) sC[i] = src[i];
   }
   for (int i = tid; i < ne * DD; i += BLOCK) {
     const int e = i / DD, c = i - (i / DD) * DD;
-    sJ[i] = c < DIM * DIM ? (double)a.mesh.jinv[(size_t)(e0 + e) * DIM * DIM + c]
-                          : (double)a.mesh.detj[e0 + e];
+    sJ[i] = c < DIM * DIM ? (double)a.mesh.jinv[(size_t)(e0 + e) * DIM * DIM + c] : a.mesh.detjd[e0 + e];
   }
   if (tid == 0 && !mbar_wait(&bar, 0, kMbarPolls)) {
     // record the failure, then wait once more (bounded) for the copies this
@@ -193,11 +194,11 @@ __global__ void __launch_bounds__(K::BLOCK) elem_kernel(StageArgs<typename K::T>
       T U[M];
 #pragma unroll
       for (int j = 0; j < M; ++j) {
-        T c[NP];
-        load_vec<T, NP>(sC + (e * M + j) * NP, c);
+        double c[NP];
+        load_vec<double, NP>(sC + (e * M + j) * NP, c);
         T acc = 0;
 #pragma unroll
-        for (int k = 0; k < NP; ++k) acc += phi[k] * c[k];
+        for (int k = 0; k < NP; ++k) acc += phi[k] * (T)c[k];
         U[j] = acc;
       }
       if (!is_physical<K::LAW, T>(a.law, U)) flag_nonphysical(a.status, e0 + e);
@@ -249,25 +250,27 @@ __global__ void __launch_bounds__(K::BLOCK) elem_kernel(StageArgs<typename K::T>
     const size_t gbase = ((size_t)e0 * M + row) * NP;
     if (a.stage == 0) {
 #pragma unroll
-      for (int k = 0; k < NP; ++k) a.Cout[gbase + k] = acc[k];
+      for (int k = 0; k < NP; ++k) a.Cout[gbase + k] = (double)acc[k];
     } else {
       const int e = row / M;
-      const T dtj = (T)(a.ctl->dt / sJ[e * DD + DIM * DIM]);
-      T* crow = sC + row * NP;
-      T c[NP];
-      load_vec<T, NP>(crow, c);
+      // FP64 update in the reference's operation order (dt/|J| in FP64)
+      const double dtj = a.ctl->dt / sJ[e * DD + DIM * DIM];
+      double* crow = sC + row * NP;
+      double c[NP];
+      load_vec<double, NP>(crow, c);
 #pragma unroll
       for (int k = 0; k < NP; ++k) {
-        T out;
+        const double r = (double)acc[k];
+        double out;
         if (a.stage == 1) {
           a.U0out[gbase + k] = c[k];
-          out = c[k] + acc[k] * dtj;
+          out = c[k] + r * dtj;
         } else if (a.stage == 2) {
-          out = (T)0.25 * (c[k] + acc[k] * dtj + (T)3. * a.U0[gbase + k]);
+          out = 0.25 * (c[k] + r * dtj + 3. * a.U0[gbase + k]);
         } else {
-          const T u0 = a.U0[gbase + k];
-          out = ((T)2.0 * (c[k] + acc[k] * dtj) + u0) / (T)3.0;
-          const double dd = (double)out - (double)u0;
+          const double u0 = a.U0[gbase + k];
+          out = (2.0 * (c[k] + r * dtj) + u0) / 3.0;
+          const double dd = out - u0;
           rsum += dd * dd;
         }
         crow[k] = out;
@@ -286,22 +289,22 @@ __global__ void __launch_bounds__(K::BLOCK) elem_kernel(StageArgs<typename K::T>
     // reference vertices (DGCell::computeMAXEV, DGCell.cc:1155-1207)
     for (int it = tid; it < ne * NV; it += BLOCK) {
       const int e = it / NV, v = it - (it / NV) * NV;
-      const T* c = sC + e * MNP;
-      T val[M];
+      const double* c = sC + e * MNP;
+      double val[M];
       if (v == 0) {
 #pragma unroll
-        for (int j = 0; j < M; ++j) val[j] = c[j * NP] * (T)a.tab.phi0;
+        for (int j = 0; j < M; ++j) val[j] = c[j * NP] * a.tab.phi0;
       } else {
         const double* pv = a.tab.phiv + (v - 1) * NP;
 #pragma unroll
         for (int j = 0; j < M; ++j) {
-          T acc = 0;
+          double acc = 0;
 #pragma unroll
-          for (int k = 0; k < NP; ++k) acc += (T)pv[k] * c[j * NP + k];
+          for (int k = 0; k < NP; ++k) acc += pv[k] * c[j * NP + k];
           val[j] = acc;
         }
       }
-      sEig[it] = (double)max_eigen<K::LAW, T>(a.law, val);
+      sEig[it] = max_eigen<K::LAW, double>(a.law, val);
     }
     __syncthreads();
     double dtl = 1e300;

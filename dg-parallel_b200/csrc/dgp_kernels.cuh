@@ -96,7 +96,8 @@ template <typename T>
 struct DevMesh {
   int E, F, NB;
   const T* jinv;      // E x DIM*DIM, [i][r] = d xi_r / d x_i
-  const T* detj;      // E, |det J|
+  const T* detj;      // E, |det J| (arithmetic type)
+  const double* detjd;// E, |det J| in FP64 (inverse mass of the stage update)
   const double* csize;// E, DGCell::computeCellSize
   const double* x0;   // E x 3 affine origin (FP64)
   const double* jac;  // E x 9 rows d x / d xi_r (FP64)
@@ -134,10 +135,11 @@ struct StageArgs {
   DevMesh<T> mesh;
   DevTables<T> tab;
   LawParams law;
-  const T* C;      // state the stage reads
-  const T* U0;     // u_n (stages 2 and 3)
-  T* Cout;         // state the stage writes (or the RHS when stage == 0)
-  T* U0out;        // stage 1 copies u_n here
+  // the state is FP64 in both forms; T is the arithmetic of the RHS
+  const double* C;   // state the stage reads
+  const double* U0;  // u_n (stages 2 and 3)
+  double* Cout;      // state the stage writes (or the RHS when stage == 0)
+  double* U0out;     // stage 1 copies u_n here
   T* slots;        // E x NLF x NQF x M
   TimeCtl* ctl;
   Status* status;
@@ -191,22 +193,20 @@ __device__ __forceinline__ void ldg_vec(const T* __restrict__ p, T (&out)[N]) {
 }
 
 // trace of a cell's state at one face point: U[j] = sum_k phi[k] C[j][k],
-// streamed field by field
+// streamed field by field (FP64 state converted to the arithmetic type)
 template <class K>
-__device__ __forceinline__ void cell_trace(const typename K::T* __restrict__ c, const typename K::T* phi,
+__device__ __forceinline__ void cell_trace(const double* __restrict__ c, const typename K::T* phi,
                                            typename K::T* U) {
   using T = typename K::T;
   constexpr int NP = K::NP;
-  constexpr int ALIGN = pow2_div(NP * (int)sizeof(T)) < pow2_div(K::MNP * (int)sizeof(T))
-                            ? pow2_div(NP * (int)sizeof(T))
-                            : pow2_div(K::MNP * (int)sizeof(T));
+  constexpr int ALIGN = pow2_div(NP * 8) < pow2_div(K::MNP * 8) ? pow2_div(NP * 8) : pow2_div(K::MNP * 8);
 #pragma unroll
   for (int j = 0; j < K::M; ++j) {
-    T cj[NP];
-    ldg_vec<T, NP, ALIGN>(c + j * NP, cj);
+    double cj[NP];
+    ldg_vec<double, NP, ALIGN>(c + j * NP, cj);
     T acc = 0;
 #pragma unroll
-    for (int k = 0; k < NP; ++k) acc += phi[k] * cj[k];
+    for (int k = 0; k < NP; ++k) acc += phi[k] * (T)cj[k];
     U[j] = acc;
   }
 }
@@ -261,32 +261,31 @@ __global__ void __launch_bounds__(K::FACE_BLOCK) face_kernel(StageArgs<typename 
 
 // -----------------------------------------------------------------------------
 // CFL time step of one cell: |cell| * cfl / (a (2p+1)), a = max eigenvalue at
-// the mean and (triangles) at the three reference vertices.
+// the mean and (triangles) at the three reference vertices; FP64 in both forms.
 template <class K>
-__device__ __forceinline__ double cell_dt(const StageArgs<typename K::T>& a, const typename K::T* c,
-                                          int e, double cfl) {
-  using T = typename K::T;
+__device__ __forceinline__ double cell_dt(const StageArgs<typename K::T>& a, const double* c, int e,
+                                          double cfl) {
   constexpr int M = K::M, NP = K::NP;
-  T mean[M];
+  double mean[M];
 #pragma unroll
-  for (int j = 0; j < M; ++j) mean[j] = c[j * NP] * (T)a.tab.phi0;
-  T am = max_eigen<K::LAW, T>(a.law, mean);
+  for (int j = 0; j < M; ++j) mean[j] = c[j * NP] * a.tab.phi0;
+  double am = max_eigen<K::LAW, double>(a.law, mean);
   if constexpr (K::DIM == 2) {
 #pragma unroll
     for (int v = 0; v < 3; ++v) {
-      T val[M];
+      double val[M];
 #pragma unroll
       for (int j = 0; j < M; ++j) {
-        T acc = 0;
+        double acc = 0;
 #pragma unroll
-        for (int k = 0; k < NP; ++k) acc += (T)a.tab.phiv[v * NP + k] * c[j * NP + k];
+        for (int k = 0; k < NP; ++k) acc += a.tab.phiv[v * NP + k] * c[j * NP + k];
         val[j] = acc;
       }
-      T b = max_eigen<K::LAW, T>(a.law, val);
+      double b = max_eigen<K::LAW, double>(a.law, val);
       am = (b > am ? b : am);
     }
   }
-  return a.mesh.csize[e] * cfl / ((double)am * (2. * K::ORDER + 1.0));
+  return a.mesh.csize[e] * cfl / (am * (2. * K::ORDER + 1.0));
 }
 
 __device__ __forceinline__ double ctl_finalize(TimeCtl* c, double dtmin) {
@@ -361,7 +360,7 @@ __global__ void __launch_bounds__(256) cfl_kernel(StageArgs<typename K::T> a) {
 // L2 projection of the law's field (DGCell::L2ProjInitial, DGCell.cc:1458-1483):
 // one thread per (cell, mode), FP64 accumulation in the reference's order.
 template <class K>
-__global__ void project_kernel(StageArgs<typename K::T> a, double t, typename K::T* out) {
+__global__ void project_kernel(StageArgs<typename K::T> a, double t, double* out) {
   using T = typename K::T;
   constexpr int M = K::M, NP = K::NP, NQ = K::NQ;
   const int gid = blockIdx.x * blockDim.x + threadIdx.x;
@@ -372,7 +371,7 @@ __global__ void project_kernel(StageArgs<typename K::T> a, double t, typename K:
   double proj[M];
 #pragma unroll
   for (int j = 0; j < M; ++j) proj[j] = 0.0;
-  const double detj = (double)a.mesh.detj[e];
+  const double detj = a.mesh.detjd[e];
   for (int q = 0; q < NQ; ++q) {
     double x[3];
     const double* xi = a.tab.qpd + 3 * q;
@@ -386,7 +385,7 @@ __global__ void project_kernel(StageArgs<typename K::T> a, double t, typename K:
     for (int j = 0; j < M; ++j) proj[j] += val[j] * a.tab.phiq[q * NP + k] * jw;
   }
   const double inv = 1. / detj;
-  for (int j = 0; j < M; ++j) out[(size_t)e * K::MNP + j * NP + k] = (T)(proj[j] * inv);
+  for (int j = 0; j < M; ++j) out[(size_t)e * K::MNP + j * NP + k] = proj[j] * inv;
 }
 
 // per-block partial sums of (u_h - u_exact)^2 |J| w of one field over the
@@ -402,7 +401,7 @@ __global__ void __launch_bounds__(256) l2err_kernel(StageArgs<typename K::T> a, 
     const double* x0 = a.mesh.x0 + 3 * (size_t)e;
     const double* J = a.mesh.jac + 9 * (size_t)e;
     const auto* c = a.C + (size_t)e * K::MNP;
-    const double detj = (double)a.mesh.detj[e];
+    const double detj = a.mesh.detjd[e];
     for (int q = 0; q < a.tab.nqe; ++q) {
       double x[3];
       const double* xi = a.tab.eqp + 3 * q;
@@ -431,7 +430,7 @@ __global__ void __launch_bounds__(256) totals_kernel(StageArgs<typename K::T> a,
   for (int j = 0; j < K::M; ++j) {
     double v = 0.0;
     if (e < a.mesh.E)
-      v = (double)a.mesh.detj[e] * refm * a.tab.phi0 * (double)a.C[(size_t)e * K::MNP + j * K::NP];
+      v = a.mesh.detjd[e] * refm * a.tab.phi0 * a.C[(size_t)e * K::MNP + j * K::NP];
     v = block_sum<256>(v, red);
     if (threadIdx.x == 0) partials[(size_t)blockIdx.x * K::M + j] = v;
   }

@@ -76,7 +76,7 @@ extern "C" int dgp_rhs_noalloc(dgp_solver s, const double* dev_state, double t, 
   DGP_CUDA(cudaSetDevice(s->device));
   const size_t tsize = s->ops.tsize;
   const int E = s->b.E, mnp = s->b.M * s->b.NP;
-  const size_t state_b = round256(s->state_count() * tsize);
+  const size_t state_b = round256(s->state_count() * 8);  // FP64 state and RHS
   const size_t ntiles = (static_cast<size_t>(E) + s->ops.TE - 1) / s->ops.TE;
   const size_t slot_b = round256(ntiles * s->ops.TE * s->tab.nlf * s->tab.nqf * s->b.M * tsize);
   const size_t need = 2 * state_b + slot_b;
@@ -93,12 +93,8 @@ extern "C" int dgp_rhs_noalloc(dgp_solver s, const double* dev_state, double t, 
   b.rhs = p + state_b + slot_b;
   const long long n = static_cast<long long>(E) * mnp;
   const int grid = static_cast<int>((n + 255) / 256);
-  if (tsize == 8)
-    permute_rows<double, double><<<grid, 256, 0, s->stream>>>(dev_state, static_cast<double*>(b.C),
-                                                               s->d_i2f, E, mnp);
-  else
-    permute_rows<double, float><<<grid, 256, 0, s->stream>>>(dev_state, static_cast<float*>(b.C),
-                                                              s->d_i2f, E, mnp);
+  permute_rows<double, double><<<grid, 256, 0, s->stream>>>(dev_state, static_cast<double*>(b.C),
+                                                             s->d_i2f, E, mnp);
   dgp::TimeCtl c{};
   c.t = t;
   c.dtmin_bits = 0x7FF0000000000000ull;
@@ -106,12 +102,8 @@ extern "C" int dgp_rhs_noalloc(dgp_solver s, const double* dev_state, double t, 
   DGP_CUDA(cudaMemcpyAsync(s->b.ctl, &s->h_ctl[0], sizeof(dgp::TimeCtl), cudaMemcpyHostToDevice, s->stream));
   s->ops.face(b, 0, 0.0, s->stream);
   s->ops.elem(b, 0, 0, s->stream);
-  if (tsize == 8)
-    permute_rows<double, double><<<grid, 256, 0, s->stream>>>(static_cast<const double*>(b.rhs), dev_rhs,
-                                                               s->d_f2i, E, mnp);
-  else
-    permute_rows<float, double><<<grid, 256, 0, s->stream>>>(static_cast<const float*>(b.rhs), dev_rhs,
-                                                              s->d_f2i, E, mnp);
+  permute_rows<double, double><<<grid, 256, 0, s->stream>>>(static_cast<const double*>(b.rhs), dev_rhs,
+                                                             s->d_f2i, E, mnp);
   DGP_CUDA(cudaGetLastError());
   DGP_CUDA(cudaStreamSynchronize(s->stream));
   return DGP_OK;

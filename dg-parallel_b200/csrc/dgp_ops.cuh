@@ -28,7 +28,7 @@ StageArgs<typename K::T> stage_args(const DeviceBuffers& b, int stage, double ti
   a.stage = stage;
   a.stage_time_factor = time_factor;
   a.fuse_cfl = fuse_cfl;
-  if (stage == 0) a.Cout = static_cast<T*>(b.rhs);
+  if (stage == 0) a.Cout = static_cast<double*>(b.rhs);
   return a;
 }
 
@@ -62,7 +62,7 @@ void ops_project(const DeviceBuffers& b, double t, cudaStream_t st) {
   using T = typename K::T;
   StageArgs<T> a = make_args<T>(b);
   const long long n = static_cast<long long>(b.E) * K::NP;
-  project_kernel<K><<<static_cast<int>((n + 127) / 128), 128, 0, st>>>(a, t, static_cast<T*>(b.C));
+  project_kernel<K><<<static_cast<int>((n + 127) / 128), 128, 0, st>>>(a, t, static_cast<double*>(b.C));
 }
 
 template <class K>

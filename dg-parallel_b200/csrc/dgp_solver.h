@@ -19,6 +19,7 @@ struct DeviceBuffers {
   int E = 0, F = 0, NB = 0, order = 0, dim = 0, M = 0, NP = 0;
   void* jinv = nullptr;
   void* detj = nullptr;
+  double* detjd = nullptr;
   double* csize = nullptr;
   double* x0 = nullptr;
   double* jac = nullptr;
@@ -65,6 +66,7 @@ inline StageArgs<T> make_args(const DeviceBuffers& b) {
   a.mesh.NB = b.NB;
   a.mesh.jinv = static_cast<const T*>(b.jinv);
   a.mesh.detj = static_cast<const T*>(b.detj);
+  a.mesh.detjd = b.detjd;
   a.mesh.csize = b.csize;
   a.mesh.x0 = b.x0;
   a.mesh.jac = b.jac;
@@ -92,10 +94,10 @@ inline StageArgs<T> make_args(const DeviceBuffers& b) {
   a.tab.ephi = b.ephi;
   a.tab.phi0 = b.phi0;
   a.law = b.law;
-  a.C = static_cast<const T*>(b.C);
-  a.U0 = static_cast<const T*>(b.U0);
-  a.Cout = static_cast<T*>(b.C);
-  a.U0out = static_cast<T*>(b.U0);
+  a.C = static_cast<const double*>(b.C);
+  a.U0 = static_cast<const double*>(b.U0);
+  a.Cout = static_cast<double*>(b.C);
+  a.U0out = static_cast<double*>(b.U0);
   a.slots = static_cast<T*>(b.slots);
   a.ctl = b.ctl;
   a.status = b.status;
