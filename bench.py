@@ -242,7 +242,9 @@ def main():
         assert n == args.steps
         err = s.l2_error(t_end, 0)
         kern = s.profile_kernels(20)
+        launches = s.launches_per_step() * 8 * ((args.steps + 7) // 8) + 1  # graphs of 8 steps + first CFL
         results[name] = {"seconds": sec, "value": units_per_step * args.steps * world / sec,
+                         "gpu_launches": launches,
                          "t_end": t_end, "density_l2_vs_exact": err, "kernel_ms": kern.tolist(),
                          "solver": s}
     fp64, mixed = results["fp64"], results["mixed"]
@@ -341,7 +343,7 @@ def main():
             "e2e": {"value": e2e_value, "unit": "DOF-stage/s", "h2d_bytes_per_step": nbytes,
                     "d2h_bytes_per_step": nbytes, "steps": args.e2e_steps,
                     "timing": "host wall clock, synchronized, C ABI with pinned host state"},
-            "gpu_launches": 48 * ((args.steps + 7) // 8) + 1,  # graphs of 8 steps x 6 kernels + first CFL
+            "gpu_launches": fp64["gpu_launches"],
             "clocks": clocks,
         }
         print(json.dumps(line))

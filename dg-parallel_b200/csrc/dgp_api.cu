@@ -16,6 +16,7 @@
 #include "../../include/dgp.h"
 #include "dgp_host.h"
 #include "dgp_handles.h"
+#include "dgp_limiter.cuh"
 #include "dgp_solver.h"
 
 namespace dgp {
@@ -79,6 +80,72 @@ uint64_t spread3(uint32_t x) {
 
 using namespace dgp;
 
+
+// Triangle moment limiter data in the internal cell order: neighbours by
+// bounding boxes (DGLimiter.cc:970-993, DGCell.cc:76-86), FP64 geometry of the
+// derivative transforms and the bounding-box centres, degree tables.
+static int setup_limiter(dgp_solver s) {
+  const HostMesh& m = s->mesh;
+  const int E = m.E;
+  std::vector<double> bmin(2 * (size_t)E), bmax(2 * (size_t)E), bbc(2 * (size_t)E);
+  for (int e = 0; e < E; ++e) {
+    const int* c = &m.cv[static_cast<size_t>(e) * m.nvc];
+    for (int k = 0; k < 2; ++k) bmin[2 * e + k] = bmax[2 * e + k] = m.X[3 * c[0] + k];
+    for (int v = 1; v < m.nvc; ++v)
+      for (int k = 0; k < 2; ++k) {
+        const double x = m.X[3 * c[v] + k];
+        if (x < bmin[2 * e + k]) bmin[2 * e + k] = x;
+        if (x > bmax[2 * e + k]) bmax[2 * e + k] = x;
+      }
+    for (int k = 0; k < 2; ++k) bbc[2 * e + k] = (bmin[2 * e + k] + bmax[2 * e + k]) / 2.;
+  }
+  std::vector<int> cf(3 * (size_t)E, -1);  // face of (cell, local face)
+  for (int f = 0; f < m.F; ++f) {
+    cf[3 * (size_t)m.eL[f] + m.lfL[f]] = f;
+    if (m.eR[f] >= 0) cf[3 * (size_t)m.eR[f] + m.lfR[f]] = f;
+  }
+  std::vector<int> nb(4 * (size_t)E, -1);
+  std::vector<double> geo(static_cast<size_t>(E) * kLimGeo);
+  for (int i = 0; i < E; ++i) {
+    const int e = s->i2f[i];
+    const double px = bbc[2 * e], py = bbc[2 * e + 1];
+    int* n = &nb[4 * (size_t)i];
+    for (int lf = 0; lf < 3; ++lf) {
+      const int f = cf[3 * (size_t)e + lf];
+      if (f < 0 || m.eR[f] < 0) continue;
+      const int o = (m.eL[f] == e) ? m.eR[f] : m.eL[f];
+      const int oi = s->f2i[o];
+      if (px > bmax[2 * o]) n[0] = oi;
+      if (px < bmin[2 * o]) n[1] = oi;
+      if (py > bmax[2 * o + 1]) n[2] = oi;
+      if (py < bmin[2 * o + 1]) n[3] = oi;
+    }
+    double X0[3], J[9], Ji[9];
+    cell_frame(m, e, X0, J);
+    invert3(J, Ji);
+    double* g = &geo[static_cast<size_t>(i) * kLimGeo];
+    g[0] = Ji[0];
+    g[1] = Ji[1];
+    g[2] = Ji[3];
+    g[3] = Ji[4];
+    g[4] = J[0];
+    g[5] = J[1];
+    g[6] = J[3];
+    g[7] = J[4];
+    g[8] = px;
+    g[9] = py;
+  }
+  std::vector<double> D, Dinv;
+  build_limiter_tables(s->tab, D, Dinv);
+  DeviceBuffers& b = s->b;
+  int rc = DGP_OK;
+  if ((rc = s->upload(&b.nb, nb)) || (rc = s->upload(&b.lgeo, geo)) || (rc = s->upload(&b.limD, D)) ||
+      (rc = s->upload(&b.limDinv, Dinv)) || (rc = s->alloc(&b.trig, static_cast<size_t>(E))) ||
+      (rc = s->alloc(&b.L, s->state_count())))
+    return rc;
+  DGP_CUDA(cudaMemset(b.trig, 0, E));
+  return DGP_OK;
+}
 
 extern "C" {
 
@@ -181,8 +248,10 @@ int dgp_solver_create(dgp_mesh mh, dgp_law law, int order, int precision, int li
   if (!mh || !law || !out) return fail(DGP_ERR_INVALID, "null argument");
   if (precision != DGP_PRECISION_FP64 && precision != DGP_PRECISION_MIXED)
     return fail(DGP_ERR_INVALID, "unknown precision");
-  if (limiter != DGP_LIMITER_NONE) return fail(DGP_ERR_UNSUPPORTED, "limiter not built for this path");
+  if (limiter != DGP_LIMITER_NONE && limiter != DGP_LIMITER_MOMENT) return fail(DGP_ERR_INVALID, "unknown limiter");
   const HostMesh& m = mh->m;
+  if (limiter == DGP_LIMITER_MOMENT && m.dim != 2)
+    return fail(DGP_ERR_UNSUPPORTED, "the moment limiter is built for triangles only");
   if ((law->kind == DGP_LAW_EULER2D || law->kind == DGP_LAW_BURGERS2D) && m.dim != 2)
     return fail(DGP_ERR_UNSUPPORTED, "2D law on a 3D mesh");
   if ((law->kind == DGP_LAW_EULER3D || law->kind == DGP_LAW_MAXWELL3D) && m.dim != 3)
@@ -382,6 +451,14 @@ int dgp_solver_create(dgp_mesh mh, dgp_law law, int order, int precision, int li
       (rc = s->alloc(&b.status, 1)))
     return bail(rc);
   DGP_CUDA(cudaMemset(slots, 0, nslot * ts));
+  // P0 fallback marks (DGCell::setToZero), on by default for the Euler laws
+  // whose isPhysical can fail
+  if ((rc = s->alloc(&b.bad, static_cast<size_t>(E)))) return bail(rc);
+  DGP_CUDA(cudaMemset(b.bad, 0, E));
+  b.p0 = (law->kind == DGP_LAW_EULER2D || law->kind == DGP_LAW_EULER3D) ? 1 : 0;
+  if (limiter == DGP_LIMITER_MOMENT && order >= 1) {
+    if ((rc = setup_limiter(s))) return bail(rc);
+  }
   TimeCtl c0{};
   c0.dtmin_bits = 0x7FF0000000000000ull;
   DGP_CUDA(cudaMemcpy(b.ctl, &c0, sizeof(TimeCtl), cudaMemcpyHostToDevice));
@@ -438,6 +515,8 @@ int dgp_project(dgp_solver s, double t) {
   if (!s) return fail(DGP_ERR_INVALID, "null solver");
   DGP_CUDA(cudaSetDevice(s->device));
   s->ops.project(s->b, t, s->stream);
+  // DGAnalysis::DGAnalysis limits the projected state once (DGAnalysis.cc:276-291)
+  if (s->limiter == DGP_LIMITER_MOMENT && s->ops.limit) s->ops.limit(s->b, 0, s->stream);
   DGP_CUDA(cudaGetLastError());
   DGP_CUDA(cudaStreamSynchronize(s->stream));
   return DGP_OK;
@@ -524,10 +603,27 @@ int dgp_cfl_dt(dgp_solver s, double cfl, double* dt) {
   return DGP_OK;
 }
 
+// RungeKuttaTVD3::advanceInTime: with the limiter, TimeIntegrator::limit
+// follows every stage and the next step's CFL reduction runs on the limited
+// state (instead of inside the last stage's element kernel)
 static void launch_step(dgp_solver s, int fuse_cfl) {
+  const bool lim = s->limiter == DGP_LIMITER_MOMENT && s->ops.limit;
   s->ops.stage(s->b, 1, 0.0, 0, s->stream);
+  if (lim) s->ops.limit(s->b, 1, s->stream);
   s->ops.stage(s->b, 2, 1.0, 0, s->stream);
-  s->ops.stage(s->b, 3, 0.5, fuse_cfl, s->stream);
+  if (lim) s->ops.limit(s->b, 1, s->stream);
+  s->ops.stage(s->b, 3, 0.5, lim ? 0 : fuse_cfl, s->stream);
+  if (lim) {
+    s->ops.limit(s->b, 1, s->stream);
+    if (fuse_cfl) s->ops.cfl(s->b, s->stream);
+  }
+}
+
+int dgp_launches_per_step(dgp_solver s, int* n) {
+  if (!s || !n) return fail(DGP_ERR_INVALID, "null argument");
+  const bool lim = s->limiter == DGP_LIMITER_MOMENT && s->ops.limit;
+  *n = 3 * (s->b.p0 ? 3 : 2) + (lim ? 3 * 2 + 1 : 0);
+  return DGP_OK;
 }
 
 int dgp_step(dgp_solver s, double t, double dt, double* resid) {
@@ -576,6 +672,42 @@ int dgp_run(dgp_solver s, double t0, double tend, double cfl, int max_steps, dou
   }
   if (t_out) *t_out = c.t;
   if (steps_out) *steps_out = c.steps;
+  return DGP_OK;
+}
+
+int dgp_limit(dgp_solver s, unsigned char* triggers) {
+  if (!s) return fail(DGP_ERR_INVALID, "null solver");
+  if (s->limiter != DGP_LIMITER_MOMENT) return fail(DGP_ERR_INVALID, "solver created without a limiter");
+  DGP_CUDA(cudaSetDevice(s->device));
+  if (s->ops.limit) s->ops.limit(s->b, 0, s->stream);
+  DGP_CUDA(cudaGetLastError());
+  DGP_CUDA(cudaStreamSynchronize(s->stream));
+  return triggers ? dgp_limiter_triggers(s, triggers) : DGP_OK;
+}
+
+int dgp_limiter_triggers(dgp_solver s, unsigned char* out) {
+  if (!s || !out) return fail(DGP_ERR_INVALID, "null argument");
+  if (s->limiter != DGP_LIMITER_MOMENT) return fail(DGP_ERR_INVALID, "solver created without a limiter");
+  DGP_CUDA(cudaSetDevice(s->device));
+  DGP_CUDA(cudaStreamSynchronize(s->stream));
+  const int E = s->b.E;
+  if (!s->b.trig) {  // P0: nothing is ever limited
+    std::memset(out, 0, E);
+    return DGP_OK;
+  }
+  std::vector<unsigned char> t(E);
+  DGP_CUDA(cudaMemcpy(t.data(), s->b.trig, E, cudaMemcpyDeviceToHost));
+  for (int i = 0; i < E; ++i) out[s->i2f[i]] = t[i];
+  return DGP_OK;
+}
+
+int dgp_set_p0_fallback(dgp_solver s, int on) {
+  if (!s) return fail(DGP_ERR_INVALID, "null solver");
+  if (s->graph) {
+    cudaGraphExecDestroy(s->graph);
+    s->graph = nullptr;
+  }
+  s->b.p0 = on ? 1 : 0;
   return DGP_OK;
 }
 

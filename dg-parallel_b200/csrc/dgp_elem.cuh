@@ -169,6 +169,7 @@ __global__ void __launch_bounds__(K::BLOCK) elem_kernel(StageArgs<typename K::T>
     const double* src = a.C + (size_t)e0 * MNP;
     for (int i = tid; i < ne * MNP; i += BLOCK) sC[i] = src[i];
   }
+  const bool p0_mark = a.p0 && tid < ne && a.bad[e0 + tid];
   for (int i = tid; i < ne * DD; i += BLOCK) {
     const int e = i / DD, c = i - (i / DD) * DD;
     sJ[i] = c < DIM * DIM ? (double)a.mesh.jinv[(size_t)(e0 + e) * DIM * DIM + c] : a.mesh.detjd[e0 + e];
@@ -182,6 +183,10 @@ __global__ void __launch_bounds__(K::BLOCK) elem_kernel(StageArgs<typename K::T>
   }
   __syncthreads();
   if (s_fail) return;
+  // P0 fallback: the face passes marked cells and zeroed their modes; the
+  // marks of this tile's cells are consumed here
+  if (p0_mark) a.bad[e0 + tid] = 0;
+  if (a.p0 && blockIdx.x == 0 && tid == 0) a.status->stage_bad = 0;
 
   // volume: fixed quadrature point per thread
   if (tid < K::EG * NQ) {

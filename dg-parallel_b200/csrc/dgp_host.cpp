@@ -477,6 +477,31 @@ void basis_eval(const RefTables& t, const double* xi, double* out) {
   }
 }
 
+void build_limiter_tables(const RefTables& t, std::vector<double>& D, std::vector<double>& Dinv) {
+  const int P = t.order;
+  const size_t total = static_cast<size_t>((P + 1) * (P + 2) * (2 * P + 3) / 6);
+  D.assign(total, 0.0);
+  Dinv.assign(total, 0.0);
+  for (int n = 0; n <= P; ++n) {
+    const int base = n * (n + 1) / 2, w = n + 1, off = n * (n + 1) * (2 * n + 1) / 6;
+    long double A[5][5], X[5][5];
+    for (int i = 0; i <= n; ++i)
+      for (int m = 0; m <= n; ++m) {
+        const double f = static_cast<double>(factl(n - i) * factl(i));
+        D[off + i * w + m] = f * t.G[base + m][base + i];
+        A[i][m] = static_cast<long double>(D[off + i * w + m]);
+      }
+    for (int k = 0; k <= n; ++k)  // column k of the inverse, back substitution
+      for (int i = n; i >= 0; --i) {
+        long double r = (i == k) ? 1.0L : 0.0L;
+        for (int m = i + 1; m <= n; ++m) r -= A[i][m] * X[m][k];
+        X[i][k] = r / A[i][i];
+      }
+    for (int m = 0; m <= n; ++m)
+      for (int i = 0; i <= n; ++i) Dinv[off + m * w + i] = static_cast<double>(X[m][i]);
+  }
+}
+
 int build_tables(int dim, int order, RefTables& t, std::string& err) {
   t = RefTables();
   t.dim = dim;

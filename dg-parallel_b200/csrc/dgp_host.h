@@ -65,6 +65,10 @@ struct RefTables {
 
 int build_tables(int dim, int order, RefTables& t, std::string& err);
 void basis_eval(const RefTables& t, const double* xi, double* out);
+// triangle moment limiter tables, per degree n a (n+1)^2 block at
+// n(n+1)(2n+1)/6: D[i][m] = d^n phi_(n,m) / du^(n-i) dv^i (constant on the
+// cell) and its inverse (D is upper triangular)
+void build_limiter_tables(const RefTables& t, std::vector<double>& D, std::vector<double>& Dinv);
 
 // Affine frame of a cell: x = x0 + sum_r xi_r J[r][:], with the node order of
 // MeshMapping::GeomShapeFunctionTri/Tet (Mapping.cc:40-71, 94-103).

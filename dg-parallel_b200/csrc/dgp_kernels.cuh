@@ -88,7 +88,7 @@ struct Status {
   int nonphysical;
   int first_bad;  // internal cell index, INT_MAX when none
   int timeouts;   // bounded waits on bulk copies that gave up (never expected)
-  int pad;
+  int stage_bad;  // cells marked for the P0 fallback in the current stage
 };
 
 // device views (internal cell order); T = arithmetic type of the hot path
@@ -145,14 +145,24 @@ struct StageArgs {
   Status* status;
   double* partials;  // per-block residual partials (stage 3)
   double stage_time_factor;  // 0, 1, 0.5: boundary time = t + factor * dt
+  unsigned char* bad;  // [E] P0-fallback marks (DGCell::setToZero)
   int stage;       // 0: RHS only, 1..3: SSP-RK3 stages
   int fuse_cfl;    // stage 3 reduces the next step's dt
   int order;
+  int p0;          // 1: P0 fallback on (face kernel marks, element kernel consumes marks)
 };
 
 __device__ __forceinline__ void flag_nonphysical(Status* st, int cell) {
   atomicAdd(&st->nonphysical, 1);
   atomicMin(&st->first_bad, cell);
+}
+
+template <typename T>
+__device__ __forceinline__ void mark_p0(const StageArgs<T>& a, int cell) {
+  if (!a.bad[cell]) {
+    a.bad[cell] = 1;
+    atomicAdd(&a.status->stage_bad, 1);
+  }
 }
 
 // -----------------------------------------------------------------------------
@@ -196,10 +206,15 @@ __device__ __forceinline__ void ldg_vec(const T* __restrict__ p, T (&out)[N]) {
 // streamed field by field (FP64 state converted to the arithmetic type)
 template <class K>
 __device__ __forceinline__ void cell_trace(const double* __restrict__ c, const typename K::T* phi,
-                                           typename K::T* U) {
+                                           typename K::T* U, bool p0 = false) {
   using T = typename K::T;
   constexpr int NP = K::NP;
   constexpr int ALIGN = pow2_div(NP * 8) < pow2_div(K::MNP * 8) ? pow2_div(NP * 8) : pow2_div(K::MNP * 8);
+  if (p0) {  // cell dropped to P0: its trace is the mean
+#pragma unroll
+    for (int j = 0; j < K::M; ++j) U[j] = phi[0] * (T)__ldg(c + j * NP);
+    return;
+  }
 #pragma unroll
   for (int j = 0; j < K::M; ++j) {
     double cj[NP];
@@ -211,22 +226,15 @@ __device__ __forceinline__ void cell_trace(const double* __restrict__ c, const t
   }
 }
 
-template <class K>
-__global__ void __launch_bounds__(K::FACE_BLOCK) face_kernel(StageArgs<typename K::T> a) {
+// One face point: traces of both sides, numerical (or boundary) flux, the two
+// face slots.  RERUN: second pass of the P0 fallback, where the traces of
+// marked cells are their means.
+template <class K, bool RERUN>
+__device__ __forceinline__ void face_point(const StageArgs<typename K::T>& a, int f, int q,
+                                           const typename K::T* s_phif, const typename K::T* s_fqw,
+                                           const int* s_qmap) {
   using T = typename K::T;
   constexpr int M = K::M, NP = K::NP, NQF = K::NQF, DIM = K::DIM, MNP = K::MNP;
-  if (a.ctl->done) return;
-  __shared__ T s_phif[K::NLF * NQF * NP];
-  __shared__ T s_fqw[NQF];
-  __shared__ int s_qmap[K::NPERM * NQF];
-  const int tid = threadIdx.x;
-  for (int i = tid; i < K::NLF * NQF * NP; i += blockDim.x) s_phif[i] = a.tab.phif[i];
-  for (int i = tid; i < NQF; i += blockDim.x) s_fqw[i] = a.tab.fqw[i];
-  for (int i = tid; i < K::NPERM * NQF; i += blockDim.x) s_qmap[i] = a.tab.qmap[i];
-  __syncthreads();
-  const int fl = tid / NQF, q = tid - (tid / NQF) * NQF;
-  const int f = blockIdx.x * K::FPB + fl;
-  if (fl >= K::FPB || f >= a.mesh.F) return;
   const int eL = a.mesh.fel[2 * f], eR = a.mesh.fel[2 * f + 1];
   const int code = a.mesh.fcode[f];
   const int lfL = code & 15, lfR = (code >> 4) & 15, perm = code >> 8;
@@ -235,13 +243,19 @@ __global__ void __launch_bounds__(K::FACE_BLOCK) face_kernel(StageArgs<typename 
   for (int i = 0; i < DIM; ++i) n[i] = a.mesh.fnrm[f * DIM + i];
   const T jw = a.mesh.fj[f] * s_fqw[q];
   T UL[M], UR[M], flux[M];
-  cell_trace<K>(a.C + (size_t)eL * MNP, s_phif + (lfL * NQF + q) * NP, UL);
-  if (!is_physical<K::LAW, T>(a.law, UL)) flag_nonphysical(a.status, eL);
+  cell_trace<K>(a.C + (size_t)eL * MNP, s_phif + (lfL * NQF + q) * NP, UL, RERUN && a.bad[eL]);
+  if (!RERUN && !is_physical<K::LAW, T>(a.law, UL)) {
+    flag_nonphysical(a.status, eL);
+    if (a.p0) mark_p0(a, eL);
+  }
   int qR = 0;
   if (eR >= 0) {
     qR = s_qmap[perm * NQF + q];
-    cell_trace<K>(a.C + (size_t)eR * MNP, s_phif + (lfR * NQF + qR) * NP, UR);
-    if (!is_physical<K::LAW, T>(a.law, UR)) flag_nonphysical(a.status, eR);
+    cell_trace<K>(a.C + (size_t)eR * MNP, s_phif + (lfR * NQF + qR) * NP, UR, RERUN && a.bad[eR]);
+    if (!RERUN && !is_physical<K::LAW, T>(a.law, UR)) {
+      flag_nonphysical(a.status, eR);
+      if (a.p0) mark_p0(a, eR);
+    }
     numerical_flux<K::LAW, K::FLUX, DIM, T>(a.law, n, UL, UR, flux);
   } else {
     const int b = -eR - 1;
@@ -256,6 +270,62 @@ __global__ void __launch_bounds__(K::FACE_BLOCK) face_kernel(StageArgs<typename 
     T* sr = a.slots + slot_index<K>(eR, lfR * NQF + qR, 0);
 #pragma unroll
     for (int j = 0; j < M; ++j) sr[j] = flux[j] * jw;
+  }
+}
+
+template <class K>
+__device__ __forceinline__ void face_tables(const StageArgs<typename K::T>& a, typename K::T* s_phif,
+                                            typename K::T* s_fqw, int* s_qmap) {
+  constexpr int NQF = K::NQF, NP = K::NP;
+  const int tid = threadIdx.x;
+  for (int i = tid; i < K::NLF * NQF * NP; i += blockDim.x) s_phif[i] = a.tab.phif[i];
+  for (int i = tid; i < NQF; i += blockDim.x) s_fqw[i] = a.tab.fqw[i];
+  for (int i = tid; i < K::NPERM * NQF; i += blockDim.x) s_qmap[i] = a.tab.qmap[i];
+  __syncthreads();
+}
+
+// P0 fallback (DGAnalysis.cc:392-417, DGCell::setToZero DGCell.cc:785-811): with
+// a.p0 set the face kernel marks every cell with a non-physical trace at a face
+// point; face_rerun_kernel then recomputes every face with the marked cells'
+// traces taken as their means and drops their modes k >= 1.
+template <class K>
+__global__ void __launch_bounds__(K::FACE_BLOCK) face_kernel(StageArgs<typename K::T> a) {
+  using T = typename K::T;
+  if (a.ctl->done) return;
+  __shared__ T s_phif[K::NLF * K::NQF * K::NP];
+  __shared__ T s_fqw[K::NQF];
+  __shared__ int s_qmap[K::NPERM * K::NQF];
+  face_tables<K>(a, s_phif, s_fqw, s_qmap);
+  const int tid = threadIdx.x;
+  const int fl = tid / K::NQF, q = tid - (tid / K::NQF) * K::NQF;
+  const int f = blockIdx.x * K::FPB + fl;
+  if (fl >= K::FPB || f >= a.mesh.F) return;
+  face_point<K, false>(a, f, q, s_phif, s_fqw, s_qmap);
+}
+
+// Second pass of the P0 fallback on a small grid: returns at once unless a
+// cell was marked in this stage (the common case costs one tiny launch).  The
+// faces read only the means of marked cells while the modes k >= 1 of those
+// cells are zeroed, so both run in the same pass.
+template <class K>
+__global__ void __launch_bounds__(K::FACE_BLOCK) face_rerun_kernel(StageArgs<typename K::T> a) {
+  using T = typename K::T;
+  if (a.ctl->done) return;
+  if (*(volatile int*)&a.status->stage_bad == 0) return;
+  __shared__ T s_phif[K::NLF * K::NQF * K::NP];
+  __shared__ T s_fqw[K::NQF];
+  __shared__ int s_qmap[K::NPERM * K::NQF];
+  face_tables<K>(a, s_phif, s_fqw, s_qmap);
+  const int tid = threadIdx.x;
+  for (int e = blockIdx.x * blockDim.x + tid; e < a.mesh.E; e += gridDim.x * blockDim.x)
+    if (a.bad[e])
+      for (int r = 0; r < K::M; ++r)
+        for (int k = 1; k < K::NP; ++k) a.Cout[((size_t)e * K::M + r) * K::NP + k] = 0.0;
+  const int fl = tid / K::NQF, q = tid - (tid / K::NQF) * K::NQF;
+  if (fl >= K::FPB) return;
+  for (int vb = blockIdx.x; vb * K::FPB < a.mesh.F; vb += gridDim.x) {
+    const int f = vb * K::FPB + fl;
+    if (f < a.mesh.F) face_point<K, true>(a, f, q, s_phif, s_fqw, s_qmap);
   }
 }
 

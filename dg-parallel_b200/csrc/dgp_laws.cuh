@@ -401,6 +401,10 @@ __device__ __forceinline__ void boundary_flux(const LawParams& lp, int bid, cons
     } else {
       flux[0] = nv * Q[0];
     }
+  } else if constexpr (LAW == DGP_LAW_BURGERS2D && FLUX == DGP_FLUX_LLF) {
+    // Lax-Friedrichs (no counterpart in DG-Parallel): far field as the ghost state
+    field_eval<T>(lp, x, time, f);
+    numerical_flux<LAW, FLUX, DIM, T>(lp, n, Q, f, flux);
   } else if constexpr (LAW == DGP_LAW_BURGERS2D) {  // Burgers2D::boundaryFlux, Burgers2D.cc:30-54
     T nvel = Q[0] * Q[0] * (T)0.5 * (n[0] + n[1]);
     if (nvel < 0) {

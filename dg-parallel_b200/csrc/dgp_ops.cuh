@@ -3,6 +3,7 @@
 #pragma once
 
 #include "dgp_elem.cuh"
+#include "dgp_limiter.cuh"
 #include "dgp_solver.h"
 
 namespace dgp {
@@ -28,6 +29,7 @@ StageArgs<typename K::T> stage_args(const DeviceBuffers& b, int stage, double ti
   a.stage = stage;
   a.stage_time_factor = time_factor;
   a.fuse_cfl = fuse_cfl;
+  a.p0 = (stage > 0 && b.p0) ? 1 : 0;
   if (stage == 0) a.Cout = static_cast<double*>(b.rhs);
   return a;
 }
@@ -39,6 +41,14 @@ void ops_face(const DeviceBuffers& b, int stage, double time_factor, cudaStream_
   face_kernel<K><<<fgrid, K::FACE_BLOCK, 0, st>>>(a);
 }
 
+// second face pass of the P0 fallback (a no-op unless a cell was marked)
+template <class K>
+void ops_face_rerun(const DeviceBuffers& b, int stage, double time_factor, cudaStream_t st) {
+  auto a = stage_args<K>(b, stage, time_factor, 0);
+  const int fgrid = (b.F + K::FPB - 1) / K::FPB;
+  face_rerun_kernel<K><<<fgrid < 296 ? fgrid : 296, K::FACE_BLOCK, 0, st>>>(a);
+}
+
 template <class K>
 void ops_elem(const DeviceBuffers& b, int stage, int fuse_cfl, cudaStream_t st) {
   auto a = stage_args<K>(b, stage, 0.0, fuse_cfl);
@@ -48,7 +58,29 @@ void ops_elem(const DeviceBuffers& b, int stage, int fuse_cfl, cudaStream_t st) 
 template <class K>
 void ops_stage(const DeviceBuffers& b, int stage, double time_factor, int fuse_cfl, cudaStream_t st) {
   ops_face<K>(b, stage, time_factor, st);
+  if (stage > 0 && b.p0) ops_face_rerun<K>(b, stage, time_factor, st);
   ops_elem<K>(b, stage, fuse_cfl, st);
+}
+
+// triangle moment limiter on the current state: limited rows of triggered
+// cells into L, then copied back
+template <class K>
+void ops_limit(const DeviceBuffers& b, int check_done, cudaStream_t st) {
+  if constexpr (K::DIM == 2 && K::ORDER >= 1) {
+    LimArgs a;
+    a.C = static_cast<const double*>(b.C);
+    a.L = b.L;
+    a.trig = b.trig;
+    a.nb = b.nb;
+    a.geo = b.lgeo;
+    a.Dn = b.limD;
+    a.Dinv = b.limDinv;
+    a.ctl = check_done ? b.ctl : nullptr;
+    a.E = b.E;
+    limit_kernel<K><<<(b.E + 127) / 128, 128, 0, st>>>(a);
+    const long long n = static_cast<long long>(b.E) * K::MNP;
+    limit_apply_kernel<K><<<static_cast<int>((n + 255) / 256), 256, 0, st>>>(a);
+  }
 }
 
 template <class K>
@@ -100,6 +132,7 @@ Ops make_ops() {
   o.l2err = &ops_l2err<K>;
   o.totals = &ops_totals<K>;
   o.grid_elem = &ops_grid_elem<K>;
+  o.limit = (K::DIM == 2 && K::ORDER >= 1) ? &ops_limit<K> : nullptr;
   return o;
 }
 

@@ -56,6 +56,15 @@ struct DeviceBuffers {
   double* partials = nullptr;
   int npartials = 0;
   LawParams law{};
+  // P0 fallback and triangle moment limiter
+  int p0 = 0;                     // 1: DGCell::setToZero fallback on
+  unsigned char* bad = nullptr;   // [E] P0 marks
+  unsigned char* trig = nullptr;  // [E] trigger degree of the last limiter pass
+  double* L = nullptr;            // limited rows
+  int* nb = nullptr;              // [E][4] left, right, bottom, top
+  double* lgeo = nullptr;         // [E][10] limiter geometry
+  double* limD = nullptr;         // derivative tables per degree
+  double* limDinv = nullptr;
 };
 
 template <typename T>
@@ -102,6 +111,7 @@ inline StageArgs<T> make_args(const DeviceBuffers& b) {
   a.ctl = b.ctl;
   a.status = b.status;
   a.partials = b.partials;
+  a.bad = b.bad;
   a.order = b.order;
   return a;
 }
@@ -125,6 +135,8 @@ struct Ops {
   void (*l2err)(const DeviceBuffers&, double t, int field, cudaStream_t) = nullptr;
   void (*totals)(const DeviceBuffers&, double refm, cudaStream_t) = nullptr;
   int (*grid_elem)(int E) = nullptr;
+  // moment limiter pass (triangles, p >= 1; nullptr elsewhere)
+  void (*limit)(const DeviceBuffers&, int check_done, cudaStream_t) = nullptr;
 };
 
 using OpsKey = std::tuple<int, int, int, int, int>;  // law, flux, dim, order, precision

@@ -18,6 +18,7 @@ LAW_SCALAR, LAW_BURGERS2D, LAW_EULER2D, LAW_EULER3D, LAW_MAXWELL3D = range(5)
 FLUX_UPWIND, FLUX_CENTRAL, FLUX_GODUNOV, FLUX_ROE, FLUX_LLF = range(5)
 FIELD_GAUSS, FIELD_VORTEX, FIELD_PULSE3D, FIELD_SINE, FIELD_GAUSS3D, FIELD_TM110 = range(6)
 FP64, MIXED = 0, 1
+LIMITER_NONE, LIMITER_MOMENT = 0, 1
 NPARAMS = 16
 
 ERRORS = {-1: "invalid argument", -2: "I/O", -3: "unsupported", -4: "CUDA", -5: "non-physical",
@@ -74,6 +75,10 @@ def lib() -> ctypes.CDLL:
         "dgp_synchronize": ([P], I),
         "dgp_solver_stream": ([P, pP], I),
         "dgp_profile_kernels": ([P, I, ctypes.POINTER(ctypes.c_float)], I),
+        "dgp_limit": ([P, ctypes.POINTER(ctypes.c_uint8)], I),
+        "dgp_limiter_triggers": ([P, ctypes.POINTER(ctypes.c_uint8)], I),
+        "dgp_set_p0_fallback": ([P, I], I),
+        "dgp_launches_per_step": ([P, pI], I),
     }
     for name, (args, res) in sig.items():
         f = getattr(L, name)
@@ -263,6 +268,26 @@ class Solver:
         out = (ctypes.c_float * 3)()
         check(lib().dgp_profile_kernels(self.h, iters, out))
         return np.array(out[:], dtype=np.float64)
+
+    def limit(self) -> np.ndarray:
+        """Apply the triangle moment limiter once; per-cell trigger degree
+        (0: untouched), file order."""
+        out = np.zeros(self.ncells, dtype=np.uint8)
+        check(lib().dgp_limit(self.h, out.ctypes.data_as(ctypes.POINTER(ctypes.c_uint8))))
+        return out
+
+    def limiter_triggers(self) -> np.ndarray:
+        out = np.zeros(self.ncells, dtype=np.uint8)
+        check(lib().dgp_limiter_triggers(self.h, out.ctypes.data_as(ctypes.POINTER(ctypes.c_uint8))))
+        return out
+
+    def set_p0_fallback(self, on: bool = True):
+        check(lib().dgp_set_p0_fallback(self.h, 1 if on else 0))
+
+    def launches_per_step(self) -> int:
+        n = ctypes.c_int()
+        check(lib().dgp_launches_per_step(self.h, ctypes.byref(n)))
+        return n.value
 
     def synchronize(self):
         check(lib().dgp_synchronize(self.h))

@@ -116,6 +116,24 @@ int dgp_step(dgp_solver s, double t, double dt, double* resid);
  * Runs device-resident (CUDA graphs), no host sync per step. */
 int dgp_run(dgp_solver s, double t0, double tend, double cfl, int max_steps, double* t_out,
             int* steps_out);
+/* kernels one step of dgp_run launches (face/element kernels per stage, the
+ * P0 fallback's second face pass, limiter passes and the CFL reduction) */
+int dgp_launches_per_step(dgp_solver s, int* n);
+/* Triangle moment limiter (DGP_LIMITER_MOMENT; replaces DGMomentLimiter::limit,
+ * DGLimiter.cc:963-1133, which indexes the quadrilateral tensor basis and is
+ * invalid on triangles).  The solver applies it after every SSP-RK3 stage
+ * (TimeIntegrator::limit, TimeIntegrator.cc:1414-1434) and once after
+ * dgp_project (DGAnalysis.cc:276-291).  dgp_limit applies it once to the
+ * current state; triggers (may be NULL) receives per cell, in file order, the
+ * lowest limited degree (0: untouched) -- the DGSensor trigger indicator.
+ * dgp_limiter_triggers returns the triggers of the last application. */
+int dgp_limit(dgp_solver s, unsigned char* triggers);
+int dgp_limiter_triggers(dgp_solver s, unsigned char* out);
+/* P0 fallback of DGBoundaryCell::computeBoundaryContributions + DGCell::setToZero
+ * (DGCell.cc:639-811): in every SSP-RK3 stage, cells with a non-physical trace
+ * at a face point drop their modes k >= 1 and the stage is assembled again.
+ * On by default for the Euler laws; 0 turns it off. */
+int dgp_set_p0_fallback(dgp_solver s, int on);
 /* non-physical states seen since the last call (isPhysical, EulerLaw.cc:1398) */
 int dgp_status(dgp_solver s, int* nonphysical, int* first_bad_cell);
 /* L2 error of one field against the law's exact field (DGCell::densityErrorL2,

@@ -58,7 +58,18 @@ struct or_solver {
   double *fjw;       /* [F][nqf] |J_f| * weight */
   /* state */
   double *C, *R, *soln;
+  /* triangle moment limiter and P0 fallback (off unless enabled) */
+  int limiter, p0;
+  int* nb;             /* [E][4] neighbours left, right, bottom, top (-1: none) */
+  double* bbc;         /* [E][2] bounding-box centres */
+  double Dn[64], Dinv[64]; /* per degree n: (n+1)^2 block at n(n+1)(2n+1)/6 */
+  double* L;           /* limited state */
+  unsigned char* trig; /* [E] trigger degree of the last limiter application */
+  unsigned char* bad;  /* [E] P0 fallback marks */
 };
+
+static void build_limiter_tables(or_solver* s);
+static void build_limiter_geometry(or_solver* s);
 
 /* ------------------------------------------------------------------------ */
 /* glibc rand(): srand(seed) then the first rand(), restating the published   */
@@ -578,6 +589,11 @@ static void boundary_flux(const or_solver* s, int bid, const double* n, const do
       return;
     }
     case OR_BURGERS2D: { /* Burgers2D::boundaryFlux, Burgers2D.cc:30-54 */
+      if (s->flux == OR_FLUX_LLF) { /* LLF (no counterpart): far field as the ghost state */
+        or_field_eval(s, x, T, f);
+        riemann_flux(s, n, x, Q, f, flux);
+        return;
+      }
       double nvel = Q[0] * Q[0] * 0.5 * (n[0] + n[1]);
       if (nvel < 0) {
         or_field_eval(s, x, T, f);
@@ -1039,6 +1055,13 @@ or_solver* or_create(const char* msh_path, int law, int flux, int order, int fie
   s->C = calloc(n, sizeof(double));
   s->R = calloc(n, sizeof(double));
   s->soln = calloc(n, sizeof(double));
+  s->L = calloc(n, sizeof(double));
+  s->trig = calloc((size_t)s->E, 1);
+  s->bad = calloc((size_t)s->E, 1);
+  if (s->dim == 2) {
+    build_limiter_tables(s);
+    build_limiter_geometry(s);
+  }
   or_project(s, 0.0);
   return s;
 }
@@ -1049,6 +1072,7 @@ void or_destroy(or_solver* s) {
   free(s->lfL); free(s->lfR); free(s->bid); free(s->jac); free(s->jinv); free(s->det);
   free(s->csize); free(s->fn); free(s->fmeas); free(s->trL); free(s->trR); free(s->fx);
   free(s->fjw); free(s->C); free(s->R); free(s->soln);
+  free(s->nb); free(s->bbc); free(s->L); free(s->trig); free(s->bad);
   free(s);
 }
 
@@ -1209,19 +1233,322 @@ double or_cfl_dt(const or_solver* s, double cfl) {
   return DT;
 }
 
+/* ------------------------------------------------------------------------ */
+/* Triangle moment limiter.  DGMomentLimiter::limit (DGLimiter.cc:963-1133)   */
+/* indexes the tensor Legendre basis of quads ((p+1)^2-1 ...) and reads past  */
+/* a triangle's coefficient row, so the triangle limiter is defined here and  */
+/* restated independently by the CUDA path.  It keeps the reference's shape:  */
+/*  - neighbours left/right/bottom/top by bounding boxes (DGLimiter.cc:977-993,*/
+/*    faces visited in local-face order, later faces overwrite);              */
+/*  - all differences use the unlimited state (the reference reads slot 0 and */
+/*    writes the copy slot, then TimeIntegrator::limit copies back);          */
+/*  - per field, degrees are visited from p down to 1; a degree whose modes   */
+/*    are all below 1e-10 in magnitude is skipped; a degree with no component */
+/*    limited ends the descent; minmod/absmin as DGLimiter.cc:1424-1447.      */
+/* The moments of degree n are the n+1 physical derivatives                   */
+/* d^n/dx^(n-a)dy^a of the cell's degree-n modal block (constant on the cell);*/
+/* component a is bounded in x by the differences of the degree-(n-1)         */
+/* derivative d^(n-1)/dx^(n-1-a)dy^a of the left/right neighbours and in y by */
+/* d^(n-1)/dx^(n-a)dy^(a-1) of the bottom/top neighbours, divided by the      */
+/* distance of the bounding-box centres (the degree-0 moment is the mean).    */
+/* A limited degree is mapped back to its modal block exactly; the mean is    */
+/* never changed.  Trigger of a cell = lowest limited degree over its fields  */
+/* (0: untouched).  Products and sums are evaluated one rounding at a time,   */
+/* in the order written, so that the CUDA path reproduces them bit for bit.   */
+/* ------------------------------------------------------------------------ */
+#define LIM_SMALL 1.0e-10
+#define LSIGN(a) ((a) < 0.0 ? -1 : 1)
+
+static double lim_minmod3(double a, double b, double c, int* lim) {
+  if (LSIGN(a) == LSIGN(b) && LSIGN(b) == LSIGN(c)) {
+    double aa = fabs(a), ab = fabs(b), ac = fabs(c);
+    if (aa < ab && aa < ac) { *lim = 0; return a; }
+    if (ab < ac) { *lim = 1; return b; }
+    *lim = 1;
+    return c;
+  }
+  *lim = 1;
+  return 0.0;
+}
+
+static double lim_minmod2(double a, double b, int* lim) {
+  if (LSIGN(a) == LSIGN(b)) {
+    if (fabs(a) < fabs(b)) { *lim = 0; return a; }
+    *lim = 1;
+    return b;
+  }
+  *lim = 1;
+  return 0.0;
+}
+
+static int blk_off(int n) { return n * (n + 1) * (2 * n + 1) / 6; }
+
+/* Dn[i][m] = d^n phi_(n,m) / du^(n-i) dv^i (constant): (n-i)! i! G[base+m][base+i];
+ * Dinv = Dn^{-1} (upper triangular, back substitution in long double) */
+static void build_limiter_tables(or_solver* s) {
+  for (int n = 0; n <= s->order; ++n) {
+    int base = n * (n + 1) / 2, w = n + 1, o = blk_off(n);
+    long double A[5][5], X[5][5];
+    for (int i = 0; i <= n; ++i)
+      for (int m = 0; m <= n; ++m) {
+        double f = (double)(fact(n - i) * fact(i));
+        s->Dn[o + i * w + m] = f * s->G[base + m][base + i];
+        A[i][m] = (long double)s->Dn[o + i * w + m];
+      }
+    for (int k = 0; k <= n; ++k) /* column k of the inverse */
+      for (int i = n; i >= 0; --i) {
+        long double r = (i == k) ? 1.0L : 0.0L;
+        for (int m = i + 1; m <= n; ++m) r -= A[i][m] * X[m][k];
+        X[i][k] = r / A[i][i];
+      }
+    for (int m = 0; m <= n; ++m)
+      for (int i = 0; i <= n; ++i) s->Dinv[o + m * w + i] = (double)X[m][i];
+  }
+}
+
+/* neighbours by bounding boxes (DGLimiter.cc:970-993; DGCell.cc:76-86) */
+static void build_limiter_geometry(or_solver* s) {
+  const int E = s->E;
+  double* bmin = malloc((size_t)E * 2 * sizeof(double));
+  double* bmax = malloc((size_t)E * 2 * sizeof(double));
+  s->bbc = malloc((size_t)E * 2 * sizeof(double));
+  s->nb = malloc((size_t)E * 4 * sizeof(int));
+  for (int e = 0; e < E; ++e) {
+    const int* c = s->cv + e * s->nvc;
+    for (int k = 0; k < 2; ++k) bmin[2 * e + k] = bmax[2 * e + k] = s->X[3 * c[0] + k];
+    for (int v = 1; v < s->nvc; ++v)
+      for (int k = 0; k < 2; ++k) {
+        double x = s->X[3 * c[v] + k];
+        if (x < bmin[2 * e + k]) bmin[2 * e + k] = x;
+        if (x > bmax[2 * e + k]) bmax[2 * e + k] = x;
+      }
+    for (int k = 0; k < 2; ++k) s->bbc[2 * e + k] = (bmin[2 * e + k] + bmax[2 * e + k]) / 2.;
+  }
+  int* cf = malloc((size_t)E * 3 * sizeof(int)); /* face of local face lf, -1: none */
+  for (int i = 0; i < E * 3; ++i) cf[i] = -1;
+  for (int f = 0; f < s->F; ++f) {
+    cf[s->eL[f] * 3 + s->lfL[f]] = f;
+    if (s->eR[f] >= 0) cf[s->eR[f] * 3 + s->lfR[f]] = f;
+  }
+  for (int e = 0; e < E; ++e) {
+    int* nb = s->nb + 4 * e;
+    nb[0] = nb[1] = nb[2] = nb[3] = -1;
+    const double px = s->bbc[2 * e], py = s->bbc[2 * e + 1];
+    for (int lf = 0; lf < 3; ++lf) {
+      int f = cf[e * 3 + lf];
+      if (f < 0 || s->eR[f] < 0) continue;
+      int o = (s->eL[f] == e) ? s->eR[f] : s->eL[f];
+      if (px > bmax[2 * o]) nb[0] = o;     /* left */
+      if (px < bmin[2 * o]) nb[1] = o;     /* right */
+      if (py > bmax[2 * o + 1]) nb[2] = o; /* bottom */
+      if (py < bmin[2 * o + 1]) nb[3] = o; /* top */
+    }
+  }
+  free(cf);
+  free(bmin);
+  free(bmax);
+}
+
+/* P[a][i]: coefficient of s^(n-i) t^i in (A s + B t)^(n-a) (C s + D t)^a */
+static void lim_transform(int n, double A, double B, double C, double D, double* P) {
+  for (int a = 0; a <= n; ++a) {
+    double poly[6] = {1.0, 0, 0, 0, 0, 0}, q[6];
+    int deg = 0;
+    for (int k = 0; k < n; ++k) {
+      double u = (k < n - a) ? A : C, v = (k < n - a) ? B : D;
+      for (int i = 0; i <= deg + 1; ++i) {
+        double x = (i <= deg) ? poly[i] * u : 0.0;
+        double y = (i >= 1) ? poly[i - 1] * v : 0.0;
+        q[i] = x + y;
+      }
+      ++deg;
+      for (int i = 0; i <= deg; ++i) poly[i] = q[i];
+    }
+    for (int i = 0; i <= n; ++i) P[a * (n + 1) + i] = poly[i];
+  }
+}
+
+/* physical degree-n derivatives of the degree-n block of one coefficient row */
+static void lim_moments(const or_solver* s, const double* row, int n, const double* P, double* g) {
+  const int base = n * (n + 1) / 2, w = n + 1;
+  const double* D = s->Dn + blk_off(n);
+  double r[5];
+  for (int i = 0; i <= n; ++i) {
+    double acc = 0.0;
+    for (int m = 0; m <= n; ++m) acc = acc + D[i * w + m] * row[base + m];
+    r[i] = acc;
+  }
+  for (int a = 0; a <= n; ++a) {
+    double acc = 0.0;
+    for (int i = 0; i <= n; ++i) acc = acc + P[a * w + i] * r[i];
+    g[a] = acc;
+  }
+}
+
+static void cell_lower_moments(const or_solver* s, const double* C, int e, int j, int n, double* h) {
+  const double* Ji = s->jinv + 9 * e;
+  double P[25];
+  lim_transform(n, Ji[0], Ji[1], Ji[3], Ji[4], P);
+  lim_moments(s, C + ((size_t)e * s->m + j) * s->Np, n, P, h);
+}
+
+static int limit_cell(const or_solver* s, const double* C, int e, double* out) {
+  const int m = s->m, Np = s->Np, p = s->order;
+  const int* nb = s->nb + 4 * e;
+  const double px = s->bbc[2 * e], py = s->bbc[2 * e + 1];
+  const double* Ji = s->jinv + 9 * e;
+  const double* J = s->jac + 9 * e;
+  int trig = 0;
+  for (int j = 0; j < m; ++j) {
+    const double* row = C + ((size_t)e * m + j) * Np;
+    double* orow = out + (size_t)j * Np;
+    for (int n = p; n >= 1; --n) {
+      const int base = n * (n + 1) / 2, w = n + 1;
+      int big = 0;
+      for (int k = 0; k <= n; ++k) big |= fabs(row[base + k]) > LIM_SMALL;
+      if (!big) continue;
+      double P[25], g[5], gl[5], he[5], hx[4][5];
+      lim_transform(n, Ji[0], Ji[1], Ji[3], Ji[4], P);
+      lim_moments(s, row, n, P, g);
+      cell_lower_moments(s, C, e, j, n - 1, he);
+      for (int d = 0; d < 4; ++d)
+        if (nb[d] >= 0) cell_lower_moments(s, C, nb[d], j, n - 1, hx[d]);
+      int any = 0;
+      for (int a = 0; a <= n; ++a) {
+        gl[a] = g[a];
+        int hasx = a <= n - 1 && (nb[0] >= 0 || nb[1] >= 0);
+        int hasy = a >= 1 && (nb[2] >= 0 || nb[3] >= 0);
+        double t1 = 0.0, t2 = 0.0;
+        int l1 = 0, l2 = 0;
+        if (hasx) {
+          double fwd = 0.0, bwd = 0.0;
+          if (nb[1] >= 0) fwd = (hx[1][a] - he[a]) / (s->bbc[2 * nb[1]] - px);
+          if (nb[0] >= 0) bwd = (he[a] - hx[0][a]) / (px - s->bbc[2 * nb[0]]);
+          if (nb[0] >= 0 && nb[1] >= 0) t1 = lim_minmod3(g[a], fwd, bwd, &l1);
+          else if (nb[0] >= 0) t1 = lim_minmod2(g[a], bwd, &l1);
+          else t1 = lim_minmod2(g[a], fwd, &l1);
+        }
+        if (hasy) {
+          double fwd = 0.0, bwd = 0.0;
+          if (nb[3] >= 0) fwd = (hx[3][a - 1] - he[a - 1]) / (s->bbc[2 * nb[3] + 1] - py);
+          if (nb[2] >= 0) bwd = (he[a - 1] - hx[2][a - 1]) / (py - s->bbc[2 * nb[2] + 1]);
+          if (nb[2] >= 0 && nb[3] >= 0) t2 = lim_minmod3(g[a], fwd, bwd, &l2);
+          else if (nb[2] >= 0) t2 = lim_minmod2(g[a], bwd, &l2);
+          else t2 = lim_minmod2(g[a], fwd, &l2);
+        }
+        if (hasx && hasy) {
+          if (l1 || l2) { gl[a] = fabs(t1) < fabs(t2) ? t1 : t2; any = 1; }
+        } else if (hasx) {
+          if (l1) { gl[a] = t1; any = 1; }
+        } else if (hasy) {
+          if (l2) { gl[a] = t2; any = 1; }
+        }
+      }
+      if (!any) break;
+      /* back to reference derivatives (d/du = J00 d/dx + J01 d/dy, ...) and modes */
+      double Q[25], r[5];
+      lim_transform(n, J[0], J[1], J[3], J[4], Q);
+      for (int i = 0; i <= n; ++i) {
+        double acc = 0.0;
+        for (int a = 0; a <= n; ++a) acc = acc + Q[i * w + a] * gl[a];
+        r[i] = acc;
+      }
+      const double* Di = s->Dinv + blk_off(n);
+      for (int k = 0; k <= n; ++k) {
+        double acc = 0.0;
+        for (int i = 0; i <= n; ++i) acc = acc + Di[k * w + i] * r[i];
+        orow[base + k] = acc;
+      }
+      if (trig == 0 || n < trig) trig = n;
+    }
+  }
+  return trig;
+}
+
+void or_set_limiter(or_solver* s, int on) {
+  s->limiter = (on && s->dim == 2 && s->order > 0) ? 1 : 0;
+}
+
+void or_set_p0_fallback(or_solver* s, int on) { s->p0 = on ? 1 : 0; }
+
+int or_limit(or_solver* s, unsigned char* trig) {
+  const size_t dof = (size_t)s->m * s->Np;
+  int count = 0;
+  if (s->dim != 2 || s->order < 1) {
+    if (trig) memset(trig, 0, (size_t)s->E);
+    return 0;
+  }
+  memcpy(s->L, s->C, (size_t)s->E * dof * sizeof(double));
+  for (int e = 0; e < s->E; ++e) {
+    int t = limit_cell(s, s->C, e, s->L + e * dof);
+    s->trig[e] = (unsigned char)t;
+    count += t != 0;
+  }
+  memcpy(s->C, s->L, (size_t)s->E * dof * sizeof(double));
+  if (trig) memcpy(trig, s->trig, (size_t)s->E);
+  return count;
+}
+
+/* Euler2d::isPhysical / Euler3d::isPhysical (EulerLaw.cc:1398-1421) */
+static int or_is_physical(const or_solver* s, const double* Q) {
+  if (s->law == OR_EULER2D) {
+    if (Q[0] < 0) return 0;
+    if ((s->gamma - 1.) * (Q[3] - 0.5 * (Q[1] * Q[1] + Q[2] * Q[2]) / Q[0]) < 0.0) return 0;
+  } else if (s->law == OR_EULER3D) {
+    if (Q[0] < 0) return 0;
+    if ((s->gamma - 1.) * (Q[3] - 0.5 * (Q[1] * Q[1] + Q[2] * Q[2] + Q[4] * Q[4]) / Q[0]) < 0.0) return 0;
+  }
+  return 1;
+}
+
+/* assembly of one stage with the P0 fallback of DGAnalysis.cc:392-417 and
+ * DGCell::setToZero (DGCell.cc:785-811): cells with a non-physical trace at
+ * a face point drop their modes k >= 1, then the RHS is assembled again.  All
+ * marked cells are zeroed before the second assembly. */
+static int assemble_stage(or_solver* s, double t, double* R) {
+  assemble(s, s->C, t, R);
+  if (!s->p0) return 0;
+  const int m = s->m, Np = s->Np;
+  int nbad = 0;
+  memset(s->bad, 0, (size_t)s->E);
+  for (int f = 0; f < s->F; ++f)
+    for (int q = 0; q < s->nqf; ++q) {
+      double U[MAXM];
+      interp(s->trL + ((size_t)f * s->nqf + q) * Np, s->C + (size_t)s->eL[f] * m * Np, m, Np, U);
+      if (!or_is_physical(s, U)) s->bad[s->eL[f]] = 1;
+      if (s->eR[f] >= 0) {
+        interp(s->trR + ((size_t)f * s->nqf + q) * Np, s->C + (size_t)s->eR[f] * m * Np, m, Np, U);
+        if (!or_is_physical(s, U)) s->bad[s->eR[f]] = 1;
+      }
+    }
+  for (int e = 0; e < s->E; ++e)
+    if (s->bad[e]) {
+      ++nbad;
+      for (int j = 0; j < m; ++j)
+        for (int k = 1; k < Np; ++k) s->C[((size_t)e * m + j) * Np + k] = 0.0;
+    }
+  if (nbad) assemble(s, s->C, t, R);
+  return nbad;
+}
+
+void or_bad_cells(const or_solver* s, unsigned char* out) { memcpy(out, s->bad, (size_t)s->E); }
+
+void or_triggers(const or_solver* s, unsigned char* out) { memcpy(out, s->trig, (size_t)s->E); }
+
 /* RungeKuttaTVD3::advanceInTime, TimeIntegrator.cc:838-990 (orthogonal basis) */
 double or_step(or_solver* s, double t, double dt) {
   const int m = s->m, Np = s->Np, dof = m * Np;
   size_t n = (size_t)s->E * dof;
+  assemble_stage(s, t, s->R); /* may drop cells to P0 before u_n is saved */
   memcpy(s->soln, s->C, n * sizeof(double));
-  assemble(s, s->C, t, s->R);
   for (int e = 0; e < s->E; ++e) {
     double dj = dt / s->det[e];
     double* c = s->C + (size_t)e * dof;
     const double* r = s->R + (size_t)e * dof;
     for (int i = 0; i < dof; ++i) c[i] += r[i] * dj;
   }
-  assemble(s, s->C, t + dt, s->R);
+  if (s->limiter) or_limit(s, NULL);
+  assemble_stage(s, t + dt, s->R);
   for (int e = 0; e < s->E; ++e) {
     double dj = dt / s->det[e];
     double* c = s->C + (size_t)e * dof;
@@ -1229,7 +1556,8 @@ double or_step(or_solver* s, double t, double dt) {
     const double* so = s->soln + (size_t)e * dof;
     for (int i = 0; i < dof; ++i) c[i] = 0.25 * (c[i] + r[i] * dj + 3. * so[i]);
   }
-  assemble(s, s->C, t + dt * 0.5, s->R);
+  if (s->limiter) or_limit(s, NULL);
+  assemble_stage(s, t + dt * 0.5, s->R);
   double resid = 0.0;
   for (int e = 0; e < s->E; ++e) {
     double dj = dt / s->det[e];
@@ -1242,6 +1570,7 @@ double or_step(or_solver* s, double t, double dt) {
       resid += tmp * tmp;
     }
   }
+  if (s->limiter) or_limit(s, NULL);
   return resid;
 }
 

@@ -51,6 +51,16 @@ double or_run(or_solver* s, double t0, double tend, double cfl, int nsteps, int*
 double or_l2_error(const or_solver* s, double t, int field_index); /* vs exact field */
 void or_field_eval(const or_solver* s, const double* x, double t, double* q);
 unsigned int or_glibc_rand_first(unsigned int seed);   /* srand(seed); rand() */
+/* triangle moment limiter (definition in dg_oracle.c): applied after every
+ * SSP-RK3 stage by or_step when enabled; or_limit applies it once to the
+ * current state and writes the per-cell trigger degree (0: untouched, file
+ * order) when trig is not NULL; returns the number of triggered cells. */
+void or_set_limiter(or_solver* s, int on);
+int or_limit(or_solver* s, unsigned char* trig);
+/* P0 fallback of DGCell::setToZero for cells with a non-physical face trace */
+void or_set_p0_fallback(or_solver* s, int on);
+void or_bad_cells(const or_solver* s, unsigned char* out); /* marks of the last stage */
+void or_triggers(const or_solver* s, unsigned char* out);  /* of the last limiter pass */
 
 #ifdef __cplusplus
 }

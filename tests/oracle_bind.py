@@ -50,6 +50,13 @@ def lib():
     L.or_run.restype = D
     L.or_l2_error.argtypes = [P, D, I]
     L.or_l2_error.restype = D
+    pU8 = ctypes.POINTER(ctypes.c_uint8)
+    L.or_set_limiter.argtypes = [P, I]
+    L.or_limit.argtypes = [P, pU8]
+    L.or_limit.restype = I
+    L.or_set_p0_fallback.argtypes = [P, I]
+    L.or_bad_cells.argtypes = [P, pU8]
+    L.or_triggers.argtypes = [P, pU8]
     L.or_glibc_rand_first.argtypes = [ctypes.c_uint]
     L.or_glibc_rand_first.restype = ctypes.c_uint
     _lib = L
@@ -106,6 +113,29 @@ class Oracle:
 
     def l2_error(self, t, field=0):
         return lib().or_l2_error(self.h, t, field)
+
+    def set_limiter(self, on=True):
+        lib().or_set_limiter(self.h, 1 if on else 0)
+
+    def set_p0_fallback(self, on=True):
+        lib().or_set_p0_fallback(self.h, 1 if on else 0)
+
+    def limit(self):
+        """Apply the triangle moment limiter once; per-cell trigger degrees."""
+        trig = np.zeros(self.ncells, dtype=np.uint8)
+        lib().or_limit(self.h, trig.ctypes.data_as(ctypes.POINTER(ctypes.c_uint8)))
+        return trig
+
+    def triggers(self):
+        """Trigger degrees of the last limiter application."""
+        out = np.zeros(self.ncells, dtype=np.uint8)
+        lib().or_triggers(self.h, out.ctypes.data_as(ctypes.POINTER(ctypes.c_uint8)))
+        return out
+
+    def bad_cells(self):
+        out = np.zeros(self.ncells, dtype=np.uint8)
+        lib().or_bad_cells(self.h, out.ctypes.data_as(ctypes.POINTER(ctypes.c_uint8)))
+        return out
 
     def close(self):
         if self.h:
