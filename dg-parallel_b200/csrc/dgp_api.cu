@@ -56,6 +56,13 @@ __global__ void gather_cells(const Tin* in, Tout* out, const int* perm, int E, i
   out[i] = static_cast<Tout>(in[(size_t)perm[e] * mnp + r]);
 }
 
+// device clock mark of a run's start (ensembles time their instances from it)
+__global__ void mark_clock(TimeCtl* c) {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  c->t_mark_ns = t;
+}
+
 uint64_t spread2(uint32_t x) {
   uint64_t v = x;
   v = (v | (v << 16)) & 0x0000FFFF0000FFFFull;
@@ -83,67 +90,351 @@ using namespace dgp;
 
 // Triangle moment limiter data in the internal cell order: neighbours by
 // bounding boxes (DGLimiter.cc:970-993, DGCell.cc:76-86), FP64 geometry of the
-// derivative transforms and the bounding-box centres, degree tables.
+// derivative transforms and the bounding-box centres, degree tables.  Padding
+// cells of an ensemble keep no neighbours and zero geometry.
 static int setup_limiter(dgp_solver s) {
-  const HostMesh& m = s->mesh;
-  const int E = m.E;
-  std::vector<double> bmin(2 * (size_t)E), bmax(2 * (size_t)E), bbc(2 * (size_t)E);
-  for (int e = 0; e < E; ++e) {
-    const int* c = &m.cv[static_cast<size_t>(e) * m.nvc];
-    for (int k = 0; k < 2; ++k) bmin[2 * e + k] = bmax[2 * e + k] = m.X[3 * c[0] + k];
-    for (int v = 1; v < m.nvc; ++v)
-      for (int k = 0; k < 2; ++k) {
-        const double x = m.X[3 * c[v] + k];
-        if (x < bmin[2 * e + k]) bmin[2 * e + k] = x;
-        if (x > bmax[2 * e + k]) bmax[2 * e + k] = x;
-      }
-    for (int k = 0; k < 2; ++k) bbc[2 * e + k] = (bmin[2 * e + k] + bmax[2 * e + k]) / 2.;
-  }
-  std::vector<int> cf(3 * (size_t)E, -1);  // face of (cell, local face)
-  for (int f = 0; f < m.F; ++f) {
-    cf[3 * (size_t)m.eL[f] + m.lfL[f]] = f;
-    if (m.eR[f] >= 0) cf[3 * (size_t)m.eR[f] + m.lfR[f]] = f;
-  }
-  std::vector<int> nb(4 * (size_t)E, -1);
-  std::vector<double> geo(static_cast<size_t>(E) * kLimGeo);
-  for (int i = 0; i < E; ++i) {
-    const int e = s->i2f[i];
-    const double px = bbc[2 * e], py = bbc[2 * e + 1];
-    int* n = &nb[4 * (size_t)i];
-    for (int lf = 0; lf < 3; ++lf) {
-      const int f = cf[3 * (size_t)e + lf];
-      if (f < 0 || m.eR[f] < 0) continue;
-      const int o = (m.eL[f] == e) ? m.eR[f] : m.eL[f];
-      const int oi = s->f2i[o];
-      if (px > bmax[2 * o]) n[0] = oi;
-      if (px < bmin[2 * o]) n[1] = oi;
-      if (py > bmax[2 * o + 1]) n[2] = oi;
-      if (py < bmin[2 * o + 1]) n[3] = oi;
+  const int Etot = s->b.E;
+  std::vector<int> nb(4 * (size_t)Etot, -1);
+  std::vector<double> geo(static_cast<size_t>(Etot) * kLimGeo, 0.0);
+  for (size_t ii = 0; ii < s->meshes.size(); ++ii) {
+    const HostMesh& m = s->meshes[ii];
+    const int E = m.E, uf = s->inst_ufirst[ii], off = s->inst_off[ii];
+    std::vector<double> bmin(2 * (size_t)E), bmax(2 * (size_t)E), bbc(2 * (size_t)E);
+    for (int e = 0; e < E; ++e) {
+      const int* c = &m.cv[static_cast<size_t>(e) * m.nvc];
+      for (int k = 0; k < 2; ++k) bmin[2 * e + k] = bmax[2 * e + k] = m.X[3 * c[0] + k];
+      for (int v = 1; v < m.nvc; ++v)
+        for (int k = 0; k < 2; ++k) {
+          const double x = m.X[3 * c[v] + k];
+          if (x < bmin[2 * e + k]) bmin[2 * e + k] = x;
+          if (x > bmax[2 * e + k]) bmax[2 * e + k] = x;
+        }
+      for (int k = 0; k < 2; ++k) bbc[2 * e + k] = (bmin[2 * e + k] + bmax[2 * e + k]) / 2.;
     }
-    double X0[3], J[9], Ji[9];
-    cell_frame(m, e, X0, J);
-    invert3(J, Ji);
-    double* g = &geo[static_cast<size_t>(i) * kLimGeo];
-    g[0] = Ji[0];
-    g[1] = Ji[1];
-    g[2] = Ji[3];
-    g[3] = Ji[4];
-    g[4] = J[0];
-    g[5] = J[1];
-    g[6] = J[3];
-    g[7] = J[4];
-    g[8] = px;
-    g[9] = py;
+    std::vector<int> cf(3 * (size_t)E, -1);  // face of (cell, local face)
+    for (int f = 0; f < m.F; ++f) {
+      cf[3 * (size_t)m.eL[f] + m.lfL[f]] = f;
+      if (m.eR[f] >= 0) cf[3 * (size_t)m.eR[f] + m.lfR[f]] = f;
+    }
+    for (int e = 0; e < E; ++e) {
+      const int i = s->f2i[uf + e];
+      (void)off;
+      const double px = bbc[2 * e], py = bbc[2 * e + 1];
+      int* n = &nb[4 * (size_t)i];
+      for (int lf = 0; lf < 3; ++lf) {
+        const int f = cf[3 * (size_t)e + lf];
+        if (f < 0 || m.eR[f] < 0) continue;
+        const int o = (m.eL[f] == e) ? m.eR[f] : m.eL[f];
+        const int oi = s->f2i[uf + o];
+        if (px > bmax[2 * o]) n[0] = oi;
+        if (px < bmin[2 * o]) n[1] = oi;
+        if (py > bmax[2 * o + 1]) n[2] = oi;
+        if (py < bmin[2 * o + 1]) n[3] = oi;
+      }
+      double X0[3], J[9], Ji[9];
+      cell_frame(m, e, X0, J);
+      invert3(J, Ji);
+      double* g = &geo[static_cast<size_t>(i) * kLimGeo];
+      g[0] = Ji[0];
+      g[1] = Ji[1];
+      g[2] = Ji[3];
+      g[3] = Ji[4];
+      g[4] = J[0];
+      g[5] = J[1];
+      g[6] = J[3];
+      g[7] = J[4];
+      g[8] = px;
+      g[9] = py;
+    }
   }
   std::vector<double> D, Dinv;
   build_limiter_tables(s->tab, D, Dinv);
   DeviceBuffers& b = s->b;
   int rc = DGP_OK;
   if ((rc = s->upload(&b.nb, nb)) || (rc = s->upload(&b.lgeo, geo)) || (rc = s->upload(&b.limD, D)) ||
-      (rc = s->upload(&b.limDinv, Dinv)) || (rc = s->alloc(&b.trig, static_cast<size_t>(E))) ||
+      (rc = s->upload(&b.limDinv, Dinv)) || (rc = s->alloc(&b.trig, static_cast<size_t>(Etot))) ||
       (rc = s->alloc(&b.L, s->state_count())))
     return rc;
-  DGP_CUDA(cudaMemset(b.trig, 0, E));
+  DGP_CUDA(cudaMemset(b.trig, 0, Etot));
+  return DGP_OK;
+}
+
+// Morton code of the cell centroids of one mesh (locality of neighbours)
+static std::vector<int> morton_order(const HostMesh& m) {
+  const int E = m.E, dim = m.dim, nvc = m.nvc;
+  double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
+  std::vector<double> cen(static_cast<size_t>(E) * 3);
+  for (int e = 0; e < E; ++e)
+    for (int c = 0; c < 3; ++c) {
+      double x = 0;
+      for (int k = 0; k < nvc; ++k) x += m.X[3 * m.cv[static_cast<size_t>(e) * nvc + k] + c];
+      x /= nvc;
+      cen[3 * e + c] = x;
+      lo[c] = std::min(lo[c], x);
+      hi[c] = std::max(hi[c], x);
+    }
+  std::vector<uint64_t> key(E);
+  for (int e = 0; e < E; ++e) {
+    uint32_t qv[3];
+    for (int c = 0; c < 3; ++c) {
+      double span = hi[c] - lo[c];
+      double u = span > 0 ? (cen[3 * e + c] - lo[c]) / span : 0.0;
+      double scale = dim == 2 ? 4294967295.0 : 2097151.0;
+      qv[c] = static_cast<uint32_t>(std::min(scale, std::max(0.0, u * scale)));
+    }
+    key[e] = dim == 2 ? (spread2(qv[0]) | (spread2(qv[1]) << 1))
+                      : (spread3(qv[0]) | (spread3(qv[1]) << 1) | (spread3(qv[2]) << 2));
+  }
+  std::vector<int> order(E);
+  std::iota(order.begin(), order.end(), 0);
+  std::stable_sort(order.begin(), order.end(), [&](int a, int c) { return key[a] < key[c]; });
+  return order;
+}
+
+// Builds the device state of a solver over the instances already in s->meshes
+// (one mesh for a single solver).  Instance i owns internal cells
+// [inst_off[i], inst_off[i] + E_i), each instance starting on an
+// element-kernel tile; ensemble=false keeps the single-solver layout (no
+// per-instance arrays, kernels see cell_inst == nullptr).
+static int build_solver(dgp_solver s, const std::vector<LawParams>& lps, int field, bool ensemble) {
+  const int n = static_cast<int>(s->meshes.size());
+  const int dim = s->meshes[0].dim;
+  const int TE = s->ops.TE;
+  const RefTables& t = s->tab;
+  s->inst_off.resize(n);
+  s->inst_ufirst.resize(n);
+  int Etot = 0, uf = 0, Ftot = 0;
+  for (int i = 0; i < n; ++i) {
+    s->inst_off[i] = Etot;
+    s->inst_ufirst[i] = uf;
+    const int Ei = s->meshes[i].E;
+    uf += Ei;
+    Etot += ensemble ? (Ei + TE - 1) / TE * TE : Ei;
+    Ftot += s->meshes[i].F;
+  }
+  DeviceBuffers& b = s->b;
+  b.E = Etot;
+  b.dim = dim;
+  b.order = s->order;
+  b.M = s->ops.M;
+  b.NP = s->ops.NP;
+  s->i2f.assign(Etot, -1);
+  s->f2i.assign(uf, -1);
+  std::vector<int> cell_inst(Etot, -1);
+  for (int i = 0; i < n; ++i) {
+    const std::vector<int> ord = morton_order(s->meshes[i]);
+    for (int r = 0; r < static_cast<int>(ord.size()); ++r) {
+      const int internal = s->inst_off[i] + r, ufile = s->inst_ufirst[i] + ord[r];
+      s->i2f[internal] = ufile;
+      s->f2i[ufile] = internal;
+      cell_inst[internal] = i;
+    }
+  }
+
+  // cell geometry (FP64 on the host); padding cells stay zero
+  std::vector<double> jinv(static_cast<size_t>(Etot) * dim * dim, 0.0), detj(Etot, 0.0), csize(Etot, 0.0),
+      x0(3 * (size_t)Etot, 0.0), jac(9 * (size_t)Etot, 0.0);
+  for (int i = 0; i < Etot; ++i) {
+    if (s->i2f[i] < 0) continue;
+    const int inst = cell_inst[i];
+    const HostMesh& m = s->meshes[inst];
+    const int e = s->i2f[i] - s->inst_ufirst[inst];
+    const int nvc = m.nvc;
+    double X0[3], J[9], Ji[9];
+    cell_frame(m, e, X0, J);
+    double d = invert3(J, Ji);
+    detj[i] = std::fabs(d);
+    for (int r = 0; r < dim; ++r)
+      for (int c = 0; c < dim; ++c) jinv[static_cast<size_t>(i) * dim * dim + r * dim + c] = Ji[r * 3 + c];
+    for (int k = 0; k < 3; ++k) x0[3 * i + k] = X0[k];
+    for (int k = 0; k < 9; ++k) jac[9 * i + k] = J[k];
+    const int* c = &m.cv[static_cast<size_t>(e) * nvc];
+    auto len = [&](int a, int bb) {
+      const double *p = &m.X[3 * c[a]], *q = &m.X[3 * c[bb]];
+      return std::sqrt((q[0] - p[0]) * (q[0] - p[0]) + (q[1] - p[1]) * (q[1] - p[1]) +
+                       (q[2] - p[2]) * (q[2] - p[2]));
+    };
+    if (dim == 2) {  // DGCell::computeCellSize (DGCell.cc:1211-1229)
+      double a = len(0, 1), bb = len(1, 2), cc = len(2, 0);
+      double hp = 0.5 * (a + bb + cc);
+      csize[i] = std::sqrt(hp * (hp - a) * (hp - bb) * (hp - cc)) / hp * 2.;
+    } else {  // minimum edge (DGCell.cc:1239-1256)
+      double L[6] = {len(0, 1), len(1, 2), len(2, 0), len(0, 3), len(1, 3), len(2, 3)};
+      double mn = L[0];
+      for (int k = 1; k < 6; ++k) mn = std::min(mn, L[k]);
+      csize[i] = mn;
+    }
+  }
+  // faces of all instances, sorted by internal left cell
+  struct FRef {
+    int inst, f;
+  };
+  std::vector<FRef> faces;
+  faces.reserve(Ftot);
+  for (int i = 0; i < n; ++i)
+    for (int f = 0; f < s->meshes[i].F; ++f) faces.push_back({i, f});
+  auto left_internal = [&](const FRef& r) {
+    return s->f2i[s->inst_ufirst[r.inst] + s->meshes[r.inst].eL[r.f]];
+  };
+  std::stable_sort(faces.begin(), faces.end(), [&](const FRef& a, const FRef& c) {
+    const int ia = left_internal(a), ic = left_internal(c);
+    return ia != ic ? ia < ic : s->meshes[a.inst].lfL[a.f] < s->meshes[c.inst].lfL[c.f];
+  });
+  std::vector<int> fel(2 * (size_t)Ftot), fcode(Ftot), bbid;
+  std::vector<double> fnrm(static_cast<size_t>(Ftot) * dim), fj(Ftot), bpts;
+  int nb = 0;
+  for (int k = 0; k < Ftot; ++k) {
+    const HostMesh& m = s->meshes[faces[k].inst];
+    const int f = faces[k].f, ufo = s->inst_ufirst[faces[k].inst];
+    fel[2 * k] = s->f2i[ufo + m.eL[f]];
+    if (m.eR[f] >= 0) {
+      fel[2 * k + 1] = s->f2i[ufo + m.eR[f]];
+    } else {
+      fel[2 * k + 1] = -(nb + 1);
+      bbid.push_back(m.bid[f]);
+      const int* fv = &m.fv[static_cast<size_t>(f) * m.nfv];
+      for (int q = 0; q < t.nqf; ++q) {
+        const double *pa = &m.X[3 * fv[0]], *pb = &m.X[3 * fv[1]];
+        double x[3];
+        if (dim == 2) {
+          double sp = t.fqp[2 * q];
+          for (int c = 0; c < 3; ++c) x[c] = pa[c] * (1 - sp) * 0.5 + pb[c] * (1 + sp) * 0.5;
+        } else {
+          const double* pc = &m.X[3 * fv[2]];
+          double u = t.fqp[2 * q], v = t.fqp[2 * q + 1];
+          for (int c = 0; c < 3; ++c) x[c] = pa[c] * (1 - u - v) + pb[c] * u + pc[c] * v;
+        }
+        bpts.insert(bpts.end(), x, x + 3);
+      }
+      ++nb;
+    }
+    fcode[k] = m.lfL[f] | ((m.eR[f] >= 0 ? m.lfR[f] : 0) << 4) | (m.rperm[f] << 8);
+    for (int c = 0; c < dim; ++c) fnrm[static_cast<size_t>(k) * dim + c] = m.fn[3 * f + c];
+    fj[k] = dim == 2 ? 0.5 * m.fmeas[f] : 2.0 * m.fmeas[f];  // |J_f| of the face map
+  }
+  b.F = Ftot;
+  b.NB = nb;
+
+  // reference tables
+  std::vector<double> qpd(static_cast<size_t>(t.nq) * 3);
+  for (int q = 0; q < t.nq; ++q)
+    for (int c = 0; c < 3; ++c) qpd[3 * q + c] = t.qp[3 * q + c];
+  int rc = DGP_OK;
+  if ((rc = s->upload_t(&b.jinv, jinv)) || (rc = s->upload_t(&b.detj, detj)) ||
+      (rc = s->upload(&b.detjd, detj)) ||
+      (rc = s->upload(&b.csize, csize)) || (rc = s->upload(&b.x0, x0)) || (rc = s->upload(&b.jac, jac)) ||
+      (rc = s->upload(&b.fel, fel)) || (rc = s->upload(&b.fcode, fcode)) ||
+      (rc = s->upload_t(&b.fnrm, fnrm)) || (rc = s->upload_t(&b.fj, fj)) ||
+      (rc = s->upload(&b.bpts, bpts.empty() ? std::vector<double>(3, 0.0) : bpts)) ||
+      (rc = s->upload(&b.bbid, bbid.empty() ? std::vector<int>(1, 0) : bbid)) ||
+      (rc = s->upload_t(&b.phi, t.phi)) || (rc = s->upload_t(&b.dphi, t.dphi)) ||
+      (rc = s->upload_t(&b.qw, t.qw)) || (rc = s->upload_t(&b.phif, t.phif)) ||
+      (rc = s->upload_t(&b.fqw, t.fqw)) || (rc = s->upload(&b.qmap, t.qmap)) ||
+      (rc = s->upload(&b.phiv, t.phiv)) || (rc = s->upload(&b.phiq, t.phi)) ||
+      (rc = s->upload(&b.qwd, t.qw)) || (rc = s->upload(&b.qpd, qpd)) ||
+      (rc = s->upload(&b.eqp, t.eqp)) || (rc = s->upload(&b.eqw, t.eqw)) ||
+      (rc = s->upload(&b.ephi, t.ephi)) || (rc = s->upload(&s->d_i2f, s->i2f)) ||
+      (rc = s->upload(&s->d_f2i, s->f2i)))
+    return rc;
+  {
+    std::vector<double> blob(s->ops.blob_elems);
+    s->ops.fill_blob(t.dphi.data(), t.phif.data(), t.phi.data(), t.qw.data(), blob.data());
+    if ((rc = s->upload_t(&b.blob, blob))) return rc;
+    b.blob_bytes = static_cast<int>(s->ops.blob_elems * s->ops.tsize);
+  }
+  b.nqe = t.nqe;
+  b.phi0 = t.phi0;
+  b.law = lps[0];
+  b.law.field = field;
+
+  const size_t nstate = s->state_count();
+  // slots are tile-transposed over whole tiles of TE cells; state buffers get
+  // 256 bytes of tail so the bulk copy of the last tile may round up to 16 bytes
+  const size_t ntiles = (static_cast<size_t>(Etot) + TE - 1) / TE;
+  const size_t nslot = ntiles * TE * t.nlf * t.nqf * b.M;
+  unsigned char *C, *U0, *slots, *rhs, *scratch;
+  const size_t ts = s->ops.tsize;  // slots hold the RHS arithmetic type; the state is FP64
+  if ((rc = s->alloc(&C, nstate * 8 + 256)) || (rc = s->alloc(&U0, nstate * 8 + 256)) ||
+      (rc = s->alloc(&slots, nslot * ts)) || (rc = s->alloc(&rhs, nstate * 8 + 256)) ||
+      (rc = s->alloc(&scratch, nstate * 8 + 256)))
+    return rc;
+  DGP_CUDA(cudaMemset(C, 0, nstate * 8 + 256));
+  DGP_CUDA(cudaMemset(U0, 0, nstate * 8 + 256));
+  b.C = C;
+  b.U0 = U0;
+  b.slots = slots;
+  b.rhs = rhs;
+  b.scratch = scratch;
+  b.npartials = std::max(s->ops.grid_elem(Etot), (Etot + 255) / 256) * std::max(b.M, 1) + 1;
+  const int nctl = ensemble ? n + 1 : 1;
+  if ((rc = s->alloc(&b.partials, b.npartials)) || (rc = s->alloc(&b.ctl, nctl)) ||
+      (rc = s->alloc(&b.status, 1)))
+    return rc;
+  DGP_CUDA(cudaMemset(slots, 0, nslot * ts));
+  {
+    std::vector<TimeCtl> c0(nctl);
+    for (auto& c : c0) {
+      c = TimeCtl{};
+      c.dtmin_bits = 0x7FF0000000000000ull;
+    }
+    DGP_CUDA(cudaMemcpy(b.ctl, c0.data(), nctl * sizeof(TimeCtl), cudaMemcpyHostToDevice));
+  }
+  b.gctl = b.ctl + (ensemble ? n : 0);
+  if (ensemble) {
+    std::vector<int> inst_end(n), tile_first(n + 1);
+    for (int i = 0; i < n; ++i) {
+      inst_end[i] = s->inst_off[i] + s->meshes[i].E;
+      tile_first[i] = s->inst_off[i] / TE;
+    }
+    tile_first[n] = (Etot + TE - 1) / TE;
+    if ((rc = s->upload(&b.cell_inst, cell_inst)) || (rc = s->upload(&b.inst_end, inst_end)) ||
+        (rc = s->upload(&b.tile_first, tile_first)) || (rc = s->upload(&b.laws, lps)))
+      return rc;
+    b.ninst = n;
+  }
+  Status st0{0, INT32_MAX};
+  DGP_CUDA(cudaMemcpy(b.status, &st0, sizeof(Status), cudaMemcpyHostToDevice));
+  // P0 fallback marks (DGCell::setToZero), on by default for the Euler laws
+  // whose isPhysical can fail
+  if ((rc = s->alloc(&b.bad, static_cast<size_t>(Etot)))) return rc;
+  DGP_CUDA(cudaMemset(b.bad, 0, Etot));
+  b.p0 = (s->law == DGP_LAW_EULER2D || s->law == DGP_LAW_EULER3D) ? 1 : 0;
+  if (s->limiter == DGP_LIMITER_MOMENT && s->order >= 1) {
+    if ((rc = setup_limiter(s))) return rc;
+  }
+  if (cudaError_t e = s->ops.prepare()) return fail(DGP_ERR_CUDA, cudaGetErrorString(e));
+  // DGAnalysis::DGAnalysis projects the far field as the initial state
+  s->ops.project(b, 0.0, s->stream);
+  DGP_CUDA(cudaGetLastError());
+  DGP_CUDA(cudaStreamSynchronize(s->stream));
+  return DGP_OK;
+}
+
+// common part of solver and ensemble-group creation: kernels, tables, stream
+static int solver_begin(dgp_solver s, int law, int flux, int dim, int order, int precision, int limiter) {
+  ensure_registry();
+  auto it = ops_registry().find(OpsKey(law, flux, dim, order, precision));
+  if (it == ops_registry().end())
+    return fail(DGP_ERR_UNSUPPORTED, "no kernels for this law/flux/element/order/precision");
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
+    return fail(DGP_ERR_CUDA, "no CUDA device available");
+  s->ops = it->second;
+  s->law = law;
+  s->flux = flux;
+  s->order = order;
+  s->precision = precision;
+  s->limiter = limiter;
+  cudaGetDevice(&s->device);
+  std::string err;
+  if (int rc = build_tables(dim, order, s->tab, err)) return fail(rc, err);
+  const RefTables& t = s->tab;
+  if (t.nq != s->ops.NQ || t.nqf != s->ops.NQF || t.Np != s->ops.NP)
+    return fail(DGP_ERR_UNSUPPORTED, "table/kernel shape mismatch");
+  if (cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking) != cudaSuccess)
+    return fail(DGP_ERR_CUDA, "stream creation failed");
+  if (cudaMallocHost(&s->h_ctl, 2 * sizeof(TimeCtl)) != cudaSuccess)
+    return fail(DGP_ERR_CUDA, "pinned allocation failed");
   return DGP_OK;
 }
 
@@ -256,219 +547,19 @@ int dgp_solver_create(dgp_mesh mh, dgp_law law, int order, int precision, int li
     return fail(DGP_ERR_UNSUPPORTED, "2D law on a 3D mesh");
   if ((law->kind == DGP_LAW_EULER3D || law->kind == DGP_LAW_MAXWELL3D) && m.dim != 3)
     return fail(DGP_ERR_UNSUPPORTED, "3D law on a 2D mesh");
-  ensure_registry();
-  auto it = ops_registry().find(OpsKey(law->kind, law->flux, m.dim, order, precision));
-  if (it == ops_registry().end())
-    return fail(DGP_ERR_UNSUPPORTED, "no kernels for this law/flux/element/order/precision");
-  int ndev = 0;
-  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
-    return fail(DGP_ERR_CUDA, "no CUDA device available");
-
   auto s = new dgp_solver_s;
-  auto bail = [&](int rc) {
+  if (int rc = solver_begin(s, law->kind, law->flux, m.dim, order, precision, limiter)) {
     delete s;
     return rc;
-  };
-  s->mesh = m;
-  s->ops = it->second;
-  s->law = law->kind;
-  s->flux = law->flux;
-  s->order = order;
-  s->precision = precision;
-  s->limiter = limiter;
-  cudaGetDevice(&s->device);
-  std::string err;
-  if (int rc = build_tables(m.dim, order, s->tab, err)) return bail(fail(rc, err));
-  const RefTables& t = s->tab;
-  if (t.nq != s->ops.NQ || t.nqf != s->ops.NQF || t.Np != s->ops.NP)
-    return bail(fail(DGP_ERR_UNSUPPORTED, "table/kernel shape mismatch"));
-  if (cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking) != cudaSuccess)
-    return bail(fail(DGP_ERR_CUDA, "stream creation failed"));
-  if (cudaMallocHost(&s->h_ctl, 2 * sizeof(TimeCtl)) != cudaSuccess)
-    return bail(fail(DGP_ERR_CUDA, "pinned allocation failed"));
-
-  const int dim = m.dim, E = m.E, nvc = m.nvc;
-  DeviceBuffers& b = s->b;
-  b.E = E;
-  b.dim = dim;
-  b.order = order;
-  b.M = s->ops.M;
-  b.NP = s->ops.NP;
-
-  // internal order: Morton code of the cell centroids (locality of neighbours)
-  {
-    double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
-    std::vector<double> cen(static_cast<size_t>(E) * 3);
-    for (int e = 0; e < E; ++e)
-      for (int c = 0; c < 3; ++c) {
-        double x = 0;
-        for (int k = 0; k < nvc; ++k) x += m.X[3 * m.cv[static_cast<size_t>(e) * nvc + k] + c];
-        x /= nvc;
-        cen[3 * e + c] = x;
-        lo[c] = std::min(lo[c], x);
-        hi[c] = std::max(hi[c], x);
-      }
-    std::vector<uint64_t> key(E);
-    for (int e = 0; e < E; ++e) {
-      uint32_t qv[3];
-      for (int c = 0; c < 3; ++c) {
-        double span = hi[c] - lo[c];
-        double u = span > 0 ? (cen[3 * e + c] - lo[c]) / span : 0.0;
-        double scale = dim == 2 ? 4294967295.0 : 2097151.0;
-        qv[c] = static_cast<uint32_t>(std::min(scale, std::max(0.0, u * scale)));
-      }
-      key[e] = dim == 2 ? (spread2(qv[0]) | (spread2(qv[1]) << 1))
-                        : (spread3(qv[0]) | (spread3(qv[1]) << 1) | (spread3(qv[2]) << 2));
-    }
-    s->i2f.resize(E);
-    std::iota(s->i2f.begin(), s->i2f.end(), 0);
-    std::stable_sort(s->i2f.begin(), s->i2f.end(), [&](int a, int c) { return key[a] < key[c]; });
-    s->f2i.resize(E);
-    for (int i = 0; i < E; ++i) s->f2i[s->i2f[i]] = i;
   }
-
-  // cell geometry (FP64 on the host)
-  std::vector<double> jinv(static_cast<size_t>(E) * dim * dim), detj(E), csize(E), x0(3 * (size_t)E),
-      jac(9 * (size_t)E);
-  for (int i = 0; i < E; ++i) {
-    const int e = s->i2f[i];
-    double X0[3], J[9], Ji[9];
-    cell_frame(m, e, X0, J);
-    double d = invert3(J, Ji);
-    detj[i] = std::fabs(d);
-    for (int r = 0; r < dim; ++r)
-      for (int c = 0; c < dim; ++c) jinv[static_cast<size_t>(i) * dim * dim + r * dim + c] = Ji[r * 3 + c];
-    for (int k = 0; k < 3; ++k) x0[3 * i + k] = X0[k];
-    for (int k = 0; k < 9; ++k) jac[9 * i + k] = J[k];
-    const int* c = &m.cv[static_cast<size_t>(e) * nvc];
-    auto len = [&](int a, int bb) {
-      const double *p = &m.X[3 * c[a]], *q = &m.X[3 * c[bb]];
-      return std::sqrt((q[0] - p[0]) * (q[0] - p[0]) + (q[1] - p[1]) * (q[1] - p[1]) +
-                       (q[2] - p[2]) * (q[2] - p[2]));
-    };
-    if (dim == 2) {  // DGCell::computeCellSize (DGCell.cc:1211-1229)
-      double a = len(0, 1), bb = len(1, 2), cc = len(2, 0);
-      double hp = 0.5 * (a + bb + cc);
-      csize[i] = std::sqrt(hp * (hp - a) * (hp - bb) * (hp - cc)) / hp * 2.;
-    } else {  // minimum edge (DGCell.cc:1239-1256)
-      double L[6] = {len(0, 1), len(1, 2), len(2, 0), len(0, 3), len(1, 3), len(2, 3)};
-      double mn = L[0];
-      for (int k = 1; k < 6; ++k) mn = std::min(mn, L[k]);
-      csize[i] = mn;
-    }
+  s->meshes.push_back(m);
+  LawParams lp{};
+  lp.field = law->field;
+  for (int i = 0; i < DGP_NPARAMS; ++i) lp.p[i] = law->p[i];
+  if (int rc = build_solver(s, {lp}, law->field, false)) {
+    delete s;
+    return rc;
   }
-  // faces sorted by internal left cell
-  std::vector<int> forder(m.F);
-  std::iota(forder.begin(), forder.end(), 0);
-  std::stable_sort(forder.begin(), forder.end(), [&](int a, int c) {
-    int ia = s->f2i[m.eL[a]], ic = s->f2i[m.eL[c]];
-    return ia != ic ? ia < ic : m.lfL[a] < m.lfL[c];
-  });
-  std::vector<int> fel(2 * (size_t)m.F), fcode(m.F), bbid;
-  std::vector<double> fnrm(static_cast<size_t>(m.F) * dim), fj(m.F), bpts;
-  int nb = 0;
-  for (int k = 0; k < m.F; ++k) {
-    const int f = forder[k];
-    fel[2 * k] = s->f2i[m.eL[f]];
-    if (m.eR[f] >= 0) {
-      fel[2 * k + 1] = s->f2i[m.eR[f]];
-    } else {
-      fel[2 * k + 1] = -(nb + 1);
-      bbid.push_back(m.bid[f]);
-      const int* fv = &m.fv[static_cast<size_t>(f) * m.nfv];
-      for (int q = 0; q < t.nqf; ++q) {
-        const double *pa = &m.X[3 * fv[0]], *pb = &m.X[3 * fv[1]];
-        double x[3];
-        if (dim == 2) {
-          double sp = t.fqp[2 * q];
-          for (int c = 0; c < 3; ++c) x[c] = pa[c] * (1 - sp) * 0.5 + pb[c] * (1 + sp) * 0.5;
-        } else {
-          const double* pc = &m.X[3 * fv[2]];
-          double u = t.fqp[2 * q], v = t.fqp[2 * q + 1];
-          for (int c = 0; c < 3; ++c) x[c] = pa[c] * (1 - u - v) + pb[c] * u + pc[c] * v;
-        }
-        bpts.insert(bpts.end(), x, x + 3);
-      }
-      ++nb;
-    }
-    fcode[k] = m.lfL[f] | ((m.eR[f] >= 0 ? m.lfR[f] : 0) << 4) | (m.rperm[f] << 8);
-    for (int c = 0; c < dim; ++c) fnrm[static_cast<size_t>(k) * dim + c] = m.fn[3 * f + c];
-    fj[k] = dim == 2 ? 0.5 * m.fmeas[f] : 2.0 * m.fmeas[f];  // |J_f| of the face map
-  }
-  b.F = m.F;
-  b.NB = nb;
-
-  // reference tables
-  std::vector<double> qpd(static_cast<size_t>(t.nq) * 3);
-  for (int q = 0; q < t.nq; ++q)
-    for (int c = 0; c < 3; ++c) qpd[3 * q + c] = t.qp[3 * q + c];
-  int rc = DGP_OK;
-  if ((rc = s->upload_t(&b.jinv, jinv)) || (rc = s->upload_t(&b.detj, detj)) ||
-      (rc = s->upload(&b.detjd, detj)) ||
-      (rc = s->upload(&b.csize, csize)) || (rc = s->upload(&b.x0, x0)) || (rc = s->upload(&b.jac, jac)) ||
-      (rc = s->upload(&b.fel, fel)) || (rc = s->upload(&b.fcode, fcode)) ||
-      (rc = s->upload_t(&b.fnrm, fnrm)) || (rc = s->upload_t(&b.fj, fj)) ||
-      (rc = s->upload(&b.bpts, bpts.empty() ? std::vector<double>(3, 0.0) : bpts)) ||
-      (rc = s->upload(&b.bbid, bbid.empty() ? std::vector<int>(1, 0) : bbid)) ||
-      (rc = s->upload_t(&b.phi, t.phi)) || (rc = s->upload_t(&b.dphi, t.dphi)) ||
-      (rc = s->upload_t(&b.qw, t.qw)) || (rc = s->upload_t(&b.phif, t.phif)) ||
-      (rc = s->upload_t(&b.fqw, t.fqw)) || (rc = s->upload(&b.qmap, t.qmap)) ||
-      (rc = s->upload(&b.phiv, t.phiv)) || (rc = s->upload(&b.phiq, t.phi)) ||
-      (rc = s->upload(&b.qwd, t.qw)) || (rc = s->upload(&b.qpd, qpd)) ||
-      (rc = s->upload(&b.eqp, t.eqp)) || (rc = s->upload(&b.eqw, t.eqw)) ||
-      (rc = s->upload(&b.ephi, t.ephi)) || (rc = s->upload(&s->d_i2f, s->i2f)) ||
-      (rc = s->upload(&s->d_f2i, s->f2i)))
-    return bail(rc);
-  {
-    std::vector<double> blob(s->ops.blob_elems);
-    s->ops.fill_blob(t.dphi.data(), t.phif.data(), t.phi.data(), t.qw.data(), blob.data());
-    if ((rc = s->upload_t(&b.blob, blob))) return bail(rc);
-    b.blob_bytes = static_cast<int>(s->ops.blob_elems * s->ops.tsize);
-  }
-  b.nqe = t.nqe;
-  b.phi0 = t.phi0;
-  b.law.field = law->field;
-  for (int i = 0; i < DGP_NPARAMS; ++i) b.law.p[i] = law->p[i];
-
-  const size_t nstate = s->state_count();
-  // slots are tile-transposed over whole tiles of TE cells; state buffers get
-  // 256 bytes of tail so the bulk copy of the last tile may round up to 16 bytes
-  const size_t ntiles = (static_cast<size_t>(E) + s->ops.TE - 1) / s->ops.TE;
-  const size_t nslot = ntiles * s->ops.TE * t.nlf * t.nqf * b.M;
-  unsigned char *C, *U0, *slots, *rhs, *scratch;
-  const size_t ts = s->ops.tsize;  // slots hold the RHS arithmetic type; the state is FP64
-  if ((rc = s->alloc(&C, nstate * 8 + 256)) || (rc = s->alloc(&U0, nstate * 8 + 256)) ||
-      (rc = s->alloc(&slots, nslot * ts)) || (rc = s->alloc(&rhs, nstate * 8 + 256)) ||
-      (rc = s->alloc(&scratch, nstate * 8 + 256)))
-    return bail(rc);
-  b.C = C;
-  b.U0 = U0;
-  b.slots = slots;
-  b.rhs = rhs;
-  b.scratch = scratch;
-  b.npartials = std::max(s->ops.grid_elem(E), (E + 255) / 256) * std::max(b.M, 1) + 1;
-  if ((rc = s->alloc(&b.partials, b.npartials)) || (rc = s->alloc(&b.ctl, 1)) ||
-      (rc = s->alloc(&b.status, 1)))
-    return bail(rc);
-  DGP_CUDA(cudaMemset(slots, 0, nslot * ts));
-  // P0 fallback marks (DGCell::setToZero), on by default for the Euler laws
-  // whose isPhysical can fail
-  if ((rc = s->alloc(&b.bad, static_cast<size_t>(E)))) return bail(rc);
-  DGP_CUDA(cudaMemset(b.bad, 0, E));
-  b.p0 = (law->kind == DGP_LAW_EULER2D || law->kind == DGP_LAW_EULER3D) ? 1 : 0;
-  if (limiter == DGP_LIMITER_MOMENT && order >= 1) {
-    if ((rc = setup_limiter(s))) return bail(rc);
-  }
-  TimeCtl c0{};
-  c0.dtmin_bits = 0x7FF0000000000000ull;
-  DGP_CUDA(cudaMemcpy(b.ctl, &c0, sizeof(TimeCtl), cudaMemcpyHostToDevice));
-  Status st0{0, INT32_MAX};
-  DGP_CUDA(cudaMemcpy(b.status, &st0, sizeof(Status), cudaMemcpyHostToDevice));
-  if (cudaError_t e = s->ops.prepare()) return bail(fail(DGP_ERR_CUDA, cudaGetErrorString(e)));
-  // DGAnalysis::DGAnalysis projects the far field as the initial state
-  s->ops.project(b, 0.0, s->stream);
-  DGP_CUDA(cudaGetLastError());
-  DGP_CUDA(cudaStreamSynchronize(s->stream));
   *out = s;
   return DGP_OK;
 }
@@ -730,7 +821,7 @@ int dgp_status(dgp_solver s, int* nonphysical, int* first_bad_cell) {
 int dgp_l2_error(dgp_solver s, double t, int field, double* err) {
   if (!s || !err || field < 0 || field >= s->b.M) return fail(DGP_ERR_INVALID, "bad argument");
   DGP_CUDA(cudaSetDevice(s->device));
-  s->ops.l2err(s->b, t, field, s->stream);
+  s->ops.l2err(s->b, t, field, 0, s->b.E, nullptr, s->stream);
   DGP_CUDA(cudaGetLastError());
   const int nblk = (s->b.E + 255) / 256;
   std::vector<double> p(nblk);
@@ -746,7 +837,7 @@ int dgp_totals(dgp_solver s, double* totals) {
   if (!s || !totals) return fail(DGP_ERR_INVALID, "bad argument");
   DGP_CUDA(cudaSetDevice(s->device));
   const double refm = s->b.dim == 2 ? 0.5 : 1.0 / 6.0;
-  s->ops.totals(s->b, refm, s->stream);
+  s->ops.totals(s->b, refm, 0, s->b.E, s->stream);
   DGP_CUDA(cudaGetLastError());
   const int nblk = (s->b.E + 255) / 256;
   std::vector<double> p(static_cast<size_t>(nblk) * s->b.M);
@@ -804,6 +895,285 @@ int dgp_synchronize(dgp_solver s) {
   if (!s) return fail(DGP_ERR_INVALID, "null solver");
   DGP_CUDA(cudaSetDevice(s->device));
   DGP_CUDA(cudaStreamSynchronize(s->stream));
+  return DGP_OK;
+}
+
+
+// ---------------------------------------------------------------------------
+// Ensembles: independent instances of uneven size run batched.  Instances of
+// one (law, flux, element, order) form a group whose cells, faces and state
+// live in one index space (each instance from a tile boundary), so that one
+// face kernel and one element kernel per stage serve the whole group; each
+// instance keeps its own time control (CFL step, end time, done flag, finish
+// clock).  Groups run on their own streams; a run is a loop of CUDA-graph
+// launches of 8 steps per group until every instance is done.
+
+int dgp_ensemble_create(int n, const dgp_mesh* meshes, const dgp_law* laws, const int* orders, int precision,
+                        int limiter, dgp_ensemble* out) {
+  if (n <= 0 || !meshes || !laws || !orders || !out) return fail(DGP_ERR_INVALID, "bad argument");
+  if (precision != DGP_PRECISION_FP64 && precision != DGP_PRECISION_MIXED)
+    return fail(DGP_ERR_INVALID, "unknown precision");
+  if (limiter != DGP_LIMITER_NONE && limiter != DGP_LIMITER_MOMENT) return fail(DGP_ERR_INVALID, "unknown limiter");
+  std::map<std::tuple<int, int, int, int>, std::vector<int>> groups;
+  for (int i = 0; i < n; ++i) {
+    if (!meshes[i] || !laws[i]) return fail(DGP_ERR_INVALID, "null mesh or law");
+    const HostMesh& m = meshes[i]->m;
+    const dgp_law_s* l = laws[i];
+    if ((l->kind == DGP_LAW_EULER2D || l->kind == DGP_LAW_BURGERS2D) && m.dim != 2)
+      return fail(DGP_ERR_UNSUPPORTED, "2D law on a 3D mesh");
+    if ((l->kind == DGP_LAW_EULER3D || l->kind == DGP_LAW_MAXWELL3D) && m.dim != 3)
+      return fail(DGP_ERR_UNSUPPORTED, "3D law on a 2D mesh");
+    if (limiter == DGP_LIMITER_MOMENT && m.dim != 2)
+      return fail(DGP_ERR_UNSUPPORTED, "the moment limiter is built for triangles only");
+    groups[std::make_tuple(l->kind, l->flux, m.dim, orders[i])].push_back(i);
+  }
+  auto e = new dgp_ensemble_s;
+  e->inst_group.assign(n, -1);
+  e->inst_index.assign(n, -1);
+  for (auto& kv : groups) {
+    const auto& members = kv.second;
+    const dgp_law_s* l0 = laws[members[0]];
+    for (int i : members)
+      if (laws[i]->p[7] != l0->p[7]) {
+        delete e;
+        return fail(DGP_ERR_INVALID, "instances of one law/order group must share gamma");
+      }
+    auto s = new dgp_solver_s;
+    if (int rc = solver_begin(s, std::get<0>(kv.first), std::get<1>(kv.first), std::get<2>(kv.first),
+                              std::get<3>(kv.first), precision, limiter)) {
+      delete s;
+      delete e;
+      return rc;
+    }
+    std::vector<LawParams> lps;
+    for (size_t k = 0; k < members.size(); ++k) {
+      const int i = members[k];
+      s->meshes.push_back(meshes[i]->m);
+      LawParams lp{};
+      lp.field = laws[i]->field;
+      for (int q = 0; q < DGP_NPARAMS; ++q) lp.p[q] = laws[i]->p[q];
+      lps.push_back(lp);
+      e->inst_group[i] = static_cast<int>(e->groups.size());
+      e->inst_index[i] = static_cast<int>(k);
+    }
+    if (int rc = build_solver(s, lps, l0->field, true)) {
+      delete s;
+      delete e;
+      return rc;
+    }
+    e->groups.push_back(s);
+  }
+  e->n = n;
+  *out = e;
+  return DGP_OK;
+}
+
+int dgp_ensemble_destroy(dgp_ensemble e) {
+  if (!e) return DGP_OK;
+  for (dgp_solver s : e->groups) dgp_solver_destroy(s);
+  delete e;
+  return DGP_OK;
+}
+
+int dgp_ensemble_info(dgp_ensemble e, int i, int* nfields, int* nmodes, int* ncells, int* group) {
+  if (!e || i < 0 || i >= e->n) return fail(DGP_ERR_INVALID, "bad instance");
+  dgp_solver s = e->groups[e->inst_group[i]];
+  if (nfields) *nfields = s->b.M;
+  if (nmodes) *nmodes = s->b.NP;
+  if (ncells) *ncells = s->meshes[e->inst_index[i]].E;
+  if (group) *group = e->inst_group[i];
+  return DGP_OK;
+}
+
+int dgp_ensemble_project(dgp_ensemble e, double t) {
+  if (!e) return fail(DGP_ERR_INVALID, "null ensemble");
+  for (dgp_solver s : e->groups)
+    if (int rc = dgp_project(s, t)) return rc;
+  return DGP_OK;
+}
+
+static int ens_rows(dgp_ensemble e, int i, dgp_solver* s, int* k, size_t* mnp) {
+  if (!e || i < 0 || i >= e->n) return fail(DGP_ERR_INVALID, "bad instance");
+  *s = e->groups[e->inst_group[i]];
+  *k = e->inst_index[i];
+  *mnp = static_cast<size_t>((*s)->b.M) * (*s)->b.NP;
+  return DGP_OK;
+}
+
+int dgp_ensemble_get_state(dgp_ensemble e, int i, double* host_state) {
+  dgp_solver s;
+  int k;
+  size_t mnp;
+  if (int rc = ens_rows(e, i, &s, &k, &mnp)) return rc;
+  if (!host_state) return fail(DGP_ERR_INVALID, "null argument");
+  DGP_CUDA(cudaSetDevice(s->device));
+  DGP_CUDA(cudaStreamSynchronize(s->stream));
+  const int E = s->meshes[k].E, off = s->inst_off[k], uf = s->inst_ufirst[k];
+  std::vector<double> tmp(static_cast<size_t>(E) * mnp);
+  DGP_CUDA(cudaMemcpy(tmp.data(), static_cast<double*>(s->b.C) + static_cast<size_t>(off) * mnp,
+                      tmp.size() * 8, cudaMemcpyDeviceToHost));
+  for (int r = 0; r < E; ++r)
+    std::memcpy(&host_state[static_cast<size_t>(s->i2f[off + r] - uf) * mnp], &tmp[r * mnp], mnp * 8);
+  return DGP_OK;
+}
+
+int dgp_ensemble_set_state(dgp_ensemble e, int i, const double* host_state) {
+  dgp_solver s;
+  int k;
+  size_t mnp;
+  if (int rc = ens_rows(e, i, &s, &k, &mnp)) return rc;
+  if (!host_state) return fail(DGP_ERR_INVALID, "null argument");
+  DGP_CUDA(cudaSetDevice(s->device));
+  DGP_CUDA(cudaStreamSynchronize(s->stream));
+  const int E = s->meshes[k].E, off = s->inst_off[k], uf = s->inst_ufirst[k];
+  std::vector<double> tmp(static_cast<size_t>(E) * mnp);
+  for (int r = 0; r < E; ++r)
+    std::memcpy(&tmp[r * mnp], &host_state[static_cast<size_t>(s->i2f[off + r] - uf) * mnp], mnp * 8);
+  DGP_CUDA(cudaMemcpy(static_cast<double*>(s->b.C) + static_cast<size_t>(off) * mnp, tmp.data(),
+                      tmp.size() * 8, cudaMemcpyHostToDevice));
+  return DGP_OK;
+}
+
+int dgp_ensemble_totals(dgp_ensemble e, int i, double* totals) {
+  dgp_solver s;
+  int k;
+  size_t mnp;
+  if (int rc = ens_rows(e, i, &s, &k, &mnp)) return rc;
+  if (!totals) return fail(DGP_ERR_INVALID, "null argument");
+  DGP_CUDA(cudaSetDevice(s->device));
+  const double refm = s->b.dim == 2 ? 0.5 : 1.0 / 6.0;
+  const int e0 = s->inst_off[k], e1 = e0 + s->meshes[k].E;
+  s->ops.totals(s->b, refm, e0, e1, s->stream);
+  DGP_CUDA(cudaGetLastError());
+  const int nblk = (e1 - e0 + 255) / 256;
+  std::vector<double> p(static_cast<size_t>(nblk) * s->b.M);
+  DGP_CUDA(cudaMemcpyAsync(p.data(), s->b.partials, p.size() * 8, cudaMemcpyDeviceToHost, s->stream));
+  DGP_CUDA(cudaStreamSynchronize(s->stream));
+  for (int j = 0; j < s->b.M; ++j) {
+    double acc = 0.0;
+    for (int q = 0; q < nblk; ++q) acc += p[static_cast<size_t>(q) * s->b.M + j];
+    totals[j] = acc;
+  }
+  return DGP_OK;
+}
+
+int dgp_ensemble_l2_error(dgp_ensemble e, int i, double t, int field, double* err) {
+  dgp_solver s;
+  int k;
+  size_t mnp;
+  if (int rc = ens_rows(e, i, &s, &k, &mnp)) return rc;
+  if (!err || field < 0 || field >= s->b.M) return fail(DGP_ERR_INVALID, "bad argument");
+  DGP_CUDA(cudaSetDevice(s->device));
+  const int e0 = s->inst_off[k], e1 = e0 + s->meshes[k].E;
+  s->ops.l2err(s->b, t, field, e0, e1, s->b.laws + k, s->stream);
+  DGP_CUDA(cudaGetLastError());
+  const int nblk = (e1 - e0 + 255) / 256;
+  std::vector<double> p(nblk);
+  DGP_CUDA(cudaMemcpyAsync(p.data(), s->b.partials, nblk * 8, cudaMemcpyDeviceToHost, s->stream));
+  DGP_CUDA(cudaStreamSynchronize(s->stream));
+  double acc = 0.0;
+  for (double v : p) acc += v;
+  *err = std::sqrt(acc);
+  return DGP_OK;
+}
+
+int dgp_ensemble_run(dgp_ensemble e, double t0, double tend, double cfl, int max_steps, double* t_out,
+                     int* steps_out, double* ms_out, double* total_ms) {
+  if (!e || !(cfl > 0)) return fail(DGP_ERR_INVALID, "bad argument");
+  if (tend <= 0 && max_steps <= 0) return fail(DGP_ERR_INVALID, "need an end time or a step count");
+  const int G = static_cast<int>(e->groups.size());
+  dgp_solver s0 = e->groups[0];
+  DGP_CUDA(cudaSetDevice(s0->device));
+  for (dgp_solver s : e->groups) {
+    // drain earlier work (set_state, project) before the controls change
+    DGP_CUDA(cudaStreamSynchronize(s->stream));
+    if (!s->graph) {
+      const int K = 8;
+      cudaGraph_t g;
+      DGP_CUDA(cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal));
+      for (int k = 0; k < K; ++k) launch_step(s, 1);
+      DGP_CUDA(cudaStreamEndCapture(s->stream, &g));
+      cudaError_t err = cudaGraphInstantiate(&s->graph, g, 0);
+      cudaGraphDestroy(g);
+      if (err != cudaSuccess) return fail(DGP_ERR_CUDA, std::string("graph: ") + cudaGetErrorString(err));
+      s->graph_steps = K;
+    }
+    const int n = s->b.ninst;
+    std::vector<TimeCtl> c(n + 1);
+    for (auto& x : c) {
+      x = TimeCtl{};
+      x.t = t0;
+      x.tend = tend;
+      x.cfl = cfl;
+      x.max_steps = max_steps;
+      x.dtmin_bits = 0x7FF0000000000000ull;
+    }
+    DGP_CUDA(cudaMemcpy(s->b.ctl, c.data(), c.size() * sizeof(TimeCtl), cudaMemcpyHostToDevice));
+  }
+  // common start: every group waits for the clock mark on the first stream
+  cudaEvent_t start;
+  DGP_CUDA(cudaEventCreateWithFlags(&start, cudaEventDisableTiming));
+  mark_clock<<<1, 1, 0, s0->stream>>>(s0->b.gctl);
+  DGP_CUDA(cudaEventRecord(start, s0->stream));
+  for (dgp_solver s : e->groups) {
+    if (s != s0) DGP_CUDA(cudaStreamWaitEvent(s->stream, start, 0));
+    s->ops.cfl(s->b, s->stream);
+  }
+  DGP_CUDA(cudaGetLastError());
+  std::vector<int> done(G, 0);
+  std::vector<TimeCtl*> gpin(G);
+  for (int g = 0; g < G; ++g) gpin[g] = &e->groups[g]->h_ctl[1];
+  for (;;) {
+    int all = 1;
+    for (int g = 0; g < G; ++g)
+      if (!done[g]) {
+        dgp_solver s = e->groups[g];
+        DGP_CUDA(cudaGraphLaunch(s->graph, s->stream));
+        DGP_CUDA(cudaMemcpyAsync(gpin[g], s->b.gctl, sizeof(TimeCtl), cudaMemcpyDeviceToHost, s->stream));
+      }
+    for (int g = 0; g < G; ++g)
+      if (!done[g]) {
+        DGP_CUDA(cudaStreamSynchronize(e->groups[g]->stream));
+        done[g] = gpin[g]->done;
+        all &= done[g];
+      }
+    if (all) break;
+  }
+  cudaEventDestroy(start);
+  // per-instance results
+  TimeCtl g0;
+  DGP_CUDA(cudaMemcpy(&g0, s0->b.gctl, sizeof(TimeCtl), cudaMemcpyDeviceToHost));
+  double tmax = 0.0;
+  for (int g = 0; g < G; ++g) {
+    dgp_solver s = e->groups[g];
+    const int n = s->b.ninst;
+    std::vector<TimeCtl> c(n);
+    DGP_CUDA(cudaMemcpy(c.data(), s->b.ctl, n * sizeof(TimeCtl), cudaMemcpyDeviceToHost));
+    for (int i = 0; i < e->n; ++i) {
+      if (e->inst_group[i] != g) continue;
+      const TimeCtl& x = c[e->inst_index[i]];
+      const double ms = (static_cast<double>(x.t_mark_ns) - static_cast<double>(g0.t_mark_ns)) * 1e-6;
+      if (!std::isfinite(x.dt) || !(x.dt > 0))
+        return fail(DGP_ERR_NONPHYSICAL, "instance " + std::to_string(i) + ": time step not positive and finite");
+      if (t_out) t_out[i] = x.t;
+      if (steps_out) steps_out[i] = x.steps;
+      if (ms_out) ms_out[i] = ms;
+      tmax = std::max(tmax, ms);
+    }
+  }
+  if (total_ms) *total_ms = tmax;
+  return DGP_OK;
+}
+
+int dgp_ensemble_launches_per_step(dgp_ensemble e, int* n) {
+  if (!e || !n) return fail(DGP_ERR_INVALID, "null argument");
+  int tot = 0;
+  for (dgp_solver s : e->groups) {
+    int k = 0;
+    if (int rc = dgp_launches_per_step(s, &k)) return rc;
+    tot += k;
+  }
+  *n = tot;
   return DGP_OK;
 }
 

@@ -127,14 +127,92 @@ void fill_table_blob(const double* dphi, const double* phif, const double* phi, 
 
 constexpr int kMbarPolls = 1 << 22;  // bound of the bulk-copy wait
 
+// Last stage, after the update: residual partial of the tile, the CFL step of
+// the next step (fused), and in the last CTA the time advance (the residual
+// summed in a fixed order).  Tiles of finished ensemble instances join with
+// active = false so that the completion count stays whole.
 template <class K>
-__global__ void __launch_bounds__(K::BLOCK) elem_kernel(StageArgs<typename K::T> a) {
+__device__ __forceinline__ void elem_last_stage(const StageArgs<typename K::T>& a, TimeCtl* c, double rsum,
+                                                bool active, const double* sC, double* sEig, int ne, int e0,
+                                                double* red) {
+  constexpr int M = K::M, NP = K::NP, MNP = K::MNP, NV = K::NV, BLOCK = K::BLOCK;
+  __shared__ bool amLast;
+  const int tid = threadIdx.x;
+  rsum = block_sum<BLOCK>(rsum, red);
+  if (tid == 0) a.partials[blockIdx.x] = rsum;
+  if (a.fuse_cfl && active) {
+    __syncthreads();
+    // eigenvalue at the cell mean (v = 0) and, on triangles, at the three
+    // reference vertices (DGCell::computeMAXEV, DGCell.cc:1155-1207)
+    for (int it = tid; it < ne * NV; it += BLOCK) {
+      const int e = it / NV, v = it - (it / NV) * NV;
+      const double* cc = sC + e * MNP;
+      double val[M];
+      if (v == 0) {
+#pragma unroll
+        for (int j = 0; j < M; ++j) val[j] = cc[j * NP] * a.tab.phi0;
+      } else {
+        const double* pv = a.tab.phiv + (v - 1) * NP;
+#pragma unroll
+        for (int j = 0; j < M; ++j) {
+          double acc = 0;
+#pragma unroll
+          for (int k = 0; k < NP; ++k) acc += pv[k] * cc[j * NP + k];
+          val[j] = acc;
+        }
+      }
+      sEig[it] = max_eigen<K::LAW, double>(a.law, val);
+    }
+    __syncthreads();
+    double dtl = 1e300;
+    if (tid < ne) {
+      double am = sEig[tid * NV];
+#pragma unroll
+      for (int v = 1; v < NV; ++v) {
+        const double b = sEig[tid * NV + v];
+        am = (b > am ? b : am);
+      }
+      dtl = a.mesh.csize[e0 + tid] * c->cfl / (am * (2. * K::ORDER + 1.0));
+    }
+    dtl = block_min<BLOCK>(dtl, red);
+    if (tid == 0) atomicMin(&c->dtmin_bits, (unsigned long long)__double_as_longlong(dtl));
+  }
+  if (tid == 0) {
+    __threadfence();
+    const unsigned v = atomicAdd(&a.gctl->blocks_done, 1u);
+    amLast = (v == gridDim.x - 1);
+  }
+  __syncthreads();
+  if (!amLast) return;
+  __threadfence();
+  if (a.cell_inst) {
+    finalize_instances<BLOCK>(a, true, a.fuse_cfl != 0);
+    return;
+  }
+  // single solver: residual in a fixed order (strided partial sums + tree)
+  double r = 0.0;
+  for (unsigned b = tid; b < gridDim.x; b += BLOCK) r += ((volatile double*)a.partials)[b];
+  r = block_sum<BLOCK>(r, red);
+  if (tid == 0) {
+    c->resid = r;
+    c->blocks_done = 0;
+    c->t = c->t + c->dt;
+    c->steps += 1;
+    if (a.fuse_cfl) {
+      const unsigned long long bits = atomicExch(&c->dtmin_bits, 0x7FF0000000000000ull);
+      ctl_finalize(c, __longlong_as_double((long long)bits));
+    }
+  }
+}
+
+template <class K>
+__global__ void __launch_bounds__(K::BLOCK) elem_kernel(const __grid_constant__ StageArgs<typename K::T> a) {
   using T = typename K::T;
   using L = ElemSmem<K>;
   constexpr int M = K::M, NP = K::NP, NQ = K::NQ, DIM = K::DIM, TE = K::TE, BLOCK = K::BLOCK;
-  constexpr int MNP = K::MNP, NS = K::NS, KV = K::KV, LDK = K::LDK, NV = K::NV, ROWS = K::ROWS;
+  constexpr int MNP = K::MNP, NS = K::NS, KV = K::KV, LDK = K::LDK, ROWS = K::ROWS;
   constexpr int NPP = L::NPP, DD = L::DD;
-  if (a.ctl->done) return;
+  if (a.gctl->done) return;
   extern __shared__ __align__(128) unsigned char smem_raw[];
   T* sT = reinterpret_cast<T*>(smem_raw);
   T* sDphi = sT + L::oDphi;
@@ -147,12 +225,22 @@ __global__ void __launch_bounds__(K::BLOCK) elem_kernel(StageArgs<typename K::T>
   double* sEig = sJ + TE * DD;
   __shared__ __align__(8) uint64_t bar;
   __shared__ double red[BLOCK / 32];
-  __shared__ bool amLast;
   __shared__ int s_fail;
 
   const int tid = threadIdx.x;
   const int e0 = blockIdx.x * TE;
-  const int ne = min(TE, a.mesh.E - e0);
+  TimeCtl* c = a.ctl;
+  int eend = a.mesh.E;
+  if (a.cell_inst) {  // ensemble: the tile belongs to one instance
+    const int inst = a.cell_inst[e0];
+    c = a.ctl + inst;
+    eend = a.inst_end[inst];
+    if (c->done) {
+      if (a.stage == 3) elem_last_stage<K>(a, c, 0.0, false, nullptr, nullptr, 0, e0, red);
+      return;
+    }
+  }
+  const int ne = min(TE, eend - e0);
   const uint32_t c_bytes = (uint32_t)(((size_t)ne * MNP * 8 + 15) / 16 * 16);
 
   if (tid == 0) {
@@ -259,7 +347,7 @@ __global__ void __launch_bounds__(K::BLOCK) elem_kernel(StageArgs<typename K::T>
     } else {
       const int e = row / M;
       // FP64 update in the reference's operation order (dt/|J| in FP64)
-      const double dtj = a.ctl->dt / sJ[e * DD + DIM * DIM];
+      const double dtj = c->dt / sJ[e * DD + DIM * DIM];
       double* crow = sC + row * NP;
       double c[NP];
       load_vec<double, NP>(crow, c);
@@ -284,70 +372,7 @@ __global__ void __launch_bounds__(K::BLOCK) elem_kernel(StageArgs<typename K::T>
     }
   }
   if (a.stage != 3) return;
-
-  // last stage: residual partial and the CFL step of the next step
-  rsum = block_sum<BLOCK>(rsum, red);
-  if (tid == 0) a.partials[blockIdx.x] = rsum;
-  if (a.fuse_cfl) {
-    __syncthreads();
-    // eigenvalue at the cell mean (v = 0) and, on triangles, at the three
-    // reference vertices (DGCell::computeMAXEV, DGCell.cc:1155-1207)
-    for (int it = tid; it < ne * NV; it += BLOCK) {
-      const int e = it / NV, v = it - (it / NV) * NV;
-      const double* c = sC + e * MNP;
-      double val[M];
-      if (v == 0) {
-#pragma unroll
-        for (int j = 0; j < M; ++j) val[j] = c[j * NP] * a.tab.phi0;
-      } else {
-        const double* pv = a.tab.phiv + (v - 1) * NP;
-#pragma unroll
-        for (int j = 0; j < M; ++j) {
-          double acc = 0;
-#pragma unroll
-          for (int k = 0; k < NP; ++k) acc += pv[k] * c[j * NP + k];
-          val[j] = acc;
-        }
-      }
-      sEig[it] = max_eigen<K::LAW, double>(a.law, val);
-    }
-    __syncthreads();
-    double dtl = 1e300;
-    if (tid < ne) {
-      double am = sEig[tid * NV];
-#pragma unroll
-      for (int v = 1; v < NV; ++v) {
-        const double b = sEig[tid * NV + v];
-        am = (b > am ? b : am);
-      }
-      dtl = a.mesh.csize[e0 + tid] * a.ctl->cfl / (am * (2. * K::ORDER + 1.0));
-    }
-    dtl = block_min<BLOCK>(dtl, red);
-    if (tid == 0) atomicMin(&a.ctl->dtmin_bits, (unsigned long long)__double_as_longlong(dtl));
-  }
-  if (tid == 0) {
-    __threadfence();
-    const unsigned v = atomicAdd(&a.ctl->blocks_done, 1u);
-    amLast = (v == gridDim.x - 1);
-  }
-  __syncthreads();
-  if (!amLast) return;
-  // the last CTA: residual in a fixed order (strided partial sums + tree)
-  __threadfence();
-  double r = 0.0;
-  for (unsigned b = tid; b < gridDim.x; b += BLOCK) r += ((volatile double*)a.partials)[b];
-  r = block_sum<BLOCK>(r, red);
-  if (tid == 0) {
-    TimeCtl* c = a.ctl;
-    c->resid = r;
-    c->blocks_done = 0;
-    c->t = c->t + c->dt;
-    c->steps += 1;
-    if (a.fuse_cfl) {
-      const unsigned long long bits = atomicExch(&c->dtmin_bits, 0x7FF0000000000000ull);
-      ctl_finalize(c, __longlong_as_double((long long)bits));
-    }
-  }
+  elem_last_stage<K>(a, c, rsum, true, sC, sEig, ne, e0, red);
 }
 
 }  // namespace dgp

@@ -35,7 +35,9 @@ struct dgp_law_s {
 };
 
 struct dgp_solver_s {
-  dgp::HostMesh mesh;
+  std::vector<dgp::HostMesh> meshes;  // one per instance (one for a single solver)
+  std::vector<int> inst_off;          // first internal cell of each instance
+  std::vector<int> inst_ufirst;       // first cell of each instance in the joined file order
   dgp::RefTables tab;
   dgp::Ops ops;
   dgp::DeviceBuffers b;
@@ -88,4 +90,10 @@ struct dgp_solver_s {
     return DGP_OK;
   }
   size_t state_count() const { return static_cast<size_t>(b.E) * b.M * b.NP; }
+};
+
+struct dgp_ensemble_s {
+  int n = 0;
+  std::vector<dgp_solver> groups;       // one batched solver per (law, flux, element, order)
+  std::vector<int> inst_group, inst_index;
 };

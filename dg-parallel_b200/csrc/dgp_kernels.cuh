@@ -82,6 +82,8 @@ struct TimeCtl {
   unsigned long long dtmin_bits;  // atomicMin accumulator (positive double bits)
   unsigned int blocks_done;       // completion counter of the reducing kernel
   unsigned int pad2;
+  unsigned long long t_mark_ns;   // device clock: run start (whole-launch entry) or
+                                  // the moment the instance finished (ensembles)
 };
 
 struct Status {
@@ -146,6 +148,16 @@ struct StageArgs {
   double* partials;  // per-block residual partials (stage 3)
   double stage_time_factor;  // 0, 1, 0.5: boundary time = t + factor * dt
   unsigned char* bad;  // [E] P0-fallback marks (DGCell::setToZero)
+  // ensembles: a batch of independent instances in one cell/face index space,
+  // each instance's cells contiguous from a tile boundary, with its own time
+  // control ctl[i]; gctl carries the launch-wide counters and the all-done
+  // flag.  A single solver has cell_inst == nullptr and gctl == ctl.
+  TimeCtl* gctl;
+  const int* cell_inst;    // [E] instance of each cell (-1: padding)
+  const int* inst_end;     // [ninst] one past the last cell of each instance
+  const int* tile_first;   // [ninst + 1] first element-kernel tile of each instance
+  const LawParams* laws;   // [ninst] field parameters of each instance
+  int ninst;
   int stage;       // 0: RHS only, 1..3: SSP-RK3 stages
   int fuse_cfl;    // stage 3 reduces the next step's dt
   int order;
@@ -229,13 +241,18 @@ __device__ __forceinline__ void cell_trace(const double* __restrict__ c, const t
 // One face point: traces of both sides, numerical (or boundary) flux, the two
 // face slots.  RERUN: second pass of the P0 fallback, where the traces of
 // marked cells are their means.
-template <class K, bool RERUN>
+template <class K, bool RERUN, bool ENS>
 __device__ __forceinline__ void face_point(const StageArgs<typename K::T>& a, int f, int q,
                                            const typename K::T* s_phif, const typename K::T* s_fqw,
                                            const int* s_qmap) {
   using T = typename K::T;
   constexpr int M = K::M, NP = K::NP, NQF = K::NQF, DIM = K::DIM, MNP = K::MNP;
   const int eL = a.mesh.fel[2 * f], eR = a.mesh.fel[2 * f + 1];
+  int inst = 0;
+  if constexpr (ENS) {
+    inst = a.cell_inst[eL];
+    if (a.ctl[inst].done) return;
+  }
   const int code = a.mesh.fcode[f];
   const int lfL = code & 15, lfR = (code >> 4) & 15, perm = code >> 8;
   T n[DIM];
@@ -260,8 +277,14 @@ __device__ __forceinline__ void face_point(const StageArgs<typename K::T>& a, in
   } else {
     const int b = -eR - 1;
     const double* x = a.mesh.bpts + ((size_t)b * NQF + q) * 3;
-    const double time = a.ctl->t + a.stage_time_factor * a.ctl->dt;
-    boundary_flux<K::LAW, K::FLUX, DIM, T>(a.law, a.mesh.bbid[b], n, x, time, UL, flux);
+    if constexpr (ENS) {  // the instance's own clock and far-field parameters
+      const TimeCtl* c = a.ctl + inst;
+      const double time = c->t + a.stage_time_factor * c->dt;
+      boundary_flux<K::LAW, K::FLUX, DIM, T>(a.laws[inst], a.mesh.bbid[b], n, x, time, UL, flux);
+    } else {
+      const double time = a.ctl->t + a.stage_time_factor * a.ctl->dt;
+      boundary_flux<K::LAW, K::FLUX, DIM, T>(a.law, a.mesh.bbid[b], n, x, time, UL, flux);
+    }
   }
   T* sl = a.slots + slot_index<K>(eL, lfL * NQF + q, 0);
 #pragma unroll
@@ -288,10 +311,11 @@ __device__ __forceinline__ void face_tables(const StageArgs<typename K::T>& a, t
 // a.p0 set the face kernel marks every cell with a non-physical trace at a face
 // point; face_rerun_kernel then recomputes every face with the marked cells'
 // traces taken as their means and drops their modes k >= 1.
-template <class K>
-__global__ void __launch_bounds__(K::FACE_BLOCK) face_kernel(StageArgs<typename K::T> a) {
+// ENS: ensemble batch (per-instance done flags, clocks and far fields)
+template <class K, bool ENS>
+__global__ void __launch_bounds__(K::FACE_BLOCK) face_kernel(const __grid_constant__ StageArgs<typename K::T> a) {
   using T = typename K::T;
-  if (a.ctl->done) return;
+  if (a.gctl->done) return;
   __shared__ T s_phif[K::NLF * K::NQF * K::NP];
   __shared__ T s_fqw[K::NQF];
   __shared__ int s_qmap[K::NPERM * K::NQF];
@@ -300,17 +324,17 @@ __global__ void __launch_bounds__(K::FACE_BLOCK) face_kernel(StageArgs<typename 
   const int fl = tid / K::NQF, q = tid - (tid / K::NQF) * K::NQF;
   const int f = blockIdx.x * K::FPB + fl;
   if (fl >= K::FPB || f >= a.mesh.F) return;
-  face_point<K, false>(a, f, q, s_phif, s_fqw, s_qmap);
+  face_point<K, false, ENS>(a, f, q, s_phif, s_fqw, s_qmap);
 }
 
 // Second pass of the P0 fallback on a small grid: returns at once unless a
 // cell was marked in this stage (the common case costs one tiny launch).  The
 // faces read only the means of marked cells while the modes k >= 1 of those
 // cells are zeroed, so both run in the same pass.
-template <class K>
-__global__ void __launch_bounds__(K::FACE_BLOCK) face_rerun_kernel(StageArgs<typename K::T> a) {
+template <class K, bool ENS>
+__global__ void __launch_bounds__(K::FACE_BLOCK) face_rerun_kernel(const __grid_constant__ StageArgs<typename K::T> a) {
   using T = typename K::T;
-  if (a.ctl->done) return;
+  if (a.gctl->done) return;
   if (*(volatile int*)&a.status->stage_bad == 0) return;
   __shared__ T s_phif[K::NLF * K::NQF * K::NP];
   __shared__ T s_fqw[K::NQF];
@@ -325,7 +349,7 @@ __global__ void __launch_bounds__(K::FACE_BLOCK) face_rerun_kernel(StageArgs<typ
   if (fl >= K::FPB) return;
   for (int vb = blockIdx.x; vb * K::FPB < a.mesh.F; vb += gridDim.x) {
     const int f = vb * K::FPB + fl;
-    if (f < a.mesh.F) face_point<K, true>(a, f, q, s_phif, s_fqw, s_qmap);
+    if (f < a.mesh.F) face_point<K, true, ENS>(a, f, q, s_phif, s_fqw, s_qmap);
   }
 }
 
@@ -401,25 +425,76 @@ __device__ __forceinline__ double block_sum(double v, double* red) {
 
 // -----------------------------------------------------------------------------
 // -----------------------------------------------------------------------------
+__device__ __forceinline__ unsigned long long device_clock_ns() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+// Ensembles: the last CTA of a reducing kernel finalizes every instance that
+// was running (time step from its dtmin accumulator, done flag, finish time)
+// and sets the launch-wide done flag once all instances are done.
+template <int BLOCK, typename T>
+__device__ __forceinline__ void finalize_instances(const StageArgs<T>& a, bool advance, bool with_dt) {
+  for (int i = threadIdx.x; i < a.ninst; i += BLOCK) {
+    TimeCtl* c = a.ctl + i;
+    if (c->done) continue;
+    if (advance) {
+      double r = 0.0;  // residual of the instance's tiles in a fixed order
+      for (int b = a.tile_first[i]; b < a.tile_first[i + 1]; ++b) r += ((volatile double*)a.partials)[b];
+      c->resid = r;
+      c->t = c->t + c->dt;
+      c->steps += 1;
+    }
+    if (with_dt) {
+      const unsigned long long bits = atomicExch(&c->dtmin_bits, 0x7FF0000000000000ull);
+      ctl_finalize(c, __longlong_as_double((long long)bits));
+      if (c->done) c->t_mark_ns = device_clock_ns();
+    }
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    int all = 1;
+    for (int i = 0; i < a.ninst; ++i) all &= (*(volatile int*)&a.ctl[i].done) != 0;
+    a.gctl->blocks_done = 0;
+    a.gctl->done = all;
+  }
+}
+
+// CFL reduction of the first step (and, with the limiter, after the last
+// stage's limiter pass).  Ensembles reduce per instance over instance-pure
+// tiles of TE cells, one tile per block.
 template <class K>
-__global__ void __launch_bounds__(256) cfl_kernel(StageArgs<typename K::T> a) {
+__global__ void __launch_bounds__(256) cfl_kernel(const __grid_constant__ StageArgs<typename K::T> a) {
   __shared__ double red[256 / 32];
   __shared__ bool amLast;
-  if (a.ctl->done) return;
-  const int e = blockIdx.x * 256 + threadIdx.x;
+  if (a.gctl->done) return;
+  TimeCtl* c = a.ctl;
+  int e = blockIdx.x * 256 + threadIdx.x, eend = a.mesh.E;
+  bool active = true;
+  if (a.cell_inst) {
+    const int e0 = blockIdx.x * K::TE;
+    const int inst = a.cell_inst[e0];
+    c = a.ctl + inst;
+    active = !c->done;
+    e = threadIdx.x < K::TE ? e0 + threadIdx.x : a.mesh.E;
+    eend = min(e0 + K::TE, a.inst_end[inst]);
+  }
   double dtl = 1e300;
-  if (e < a.mesh.E) dtl = cell_dt<K>(a, a.C + (size_t)e * K::MNP, e, a.ctl->cfl);
+  if (active && e < eend) dtl = cell_dt<K>(a, a.C + (size_t)e * K::MNP, e, c->cfl);
   dtl = block_min<256>(dtl, red);
   if (threadIdx.x == 0) {
-    atomicMin(&a.ctl->dtmin_bits, (unsigned long long)__double_as_longlong(dtl));
+    if (active) atomicMin(&c->dtmin_bits, (unsigned long long)__double_as_longlong(dtl));
     __threadfence();
-    unsigned v = atomicAdd(&a.ctl->blocks_done, 1u);
+    unsigned v = atomicAdd(&a.gctl->blocks_done, 1u);
     amLast = (v == gridDim.x - 1);
   }
   __syncthreads();
-  if (amLast && threadIdx.x == 0) {
-    __threadfence();
-    TimeCtl* c = a.ctl;
+  if (!amLast) return;
+  __threadfence();
+  if (a.cell_inst) {
+    finalize_instances<256>(a, false, true);
+  } else if (threadIdx.x == 0) {
     c->blocks_done = 0;
     unsigned long long bits = atomicExch(&c->dtmin_bits, 0x7FF0000000000000ull);
     ctl_finalize(c, __longlong_as_double((long long)bits));
@@ -430,12 +505,18 @@ __global__ void __launch_bounds__(256) cfl_kernel(StageArgs<typename K::T> a) {
 // L2 projection of the law's field (DGCell::L2ProjInitial, DGCell.cc:1458-1483):
 // one thread per (cell, mode), FP64 accumulation in the reference's order.
 template <class K>
-__global__ void project_kernel(StageArgs<typename K::T> a, double t, double* out) {
+__global__ void project_kernel(const __grid_constant__ StageArgs<typename K::T> a, double t, double* out) {
   using T = typename K::T;
   constexpr int M = K::M, NP = K::NP, NQ = K::NQ;
   const int gid = blockIdx.x * blockDim.x + threadIdx.x;
   const int e = gid / NP, k = gid - (gid / NP) * NP;
   if (e >= a.mesh.E) return;
+  const int inst = a.cell_inst ? a.cell_inst[e] : 0;
+  if (inst < 0) {  // ensemble padding
+    for (int j = 0; j < M; ++j) out[(size_t)e * K::MNP + j * NP + k] = 0.0;
+    return;
+  }
+  const LawParams& lp = a.laws ? a.laws[inst] : a.law;
   const double* x0 = a.mesh.x0 + 3 * (size_t)e;
   const double* J = a.mesh.jac + 9 * (size_t)e;
   double proj[M];
@@ -450,7 +531,7 @@ __global__ void project_kernel(StageArgs<typename K::T> a, double t, double* out
       for (int r = 0; r < K::DIM; ++r) x[c] += xi[r] * J[r * 3 + c];
     }
     double val[M];
-    field_eval<double>(a.law, x, t, val);
+    field_eval<double>(lp, x, t, val);
     const double jw = detj * a.tab.qwd[q];
     for (int j = 0; j < M; ++j) proj[j] += val[j] * a.tab.phiq[q * NP + k] * jw;
   }
@@ -461,13 +542,15 @@ __global__ void project_kernel(StageArgs<typename K::T> a, double t, double* out
 // per-block partial sums of (u_h - u_exact)^2 |J| w of one field over the
 // error rule of degree 2(p+1) (DGCell::densityErrorL2, DGError.cc:805-826)
 template <class K>
-__global__ void __launch_bounds__(256) l2err_kernel(StageArgs<typename K::T> a, double t, int field,
-                                                     double* partials) {
+__global__ void __launch_bounds__(256) l2err_kernel(const __grid_constant__ StageArgs<typename K::T> a, double t,
+                                                     int field, double* partials, int e_begin, int e_end,
+                                                     const LawParams* lpp) {
   constexpr int M = K::M, NP = K::NP;
   __shared__ double red[256 / 32];
-  const int e = blockIdx.x * 256 + threadIdx.x;
+  const int e = e_begin + blockIdx.x * 256 + threadIdx.x;
+  const LawParams& lp = lpp ? *lpp : a.law;
   double acc = 0.0;
-  if (e < a.mesh.E) {
+  if (e < e_end) {
     const double* x0 = a.mesh.x0 + 3 * (size_t)e;
     const double* J = a.mesh.jac + 9 * (size_t)e;
     const auto* c = a.C + (size_t)e * K::MNP;
@@ -482,7 +565,7 @@ __global__ void __launch_bounds__(256) l2err_kernel(StageArgs<typename K::T> a, 
       double uh = 0.0;
       for (int k = 0; k < NP; ++k) uh += a.tab.ephi[q * NP + k] * (double)c[field * NP + k];
       double ex[M];
-      field_eval<double>(a.law, x, t, ex);
+      field_eval<double>(lp, x, t, ex);
       const double d = uh - ex[field];
       acc += d * d * detj * a.tab.eqw[q];
     }
@@ -493,13 +576,13 @@ __global__ void __launch_bounds__(256) l2err_kernel(StageArgs<typename K::T> a, 
 
 // per-block partial cell integrals of every field: |J| * |ref| * phi0 * c[j][0]
 template <class K>
-__global__ void __launch_bounds__(256) totals_kernel(StageArgs<typename K::T> a, double refm,
-                                                      double* partials) {
+__global__ void __launch_bounds__(256) totals_kernel(const __grid_constant__ StageArgs<typename K::T> a, double refm,
+                                                      double* partials, int e_begin, int e_end) {
   __shared__ double red[256 / 32];
-  const int e = blockIdx.x * 256 + threadIdx.x;
+  const int e = e_begin + blockIdx.x * 256 + threadIdx.x;
   for (int j = 0; j < K::M; ++j) {
     double v = 0.0;
-    if (e < a.mesh.E)
+    if (e < e_end)
       v = a.mesh.detjd[e] * refm * a.tab.phi0 * a.C[(size_t)e * K::MNP + j * K::NP];
     v = block_sum<256>(v, red);
     if (threadIdx.x == 0) partials[(size_t)blockIdx.x * K::M + j] = v;

@@ -46,9 +46,18 @@ struct LimArgs {
   const double* geo;    // [E][kLimGeo]
   const double* Dn;     // per degree n: (n+1)^2 block at n(n+1)(2n+1)/6
   const double* Dinv;
-  const TimeCtl* ctl;   // kernels are no-ops once the run is done
+  const TimeCtl* ctl;   // kernels are no-ops once the run is done (nullptr: always run)
+  const TimeCtl* gctl;
+  const int* cell_inst; // ensembles: instance of each cell (-1: padding); finished
+                        // instances are left alone
   int E;
 };
+
+__device__ __forceinline__ bool lim_skip_cell(const LimArgs& a, int e) {
+  if (!a.cell_inst) return false;
+  const int i = a.cell_inst[e];
+  return i < 0 || (a.ctl && a.ctl[i].done);
+}
 
 __device__ __forceinline__ double lim_minmod3(double a, double b, double c, bool& lim) {
   const bool sa = a < 0.0, sb = b < 0.0, sc = c < 0.0;
@@ -236,9 +245,9 @@ __device__ __forceinline__ void lim_descend(const LimArgs& a, int e, int j, cons
 template <class K>
 __global__ void __launch_bounds__(128) limit_kernel(LimArgs a) {
   constexpr int M = K::M, NP = K::NP, P = K::ORDER;
-  if (a.ctl && a.ctl->done) return;
+  if (a.ctl && a.gctl->done) return;
   const int e = blockIdx.x * blockDim.x + threadIdx.x;
-  if (e >= a.E) return;
+  if (e >= a.E || lim_skip_cell(a, e)) return;
   int nb[4];
 #pragma unroll
   for (int d = 0; d < 4; ++d) nb[d] = __ldg(a.nb + 4 * e + d);
@@ -271,10 +280,11 @@ __global__ void __launch_bounds__(128) limit_kernel(LimArgs a) {
 // copy the limited rows of triggered cells back into the state
 template <class K>
 __global__ void __launch_bounds__(256) limit_apply_kernel(LimArgs a) {
-  if (a.ctl && a.ctl->done) return;
+  if (a.ctl && a.gctl->done) return;
   const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   if (i >= (long long)a.E * K::MNP) return;
   const int e = static_cast<int>(i / K::MNP);
+  if (lim_skip_cell(a, e)) return;
   if (a.trig[e]) const_cast<double*>(a.C)[i] = a.L[i];
 }
 

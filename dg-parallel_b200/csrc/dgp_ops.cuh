@@ -38,7 +38,10 @@ template <class K>
 void ops_face(const DeviceBuffers& b, int stage, double time_factor, cudaStream_t st) {
   auto a = stage_args<K>(b, stage, time_factor, 0);
   const int fgrid = (b.F + K::FPB - 1) / K::FPB;
-  face_kernel<K><<<fgrid, K::FACE_BLOCK, 0, st>>>(a);
+  if (b.cell_inst)
+    face_kernel<K, true><<<fgrid, K::FACE_BLOCK, 0, st>>>(a);
+  else
+    face_kernel<K, false><<<fgrid, K::FACE_BLOCK, 0, st>>>(a);
 }
 
 // second face pass of the P0 fallback (a no-op unless a cell was marked)
@@ -46,7 +49,11 @@ template <class K>
 void ops_face_rerun(const DeviceBuffers& b, int stage, double time_factor, cudaStream_t st) {
   auto a = stage_args<K>(b, stage, time_factor, 0);
   const int fgrid = (b.F + K::FPB - 1) / K::FPB;
-  face_rerun_kernel<K><<<fgrid < 296 ? fgrid : 296, K::FACE_BLOCK, 0, st>>>(a);
+  const int g = fgrid < 296 ? fgrid : 296;
+  if (b.cell_inst)
+    face_rerun_kernel<K, true><<<g, K::FACE_BLOCK, 0, st>>>(a);
+  else
+    face_rerun_kernel<K, false><<<g, K::FACE_BLOCK, 0, st>>>(a);
 }
 
 template <class K>
@@ -76,6 +83,8 @@ void ops_limit(const DeviceBuffers& b, int check_done, cudaStream_t st) {
     a.Dn = b.limD;
     a.Dinv = b.limDinv;
     a.ctl = check_done ? b.ctl : nullptr;
+    a.gctl = b.gctl;
+    a.cell_inst = b.cell_inst;
     a.E = b.E;
     limit_kernel<K><<<(b.E + 127) / 128, 128, 0, st>>>(a);
     const long long n = static_cast<long long>(b.E) * K::MNP;
@@ -86,7 +95,9 @@ void ops_limit(const DeviceBuffers& b, int check_done, cudaStream_t st) {
 template <class K>
 void ops_cfl(const DeviceBuffers& b, cudaStream_t st) {
   StageArgs<typename K::T> a = make_args<typename K::T>(b);
-  cfl_kernel<K><<<(b.E + 255) / 256, 256, 0, st>>>(a);
+  // ensembles: one block per instance-pure tile
+  const int grid = b.cell_inst ? ops_grid_elem<K>(b.E) : (b.E + 255) / 256;
+  cfl_kernel<K><<<grid, 256, 0, st>>>(a);
 }
 
 template <class K>
@@ -98,15 +109,16 @@ void ops_project(const DeviceBuffers& b, double t, cudaStream_t st) {
 }
 
 template <class K>
-void ops_l2err(const DeviceBuffers& b, double t, int field, cudaStream_t st) {
+void ops_l2err(const DeviceBuffers& b, double t, int field, int e_begin, int e_end, const LawParams* lp,
+               cudaStream_t st) {
   StageArgs<typename K::T> a = make_args<typename K::T>(b);
-  l2err_kernel<K><<<(b.E + 255) / 256, 256, 0, st>>>(a, t, field, b.partials);
+  l2err_kernel<K><<<(e_end - e_begin + 255) / 256, 256, 0, st>>>(a, t, field, b.partials, e_begin, e_end, lp);
 }
 
 template <class K>
-void ops_totals(const DeviceBuffers& b, double refm, cudaStream_t st) {
+void ops_totals(const DeviceBuffers& b, double refm, int e_begin, int e_end, cudaStream_t st) {
   StageArgs<typename K::T> a = make_args<typename K::T>(b);
-  totals_kernel<K><<<(b.E + 255) / 256, 256, 0, st>>>(a, refm, b.partials);
+  totals_kernel<K><<<(e_end - e_begin + 255) / 256, 256, 0, st>>>(a, refm, b.partials, e_begin, e_end);
 }
 
 template <class K>

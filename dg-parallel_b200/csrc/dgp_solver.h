@@ -65,6 +65,13 @@ struct DeviceBuffers {
   double* lgeo = nullptr;         // [E][10] limiter geometry
   double* limD = nullptr;         // derivative tables per degree
   double* limDinv = nullptr;
+  // ensembles (nullptr / 0 for a single solver; then gctl == ctl)
+  TimeCtl* gctl = nullptr;
+  int* cell_inst = nullptr;
+  int* inst_end = nullptr;
+  int* tile_first = nullptr;
+  LawParams* laws = nullptr;
+  int ninst = 0;
 };
 
 template <typename T>
@@ -112,6 +119,12 @@ inline StageArgs<T> make_args(const DeviceBuffers& b) {
   a.status = b.status;
   a.partials = b.partials;
   a.bad = b.bad;
+  a.gctl = b.gctl ? b.gctl : b.ctl;
+  a.cell_inst = b.cell_inst;
+  a.inst_end = b.inst_end;
+  a.tile_first = b.tile_first;
+  a.laws = b.laws;
+  a.ninst = b.ninst;
   a.order = b.order;
   return a;
 }
@@ -132,8 +145,10 @@ struct Ops {
   void (*elem)(const DeviceBuffers&, int stage, int fuse_cfl, cudaStream_t) = nullptr;
   void (*cfl)(const DeviceBuffers&, cudaStream_t) = nullptr;
   void (*project)(const DeviceBuffers&, double t, cudaStream_t) = nullptr;
-  void (*l2err)(const DeviceBuffers&, double t, int field, cudaStream_t) = nullptr;
-  void (*totals)(const DeviceBuffers&, double refm, cudaStream_t) = nullptr;
+  // over cells [e_begin, e_end); lp: field parameters (nullptr: the solver's law)
+  void (*l2err)(const DeviceBuffers&, double t, int field, int e_begin, int e_end, const LawParams* lp,
+                cudaStream_t) = nullptr;
+  void (*totals)(const DeviceBuffers&, double refm, int e_begin, int e_end, cudaStream_t) = nullptr;
   int (*grid_elem)(int E) = nullptr;
   // moment limiter pass (triangles, p >= 1; nullptr elsewhere)
   void (*limit)(const DeviceBuffers&, int check_done, cudaStream_t) = nullptr;

@@ -79,6 +79,16 @@ def lib() -> ctypes.CDLL:
         "dgp_limiter_triggers": ([P, ctypes.POINTER(ctypes.c_uint8)], I),
         "dgp_set_p0_fallback": ([P, I], I),
         "dgp_launches_per_step": ([P, pI], I),
+        "dgp_ensemble_create": ([I, pP, pP, pI, I, I, pP], I),
+        "dgp_ensemble_destroy": ([P], I),
+        "dgp_ensemble_info": ([P, I, pI, pI, pI, pI], I),
+        "dgp_ensemble_project": ([P, D], I),
+        "dgp_ensemble_get_state": ([P, I, pD], I),
+        "dgp_ensemble_set_state": ([P, I, pD], I),
+        "dgp_ensemble_run": ([P, D, D, D, I, pD, pI, pD, pD], I),
+        "dgp_ensemble_totals": ([P, I, pD], I),
+        "dgp_ensemble_l2_error": ([P, I, D, I, pD], I),
+        "dgp_ensemble_launches_per_step": ([P, pI], I),
     }
     for name, (args, res) in sig.items():
         f = getattr(L, name)
@@ -302,3 +312,75 @@ class Solver:
             self.close()
         except Exception:
             pass
+
+
+class Ensemble:
+    """Independent instances (mesh, law, order) run batched on one GPU; states
+    and results are per instance."""
+
+    def __init__(self, meshes, laws, orders, precision: int = FP64, limiter: int = 0):
+        n = len(meshes)
+        assert len(laws) == n and len(orders) == n
+        self.meshes, self.laws = list(meshes), list(laws)
+        mh = (ctypes.c_void_p * n)(*[m.h.value for m in meshes])
+        lh = (ctypes.c_void_p * n)(*[l.h.value for l in laws])
+        od = np.ascontiguousarray(orders, dtype=np.int32)
+        self.h = ctypes.c_void_p()
+        check(lib().dgp_ensemble_create(n, mh, lh, _ip(od), precision, limiter, ctypes.byref(self.h)))
+        self.n = n
+        self.shapes, self.groups = [], []
+        for i in range(n):
+            m, k, e, g = (ctypes.c_int() for _ in range(4))
+            check(lib().dgp_ensemble_info(self.h, i, ctypes.byref(m), ctypes.byref(k), ctypes.byref(e),
+                                          ctypes.byref(g)))
+            self.shapes.append((e.value, m.value, k.value))
+            self.groups.append(g.value)
+
+    def project(self, t: float = 0.0):
+        check(lib().dgp_ensemble_project(self.h, t))
+
+    def get_state(self, i: int) -> np.ndarray:
+        out = np.zeros(self.shapes[i])
+        check(lib().dgp_ensemble_get_state(self.h, i, _dp(out)))
+        return out
+
+    def set_state(self, i: int, c: np.ndarray):
+        c = np.ascontiguousarray(c, dtype=np.float64).reshape(self.shapes[i])
+        check(lib().dgp_ensemble_set_state(self.h, i, _dp(c)))
+
+    def run(self, t0: float, tend: float, cfl: float, max_steps: int = 0):
+        """Returns (final times, steps, per-instance device ms, total device ms)."""
+        t = np.zeros(self.n)
+        steps = np.zeros(self.n, dtype=np.int32)
+        ms = np.zeros(self.n)
+        tot = ctypes.c_double()
+        check(lib().dgp_ensemble_run(self.h, t0, tend, cfl, max_steps, _dp(t), _ip(steps), _dp(ms),
+                                     ctypes.byref(tot)))
+        return t, steps, ms, tot.value
+
+    def totals(self, i: int) -> np.ndarray:
+        out = np.zeros(self.shapes[i][1])
+        check(lib().dgp_ensemble_totals(self.h, i, _dp(out)))
+        return out
+
+    def l2_error(self, i: int, t: float, field: int = 0) -> float:
+        e = ctypes.c_double()
+        check(lib().dgp_ensemble_l2_error(self.h, i, t, field, ctypes.byref(e)))
+        return e.value
+
+    def launches_per_step(self) -> int:
+        n = ctypes.c_int()
+        check(lib().dgp_ensemble_launches_per_step(self.h, ctypes.byref(n)))
+        return n.value
+
+    def close(self):
+        if self.h:
+            lib().dgp_ensemble_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+

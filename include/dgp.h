@@ -64,6 +64,7 @@ extern "C" {
 typedef struct dgp_mesh_s* dgp_mesh;
 typedef struct dgp_law_s* dgp_law;
 typedef struct dgp_solver_s* dgp_solver;
+typedef struct dgp_ensemble_s* dgp_ensemble;
 
 const char* dgp_last_error(void);
 int dgp_version(void);
@@ -161,6 +162,32 @@ int dgp_profile_kernels(dgp_solver s, int iters, float* ms);
  * it before any stream capture.  Returns after the solver's stream is idle. */
 int dgp_rhs_noalloc(dgp_solver s, const double* dev_state, double t, double* dev_rhs);
 
+/* ---- ensembles (no counterpart in DG-Parallel, which runs one DGAnalysis per
+ * process): n independent instances of uneven size, each with its own mesh,
+ * law parameters and order, run batched on one GPU.  Instances with the same
+ * (law, flux, element, order) share one set of kernels over a joined cell and
+ * face index space; each keeps its own CFL step, end time and step count.  A
+ * group's instances must share the law's gamma; field parameters (amplitude,
+ * centre, ...) may differ.  Instance states use the layout of a single solver
+ * on that instance's mesh. */
+int dgp_ensemble_create(int n, const dgp_mesh* meshes, const dgp_law* laws, const int* orders, int precision,
+                        int limiter, dgp_ensemble* out);
+int dgp_ensemble_destroy(dgp_ensemble e);
+/* group: index of the kernel group the instance runs in */
+int dgp_ensemble_info(dgp_ensemble e, int i, int* nfields, int* nmodes, int* ncells, int* group);
+int dgp_ensemble_project(dgp_ensemble e, double t);
+int dgp_ensemble_get_state(dgp_ensemble e, int i, double* host_state);
+int dgp_ensemble_set_state(dgp_ensemble e, int i, const double* host_state);
+/* every instance from t0 to tend (or max_steps steps) at its own CFL step;
+ * per-instance arrays (may be NULL): final time, steps taken, device time from
+ * the common start to the instance's last step (ms); total_ms: the latest of
+ * those.  Device-resident: CUDA graphs of 8 steps per group until all are done. */
+int dgp_ensemble_run(dgp_ensemble e, double t0, double tend, double cfl, int max_steps, double* t_out,
+                     int* steps_out, double* ms_out, double* total_ms);
+/* conserved totals (FP64) and L2 error against the instance's exact field */
+int dgp_ensemble_totals(dgp_ensemble e, int i, double* totals);
+int dgp_ensemble_l2_error(dgp_ensemble e, int i, double t, int field, double* err);
+int dgp_ensemble_launches_per_step(dgp_ensemble e, int* n);
 #ifdef __cplusplus
 }
 #endif
