@@ -44,7 +44,38 @@ void ensure_registry() {
     register_euler2d_llf_ops();
     register_euler3d_ops();
     register_maxwell3d_ops();
+    register_burgers_tile_ops();
+    register_euler2d_roe_tile_ops();
   });
+}
+
+// Autotuner results: the tile shape (threads of the element and face kernels)
+// that measured fastest for a (law, flux, element, order, precision) at a
+// problem size (bucket: floor(log2(cells))).  Consulted when solvers and
+// ensemble groups are created; filled by dgp_autotune / dgp_autotune_ensemble.
+std::mutex g_tune_mutex;
+std::map<std::tuple<int, int, int, int, int, int>, int> g_tune;
+
+int size_bucket(long long cells) {
+  int b = 0;
+  while ((1LL << (b + 1)) <= cells) ++b;
+  return b;
+}
+
+int tuned_block(int law, int flux, int dim, int order, int precision, long long cells) {
+  std::lock_guard<std::mutex> lock(g_tune_mutex);
+  auto it = g_tune.find(std::make_tuple(law, flux, dim, order, precision, size_bucket(cells)));
+  return it == g_tune.end() ? kDefaultBlock : it->second;
+}
+
+void set_tuned_block(int law, int flux, int dim, int order, int precision, long long cells, int block) {
+  std::lock_guard<std::mutex> lock(g_tune_mutex);
+  g_tune[std::make_tuple(law, flux, dim, order, precision, size_bucket(cells))] = block;
+}
+
+bool has_block(int law, int flux, int dim, int order, int precision, int block) {
+  ensure_registry();
+  return ops_registry().count(OpsKey(law, flux, dim, order, precision, block)) != 0;
 }
 
 // gather cells by `perm` and convert the arithmetic type
@@ -411,9 +442,10 @@ static int build_solver(dgp_solver s, const std::vector<LawParams>& lps, int fie
 }
 
 // common part of solver and ensemble-group creation: kernels, tables, stream
-static int solver_begin(dgp_solver s, int law, int flux, int dim, int order, int precision, int limiter) {
+static int solver_begin(dgp_solver s, int law, int flux, int dim, int order, int precision, int limiter,
+                        int block) {
   ensure_registry();
-  auto it = ops_registry().find(OpsKey(law, flux, dim, order, precision));
+  auto it = ops_registry().find(OpsKey(law, flux, dim, order, precision, block));
   if (it == ops_registry().end())
     return fail(DGP_ERR_UNSUPPORTED, "no kernels for this law/flux/element/order/precision");
   int ndev = 0;
@@ -548,7 +580,8 @@ int dgp_solver_create(dgp_mesh mh, dgp_law law, int order, int precision, int li
   if ((law->kind == DGP_LAW_EULER3D || law->kind == DGP_LAW_MAXWELL3D) && m.dim != 3)
     return fail(DGP_ERR_UNSUPPORTED, "3D law on a 2D mesh");
   auto s = new dgp_solver_s;
-  if (int rc = solver_begin(s, law->kind, law->flux, m.dim, order, precision, limiter)) {
+  const int block = tuned_block(law->kind, law->flux, m.dim, order, precision, m.E);
+  if (int rc = solver_begin(s, law->kind, law->flux, m.dim, order, precision, limiter, block)) {
     delete s;
     return rc;
   }
@@ -939,8 +972,12 @@ int dgp_ensemble_create(int n, const dgp_mesh* meshes, const dgp_law* laws, cons
         return fail(DGP_ERR_INVALID, "instances of one law/order group must share gamma");
       }
     auto s = new dgp_solver_s;
+    long long cells = 0;
+    for (int i : members) cells += meshes[i]->m.E;
+    const int block = tuned_block(std::get<0>(kv.first), std::get<1>(kv.first), std::get<2>(kv.first),
+                                  std::get<3>(kv.first), precision, cells);
     if (int rc = solver_begin(s, std::get<0>(kv.first), std::get<1>(kv.first), std::get<2>(kv.first),
-                              std::get<3>(kv.first), precision, limiter)) {
+                              std::get<3>(kv.first), precision, limiter, block)) {
       delete s;
       delete e;
       return rc;
@@ -1175,6 +1212,138 @@ int dgp_ensemble_launches_per_step(dgp_ensemble e, int* n) {
   }
   *n = tot;
   return DGP_OK;
+}
+
+
+// ---------------------------------------------------------------------------
+// Autotuner: times `iters` SSP-RK3 steps (after 2 warm-up steps) of every
+// tile shape built for the configuration, on the caller's mesh(es), with CUDA
+// events on the solver's stream, and records the fastest for later creations.
+
+// mean ms per step of a built solver (single or ensemble group)
+static int time_steps(dgp_solver s, int iters, float* ms) {
+  DGP_CUDA(cudaSetDevice(s->device));
+  // controls: t = 0, no end, the CFL step of the current state
+  const int nctl = s->b.ninst ? s->b.ninst + 1 : 1;
+  std::vector<TimeCtl> c(nctl);
+  for (auto& x : c) {
+    x = TimeCtl{};
+    x.cfl = 0.1;
+    x.dtmin_bits = 0x7FF0000000000000ull;
+  }
+  DGP_CUDA(cudaMemcpy(s->b.ctl, c.data(), nctl * sizeof(TimeCtl), cudaMemcpyHostToDevice));
+  s->ops.cfl(s->b, s->stream);
+  launch_step(s, 0);
+  launch_step(s, 0);
+  cudaEvent_t e0, e1;
+  DGP_CUDA(cudaEventCreate(&e0));
+  DGP_CUDA(cudaEventCreate(&e1));
+  DGP_CUDA(cudaEventRecord(e0, s->stream));
+  for (int k = 0; k < iters; ++k) launch_step(s, 0);
+  DGP_CUDA(cudaEventRecord(e1, s->stream));
+  DGP_CUDA(cudaGetLastError());
+  DGP_CUDA(cudaEventSynchronize(e1));
+  float t = 0;
+  DGP_CUDA(cudaEventElapsedTime(&t, e0, e1));
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  *ms = t / iters;
+  return DGP_OK;
+}
+
+static const int kTileBlocks[3] = {64, 128, 256};
+
+int dgp_autotune(dgp_mesh mh, dgp_law law, int order, int precision, int limiter, int iters, int* best_block,
+                 float* ms_per_step) {
+  if (!mh || !law || iters <= 0) return fail(DGP_ERR_INVALID, "bad argument");
+  const HostMesh& m = mh->m;
+  int best = 0;
+  float best_ms = 0;
+  for (int v = 0; v < 3; ++v) {
+    if (ms_per_step) ms_per_step[v] = -1.0f;
+    const int block = kTileBlocks[v];
+    if (!has_block(law->kind, law->flux, m.dim, order, precision, block)) continue;
+    set_tuned_block(law->kind, law->flux, m.dim, order, precision, m.E, block);
+    dgp_solver s = nullptr;
+    if (int rc = dgp_solver_create(mh, law, order, precision, limiter, &s)) return rc;
+    float ms = 0;
+    int rc = time_steps(s, iters, &ms);
+    dgp_solver_destroy(s);
+    if (rc) return rc;
+    if (ms_per_step) ms_per_step[v] = ms;
+    if (!best || ms < best_ms) {
+      best = block;
+      best_ms = ms;
+    }
+  }
+  if (!best) return fail(DGP_ERR_UNSUPPORTED, "no kernels for this law/flux/element/order/precision");
+  set_tuned_block(law->kind, law->flux, m.dim, order, precision, m.E, best);
+  if (best_block) *best_block = best;
+  return DGP_OK;
+}
+
+int dgp_autotune_ensemble(int n, const dgp_mesh* meshes, const dgp_law* laws, const int* orders, int precision,
+                          int limiter, int iters) {
+  if (n <= 0 || !meshes || !laws || !orders || iters <= 0) return fail(DGP_ERR_INVALID, "bad argument");
+  // one candidate ensemble per group key, timed group by group
+  std::map<std::tuple<int, int, int, int>, std::vector<int>> groups;
+  for (int i = 0; i < n; ++i) {
+    if (!meshes[i] || !laws[i]) return fail(DGP_ERR_INVALID, "null mesh or law");
+    groups[std::make_tuple(laws[i]->kind, laws[i]->flux, meshes[i]->m.dim, orders[i])].push_back(i);
+  }
+  for (auto& kv : groups) {
+    const int law = std::get<0>(kv.first), flux = std::get<1>(kv.first), dim = std::get<2>(kv.first),
+              order = std::get<3>(kv.first);
+    std::vector<dgp_mesh> ms;
+    std::vector<dgp_law> ls;
+    std::vector<int> os;
+    long long cells = 0;
+    for (int i : kv.second) {
+      ms.push_back(meshes[i]);
+      ls.push_back(laws[i]);
+      os.push_back(order);
+      cells += meshes[i]->m.E;
+    }
+    int best = 0;
+    float best_ms = 0;
+    for (int block : kTileBlocks) {
+      if (!has_block(law, flux, dim, order, precision, block)) continue;
+      set_tuned_block(law, flux, dim, order, precision, cells, block);
+      dgp_ensemble e = nullptr;
+      if (int rc = dgp_ensemble_create(static_cast<int>(ms.size()), ms.data(), ls.data(), os.data(), precision,
+                                       limiter, &e))
+        return rc;
+      float t = 0;
+      int rc = time_steps(e->groups[0], iters, &t);
+      dgp_ensemble_destroy(e);
+      if (rc) return rc;
+      if (!best || t < best_ms) {
+        best = block;
+        best_ms = t;
+      }
+    }
+    if (best) set_tuned_block(law, flux, dim, order, precision, cells, best);
+  }
+  return DGP_OK;
+}
+
+int dgp_tune_set(int law, int flux, int dim, int order, int precision, int cells, int block) {
+  if (!has_block(law, flux, dim, order, precision, block))
+    return fail(DGP_ERR_UNSUPPORTED, "no kernels with this tile shape for this configuration");
+  set_tuned_block(law, flux, dim, order, precision, cells, block);
+  return DGP_OK;
+}
+
+int dgp_solver_block(dgp_solver s, int* block, int* cells_per_tile) {
+  if (!s) return fail(DGP_ERR_INVALID, "null solver");
+  if (block) *block = s->ops.elem_block;
+  if (cells_per_tile) *cells_per_tile = s->ops.TE;
+  return DGP_OK;
+}
+
+int dgp_ensemble_group_block(dgp_ensemble e, int group, int* block, int* cells_per_tile) {
+  if (!e || group < 0 || group >= static_cast<int>(e->groups.size())) return fail(DGP_ERR_INVALID, "bad group");
+  return dgp_solver_block(e->groups[group], block, cells_per_tile);
 }
 
 }  // extern "C"

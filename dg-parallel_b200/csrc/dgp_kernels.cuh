@@ -29,7 +29,10 @@ constexpr int tri_vol_points(int p) { return p == 0 ? 1 : p == 1 ? 3 : p == 2 ? 
 constexpr int tet_vol_points(int p) { return p == 0 ? 1 : p == 1 ? 4 : p == 2 ? 14 : 24; }
 constexpr int tet_face_points(int p) { return p == 0 ? 1 : p == 1 ? 4 : p == 2 ? 7 : 13; }
 
-template <int LAW_, int FLUX_, int DIM_, int ORDER_, typename T_>
+// BLOCK_: threads of the element and face kernels; it sets the cells per
+// element-kernel tile (TE) and the faces per face-kernel CTA, the shapes the
+// autotuner chooses among (64, 128, 256).
+template <int LAW_, int FLUX_, int DIM_, int ORDER_, typename T_, int BLOCK_ = 128>
 struct Cfg {
   using T = T_;
   static constexpr int LAW = LAW_, FLUX = FLUX_, DIM = DIM_, ORDER = ORDER_;
@@ -45,11 +48,13 @@ struct Cfg {
   static constexpr int KV = NQ * DIM;    // volume contraction length
   // element kernel: one thread per (cell, field) row of the tile, all modes of
   // the row in registers; TE cells per CTA, capped by a shared-memory budget
-  static constexpr int BLOCK = 128;
+  static constexpr int BLOCK = BLOCK_;
   static constexpr int NV = DIM == 2 ? 4 : 1;  // states of the CFL (mean + vertices)
   static constexpr int LDK = KV | 1;           // row stride of G (odd: conflict-free)
-  static constexpr int CELL_BYTES = (int)sizeof(T) * (MNP + M * LDK) + 8 * (NV + DIM * DIM + 1);
-  static constexpr int TE_SMEM = (64 * 1024) / CELL_BYTES;
+  static constexpr int CELL_BYTES = 8 * MNP + (int)sizeof(T) * M * LDK + 8 * (NV + DIM * DIM + 1);
+  // shared-memory budget of a tile: 512 bytes per thread, at most 100 KB
+  static constexpr int SMEM_BUDGET = BLOCK * 512 < 100 * 1024 ? BLOCK * 512 : 100 * 1024;
+  static constexpr int TE_SMEM = SMEM_BUDGET / CELL_BYTES;
   static constexpr int TE_ROWS = BLOCK / M;
   static constexpr int TE = TE_SMEM < TE_ROWS ? (TE_SMEM < 1 ? 1 : TE_SMEM) : TE_ROWS;
   static constexpr int ROWS = TE * M;
@@ -57,7 +62,7 @@ struct Cfg {
   // face slots live tile-transposed, [tile][face point][row], so that the
   // element kernel reads them row-coalesced: slot(e, s, j) =
   // ((e / TE) * NS + s) * ROWS + (e % TE) * M + j
-  static constexpr int FACE_BLOCK = 128;
+  static constexpr int FACE_BLOCK = BLOCK;
   static constexpr int FPB = FACE_BLOCK / NQF;  // faces per face-kernel CTA
   static constexpr int LDM = MNP | 1;           // staged coefficient row stride
 };

@@ -130,6 +130,7 @@ Ops make_ops() {
   o.NQF = K::NQF;
   o.TE = K::TE;
   o.elem_block = K::BLOCK;
+  o.fpb = K::FPB;
   o.elem_smem = elem_kernel_smem<K>();
   o.tsize = sizeof(typename K::T);
   o.blob_elems = ElemSmem<K>::blob_elems;
@@ -148,12 +149,19 @@ Ops make_ops() {
   return o;
 }
 
-template <int LAW, int FLUX, int DIM, int ORDER>
+template <int LAW, int FLUX, int DIM, int ORDER, int BLOCK = kDefaultBlock>
 void add_ops() {
-  ops_registry()[OpsKey(LAW, FLUX, DIM, ORDER, DGP_PRECISION_FP64)] =
-      make_ops<Cfg<LAW, FLUX, DIM, ORDER, double>>();
-  ops_registry()[OpsKey(LAW, FLUX, DIM, ORDER, DGP_PRECISION_MIXED)] =
-      make_ops<Cfg<LAW, FLUX, DIM, ORDER, float>>();
+  ops_registry()[OpsKey(LAW, FLUX, DIM, ORDER, DGP_PRECISION_FP64, BLOCK)] =
+      make_ops<Cfg<LAW, FLUX, DIM, ORDER, double, BLOCK>>();
+  ops_registry()[OpsKey(LAW, FLUX, DIM, ORDER, DGP_PRECISION_MIXED, BLOCK)] =
+      make_ops<Cfg<LAW, FLUX, DIM, ORDER, float, BLOCK>>();
+}
+
+// the other tile shapes the autotuner chooses among
+template <int LAW, int FLUX, int DIM, int ORDER>
+void add_tile_ops() {
+  add_ops<LAW, FLUX, DIM, ORDER, 64>();
+  add_ops<LAW, FLUX, DIM, ORDER, 256>();
 }
 
 }  // namespace dgp

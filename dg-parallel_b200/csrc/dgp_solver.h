@@ -132,6 +132,7 @@ inline StageArgs<T> make_args(const DeviceBuffers& b) {
 // Kernel set of one instantiation.
 struct Ops {
   int M = 0, NP = 0, NQ = 0, NQF = 0, TE = 0, elem_block = 0, precision = 0;
+  int fpb = 0;  // faces per face-kernel CTA
   size_t elem_smem = 0;
   size_t tsize = 8;
   size_t blob_elems = 0;
@@ -154,7 +155,9 @@ struct Ops {
   void (*limit)(const DeviceBuffers&, int check_done, cudaStream_t) = nullptr;
 };
 
-using OpsKey = std::tuple<int, int, int, int, int>;  // law, flux, dim, order, precision
+// law, flux, dim, order, precision, block (tile variant: 64, 128 or 256 threads)
+using OpsKey = std::tuple<int, int, int, int, int, int>;
+constexpr int kDefaultBlock = 128;
 std::map<OpsKey, Ops>& ops_registry();
 void register_scalar_ops();
 void register_burgers_ops();
@@ -163,6 +166,8 @@ void register_euler2d_roe_ops();
 void register_euler2d_llf_ops();
 void register_euler3d_ops();
 void register_maxwell3d_ops();
+void register_burgers_tile_ops();
+void register_euler2d_roe_tile_ops();
 
 template <class K>
 Ops make_ops();

@@ -89,6 +89,11 @@ def lib() -> ctypes.CDLL:
         "dgp_ensemble_totals": ([P, I, pD], I),
         "dgp_ensemble_l2_error": ([P, I, D, I, pD], I),
         "dgp_ensemble_launches_per_step": ([P, pI], I),
+        "dgp_autotune": ([P, P, I, I, I, I, pI, ctypes.POINTER(ctypes.c_float)], I),
+        "dgp_autotune_ensemble": ([I, pP, pP, pI, I, I, I], I),
+        "dgp_tune_set": ([I, I, I, I, I, I, I], I),
+        "dgp_solver_block": ([P, pI, pI], I),
+        "dgp_ensemble_group_block": ([P, I, pI, pI], I),
     }
     for name, (args, res) in sig.items():
         f = getattr(L, name)
@@ -299,6 +304,12 @@ class Solver:
         check(lib().dgp_launches_per_step(self.h, ctypes.byref(n)))
         return n.value
 
+    def block(self) -> tuple[int, int]:
+        """(threads, cells per element-kernel tile) of the tile shape in use."""
+        b, te = ctypes.c_int(), ctypes.c_int()
+        check(lib().dgp_solver_block(self.h, ctypes.byref(b), ctypes.byref(te)))
+        return b.value, te.value
+
     def synchronize(self):
         check(lib().dgp_synchronize(self.h))
 
@@ -312,6 +323,30 @@ class Solver:
             self.close()
         except Exception:
             pass
+
+
+def autotune(mesh: "Mesh", law: "Law", order: int, precision: int = FP64, limiter: int = 0,
+             iters: int = 10):
+    """Time the tile shapes (64/128/256 threads) on this mesh; the fastest is
+    used by solvers created afterwards for the same configuration and size.
+    Returns (best block, ms per step of each candidate, -1 where not built)."""
+    best = ctypes.c_int()
+    ms = (ctypes.c_float * 3)()
+    check(lib().dgp_autotune(mesh.h, law.h, order, precision, limiter, iters, ctypes.byref(best), ms))
+    return best.value, [float(x) for x in ms]
+
+
+def tune_set(law: int, flux: int, dim: int, order: int, precision: int, cells: int, block: int):
+    """Record a tile shape by hand for meshes of `cells` cells (same size bucket)."""
+    check(lib().dgp_tune_set(law, flux, dim, order, precision, cells, block))
+
+
+def autotune_ensemble(meshes, laws, orders, precision: int = FP64, limiter: int = 0, iters: int = 5):
+    n = len(meshes)
+    mh = (ctypes.c_void_p * n)(*[m.h.value for m in meshes])
+    lh = (ctypes.c_void_p * n)(*[l.h.value for l in laws])
+    od = np.ascontiguousarray(orders, dtype=np.int32)
+    check(lib().dgp_autotune_ensemble(n, mh, lh, _ip(od), precision, limiter, iters))
 
 
 class Ensemble:
@@ -372,6 +407,12 @@ class Ensemble:
         n = ctypes.c_int()
         check(lib().dgp_ensemble_launches_per_step(self.h, ctypes.byref(n)))
         return n.value
+
+    def group_block(self, g: int) -> tuple[int, int]:
+        """(threads, cells per element-kernel tile) of kernel group g."""
+        b, te = ctypes.c_int(), ctypes.c_int()
+        check(lib().dgp_ensemble_group_block(self.h, g, ctypes.byref(b), ctypes.byref(te)))
+        return b.value, te.value
 
     def close(self):
         if self.h:

@@ -188,6 +188,23 @@ int dgp_ensemble_run(dgp_ensemble e, double t0, double tend, double cfl, int max
 int dgp_ensemble_totals(dgp_ensemble e, int i, double* totals);
 int dgp_ensemble_l2_error(dgp_ensemble e, int i, double t, int field, double* err);
 int dgp_ensemble_launches_per_step(dgp_ensemble e, int* n);
+/* ---- autotuner: the tile shape (threads of the element and face kernels,
+ * which sets the cells per element-kernel tile and the faces per face-kernel
+ * CTA; 64, 128 or 256 where built) that runs fastest for a configuration at a
+ * problem size.  Each candidate is timed over `iters` SSP-RK3 steps with CUDA
+ * events; the winner is recorded in a process-wide table keyed by (law, flux,
+ * element, order, precision, floor(log2 cells)) that dgp_solver_create and
+ * dgp_ensemble_create consult (128 threads when nothing is recorded).
+ * ms_per_step[3] (may be NULL) gets each candidate's time, -1 where not built. */
+int dgp_autotune(dgp_mesh m, dgp_law law, int order, int precision, int limiter, int iters, int* best_block,
+                 float* ms_per_step);
+/* the same for every (law, flux, element, order) group of an ensemble */
+int dgp_autotune_ensemble(int n, const dgp_mesh* meshes, const dgp_law* laws, const int* orders, int precision,
+                          int limiter, int iters);
+/* records a tile shape by hand (as the autotuner would) for meshes of `cells` cells */
+int dgp_tune_set(int law, int flux, int dim, int order, int precision, int cells, int block);
+int dgp_solver_block(dgp_solver s, int* block, int* cells_per_tile);
+int dgp_ensemble_group_block(dgp_ensemble e, int group, int* block, int* cells_per_tile);
 #ifdef __cplusplus
 }
 #endif

@@ -95,3 +95,44 @@ def test_ensemble_mixed_form(tmp_path):
         assert rel(e32.get_state(i), e64.get_state(i)) < 1e-3
         tot64, tot32 = e64.totals(i), e32.totals(i)
         assert abs(tot32[0] - tot64[0]) < 1e-4 * max(1.0, abs(tot64[0]))
+
+
+def test_autotune_picks_a_built_shape(tmp_path):
+    m = meshgen.tri_square(24, 24, 0.0, 10.0, 0.0, 10.0, jitter=0.15, seed=2)
+    p = str(tmp_path / "vortex24.msh")
+    meshgen.write_msh_v1(m, p)
+    from cases import VORTEX
+    mesh = dgp.Mesh.from_msh(p)
+    law = dgp.Law(dgp.LAW_EULER2D, dgp.FLUX_ROE, dgp.FIELD_VORTEX, VORTEX)
+    best, ms = dgp.autotune(mesh, law, 3, dgp.FP64, 0, iters=3)
+    assert best in (64, 128, 256) and all(x > 0 for x in ms)
+    s = dgp.Solver(mesh, law, 3)
+    assert s.block()[0] == best
+
+
+@pytest.mark.parametrize("order", [1, 4])
+def test_tile_shapes_give_identical_states(tmp_path, order):
+    # every cell sees the same arithmetic whatever the tile: states agree exactly
+    m = meshgen.tri_square(20, 20, 0.0, 1.0, 0.0, 1.0, jitter=0.15, seed=3)
+    p = str(tmp_path / "b20.msh")
+    meshgen.write_msh_v1(m, p)
+    law = dgp.Law(dgp.LAW_BURGERS2D, dgp.FLUX_LLF, dgp.FIELD_SINE, params(amplitude=1.0))
+    out = {}
+    for block in (64, 128, 256):
+        dgp.tune_set(dgp.LAW_BURGERS2D, dgp.FLUX_LLF, 2, order, dgp.FP64, 800, block)
+        s = dgp.Solver(dgp.Mesh.from_msh(p), law, order, dgp.FP64, dgp.LIMITER_MOMENT)
+        assert s.block()[0] == block
+        s.project(0.0)
+        s.run(0.0, 0.12, 0.1)
+        out[block] = s.get_state()
+    dgp.tune_set(dgp.LAW_BURGERS2D, dgp.FLUX_LLF, 2, order, dgp.FP64, 800, 128)
+    assert np.array_equal(out[64], out[128]) and np.array_equal(out[256], out[128])
+
+
+def test_autotune_ensemble_groups(tmp_path):
+    paths, laws, orders, prms = _instances(tmp_path)
+    meshes = [dgp.Mesh.from_msh(p) for p in paths]
+    dgp.autotune_ensemble(meshes, laws, orders, dgp.FP64, dgp.LIMITER_MOMENT, iters=2)
+    ens = dgp.Ensemble(meshes, laws, orders, dgp.FP64, dgp.LIMITER_MOMENT)
+    for g in set(ens.groups):
+        assert ens.group_block(g)[0] in (64, 128, 256)
