@@ -175,6 +175,8 @@ def main():
                     help="skip the untimed runs to t = 2 that state the density L2 errors")
     ap.add_argument("--ensemble", action="store_true",
                     help="only the batched-ensemble measurement (96 Burgers instances to t = 0.5, ~2 min)")
+    ap.add_argument("--adjoint", action="store_true",
+                    help="only the discrete-adjoint measurement (Euler vortex 128x128x2 P2, 400 steps)")
     ap.add_argument("--profile-case", choices=["fp64", "mixed"], default=None,
                     help="only set up the workload and run --warmup + --steps steps (for ncu)")
     args = ap.parse_args()
@@ -184,6 +186,11 @@ def main():
         return run_reference_arm(args)
     if args.profile_case:
         return profile_case(args)
+    if args.adjoint:
+        import torch
+        torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+        print(json.dumps({"adjoint": adjoint_bench()}))
+        return 0
     if args.ensemble:
         import torch
         torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
@@ -422,6 +429,89 @@ def ensemble_bench(n=96, seed=6, tend=0.5):
                    "t_end": tend, "cfl": 0.1, "seed": seed},
     }
     ens.close()
+    return out
+
+
+def adjoint_bench(n=128, order=2, nsteps=400, every=20, nrec=64, ndir=16, eps=1e-3):
+    """Discrete adjoint on the Euler vortex: 128x128x2 jittered triangles on
+    [0,10]^2, P2, Roe flux, nsteps SSP-RK3 steps of a fixed dt (half the CFL
+    0.1 step of the initial state), checkpoint every `every` steps.
+    J = sum over nrec seeded uniform receivers of (rho(x_r, T) - rho_obs)^2 with
+    rho_obs from a forward run with vortex strength 5.5.  The gradient with
+    respect to every initial coefficient is computed in the mixed form (FP32
+    right-hand side and adjoint arithmetic) and in FP64, and checked by central
+    differences (eps along ndir seeded Gaussian directions) of the FP64 forward
+    map.  Times are CUDA-event times on the solver's stream."""
+    import numpy as np
+    import torch
+    import dgp
+    from dgp import meshgen
+    m = meshgen.tri_square(n, n, 0.0, 10.0, 0.0, 10.0, jitter=0.15, seed=2)
+    mesh = dgp.Mesh.from_arrays(2, m.vertices, m.cells, m.domain_tag, m.bfaces, m.btags)
+    prm = vortex_params()
+    prm_obs = prm.copy()
+    prm_obs[8] = 5.5
+    pts = np.random.default_rng(4).uniform(0.5, 9.5, size=(nrec, 2))
+    so = dgp.Solver(mesh, dgp.Law(dgp.LAW_EULER2D, dgp.FLUX_ROE, dgp.FIELD_VORTEX, prm_obs), order, dgp.FP64)
+    so.project(0.0)
+    dt = 0.5 * so.cfl_dt(0.1)
+    so.set_receivers(pts, np.zeros(nrec))
+    so.forward_checkpointed(0.0, dt, nsteps, every)
+    obs, _ = so.receiver_values()
+    so.close()
+    law = dgp.Law(dgp.LAW_EULER2D, dgp.FLUX_ROE, dgp.FIELD_VORTEX, prm)
+    out = {"workload": f"euler2d vortex {n}x{n}x2 P{order} roe, {nsteps} steps, checkpoint every {every}",
+           "cells": 2 * n * n, "receivers": nrec, "dt": dt}
+    grads = {}
+    for name, prec in (("fp64", dgp.FP64), ("mixed", dgp.MIXED)):
+        s = dgp.Solver(mesh, law, order, prec)
+        s.project(0.0)
+        s.set_receivers(pts, obs)
+        u0 = s.get_state()
+        stream = torch.cuda.ExternalStream(s.stream())
+
+        def timed(fn):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            torch.cuda.synchronize()
+            e0.record(stream)
+            r = fn()
+            e1.record(stream)
+            e1.synchronize()
+            return r, e0.elapsed_time(e1)
+
+        # plain forward solve: the same nsteps fixed-dt steps, no checkpoints
+        s.forward_checkpointed(0.0, dt, 4, 4)  # warm-up
+        s.set_state(u0)
+        _, t_plain = timed(lambda: s.forward_checkpointed(0.0, dt, nsteps, nsteps))
+        s.set_state(u0)
+        J, t_fwd = timed(lambda: s.forward_checkpointed(0.0, dt, nsteps, every))
+        g, t_bwd = timed(lambda: s.backward())
+        grads[name] = g
+        out[name] = {"J": J, "forward_ms": t_plain, "forward_checkpointed_ms": t_fwd, "backward_ms": t_bwd,
+                     "gradient_over_forward": (t_fwd + t_bwd) / t_plain, "backward_over_forward": t_bwd / t_plain}
+        s.close()
+    # central differences of the FP64 forward map
+    s = dgp.Solver(mesh, law, order, dgp.FP64)
+    s.project(0.0)
+    s.set_receivers(pts, obs)
+    u0 = s.get_state()
+    rng = np.random.default_rng(5)
+    err64, err32 = [], []
+    for _ in range(ndir):
+        d = rng.standard_normal(u0.shape)
+        s.set_state(u0 + eps * d)
+        jp = s.forward_checkpointed(0.0, dt, nsteps, nsteps)
+        s.set_state(u0 - eps * d)
+        jm = s.forward_checkpointed(0.0, dt, nsteps, nsteps)
+        fd = (jp - jm) / (2 * eps)
+        for g, lst in ((grads["fp64"], err64), (grads["mixed"], err32)):
+            ad = float(np.sum(g * d))
+            lst.append(abs(fd - ad) / max(abs(fd), abs(ad)))
+    s.close()
+    out["fd_check"] = {"eps": eps, "directions": ndir, "max_rel_err_fp64": max(err64),
+                       "max_rel_err_mixed": max(err32),
+                       "mixed_vs_fp64_gradient_rel": float(np.abs(grads["mixed"] - grads["fp64"]).max()
+                                                           / np.abs(grads["fp64"]).max())}
     return out
 
 

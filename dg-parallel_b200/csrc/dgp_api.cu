@@ -16,6 +16,7 @@
 #include "../../include/dgp.h"
 #include "dgp_host.h"
 #include "dgp_handles.h"
+#include "dgp_adjoint.cuh"
 #include "dgp_limiter.cuh"
 #include "dgp_solver.h"
 
@@ -92,6 +93,19 @@ __global__ void mark_clock(TimeCtl* c) {
   unsigned long long t;
   asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
   c->t_mark_ns = t;
+}
+
+// controls of one adjoint segment: time and step of the forward recompute,
+// the segment's start time for the adjoint kernels (values travel as kernel
+// parameters, so consecutive segments queued without a host sync do not race)
+__global__ void set_segment_time(TimeCtl* c, double t, double dt, double* t_seg) {
+  c->t = t;
+  c->dt = dt;
+  c->tend = 0.0;
+  c->max_steps = 0;
+  c->done = 0;
+  c->blocks_done = 0;
+  *t_seg = t;
 }
 
 uint64_t spread2(uint32_t x) {
@@ -1344,6 +1358,230 @@ int dgp_solver_block(dgp_solver s, int* block, int* cells_per_tile) {
 int dgp_ensemble_group_block(dgp_ensemble e, int group, int* block, int* cells_per_tile) {
   if (!e || group < 0 || group >= static_cast<int>(e->groups.size())) return fail(DGP_ERR_INVALID, "bad group");
   return dgp_solver_block(e->groups[group], block, cells_per_tile);
+}
+
+
+// ---------------------------------------------------------------------------
+// Discrete adjoint (no counterpart in DG-Parallel): gradient of an objective of
+// the final state with respect to the initial coefficients, through the
+// SSP-RK3 steps with a fixed time step, by checkpoint and recompute.
+
+static int adj_buffer(dgp_solver s, double** p, size_t* have, size_t states) {
+  if (*have >= states && *p) return DGP_OK;
+  if (*p) {
+    cudaFree(*p);
+    s->allocs.erase(std::remove(s->allocs.begin(), s->allocs.end(), static_cast<void*>(*p)), s->allocs.end());
+    *p = nullptr;
+  }
+  if (int rc = s->alloc(p, states * s->state_count() + 32)) return rc;
+  *have = states;
+  return DGP_OK;
+}
+
+int dgp_adjoint_set_receivers(dgp_solver s, int n, const double* points, const double* observed) {
+  if (!s || n <= 0 || !points || !observed) return fail(DGP_ERR_INVALID, "bad argument");
+  if (s->b.ninst) return fail(DGP_ERR_UNSUPPORTED, "receivers are set on a single solver");
+  DGP_CUDA(cudaSetDevice(s->device));
+  const HostMesh& m = s->meshes[0];
+  const int dim = m.dim, NP = s->b.NP;
+  std::vector<int> cell(n, -1);
+  std::vector<double> phi(static_cast<size_t>(n) * NP);
+  for (int r = 0; r < n; ++r) {
+    const double* x = points + static_cast<size_t>(r) * dim;
+    // the first cell whose barycentric coordinates are all >= -1e-12
+    for (int e = 0; e < m.E && cell[r] < 0; ++e) {
+      double X0[3], J[9], Ji[9];
+      cell_frame(m, e, X0, J);
+      invert3(J, Ji);
+      double xi[3] = {0, 0, 0};
+      for (int q = 0; q < dim; ++q)
+        for (int c = 0; c < dim; ++c) xi[q] += Ji[c * 3 + q] * (x[c] - X0[c]);
+      double sum = 0.0, mn = 1.0;
+      for (int q = 0; q < dim; ++q) {
+        sum += xi[q];
+        mn = std::min(mn, xi[q]);
+      }
+      if (mn >= -1e-12 && sum <= 1.0 + 1e-12) {
+        cell[r] = s->f2i[e];
+        basis_eval(s->tab, xi, &phi[static_cast<size_t>(r) * NP]);
+      }
+    }
+    if (cell[r] < 0) return fail(DGP_ERR_INVALID, "receiver " + std::to_string(r) + " lies outside the mesh");
+  }
+  AdjointState& a = s->adj;
+  std::vector<double> obs(observed, observed + n);
+  int rc = DGP_OK;
+  if ((rc = s->upload(&a.rcell, cell)) || (rc = s->upload(&a.rphi, phi)) || (rc = s->upload(&a.robs, obs)) ||
+      (rc = s->alloc(&a.rrho, static_cast<size_t>(n))) || (rc = s->alloc(&a.rJ, 1)))
+    return rc;
+  a.nrec = n;
+  return DGP_OK;
+}
+
+static Receivers receivers_of(dgp_solver s) {
+  Receivers r;
+  r.n = s->adj.nrec;
+  r.cell = s->adj.rcell;
+  r.phi = s->adj.rphi;
+  r.obs = s->adj.robs;
+  r.np = s->b.NP;
+  r.mnp = s->b.M * s->b.NP;
+  return r;
+}
+
+int dgp_receiver_values(dgp_solver s, double* rho, double* J) {
+  if (!s) return fail(DGP_ERR_INVALID, "null solver");
+  if (!s->adj.nrec) return fail(DGP_ERR_INVALID, "no receivers set");
+  DGP_CUDA(cudaSetDevice(s->device));
+  receiver_values_kernel<<<1, 256, 0, s->stream>>>(receivers_of(s), static_cast<const double*>(s->b.C),
+                                                    s->adj.rrho, s->adj.rJ);
+  DGP_CUDA(cudaGetLastError());
+  DGP_CUDA(cudaStreamSynchronize(s->stream));
+  if (rho) DGP_CUDA(cudaMemcpy(rho, s->adj.rrho, s->adj.nrec * 8, cudaMemcpyDeviceToHost));
+  double j = 0;
+  DGP_CUDA(cudaMemcpy(&j, s->adj.rJ, 8, cudaMemcpyDeviceToHost));
+  if (J) *J = j;
+  return DGP_OK;
+}
+
+int dgp_forward_checkpointed(dgp_solver s, double t0, double dt, int nsteps, int every, double* J) {
+  if (!s || !(dt > 0) || nsteps <= 0 || every <= 0) return fail(DGP_ERR_INVALID, "bad argument");
+  if (s->b.ninst) return fail(DGP_ERR_UNSUPPORTED, "the adjoint runs on a single solver");
+  if (!s->ops.adj_stage) return fail(DGP_ERR_UNSUPPORTED, "no discrete adjoint for this law/flux");
+  if (s->limiter == DGP_LIMITER_MOMENT) return fail(DGP_ERR_UNSUPPORTED, "adjoint with the limiter on");
+  DGP_CUDA(cudaSetDevice(s->device));
+  AdjointState& a = s->adj;
+  const int nseg = (nsteps + every - 1) / every;
+  if (int rc = adj_buffer(s, &a.ckpt, &a.ckpt_states, static_cast<size_t>(nseg) + 1)) return rc;
+  if (!a.t_seg && (s->alloc(&a.t_seg, 1) != DGP_OK)) return DGP_ERR_NOMEM;
+  a.nsteps = nsteps;
+  a.every = every;
+  a.nseg = nseg;
+  a.t0 = t0;
+  a.dt = dt;
+  const size_t ns = s->state_count(), bytes = ns * 8;
+  const int p0 = s->b.p0;
+  s->b.p0 = 0;  // the adjoint differentiates the plain operator
+  set_segment_time<<<1, 1, 0, s->stream>>>(s->b.ctl, t0, dt, a.t_seg);
+  for (int seg = 0; seg < nseg; ++seg) {
+    DGP_CUDA(cudaMemcpyAsync(a.ckpt + static_cast<size_t>(seg) * ns, s->b.C, bytes, cudaMemcpyDeviceToDevice,
+                             s->stream));
+    const int len = std::min(every, nsteps - seg * every);
+    for (int k = 0; k < len; ++k) launch_step(s, 0);
+  }
+  DGP_CUDA(cudaMemcpyAsync(a.ckpt + static_cast<size_t>(nseg) * ns, s->b.C, bytes, cudaMemcpyDeviceToDevice,
+                           s->stream));
+  s->b.p0 = p0;
+  DGP_CUDA(cudaGetLastError());
+  a.ready = true;
+  if (a.nrec) return dgp_receiver_values(s, nullptr, J);
+  DGP_CUDA(cudaStreamSynchronize(s->stream));
+  if (J) *J = 0.0;
+  return DGP_OK;
+}
+
+int dgp_backward(dgp_solver s, const double* dJ_duT, double* dJ_du0) {
+  if (!s || !dJ_du0) return fail(DGP_ERR_INVALID, "null argument");
+  AdjointState& a = s->adj;
+  if (!a.ready) return fail(DGP_ERR_INVALID, "run dgp_forward_checkpointed first");
+  if (!dJ_duT && !a.nrec) return fail(DGP_ERR_INVALID, "no seed and no receivers");
+  DGP_CUDA(cudaSetDevice(s->device));
+  const size_t ns = s->state_count(), bytes = ns * 8;
+  if (int rc = adj_buffer(s, &a.store, &a.store_states, static_cast<size_t>(3) * a.every)) return rc;
+  if (!a.lam) {
+    size_t one = 0;
+    if (int rc = adj_buffer(s, &a.lam, &one, 1)) return rc;
+    one = 0;
+    if (int rc = adj_buffer(s, &a.lam2, &one, 1)) return rc;
+    one = 0;
+    if (int rc = adj_buffer(s, &a.lam1, &one, 1)) return rc;
+    one = 0;
+    if (int rc = adj_buffer(s, &a.acc, &one, 1)) return rc;
+  }
+  // seed: dJ/du_T
+  if (dJ_duT) {
+    if (int rc = host_to_state(s, dJ_duT, a.lam)) return rc;
+  } else {
+    DGP_CUDA(cudaMemsetAsync(a.lam, 0, bytes, s->stream));
+    const double* uT = a.ckpt + static_cast<size_t>(a.nseg) * ns;
+    receiver_values_kernel<<<1, 256, 0, s->stream>>>(receivers_of(s), uT, a.rrho, a.rJ);
+    receiver_seed_kernel<<<1, 32, 0, s->stream>>>(receivers_of(s), a.rrho, a.lam);
+  }
+  const int p0 = s->b.p0;
+  s->b.p0 = 0;
+  double* X = static_cast<double*>(s->b.C);
+  for (int seg = a.nseg - 1; seg >= 0; --seg) {
+    const int len = std::min(a.every, a.nsteps - seg * a.every);
+    const double tseg = a.t0 + static_cast<double>(seg) * a.every * a.dt;
+    // recompute the segment from its checkpoint, keeping every stage state
+    DGP_CUDA(cudaMemcpyAsync(X, a.ckpt + static_cast<size_t>(seg) * ns, bytes, cudaMemcpyDeviceToDevice,
+                             s->stream));
+    set_segment_time<<<1, 1, 0, s->stream>>>(s->b.ctl, tseg, a.dt, a.t_seg);
+    for (int j = 0; j < len; ++j) {
+      double* S0 = a.store + (static_cast<size_t>(j) * 3 + 0) * ns;
+      double* S1 = a.store + (static_cast<size_t>(j) * 3 + 1) * ns;
+      double* S2 = a.store + (static_cast<size_t>(j) * 3 + 2) * ns;
+      DeviceBuffers b = s->b;
+      b.U0 = S0;
+      b.C = X;
+      b.Cout = S1;
+      s->ops.stage(b, 1, 0.0, 0, s->stream);
+      b.C = S1;
+      b.Cout = S2;
+      s->ops.stage(b, 2, 1.0, 0, s->stream);
+      b.C = S2;
+      b.Cout = X;
+      s->ops.stage(b, 3, 0.5, 0, s->stream);
+    }
+    // reversed steps
+    for (int j = len - 1; j >= 0; --j) {
+      DeviceBuffers b = s->b;
+      AdjStage g{};
+      g.dt = a.dt;
+      g.t_seg = a.t_seg;
+      // u3 = (2 (u2 + dt L(u2)) + u) / 3
+      b.C = a.store + (static_cast<size_t>(j) * 3 + 2) * ns;
+      g.mu = a.lam;
+      g.out = a.lam2;
+      g.acc = a.acc;
+      g.ca = 2.0 / 3.0;
+      g.cb = 2.0 / 3.0;
+      g.cc = 0.0;
+      g.cd = 0.0;
+      g.ce = 1.0 / 3.0;
+      g.t_offset = (j + 0.5) * a.dt;
+      s->ops.adj_stage(b, g, s->stream);
+      // u2 = (u1 + dt L(u1) + 3 u) / 4
+      b.C = a.store + (static_cast<size_t>(j) * 3 + 1) * ns;
+      g.mu = a.lam2;
+      g.out = a.lam1;
+      g.ca = 0.25;
+      g.cb = 0.25;
+      g.cc = 0.0;
+      g.cd = 1.0;
+      g.ce = 0.75;
+      g.t_offset = (j + 1.0) * a.dt;
+      s->ops.adj_stage(b, g, s->stream);
+      // u1 = u + dt L(u)
+      b.C = a.store + (static_cast<size_t>(j) * 3 + 0) * ns;
+      g.mu = a.lam1;
+      g.out = a.lam;
+      g.ca = 1.0;
+      g.cb = 1.0;
+      g.cc = 1.0;
+      g.cd = 0.0;
+      g.ce = 0.0;
+      g.t_offset = j * a.dt;
+      s->ops.adj_stage(b, g, s->stream);
+    }
+  }
+  s->b.p0 = p0;
+  // the forward state is left at u_T
+  DGP_CUDA(cudaMemcpyAsync(X, a.ckpt + static_cast<size_t>(a.nseg) * ns, bytes, cudaMemcpyDeviceToDevice,
+                           s->stream));
+  DGP_CUDA(cudaGetLastError());
+  DGP_CUDA(cudaStreamSynchronize(s->stream));
+  return state_to_host(s, a.lam, dJ_du0);
 }
 
 }  // extern "C"

@@ -34,7 +34,33 @@ struct dgp_law_s {
   double p[DGP_NPARAMS];
 };
 
+// Discrete adjoint bookkeeping of a solver: checkpoints of the last
+// dgp_forward_checkpointed, the stage states of one recomputed segment, the
+// adjoint vectors and the receiver objective.
+struct AdjointState {
+  int nsteps = 0, every = 0, nseg = 0;
+  double t0 = 0, dt = 0;
+  double* ckpt = nullptr;   // (nseg + 1) states
+  size_t ckpt_states = 0;
+  double* store = nullptr;  // every x 3 stage states (u_n, u1, u2) of a segment
+  size_t store_states = 0;
+  double* lam = nullptr;    // lambda (input of the reversed step, output of it)
+  double* lam2 = nullptr;
+  double* lam1 = nullptr;
+  double* acc = nullptr;
+  double* t_seg = nullptr;  // device scalar
+  bool ready = false;       // a forward pass is recorded
+  // receivers: J = sum_r (rho(x_r) - obs_r)^2
+  int nrec = 0;
+  int* rcell = nullptr;
+  double* rphi = nullptr;
+  double* robs = nullptr;
+  double* rrho = nullptr;
+  double* rJ = nullptr;
+};
+
 struct dgp_solver_s {
+  AdjointState adj;
   std::vector<dgp::HostMesh> meshes;  // one per instance (one for a single solver)
   std::vector<int> inst_off;          // first internal cell of each instance
   std::vector<int> inst_ufirst;       // first cell of each instance in the joined file order

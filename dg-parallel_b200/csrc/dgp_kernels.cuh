@@ -349,7 +349,7 @@ __global__ void __launch_bounds__(K::FACE_BLOCK) face_rerun_kernel(const __grid_
   for (int e = blockIdx.x * blockDim.x + tid; e < a.mesh.E; e += gridDim.x * blockDim.x)
     if (a.bad[e])
       for (int r = 0; r < K::M; ++r)
-        for (int k = 1; k < K::NP; ++k) a.Cout[((size_t)e * K::M + r) * K::NP + k] = 0.0;
+        for (int k = 1; k < K::NP; ++k) const_cast<double*>(a.C)[((size_t)e * K::M + r) * K::NP + k] = 0.0;
   const int fl = tid / K::NQF, q = tid - (tid / K::NQF) * K::NQF;
   if (fl >= K::FPB) return;
   for (int vb = blockIdx.x; vb * K::FPB < a.mesh.F; vb += gridDim.x) {

@@ -2,18 +2,34 @@
 // instantiation units).
 #pragma once
 
+#include "dgp_adjoint.cuh"
 #include "dgp_elem.cuh"
 #include "dgp_limiter.cuh"
 #include "dgp_solver.h"
 
 namespace dgp {
 
+// the discrete adjoint covers the laws whose numerical fluxes are closed-form
+// (the exact Riemann solver's Newton iteration is not differentiated)
+template <class K>
+constexpr bool adjoint_built() {
+  return K::FLUX != DGP_FLUX_GODUNOV;
+}
+
 template <class K>
 cudaError_t ops_prepare() {
   const size_t smem = elem_kernel_smem<K>();
-  if (smem > 48 * 1024)
-    return cudaFuncSetAttribute(elem_kernel<K>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                static_cast<int>(smem));
+  if (smem > 48 * 1024) {
+    cudaError_t e = cudaFuncSetAttribute(elem_kernel<K>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         static_cast<int>(smem));
+    if (e != cudaSuccess) return e;
+  }
+  if constexpr (adjoint_built<K>()) {
+    const size_t as = adj_elem_smem<K>();
+    if (as > 48 * 1024)
+      return cudaFuncSetAttribute(adj_elem_kernel<K>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  static_cast<int>(as));
+  }
   return cudaSuccess;
 }
 
@@ -92,6 +108,29 @@ void ops_limit(const DeviceBuffers& b, int check_done, cudaStream_t st) {
   }
 }
 
+// one reversed stage of the discrete adjoint (face kernel, then element kernel)
+template <class K>
+void ops_adj_stage(const DeviceBuffers& b, const AdjStage& g, cudaStream_t st) {
+  if constexpr (adjoint_built<K>()) {
+    AdjArgs<typename K::T> a;
+    a.s = make_args<typename K::T>(b);
+    a.mu = g.mu;
+    a.out = g.out;
+    a.acc = g.acc;
+    a.ca = g.ca;
+    a.cb = g.cb;
+    a.cc = g.cc;
+    a.cd = g.cd;
+    a.ce = g.ce;
+    a.dt = g.dt;
+    a.t_seg = g.t_seg;
+    a.t_offset = g.t_offset;
+    const int fgrid = (b.F + K::FPB - 1) / K::FPB;
+    adj_face_kernel<K><<<fgrid, K::FACE_BLOCK, 0, st>>>(a);
+    adj_elem_kernel<K><<<ops_grid_elem<K>(b.E), K::BLOCK, adj_elem_smem<K>(), st>>>(a);
+  }
+}
+
 template <class K>
 void ops_cfl(const DeviceBuffers& b, cudaStream_t st) {
   StageArgs<typename K::T> a = make_args<typename K::T>(b);
@@ -146,6 +185,7 @@ Ops make_ops() {
   o.totals = &ops_totals<K>;
   o.grid_elem = &ops_grid_elem<K>;
   o.limit = (K::DIM == 2 && K::ORDER >= 1) ? &ops_limit<K> : nullptr;
+  o.adj_stage = adjoint_built<K>() ? &ops_adj_stage<K> : nullptr;
   return o;
 }
 

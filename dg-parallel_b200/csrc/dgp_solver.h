@@ -47,6 +47,7 @@ struct DeviceBuffers {
   double* ephi = nullptr;
   double phi0 = 0.0;
   void* C = nullptr;      // state [cell][field][mode], updated in place by the stages
+  void* Cout = nullptr;   // when set, the stages write here instead of into C
   void* U0 = nullptr;     // u_n of the current step
   void* slots = nullptr;  // per-cell face slots
   void* rhs = nullptr;    // assembled RHS for dgp_rhs
@@ -112,7 +113,7 @@ inline StageArgs<T> make_args(const DeviceBuffers& b) {
   a.law = b.law;
   a.C = static_cast<const double*>(b.C);
   a.U0 = static_cast<const double*>(b.U0);
-  a.Cout = static_cast<double*>(b.C);
+  a.Cout = static_cast<double*>(b.Cout ? b.Cout : b.C);
   a.U0out = static_cast<double*>(b.U0);
   a.slots = static_cast<T*>(b.slots);
   a.ctl = b.ctl;
@@ -128,6 +129,18 @@ inline StageArgs<T> make_args(const DeviceBuffers& b) {
   a.order = b.order;
   return a;
 }
+
+// One reversed stage of the discrete adjoint: out = ca mu + cb dt w + cc acc,
+// acc <- cd acc + ce mu, with w the transposed linearised L at the stage
+// state (b.C) and the stage time *t_seg + t_offset.
+struct AdjStage {
+  const double* mu;
+  double* out;
+  double* acc;
+  double ca, cb, cc, cd, ce, dt;
+  const double* t_seg;
+  double t_offset;
+};
 
 // Kernel set of one instantiation.
 struct Ops {
@@ -153,6 +166,8 @@ struct Ops {
   int (*grid_elem)(int E) = nullptr;
   // moment limiter pass (triangles, p >= 1; nullptr elsewhere)
   void (*limit)(const DeviceBuffers&, int check_done, cudaStream_t) = nullptr;
+  // discrete adjoint stage (nullptr where the adjoint is not built)
+  void (*adj_stage)(const DeviceBuffers&, const AdjStage&, cudaStream_t) = nullptr;
 };
 
 // law, flux, dim, order, precision, block (tile variant: 64, 128 or 256 threads)

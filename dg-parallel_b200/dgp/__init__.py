@@ -92,6 +92,10 @@ def lib() -> ctypes.CDLL:
         "dgp_autotune": ([P, P, I, I, I, I, pI, ctypes.POINTER(ctypes.c_float)], I),
         "dgp_autotune_ensemble": ([I, pP, pP, pI, I, I, I], I),
         "dgp_tune_set": ([I, I, I, I, I, I, I], I),
+        "dgp_adjoint_set_receivers": ([P, I, pD, pD], I),
+        "dgp_receiver_values": ([P, pD, pD], I),
+        "dgp_forward_checkpointed": ([P, D, D, I, I, pD], I),
+        "dgp_backward": ([P, pD, pD], I),
         "dgp_solver_block": ([P, pI, pI], I),
         "dgp_ensemble_group_block": ([P, I, pI, pI], I),
     }
@@ -309,6 +313,35 @@ class Solver:
         b, te = ctypes.c_int(), ctypes.c_int()
         check(lib().dgp_solver_block(self.h, ctypes.byref(b), ctypes.byref(te)))
         return b.value, te.value
+
+    # ---- discrete adjoint
+    def set_receivers(self, points: np.ndarray, observed: np.ndarray):
+        """J = sum_r (field0(x_r, T) - observed_r)^2; points (n, dim)."""
+        pts = np.ascontiguousarray(points, dtype=np.float64)
+        obs = np.ascontiguousarray(observed, dtype=np.float64)
+        self._nrec = len(obs)
+        check(lib().dgp_adjoint_set_receivers(self.h, len(obs), _dp(pts), _dp(obs)))
+
+    def receiver_values(self) -> tuple[np.ndarray, float]:
+        rho = np.zeros(self._nrec)
+        J = ctypes.c_double()
+        check(lib().dgp_receiver_values(self.h, _dp(rho), ctypes.byref(J)))
+        return rho, J.value
+
+    def forward_checkpointed(self, t0: float, dt: float, nsteps: int, every: int) -> float:
+        J = ctypes.c_double()
+        check(lib().dgp_forward_checkpointed(self.h, t0, dt, nsteps, every, ctypes.byref(J)))
+        return J.value
+
+    def backward(self, seed: np.ndarray | None = None) -> np.ndarray:
+        """dJ/du0 of the last forward_checkpointed (seed: dJ/du_T, default the
+        receiver objective's)."""
+        out = np.zeros(self.shape)
+        sd = None
+        if seed is not None:
+            sd = np.ascontiguousarray(seed, dtype=np.float64).reshape(self.shape)
+        check(lib().dgp_backward(self.h, _dp(sd) if sd is not None else None, _dp(out)))
+        return out
 
     def synchronize(self):
         check(lib().dgp_synchronize(self.h))

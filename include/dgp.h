@@ -188,6 +188,23 @@ int dgp_ensemble_run(dgp_ensemble e, double t0, double tend, double cfl, int max
 int dgp_ensemble_totals(dgp_ensemble e, int i, double* totals);
 int dgp_ensemble_l2_error(dgp_ensemble e, int i, double t, int field, double* err);
 int dgp_ensemble_launches_per_step(dgp_ensemble e, int* n);
+/* ---- discrete adjoint (no counterpart in DG-Parallel): gradient with respect
+ * to the initial coefficients of an objective of the state after nsteps
+ * SSP-RK3 steps of fixed size dt, by checkpoint (every `every` steps) and
+ * recompute.  The backward pass runs the transposed linearised operator
+ * (transposed volume contraction and lift, Jacobians of the numerical and
+ * boundary fluxes, reversed stage combination) on the device.  Built for the
+ * closed-form fluxes (not the exact Riemann solver), without the limiter.
+ * Receivers define J = sum_r (u_0(x_r, T) - observed_r)^2 on field 0 (the
+ * density of the Euler laws); points are dim doubles each. */
+int dgp_adjoint_set_receivers(dgp_solver s, int n, const double* points, const double* observed);
+/* field 0 at the receivers for the current state (rho may be NULL) and J */
+int dgp_receiver_values(dgp_solver s, double* rho, double* J);
+/* from the current state at time t0; leaves the state at the final time; J may be NULL */
+int dgp_forward_checkpointed(dgp_solver s, double t0, double dt, int nsteps, int every, double* J);
+/* dJ/du0 (host, file order [cell][field][mode]) of the last forward pass; the
+ * seed dJ/du_T is dJ_duT when not NULL, else the receiver objective's */
+int dgp_backward(dgp_solver s, const double* dJ_duT, double* dJ_du0);
 /* ---- autotuner: the tile shape (threads of the element and face kernels,
  * which sets the cells per element-kernel tile and the faces per face-kernel
  * CTA; 64, 128 or 256 where built) that runs fastest for a configuration at a

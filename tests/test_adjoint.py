@@ -1,0 +1,163 @@
+"""Discrete adjoint: the gradient of a receiver objective through SSP-RK3
+steps of fixed size, checked against central finite differences of the same
+forward map (FP64), and the mixed form against the FP64 gradient.
+
+J = sum_r (rho(x_r, T) - rho_obs_r)^2, rho_obs from a forward run with a
+different vortex strength (or amplitude, or width).  The forward map is the
+device operator with a fixed dt, so finite differences see exactly the
+function the adjoint differentiates.
+"""
+import numpy as np
+import pytest
+
+import dgp
+from dgp import meshgen
+from cases import SCALAR2D, TM110, VORTEX, params, rel
+
+pytestmark = pytest.mark.gpu
+
+
+def _mesh(tmp_path, n, box, seed, dim=2):
+    if dim == 2:
+        m = meshgen.tri_square(n, n, box[0], box[1], box[0], box[1], jitter=0.15, seed=seed)
+    else:
+        m = meshgen.tet_cube(n, box[0], box[1], jitter=0.1, seed=seed)
+    p = str(tmp_path / f"adj{dim}_{n}_{seed}.msh")
+    meshgen.write_msh_v1(m, p)
+    return p
+
+
+def _receivers(rng, n, lo, hi, dim=2):
+    return rng.uniform(lo, hi, size=(n, dim))
+
+
+def _setup(msh, law_id, flux, field, order, prm, prm_obs, pts, nsteps, every, precision=dgp.FP64):
+    mesh = dgp.Mesh.from_msh(msh)
+    # observations: forward run with the perturbed parameters
+    so = dgp.Solver(mesh, dgp.Law(law_id, flux, field, prm_obs), order, dgp.FP64)
+    so.project(0.0)
+    s = dgp.Solver(mesh, dgp.Law(law_id, flux, field, prm), order, precision)
+    s.project(0.0)
+    dt = 0.5 * s.cfl_dt(0.1)
+    so.set_receivers(pts, np.zeros(len(pts)))
+    so.forward_checkpointed(0.0, dt, nsteps, every)
+    obs, _ = so.receiver_values()
+    s.set_receivers(pts, obs)
+    return s, dt
+
+
+def _fd_check(s, dt, nsteps, every, ndir, eps, tol, seed=5):
+    u0 = s.get_state()
+    J0 = s.forward_checkpointed(0.0, dt, nsteps, every)
+    g = s.backward()
+    assert J0 > 0 and np.isfinite(g).all() and np.abs(g).max() > 0
+    rng = np.random.default_rng(seed)
+    for _ in range(ndir):
+        d = rng.standard_normal(u0.shape)
+        s.set_state(u0 + eps * d)
+        jp = s.forward_checkpointed(0.0, dt, nsteps, every)
+        s.set_state(u0 - eps * d)
+        jm = s.forward_checkpointed(0.0, dt, nsteps, every)
+        fd = (jp - jm) / (2 * eps)
+        ad = float(np.sum(g * d))
+        assert abs(fd - ad) <= tol * max(abs(fd), abs(ad)), (fd, ad)
+    s.set_state(u0)
+    return g
+
+
+def test_adjoint_euler_roe_matches_fd(tmp_path):
+    msh = _mesh(tmp_path, 12, (0.0, 10.0), 2)
+    pts = _receivers(np.random.default_rng(4), 64, 1.0, 9.0)
+    obs_prm = VORTEX.copy()
+    obs_prm[8] = 5.5
+    s, dt = _setup(msh, dgp.LAW_EULER2D, dgp.FLUX_ROE, dgp.FIELD_VORTEX, 2, VORTEX, obs_prm, pts, 24, 5)
+    _fd_check(s, dt, 24, 5, 4, 1e-6, 1e-6)
+
+
+def test_adjoint_euler_llf_matches_fd(tmp_path):
+    msh = _mesh(tmp_path, 10, (0.0, 10.0), 3)
+    pts = _receivers(np.random.default_rng(7), 32, 1.0, 9.0)
+    obs_prm = VORTEX.copy()
+    obs_prm[8] = 5.5
+    s, dt = _setup(msh, dgp.LAW_EULER2D, dgp.FLUX_LLF, dgp.FIELD_VORTEX, 3, VORTEX, obs_prm, pts, 12, 4)
+    _fd_check(s, dt, 12, 4, 3, 1e-6, 1e-5)
+
+
+def test_adjoint_scalar_is_exact_for_linear_operator(tmp_path):
+    msh = _mesh(tmp_path, 10, (0.0, 1.0), 1)
+    pts = _receivers(np.random.default_rng(8), 16, 0.1, 0.9)
+    obs_prm = SCALAR2D.copy()
+    obs_prm[6] = 0.02
+    s, dt = _setup(msh, dgp.LAW_SCALAR, dgp.FLUX_UPWIND, dgp.FIELD_GAUSS, 2, SCALAR2D, obs_prm, pts, 20, 7)
+    # J is quadratic in u0: central differences are exact up to rounding
+    _fd_check(s, dt, 20, 7, 3, 1e-3, 1e-8)
+
+
+def test_adjoint_burgers_llf_matches_fd(tmp_path):
+    msh = _mesh(tmp_path, 10, (0.0, 1.0), 9)
+    pts = _receivers(np.random.default_rng(9), 16, 0.1, 0.9)
+    s, dt = _setup(msh, dgp.LAW_BURGERS2D, dgp.FLUX_LLF, dgp.FIELD_SINE, 2, params(amplitude=0.3),
+                   params(amplitude=0.35), pts, 15, 4)
+    _fd_check(s, dt, 15, 4, 3, 1e-7, 1e-5)
+
+
+def test_adjoint_maxwell_tets_matches_fd(tmp_path):
+    msh = _mesh(tmp_path, 3, (0.0, 1.0), 3, dim=3)
+    pts = _receivers(np.random.default_rng(10), 12, 0.15, 0.85, dim=3)
+    obs_prm = TM110.copy()
+    obs_prm[10] = 1.1
+    s, dt = _setup(msh, dgp.LAW_MAXWELL3D, dgp.FLUX_UPWIND, dgp.FIELD_TM110, 1, TM110, obs_prm, pts, 10, 3)
+    _fd_check(s, dt, 10, 3, 2, 1e-3, 1e-8)
+
+
+def test_adjoint_seed_and_checkpoint_interval_invariance(tmp_path):
+    msh = _mesh(tmp_path, 8, (0.0, 10.0), 2)
+    pts = _receivers(np.random.default_rng(4), 16, 1.0, 9.0)
+    obs_prm = VORTEX.copy()
+    obs_prm[8] = 5.5
+    s, dt = _setup(msh, dgp.LAW_EULER2D, dgp.FLUX_ROE, dgp.FIELD_VORTEX, 2, VORTEX, obs_prm, pts, 12, 4)
+    u0 = s.get_state()
+    s.forward_checkpointed(0.0, dt, 12, 4)
+    g4 = s.backward()
+    s.set_state(u0)
+    s.forward_checkpointed(0.0, dt, 12, 12)
+    g12 = s.backward()
+    # recomputation reproduces the forward states exactly
+    assert np.array_equal(g4, g12)
+    # an explicit seed: d/du0 of <c, u_T> for a fixed c
+    s.set_state(u0)
+    s.forward_checkpointed(0.0, dt, 12, 3)
+    c = np.random.default_rng(3).standard_normal(u0.shape)
+    gc = s.backward(c)
+    d = np.random.default_rng(4).standard_normal(u0.shape)
+    eps = 1e-6
+    s.set_state(u0 + eps * d)
+    s.forward_checkpointed(0.0, dt, 12, 3)
+    up = s.get_state()
+    s.set_state(u0 - eps * d)
+    s.forward_checkpointed(0.0, dt, 12, 3)
+    um = s.get_state()
+    fd = float(np.sum(c * (up - um))) / (2 * eps)
+    assert abs(fd - float(np.sum(gc * d))) <= 1e-6 * abs(fd)
+
+
+def test_adjoint_mixed_form_close_to_fp64(tmp_path):
+    msh = _mesh(tmp_path, 12, (0.0, 10.0), 2)
+    pts = _receivers(np.random.default_rng(4), 64, 1.0, 9.0)
+    obs_prm = VORTEX.copy()
+    obs_prm[8] = 5.5
+    s64, dt = _setup(msh, dgp.LAW_EULER2D, dgp.FLUX_ROE, dgp.FIELD_VORTEX, 2, VORTEX, obs_prm, pts, 20, 5)
+    s32, _ = _setup(msh, dgp.LAW_EULER2D, dgp.FLUX_ROE, dgp.FIELD_VORTEX, 2, VORTEX, obs_prm, pts, 20, 5,
+                    precision=dgp.MIXED)
+    s64.forward_checkpointed(0.0, dt, 20, 5)
+    s32.forward_checkpointed(0.0, dt, 20, 5)
+    g64, g32 = s64.backward(), s32.backward()
+    assert rel(g32, g64) < 1e-3
+
+
+def test_adjoint_refused_where_not_built(tmp_path):
+    msh = _mesh(tmp_path, 6, (0.0, 10.0), 2)
+    mesh = dgp.Mesh.from_msh(msh)
+    s = dgp.Solver(mesh, dgp.Law(dgp.LAW_EULER2D, dgp.FLUX_GODUNOV, dgp.FIELD_VORTEX, VORTEX), 2)
+    with pytest.raises(dgp.DGPError):
+        s.forward_checkpointed(0.0, 1e-3, 2, 1)
