@@ -440,8 +440,8 @@ def adjoint_bench(n=128, order=2, nsteps=400, every=20, nrec=64, ndir=16, eps=1e
     rho_obs from a forward run with vortex strength 5.5.  The gradient with
     respect to every initial coefficient is computed in the mixed form (FP32
     right-hand side and adjoint arithmetic) and in FP64, and checked by central
-    differences (eps along ndir seeded Gaussian directions) of the FP64 forward
-    map.  Times are CUDA-event times on the solver's stream."""
+    differences (step eps along ndir seeded Gaussian directions of unit 2-norm)
+    of the FP64 forward map.  Times are CUDA-event times on the solver's stream."""
     import numpy as np
     import torch
     import dgp
@@ -499,6 +499,7 @@ def adjoint_bench(n=128, order=2, nsteps=400, every=20, nrec=64, ndir=16, eps=1e
     err64, err32 = [], []
     for _ in range(ndir):
         d = rng.standard_normal(u0.shape)
+        d /= np.linalg.norm(d)  # unit direction in coefficient space
         s.set_state(u0 + eps * d)
         jp = s.forward_checkpointed(0.0, dt, nsteps, nsteps)
         s.set_state(u0 - eps * d)

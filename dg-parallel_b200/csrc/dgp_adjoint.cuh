@@ -41,6 +41,9 @@ struct AdjArgs {
   double t_offset;     // stage time = *t_seg + t_offset
 };
 
+// input directions per dual-number pass of the face Jacobians
+constexpr int kAdjLanes = 2;
+
 // trace of nu = mu / |J| at one face point
 template <class K>
 __device__ __forceinline__ void nu_trace(const double* __restrict__ mu, double inv_detj,
@@ -84,58 +87,63 @@ __global__ void __launch_bounds__(K::FACE_BLOCK) adj_face_kernel(const __grid_co
     const T* phiR = s_phif + (lfR * NQF + qR) * NP;
     cell_trace<K>(a.s.C + (size_t)eR * MNP, phiR, UR);
     nu_trace<K>(a.mu + (size_t)eR * MNP, 1.0 / m.detjd[eR], phiR, VR);
-    // the Jacobian one input direction at a time (one-lane dual numbers keep
-    // the flux in registers); column c < M is d/dU_L[c], c >= M d/dU_R[c - M]
-    using D = Dual<T, 1>;
+    // the Jacobian W input directions per pass (narrow dual numbers keep the
+    // flux in registers); direction c < M is d/dU_L[c], c >= M is d/dU_R[c - M]
+    constexpr int W = kAdjLanes;
+    using D = Dual<T, W>;
     T fb[M];
 #pragma unroll
     for (int j = 0; j < M; ++j) fb[j] = (VR[j] - VL[j]) * jw;
 #pragma unroll 1
-    for (int c = 0; c < 2 * M; ++c) {
+    for (int c0 = 0; c0 < 2 * M; c0 += W) {
       D dl[M], dr[M], nd[DIM], F[M];
 #pragma unroll
       for (int j = 0; j < M; ++j) {
-        dl[j] = D::var(UL[j], c == j ? 0 : 1);
-        dr[j] = D::var(UR[j], c == M + j ? 0 : 1);
+        dl[j] = D::var(UL[j], j - c0);
+        dr[j] = D::var(UR[j], M + j - c0);
       }
 #pragma unroll
       for (int i = 0; i < DIM; ++i) nd[i] = D(n[i]);
       numerical_flux<K::LAW, K::FLUX, DIM, D>(a.s.law, nd, dl, dr, F);
-      T g = 0;
 #pragma unroll
-      for (int j = 0; j < M; ++j) g += fb[j] * F[j].d[0];
-      if (c < M) {
+      for (int w = 0; w < W; ++w) {
+        T g = 0;
 #pragma unroll
-        for (int k = 0; k < M; ++k)
+        for (int j = 0; j < M; ++j) g += fb[j] * F[j].d[w];
+        const int c = c0 + w;
+#pragma unroll
+        for (int k = 0; k < M; ++k) {
           if (k == c) gL[k] = g;
-      } else {
-#pragma unroll
-        for (int k = 0; k < M; ++k)
-          if (k == c - M) gR[k] = g;
+          if (k + M == c) gR[k] = g;
+        }
       }
     }
     T* sr = a.s.slots + slot_index<K>(eR, lfR * NQF + qR, 0);
 #pragma unroll
     for (int c = 0; c < M; ++c) sr[c] = gR[c];
   } else {
-    using D = Dual<T, 1>;
+    constexpr int W = kAdjLanes;
+    using D = Dual<T, W>;
     const int b = -eR - 1;
     const double* x = m.bpts + ((size_t)b * NQF + q) * 3;
     const double time = *a.t_seg + a.t_offset;
 #pragma unroll 1
-    for (int c = 0; c < M; ++c) {
+    for (int c0 = 0; c0 < M; c0 += W) {
       D dl[M], nd[DIM], F[M];
 #pragma unroll
-      for (int j = 0; j < M; ++j) dl[j] = D::var(UL[j], c == j ? 0 : 1);
+      for (int j = 0; j < M; ++j) dl[j] = D::var(UL[j], j - c0);
 #pragma unroll
       for (int i = 0; i < DIM; ++i) nd[i] = D(n[i]);
       boundary_flux<K::LAW, K::FLUX, DIM, D>(a.s.law, m.bbid[b], nd, x, time, dl, F);
-      T g = 0;
 #pragma unroll
-      for (int j = 0; j < M; ++j) g += -VL[j] * jw * F[j].d[0];
+      for (int w = 0; w < W; ++w) {
+        T g = 0;
 #pragma unroll
-      for (int k = 0; k < M; ++k)
-        if (k == c) gL[k] = g;
+        for (int j = 0; j < M; ++j) g += -VL[j] * jw * F[j].d[w];
+#pragma unroll
+        for (int k = 0; k < M; ++k)
+          if (k == c0 + w) gL[k] = g;
+      }
     }
   }
   T* sl = a.s.slots + slot_index<K>(eL, lfL * NQF + q, 0);

@@ -397,17 +397,19 @@ static int build_solver(dgp_solver s, const std::vector<LawParams>& lps, int fie
   // 256 bytes of tail so the bulk copy of the last tile may round up to 16 bytes
   const size_t ntiles = (static_cast<size_t>(Etot) + TE - 1) / TE;
   const size_t nslot = ntiles * TE * t.nlf * t.nqf * b.M;
-  unsigned char *C, *U0, *slots, *rhs, *scratch;
-  const size_t ts = s->ops.tsize;  // slots hold the RHS arithmetic type; the state is FP64
+  unsigned char *C, *U0, *slots, *tr, *rhs, *scratch;
+  const size_t ts = s->ops.tsize;  // slots and traces hold the RHS arithmetic type; the state is FP64
   if ((rc = s->alloc(&C, nstate * 8 + 256)) || (rc = s->alloc(&U0, nstate * 8 + 256)) ||
-      (rc = s->alloc(&slots, nslot * ts)) || (rc = s->alloc(&rhs, nstate * 8 + 256)) ||
-      (rc = s->alloc(&scratch, nstate * 8 + 256)))
+      (rc = s->alloc(&slots, nslot * ts)) || (rc = s->alloc(&tr, nslot * ts)) ||
+      (rc = s->alloc(&rhs, nstate * 8 + 256)) || (rc = s->alloc(&scratch, nstate * 8 + 256)))
     return rc;
+  DGP_CUDA(cudaMemset(tr, 0, nslot * ts));
   DGP_CUDA(cudaMemset(C, 0, nstate * 8 + 256));
   DGP_CUDA(cudaMemset(U0, 0, nstate * 8 + 256));
   b.C = C;
   b.U0 = U0;
   b.slots = slots;
+  b.tr = tr;
   b.rhs = rhs;
   b.scratch = scratch;
   b.npartials = std::max(s->ops.grid_elem(Etot), (Etot + 255) / 256) * std::max(b.M, 1) + 1;
@@ -450,6 +452,7 @@ static int build_solver(dgp_solver s, const std::vector<LawParams>& lps, int fie
   if (cudaError_t e = s->ops.prepare()) return fail(DGP_ERR_CUDA, cudaGetErrorString(e));
   // DGAnalysis::DGAnalysis projects the far field as the initial state
   s->ops.project(b, 0.0, s->stream);
+  s->ops.trace(b, nullptr, s->stream);
   DGP_CUDA(cudaGetLastError());
   DGP_CUDA(cudaStreamSynchronize(s->stream));
   return DGP_OK;
@@ -655,6 +658,7 @@ int dgp_project(dgp_solver s, double t) {
   s->ops.project(s->b, t, s->stream);
   // DGAnalysis::DGAnalysis limits the projected state once (DGAnalysis.cc:276-291)
   if (s->limiter == DGP_LIMITER_MOMENT && s->ops.limit) s->ops.limit(s->b, 0, s->stream);
+  s->ops.trace(s->b, nullptr, s->stream);
   DGP_CUDA(cudaGetLastError());
   DGP_CUDA(cudaStreamSynchronize(s->stream));
   return DGP_OK;
@@ -683,7 +687,11 @@ int dgp_set_state(dgp_solver s, const double* host_state) {
   if (!s || !host_state) return fail(DGP_ERR_INVALID, "null argument");
   DGP_CUDA(cudaSetDevice(s->device));
   DGP_CUDA(cudaStreamSynchronize(s->stream));
-  return host_to_state(s, host_state, s->b.C);
+  if (int rc = host_to_state(s, host_state, s->b.C)) return rc;
+  s->ops.trace(s->b, nullptr, s->stream);
+  DGP_CUDA(cudaGetLastError());
+  DGP_CUDA(cudaStreamSynchronize(s->stream));
+  return DGP_OK;
 }
 
 int dgp_get_state(dgp_solver s, double* host_state) {
@@ -701,6 +709,7 @@ int dgp_set_state_device(dgp_solver s, const double* dev_state) {
   const int grid = static_cast<int>((n + 255) / 256);
   gather_cells<double, double><<<grid, 256, 0, s->stream>>>(dev_state, static_cast<double*>(s->b.C),
                                                             s->d_i2f, s->b.E, mnp);
+  s->ops.trace(s->b, nullptr, s->stream);
   DGP_CUDA(cudaGetLastError());
   DGP_CUDA(cudaStreamSynchronize(s->stream));
   return DGP_OK;
@@ -1082,6 +1091,9 @@ int dgp_ensemble_set_state(dgp_ensemble e, int i, const double* host_state) {
     std::memcpy(&tmp[r * mnp], &host_state[static_cast<size_t>(s->i2f[off + r] - uf) * mnp], mnp * 8);
   DGP_CUDA(cudaMemcpy(static_cast<double*>(s->b.C) + static_cast<size_t>(off) * mnp, tmp.data(),
                       tmp.size() * 8, cudaMemcpyHostToDevice));
+  s->ops.trace(s->b, nullptr, s->stream);
+  DGP_CUDA(cudaGetLastError());
+  DGP_CUDA(cudaStreamSynchronize(s->stream));
   return DGP_OK;
 }
 
@@ -1516,6 +1528,7 @@ int dgp_backward(dgp_solver s, const double* dJ_duT, double* dJ_du0) {
     // recompute the segment from its checkpoint, keeping every stage state
     DGP_CUDA(cudaMemcpyAsync(X, a.ckpt + static_cast<size_t>(seg) * ns, bytes, cudaMemcpyDeviceToDevice,
                              s->stream));
+    s->ops.trace(s->b, nullptr, s->stream);
     set_segment_time<<<1, 1, 0, s->stream>>>(s->b.ctl, tseg, a.dt, a.t_seg);
     for (int j = 0; j < len; ++j) {
       double* S0 = a.store + (static_cast<size_t>(j) * 3 + 0) * ns;
@@ -1579,6 +1592,7 @@ int dgp_backward(dgp_solver s, const double* dJ_duT, double* dJ_du0) {
   // the forward state is left at u_T
   DGP_CUDA(cudaMemcpyAsync(X, a.ckpt + static_cast<size_t>(a.nseg) * ns, bytes, cudaMemcpyDeviceToDevice,
                            s->stream));
+  s->ops.trace(s->b, nullptr, s->stream);
   DGP_CUDA(cudaGetLastError());
   DGP_CUDA(cudaStreamSynchronize(s->stream));
   return state_to_host(s, a.lam, dJ_du0);

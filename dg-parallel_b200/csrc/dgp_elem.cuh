@@ -369,6 +369,20 @@ __global__ void __launch_bounds__(K::BLOCK) elem_kernel(const __grid_constant__ 
         crow[k] = out;
         a.Cout[gbase + k] = out;
       }
+      // face-point traces of the new state for the next stage's face kernel
+      T o[NP];
+#pragma unroll
+      for (int k = 0; k < NP; ++k) o[k] = (T)crow[k];
+      T* tr = a.tr + (size_t)blockIdx.x * NS * ROWS + row;
+#pragma unroll 4
+      for (int s = 0; s < NS; ++s) {
+        T p[NPP];
+        load_vec<T, NPP>(sPhif + s * NPP, p);
+        T t = 0;
+#pragma unroll
+        for (int k = 0; k < NP; ++k) t += p[k] * o[k];
+        tr[(size_t)s * ROWS] = t;
+      }
     }
   }
   if (a.stage != 3) return;

@@ -148,6 +148,8 @@ struct StageArgs {
   double* Cout;      // state the stage writes (or the RHS when stage == 0)
   double* U0out;     // stage 1 copies u_n here
   T* slots;        // E x NLF x NQF x M
+  T* tr;           // face-point traces of the state C, slot layout (kept current by the
+                   // element kernel and by trace_kernel after any other change of C)
   TimeCtl* ctl;
   Status* status;
   double* partials;  // per-block residual partials (stage 3)
@@ -243,6 +245,44 @@ __device__ __forceinline__ void cell_trace(const double* __restrict__ c, const t
   }
 }
 
+// the M field values of a cell's trace at face point s (slot layout, M
+// contiguous values)
+template <class K>
+__device__ __forceinline__ void load_trace(const typename K::T* __restrict__ tr, int e, int s,
+                                           typename K::T* U) {
+  using T = typename K::T;
+  constexpr int B = (int)(K::M * sizeof(T));
+  constexpr int ALIGN = pow2_div(B) < 16 ? pow2_div(B) : 16;
+  T v[K::M];
+  ldg_vec<T, K::M, ALIGN>(tr + slot_index<K>(e, s, 0), v);
+#pragma unroll
+  for (int j = 0; j < K::M; ++j) U[j] = v[j];
+}
+
+// Face-point traces of the state, for every cell (only == nullptr) or the
+// cells with only[e] != 0: one CTA per tile, one thread per (cell, field)
+// row, in the order the element kernel uses for its fresh state.
+template <class K>
+__global__ void __launch_bounds__(K::BLOCK) trace_kernel(const __grid_constant__ StageArgs<typename K::T> a,
+                                                          const unsigned char* only) {
+  using T = typename K::T;
+  constexpr int M = K::M, NP = K::NP, NS = K::NS, ROWS = K::ROWS;
+  const int e0 = blockIdx.x * K::TE, row = threadIdx.x;
+  const int e = e0 + row / M;
+  if (row >= ROWS || e >= a.mesh.E) return;
+  if (only && !only[e]) return;
+  T c[NP];
+#pragma unroll
+  for (int k = 0; k < NP; ++k) c[k] = (T)a.C[((size_t)e0 * M + row) * NP + k];
+  T* out = a.tr + (size_t)blockIdx.x * NS * ROWS + row;
+  for (int s = 0; s < NS; ++s) {
+    T acc = 0;
+#pragma unroll
+    for (int k = 0; k < NP; ++k) acc += __ldg(a.tab.phif + s * NP + k) * c[k];
+    out[(size_t)s * ROWS] = acc;
+  }
+}
+
 // One face point: traces of both sides, numerical (or boundary) flux, the two
 // face slots.  RERUN: second pass of the P0 fallback, where the traces of
 // marked cells are their means.
@@ -265,7 +305,10 @@ __device__ __forceinline__ void face_point(const StageArgs<typename K::T>& a, in
   for (int i = 0; i < DIM; ++i) n[i] = a.mesh.fnrm[f * DIM + i];
   const T jw = a.mesh.fj[f] * s_fqw[q];
   T UL[M], UR[M], flux[M];
-  cell_trace<K>(a.C + (size_t)eL * MNP, s_phif + (lfL * NQF + q) * NP, UL, RERUN && a.bad[eL]);
+  if constexpr (RERUN)
+    cell_trace<K>(a.C + (size_t)eL * MNP, s_phif + (lfL * NQF + q) * NP, UL, a.bad[eL]);
+  else
+    load_trace<K>(a.tr, eL, lfL * NQF + q, UL);
   if (!RERUN && !is_physical<K::LAW, T>(a.law, UL)) {
     flag_nonphysical(a.status, eL);
     if (a.p0) mark_p0(a, eL);
@@ -273,7 +316,10 @@ __device__ __forceinline__ void face_point(const StageArgs<typename K::T>& a, in
   int qR = 0;
   if (eR >= 0) {
     qR = s_qmap[perm * NQF + q];
-    cell_trace<K>(a.C + (size_t)eR * MNP, s_phif + (lfR * NQF + qR) * NP, UR, RERUN && a.bad[eR]);
+    if constexpr (RERUN)
+      cell_trace<K>(a.C + (size_t)eR * MNP, s_phif + (lfR * NQF + qR) * NP, UR, a.bad[eR]);
+    else
+      load_trace<K>(a.tr, eR, lfR * NQF + qR, UR);
     if (!RERUN && !is_physical<K::LAW, T>(a.law, UR)) {
       flag_nonphysical(a.status, eR);
       if (a.p0) mark_p0(a, eR);
@@ -321,15 +367,17 @@ template <class K, bool ENS>
 __global__ void __launch_bounds__(K::FACE_BLOCK) face_kernel(const __grid_constant__ StageArgs<typename K::T> a) {
   using T = typename K::T;
   if (a.gctl->done) return;
-  __shared__ T s_phif[K::NLF * K::NQF * K::NP];
+  // the traces come precomputed: only the weights and orientation maps
   __shared__ T s_fqw[K::NQF];
   __shared__ int s_qmap[K::NPERM * K::NQF];
-  face_tables<K>(a, s_phif, s_fqw, s_qmap);
   const int tid = threadIdx.x;
+  for (int i = tid; i < K::NQF; i += blockDim.x) s_fqw[i] = a.tab.fqw[i];
+  for (int i = tid; i < K::NPERM * K::NQF; i += blockDim.x) s_qmap[i] = a.tab.qmap[i];
+  __syncthreads();
   const int fl = tid / K::NQF, q = tid - (tid / K::NQF) * K::NQF;
   const int f = blockIdx.x * K::FPB + fl;
   if (fl >= K::FPB || f >= a.mesh.F) return;
-  face_point<K, false, ENS>(a, f, q, s_phif, s_fqw, s_qmap);
+  face_point<K, false, ENS>(a, f, q, nullptr, s_fqw, s_qmap);
 }
 
 // Second pass of the P0 fallback on a small grid: returns at once unless a

@@ -12,10 +12,11 @@
 //
 // How: the caller passes the state and the output as device buffers.  Every
 // intermediate -- the state in the solver's internal cell order, the per-cell
-// face slots written by the face kernel, the RHS in internal order -- lives
-// in one file-scope __device__ array of kScratchBytes (32 MiB).  The array is
-// part of the library image: every GPU that loads libdgp.so holds it until the
-// process exits.  Meshes whose intermediates do not fit are rejected.
+// face slots written by the face kernel, the face-point traces, the RHS in
+// internal order -- lives in one file-scope __device__ array of kScratchBytes
+// (32 MiB).  The array is part of the library image: every GPU that loads
+// libdgp.so holds it until the process exits.  Meshes whose intermediates do
+// not fit are rejected.
 //
 // The array is shared by all calls and keeps the last call's contents; every
 // byte a call reads is written earlier in the same call, so nothing has to be
@@ -79,7 +80,7 @@ extern "C" int dgp_rhs_noalloc(dgp_solver s, const double* dev_state, double t, 
   const size_t state_b = round256(s->state_count() * 8);  // FP64 state and RHS
   const size_t ntiles = (static_cast<size_t>(E) + s->ops.TE - 1) / s->ops.TE;
   const size_t slot_b = round256(ntiles * s->ops.TE * s->tab.nlf * s->tab.nqf * s->b.M * tsize);
-  const size_t need = 2 * state_b + slot_b;
+  const size_t need = 2 * state_b + 2 * slot_b;
   if (need > kScratchBytes)
     return fail(DGP_ERR_INVALID, "dgp_rhs_noalloc: this mesh needs " + std::to_string(need) +
                                      " bytes of scratch; the static scratch holds " +
@@ -91,6 +92,7 @@ extern "C" int dgp_rhs_noalloc(dgp_solver s, const double* dev_state, double t, 
   b.C = p;
   b.slots = p + state_b;
   b.rhs = p + state_b + slot_b;
+  b.tr = p + 2 * state_b + slot_b;
   const long long n = static_cast<long long>(E) * mnp;
   const int grid = static_cast<int>((n + 255) / 256);
   permute_rows<double, double><<<grid, 256, 0, s->stream>>>(dev_state, static_cast<double*>(b.C),
@@ -100,6 +102,7 @@ extern "C" int dgp_rhs_noalloc(dgp_solver s, const double* dev_state, double t, 
   c.dtmin_bits = 0x7FF0000000000000ull;
   s->h_ctl[0] = c;
   DGP_CUDA(cudaMemcpyAsync(s->b.ctl, &s->h_ctl[0], sizeof(dgp::TimeCtl), cudaMemcpyHostToDevice, s->stream));
+  s->ops.trace(b, nullptr, s->stream);
   s->ops.face(b, 0, 0.0, s->stream);
   s->ops.elem(b, 0, 0, s->stream);
   permute_rows<double, double><<<grid, 256, 0, s->stream>>>(static_cast<const double*>(b.rhs), dev_rhs,

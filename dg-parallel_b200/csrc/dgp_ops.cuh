@@ -85,6 +85,12 @@ void ops_stage(const DeviceBuffers& b, int stage, double time_factor, int fuse_c
   ops_elem<K>(b, stage, fuse_cfl, st);
 }
 
+template <class K>
+void ops_trace(const DeviceBuffers& b, const unsigned char* only, cudaStream_t st) {
+  auto a = make_args<typename K::T>(b);
+  trace_kernel<K><<<ops_grid_elem<K>(b.E), K::BLOCK, 0, st>>>(a, only);
+}
+
 // triangle moment limiter on the current state: limited rows of triggered
 // cells into L, then copied back
 template <class K>
@@ -105,6 +111,7 @@ void ops_limit(const DeviceBuffers& b, int check_done, cudaStream_t st) {
     limit_kernel<K><<<(b.E + 127) / 128, 128, 0, st>>>(a);
     const long long n = static_cast<long long>(b.E) * K::MNP;
     limit_apply_kernel<K><<<static_cast<int>((n + 255) / 256), 256, 0, st>>>(a);
+    ops_trace<K>(b, b.trig, st);
   }
 }
 
@@ -186,6 +193,7 @@ Ops make_ops() {
   o.grid_elem = &ops_grid_elem<K>;
   o.limit = (K::DIM == 2 && K::ORDER >= 1) ? &ops_limit<K> : nullptr;
   o.adj_stage = adjoint_built<K>() ? &ops_adj_stage<K> : nullptr;
+  o.trace = &ops_trace<K>;
   return o;
 }
 

@@ -50,6 +50,7 @@ struct DeviceBuffers {
   void* Cout = nullptr;   // when set, the stages write here instead of into C
   void* U0 = nullptr;     // u_n of the current step
   void* slots = nullptr;  // per-cell face slots
+  void* tr = nullptr;     // face-point traces of C (slot layout)
   void* rhs = nullptr;    // assembled RHS for dgp_rhs
   void* scratch = nullptr;// state-sized staging for device-side set/get
   TimeCtl* ctl = nullptr;
@@ -116,6 +117,7 @@ inline StageArgs<T> make_args(const DeviceBuffers& b) {
   a.Cout = static_cast<double*>(b.Cout ? b.Cout : b.C);
   a.U0out = static_cast<double*>(b.U0);
   a.slots = static_cast<T*>(b.slots);
+  a.tr = static_cast<T*>(b.tr);
   a.ctl = b.ctl;
   a.status = b.status;
   a.partials = b.partials;
@@ -166,6 +168,8 @@ struct Ops {
   int (*grid_elem)(int E) = nullptr;
   // moment limiter pass (triangles, p >= 1; nullptr elsewhere)
   void (*limit)(const DeviceBuffers&, int check_done, cudaStream_t) = nullptr;
+  // face-point traces of C (only: cells to refresh, nullptr for all)
+  void (*trace)(const DeviceBuffers&, const unsigned char* only, cudaStream_t) = nullptr;
   // discrete adjoint stage (nullptr where the adjoint is not built)
   void (*adj_stage)(const DeviceBuffers&, const AdjStage&, cudaStream_t) = nullptr;
 };
