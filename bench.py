@@ -247,7 +247,12 @@ def main():
 
     results = {}
     clocks = None
+    tiles = {}
     for name, prec in (("fp64", dgp.FP64), ("mixed", dgp.MIXED)):
+        # tile shape of the element and face kernels from the autotuner
+        # (untimed; a few steps of each built shape on this mesh)
+        best, cand = dgp.autotune(mesh, law, 3, prec, 0, iters=5)
+        tiles[name] = {"block": best, "ms_per_step_64_128_256": cand}
         s = dgp.Solver(mesh, law, 3, prec)
         sampler = ClockSampler(local) if (name == "fp64" and rank == 0) else None
         sec, t_end, n = timed_run(s, args.steps, args.warmup, sampler)
@@ -338,7 +343,8 @@ def main():
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic",
             "config": dict(WORKLOAD, parallelism=f"replicas{world}",
-                           l2="working set 150 MB > 126 MB L2; each step streams ~1 GB"),
+                           l2="working set 290 MB > 126 MB L2; each step streams ~1 GB",
+                           tiles=tiles),
             "mixed": {"value": mixed["value"],
                       "dtype": "f32 RHS (traces, fluxes, contractions, face slots); f64 state, "
                                "RK update, inverse mass, time, totals",

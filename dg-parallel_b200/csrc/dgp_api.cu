@@ -359,6 +359,13 @@ static int build_solver(dgp_solver s, const std::vector<LawParams>& lps, int fie
   }
   b.F = Ftot;
   b.NB = nb;
+  // per-cell geometry padded to whole tiles (the element kernel copies a
+  // tile's J^{-1} and |J| in one piece)
+  {
+    const size_t ecap = (static_cast<size_t>(Etot) + TE - 1) / TE * TE;
+    jinv.resize(ecap * dim * dim, 0.0);
+    detj.resize(ecap, 1.0);
+  }
 
   // reference tables
   std::vector<double> qpd(static_cast<size_t>(t.nq) * 3);

@@ -93,15 +93,19 @@ struct ElemSmem {
   static constexpr size_t blob_elems = oQw + (K::NQ + V - 1) / V * V;
   static constexpr size_t blob_bytes = blob_elems * sizeof(T);
   // tile, byte offsets: FP64 coefficients [ROWS][NP], G [ROWS][LDK] (T),
-  // then FP64 J^{-1}, |J| [TE][DD] and CFL eigenvalues [TE][NV]
+  // FP64 J^{-1}, |J| [TE][DD] and CFL eigenvalues [TE][NV], FP64 u_n
+  // [ROWS][NP], face slots [NS][ROWS] (T)
   static constexpr size_t r16(size_t n) { return (n + 15) / 16 * 16; }
   static constexpr size_t oCB = r16(blob_bytes);
   static constexpr size_t oGB = oCB + r16((size_t)K::ROWS * K::NP * 8);
   static constexpr size_t oJB = oGB + r16((size_t)K::ROWS * K::LDK * sizeof(T));
-  static constexpr size_t bytes = oJB + 8 * ((size_t)K::TE * DD + (size_t)K::TE * K::NV);
-  // the tile's coefficients can be bulk copied when every tile starts on a
-  // 16-byte boundary
+  static constexpr size_t oUB = oJB + r16(8 * ((size_t)K::TE * DD + (size_t)K::TE * K::NV));
+  static constexpr size_t oSB = oUB + r16((size_t)K::ROWS * K::NP * 8);
+  static constexpr size_t bytes = oSB + r16((size_t)K::NS * K::ROWS * sizeof(T));
+  // the tile's coefficients (and u_n) can be bulk copied when every tile starts
+  // on a 16-byte boundary; the slots of a tile are one contiguous block
   static constexpr bool bulk_c = ((size_t)K::TE * K::MNP * 8) % 16 == 0;
+  static constexpr bool bulk_s = ((size_t)K::NS * K::ROWS * sizeof(T)) % 16 == 0;
 };
 
 template <class K>
@@ -127,21 +131,18 @@ void fill_table_blob(const double* dphi, const double* phif, const double* phi, 
 
 constexpr int kMbarPolls = 1 << 22;  // bound of the bulk-copy wait
 
-// Last stage, after the update: residual partial of the tile, the CFL step of
-// the next step (fused), and in the last CTA the time advance (the residual
-// summed in a fixed order).  Tiles of finished ensemble instances join with
-// active = false so that the completion count stays whole.
+// Last stage, per tile after the update: residual partial of the tile and
+// its contribution to the CFL step of the next step (fused).  Tiles of
+// finished ensemble instances join with active = false (partial 0).
 template <class K>
-__device__ __forceinline__ void elem_last_stage(const StageArgs<typename K::T>& a, TimeCtl* c, double rsum,
-                                                bool active, const double* sC, double* sEig, int ne, int e0,
-                                                double* red) {
+__device__ __forceinline__ void elem_tile_tail(const StageArgs<typename K::T>& a, TimeCtl* c, int tile,
+                                               double rsum, bool active, const double* sC, double* sEig,
+                                               int ne, int e0, double* red, const double* sPv, double csz) {
   constexpr int M = K::M, NP = K::NP, MNP = K::MNP, NV = K::NV, BLOCK = K::BLOCK;
-  __shared__ bool amLast;
   const int tid = threadIdx.x;
   rsum = block_sum<BLOCK>(rsum, red);
-  if (tid == 0) a.partials[blockIdx.x] = rsum;
+  if (tid == 0) a.partials[tile] = rsum;
   if (a.fuse_cfl && active) {
-    __syncthreads();
     // eigenvalue at the cell mean (v = 0) and, on triangles, at the three
     // reference vertices (DGCell::computeMAXEV, DGCell.cc:1155-1207)
     for (int it = tid; it < ne * NV; it += BLOCK) {
@@ -152,7 +153,7 @@ __device__ __forceinline__ void elem_last_stage(const StageArgs<typename K::T>& 
 #pragma unroll
         for (int j = 0; j < M; ++j) val[j] = cc[j * NP] * a.tab.phi0;
       } else {
-        const double* pv = a.tab.phiv + (v - 1) * NP;
+        const double* pv = sPv + (v - 1) * NP;
 #pragma unroll
         for (int j = 0; j < M; ++j) {
           double acc = 0;
@@ -172,11 +173,22 @@ __device__ __forceinline__ void elem_last_stage(const StageArgs<typename K::T>& 
         const double b = sEig[tid * NV + v];
         am = (b > am ? b : am);
       }
-      dtl = a.mesh.csize[e0 + tid] * c->cfl / (am * (2. * K::ORDER + 1.0));
+      dtl = csz * c->cfl / (am * (2. * K::ORDER + 1.0));
     }
     dtl = block_min<BLOCK>(dtl, red);
     if (tid == 0) atomicMin(&c->dtmin_bits, (unsigned long long)__double_as_longlong(dtl));
   }
+}
+
+// Last stage, once per CTA: completion count; the last CTA advances the time
+// (residual summed over the ntiles tile partials in a fixed order) and, with
+// the fused CFL, finalizes the next step.
+template <class K>
+__device__ __forceinline__ void elem_finish(const StageArgs<typename K::T>& a, TimeCtl* c, int ntiles,
+                                            double* red) {
+  constexpr int BLOCK = K::BLOCK;
+  __shared__ bool amLast;
+  const int tid = threadIdx.x;
   if (tid == 0) {
     __threadfence();
     const unsigned v = atomicAdd(&a.gctl->blocks_done, 1u);
@@ -191,7 +203,7 @@ __device__ __forceinline__ void elem_last_stage(const StageArgs<typename K::T>& 
   }
   // single solver: residual in a fixed order (strided partial sums + tree)
   double r = 0.0;
-  for (unsigned b = tid; b < gridDim.x; b += BLOCK) r += ((volatile double*)a.partials)[b];
+  for (int b = tid; b < ntiles; b += BLOCK) r += ((volatile double*)a.partials)[b];
   r = block_sum<BLOCK>(r, red);
   if (tid == 0) {
     c->resid = r;
@@ -205,76 +217,26 @@ __device__ __forceinline__ void elem_last_stage(const StageArgs<typename K::T>& 
   }
 }
 
+// One tile, its inputs in shared memory: volume term, contraction with the
+// reference gradients, lift of the face slots, FP64 inverse mass and stage
+// combination, then the face-point traces of the new state.  sJi: J^{-1} in T
+// [TE][DIM*DIM]; sDet: |J| FP64 [TE]; sU0: u_n (stages 2, 3); sS: face slots
+// [NS][ROWS].  The last stage accumulates the residual into rsum.
 template <class K>
-__global__ void __launch_bounds__(K::BLOCK) elem_kernel(const __grid_constant__ StageArgs<typename K::T> a) {
+__device__ __forceinline__ void elem_tile(const StageArgs<typename K::T>& a, const TimeCtl* c, int tile, int e0,
+                                          int ne, const typename K::T* sT, double* sC, typename K::T* sG,
+                                          const typename K::T* sJi, const double* sDet, const double* sU0,
+                                          const typename K::T* sS, double& rsum) {
   using T = typename K::T;
   using L = ElemSmem<K>;
-  constexpr int M = K::M, NP = K::NP, NQ = K::NQ, DIM = K::DIM, TE = K::TE, BLOCK = K::BLOCK;
-  constexpr int MNP = K::MNP, NS = K::NS, KV = K::KV, LDK = K::LDK, ROWS = K::ROWS;
-  constexpr int NPP = L::NPP, DD = L::DD;
-  if (a.gctl->done) return;
-  extern __shared__ __align__(128) unsigned char smem_raw[];
-  T* sT = reinterpret_cast<T*>(smem_raw);
-  T* sDphi = sT + L::oDphi;
-  T* sPhif = sT + L::oPhif;
-  T* sPhi = sT + L::oPhi;
-  T* sQw = sT + L::oQw;
-  double* sC = reinterpret_cast<double*>(smem_raw + L::oCB);
-  T* sG = reinterpret_cast<T*>(smem_raw + L::oGB);
-  double* sJ = reinterpret_cast<double*>(smem_raw + L::oJB);
-  double* sEig = sJ + TE * DD;
-  __shared__ __align__(8) uint64_t bar;
-  __shared__ double red[BLOCK / 32];
-  __shared__ int s_fail;
-
+  constexpr int M = K::M, NP = K::NP, NQ = K::NQ, DIM = K::DIM;
+  constexpr int NS = K::NS, KV = K::KV, LDK = K::LDK, ROWS = K::ROWS;
+  constexpr int NPP = L::NPP;
+  const T* sDphi = sT + L::oDphi;
+  const T* sPhif = sT + L::oPhif;
+  const T* sPhi = sT + L::oPhi;
+  const T* sQw = sT + L::oQw;
   const int tid = threadIdx.x;
-  const int e0 = blockIdx.x * TE;
-  TimeCtl* c = a.ctl;
-  int eend = a.mesh.E;
-  if (a.cell_inst) {  // ensemble: the tile belongs to one instance
-    const int inst = a.cell_inst[e0];
-    c = a.ctl + inst;
-    eend = a.inst_end[inst];
-    if (c->done) {
-      if (a.stage == 3) elem_last_stage<K>(a, c, 0.0, false, nullptr, nullptr, 0, e0, red);
-      return;
-    }
-  }
-  const int ne = min(TE, eend - e0);
-  const uint32_t c_bytes = (uint32_t)(((size_t)ne * MNP * 8 + 15) / 16 * 16);
-
-  if (tid == 0) {
-    s_fail = 0;
-    mbar_init(&bar, 1);
-  }
-  __syncthreads();
-  if (tid == 0) {
-    mbar_arrive_expect_tx(&bar, (uint32_t)L::blob_bytes + (L::bulk_c ? c_bytes : 0u));
-    bulk_g2s(sT, a.tab.blob, (uint32_t)L::blob_bytes, &bar);
-    if constexpr (L::bulk_c) bulk_g2s(sC, a.C + (size_t)e0 * MNP, c_bytes, &bar);
-  }
-  if constexpr (!L::bulk_c) {
-    const double* src = a.C + (size_t)e0 * MNP;
-    for (int i = tid; i < ne * MNP; i += BLOCK) sC[i] = src[i];
-  }
-  const bool p0_mark = a.p0 && tid < ne && a.bad[e0 + tid];
-  for (int i = tid; i < ne * DD; i += BLOCK) {
-    const int e = i / DD, c = i - (i / DD) * DD;
-    sJ[i] = c < DIM * DIM ? (double)a.mesh.jinv[(size_t)(e0 + e) * DIM * DIM + c] : a.mesh.detjd[e0 + e];
-  }
-  if (tid == 0 && !mbar_wait(&bar, 0, kMbarPolls)) {
-    // record the failure, then wait once more (bounded) for the copies this
-    // CTA issued before its shared memory is released
-    s_fail = 1;
-    atomicAdd(&a.status->timeouts, 1);
-    mbar_wait(&bar, 0, kMbarPolls);
-  }
-  __syncthreads();
-  if (s_fail) return;
-  // P0 fallback: the face passes marked cells and zeroed their modes; the
-  // marks of this tile's cells are consumed here
-  if (p0_mark) a.bad[e0 + tid] = 0;
-  if (a.p0 && blockIdx.x == 0 && tid == 0) a.status->stage_bad = 0;
 
   // volume: fixed quadrature point per thread
   if (tid < K::EG * NQ) {
@@ -287,21 +249,20 @@ __global__ void __launch_bounds__(K::BLOCK) elem_kernel(const __grid_constant__ 
       T U[M];
 #pragma unroll
       for (int j = 0; j < M; ++j) {
-        double c[NP];
-        load_vec<double, NP>(sC + (e * M + j) * NP, c);
+        double cv[NP];
+        load_vec<double, NP>(sC + (e * M + j) * NP, cv);
         T acc = 0;
 #pragma unroll
-        for (int k = 0; k < NP; ++k) acc += phi[k] * (T)c[k];
+        for (int k = 0; k < NP; ++k) acc += phi[k] * (T)cv[k];
         U[j] = acc;
       }
       if (!is_physical<K::LAW, T>(a.law, U)) flag_nonphysical(a.status, e0 + e);
       T F[M][DIM];
       volume_flux<K::LAW, DIM, T>(a.law, U, F);
-      const double* Jd = sJ + e * DD;
       T J[DIM * DIM];
 #pragma unroll
-      for (int i = 0; i < DIM * DIM; ++i) J[i] = (T)Jd[i];
-      const T jw = (T)Jd[DIM * DIM] * w;
+      for (int i = 0; i < DIM * DIM; ++i) J[i] = sJi[e * DIM * DIM + i];
+      const T jw = (T)sDet[e] * w;
 #pragma unroll
       for (int j = 0; j < M; ++j)
 #pragma unroll
@@ -316,7 +277,6 @@ __global__ void __launch_bounds__(K::BLOCK) elem_kernel(const __grid_constant__ 
   __syncthreads();
 
   // contraction + lift + inverse mass + stage combination, one row per thread
-  double rsum = 0.0;
   const int row = tid;
   if (row < ne * M) {
     T acc[NPP];
@@ -331,10 +291,9 @@ __global__ void __launch_bounds__(K::BLOCK) elem_kernel(const __grid_constant__ 
 #pragma unroll
       for (int k = 0; k < NPP; ++k) acc[k] += gv * d[k];
     }
-    const T* sl = a.slots + (size_t)blockIdx.x * NS * ROWS + row;
 #pragma unroll 4
     for (int s = 0; s < NS; ++s) {
-      const T sv = __ldg(sl + (size_t)s * ROWS);
+      const T sv = sS[s * ROWS + row];
       T p[NPP];
       load_vec<T, NPP>(sPhif + s * NPP, p);
 #pragma unroll
@@ -347,22 +306,22 @@ __global__ void __launch_bounds__(K::BLOCK) elem_kernel(const __grid_constant__ 
     } else {
       const int e = row / M;
       // FP64 update in the reference's operation order (dt/|J| in FP64)
-      const double dtj = c->dt / sJ[e * DD + DIM * DIM];
+      const double dtj = c->dt / sDet[e];
       double* crow = sC + row * NP;
-      double c[NP];
-      load_vec<double, NP>(crow, c);
+      double cv[NP];
+      load_vec<double, NP>(crow, cv);
 #pragma unroll
       for (int k = 0; k < NP; ++k) {
         const double r = (double)acc[k];
         double out;
         if (a.stage == 1) {
-          a.U0out[gbase + k] = c[k];
-          out = c[k] + r * dtj;
+          a.U0out[gbase + k] = cv[k];
+          out = cv[k] + r * dtj;
         } else if (a.stage == 2) {
-          out = 0.25 * (c[k] + r * dtj + 3. * a.U0[gbase + k]);
+          out = 0.25 * (cv[k] + r * dtj + 3. * sU0[row * NP + k]);
         } else {
-          const double u0 = a.U0[gbase + k];
-          out = (2.0 * (c[k] + r * dtj) + u0) / 3.0;
+          const double u0 = sU0[row * NP + k];
+          out = (2.0 * (cv[k] + r * dtj) + u0) / 3.0;
           const double dd = out - u0;
           rsum += dd * dd;
         }
@@ -373,7 +332,7 @@ __global__ void __launch_bounds__(K::BLOCK) elem_kernel(const __grid_constant__ 
       T o[NP];
 #pragma unroll
       for (int k = 0; k < NP; ++k) o[k] = (T)crow[k];
-      T* tr = a.tr + (size_t)blockIdx.x * NS * ROWS + row;
+      T* tr = a.tr + (size_t)tile * NS * ROWS + row;
 #pragma unroll 4
       for (int s = 0; s < NS; ++s) {
         T p[NPP];
@@ -385,8 +344,122 @@ __global__ void __launch_bounds__(K::BLOCK) elem_kernel(const __grid_constant__ 
       }
     }
   }
+}
+
+// geometry of a tile inside the ElemSmem geometry area: |J| FP64 [TE], CFL
+// eigenvalues FP64 [TE][NV], J^{-1} T [TE][DIM*DIM]
+template <class K>
+struct GeoArea {
+  static constexpr size_t oDet = 0;
+  static constexpr size_t oEig = 8 * (size_t)K::TE;
+  static constexpr size_t oJi = oEig + 8 * (size_t)K::TE * K::NV;
+};
+
+// One CTA per tile of TE cells.  Used where the persistent kernel's 16-byte
+// alignment conditions do not hold.
+template <class K>
+__global__ void __launch_bounds__(K::BLOCK) elem_kernel(const __grid_constant__ StageArgs<typename K::T> a) {
+  using T = typename K::T;
+  using L = ElemSmem<K>;
+  using G = GeoArea<K>;
+  constexpr int MNP = K::MNP, NS = K::NS, DIM = K::DIM, TE = K::TE, BLOCK = K::BLOCK, ROWS = K::ROWS;
+  if (a.gctl->done) return;
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  T* sT = reinterpret_cast<T*>(smem_raw);
+  double* sC = reinterpret_cast<double*>(smem_raw + L::oCB);
+  T* sG = reinterpret_cast<T*>(smem_raw + L::oGB);
+  double* sDet = reinterpret_cast<double*>(smem_raw + L::oJB + G::oDet);
+  double* sEig = reinterpret_cast<double*>(smem_raw + L::oJB + G::oEig);
+  T* sJi = reinterpret_cast<T*>(smem_raw + L::oJB + G::oJi);
+  double* sU0 = reinterpret_cast<double*>(smem_raw + L::oUB);
+  T* sS = reinterpret_cast<T*>(smem_raw + L::oSB);
+  __shared__ __align__(8) uint64_t bar;
+  __shared__ double red[BLOCK / 32];
+  __shared__ int s_fail;
+
+  const int tid = threadIdx.x;
+  const int tile = blockIdx.x;
+  const int e0 = tile * TE;
+  TimeCtl* c = a.ctl;
+  int eend = a.mesh.E;
+  if (a.cell_inst) {  // ensemble: the tile belongs to one instance
+    const int inst = a.cell_inst[e0];
+    c = a.ctl + inst;
+    eend = a.inst_end[inst];
+    if (c->done) {
+      if (a.stage == 3) {
+        elem_tile_tail<K>(a, c, tile, 0.0, false, nullptr, nullptr, 0, e0, red, nullptr, 0.0);
+        elem_finish<K>(a, c, gridDim.x, red);
+      }
+      return;
+    }
+  }
+  const int ne = min(TE, eend - e0);
+  const uint32_t c_bytes = (uint32_t)(((size_t)ne * MNP * 8 + 15) / 16 * 16);
+
+  if (tid == 0) {
+    s_fail = 0;
+    mbar_init(&bar, 1);
+  }
+  __syncthreads();
+  // one mbarrier for every input of the tile: tables, state, u_n (stages 2
+  // and 3), face slots; the geometry is loaded by the threads meanwhile
+  const bool need_u0 = a.stage >= 2;
+  constexpr uint32_t s_bytes = (uint32_t)(NS * ROWS * sizeof(T));
+  const T* slot_src = a.slots + (size_t)tile * NS * ROWS;
+  if (tid == 0) {
+    uint32_t tx = (uint32_t)L::blob_bytes;
+    if constexpr (L::bulk_c) tx += c_bytes * (need_u0 ? 2u : 1u);
+    if constexpr (L::bulk_s) tx += s_bytes;
+    mbar_arrive_expect_tx(&bar, tx);
+    bulk_g2s(sT, a.tab.blob, (uint32_t)L::blob_bytes, &bar);
+    if constexpr (L::bulk_c) {
+      bulk_g2s(sC, a.C + (size_t)e0 * MNP, c_bytes, &bar);
+      if (need_u0) bulk_g2s(sU0, a.U0 + (size_t)e0 * MNP, c_bytes, &bar);
+    }
+    if constexpr (L::bulk_s) bulk_g2s(sS, slot_src, s_bytes, &bar);
+  }
+  if constexpr (!L::bulk_c) {
+    const double* src = a.C + (size_t)e0 * MNP;
+    for (int i = tid; i < ne * MNP; i += BLOCK) sC[i] = src[i];
+    if (need_u0) {
+      const double* u0 = a.U0 + (size_t)e0 * MNP;
+      for (int i = tid; i < ne * MNP; i += BLOCK) sU0[i] = u0[i];
+    }
+  }
+  if constexpr (!L::bulk_s) {
+    for (int i = tid; i < NS * ROWS; i += BLOCK) sS[i] = slot_src[i];
+  }
+  const bool p0_mark = a.p0 && tid < ne && a.bad[e0 + tid];
+  // the last stage's CFL inputs, fetched while the copies fly
+  __shared__ double sPv[(K::NV - 1) * K::NP + 1];
+  double csz = 0.0;
+  if (a.stage == 3 && a.fuse_cfl) {
+    if (tid < ne) csz = a.mesh.csize[e0 + tid];
+    for (int i = tid; i < (K::NV - 1) * K::NP; i += BLOCK) sPv[i] = a.tab.phiv[i];
+  }
+  for (int i = tid; i < ne * DIM * DIM; i += BLOCK) sJi[i] = a.mesh.jinv[(size_t)e0 * DIM * DIM + i];
+  for (int i = tid; i < ne; i += BLOCK) sDet[i] = a.mesh.detjd[e0 + i];
+  if (tid == 0 && !mbar_wait(&bar, 0, kMbarPolls)) {
+    // record the failure, then wait once more (bounded) for the copies this
+    // CTA issued before its shared memory is released
+    s_fail = 1;
+    atomicAdd(&a.status->timeouts, 1);
+    mbar_wait(&bar, 0, kMbarPolls);
+  }
+  __syncthreads();
+  if (s_fail) return;
+  // P0 fallback: the face passes marked cells and zeroed their modes; the
+  // marks of this tile's cells are consumed here
+  if (p0_mark) a.bad[e0 + tid] = 0;
+  if (a.p0 && blockIdx.x == 0 && tid == 0) a.status->stage_bad = 0;
+
+  double rsum = 0.0;
+  elem_tile<K>(a, c, tile, e0, ne, sT, sC, sG, sJi, sDet, sU0, sS, rsum);
   if (a.stage != 3) return;
-  elem_last_stage<K>(a, c, rsum, true, sC, sEig, ne, e0, red);
+  __syncthreads();
+  elem_tile_tail<K>(a, c, tile, rsum, true, sC, sEig, ne, e0, red, sPv, csz);
+  elem_finish<K>(a, c, gridDim.x, red);
 }
 
 }  // namespace dgp

@@ -24,6 +24,7 @@ cudaError_t ops_prepare() {
                                          static_cast<int>(smem));
     if (e != cudaSuccess) return e;
   }
+
   if constexpr (adjoint_built<K>()) {
     const size_t as = adj_elem_smem<K>();
     if (as > 48 * 1024)

@@ -30,6 +30,12 @@ __device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t by
       : "memory");
 }
 
+// orders this CTA's earlier generic-proxy accesses of shared memory before
+// later bulk (async-proxy) copies into it
+__device__ __forceinline__ void fence_proxy_async_smem() {
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+
 // waits for phase `parity` of the barrier; gives up after max_iters polls
 __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, int max_iters) {
   uint32_t ok = 0;
