@@ -325,8 +325,8 @@ static int build_solver(dgp_solver s, const std::vector<LawParams>& lps, int fie
     const int ia = left_internal(a), ic = left_internal(c);
     return ia != ic ? ia < ic : s->meshes[a.inst].lfL[a.f] < s->meshes[c.inst].lfL[c.f];
   });
-  std::vector<int> fel(2 * (size_t)Ftot), fcode(Ftot), bbid;
-  std::vector<double> fnrm(static_cast<size_t>(Ftot) * dim), fj(Ftot), bpts;
+  std::vector<int> fel(2 * (size_t)Ftot), fcode(Ftot), bbid, bpart;
+  std::vector<double> fnrm(static_cast<size_t>(Ftot) * dim), fj(Ftot), bpts, bpphi;
   int nb = 0;
   for (int k = 0; k < Ftot; ++k) {
     const HostMesh& m = s->meshes[faces[k].inst];
@@ -351,6 +351,27 @@ static int build_solver(dgp_solver s, const std::vector<LawParams>& lps, int fie
         }
         bpts.insert(bpts.end(), x, x + 3);
       }
+      // periodic partner: its left cell's basis at the mirrored points
+      // (DGBoundaryCell::setPeriodicBC, DGCell.cc:557-577)
+      const int pf = m.pface.empty() ? -1 : m.pface[f];
+      bpart.push_back(pf >= 0 ? s->f2i[ufo + m.eL[pf]] : -1);
+      std::vector<double> ph(static_cast<size_t>(t.nqf) * t.Np, 0.0);
+      if (pf >= 0) {
+        const int pe = m.eL[pf];
+        double X0[3], J[9], Ji[9];
+        cell_frame(m, pe, X0, J);
+        invert3(J, Ji);
+        for (int q = 0; q < t.nqf; ++q) {
+          const double* x = &bpts[bpts.size() - 3 * static_cast<size_t>(t.nqf) + 3 * q];
+          double xm[3] = {x[0], x[1], x[2]};
+          if (m.bid[f] == 510) xm[0] = -x[0];
+          else xm[1] = -x[1];
+          double d[3] = {xm[0] - X0[0], xm[1] - X0[1], xm[2] - X0[2]}, xi[3] = {0, 0, 0};
+          for (int r = 0; r < dim; ++r) xi[r] = Ji[0 * 3 + r] * d[0] + Ji[1 * 3 + r] * d[1] + Ji[2 * 3 + r] * d[2];
+          basis_eval(t, xi, &ph[static_cast<size_t>(q) * t.Np]);
+        }
+      }
+      bpphi.insert(bpphi.end(), ph.begin(), ph.end());
       ++nb;
     }
     fcode[k] = m.lfL[f] | ((m.eR[f] >= 0 ? m.lfR[f] : 0) << 4) | (m.rperm[f] << 8);
@@ -379,6 +400,8 @@ static int build_solver(dgp_solver s, const std::vector<LawParams>& lps, int fie
       (rc = s->upload_t(&b.fnrm, fnrm)) || (rc = s->upload_t(&b.fj, fj)) ||
       (rc = s->upload(&b.bpts, bpts.empty() ? std::vector<double>(3, 0.0) : bpts)) ||
       (rc = s->upload(&b.bbid, bbid.empty() ? std::vector<int>(1, 0) : bbid)) ||
+      (rc = s->upload(&b.bpart, bpart.empty() ? std::vector<int>(1, -1) : bpart)) ||
+      (rc = s->upload_t(&b.bpphi, bpphi.empty() ? std::vector<double>(1, 0.0) : bpphi)) ||
       (rc = s->upload_t(&b.phi, t.phi)) || (rc = s->upload_t(&b.dphi, t.dphi)) ||
       (rc = s->upload_t(&b.qw, t.qw)) || (rc = s->upload_t(&b.phif, t.phif)) ||
       (rc = s->upload_t(&b.fqw, t.fqw)) || (rc = s->upload(&b.qmap, t.qmap)) ||
@@ -1468,6 +1491,9 @@ int dgp_forward_checkpointed(dgp_solver s, double t0, double dt, int nsteps, int
   if (s->b.ninst) return fail(DGP_ERR_UNSUPPORTED, "the adjoint runs on a single solver");
   if (!s->ops.adj_stage) return fail(DGP_ERR_UNSUPPORTED, "no discrete adjoint for this law/flux");
   if (s->limiter == DGP_LIMITER_MOMENT) return fail(DGP_ERR_UNSUPPORTED, "adjoint with the limiter on");
+  for (const HostMesh& hm : s->meshes)
+    for (int pf : hm.pface)
+      if (pf >= 0) return fail(DGP_ERR_UNSUPPORTED, "adjoint on a mesh with periodic edges");
   DGP_CUDA(cudaSetDevice(s->device));
   AdjointState& a = s->adj;
   const int nseg = (nsteps + every - 1) / every;

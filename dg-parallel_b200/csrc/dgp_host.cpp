@@ -194,6 +194,30 @@ int build_faces(HostMesh& m, const std::vector<FaceKey>& bkeys_in, std::string& 
     for (int k = 0; k < 3; ++k) m.fn[3 * f + k] = n[k];
     m.fmeas[f] = meas;
   }
+  // periodic pairs (mMesh::setPeriodicBC, mMesh.cc:457-524): a boundary edge
+  // tagged 510 pairs with the first other 510 edge whose two vertices have the
+  // same y coordinates (within 1e-10, either order), 610 likewise with x
+  m.pface.assign(m.F, -1);
+  if (m.dim == 2) {
+    const double SN = 1.0e-10;
+    for (int f = 0; f < m.F; ++f) {
+      const int id = m.bid[f];
+      if (m.eR[f] >= 0 || (id != 510 && id != 610)) continue;
+      const int c = (id == 510) ? 1 : 0;
+      const double* v1 = &m.X[3 * m.fv[2 * f]];
+      const double* v2 = &m.X[3 * m.fv[2 * f + 1]];
+      for (int g = 0; g < m.F; ++g) {
+        if (g == f || m.eR[g] >= 0 || m.bid[g] != id) continue;
+        const double* a1 = &m.X[3 * m.fv[2 * g]];
+        const double* a2 = &m.X[3 * m.fv[2 * g + 1]];
+        if ((std::fabs(v1[c] - a1[c]) < SN && std::fabs(v2[c] - a2[c]) < SN) ||
+            (std::fabs(v1[c] - a2[c]) < SN && std::fabs(v2[c] - a1[c]) < SN)) {
+          m.pface[f] = g;
+          break;
+        }
+      }
+    }
+  }
   return DGP_OK;
 }
 

@@ -28,6 +28,7 @@ struct HostMesh {
   std::vector<int> rperm;    // right local face orientation w.r.t. the face frame
   std::vector<double> fn;    // F x 3 unit normal, outward from the left cell
   std::vector<double> fmeas; // F face length / area
+  std::vector<int> pface;    // F periodic partner face of a 510/610 boundary edge (-1: none)
 };
 
 // Reads a Gmsh v1 file; returns 0 or a DGP_ERR_* code with `err` set.

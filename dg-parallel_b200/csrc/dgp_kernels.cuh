@@ -116,6 +116,8 @@ struct DevMesh {
   const T* fj;        // F: |J_f|
   const double* bpts; // NB x NQF x 3 physical points of boundary faces
   const int* bbid;    // NB classification ids
+  const int* bpart;   // NB periodic partner cell (-1: none)
+  const T* bpphi;     // NB x NQF x NP partner basis at the mirrored points
 };
 
 template <typename T>
@@ -326,6 +328,12 @@ __device__ __forceinline__ void face_point(const StageArgs<typename K::T>& a, in
       flag_nonphysical(a.status, eR);
       if (a.p0) mark_p0(a, eR);
     }
+    numerical_flux<K::LAW, K::FLUX, DIM, T>(a.law, n, UL, UR, flux);
+  } else if (a.mesh.bpart[-eR - 1] >= 0) {
+    // periodic edge (DGCell.cc:687-705): the partner cell's trace at the
+    // mirrored point through the numerical flux; only the left cell gets it
+    const int b = -eR - 1, pe = a.mesh.bpart[b];
+    cell_trace<K>(a.C + (size_t)pe * MNP, a.mesh.bpphi + ((size_t)b * NQF + q) * NP, UR, RERUN && a.bad[pe]);
     numerical_flux<K::LAW, K::FLUX, DIM, T>(a.law, n, UL, UR, flux);
   } else {
     const int b = -eR - 1;

@@ -29,6 +29,8 @@ struct DeviceBuffers {
   void* fj = nullptr;
   double* bpts = nullptr;
   int* bbid = nullptr;
+  int* bpart = nullptr;
+  void* bpphi = nullptr;
   void* blob = nullptr;   // element-kernel tables in shared-memory layout
   int blob_bytes = 0;
   void* phi = nullptr;
@@ -94,6 +96,8 @@ inline StageArgs<T> make_args(const DeviceBuffers& b) {
   a.mesh.fj = static_cast<const T*>(b.fj);
   a.mesh.bpts = b.bpts;
   a.mesh.bbid = b.bbid;
+  a.mesh.bpart = b.bpart;
+  a.mesh.bpphi = static_cast<const T*>(b.bpphi);
   a.tab.blob = static_cast<const T*>(b.blob);
   a.tab.blob_bytes = b.blob_bytes;
   a.tab.phi = static_cast<const T*>(b.phi);

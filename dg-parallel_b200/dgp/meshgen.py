@@ -59,8 +59,13 @@ def _jitter(coords: np.ndarray, interior: np.ndarray, h: np.ndarray, jitter: flo
 
 def tri_square(nx: int, ny: int, x0: float = 0.0, x1: float = 1.0, y0: float = 0.0,
                y1: float = 1.0, jitter: float = 0.15, seed: int = 1,
-               boundary_tag: int = 1, domain_tag: int = 100) -> Mesh:
-    """Structured ``nx x ny`` rectangle grid cut into ``2*nx*ny`` jittered triangles."""
+               boundary_tag: int = 1, domain_tag: int = 100, side_tags=None) -> Mesh:
+    """Structured ``nx x ny`` rectangle grid cut into ``2*nx*ny`` jittered triangles.
+
+    ``side_tags`` = (bottom, right, top, left) classification ids overrides
+    ``boundary_tag`` per side; DG-Parallel pairs sides tagged 510 (left/right)
+    and 610 (bottom/top) as periodic (``mMesh::setPeriodicBC``, mMesh.cc:457-524).
+    """
     ii, jj = np.meshgrid(np.arange(nx + 1), np.arange(ny + 1), indexing="xy")
     hx = (x1 - x0) / nx
     hy = (y1 - y0) / ny
@@ -88,15 +93,20 @@ def tri_square(nx: int, ny: int, x0: float = 0.0, x1: float = 1.0, y0: float = 0
     cells[0::2] = t1
     cells[1::2] = t2
 
-    b = []
+    st = side_tags if side_tags is not None else (boundary_tag,) * 4
+    b, t = [], []
     for i in range(nx):
         b.append((vid(i, 0), vid(i + 1, 0)))
+        t.append(st[0])
         b.append((vid(i + 1, ny), vid(i, ny)))
+        t.append(st[2])
     for j in range(ny):
         b.append((vid(nx, j), vid(nx, j + 1)))
+        t.append(st[1])
         b.append((vid(0, j + 1), vid(0, j)))
+        t.append(st[3])
     bfaces = np.array(b, dtype=np.int64)
-    btags = np.full(len(b), boundary_tag, dtype=np.int64)
+    btags = np.array(t, dtype=np.int64)
     return Mesh(2, verts, cells, bfaces, btags, domain_tag)
 
 

@@ -66,6 +66,7 @@ struct or_solver {
   double* L;           /* limited state */
   unsigned char* trig; /* [E] trigger degree of the last limiter application */
   unsigned char* bad;  /* [E] P0 fallback marks */
+  int* pcell;          /* [F] periodic partner's cell of a boundary face (-1: none) */
 };
 
 static void build_limiter_tables(or_solver* s);
@@ -983,6 +984,45 @@ static void build_geometry(or_solver* s) {
   }
 }
 
+/* Periodic pairs (mMesh::setPeriodicBC, mMesh.cc:457-524): a boundary face
+ * tagged 510 pairs with the first other 510 face whose two vertices have the
+ * same y coordinates (1e-10, either order), 610 likewise with x; the partner
+ * trace is the partner face's left cell evaluated at the mirrored point
+ * (-x, y) for 510, (x, -y) for 610 (DGBoundaryCell::setPeriodicBC,
+ * DGCell.cc:557-577).  Triangles only, as in the reference. */
+static void build_periodic(or_solver* s) {
+  s->pcell = malloc((size_t)s->F * sizeof(int));
+  for (int f = 0; f < s->F; ++f) s->pcell[f] = -1;
+  if (s->dim != 2) return;
+  const double SN = 1.0e-10;
+  for (int f = 0; f < s->F; ++f) {
+    const int id = s->bid[f];
+    if (s->eR[f] >= 0 || (id != 510 && id != 610)) continue;
+    const int c = (id == 510) ? 1 : 0; /* coordinate that must match */
+    const double* v1 = s->X + 3 * s->fv[f * 2];
+    const double* v2 = s->X + 3 * s->fv[f * 2 + 1];
+    for (int g = 0; g < s->F; ++g) {
+      if (g == f || s->eR[g] >= 0 || s->bid[g] != id) continue;
+      const double* a1 = s->X + 3 * s->fv[g * 2];
+      const double* a2 = s->X + 3 * s->fv[g * 2 + 1];
+      if ((fabs(v1[c] - a1[c]) < SN && fabs(v2[c] - a2[c]) < SN) ||
+          (fabs(v1[c] - a2[c]) < SN && fabs(v2[c] - a1[c]) < SN)) {
+        const int pe = s->eL[g];
+        s->pcell[f] = pe;
+        for (int q = 0; q < s->nqf; ++q) {
+          const double* x = s->fx + (f * s->nqf + q) * 3;
+          double xm[3] = {x[0], x[1], x[2]}, xi[3];
+          if (id == 510) xm[0] = -x[0];
+          else xm[1] = -x[1];
+          to_ref(s, pe, xm, xi);
+          basis_eval(s, xi, s->trR + ((size_t)f * s->nqf + q) * s->Np);
+        }
+        break;
+      }
+    }
+  }
+}
+
 static int np_of(int dim, int p) {
   return dim == 2 ? (p + 1) * (p + 2) / 2 : (p + 1) * (p + 2) * (p + 3) / 6;
 }
@@ -1051,6 +1091,7 @@ or_solver* or_create(const char* msh_path, int law, int flux, int order, int fie
     }
   }
   build_geometry(s);
+  build_periodic(s);
   size_t n = (size_t)s->E * s->m * s->Np;
   s->C = calloc(n, sizeof(double));
   s->R = calloc(n, sizeof(double));
@@ -1072,7 +1113,7 @@ void or_destroy(or_solver* s) {
   free(s->lfL); free(s->lfR); free(s->bid); free(s->jac); free(s->jinv); free(s->det);
   free(s->csize); free(s->fn); free(s->fmeas); free(s->trL); free(s->trR); free(s->fx);
   free(s->fjw); free(s->C); free(s->R); free(s->soln);
-  free(s->nb); free(s->bbc); free(s->L); free(s->trig); free(s->bad);
+  free(s->nb); free(s->bbc); free(s->L); free(s->trig); free(s->bad); free(s->pcell);
   free(s);
 }
 
@@ -1188,6 +1229,9 @@ static void assemble(or_solver* s, const double* C, double t, double* R) {
       interp(pl, C + (size_t)eL * m * Np, m, Np, UL);
       if (eR >= 0) {
         interp(pr, C + (size_t)eR * m * Np, m, Np, UR);
+        riemann_flux(s, n, x, UL, UR, flux);
+      } else if (s->pcell[f] >= 0) { /* periodic: the partner's trace (DGCell.cc:687-705) */
+        interp(pr, C + (size_t)s->pcell[f] * m * Np, m, Np, UR);
         riemann_flux(s, n, x, UL, UR, flux);
       } else {
         boundary_flux(s, s->bid[f], n, x, t, UL, flux);

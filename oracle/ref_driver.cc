@@ -359,6 +359,13 @@ int main(int argc, char** argv) {
     DGBoundaryCell* bc = new DGBoundaryCell(ent, new MeshMapping(ent), &gi);
     ent->setCell(bc);
   }
+  // partner traces of periodic faces (DGAnalysis::setPeriodicBC, DGPref.cc:1389-1403)
+  for (mMesh::iter it = mesh->begin(dim - 1); it != mesh->end(dim - 1); ++it) {
+    mEntity* ent = *it;
+    const int id = ent->getClassification()->getId();
+    if ((id == 510 || id == 610) && ent->getAttachedEntity(TYPE_CELL))
+      ((DGBoundaryCell*)ent->getCell())->setPeriodicBC();
+  }
   const int Np = byFile[0]->fSize;
 
   if (!P.conn.empty()) {

@@ -24,6 +24,7 @@ SINE = params(amplitude=0.25)
 SCALAR3D = params(velocity=(1.0, 0.5, 0.25), center=(0.5, 0.5, 0.5), width=0.05)
 PULSE3D = params(velocity=(1.0, 0.5, 0.25), center=(0.5, 0.5, 0.5), width=0.05, gamma=1.4)
 TM110 = params(cavity=1.0)
+SCALAR_PERIODIC = params(velocity=(1.0, 0.5, 0.0), center=(0.2, -0.1, 0.0), width=0.1)
 
 # golden case -> (law, flux, field, order, params)
 GOLDEN_CASES = {
@@ -40,6 +41,9 @@ GOLDEN_CASES = {
     "scalar_tet_p2": (dgp.LAW_SCALAR, dgp.FLUX_UPWIND, dgp.FIELD_GAUSS3D, 2, SCALAR3D),
     "euler3d_p1": (dgp.LAW_EULER3D, dgp.FLUX_GODUNOV, dgp.FIELD_PULSE3D, 1, PULSE3D),
     "euler3d_p2": (dgp.LAW_EULER3D, dgp.FLUX_GODUNOV, dgp.FIELD_PULSE3D, 2, PULSE3D),
+    # periodic edges (510 left/right, 610 bottom/top) on [-1,1]^2
+    "scalar_periodic_p2": (dgp.LAW_SCALAR, dgp.FLUX_UPWIND, dgp.FIELD_GAUSS, 2, SCALAR_PERIODIC),
+    "burgers_periodic_p3": (dgp.LAW_BURGERS2D, dgp.FLUX_CENTRAL, dgp.FIELD_SINE, 3, SINE),
 }
 
 # Relative tolerance (max abs difference / max abs value) of the oracle -- exact

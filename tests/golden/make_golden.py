@@ -13,7 +13,7 @@ case, the mesh file and an .npz with:
 * ``log``    per step: dt, time, residual
 
 The reference run uses one worker thread so that stage times are honoured (see
-oracle/ref_driver.cc).  Usage: python tests/golden/make_golden.py
+oracle/ref_driver.cc).  Usage: python tests/golden/make_golden.py [case ...]
 """
 from __future__ import annotations
 
@@ -34,6 +34,7 @@ DRIVER = os.path.join(ROOT, "oracle", "_ref", "ref_driver")
 # name: (mesh builder, driver arguments, steps)
 SQUARE = dict(nx=4, ny=4, seed=1)
 VORTEX_BOX = dict(nx=4, ny=4, x0=0.0, x1=10.0, y0=0.0, y1=10.0, seed=2)
+PERIODIC_BOX = dict(nx=5, ny=4, x0=-1.0, x1=1.0, y0=-1.0, y1=1.0, seed=7, side_tags=(610, 510, 610, 510))
 CASES = {
     "scalar_tri_p1": ("tri", SQUARE, ["--case", "gauss", "--order", "1"], 3),
     "scalar_tri_p2": ("tri", SQUARE, ["--case", "gauss", "--order", "2"], 3),
@@ -54,6 +55,10 @@ CASES = {
     "euler3d_p2": ("tet", dict(n=2, seed=3), ["--case", "pulse3d", "--order", "2", "--ax", "1",
                                                "--ay", "0.5", "--az", "0.25", "--cx", "0.5",
                                                "--cy", "0.5", "--cz", "0.5", "--s", "0.05"], 3),
+    # periodic in x (sides tagged 510) and y (610) on [-1,1]^2
+    "scalar_periodic_p2": ("tri", PERIODIC_BOX, ["--case", "gauss", "--order", "2", "--cx", "0.2",
+                                                  "--cy", "-0.1", "--s", "0.1"], 4),
+    "burgers_periodic_p3": ("tri", PERIODIC_BOX, ["--case", "sine", "--order", "3", "--amp", "0.25"], 4),
 }
 
 
@@ -85,7 +90,10 @@ def run_case(name, kind, margs, dargs, steps):
 def main():
     if not os.path.exists(DRIVER):
         sys.exit("build the reference first: make -C oracle ref")
+    only = set(sys.argv[1:])  # case names (default: all)
     for name, (kind, margs, dargs, steps) in CASES.items():
+        if only and name not in only:
+            continue
         run_case(name, kind, margs, dargs, steps)
         print("wrote", name)
 
