@@ -179,6 +179,9 @@ def main():
                     help="only the discrete-adjoint measurement (Euler vortex 128x128x2 P2, 400 steps)")
     ap.add_argument("--profile-case", choices=["fp64", "mixed"], default=None,
                     help="only set up the workload and run --warmup + --steps steps (for ncu)")
+    ap.add_argument("--block", type=int, default=0, choices=[0, 64, 128, 256],
+                    help="--profile-case: tile shape (threads) of the element and face kernels "
+                         "(0: the autotuner's pick, as the bench line)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
@@ -485,16 +488,31 @@ def adjoint_bench(n=128, order=2, nsteps=400, every=20, nrec=64, ndir=16, eps=1e
             e1.synchronize()
             return r, e0.elapsed_time(e1)
 
+        # warm-up of both modes: every buffer (checkpoints, the recorded
+        # stage states, adjoint vectors) is allocated outside the timed runs
+        s.forward_checkpointed(0.0, dt, nsteps, every)
+        s.backward()
+        s.set_state(u0)
+        s.forward_checkpointed(0.0, dt, nsteps, 0)
+        s.backward()
         # plain forward solve: the same nsteps fixed-dt steps, no checkpoints
-        s.forward_checkpointed(0.0, dt, 4, 4)  # warm-up
         s.set_state(u0)
         _, t_plain = timed(lambda: s.forward_checkpointed(0.0, dt, nsteps, nsteps))
         s.set_state(u0)
         J, t_fwd = timed(lambda: s.forward_checkpointed(0.0, dt, nsteps, every))
         g, t_bwd = timed(lambda: s.backward())
         grads[name] = g
+        # every stage state kept in HBM (3 x nsteps states), no recompute
+        s.set_state(u0)
+        _, t_fwd_rec = timed(lambda: s.forward_checkpointed(0.0, dt, nsteps, 0))
+        g_rec, t_bwd_rec = timed(lambda: s.backward())
         out[name] = {"J": J, "forward_ms": t_plain, "forward_checkpointed_ms": t_fwd, "backward_ms": t_bwd,
-                     "gradient_over_forward": (t_fwd + t_bwd) / t_plain, "backward_over_forward": t_bwd / t_plain}
+                     "gradient_over_forward": (t_fwd + t_bwd) / t_plain, "backward_over_forward": t_bwd / t_plain,
+                     "recorded": {"stage_states_gb": 3 * nsteps * u0.nbytes / 1e9, "forward_ms": t_fwd_rec,
+                                  "backward_ms": t_bwd_rec, "backward_over_forward": t_bwd_rec / t_plain,
+                                  "gradient_over_forward": (t_fwd_rec + t_bwd_rec) / t_plain,
+                                  "gradient_equals_checkpointed": bool(np.array_equal(g_rec, g)),
+                                  "gradient_max_rel_diff": float(np.abs(g_rec - g).max() / np.abs(g).max())}}
         s.close()
     # central differences of the FP64 forward map
     s = dgp.Solver(mesh, law, order, dgp.FP64)
@@ -528,11 +546,16 @@ def profile_case(args):
     m = make_mesh()
     mesh = dgp.Mesh.from_arrays(2, m.vertices, m.cells, 100, m.bfaces, m.btags)
     law = dgp.Law(dgp.LAW_EULER2D, dgp.FLUX_ROE, dgp.FIELD_VORTEX, vortex_params())
-    s = dgp.Solver(mesh, law, 3, dgp.FP64 if args.profile_case == "fp64" else dgp.MIXED)
+    prec = dgp.FP64 if args.profile_case == "fp64" else dgp.MIXED
+    if args.block:
+        dgp.tune_set(dgp.LAW_EULER2D, dgp.FLUX_ROE, 2, 3, prec, m.cells.shape[0], args.block)
+    else:
+        dgp.autotune(mesh, law, 3, prec, 0, iters=5)
+    s = dgp.Solver(mesh, law, 3, prec)
     t, _ = s.run(0.0, 0.0, 0.1, args.warmup)
     t, n = s.run(t, 0.0, 0.1, args.steps)
     s.synchronize()
-    print(f"profile case {args.profile_case}: {n} steps, t = {t:.6e}")
+    print(f"profile case {args.profile_case}: {n} steps, t = {t:.6e}, block {s.block()[0]}")
     return 0
 
 

@@ -37,8 +37,8 @@ struct AdjArgs {
   double* acc;         // running sum of the reversed stages (read and/or written)
   double ca, cb, cc, cd, ce;
   double dt;
-  const double* t_seg; // device: time of the first step of the segment
-  double t_offset;     // stage time = *t_seg + t_offset
+  const double* t_seg; // device: time at the start of the step
+  double t_factor;     // stage time = *t_seg + t_factor * dt (as the forward stage)
 };
 
 // input directions per dual-number pass of the face Jacobians
@@ -126,7 +126,7 @@ __global__ void __launch_bounds__(K::FACE_BLOCK) adj_face_kernel(const __grid_co
     using D = Dual<T, W>;
     const int b = -eR - 1;
     const double* x = m.bpts + ((size_t)b * NQF + q) * 3;
-    const double time = *a.t_seg + a.t_offset;
+    const double time = __fma_rn(a.t_factor, a.dt, *a.t_seg);
 #pragma unroll 1
     for (int c0 = 0; c0 < M; c0 += W) {
       D dl[M], nd[DIM], F[M];

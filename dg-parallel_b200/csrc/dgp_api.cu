@@ -96,8 +96,10 @@ __global__ void mark_clock(TimeCtl* c) {
 }
 
 // controls of one adjoint segment: time and step of the forward recompute,
-// the segment's start time for the adjoint kernels (values travel as kernel
-// parameters, so consecutive segments queued without a host sync do not race)
+// a step's start time for the fixed-step forward, its recomputation and the
+// reversed stages: t0 + k dt from the host for step k, so all three see the
+// same boundary times bit for bit (values travel as kernel parameters, so
+// steps queued without a host sync do not race)
 __global__ void set_segment_time(TimeCtl* c, double t, double dt, double* t_seg) {
   c->t = t;
   c->dt = dt;
@@ -197,10 +199,10 @@ static int setup_limiter(dgp_solver s) {
   DeviceBuffers& b = s->b;
   int rc = DGP_OK;
   if ((rc = s->upload(&b.nb, nb)) || (rc = s->upload(&b.lgeo, geo)) || (rc = s->upload(&b.limD, D)) ||
-      (rc = s->upload(&b.limDinv, Dinv)) || (rc = s->alloc(&b.trig, static_cast<size_t>(Etot))) ||
-      (rc = s->alloc(&b.L, s->state_count())))
+      (rc = s->upload(&b.limDinv, Dinv)) || (rc = s->alloc(&b.trig, static_cast<size_t>(Etot) * b.M)) ||
+      (rc = s->alloc(&b.lbig, static_cast<size_t>(Etot) * b.M)) || (rc = s->alloc(&b.lmo, s->state_count())))
     return rc;
-  DGP_CUDA(cudaMemset(b.trig, 0, Etot));
+  DGP_CUDA(cudaMemset(b.trig, 0, static_cast<size_t>(Etot) * b.M));
   return DGP_OK;
 }
 
@@ -694,22 +696,31 @@ int dgp_project(dgp_solver s, double t) {
   return DGP_OK;
 }
 
-// host FP64 [cell][field][mode] in file order <-> device state in internal order
+// host FP64 [cell][field][mode] in file order <-> device state in internal order:
+// one copy of the whole array through the state-sized staging buffer, the
+// reordering by a gather kernel on the solver's stream
 static int host_to_state(dgp_solver s, const double* in, void* dst) {
-  const size_t mnp = static_cast<size_t>(s->b.M) * s->b.NP, n = s->state_count();
-  std::vector<double> tmp(n);
-  for (int i = 0; i < s->b.E; ++i)
-    std::memcpy(&tmp[i * mnp], &in[static_cast<size_t>(s->i2f[i]) * mnp], mnp * 8);
-  DGP_CUDA(cudaMemcpy(dst, tmp.data(), n * 8, cudaMemcpyHostToDevice));
+  const int mnp = s->b.M * s->b.NP;
+  const size_t n = s->state_count();
+  DGP_CUDA(cudaMemcpyAsync(s->b.scratch, in, n * 8, cudaMemcpyHostToDevice, s->stream));
+  const int grid = static_cast<int>((n + 255) / 256);
+  gather_cells<double, double><<<grid, 256, 0, s->stream>>>(static_cast<const double*>(s->b.scratch),
+                                                            static_cast<double*>(dst), s->d_i2f, s->b.E, mnp);
+  DGP_CUDA(cudaGetLastError());
+  DGP_CUDA(cudaStreamSynchronize(s->stream));
   return DGP_OK;
 }
 
 static int state_to_host(dgp_solver s, const void* src, double* out) {
-  const size_t mnp = static_cast<size_t>(s->b.M) * s->b.NP, n = s->state_count();
-  std::vector<double> tmp(n);
-  DGP_CUDA(cudaMemcpy(tmp.data(), src, n * 8, cudaMemcpyDeviceToHost));
-  for (int i = 0; i < s->b.E; ++i)
-    std::memcpy(&out[static_cast<size_t>(s->i2f[i]) * mnp], &tmp[i * mnp], mnp * 8);
+  const int mnp = s->b.M * s->b.NP;
+  const size_t n = s->state_count();
+  const int grid = static_cast<int>((n + 255) / 256);
+  gather_cells<double, double><<<grid, 256, 0, s->stream>>>(static_cast<const double*>(src),
+                                                            static_cast<double*>(s->b.scratch), s->d_f2i, s->b.E,
+                                                            mnp);
+  DGP_CUDA(cudaGetLastError());
+  DGP_CUDA(cudaMemcpyAsync(out, s->b.scratch, n * 8, cudaMemcpyDeviceToHost, s->stream));
+  DGP_CUDA(cudaStreamSynchronize(s->stream));
   return DGP_OK;
 }
 
@@ -824,24 +835,33 @@ int dgp_run(dgp_solver s, double t0, double tend, double cfl, int max_steps, dou
     if (steps_out) *steps_out = 0;
     return DGP_OK;
   }
-  if (!s->graph) {
-    // K steps per graph; finished steps turn the remaining kernels into no-ops
-    const int K = 8;
+  // K steps per graph; finished steps turn the remaining kernels into no-ops.
+  // The last steps of a run with a step limit go through a one-step graph.
+  const int K = 8;
+  auto capture = [&](int steps, cudaGraphExec_t* out) -> int {
     cudaGraph_t g;
     DGP_CUDA(cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal));
-    for (int k = 0; k < K; ++k) launch_step(s, 1);
+    for (int k = 0; k < steps; ++k) launch_step(s, 1);
     DGP_CUDA(cudaStreamEndCapture(s->stream, &g));
-    cudaError_t e = cudaGraphInstantiate(&s->graph, g, 0);
+    cudaError_t e = cudaGraphInstantiate(out, g, 0);
     cudaGraphDestroy(g);
     if (e != cudaSuccess) return fail(DGP_ERR_CUDA, std::string("graph: ") + cudaGetErrorString(e));
+    return DGP_OK;
+  };
+  const bool tail = max_steps > 0 && max_steps % K != 0;
+  if (!s->graph) {
+    if (int rc = capture(K, &s->graph)) return rc;
     s->graph_steps = K;
   }
+  if (tail && !s->graph1)
+    if (int rc = capture(1, &s->graph1)) return rc;
   if (int rc = set_ctl(s, t0, 0.0, tend, cfl, max_steps)) return rc;
   s->ops.cfl(s->b, s->stream);
   DGP_CUDA(cudaGetLastError());
-  TimeCtl c;
+  TimeCtl c{};
   for (long long guard = 0;; ++guard) {
-    DGP_CUDA(cudaGraphLaunch(s->graph, s->stream));
+    const bool one = tail && max_steps - c.steps < K;
+    DGP_CUDA(cudaGraphLaunch(one ? s->graph1 : s->graph, s->stream));
     if (int rc = read_ctl(s, &c)) return rc;
     if (c.done) break;
     if (!std::isfinite(c.dt) || !(c.dt > 0))
@@ -872,18 +892,29 @@ int dgp_limiter_triggers(dgp_solver s, unsigned char* out) {
     std::memset(out, 0, E);
     return DGP_OK;
   }
-  std::vector<unsigned char> t(E);
-  DGP_CUDA(cudaMemcpy(t.data(), s->b.trig, E, cudaMemcpyDeviceToHost));
-  for (int i = 0; i < E; ++i) out[s->i2f[i]] = t[i];
+  // per row on the device; a cell's trigger is the lowest over its fields
+  const int M = s->b.M;
+  std::vector<unsigned char> t(static_cast<size_t>(E) * M);
+  DGP_CUDA(cudaMemcpy(t.data(), s->b.trig, t.size(), cudaMemcpyDeviceToHost));
+  // 0 (untouched) maps to 255 so that the minimum over the fields is the
+  // lowest limited degree
+  const int* i2f = s->i2f.data();
+  const unsigned char* tp = t.data();
+  if (M == 1) {
+    for (int i = 0; i < E; ++i) out[i2f[i]] = tp[i];
+  } else {
+    for (int i = 0; i < E; ++i) {
+      unsigned v = 255;
+      for (int j = 0; j < M; ++j) v = std::min(v, (unsigned)(unsigned char)(tp[static_cast<size_t>(i) * M + j] - 1));
+      out[i2f[i]] = static_cast<unsigned char>(v + 1);
+    }
+  }
   return DGP_OK;
 }
 
 int dgp_set_p0_fallback(dgp_solver s, int on) {
   if (!s) return fail(DGP_ERR_INVALID, "null solver");
-  if (s->graph) {
-    cudaGraphExecDestroy(s->graph);
-    s->graph = nullptr;
-  }
+  s->drop_graphs();
   s->b.p0 = on ? 1 : 0;
   return DGP_OK;
 }
@@ -1486,8 +1517,24 @@ int dgp_receiver_values(dgp_solver s, double* rho, double* J) {
   return DGP_OK;
 }
 
+// one SSP-RK3 step from X back into X, keeping u_n, u1, u2 in S (three
+// consecutive states)
+static void step_keeping_stages(dgp_solver s, double* X, double* S, size_t ns) {
+  DeviceBuffers b = s->b;
+  b.U0 = S;
+  b.C = X;
+  b.Cout = S + ns;
+  s->ops.stage(b, 1, 0.0, 0, s->stream);
+  b.C = S + ns;
+  b.Cout = S + 2 * ns;
+  s->ops.stage(b, 2, 1.0, 0, s->stream);
+  b.C = S + 2 * ns;
+  b.Cout = X;
+  s->ops.stage(b, 3, 0.5, 0, s->stream);
+}
+
 int dgp_forward_checkpointed(dgp_solver s, double t0, double dt, int nsteps, int every, double* J) {
-  if (!s || !(dt > 0) || nsteps <= 0 || every <= 0) return fail(DGP_ERR_INVALID, "bad argument");
+  if (!s || !(dt > 0) || nsteps <= 0 || every < 0) return fail(DGP_ERR_INVALID, "bad argument");
   if (s->b.ninst) return fail(DGP_ERR_UNSUPPORTED, "the adjoint runs on a single solver");
   if (!s->ops.adj_stage) return fail(DGP_ERR_UNSUPPORTED, "no discrete adjoint for this law/flux");
   if (s->limiter == DGP_LIMITER_MOMENT) return fail(DGP_ERR_UNSUPPORTED, "adjoint with the limiter on");
@@ -1496,8 +1543,14 @@ int dgp_forward_checkpointed(dgp_solver s, double t0, double dt, int nsteps, int
       if (pf >= 0) return fail(DGP_ERR_UNSUPPORTED, "adjoint on a mesh with periodic edges");
   DGP_CUDA(cudaSetDevice(s->device));
   AdjointState& a = s->adj;
+  // every == 0: one segment whose stage states are all kept (no recompute)
+  const bool record = every == 0;
+  if (record) every = nsteps;
   const int nseg = (nsteps + every - 1) / every;
   if (int rc = adj_buffer(s, &a.ckpt, &a.ckpt_states, static_cast<size_t>(nseg) + 1)) return rc;
+  if (record)
+    if (int rc = adj_buffer(s, &a.store, &a.store_states, static_cast<size_t>(3) * nsteps)) return rc;
+  a.recorded = record;
   if (!a.t_seg && (s->alloc(&a.t_seg, 1) != DGP_OK)) return DGP_ERR_NOMEM;
   a.nsteps = nsteps;
   a.every = every;
@@ -1507,12 +1560,19 @@ int dgp_forward_checkpointed(dgp_solver s, double t0, double dt, int nsteps, int
   const size_t ns = s->state_count(), bytes = ns * 8;
   const int p0 = s->b.p0;
   s->b.p0 = 0;  // the adjoint differentiates the plain operator
-  set_segment_time<<<1, 1, 0, s->stream>>>(s->b.ctl, t0, dt, a.t_seg);
   for (int seg = 0; seg < nseg; ++seg) {
     DGP_CUDA(cudaMemcpyAsync(a.ckpt + static_cast<size_t>(seg) * ns, s->b.C, bytes, cudaMemcpyDeviceToDevice,
                              s->stream));
     const int len = std::min(every, nsteps - seg * every);
-    for (int k = 0; k < len; ++k) launch_step(s, 0);
+    double* X = static_cast<double*>(s->b.C);
+    for (int k = 0; k < len; ++k) {
+      const double tk = t0 + static_cast<double>(seg * every + k) * dt;
+      set_segment_time<<<1, 1, 0, s->stream>>>(s->b.ctl, tk, dt, a.t_seg);
+      if (record)
+        step_keeping_stages(s, X, a.store + static_cast<size_t>(k) * 3 * ns, ns);
+      else
+        launch_step(s, 0);
+    }
   }
   DGP_CUDA(cudaMemcpyAsync(a.ckpt + static_cast<size_t>(nseg) * ns, s->b.C, bytes, cudaMemcpyDeviceToDevice,
                            s->stream));
@@ -1557,30 +1617,20 @@ int dgp_backward(dgp_solver s, const double* dJ_duT, double* dJ_du0) {
   double* X = static_cast<double*>(s->b.C);
   for (int seg = a.nseg - 1; seg >= 0; --seg) {
     const int len = std::min(a.every, a.nsteps - seg * a.every);
-    const double tseg = a.t0 + static_cast<double>(seg) * a.every * a.dt;
-    // recompute the segment from its checkpoint, keeping every stage state
-    DGP_CUDA(cudaMemcpyAsync(X, a.ckpt + static_cast<size_t>(seg) * ns, bytes, cudaMemcpyDeviceToDevice,
-                             s->stream));
-    s->ops.trace(s->b, nullptr, s->stream);
-    set_segment_time<<<1, 1, 0, s->stream>>>(s->b.ctl, tseg, a.dt, a.t_seg);
-    for (int j = 0; j < len; ++j) {
-      double* S0 = a.store + (static_cast<size_t>(j) * 3 + 0) * ns;
-      double* S1 = a.store + (static_cast<size_t>(j) * 3 + 1) * ns;
-      double* S2 = a.store + (static_cast<size_t>(j) * 3 + 2) * ns;
-      DeviceBuffers b = s->b;
-      b.U0 = S0;
-      b.C = X;
-      b.Cout = S1;
-      s->ops.stage(b, 1, 0.0, 0, s->stream);
-      b.C = S1;
-      b.Cout = S2;
-      s->ops.stage(b, 2, 1.0, 0, s->stream);
-      b.C = S2;
-      b.Cout = X;
-      s->ops.stage(b, 3, 0.5, 0, s->stream);
+    auto step_time = [&](int j) { return a.t0 + static_cast<double>(seg * a.every + j) * a.dt; };
+    if (!a.recorded) {
+      // recompute the segment from its checkpoint, keeping every stage state
+      DGP_CUDA(cudaMemcpyAsync(X, a.ckpt + static_cast<size_t>(seg) * ns, bytes, cudaMemcpyDeviceToDevice,
+                               s->stream));
+      s->ops.trace(s->b, nullptr, s->stream);
+      for (int j = 0; j < len; ++j) {
+        set_segment_time<<<1, 1, 0, s->stream>>>(s->b.ctl, step_time(j), a.dt, a.t_seg);
+        step_keeping_stages(s, X, a.store + static_cast<size_t>(j) * 3 * ns, ns);
+      }
     }
     // reversed steps
     for (int j = len - 1; j >= 0; --j) {
+      set_segment_time<<<1, 1, 0, s->stream>>>(s->b.ctl, step_time(j), a.dt, a.t_seg);
       DeviceBuffers b = s->b;
       AdjStage g{};
       g.dt = a.dt;
@@ -1595,7 +1645,7 @@ int dgp_backward(dgp_solver s, const double* dJ_duT, double* dJ_du0) {
       g.cc = 0.0;
       g.cd = 0.0;
       g.ce = 1.0 / 3.0;
-      g.t_offset = (j + 0.5) * a.dt;
+      g.t_factor = 0.5;
       s->ops.adj_stage(b, g, s->stream);
       // u2 = (u1 + dt L(u1) + 3 u) / 4
       b.C = a.store + (static_cast<size_t>(j) * 3 + 1) * ns;
@@ -1606,7 +1656,7 @@ int dgp_backward(dgp_solver s, const double* dJ_duT, double* dJ_du0) {
       g.cc = 0.0;
       g.cd = 1.0;
       g.ce = 0.75;
-      g.t_offset = (j + 1.0) * a.dt;
+      g.t_factor = 1.0;
       s->ops.adj_stage(b, g, s->stream);
       // u1 = u + dt L(u)
       b.C = a.store + (static_cast<size_t>(j) * 3 + 0) * ns;
@@ -1617,7 +1667,7 @@ int dgp_backward(dgp_solver s, const double* dJ_duT, double* dJ_du0) {
       g.cc = 1.0;
       g.cd = 0.0;
       g.ce = 0.0;
-      g.t_offset = j * a.dt;
+      g.t_factor = 0.0;
       s->ops.adj_stage(b, g, s->stream);
     }
   }

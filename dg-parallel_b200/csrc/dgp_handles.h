@@ -50,6 +50,7 @@ struct AdjointState {
   double* acc = nullptr;
   double* t_seg = nullptr;  // device scalar
   bool ready = false;       // a forward pass is recorded
+  bool recorded = false;    // every stage state of the forward pass is kept (no recompute)
   // receivers: J = sum_r (rho(x_r) - obs_r)^2
   int nrec = 0;
   int* rcell = nullptr;
@@ -73,11 +74,17 @@ struct dgp_solver_s {
   int* d_i2f = nullptr;
   int* d_f2i = nullptr;
   std::vector<void*> allocs;
-  cudaGraphExec_t graph = nullptr;
+  cudaGraphExec_t graph = nullptr;   // graph_steps SSP-RK3 steps
+  cudaGraphExec_t graph1 = nullptr;  // one step (the tail of a run with a step limit)
   int graph_steps = 0;
   dgp::TimeCtl* h_ctl = nullptr;  // pinned, 2 entries
-  ~dgp_solver_s() {
+  void drop_graphs() {
     if (graph) cudaGraphExecDestroy(graph);
+    if (graph1) cudaGraphExecDestroy(graph1);
+    graph = graph1 = nullptr;
+  }
+  ~dgp_solver_s() {
+    drop_graphs();
     for (void* p : allocs) cudaFree(p);
     if (h_ctl) cudaFreeHost(h_ctl);
     if (stream) cudaStreamDestroy(stream);

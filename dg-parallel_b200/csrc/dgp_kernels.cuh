@@ -287,9 +287,60 @@ __global__ void __launch_bounds__(K::BLOCK) trace_kernel(const __grid_constant__
   }
 }
 
-// One face point: traces of both sides, numerical (or boundary) flux, the two
-// face slots.  RERUN: second pass of the P0 fallback, where the traces of
-// marked cells are their means.
+// One face point once its traces are in registers: non-physical checks (P0
+// marks), numerical, periodic or boundary flux, the two face slots.  UR holds
+// the right cell's trace at its point qR for interior faces.  RERUN: second
+// pass of the P0 fallback (no checks; a periodic partner marked bad gives its
+// mean).
+template <class K, bool RERUN, bool ENS>
+__device__ __forceinline__ void face_finish(const StageArgs<typename K::T>& a, int f, int q, int eL, int eR,
+                                            int inst, int lfL, int lfR, int qR, const typename K::T (&n)[K::DIM],
+                                            typename K::T jw, const typename K::T (&UL)[K::M],
+                                            const typename K::T (&UR)[K::M]) {
+  using T = typename K::T;
+  constexpr int M = K::M, NP = K::NP, NQF = K::NQF, DIM = K::DIM, MNP = K::MNP;
+  T flux[M];
+  if (!RERUN && !is_physical<K::LAW, T>(a.law, UL)) {
+    flag_nonphysical(a.status, eL);
+    if (a.p0) mark_p0(a, eL);
+  }
+  if (eR >= 0) {
+    if (!RERUN && !is_physical<K::LAW, T>(a.law, UR)) {
+      flag_nonphysical(a.status, eR);
+      if (a.p0) mark_p0(a, eR);
+    }
+    numerical_flux<K::LAW, K::FLUX, DIM, T>(a.law, n, UL, UR, flux);
+  } else if (a.mesh.bpart[-eR - 1] >= 0) {
+    // periodic edge (DGCell.cc:687-705): the partner cell's trace at the
+    // mirrored point through the numerical flux; only the left cell gets it
+    const int b = -eR - 1, pe = a.mesh.bpart[b];
+    T UP[M];
+    cell_trace<K>(a.C + (size_t)pe * MNP, a.mesh.bpphi + ((size_t)b * NQF + q) * NP, UP, RERUN && a.bad[pe]);
+    numerical_flux<K::LAW, K::FLUX, DIM, T>(a.law, n, UL, UP, flux);
+  } else {
+    const int b = -eR - 1;
+    const double* x = a.mesh.bpts + ((size_t)b * NQF + q) * 3;
+    if constexpr (ENS) {  // the instance's own clock and far-field parameters
+      const TimeCtl* c = a.ctl + inst;
+      const double time = __fma_rn(a.stage_time_factor, c->dt, c->t);
+      boundary_flux<K::LAW, K::FLUX, DIM, T>(a.laws[inst], a.mesh.bbid[b], n, x, time, UL, flux);
+    } else {
+      const double time = __fma_rn(a.stage_time_factor, a.ctl->dt, a.ctl->t);
+      boundary_flux<K::LAW, K::FLUX, DIM, T>(a.law, a.mesh.bbid[b], n, x, time, UL, flux);
+    }
+  }
+  T* sl = a.slots + slot_index<K>(eL, lfL * NQF + q, 0);
+#pragma unroll
+  for (int j = 0; j < M; ++j) sl[j] = -flux[j] * jw;
+  if (eR >= 0) {
+    T* sr = a.slots + slot_index<K>(eR, lfR * NQF + qR, 0);
+#pragma unroll
+    for (int j = 0; j < M; ++j) sr[j] = flux[j] * jw;
+  }
+}
+
+// One face point: traces of both sides (precomputed, or for RERUN evaluated
+// from the coefficients with marked cells at their means), then face_finish.
 template <class K, bool RERUN, bool ENS>
 __device__ __forceinline__ void face_point(const StageArgs<typename K::T>& a, int f, int q,
                                            const typename K::T* s_phif, const typename K::T* s_fqw,
@@ -308,15 +359,11 @@ __device__ __forceinline__ void face_point(const StageArgs<typename K::T>& a, in
 #pragma unroll
   for (int i = 0; i < DIM; ++i) n[i] = a.mesh.fnrm[f * DIM + i];
   const T jw = a.mesh.fj[f] * s_fqw[q];
-  T UL[M], UR[M], flux[M];
+  T UL[M], UR[M];
   if constexpr (RERUN)
     cell_trace<K>(a.C + (size_t)eL * MNP, s_phif + (lfL * NQF + q) * NP, UL, a.bad[eL]);
   else
     load_trace<K>(a.tr, eL, lfL * NQF + q, UL);
-  if (!RERUN && !is_physical<K::LAW, T>(a.law, UL)) {
-    flag_nonphysical(a.status, eL);
-    if (a.p0) mark_p0(a, eL);
-  }
   int qR = 0;
   if (eR >= 0) {
     qR = s_qmap[perm * NQF + q];
@@ -324,37 +371,8 @@ __device__ __forceinline__ void face_point(const StageArgs<typename K::T>& a, in
       cell_trace<K>(a.C + (size_t)eR * MNP, s_phif + (lfR * NQF + qR) * NP, UR, a.bad[eR]);
     else
       load_trace<K>(a.tr, eR, lfR * NQF + qR, UR);
-    if (!RERUN && !is_physical<K::LAW, T>(a.law, UR)) {
-      flag_nonphysical(a.status, eR);
-      if (a.p0) mark_p0(a, eR);
-    }
-    numerical_flux<K::LAW, K::FLUX, DIM, T>(a.law, n, UL, UR, flux);
-  } else if (a.mesh.bpart[-eR - 1] >= 0) {
-    // periodic edge (DGCell.cc:687-705): the partner cell's trace at the
-    // mirrored point through the numerical flux; only the left cell gets it
-    const int b = -eR - 1, pe = a.mesh.bpart[b];
-    cell_trace<K>(a.C + (size_t)pe * MNP, a.mesh.bpphi + ((size_t)b * NQF + q) * NP, UR, RERUN && a.bad[pe]);
-    numerical_flux<K::LAW, K::FLUX, DIM, T>(a.law, n, UL, UR, flux);
-  } else {
-    const int b = -eR - 1;
-    const double* x = a.mesh.bpts + ((size_t)b * NQF + q) * 3;
-    if constexpr (ENS) {  // the instance's own clock and far-field parameters
-      const TimeCtl* c = a.ctl + inst;
-      const double time = c->t + a.stage_time_factor * c->dt;
-      boundary_flux<K::LAW, K::FLUX, DIM, T>(a.laws[inst], a.mesh.bbid[b], n, x, time, UL, flux);
-    } else {
-      const double time = a.ctl->t + a.stage_time_factor * a.ctl->dt;
-      boundary_flux<K::LAW, K::FLUX, DIM, T>(a.law, a.mesh.bbid[b], n, x, time, UL, flux);
-    }
   }
-  T* sl = a.slots + slot_index<K>(eL, lfL * NQF + q, 0);
-#pragma unroll
-  for (int j = 0; j < M; ++j) sl[j] = -flux[j] * jw;
-  if (eR >= 0) {
-    T* sr = a.slots + slot_index<K>(eR, lfR * NQF + qR, 0);
-#pragma unroll
-    for (int j = 0; j < M; ++j) sr[j] = flux[j] * jw;
-  }
+  face_finish<K, RERUN, ENS>(a, f, q, eL, eR, inst, lfL, lfR, qR, n, jw, UL, UR);
 }
 
 template <class K>

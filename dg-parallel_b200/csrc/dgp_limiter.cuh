@@ -9,8 +9,10 @@
 //     970-993 (faces in local-face order, a later face overwrites).
 //   * Every difference reads the unlimited state (the reference reads slot 0
 //     and writes the copy slot; TimeIntegrator::limit copies back after all
-//     cells, TimeIntegrator.cc:1414-1434): one kernel computes the limited rows
-//     into L, a second copies the rows of triggered cells back.
+//     cells, TimeIntegrator.cc:1414-1434): a first kernel writes the moments
+//     of every degree of every (cell, field) row of the unlimited state, a
+//     second limits each row from those moments alone, so that it can write
+//     the limited blocks (and the row's face-point traces) in place.
 //   * Per field, degrees n = p..1: a degree whose modes are all below 1e-10 in
 //     magnitude is skipped; a degree with no limited component ends the
 //     descent.  minmod and absmin as DGLimiter.cc:1424-1447.
@@ -23,7 +25,7 @@
 //     centres (degree 0: the cell mean).  A limited degree maps back to its
 //     modal block exactly; the mean never changes.
 //   * Trigger (the sensor) of a cell: lowest limited degree over its fields,
-//     0 when untouched.
+//     0 when untouched (the kernels record it per row; the host reduces).
 // Products and sums are single-rounding intrinsics in a fixed order (no FMA
 // contraction), so the moments -- and therefore the trigger set -- match the
 // CPU restatement bit for bit on the same state.
@@ -39,13 +41,16 @@ constexpr int kLimGeo = 10;
 constexpr double kLimSmall = 1.0e-10;
 
 struct LimArgs {
-  const double* C;      // state (unlimited)
-  double* L;            // limited rows (written for triggered cells)
-  unsigned char* trig;  // [E] trigger degree
+  double* C;            // state, limited in place
+  double* Mo;           // [E * M][NP] moments of every degree of each row of the unlimited state
+  unsigned char* big;   // [E * M] bit n: a mode of degree n above kLimSmall in magnitude
+  unsigned char* trig;  // [E * M] trigger degree of each row (0: untouched)
   const int* nb;        // [E][4] left, right, bottom, top (-1: none)
   const double* geo;    // [E][kLimGeo]
   const double* Dn;     // per degree n: (n+1)^2 block at n(n+1)(2n+1)/6
   const double* Dinv;
+  void* tr;             // face-point traces (slot layout, type of the right-hand side)
+  const void* phif;     // [NS][NP] face-point basis values (same type)
   const TimeCtl* ctl;   // kernels are no-ops once the run is done (nullptr: always run)
   const TimeCtl* gctl;
   const int* cell_inst; // ensembles: instance of each cell (-1: padding); finished
@@ -135,37 +140,62 @@ __device__ __forceinline__ void lim_moments(const double* __restrict__ row, cons
   }
 }
 
-template <int N>
-__device__ __forceinline__ void lim_lower(const LimArgs& a, int cell, const double* __restrict__ row,
-                                          double (&h)[N + 1]) {
-  const double* gg = a.geo + (size_t)cell * kLimGeo;
-  double P[N + 1][N + 1];
-  lim_transform<N>(__ldg(gg + 0), __ldg(gg + 1), __ldg(gg + 2), __ldg(gg + 3), P);
-  lim_moments<N>(row, a.Dn, P, h);
+// one thread per (cell, field) row: the degree-n physical derivatives of
+// every degree-n block, n = 0..p, and the mask of the degrees with a mode above
+// kLimSmall
+template <int N, int NP>
+__device__ __forceinline__ void lim_row_moments(const double* __restrict__ row, const double* __restrict__ Dn,
+                                                const double* gg, double* __restrict__ mo, unsigned& big) {
+  constexpr int base = N * (N + 1) / 2;
+  double P[N + 1][N + 1], g[N + 1];
+  lim_transform<N>(gg[0], gg[1], gg[2], gg[3], P);
+  lim_moments<N>(row, Dn, P, g);
+  bool b = false;
+#pragma unroll
+  for (int m = 0; m <= N; ++m) {
+    mo[base + m] = g[m];
+    b |= fabs(row[base + m]) > kLimSmall;
+  }
+  if (b) big |= 1u << N;
+  if constexpr (N >= 1) lim_row_moments<N - 1, NP>(row, Dn, gg, mo, big);
 }
 
-// one degree N of one field; returns false when the descent ends
-template <int N, int M, int NP>
-__device__ __forceinline__ bool lim_degree(const LimArgs& a, int e, int j, const int (&nb)[4], const double* gg,
-                                           int& trig, unsigned& modified) {
-  constexpr int base = N * (N + 1) / 2, w = N + 1, off = N * (N + 1) * (2 * N + 1) / 6;
-  const double* row = a.C + ((size_t)e * M + j) * NP;
-  bool big = false;
+template <class K>
+__global__ void __launch_bounds__(128) limit_moments_kernel(LimArgs a) {
+  constexpr int M = K::M, NP = K::NP, P = K::ORDER;
+  if (a.ctl && a.gctl->done) return;
+  const size_t R = (size_t)a.E * M;
+  const size_t r = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+  if (r >= R) return;
+  const int e = static_cast<int>(r / M);
+  if (lim_skip_cell(a, e)) return;
+  double gg[4];
 #pragma unroll
-  for (int m = 0; m <= N; ++m) big |= fabs(row[base + m]) > kLimSmall;
-  if (!big) return true;
-  double P[N + 1][N + 1], g[N + 1], gl[N + 1], he[N], hx[4][N];
-  lim_transform<N>(gg[0], gg[1], gg[2], gg[3], P);
-  lim_moments<N>(row, a.Dn, P, g);
-  lim_lower<N - 1>(a, e, row, he);
+  for (int i = 0; i < 4; ++i) gg[i] = __ldg(a.geo + (size_t)e * kLimGeo + i);
+  double row[NP];
 #pragma unroll
-  for (int d = 0; d < 4; ++d)
-    if (nb[d] >= 0) lim_lower<N - 1>(a, nb[d], a.C + ((size_t)nb[d] * M + j) * NP, hx[d]);
-  const double px = gg[8], py = gg[9];
+  for (int k = 0; k < NP; ++k) row[k] = a.C[r * NP + k];
+  unsigned big = 0;
+  lim_row_moments<P, NP>(row, a.Dn, gg, a.Mo + r * NP, big);
+  a.big[r] = static_cast<unsigned char>(big);
+}
+
+// one degree N of one row from the moments in registers (mo: the row's own,
+// mn: the neighbours' degrees 0..p-1, pc: the neighbours' bounding-box centre
+// coordinate across the shared direction); returns false when the descent ends
+template <int N, int NP, int NL>
+__device__ __forceinline__ bool lim_degree(const LimArgs& a, const double (&mo)[NP], const double (&mn)[4][NL],
+                                           const double (&pc)[4], const int (&nb)[4], const double* gg,
+                                           unsigned big, double* row, unsigned& mod) {
+  constexpr int base = N * (N + 1) / 2, lo = (N - 1) * N / 2, w = N + 1, off = N * (N + 1) * (2 * N + 1) / 6;
+  if (!((big >> N) & 1u)) return true;
+  const double px = gg[4], py = gg[5];
+  double gl[N + 1];
   bool any = false;
 #pragma unroll
   for (int c = 0; c <= N; ++c) {
-    gl[c] = g[c];
+    const double g = mo[base + c];
+    gl[c] = g;
     const bool hasx = c <= N - 1 && (nb[0] >= 0 || nb[1] >= 0);
     const bool hasy = c >= 1 && (nb[2] >= 0 || nb[3] >= 0);
     double t1 = 0.0, t2 = 0.0;
@@ -173,24 +203,24 @@ __device__ __forceinline__ bool lim_degree(const LimArgs& a, int e, int j, const
     if (hasx) {
       double fwd = 0.0, bwd = 0.0;
       if (c <= N - 1) {
-        if (nb[1] >= 0) fwd = __dsub_rn(hx[1][c], he[c]) / __dsub_rn(__ldg(a.geo + (size_t)nb[1] * kLimGeo + 8), px);
-        if (nb[0] >= 0) bwd = __dsub_rn(he[c], hx[0][c]) / __dsub_rn(px, __ldg(a.geo + (size_t)nb[0] * kLimGeo + 8));
+        const double he = mo[lo + c];
+        if (nb[1] >= 0) fwd = __dsub_rn(mn[1][lo + c], he) / __dsub_rn(pc[1], px);
+        if (nb[0] >= 0) bwd = __dsub_rn(he, mn[0][lo + c]) / __dsub_rn(px, pc[0]);
       }
-      if (nb[0] >= 0 && nb[1] >= 0) t1 = lim_minmod3(g[c], fwd, bwd, l1);
-      else if (nb[0] >= 0) t1 = lim_minmod2(g[c], bwd, l1);
-      else t1 = lim_minmod2(g[c], fwd, l1);
+      if (nb[0] >= 0 && nb[1] >= 0) t1 = lim_minmod3(g, fwd, bwd, l1);
+      else if (nb[0] >= 0) t1 = lim_minmod2(g, bwd, l1);
+      else t1 = lim_minmod2(g, fwd, l1);
     }
     if (hasy) {
       double fwd = 0.0, bwd = 0.0;
       if (c >= 1) {
-        if (nb[3] >= 0)
-          fwd = __dsub_rn(hx[3][c - 1], he[c - 1]) / __dsub_rn(__ldg(a.geo + (size_t)nb[3] * kLimGeo + 9), py);
-        if (nb[2] >= 0)
-          bwd = __dsub_rn(he[c - 1], hx[2][c - 1]) / __dsub_rn(py, __ldg(a.geo + (size_t)nb[2] * kLimGeo + 9));
+        const double he = mo[lo + c - 1];
+        if (nb[3] >= 0) fwd = __dsub_rn(mn[3][lo + c - 1], he) / __dsub_rn(pc[3], py);
+        if (nb[2] >= 0) bwd = __dsub_rn(he, mn[2][lo + c - 1]) / __dsub_rn(py, pc[2]);
       }
-      if (nb[2] >= 0 && nb[3] >= 0) t2 = lim_minmod3(g[c], fwd, bwd, l2);
-      else if (nb[2] >= 0) t2 = lim_minmod2(g[c], bwd, l2);
-      else t2 = lim_minmod2(g[c], fwd, l2);
+      if (nb[2] >= 0 && nb[3] >= 0) t2 = lim_minmod3(g, fwd, bwd, l2);
+      else if (nb[2] >= 0) t2 = lim_minmod2(g, bwd, l2);
+      else t2 = lim_minmod2(g, fwd, l2);
     }
     if (hasx && hasy) {
       if (l1 || l2) {
@@ -211,81 +241,103 @@ __device__ __forceinline__ bool lim_degree(const LimArgs& a, int e, int j, const
   }
   if (!any) return false;
   // back to reference derivatives (d/du = x_u d/dx + y_u d/dy, ...) and modes
-  double Q[N + 1][N + 1], r[N + 1];
-  lim_transform<N>(gg[4], gg[5], gg[6], gg[7], Q);
+  double Q[N + 1][N + 1], q[N + 1];
+  lim_transform<N>(gg[0], gg[1], gg[2], gg[3], Q);
 #pragma unroll
   for (int i = 0; i <= N; ++i) {
     double acc = 0.0;
 #pragma unroll
     for (int c = 0; c <= N; ++c) acc = __dadd_rn(acc, __dmul_rn(Q[i][c], gl[c]));
-    r[i] = acc;
+    q[i] = acc;
   }
-  double* out = a.L + ((size_t)e * M + j) * NP;
 #pragma unroll
   for (int k = 0; k <= N; ++k) {
     double acc = 0.0;
 #pragma unroll
-    for (int i = 0; i <= N; ++i) acc = __dadd_rn(acc, __dmul_rn(__ldg(a.Dinv + off + k * w + i), r[i]));
-    out[base + k] = acc;
+    for (int i = 0; i <= N; ++i) acc = __dadd_rn(acc, __dmul_rn(__ldg(a.Dinv + off + k * w + i), q[i]));
+    row[base + k] = acc;
   }
-  modified |= 1u << N;
-  trig = (trig == 0 || N < trig) ? N : trig;
+  mod |= 1u << N;
   return true;
 }
 
-template <int N, int M, int NP>
-__device__ __forceinline__ void lim_descend(const LimArgs& a, int e, int j, const int (&nb)[4], const double* gg,
-                                            int& trig, unsigned& modified) {
+template <int N, int NP, int NL>
+__device__ __forceinline__ void lim_descend(const LimArgs& a, const double (&mo)[NP], const double (&mn)[4][NL],
+                                            const double (&pc)[4], const int (&nb)[4], const double* gg,
+                                            unsigned big, double* row, unsigned& mod) {
   if constexpr (N >= 1) {
-    if (lim_degree<N, M, NP>(a, e, j, nb, gg, trig, modified)) lim_descend<N - 1, M, NP>(a, e, j, nb, gg, trig, modified);
+    if (lim_degree<N, NP, NL>(a, mo, mn, pc, nb, gg, big, row, mod))
+      lim_descend<N - 1, NP, NL>(a, mo, mn, pc, nb, gg, big, row, mod);
   }
 }
 
-// one thread per cell: limited rows of triggered cells into L, trigger into trig
+// one thread per (cell, field) row: limits the row from the moments, writes the
+// limited blocks into the state and the row's face-point traces.  Every input
+// of the descent (the row's moments, the neighbours' moments of degrees below
+// p and their centres) is loaded up front, so the descent waits on one round
+// of loads whatever its depth.
 template <class K>
 __global__ void __launch_bounds__(128) limit_kernel(LimArgs a) {
-  constexpr int M = K::M, NP = K::NP, P = K::ORDER;
+  using T = typename K::T;
+  constexpr int M = K::M, NP = K::NP, P = K::ORDER, NS = K::NS;
+  constexpr int NL = P * (P + 1) / 2;  // moments of degrees 0..p-1
   if (a.ctl && a.gctl->done) return;
-  const int e = blockIdx.x * blockDim.x + threadIdx.x;
-  if (e >= a.E || lim_skip_cell(a, e)) return;
-  int nb[4];
+  const size_t R = (size_t)a.E * M;
+  const size_t r = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+  if (r >= R) return;
+  const int e = static_cast<int>(r / M);
+  if (lim_skip_cell(a, e)) return;
+  const int j = static_cast<int>(r - (size_t)e * M);
+  const unsigned big = a.big[r];
+  const int4 n4 = __ldg(reinterpret_cast<const int4*>(a.nb) + e);
+  // Q needs d x/du, d y/du, d x/dv, d y/dv; then the bounding-box centre
+  double gg[6];
 #pragma unroll
-  for (int d = 0; d < 4; ++d) nb[d] = __ldg(a.nb + 4 * e + d);
-  double gg[kLimGeo];
-#pragma unroll
-  for (int i = 0; i < kLimGeo; ++i) gg[i] = __ldg(a.geo + (size_t)e * kLimGeo + i);
+  for (int i = 0; i < 6; ++i) gg[i] = __ldg(a.geo + (size_t)e * kLimGeo + 4 + i);
   int trig = 0;
-  unsigned modified[M];
+  if (big >> 1) {
+    const int nb[4] = {n4.x, n4.y, n4.z, n4.w};
+    double mo[NP], mn[4][NL], pc[4];
 #pragma unroll
-  for (int j = 0; j < M; ++j) {
-    modified[j] = 0;
-    lim_descend<P, M, NP>(a, e, j, nb, gg, trig, modified[j]);
-  }
-  if (trig) {
-    // the untouched blocks of a triggered cell complete its row in L
+    for (int k = 0; k < NP; ++k) mo[k] = a.Mo[r * NP + k];
 #pragma unroll
-    for (int j = 0; j < M; ++j) {
-      const double* row = a.C + ((size_t)e * M + j) * NP;
-      double* out = a.L + ((size_t)e * M + j) * NP;
+    for (int d = 0; d < 4; ++d) {
+      const int n = nb[d] >= 0 ? nb[d] : e;  // a missing neighbour is never read
+      const double* src = a.Mo + ((size_t)n * M + j) * NP;
 #pragma unroll
-      for (int n = 0; n <= P; ++n)
-        if (!((modified[j] >> n) & 1u))
+      for (int k = 0; k < NL; ++k) mn[d][k] = src[k];
+      pc[d] = __ldg(a.geo + (size_t)n * kLimGeo + (d < 2 ? 8 : 9));
+    }
+    double row[NP];
+    unsigned mod = 0;
+    lim_descend<P, NP, NL>(a, mo, mn, pc, nb, gg, big, row, mod);
+    if (mod) {
+      trig = __ffs(mod) - 1;  // lowest limited degree
+      // the row as it leaves the limiter: unchanged blocks from the state,
+      // limited blocks from the descent (written back in place)
+      double* c = a.C + r * NP;
+      T ck[NP];
 #pragma unroll
-          for (int k = 0; k <= n; ++k) out[n * (n + 1) / 2 + k] = row[n * (n + 1) / 2 + k];
+      for (int k = 0; k < NP; ++k) ck[k] = (T)c[k];
+#pragma unroll
+      for (int n = 1; n <= P; ++n)
+        if ((mod >> n) & 1u)
+#pragma unroll
+          for (int k = n * (n + 1) / 2; k < (n + 1) * (n + 2) / 2; ++k) {
+            c[k] = row[k];
+            ck[k] = (T)row[k];
+          }
+      const T* phif = static_cast<const T*>(a.phif);
+      T* tr = static_cast<T*>(a.tr);
+      for (int s = 0; s < NS; ++s) {
+        T acc = 0;
+#pragma unroll
+        for (int k = 0; k < NP; ++k) acc += __ldg(phif + s * NP + k) * ck[k];
+        tr[slot_index<K>(e, s, j)] = acc;
+      }
     }
   }
-  a.trig[e] = static_cast<unsigned char>(trig);
-}
-
-// copy the limited rows of triggered cells back into the state
-template <class K>
-__global__ void __launch_bounds__(256) limit_apply_kernel(LimArgs a) {
-  if (a.ctl && a.gctl->done) return;
-  const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-  if (i >= (long long)a.E * K::MNP) return;
-  const int e = static_cast<int>(i / K::MNP);
-  if (lim_skip_cell(a, e)) return;
-  if (a.trig[e]) const_cast<double*>(a.C)[i] = a.L[i];
+  a.trig[r] = static_cast<unsigned char>(trig);
 }
 
 }  // namespace dgp

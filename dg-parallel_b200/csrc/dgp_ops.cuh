@@ -92,27 +92,30 @@ void ops_trace(const DeviceBuffers& b, const unsigned char* only, cudaStream_t s
   trace_kernel<K><<<ops_grid_elem<K>(b.E), K::BLOCK, 0, st>>>(a, only);
 }
 
-// triangle moment limiter on the current state: limited rows of triggered
-// cells into L, then copied back
+// triangle moment limiter on the current state: moments of every row, then
+// the limited rows (and their traces) in place
 template <class K>
 void ops_limit(const DeviceBuffers& b, int check_done, cudaStream_t st) {
   if constexpr (K::DIM == 2 && K::ORDER >= 1) {
     LimArgs a;
-    a.C = static_cast<const double*>(b.C);
-    a.L = b.L;
+    a.C = static_cast<double*>(b.C);
+    a.Mo = b.lmo;
+    a.big = b.lbig;
     a.trig = b.trig;
     a.nb = b.nb;
     a.geo = b.lgeo;
     a.Dn = b.limD;
     a.Dinv = b.limDinv;
+    a.tr = b.tr;
+    a.phif = b.phif;
     a.ctl = check_done ? b.ctl : nullptr;
     a.gctl = b.gctl;
     a.cell_inst = b.cell_inst;
     a.E = b.E;
-    limit_kernel<K><<<(b.E + 127) / 128, 128, 0, st>>>(a);
-    const long long n = static_cast<long long>(b.E) * K::MNP;
-    limit_apply_kernel<K><<<static_cast<int>((n + 255) / 256), 256, 0, st>>>(a);
-    ops_trace<K>(b, b.trig, st);
+    const long long rows = static_cast<long long>(b.E) * K::M;
+    const int grid = static_cast<int>((rows + 127) / 128);
+    limit_moments_kernel<K><<<grid, 128, 0, st>>>(a);
+    limit_kernel<K><<<grid, 128, 0, st>>>(a);
   }
 }
 
@@ -132,7 +135,7 @@ void ops_adj_stage(const DeviceBuffers& b, const AdjStage& g, cudaStream_t st) {
     a.ce = g.ce;
     a.dt = g.dt;
     a.t_seg = g.t_seg;
-    a.t_offset = g.t_offset;
+    a.t_factor = g.t_factor;
     const int fgrid = (b.F + K::FPB - 1) / K::FPB;
     adj_face_kernel<K><<<fgrid, K::FACE_BLOCK, 0, st>>>(a);
     adj_elem_kernel<K><<<ops_grid_elem<K>(b.E), K::BLOCK, adj_elem_smem<K>(), st>>>(a);

@@ -63,8 +63,9 @@ struct DeviceBuffers {
   // P0 fallback and triangle moment limiter
   int p0 = 0;                     // 1: DGCell::setToZero fallback on
   unsigned char* bad = nullptr;   // [E] P0 marks
-  unsigned char* trig = nullptr;  // [E] trigger degree of the last limiter pass
-  double* L = nullptr;            // limited rows
+  unsigned char* trig = nullptr;  // [E * M] trigger degree of each row in the last limiter pass
+  unsigned char* lbig = nullptr;  // [E * M] degrees with a mode above the limiter's threshold
+  double* lmo = nullptr;          // [E * M][NP] moments of every degree of each row
   int* nb = nullptr;              // [E][4] left, right, bottom, top
   double* lgeo = nullptr;         // [E][10] limiter geometry
   double* limD = nullptr;         // derivative tables per degree
@@ -138,14 +139,15 @@ inline StageArgs<T> make_args(const DeviceBuffers& b) {
 
 // One reversed stage of the discrete adjoint: out = ca mu + cb dt w + cc acc,
 // acc <- cd acc + ce mu, with w the transposed linearised L at the stage
-// state (b.C) and the stage time *t_seg + t_offset.
+// state (b.C) and the stage time *t_seg + t_factor * dt (t_seg: the step's
+// start time, t_factor 0, 1, 0.5 as the forward stage).
 struct AdjStage {
   const double* mu;
   double* out;
   double* acc;
   double ca, cb, cc, cd, ce, dt;
   const double* t_seg;
-  double t_offset;
+  double t_factor;
 };
 
 // Kernel set of one instantiation.

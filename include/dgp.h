@@ -200,7 +200,10 @@ int dgp_ensemble_launches_per_step(dgp_ensemble e, int* n);
 int dgp_adjoint_set_receivers(dgp_solver s, int n, const double* points, const double* observed);
 /* field 0 at the receivers for the current state (rho may be NULL) and J */
 int dgp_receiver_values(dgp_solver s, double* rho, double* J);
-/* from the current state at time t0; leaves the state at the final time; J may be NULL */
+/* from the current state at time t0; leaves the state at the final time; J may be NULL.
+ * every > 0: checkpoint every `every` steps, the backward pass recomputes each
+ * segment; every == 0: keep all 3 * nsteps stage states in device memory, the
+ * backward pass recomputes nothing (DGP_ERR_NOMEM when they do not fit). */
 int dgp_forward_checkpointed(dgp_solver s, double t0, double dt, int nsteps, int every, double* J);
 /* dJ/du0 (host, file order [cell][field][mode]) of the last forward pass; the
  * seed dJ/du_T is dJ_duT when not NULL, else the receiver objective's */

@@ -124,6 +124,16 @@ def test_adjoint_seed_and_checkpoint_interval_invariance(tmp_path):
     g12 = s.backward()
     # recomputation reproduces the forward states exactly
     assert np.array_equal(g4, g12)
+    # every == 0 keeps all stage states instead of recomputing: same gradient
+    s.set_state(u0)
+    s.forward_checkpointed(0.0, dt, 12, 12)
+    uT = s.get_state()
+    s.set_state(u0)
+    s.forward_checkpointed(0.0, dt, 12, 0)
+    assert np.array_equal(s.get_state(), uT)
+    g0 = s.backward()
+    assert np.array_equal(g0, g4)
+    assert np.array_equal(s.get_state(), uT)
     # an explicit seed: d/du0 of <c, u_T> for a fixed c
     s.set_state(u0)
     s.forward_checkpointed(0.0, dt, 12, 3)
