@@ -126,6 +126,22 @@ def cpu_reference(mesh, steps: int, warmup: int, threads: int):
             "steps": int(kv["steps"]), "threads": int(kv["threads"])}
 
 
+def elem_kernel_bytes(E, M, NP, NS, DIM, tsize):
+    """Bytes one element-kernel launch must move: state read, u_n read (stage 1
+    writes it instead), new state written (FP64), face slots read and face-point
+    traces written (right-hand-side type), J^{-1} (right-hand-side type) and
+    |J| (FP64) per cell."""
+    state = E * M * NP * 8
+    return 3 * state + 2 * E * NS * M * tsize + E * (DIM * DIM * tsize + 8)
+
+
+def stage_formula_bytes(E, F, M, NP, DIM):
+    """Algorithmic bytes of one whole stage by the per-element-stage formula of
+    the workload's roofline definition: coefficients (2 + 2/3) m Np 8 (FP64
+    state), geometry (d^2 + 1) 8, faces (F/E)(8 d + 8 + 2*4 + 2) per element."""
+    return E * ((2 + 2.0 / 3.0) * M * NP * 8 + (DIM * DIM + 1) * 8) + F * (8 * DIM + 8 + 2 * 4 + 2)
+
+
 def cpu_model():
     try:
         for line in open("/proc/cpuinfo"):
@@ -177,6 +193,9 @@ def main():
                     help="only the batched-ensemble measurement (96 Burgers instances to t = 0.5, ~2 min)")
     ap.add_argument("--adjoint", action="store_true",
                     help="only the discrete-adjoint measurement (Euler vortex 128x128x2 P2, 400 steps)")
+    ap.add_argument("--configs", action="store_true",
+                    help="only the other workloads: scalar P2 on 2048 triangles (200 steps) and "
+                         "Maxwell P2 on 663552 tets (one TM110 period), both forms, ~2 min")
     ap.add_argument("--profile-case", choices=["fp64", "mixed"], default=None,
                     help="only set up the workload and run --warmup + --steps steps (for ncu)")
     ap.add_argument("--block", type=int, default=0, choices=[0, 64, 128, 256],
@@ -198,6 +217,11 @@ def main():
         import torch
         torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
         print(json.dumps({"ensemble": ensemble_bench()}))
+        return 0
+    if args.configs:
+        import torch
+        torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+        print(json.dumps({"configs": configs_bench()}))
         return 0
 
     import numpy as np
@@ -316,17 +340,19 @@ def main():
         face_ms, elem_ms, elem3_ms = fp64["kernel_ms"]
         M, NP, NQF, NLF = 4, 10, 4, 3
         F = mesh.nfaces
-        state_b = E * M * NP * 8
         slot_b = E * NLF * NQF * M * 8
-        geo_e = E * (4 + 1) * 8
         geo_f = F * (2 * 8 + 8 + 8 + 4)
-        elem_bytes = state_b * 3 + slot_b + geo_e     # read C, U0, slots, geometry; write C
-        face_bytes = state_b + geo_f + slot_b         # read C (each cell once), write slots
+        elem_bytes = elem_kernel_bytes(E, M, NP, NLF * NQF, 2, 8)
+        face_bytes = 2 * slot_b + geo_f               # read both sides' traces, write slots, geometry
         if elem_ms >= face_ms:
             kname, kms, kbytes = "elem_kernel (volume + lift + RK3 stage)", elem_ms, elem_bytes
         else:
             kname, kms, kbytes = "face_kernel (traces + Roe flux + slot scatter)", face_ms, face_bytes
         achieved = kbytes / (kms * 1e-3) / 1e9
+        # the whole stage (face + element kernel) against the per-element-stage
+        # formula (coefficients, geometry and face data, no intermediates)
+        st_bytes = stage_formula_bytes(E, F, M, NP, 2)
+        st_ach = st_bytes / ((face_ms + elem_ms) * 1e-3) / 1e9
         traffic = None
         tfile = os.path.join(ROOT, "profiles", "traffic.json")
         if os.path.exists(tfile):
@@ -361,7 +387,11 @@ def main():
             "roofline": {"kernel": kname, "bound": "hbm", "achieved": achieved,
                          "peak": peaks.get("hbm_gbs"), "unit": "GB/s",
                          "frac": achieved / peaks.get("hbm_gbs"), "traffic": traffic,
-                         "peak_source": peak_src, "algorithmic_bytes_per_launch": kbytes},
+                         "peak_source": peak_src, "algorithmic_bytes_per_launch": kbytes,
+                         "stage_formula": {"bytes_per_dof_stage": st_bytes / (E * M * NP),
+                                           "bytes_per_stage": st_bytes,
+                                           "stage_ms": face_ms + elem_ms, "achieved": st_ach,
+                                           "frac": st_ach / peaks.get("hbm_gbs")}},
             "cpu_baseline": cpu,
             "e2e": {"value": e2e_value, "unit": "DOF-stage/s", "h2d_bytes_per_step": nbytes,
                     "d2h_bytes_per_step": nbytes, "steps": args.e2e_steps,
@@ -438,6 +468,98 @@ def ensemble_bench(n=96, seed=6, tend=0.5):
                    "t_end": tend, "cfl": 0.1, "seed": seed},
     }
     ens.close()
+    return out
+
+
+def configs_bench(steps=200):
+    """The other workloads, both forms, CUDA events on the solver's stream:
+
+    scalar: u_t + a.grad u = 0, a = (1, 0.5), Gaussian (centre (0.3, 0.3),
+      s = 0.01) on the unit square cut into 32x32x2 = 2048 jittered triangles
+      (seed 1), P2, upwind, exact-solution inflow, CFL 0.1, 200 steps; also
+      DG-Parallel's pthreads path on all host cores and on one.
+    maxwell: 3D Maxwell (eps = mu = 1), upwind flux, PEC walls, TM110 cavity
+      mode on the unit cube cut into 48^3 x 6 = 663552 jittered tets (seed 3),
+      P2, CFL 0.1; `steps` timed steps, then one full period (T = sqrt 2) for
+      the Ez L2 error against the exact mode.  The reference has no 3D Maxwell
+      law (its field storage caps at 5 fields), so there is no CPU reference.
+    Roofline: the element kernel's bytes (elem_kernel_bytes) over its CUDA-event
+    time, and the whole stage against the per-element-stage formula."""
+    import numpy as np
+    import torch
+    import dgp
+    from dgp import meshgen
+    peaks, peak_src = load_peaks()
+    hbm = peaks.get("hbm_gbs")
+
+    def timed(s, nsteps):
+        s.project(0.0)
+        t, _ = s.run(0.0, 0.0, 0.1, 8)
+        stream = torch.cuda.ExternalStream(s.stream())
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record(stream)
+        t_end, n = s.run(t, 0.0, 0.1, nsteps)
+        e1.record(stream)
+        e1.synchronize()
+        return e0.elapsed_time(e1) / 1e3, t_end, n
+
+    def measure(mesh, law, order, M, NP, NS, DIM, field, t_full=None):
+        E, F = mesh.ncells, mesh.nfaces
+        res = {"cells": E, "faces": F, "dofs": E * M * NP}
+        for name, prec, tsize in (("fp64", dgp.FP64, 8), ("mixed", dgp.MIXED, 4)):
+            s = dgp.Solver(mesh, law, order, prec)
+            sec, t_end, n = timed(s, steps)
+            kern = s.profile_kernels(10)
+            face_ms, elem_ms = float(kern[0]), float(kern[1])
+            eb = elem_kernel_bytes(E, M, NP, NS, DIM, tsize)
+            sb = stage_formula_bytes(E, F, M, NP, DIM)
+            r = {"value": E * M * NP * 3 * n / sec, "unit": "DOF-stage/s", "steps": n,
+                 "ms_per_step": sec / n * 1e3, "kernel_ms": kern.tolist(),
+                 "roofline": {"kernel": "elem_kernel", "bound": "hbm",
+                              "algorithmic_bytes_per_launch": eb,
+                              "achieved": eb / (elem_ms * 1e-3) / 1e9, "peak": hbm, "unit": "GB/s",
+                              "frac": eb / (elem_ms * 1e-3) / 1e9 / hbm, "peak_source": peak_src,
+                              "stage_formula": {"bytes_per_stage": sb, "stage_ms": face_ms + elem_ms,
+                                                "frac": sb / ((face_ms + elem_ms) * 1e-3) / 1e9 / hbm}},
+                 "l2_vs_exact_after_timed_steps": s.l2_error(t_end, field)}
+            if t_full is not None:
+                s.project(0.0)
+                w = time.perf_counter()
+                t_f, n_f = s.run(0.0, t_full, 0.1)
+                r["full_run"] = {"t": t_f, "steps": n_f, "wall_s": time.perf_counter() - w,
+                                 "l2_vs_exact": s.l2_error(t_f, field)}
+            s.close()
+            res[name] = r
+        res["mixed_over_fp64"] = res["mixed"]["value"] / res["fp64"]["value"]
+        return res
+
+    out = {}
+    m1 = meshgen.tri_square(32, 32, 0.0, 1.0, 0.0, 1.0, jitter=0.15, seed=1)
+    mesh1 = dgp.Mesh.from_arrays(2, m1.vertices, m1.cells, m1.domain_tag, m1.bfaces, m1.btags)
+    law1 = dgp.Law(dgp.LAW_SCALAR, dgp.FLUX_UPWIND, dgp.FIELD_GAUSS,
+                   dgp.law_params(velocity=(1.0, 0.5, 0.0), center=(0.3, 0.3, 0.0), width=0.01))
+    out["scalar_p2_2048tri"] = measure(mesh1, law1, 2, 1, 6, 3 * 3, 2, 0)
+    out["scalar_p2_2048tri"]["note"] = "launch/latency bound (12288 DOFs); not roofline-graded"
+    if os.path.exists(REF_DRIVER):
+        cpu = {}
+        with tempfile.TemporaryDirectory() as td:
+            msh = os.path.join(td, "scalar32.msh")
+            meshgen.write_msh_v1(m1, msh)
+            for thr in (os.cpu_count() or 1, 1):
+                cmd = [REF_DRIVER, "--mesh", msh, "--case", "gauss", "--order", "2", "--cfl", "0.1",
+                       "--ax", "1", "--ay", "0.5", "--cx", "0.3", "--cy", "0.3", "--s", "0.01",
+                       "--threads", str(thr), "--bench", str(steps), "--warmup", "3"]
+                p = subprocess.run(cmd, capture_output=True, text=True, timeout=600)
+                line = next((ln for ln in p.stdout.splitlines() if ln.startswith("BENCH")), None)
+                if p.returncode == 0 and line:
+                    kv = dict(tok.split("=") for tok in line.split()[1:])
+                    cpu[f"threads_{thr}"] = float(kv["dof_stage_per_s"])
+        out["scalar_p2_2048tri"]["cpu_reference_dof_stage_per_s"] = cpu
+    m3 = meshgen.tet_cube(48, 0.0, 1.0, jitter=0.1, seed=3, boundary_tag=40000)
+    mesh3 = dgp.Mesh.from_arrays(3, m3.vertices, m3.cells, m3.domain_tag, m3.bfaces, m3.btags)
+    law3 = dgp.Law(dgp.LAW_MAXWELL3D, dgp.FLUX_UPWIND, dgp.FIELD_TM110, dgp.law_params(cavity=1.0))
+    out["maxwell3d_p2_663552tet"] = measure(mesh3, law3, 2, 6, 10, 4 * 7, 3, 2, t_full=np.sqrt(2.0))
     return out
 
 

@@ -7,6 +7,8 @@
 #include <cmath>
 #include <cstdint>
 #include <cstring>
+#include <cstdio>
+#include <fstream>
 #include <map>
 #include <mutex>
 #include <numeric>
@@ -328,14 +330,17 @@ static int build_solver(dgp_solver s, const std::vector<LawParams>& lps, int fie
     return ia != ic ? ia < ic : s->meshes[a.inst].lfL[a.f] < s->meshes[c.inst].lfL[c.f];
   });
   std::vector<int> fel(2 * (size_t)Ftot), fcode(Ftot), bbid, bpart;
+  std::vector<int> cface(static_cast<size_t>(Etot) * t.nlf, -1);  // local face -> face, per cell
   std::vector<double> fnrm(static_cast<size_t>(Ftot) * dim), fj(Ftot), bpts, bpphi;
   int nb = 0;
   for (int k = 0; k < Ftot; ++k) {
     const HostMesh& m = s->meshes[faces[k].inst];
     const int f = faces[k].f, ufo = s->inst_ufirst[faces[k].inst];
     fel[2 * k] = s->f2i[ufo + m.eL[f]];
+    cface[static_cast<size_t>(fel[2 * k]) * t.nlf + m.lfL[f]] = k;
     if (m.eR[f] >= 0) {
       fel[2 * k + 1] = s->f2i[ufo + m.eR[f]];
+      cface[static_cast<size_t>(fel[2 * k + 1]) * t.nlf + m.lfR[f]] = k;
     } else {
       fel[2 * k + 1] = -(nb + 1);
       bbid.push_back(m.bid[f]);
@@ -444,7 +449,7 @@ static int build_solver(dgp_solver s, const std::vector<LawParams>& lps, int fie
   b.tr = tr;
   b.rhs = rhs;
   b.scratch = scratch;
-  b.npartials = std::max(s->ops.grid_elem(Etot), (Etot + 255) / 256) * std::max(b.M, 1) + 1;
+  b.npartials = std::max(s->ops.grid_elem(Etot), (Etot + 255) / 256) * std::max(b.M, 3) + 1;
   const int nctl = ensemble ? n + 1 : 1;
   if ((rc = s->alloc(&b.partials, b.npartials)) || (rc = s->alloc(&b.ctl, nctl)) ||
       (rc = s->alloc(&b.status, 1)))
@@ -478,8 +483,16 @@ static int build_solver(dgp_solver s, const std::vector<LawParams>& lps, int fie
   if ((rc = s->alloc(&b.bad, static_cast<size_t>(Etot)))) return rc;
   DGP_CUDA(cudaMemset(b.bad, 0, Etot));
   b.p0 = (s->law == DGP_LAW_EULER2D || s->law == DGP_LAW_EULER3D) ? 1 : 0;
+  b.limiter_kind = s->order >= 1 ? s->limiter : DGP_LIMITER_NONE;
   if (s->limiter == DGP_LIMITER_MOMENT && s->order >= 1) {
     if ((rc = setup_limiter(s))) return rc;
+  }
+  if (s->limiter == DGP_LIMITER_BARTH && s->order >= 1) {
+    // FP64 face-point basis values and each cell's faces; triggers per row
+    if ((rc = s->upload(&b.cface, cface)) || (rc = s->upload(&b.bphif, t.phif)) ||
+        (rc = s->alloc(&b.trig, static_cast<size_t>(Etot) * b.M)))
+      return rc;
+    DGP_CUDA(cudaMemset(b.trig, 0, static_cast<size_t>(Etot) * b.M));
   }
   if (cudaError_t e = s->ops.prepare()) return fail(DGP_ERR_CUDA, cudaGetErrorString(e));
   // DGAnalysis::DGAnalysis projects the far field as the initial state
@@ -620,7 +633,8 @@ int dgp_solver_create(dgp_mesh mh, dgp_law law, int order, int precision, int li
   if (!mh || !law || !out) return fail(DGP_ERR_INVALID, "null argument");
   if (precision != DGP_PRECISION_FP64 && precision != DGP_PRECISION_MIXED)
     return fail(DGP_ERR_INVALID, "unknown precision");
-  if (limiter != DGP_LIMITER_NONE && limiter != DGP_LIMITER_MOMENT) return fail(DGP_ERR_INVALID, "unknown limiter");
+  if (limiter != DGP_LIMITER_NONE && limiter != DGP_LIMITER_MOMENT && limiter != DGP_LIMITER_BARTH)
+    return fail(DGP_ERR_INVALID, "unknown limiter");
   const HostMesh& m = mh->m;
   if (limiter == DGP_LIMITER_MOMENT && m.dim != 2)
     return fail(DGP_ERR_UNSUPPORTED, "the moment limiter is built for triangles only");
@@ -689,7 +703,7 @@ int dgp_project(dgp_solver s, double t) {
   DGP_CUDA(cudaSetDevice(s->device));
   s->ops.project(s->b, t, s->stream);
   // DGAnalysis::DGAnalysis limits the projected state once (DGAnalysis.cc:276-291)
-  if (s->limiter == DGP_LIMITER_MOMENT && s->ops.limit) s->ops.limit(s->b, 0, s->stream);
+  if (s->limiter != DGP_LIMITER_NONE && s->ops.limit) s->ops.limit(s->b, 0, s->stream);
   s->ops.trace(s->b, nullptr, s->stream);
   DGP_CUDA(cudaGetLastError());
   DGP_CUDA(cudaStreamSynchronize(s->stream));
@@ -721,6 +735,108 @@ static int state_to_host(dgp_solver s, const void* src, double* out) {
   DGP_CUDA(cudaGetLastError());
   DGP_CUDA(cudaMemcpyAsync(out, s->b.scratch, n * 8, cudaMemcpyDeviceToHost, s->stream));
   DGP_CUDA(cudaStreamSynchronize(s->stream));
+  return DGP_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Checkpoints in the data format of DGAnalysis::write / read (DGPref.cc:712-766,
+// DGCell::write / read DGCell.cc:1523-1540, mMesh::writeMEntity / readMEntity
+// mMesh.cc:401-455): TACT, ITER, "dim cells faces", then per cell its entity
+// (type, geometric order, vertex ids) followed by "order" and the coefficients
+// [field][mode], then the face entities.  DGAnalysis::write omits the geometric
+// order that readMEntity expects; files are written the way readMEntity reads
+// them, and both layouts are read.
+static const int kTypeEdge = 1, kTypeTri = 2, kTypeTet = 4;  // mEntity::mType
+
+int dgp_checkpoint_write(dgp_solver s, const char* path, double t, int iter) {
+  if (!s || !path) return fail(DGP_ERR_INVALID, "null argument");
+  if (s->b.ninst) return fail(DGP_ERR_UNSUPPORTED, "checkpoints are written for a single solver");
+  DGP_CUDA(cudaSetDevice(s->device));
+  DGP_CUDA(cudaStreamSynchronize(s->stream));
+  const HostMesh& m = s->meshes[0];
+  const size_t mnp = static_cast<size_t>(s->b.M) * s->b.NP;
+  std::vector<double> c(static_cast<size_t>(m.E) * mnp);
+  if (int rc = state_to_host(s, s->b.C, c.data())) return rc;
+  FILE* f = std::fopen(path, "w");
+  if (!f) return fail(DGP_ERR_IO, std::string("cannot write ") + path);
+  const int ctype = m.dim == 2 ? kTypeTri : kTypeTet, ftype = m.dim == 2 ? kTypeEdge : kTypeTri;
+  std::fprintf(f, "%.17g\n%d\n%d %d %d\n", t, iter, m.dim, m.E, m.F);
+  for (int e = 0; e < m.E; ++e) {
+    std::fprintf(f, "%d 1 ", ctype);
+    for (int k = 0; k < m.nvc; ++k) std::fprintf(f, "%d ", m.vid[m.cv[static_cast<size_t>(e) * m.nvc + k]]);
+    std::fprintf(f, "\n%d ", s->order);
+    for (size_t i = 0; i < mnp; ++i) std::fprintf(f, "%.17g ", c[e * mnp + i]);
+  }
+  for (int fc = 0; fc < m.F; ++fc) {
+    std::fprintf(f, "%d 1 ", ftype);
+    for (int k = 0; k < m.nfv; ++k) std::fprintf(f, "%d ", m.vid[m.fv[static_cast<size_t>(fc) * m.nfv + k]]);
+    std::fprintf(f, "\n");
+  }
+  const bool ok = std::ferror(f) == 0;
+  std::fclose(f);
+  return ok ? DGP_OK : fail(DGP_ERR_IO, std::string("write failed: ") + path);
+}
+
+int dgp_checkpoint_read(dgp_solver s, const char* path, double* t, int* iter) {
+  if (!s || !path) return fail(DGP_ERR_INVALID, "null argument");
+  if (s->b.ninst) return fail(DGP_ERR_UNSUPPORTED, "checkpoints are read into a single solver");
+  std::ifstream in(path);
+  if (!in) return fail(DGP_ERR_IO, std::string("cannot read ") + path);
+  std::vector<std::string> tok;
+  for (std::string w; in >> w;) tok.push_back(w);
+  const HostMesh& m = s->meshes[0];
+  const size_t mnp = static_cast<size_t>(s->b.M) * s->b.NP;
+  if (tok.size() < 5) return fail(DGP_ERR_IO, "checkpoint header is incomplete");
+  double tt = std::strtod(tok[0].c_str(), nullptr);
+  const int it = std::atoi(tok[1].c_str()), dim = std::atoi(tok[2].c_str());
+  const int ncell = std::atoi(tok[3].c_str()), nface = std::atoi(tok[4].c_str());
+  if (dim != m.dim || ncell != m.E) return fail(DGP_ERR_IO, "checkpoint does not match the solver's mesh");
+  // layout: with or without the geometric order after each type, with or
+  // without the face list
+  const size_t rest = tok.size() - 5;
+  int go = -1;
+  for (int g = 1; g >= 0 && go < 0; --g)
+    for (int fl = 1; fl >= 0 && go < 0; --fl) {
+      const size_t need = static_cast<size_t>(ncell) * (1 + g + m.nvc + 1 + mnp) +
+                          (fl ? static_cast<size_t>(nface) * (1 + g + m.nfv) : 0);
+      if (need == rest) go = g;
+    }
+  if (go < 0) return fail(DGP_ERR_IO, "checkpoint size does not match the solver's fields and order");
+  // cells by their sorted vertex ids
+  std::map<std::vector<int>, int> byv;
+  for (int e = 0; e < m.E; ++e) {
+    std::vector<int> key(m.nvc);
+    for (int k = 0; k < m.nvc; ++k) key[k] = m.vid[m.cv[static_cast<size_t>(e) * m.nvc + k]];
+    std::sort(key.begin(), key.end());
+    byv[key] = e;
+  }
+  std::vector<double> c(static_cast<size_t>(m.E) * mnp, 0.0);
+  std::vector<char> seen(m.E, 0);
+  size_t p = 5;
+  for (int i = 0; i < ncell; ++i) {
+    ++p;  // type
+    p += go;
+    std::vector<int> key(m.nvc);
+    for (int k = 0; k < m.nvc; ++k) key[k] = std::atoi(tok[p++].c_str());
+    std::sort(key.begin(), key.end());
+    const int order = std::atoi(tok[p++].c_str());
+    auto f = byv.find(key);
+    if (f == byv.end()) return fail(DGP_ERR_IO, "checkpoint cell " + std::to_string(i) + " is not in the mesh");
+    if (order != s->order) return fail(DGP_ERR_UNSUPPORTED, "checkpoint cell order differs from the solver's");
+    const int e = f->second;
+    seen[e] = 1;
+    for (size_t k = 0; k < mnp; ++k) c[e * mnp + k] = std::strtod(tok[p++].c_str(), nullptr);
+  }
+  for (int e = 0; e < m.E; ++e)
+    if (!seen[e]) return fail(DGP_ERR_IO, "checkpoint misses cell " + std::to_string(e));
+  DGP_CUDA(cudaSetDevice(s->device));
+  DGP_CUDA(cudaStreamSynchronize(s->stream));
+  if (int rc = host_to_state(s, c.data(), s->b.C)) return rc;
+  s->ops.trace(s->b, nullptr, s->stream);
+  DGP_CUDA(cudaGetLastError());
+  DGP_CUDA(cudaStreamSynchronize(s->stream));
+  if (t) *t = tt;
+  if (iter) *iter = it;
   return DGP_OK;
 }
 
@@ -795,7 +911,7 @@ int dgp_cfl_dt(dgp_solver s, double cfl, double* dt) {
 // follows every stage and the next step's CFL reduction runs on the limited
 // state (instead of inside the last stage's element kernel)
 static void launch_step(dgp_solver s, int fuse_cfl) {
-  const bool lim = s->limiter == DGP_LIMITER_MOMENT && s->ops.limit;
+  const bool lim = s->limiter != DGP_LIMITER_NONE && s->ops.limit;
   s->ops.stage(s->b, 1, 0.0, 0, s->stream);
   if (lim) s->ops.limit(s->b, 1, s->stream);
   s->ops.stage(s->b, 2, 1.0, 0, s->stream);
@@ -805,12 +921,14 @@ static void launch_step(dgp_solver s, int fuse_cfl) {
     s->ops.limit(s->b, 1, s->stream);
     if (fuse_cfl) s->ops.cfl(s->b, s->stream);
   }
+  if (!s->probes.empty()) launch_probe_recorders(s);
 }
 
 int dgp_launches_per_step(dgp_solver s, int* n) {
   if (!s || !n) return fail(DGP_ERR_INVALID, "null argument");
-  const bool lim = s->limiter == DGP_LIMITER_MOMENT && s->ops.limit;
-  *n = 3 * (s->b.p0 ? 3 : 2) + (lim ? 3 * 2 + 1 : 0);
+  const bool lim = s->limiter != DGP_LIMITER_NONE && s->ops.limit;
+  const int per_pass = s->limiter == DGP_LIMITER_BARTH ? 1 : 2;
+  *n = 3 * (s->b.p0 ? 3 : 2) + (lim ? 3 * per_pass + 1 : 0);
   return DGP_OK;
 }
 
@@ -856,6 +974,7 @@ int dgp_run(dgp_solver s, double t0, double tend, double cfl, int max_steps, dou
   if (tail && !s->graph1)
     if (int rc = capture(1, &s->graph1)) return rc;
   if (int rc = set_ctl(s, t0, 0.0, tend, cfl, max_steps)) return rc;
+  if (int rc = reset_probe_recorders(s)) return rc;
   s->ops.cfl(s->b, s->stream);
   DGP_CUDA(cudaGetLastError());
   TimeCtl c{};
@@ -874,7 +993,7 @@ int dgp_run(dgp_solver s, double t0, double tend, double cfl, int max_steps, dou
 
 int dgp_limit(dgp_solver s, unsigned char* triggers) {
   if (!s) return fail(DGP_ERR_INVALID, "null solver");
-  if (s->limiter != DGP_LIMITER_MOMENT) return fail(DGP_ERR_INVALID, "solver created without a limiter");
+  if (s->limiter == DGP_LIMITER_NONE) return fail(DGP_ERR_INVALID, "solver created without a limiter");
   DGP_CUDA(cudaSetDevice(s->device));
   if (s->ops.limit) s->ops.limit(s->b, 0, s->stream);
   DGP_CUDA(cudaGetLastError());
@@ -884,7 +1003,7 @@ int dgp_limit(dgp_solver s, unsigned char* triggers) {
 
 int dgp_limiter_triggers(dgp_solver s, unsigned char* out) {
   if (!s || !out) return fail(DGP_ERR_INVALID, "null argument");
-  if (s->limiter != DGP_LIMITER_MOMENT) return fail(DGP_ERR_INVALID, "solver created without a limiter");
+  if (s->limiter == DGP_LIMITER_NONE) return fail(DGP_ERR_INVALID, "solver created without a limiter");
   DGP_CUDA(cudaSetDevice(s->device));
   DGP_CUDA(cudaStreamSynchronize(s->stream));
   const int E = s->b.E;
@@ -947,6 +1066,30 @@ int dgp_l2_error(dgp_solver s, double t, int field, double* err) {
   double acc = 0.0;
   for (double v : p) acc += v;
   *err = std::sqrt(acc);
+  return DGP_OK;
+}
+
+int dgp_error_norms(dgp_solver s, double t, int quantity, int rule, double* norms) {
+  if (!s || !norms || (rule != 0 && rule != 1) || quantity >= s->b.M || quantity < -2)
+    return fail(DGP_ERR_INVALID, "bad argument");
+  if (quantity < 0 && s->law != DGP_LAW_EULER2D && s->law != DGP_LAW_EULER3D)
+    return fail(DGP_ERR_INVALID, "pressure and entropy errors are defined for the Euler laws");
+  DGP_CUDA(cudaSetDevice(s->device));
+  s->ops.norms(s->b, t, quantity, rule, 0, s->b.E, nullptr, s->stream);
+  DGP_CUDA(cudaGetLastError());
+  const int nblk = (s->b.E + 255) / 256;
+  std::vector<double> p(3 * static_cast<size_t>(nblk));
+  DGP_CUDA(cudaMemcpyAsync(p.data(), s->b.partials, p.size() * 8, cudaMemcpyDeviceToHost, s->stream));
+  DGP_CUDA(cudaStreamSynchronize(s->stream));
+  double l1 = 0.0, l2 = 0.0, li = 0.0;
+  for (int k = 0; k < nblk; ++k) {
+    l1 += p[3 * k];
+    l2 += p[3 * k + 1];
+    li = std::max(li, p[3 * k + 2]);
+  }
+  norms[0] = l1;
+  norms[1] = std::sqrt(l2);
+  norms[2] = li;
   return DGP_OK;
 }
 
@@ -1030,7 +1173,8 @@ int dgp_ensemble_create(int n, const dgp_mesh* meshes, const dgp_law* laws, cons
   if (n <= 0 || !meshes || !laws || !orders || !out) return fail(DGP_ERR_INVALID, "bad argument");
   if (precision != DGP_PRECISION_FP64 && precision != DGP_PRECISION_MIXED)
     return fail(DGP_ERR_INVALID, "unknown precision");
-  if (limiter != DGP_LIMITER_NONE && limiter != DGP_LIMITER_MOMENT) return fail(DGP_ERR_INVALID, "unknown limiter");
+  if (limiter != DGP_LIMITER_NONE && limiter != DGP_LIMITER_MOMENT && limiter != DGP_LIMITER_BARTH)
+    return fail(DGP_ERR_INVALID, "unknown limiter");
   std::map<std::tuple<int, int, int, int>, std::vector<int>> groups;
   for (int i = 0; i < n; ++i) {
     if (!meshes[i] || !laws[i]) return fail(DGP_ERR_INVALID, "null mesh or law");
@@ -1455,32 +1599,11 @@ int dgp_adjoint_set_receivers(dgp_solver s, int n, const double* points, const d
   if (!s || n <= 0 || !points || !observed) return fail(DGP_ERR_INVALID, "bad argument");
   if (s->b.ninst) return fail(DGP_ERR_UNSUPPORTED, "receivers are set on a single solver");
   DGP_CUDA(cudaSetDevice(s->device));
-  const HostMesh& m = s->meshes[0];
-  const int dim = m.dim, NP = s->b.NP;
-  std::vector<int> cell(n, -1);
-  std::vector<double> phi(static_cast<size_t>(n) * NP);
-  for (int r = 0; r < n; ++r) {
-    const double* x = points + static_cast<size_t>(r) * dim;
-    // the first cell whose barycentric coordinates are all >= -1e-12
-    for (int e = 0; e < m.E && cell[r] < 0; ++e) {
-      double X0[3], J[9], Ji[9];
-      cell_frame(m, e, X0, J);
-      invert3(J, Ji);
-      double xi[3] = {0, 0, 0};
-      for (int q = 0; q < dim; ++q)
-        for (int c = 0; c < dim; ++c) xi[q] += Ji[c * 3 + q] * (x[c] - X0[c]);
-      double sum = 0.0, mn = 1.0;
-      for (int q = 0; q < dim; ++q) {
-        sum += xi[q];
-        mn = std::min(mn, xi[q]);
-      }
-      if (mn >= -1e-12 && sum <= 1.0 + 1e-12) {
-        cell[r] = s->f2i[e];
-        basis_eval(s->tab, xi, &phi[static_cast<size_t>(r) * NP]);
-      }
-    }
+  std::vector<int> cell;
+  std::vector<double> phi;
+  if (int rc = locate_points(s, n, points, cell, phi)) return rc;
+  for (int r = 0; r < n; ++r)
     if (cell[r] < 0) return fail(DGP_ERR_INVALID, "receiver " + std::to_string(r) + " lies outside the mesh");
-  }
   AdjointState& a = s->adj;
   std::vector<double> obs(observed, observed + n);
   int rc = DGP_OK;
@@ -1537,7 +1660,7 @@ int dgp_forward_checkpointed(dgp_solver s, double t0, double dt, int nsteps, int
   if (!s || !(dt > 0) || nsteps <= 0 || every < 0) return fail(DGP_ERR_INVALID, "bad argument");
   if (s->b.ninst) return fail(DGP_ERR_UNSUPPORTED, "the adjoint runs on a single solver");
   if (!s->ops.adj_stage) return fail(DGP_ERR_UNSUPPORTED, "no discrete adjoint for this law/flux");
-  if (s->limiter == DGP_LIMITER_MOMENT) return fail(DGP_ERR_UNSUPPORTED, "adjoint with the limiter on");
+  if (s->limiter != DGP_LIMITER_NONE) return fail(DGP_ERR_UNSUPPORTED, "adjoint with the limiter on");
   for (const HostMesh& hm : s->meshes)
     for (int pf : hm.pface)
       if (pf >= 0) return fail(DGP_ERR_UNSUPPORTED, "adjoint on a mesh with periodic edges");

@@ -60,8 +60,13 @@ struct AdjointState {
   double* rJ = nullptr;
 };
 
+struct dgp_probe_s;
+
 struct dgp_solver_s {
   AdjointState adj;
+  dgp::PointLocator locator;            // built on first use (receivers, probes)
+  bool locator_ready = false;
+  std::vector<dgp_probe_s*> probes;     // probes of this solver (recorders sample in every step)
   std::vector<dgp::HostMesh> meshes;  // one per instance (one for a single solver)
   std::vector<int> inst_off;          // first internal cell of each instance
   std::vector<int> inst_ufirst;       // first cell of each instance in the joined file order
@@ -83,7 +88,8 @@ struct dgp_solver_s {
     if (graph1) cudaGraphExecDestroy(graph1);
     graph = graph1 = nullptr;
   }
-  ~dgp_solver_s() {
+  ~dgp_solver_s();
+  void destroy_resources() {
     drop_graphs();
     for (void* p : allocs) cudaFree(p);
     if (h_ctl) cudaFreeHost(h_ctl);
@@ -124,6 +130,39 @@ struct dgp_solver_s {
   }
   size_t state_count() const { return static_cast<size_t>(b.E) * b.M * b.NP; }
 };
+
+// Point probes (DGPointSensor / DGLineSensor, DGSensor.cc:88-186): cells and
+// basis values of the points, located once on the host; evaluated on the
+// device, on demand or inside every step of a run (recorder).
+struct dgp_probe_s {
+  dgp_solver s = nullptr;  // cleared when the solver is destroyed first
+  int n = 0, found = 0;
+  int* cell = nullptr;     // [n] internal cell (-1: outside the mesh)
+  double* phi = nullptr;   // [n][Np] basis values at the points
+  double* vals = nullptr;  // [n][M]
+  int every = 0, max_samples = 0;  // recorder: every `every` steps of a run
+  double* rec = nullptr;           // [max_samples][n][M]
+  double* rec_t = nullptr;         // [max_samples] times
+  int* rec_n = nullptr;            // samples taken in the current run
+  std::vector<void*> allocs;
+  ~dgp_probe_s() {
+    for (void* p : allocs) cudaFree(p);
+  }
+};
+
+namespace dgp {
+// point location on a single solver's mesh: internal cell (-1: outside) and
+// basis values of each point (dgp_probe.cu)
+int locate_points(dgp_solver s, int n, const double* points, std::vector<int>& cell, std::vector<double>& phi);
+// probe recorders: launched at the end of every step; reset when a run starts
+void launch_probe_recorders(dgp_solver s);
+int reset_probe_recorders(dgp_solver s);
+}  // namespace dgp
+
+inline dgp_solver_s::~dgp_solver_s() {
+  for (dgp_probe_s* p : probes) p->s = nullptr;
+  destroy_resources();
+}
 
 struct dgp_ensemble_s {
   int n = 0;

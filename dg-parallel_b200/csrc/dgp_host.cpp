@@ -415,6 +415,96 @@ void cell_frame(const HostMesh& m, int e, double* x0, double* J) {
   if (m.dim == 2) J[8] = 1.0;
 }
 
+void PointLocator::build(const HostMesh& mesh) {
+  m = &mesh;
+  const int dim = mesh.dim, E = mesh.E;
+  double hi[3] = {0, 0, 0};
+  for (int k = 0; k < 3; ++k) {
+    lo[k] = 1e300;
+    hi[k] = -1e300;
+  }
+  for (int v = 0; v < (int)(mesh.X.size() / 3); ++v)
+    for (int k = 0; k < dim; ++k) {
+      lo[k] = std::min(lo[k], mesh.X[3 * v + k]);
+      hi[k] = std::max(hi[k], mesh.X[3 * v + k]);
+    }
+  // about one cell per bucket
+  const double per = std::pow(std::max(E, 1), 1.0 / dim);
+  for (int k = 0; k < 3; ++k) {
+    n[k] = k < dim ? std::max(1, (int)per) : 1;
+    const double ext = k < dim ? std::max(hi[k] - lo[k], 1e-300) : 1.0;
+    h[k] = ext / n[k];
+  }
+  auto bucket_range = [&](int e, int* b0, int* b1) {
+    const int* c = &mesh.cv[static_cast<size_t>(e) * mesh.nvc];
+    for (int k = 0; k < 3; ++k) {
+      if (k >= dim) {
+        b0[k] = b1[k] = 0;
+        continue;
+      }
+      double mn = 1e300, mx = -1e300;
+      for (int v = 0; v < mesh.nvc; ++v) {
+        mn = std::min(mn, mesh.X[3 * c[v] + k]);
+        mx = std::max(mx, mesh.X[3 * c[v] + k]);
+      }
+      b0[k] = std::max(0, std::min(n[k] - 1, (int)std::floor((mn - lo[k]) / h[k])));
+      b1[k] = std::max(0, std::min(n[k] - 1, (int)std::floor((mx - lo[k]) / h[k])));
+    }
+  };
+  const size_t nb = static_cast<size_t>(n[0]) * n[1] * n[2];
+  std::vector<int> cnt(nb + 1, 0);
+  for (int pass = 0; pass < 2; ++pass) {
+    if (pass == 1) {
+      off.assign(nb + 1, 0);
+      for (size_t b = 0; b < nb; ++b) off[b + 1] = off[b] + cnt[b];
+      ids.assign(off[nb], 0);
+      std::fill(cnt.begin(), cnt.end(), 0);
+    }
+    for (int e = 0; e < E; ++e) {
+      int b0[3], b1[3];
+      bucket_range(e, b0, b1);
+      for (int z = b0[2]; z <= b1[2]; ++z)
+        for (int y = b0[1]; y <= b1[1]; ++y)
+          for (int x = b0[0]; x <= b1[0]; ++x) {
+            const size_t b = (static_cast<size_t>(z) * n[1] + y) * n[0] + x;
+            if (pass == 1) ids[off[b] + cnt[b]] = e;
+            cnt[b]++;
+          }
+    }
+  }
+}
+
+int PointLocator::locate(const double* x, double* xi) const {
+  const int dim = m->dim;
+  int bi[3] = {0, 0, 0};
+  for (int k = 0; k < dim; ++k) {
+    const double u = (x[k] - lo[k]) / h[k];
+    if (u < -1e-9 * n[k] || u > n[k] * (1 + 1e-9)) return -1;
+    bi[k] = std::max(0, std::min(n[k] - 1, (int)std::floor(u)));
+  }
+  const size_t b = (static_cast<size_t>(bi[2]) * n[1] + bi[1]) * n[0] + bi[0];
+  int best = -1;
+  for (int i = off[b]; i < off[b + 1]; ++i) {
+    const int e = ids[i];
+    if (best >= 0 && e >= best) continue;
+    double X0[3], J[9], Ji[9], r[3] = {0, 0, 0};
+    cell_frame(*m, e, X0, J);
+    invert3(J, Ji);
+    for (int q = 0; q < dim; ++q)
+      for (int c = 0; c < dim; ++c) r[q] += Ji[c * 3 + q] * (x[c] - X0[c]);
+    double sum = 0.0, mn = 1.0;
+    for (int q = 0; q < dim; ++q) {
+      sum += r[q];
+      mn = std::min(mn, r[q]);
+    }
+    if (mn >= -1e-12 && sum <= 1.0 + 1e-12) {
+      best = e;
+      for (int q = 0; q < 3; ++q) xi[q] = q < dim ? r[q] : 0.0;
+    }
+  }
+  return best;
+}
+
 double invert3(const double* A, double* B) {
   double det = A[0] * (A[4] * A[8] - A[5] * A[7]) - A[1] * (A[3] * A[8] - A[5] * A[6]) +
                A[2] * (A[3] * A[7] - A[4] * A[6]);

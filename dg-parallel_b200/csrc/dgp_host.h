@@ -76,4 +76,20 @@ void build_limiter_tables(const RefTables& t, std::vector<double>& D, std::vecto
 void cell_frame(const HostMesh& m, int e, double* x0, double* J);
 double invert3(const double* A, double* B);
 
+// Point location over the cells of one mesh (DGCell::inCell, DGCell.cc:1499-1521:
+// bounding box, then the reference coordinates of the point inside the
+// reference simplex).  A uniform grid of buckets holds every cell whose
+// bounding box meets the bucket; a point takes the lowest-index cell whose
+// reference coordinates are all >= -1e-12 (points on shared faces resolve the
+// same way whatever the bucketing).
+struct PointLocator {
+  const HostMesh* m = nullptr;
+  double lo[3] = {0, 0, 0}, h[3] = {1, 1, 1};
+  int n[3] = {1, 1, 1};
+  std::vector<int> off, ids;  // bucket -> cells (CSR)
+  void build(const HostMesh& mesh);
+  // cell index (file order of the mesh) or -1; xi: reference coordinates
+  int locate(const double* x, double* xi) const;
+};
+
 }  // namespace dgp

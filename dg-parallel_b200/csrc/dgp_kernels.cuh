@@ -655,6 +655,86 @@ __global__ void __launch_bounds__(256) l2err_kernel(const __grid_constant__ Stag
   if (threadIdx.x == 0) partials[blockIdx.x] = acc;
 }
 
+// Error family of DGError.cc (DGCell::L1exact :549, LinfError :567,
+// L1exactPressure :601, entropyErrorL1_2D/3D :621-665, pressureErrorL2 :774,
+// densityErrorL2 :805, entropyErrorL2_2D :687): per-block partial L1 and
+// squared-L2 sums and the maximum of |d| over the rule's points, where d is the
+// difference to the exact field of a field (quantity >= 0), of the pressure
+// (-1) or the entropy deviation (p / p_ex) / (rho / rho_ex)^gamma - 1 (-2),
+// gamma = 1.4 as those functions fix it.  rule 0: the volume rule of degree
+// 2p; rule 1: degree 2(p+1).  partials[3 * block + {0, 1, 2}].
+template <int LAW, int DIM>
+__device__ __forceinline__ double err_pressure(const double* v) {
+  double m2 = v[1] * v[1] + v[2] * v[2];
+  if constexpr (LAW == DGP_LAW_EULER3D) m2 += v[4] * v[4];
+  return (1.4 - 1.) * (v[3] - 0.5 * m2 / v[0]);
+}
+
+template <class K>
+__global__ void __launch_bounds__(256) norms_kernel(const __grid_constant__ StageArgs<typename K::T> a, double t,
+                                                     int quantity, int rule, double* partials, int e_begin,
+                                                     int e_end, const LawParams* lpp) {
+  constexpr int M = K::M, NP = K::NP;
+  __shared__ double red[256 / 32];
+  const int e = e_begin + blockIdx.x * 256 + threadIdx.x;
+  const LawParams& lp = lpp ? *lpp : a.law;
+  double l1 = 0.0, l2 = 0.0, li = 0.0;
+  if (e < e_end) {
+    const double* x0 = a.mesh.x0 + 3 * (size_t)e;
+    const double* J = a.mesh.jac + 9 * (size_t)e;
+    const double* c = a.C + (size_t)e * K::MNP;
+    const double detj = a.mesh.detjd[e];
+    const int nq = rule ? a.tab.nqe : K::NQ;
+    for (int q = 0; q < nq; ++q) {
+      const double* xi = rule ? a.tab.eqp + 3 * q : a.tab.qpd + 3 * q;
+      const double* ph = rule ? a.tab.ephi + q * NP : a.tab.phiq + q * NP;
+      const double w = rule ? a.tab.eqw[q] : a.tab.qwd[q];
+      double x[3];
+      for (int cc = 0; cc < 3; ++cc) {
+        x[cc] = x0[cc];
+        for (int r = 0; r < K::DIM; ++r) x[cc] += xi[r] * J[r * 3 + cc];
+      }
+      double v[M], ex[M];
+#pragma unroll
+      for (int j = 0; j < M; ++j) {
+        double acc = 0.0;
+        for (int k = 0; k < NP; ++k) acc += ph[k] * c[j * NP + k];
+        v[j] = acc;
+      }
+      field_eval<double>(lp, x, t, ex);
+      double d = 0.0;
+      if constexpr (K::LAW == DGP_LAW_EULER2D || K::LAW == DGP_LAW_EULER3D) {
+        if (quantity == -2) {
+          d = (err_pressure<K::LAW, K::DIM>(v) / err_pressure<K::LAW, K::DIM>(ex)) / pow(v[0] / ex[0], 1.4) - 1.;
+        } else if (quantity == -1) {
+          d = err_pressure<K::LAW, K::DIM>(v) - err_pressure<K::LAW, K::DIM>(ex);
+        }
+      }
+      if (quantity >= 0) {
+#pragma unroll
+        for (int j = 0; j < M; ++j)
+          if (j == quantity) d = v[j] - ex[j];
+      }
+      const double jw = detj * w;
+      l1 += fabs(d) * jw;
+      l2 += d * d * jw;
+      li = fabs(d) > li ? fabs(d) : li;
+    }
+  }
+  l1 = block_sum<256>(l1, red);
+  l2 = block_sum<256>(l2, red);
+  for (int o = 16; o > 0; o >>= 1) li = fmax(li, __shfl_xor_sync(0xffffffffu, li, o));
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = li;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double m = 0.0;
+    for (int w = 0; w < 256 / 32; ++w) m = fmax(m, red[w]);
+    partials[3 * (size_t)blockIdx.x] = l1;
+    partials[3 * (size_t)blockIdx.x + 1] = l2;
+    partials[3 * (size_t)blockIdx.x + 2] = m;
+  }
+}
+
 // per-block partial cell integrals of every field: |J| * |ref| * phi0 * c[j][0]
 template <class K>
 __global__ void __launch_bounds__(256) totals_kernel(const __grid_constant__ StageArgs<typename K::T> a, double refm,

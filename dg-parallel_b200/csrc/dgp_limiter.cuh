@@ -21,8 +21,8 @@
 //     cell).  Component a is bounded in x by the differences of the
 //     derivative d^(n-1)/dx^(n-1-a)dy^a of the degree-(n-1) blocks of the
 //     left/right neighbours, in y by d^(n-1)/dx^(n-a)dy^(a-1) of the
-//     bottom/top neighbours, each divided by the distance of the bounding-box
-//     centres (degree 0: the cell mean).  A limited degree maps back to its
+//     bottom/top neighbours, each times the reciprocal (rounded once) of the
+//     distance of the bounding-box centres (degree 0: the cell mean).  A limited degree maps back to its
 //     modal block exactly; the mean never changes.
 //   * Trigger (the sensor) of a cell: lowest limited degree over its fields,
 //     0 when untouched (the kernels record it per row; the host reduces).
@@ -181,15 +181,14 @@ __global__ void __launch_bounds__(128) limit_moments_kernel(LimArgs a) {
 }
 
 // one degree N of one row from the moments in registers (mo: the row's own,
-// mn: the neighbours' degrees 0..p-1, pc: the neighbours' bounding-box centre
-// coordinate across the shared direction); returns false when the descent ends
+// mn: the neighbours' degrees 0..p-1, rc: reciprocals of the signed distances
+// to the neighbours' bounding-box centres); returns false when the descent ends
 template <int N, int NP, int NL>
 __device__ __forceinline__ bool lim_degree(const LimArgs& a, const double (&mo)[NP], const double (&mn)[4][NL],
-                                           const double (&pc)[4], const int (&nb)[4], const double* gg,
+                                           const double (&rc)[4], const int (&nb)[4], const double* gg,
                                            unsigned big, double* row, unsigned& mod) {
   constexpr int base = N * (N + 1) / 2, lo = (N - 1) * N / 2, w = N + 1, off = N * (N + 1) * (2 * N + 1) / 6;
   if (!((big >> N) & 1u)) return true;
-  const double px = gg[4], py = gg[5];
   double gl[N + 1];
   bool any = false;
 #pragma unroll
@@ -204,8 +203,8 @@ __device__ __forceinline__ bool lim_degree(const LimArgs& a, const double (&mo)[
       double fwd = 0.0, bwd = 0.0;
       if (c <= N - 1) {
         const double he = mo[lo + c];
-        if (nb[1] >= 0) fwd = __dsub_rn(mn[1][lo + c], he) / __dsub_rn(pc[1], px);
-        if (nb[0] >= 0) bwd = __dsub_rn(he, mn[0][lo + c]) / __dsub_rn(px, pc[0]);
+        if (nb[1] >= 0) fwd = __dmul_rn(__dsub_rn(mn[1][lo + c], he), rc[1]);
+        if (nb[0] >= 0) bwd = __dmul_rn(__dsub_rn(he, mn[0][lo + c]), rc[0]);
       }
       if (nb[0] >= 0 && nb[1] >= 0) t1 = lim_minmod3(g, fwd, bwd, l1);
       else if (nb[0] >= 0) t1 = lim_minmod2(g, bwd, l1);
@@ -215,8 +214,8 @@ __device__ __forceinline__ bool lim_degree(const LimArgs& a, const double (&mo)[
       double fwd = 0.0, bwd = 0.0;
       if (c >= 1) {
         const double he = mo[lo + c - 1];
-        if (nb[3] >= 0) fwd = __dsub_rn(mn[3][lo + c - 1], he) / __dsub_rn(pc[3], py);
-        if (nb[2] >= 0) bwd = __dsub_rn(he, mn[2][lo + c - 1]) / __dsub_rn(py, pc[2]);
+        if (nb[3] >= 0) fwd = __dmul_rn(__dsub_rn(mn[3][lo + c - 1], he), rc[3]);
+        if (nb[2] >= 0) bwd = __dmul_rn(__dsub_rn(he, mn[2][lo + c - 1]), rc[2]);
       }
       if (nb[2] >= 0 && nb[3] >= 0) t2 = lim_minmod3(g, fwd, bwd, l2);
       else if (nb[2] >= 0) t2 = lim_minmod2(g, bwd, l2);
@@ -263,11 +262,11 @@ __device__ __forceinline__ bool lim_degree(const LimArgs& a, const double (&mo)[
 
 template <int N, int NP, int NL>
 __device__ __forceinline__ void lim_descend(const LimArgs& a, const double (&mo)[NP], const double (&mn)[4][NL],
-                                            const double (&pc)[4], const int (&nb)[4], const double* gg,
+                                            const double (&rc)[4], const int (&nb)[4], const double* gg,
                                             unsigned big, double* row, unsigned& mod) {
   if constexpr (N >= 1) {
-    if (lim_degree<N, NP, NL>(a, mo, mn, pc, nb, gg, big, row, mod))
-      lim_descend<N - 1, NP, NL>(a, mo, mn, pc, nb, gg, big, row, mod);
+    if (lim_degree<N, NP, NL>(a, mo, mn, rc, nb, gg, big, row, mod))
+      lim_descend<N - 1, NP, NL>(a, mo, mn, rc, nb, gg, big, row, mod);
   }
 }
 
@@ -297,7 +296,7 @@ __global__ void __launch_bounds__(128) limit_kernel(LimArgs a) {
   int trig = 0;
   if (big >> 1) {
     const int nb[4] = {n4.x, n4.y, n4.z, n4.w};
-    double mo[NP], mn[4][NL], pc[4];
+    double mo[NP], mn[4][NL], rc[4];
 #pragma unroll
     for (int k = 0; k < NP; ++k) mo[k] = a.Mo[r * NP + k];
 #pragma unroll
@@ -306,11 +305,14 @@ __global__ void __launch_bounds__(128) limit_kernel(LimArgs a) {
       const double* src = a.Mo + ((size_t)n * M + j) * NP;
 #pragma unroll
       for (int k = 0; k < NL; ++k) mn[d][k] = src[k];
-      pc[d] = __ldg(a.geo + (size_t)n * kLimGeo + (d < 2 ? 8 : 9));
+      const double pc = __ldg(a.geo + (size_t)n * kLimGeo + (d < 2 ? 8 : 9));
+      const double own = gg[d < 2 ? 4 : 5];
+      // left / bottom: own - theirs; right / top: theirs - own
+      rc[d] = 1.0 / ((d & 1) ? __dsub_rn(pc, own) : __dsub_rn(own, pc));
     }
     double row[NP];
     unsigned mod = 0;
-    lim_descend<P, NP, NL>(a, mo, mn, pc, nb, gg, big, row, mod);
+    lim_descend<P, NP, NL>(a, mo, mn, rc, nb, gg, big, row, mod);
     if (mod) {
       trig = __ffs(mod) - 1;  // lowest limited degree
       // the row as it leaves the limiter: unchanged blocks from the state,
@@ -338,6 +340,135 @@ __global__ void __launch_bounds__(128) limit_kernel(LimArgs a) {
     }
   }
   a.trig[r] = static_cast<unsigned char>(trig);
+}
+
+// -----------------------------------------------------------------------------
+// Barth limiter (DGBarthLimiter::limit, DGLimiter.cc:184-287), cell by cell as
+// the reference computes it on the cell's coefficients:
+//   * bounds: max / min over the interior-face neighbours' means (the cell's
+//     own mean is not included); a cell without an interior neighbour is left
+//     alone (the reference would read uninitialised bounds);
+//   * every face point of every face of the cell (boundary faces included):
+//     val = the cell's coefficients against the LEFT cell's basis values at the
+//     point (the reference interpolates with pg->fctleft whichever side the
+//     cell is on), phi = (bound - mean) / (val - mean) where val leaves
+//     [min, max], 1 inside, clamped at 0; the field's slope factor is the
+//     minimum over the points;
+//   * degrees p..2: the block is zeroed when the factor is below 0.9; the
+//     degree-1 block is scaled by the factor.
+// The mean (mode 0) never changes, so every cell reads its neighbours' means
+// from the state being limited in place.  Triggers: 1 where a factor is below 1.
+struct BarthArgs {
+  double* C;
+  unsigned char* trig;  // [E * M] (the cell's value in every row)
+  const int* cface;     // [E][NLF] face of each local face
+  const int* fel;       // [F][2]
+  const int* fcode;     // [F] lfL | lfR << 4 | perm << 8
+  const double* phif;   // [NLF * NQF][NP] FP64 face-point basis values
+  double phi0;          // constant basis function (mean = c0 * phi0)
+  void* tr;             // face-point traces (slot layout, right-hand-side type)
+  const void* phif_t;   // the same basis values in the right-hand-side type
+  const TimeCtl* ctl;
+  const TimeCtl* gctl;
+  const int* cell_inst;
+  int E;
+};
+
+template <class K>
+__global__ void __launch_bounds__(128) barth_kernel(BarthArgs a) {
+  using T = typename K::T;
+  constexpr int M = K::M, NP = K::NP, NLF = K::NLF, NQF = K::NQF, NS = K::NS;
+  constexpr int S1 = K::DIM == 2 ? 3 : 4;  // modes of degree <= 1
+  if (a.ctl && a.gctl->done) return;
+  const int e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= a.E) return;
+  if (a.cell_inst) {
+    const int i = a.cell_inst[e];
+    if (i < 0 || (a.ctl && a.ctl[i].done)) return;
+  }
+  int fc[NLF];
+#pragma unroll
+  for (int l = 0; l < NLF; ++l) fc[l] = __ldg(a.cface + (size_t)e * NLF + l);
+  double mx[M], mn[M];
+  int kk = 0;
+#pragma unroll
+  for (int l = 0; l < NLF; ++l) {
+    const int f = fc[l];
+    if (f < 0) continue;
+    const int eL = __ldg(a.fel + 2 * f), eR = __ldg(a.fel + 2 * f + 1);
+    if (eR < 0) continue;
+    const int o = eL == e ? eR : eL;
+#pragma unroll
+    for (int j = 0; j < M; ++j) {
+      const double m = __dmul_rn(a.C[((size_t)o * M + j) * NP], a.phi0);
+      if (kk == 0) {
+        mx[j] = m;
+        mn[j] = m;
+      } else {
+        mx[j] = m > mx[j] ? m : mx[j];
+        mn[j] = m < mn[j] ? m : mn[j];
+      }
+    }
+    ++kk;
+  }
+  unsigned char trig = 0;
+  if (kk > 0) {
+    double* c = a.C + (size_t)e * M * NP;
+    double slope[M], mean[M];
+#pragma unroll
+    for (int j = 0; j < M; ++j) {
+      slope[j] = 1.0;
+      mean[j] = __dmul_rn(c[j * NP], a.phi0);
+    }
+#pragma unroll
+    for (int l = 0; l < NLF; ++l) {
+      const int f = fc[l];
+      if (f < 0) continue;
+      const int lfL = __ldg(a.fcode + f) & 15;
+      for (int q = 0; q < NQF; ++q) {
+        const double* ph = a.phif + (size_t)(lfL * NQF + q) * NP;
+#pragma unroll
+        for (int j = 0; j < M; ++j) {
+          double v = 0.0;
+#pragma unroll
+          for (int k = 0; k < NP; ++k) v = __dadd_rn(v, __dmul_rn(c[j * NP + k], __ldg(ph + k)));
+          double phin = 1.0;
+          if (v > mx[j]) phin = __dsub_rn(mx[j], mean[j]) / __dsub_rn(v, mean[j]);
+          else if (v < mn[j]) phin = __dsub_rn(mn[j], mean[j]) / __dsub_rn(v, mean[j]);
+          if (phin < 0.0) phin = 0.0;
+          slope[j] = slope[j] < phin ? slope[j] : phin;
+        }
+      }
+    }
+#pragma unroll
+    for (int j = 0; j < M; ++j) {
+      if (!(slope[j] < 1.0)) continue;
+      trig = 1;
+      if (slope[j] < 0.9)
+        for (int k = S1; k < NP; ++k) c[j * NP + k] = 0.0;  // degrees p..2
+#pragma unroll
+      for (int k = 1; k < S1; ++k) c[j * NP + k] = __dmul_rn(c[j * NP + k], slope[j]);
+    }
+    if (trig) {
+      // the cell's face-point traces for the next stage's face kernel
+      const T* pt = static_cast<const T*>(a.phif_t);
+      T* tr = static_cast<T*>(a.tr);
+#pragma unroll 1
+      for (int j = 0; j < M; ++j) {
+        T ck[NP];
+#pragma unroll
+        for (int k = 0; k < NP; ++k) ck[k] = (T)c[j * NP + k];
+        for (int s = 0; s < NS; ++s) {
+          T acc = 0;
+#pragma unroll
+          for (int k = 0; k < NP; ++k) acc += __ldg(pt + s * NP + k) * ck[k];
+          tr[slot_index<K>(e, s, j)] = acc;
+        }
+      }
+    }
+  }
+#pragma unroll
+  for (int j = 0; j < M; ++j) a.trig[(size_t)e * M + j] = trig;
 }
 
 }  // namespace dgp

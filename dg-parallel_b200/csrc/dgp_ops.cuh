@@ -92,10 +92,31 @@ void ops_trace(const DeviceBuffers& b, const unsigned char* only, cudaStream_t s
   trace_kernel<K><<<ops_grid_elem<K>(b.E), K::BLOCK, 0, st>>>(a, only);
 }
 
-// triangle moment limiter on the current state: moments of every row, then
-// the limited rows (and their traces) in place
+// the solver's limiter on the current state.  Barth: one pass in place.
+// Triangle moment limiter: moments of every row, then the limited rows (and
+// their traces) in place.
 template <class K>
 void ops_limit(const DeviceBuffers& b, int check_done, cudaStream_t st) {
+  if constexpr (K::ORDER >= 1) {
+    if (b.limiter_kind == DGP_LIMITER_BARTH) {
+      BarthArgs a;
+      a.C = static_cast<double*>(b.C);
+      a.trig = b.trig;
+      a.cface = b.cface;
+      a.fel = b.fel;
+      a.fcode = b.fcode;
+      a.phif = b.bphif;
+      a.phi0 = b.phi0;
+      a.tr = b.tr;
+      a.phif_t = b.phif;
+      a.ctl = check_done ? b.ctl : nullptr;
+      a.gctl = b.gctl;
+      a.cell_inst = b.cell_inst;
+      a.E = b.E;
+      barth_kernel<K><<<(b.E + 127) / 128, 128, 0, st>>>(a);
+      return;
+    }
+  }
   if constexpr (K::DIM == 2 && K::ORDER >= 1) {
     LimArgs a;
     a.C = static_cast<double*>(b.C);
@@ -159,6 +180,14 @@ void ops_project(const DeviceBuffers& b, double t, cudaStream_t st) {
 }
 
 template <class K>
+void ops_norms(const DeviceBuffers& b, double t, int quantity, int rule, int e_begin, int e_end,
+               const LawParams* lp, cudaStream_t st) {
+  auto a = make_args<typename K::T>(b);
+  norms_kernel<K><<<(e_end - e_begin + 255) / 256, 256, 0, st>>>(a, t, quantity, rule, b.partials, e_begin, e_end,
+                                                                 lp);
+}
+
+template <class K>
 void ops_l2err(const DeviceBuffers& b, double t, int field, int e_begin, int e_end, const LawParams* lp,
                cudaStream_t st) {
   StageArgs<typename K::T> a = make_args<typename K::T>(b);
@@ -193,9 +222,10 @@ Ops make_ops() {
   o.cfl = &ops_cfl<K>;
   o.project = &ops_project<K>;
   o.l2err = &ops_l2err<K>;
+  o.norms = &ops_norms<K>;
   o.totals = &ops_totals<K>;
   o.grid_elem = &ops_grid_elem<K>;
-  o.limit = (K::DIM == 2 && K::ORDER >= 1) ? &ops_limit<K> : nullptr;
+  o.limit = K::ORDER >= 1 ? &ops_limit<K> : nullptr;
   o.adj_stage = adjoint_built<K>() ? &ops_adj_stage<K> : nullptr;
   o.trace = &ops_trace<K>;
   return o;

@@ -63,6 +63,9 @@ struct DeviceBuffers {
   // P0 fallback and triangle moment limiter
   int p0 = 0;                     // 1: DGCell::setToZero fallback on
   unsigned char* bad = nullptr;   // [E] P0 marks
+  int limiter_kind = 0;           // DGP_LIMITER_* of the solver
+  int* cface = nullptr;           // Barth: [E][NLF] face of each local face
+  double* bphif = nullptr;        // Barth: FP64 face-point basis values [NLF * NQF][NP]
   unsigned char* trig = nullptr;  // [E * M] trigger degree of each row in the last limiter pass
   unsigned char* lbig = nullptr;  // [E * M] degrees with a mode above the limiter's threshold
   double* lmo = nullptr;          // [E * M][NP] moments of every degree of each row
@@ -168,6 +171,8 @@ struct Ops {
   void (*cfl)(const DeviceBuffers&, cudaStream_t) = nullptr;
   void (*project)(const DeviceBuffers&, double t, cudaStream_t) = nullptr;
   // over cells [e_begin, e_end); lp: field parameters (nullptr: the solver's law)
+  void (*norms)(const DeviceBuffers&, double t, int quantity, int rule, int e_begin, int e_end, const LawParams* lp,
+                cudaStream_t);
   void (*l2err)(const DeviceBuffers&, double t, int field, int e_begin, int e_end, const LawParams* lp,
                 cudaStream_t) = nullptr;
   void (*totals)(const DeviceBuffers&, double refm, int e_begin, int e_end, cudaStream_t) = nullptr;

@@ -18,7 +18,7 @@ LAW_SCALAR, LAW_BURGERS2D, LAW_EULER2D, LAW_EULER3D, LAW_MAXWELL3D = range(5)
 FLUX_UPWIND, FLUX_CENTRAL, FLUX_GODUNOV, FLUX_ROE, FLUX_LLF = range(5)
 FIELD_GAUSS, FIELD_VORTEX, FIELD_PULSE3D, FIELD_SINE, FIELD_GAUSS3D, FIELD_TM110 = range(6)
 FP64, MIXED = 0, 1
-LIMITER_NONE, LIMITER_MOMENT = 0, 1
+LIMITER_NONE, LIMITER_MOMENT, LIMITER_BARTH = 0, 1, 2
 NPARAMS = 16
 
 ERRORS = {-1: "invalid argument", -2: "I/O", -3: "unsupported", -4: "CUDA", -5: "non-physical",
@@ -71,6 +71,15 @@ def lib() -> ctypes.CDLL:
         "dgp_run": ([P, D, D, D, I, pD, pI], I),
         "dgp_status": ([P, pI, pI], I),
         "dgp_l2_error": ([P, D, I, pD], I),
+        "dgp_error_norms": ([P, D, I, I, pD], I),
+        "dgp_checkpoint_write": ([P, ctypes.c_char_p, D, I], I),
+        "dgp_checkpoint_read": ([P, ctypes.c_char_p, pD, pI], I),
+        "dgp_probe_create": ([P, I, pD, pP, pI], I),
+        "dgp_probe_destroy": ([P], I),
+        "dgp_probe_info": ([P, pI, pI], I),
+        "dgp_probe_eval": ([P, pD], I),
+        "dgp_probe_record": ([P, I, I], I),
+        "dgp_probe_samples": ([P, pI, pD, pD], I),
         "dgp_totals": ([P, pD], I),
         "dgp_synchronize": ([P], I),
         "dgp_solver_stream": ([P, pP], I),
@@ -270,6 +279,25 @@ class Solver:
         check(lib().dgp_l2_error(self.h, t, field, ctypes.byref(e)))
         return e.value
 
+    def write_checkpoint(self, path: str, t: float, iteration: int = 0):
+        """DGAnalysis::write's data stream (readable by DGAnalysis::read)."""
+        check(lib().dgp_checkpoint_write(self.h, path.encode(), t, iteration))
+
+    def read_checkpoint(self, path: str) -> tuple[float, int]:
+        """Load a DGAnalysis::write / dgp_checkpoint_write file; returns (t, iteration)."""
+        t = ctypes.c_double()
+        it = ctypes.c_int()
+        check(lib().dgp_checkpoint_read(self.h, path.encode(), ctypes.byref(t), ctypes.byref(it)))
+        return t.value, it.value
+
+    def error_norms(self, t: float, quantity: int = 0, rule: int = 1) -> np.ndarray:
+        """(L1, L2, Linf) against the exact field: quantity >= 0 a field, -1 the
+        pressure, -2 the entropy deviation (Euler); rule 0 the volume rule of
+        degree 2p, 1 the rule of degree 2(p+1)."""
+        out = np.zeros(3)
+        check(lib().dgp_error_norms(self.h, t, quantity, rule, _dp(out)))
+        return out
+
     def totals(self) -> np.ndarray:
         out = np.zeros(self.nfields)
         check(lib().dgp_totals(self.h, _dp(out)))
@@ -356,6 +384,71 @@ class Solver:
             self.close()
         except Exception:
             pass
+
+
+class Probe:
+    """Point probe (DGPointSensor; a line sensor is a Probe over line_points):
+    every field at every point, evaluated on the device, on demand or recorded
+    inside the steps of a run."""
+
+    def __init__(self, solver: "Solver", points):
+        pts = np.ascontiguousarray(points, dtype=np.float64)
+        self.solver = solver
+        self.n = pts.shape[0]
+        self.nfields = solver.nfields
+        found = np.zeros(self.n, dtype=np.int32)
+        h = ctypes.c_void_p()
+        check(lib().dgp_probe_create(solver.h, self.n, _dp(pts), ctypes.byref(h), _ip(found)))
+        self.h = h
+        self.found = found.astype(bool)
+
+    def eval(self) -> np.ndarray:
+        """[n][fields] of the current state (NaN outside the mesh)."""
+        out = np.zeros((self.n, self.nfields))
+        check(lib().dgp_probe_eval(self.h, _dp(out)))
+        return out
+
+    def record(self, every: int, max_samples: int):
+        """Sample after every `every`-th step of the following runs (0: stop)."""
+        self.max_samples = max_samples
+        check(lib().dgp_probe_record(self.h, every, max_samples))
+
+    def samples(self):
+        """(times [k], values [k][n][fields]) of the last run."""
+        k = ctypes.c_int()
+        ms = max(getattr(self, "max_samples", 0), 1)
+        t = np.zeros(ms)
+        v = np.zeros((ms, self.n, self.nfields))
+        check(lib().dgp_probe_samples(self.h, ctypes.byref(k), _dp(t), _dp(v)))
+        return t[:k.value].copy(), v[:k.value].copy()
+
+    def close(self):
+        if self.h:
+            lib().dgp_probe_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def line_points(p1, p2, n: int) -> np.ndarray:
+    """DGLineSensor's samples: p1 + (p2 - p1) i / (n - 1), i = 0..n-1."""
+    p1 = np.asarray(p1, dtype=np.float64)
+    p2 = np.asarray(p2, dtype=np.float64)
+    return p1[None, :] + (p2 - p1)[None, :] * (np.arange(n, dtype=np.float64) / (n - 1))[:, None]
+
+
+def first_crossing(values: np.ndarray, field: int, threshold: float) -> int:
+    """DGTresholdLineSensor: index of the first sample whose field value lies on
+    the other side of `threshold` from the previous sample's (-1: none)."""
+    v = values[:, field]
+    for i in range(1, len(v)):
+        if (v[i] > threshold and v[i - 1] < threshold) or (v[i] < threshold and v[i - 1] > threshold):
+            return i
+    return -1
 
 
 def autotune(mesh: "Mesh", law: "Law", order: int, precision: int = FP64, limiter: int = 0,

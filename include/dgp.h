@@ -60,11 +60,13 @@ extern "C" {
 
 #define DGP_LIMITER_NONE 0
 #define DGP_LIMITER_MOMENT 1
+#define DGP_LIMITER_BARTH 2
 
 typedef struct dgp_mesh_s* dgp_mesh;
 typedef struct dgp_law_s* dgp_law;
 typedef struct dgp_solver_s* dgp_solver;
 typedef struct dgp_ensemble_s* dgp_ensemble;
+typedef struct dgp_probe_s* dgp_probe;
 
 const char* dgp_last_error(void);
 int dgp_version(void);
@@ -127,7 +129,13 @@ int dgp_launches_per_step(dgp_solver s, int* n);
  * dgp_project (DGAnalysis.cc:276-291).  dgp_limit applies it once to the
  * current state; triggers (may be NULL) receives per cell, in file order, the
  * lowest limited degree (0: untouched) -- the DGSensor trigger indicator.
- * dgp_limiter_triggers returns the triggers of the last application. */
+ * dgp_limiter_triggers returns the triggers of the last application.
+ * Barth limiter (DGP_LIMITER_BARTH; DGBarthLimiter::limit, DGLimiter.cc:184-287,
+ * triangles and tets): per cell and field, the slope factor from the
+ * neighbours' mean bounds at the face points scales the degree-1 modes and,
+ * below 0.9, zeroes the higher ones, in place (the reference's
+ * TimeIntegrator::limit would copy the unwritten second slot back over it);
+ * applied at the same places; triggers are 1 where a factor is below 1. */
 int dgp_limit(dgp_solver s, unsigned char* triggers);
 int dgp_limiter_triggers(dgp_solver s, unsigned char* out);
 /* P0 fallback of DGBoundaryCell::computeBoundaryContributions + DGCell::setToZero
@@ -140,6 +148,43 @@ int dgp_status(dgp_solver s, int* nonphysical, int* first_bad_cell);
 /* L2 error of one field against the law's exact field (DGCell::densityErrorL2,
  * DGError.cc:805-826), FP64 reduction */
 int dgp_l2_error(dgp_solver s, double t, int field, double* err);
+/* Error norms against the exact field at time t, the family of DGError.cc
+ * (DGCell::L1exact :549, LinfError :567, L1exactPressure :601,
+ * entropyErrorL1_2D/3D :621-665, pressureErrorL2 :774, densityErrorL2 :805,
+ * entropyErrorL2_2D :687; gamma 1.4 as there).  quantity >= 0: that field; -1:
+ * pressure, -2: entropy deviation (p / p_ex) / (rho / rho_ex)^gamma - 1 (Euler
+ * laws).  rule 0: the volume rule of degree 2p (as the L1 / Linf functions),
+ * 1: degree 2(p+1) (as the L2 functions).  norms[3] = L1, L2, Linf. */
+int dgp_error_norms(dgp_solver s, double t, int quantity, int rule, double* norms);
+
+/* Point probes (DGPointSensor / DGLineSensor, DGSensor.cc:88-186; a line
+ * sensor is a probe over points sampled along the segment).  The points (dim
+ * doubles each) are located once on the host (a point takes the lowest-index
+ * cell, in file order, that contains it, as DGCell::inCell tests it;
+ * found[i] = 0 for points outside the mesh, whose values read NaN).
+ * dgp_probe_eval: every field at every point of the current state, [n][M].
+ * dgp_probe_record: during dgp_run, sample the state after every `every`-th
+ * step into a device buffer of max_samples samples, inside the run's step
+ * graph (no host round trip per sample); every = 0 stops recording.
+ * dgp_probe_samples: the samples of the last run, times [k] and values
+ * [k][n][M].  Destroy probes before their solver (a probe whose solver was
+ * destroyed returns DGP_ERR_INVALID). */
+int dgp_probe_create(dgp_solver s, int n, const double* points, dgp_probe* out, int* found);
+int dgp_probe_destroy(dgp_probe p);
+int dgp_probe_info(dgp_probe p, int* n, int* found);
+int dgp_probe_eval(dgp_probe p, double* values);
+int dgp_probe_record(dgp_probe p, int every, int max_samples);
+int dgp_probe_samples(dgp_probe p, int* nsamples, double* times, double* values);
+
+/* Checkpoints in the data format of DGAnalysis::write / read (DGPref.cc:712-766):
+ * TACT, ITER, "dim cells faces", per cell its entity (type, geometric order,
+ * vertex ids; mMesh::readMEntity, mMesh.cc:413-455) then the order and the
+ * coefficients [field][mode] (DGCell::write, DGCell.cc:1523-1531), then the
+ * face entities.  Written as readMEntity reads them (DGAnalysis::write leaves
+ * out the geometric order); both layouts are read, cells matched by their
+ * vertex ids.  Coefficients carry 17 significant digits (round trip exact). */
+int dgp_checkpoint_write(dgp_solver s, const char* path, double t, int iter);
+int dgp_checkpoint_read(dgp_solver s, const char* path, double* t, int* iter);
 /* sum over cells of the cell integral of every field (conserved totals), FP64 */
 int dgp_totals(dgp_solver s, double* totals);
 int dgp_synchronize(dgp_solver s);

@@ -1293,8 +1293,9 @@ double or_cfl_dt(const or_solver* s, double cfl) {
 /* d^n/dx^(n-a)dy^a of the cell's degree-n modal block (constant on the cell);*/
 /* component a is bounded in x by the differences of the degree-(n-1)         */
 /* derivative d^(n-1)/dx^(n-1-a)dy^a of the left/right neighbours and in y by */
-/* d^(n-1)/dx^(n-a)dy^(a-1) of the bottom/top neighbours, divided by the      */
-/* distance of the bounding-box centres (the degree-0 moment is the mean).    */
+/* d^(n-1)/dx^(n-a)dy^(a-1) of the bottom/top neighbours, times the reciprocal */
+/* (rounded once) of the distance of the bounding-box centres (the degree-0   */
+/* moment is the mean).                                                       */
 /* A limited degree is mapped back to its modal block exactly; the mean is    */
 /* never changed.  Trigger of a cell = lowest limited degree over its fields  */
 /* (0: untouched).  Products and sums are evaluated one rounding at a time,   */
@@ -1443,6 +1444,13 @@ static int limit_cell(const or_solver* s, const double* C, int e, double* out) {
   const double* Ji = s->jinv + 9 * e;
   const double* J = s->jac + 9 * e;
   int trig = 0;
+  /* reciprocals of the signed centre distances: left/bottom own - theirs,
+   * right/top theirs - own, each rounded once */
+  double rc[4] = {0.0, 0.0, 0.0, 0.0};
+  if (nb[0] >= 0) rc[0] = 1.0 / (px - s->bbc[2 * nb[0]]);
+  if (nb[1] >= 0) rc[1] = 1.0 / (s->bbc[2 * nb[1]] - px);
+  if (nb[2] >= 0) rc[2] = 1.0 / (py - s->bbc[2 * nb[2] + 1]);
+  if (nb[3] >= 0) rc[3] = 1.0 / (s->bbc[2 * nb[3] + 1] - py);
   for (int j = 0; j < m; ++j) {
     const double* row = C + ((size_t)e * m + j) * Np;
     double* orow = out + (size_t)j * Np;
@@ -1466,16 +1474,16 @@ static int limit_cell(const or_solver* s, const double* C, int e, double* out) {
         int l1 = 0, l2 = 0;
         if (hasx) {
           double fwd = 0.0, bwd = 0.0;
-          if (nb[1] >= 0) fwd = (hx[1][a] - he[a]) / (s->bbc[2 * nb[1]] - px);
-          if (nb[0] >= 0) bwd = (he[a] - hx[0][a]) / (px - s->bbc[2 * nb[0]]);
+          if (nb[1] >= 0) fwd = (hx[1][a] - he[a]) * rc[1];
+          if (nb[0] >= 0) bwd = (he[a] - hx[0][a]) * rc[0];
           if (nb[0] >= 0 && nb[1] >= 0) t1 = lim_minmod3(g[a], fwd, bwd, &l1);
           else if (nb[0] >= 0) t1 = lim_minmod2(g[a], bwd, &l1);
           else t1 = lim_minmod2(g[a], fwd, &l1);
         }
         if (hasy) {
           double fwd = 0.0, bwd = 0.0;
-          if (nb[3] >= 0) fwd = (hx[3][a - 1] - he[a - 1]) / (s->bbc[2 * nb[3] + 1] - py);
-          if (nb[2] >= 0) bwd = (he[a - 1] - hx[2][a - 1]) / (py - s->bbc[2 * nb[2] + 1]);
+          if (nb[3] >= 0) fwd = (hx[3][a - 1] - he[a - 1]) * rc[3];
+          if (nb[2] >= 0) bwd = (he[a - 1] - hx[2][a - 1]) * rc[2];
           if (nb[2] >= 0 && nb[3] >= 0) t2 = lim_minmod3(g[a], fwd, bwd, &l2);
           else if (nb[2] >= 0) t2 = lim_minmod2(g[a], bwd, &l2);
           else t2 = lim_minmod2(g[a], fwd, &l2);
@@ -1509,8 +1517,93 @@ static int limit_cell(const or_solver* s, const double* C, int e, double* out) {
   return trig;
 }
 
+/* Barth limiter (DGBarthLimiter::limit, DGLimiter.cc:184-287) on every cell,
+ * in place (the reference's TimeIntegrator::limit would copy the second
+ * coefficient slot, which Barth never writes, back over it).  Per cell and
+ * field: bounds = max/min of the interior-face neighbours' means (the cell's
+ * own mean excluded; no interior neighbour: the cell is left alone, where the
+ * reference reads uninitialised bounds); at every point of every face of the
+ * cell, the cell's coefficients against the face's LEFT-cell basis values
+ * (pg->fctleft, whichever side the cell is on), phi = (bound - mean) /
+ * (val - mean) outside the bounds, 1 inside, clamped at 0; slope = min phi;
+ * modes of degree >= 2 zeroed when slope < 0.9, degree-1 modes times slope.
+ * The means never change, so the cell order does not matter.  trig: 1 where
+ * a slope is below 1. */
+static int barth_apply(or_solver* s, unsigned char* trig) {
+  const int m = s->m, Np = s->Np, E = s->E, nqf = s->nqf;
+  const int s1 = s->dim == 2 ? 3 : 4; /* modes of degree <= 1 */
+  double* mx = (double*)malloc(sizeof(double) * (size_t)E * m);
+  double* mn = (double*)malloc(sizeof(double) * (size_t)E * m);
+  double* slope = (double*)malloc(sizeof(double) * (size_t)E * m);
+  int* kk = (int*)calloc((size_t)E, sizeof(int));
+  for (int f = 0; f < s->F; ++f) {
+    if (s->eR[f] < 0) continue;
+    for (int side = 0; side < 2; ++side) {
+      const int c = side ? s->eR[f] : s->eL[f], o = side ? s->eL[f] : s->eR[f];
+      for (int j = 0; j < m; ++j) {
+        const double mo = s->C[((size_t)o * m + j) * Np] * s->phi0;
+        double* X = mx + (size_t)c * m + j;
+        double* N = mn + (size_t)c * m + j;
+        if (kk[c] == 0) {
+          *X = mo;
+          *N = mo;
+        } else {
+          *X = mo > *X ? mo : *X;
+          *N = mo < *N ? mo : *N;
+        }
+      }
+      kk[c]++;
+    }
+  }
+  for (size_t i = 0; i < (size_t)E * m; ++i) slope[i] = 1.0;
+  for (int f = 0; f < s->F; ++f)
+    for (int side = 0; side < 2; ++side) {
+      const int c = side ? s->eR[f] : s->eL[f];
+      if (c < 0 || kk[c] == 0) continue;
+      const double* a = s->C + (size_t)c * m * Np;
+      for (int q = 0; q < nqf; ++q) {
+        double val[MAXM];
+        interp(s->trL + ((size_t)f * nqf + q) * Np, a, m, Np, val);
+        for (int j = 0; j < m; ++j) {
+          const double mean = a[j * Np] * s->phi0;
+          const double X = mx[(size_t)c * m + j], N = mn[(size_t)c * m + j];
+          double phin = 1.0;
+          if (val[j] > X) phin = (X - mean) / (val[j] - mean);
+          else if (val[j] < N) phin = (N - mean) / (val[j] - mean);
+          if (phin < 0.0) phin = 0.0;
+          double* sl = slope + (size_t)c * m + j;
+          *sl = *sl < phin ? *sl : phin;
+        }
+      }
+    }
+  int count = 0;
+  for (int e = 0; e < E; ++e) {
+    int t = 0;
+    if (kk[e] > 0)
+      for (int j = 0; j < m; ++j) {
+        const double sl = slope[(size_t)e * m + j];
+        if (!(sl < 1.0)) continue;
+        double* a = s->C + ((size_t)e * m + j) * Np;
+        t = 1;
+        if (sl < 0.9)
+          for (int k = s1; k < Np; ++k) a[k] = 0.0;
+        for (int k = 1; k < s1 && k < Np; ++k) a[k] = a[k] * sl;
+      }
+    s->trig[e] = (unsigned char)t;
+    count += t;
+  }
+  if (trig) memcpy(trig, s->trig, (size_t)E);
+  free(mx);
+  free(mn);
+  free(slope);
+  free(kk);
+  return count;
+}
+
+/* on: 1 triangle moment limiter (triangles), 2 Barth limiter, 0 off */
 void or_set_limiter(or_solver* s, int on) {
-  s->limiter = (on && s->dim == 2 && s->order > 0) ? 1 : 0;
+  if (on == 2) s->limiter = s->order > 0 ? 2 : 0;
+  else s->limiter = (on && s->dim == 2 && s->order > 0) ? 1 : 0;
 }
 
 void or_set_p0_fallback(or_solver* s, int on) { s->p0 = on ? 1 : 0; }
@@ -1518,6 +1611,7 @@ void or_set_p0_fallback(or_solver* s, int on) { s->p0 = on ? 1 : 0; }
 int or_limit(or_solver* s, unsigned char* trig) {
   const size_t dof = (size_t)s->m * s->Np;
   int count = 0;
+  if (s->limiter == 2) return barth_apply(s, trig);
   if (s->dim != 2 || s->order < 1) {
     if (trig) memset(trig, 0, (size_t)s->E);
     return 0;
@@ -1641,6 +1735,68 @@ double or_run(or_solver* s, double t0, double tend, double cfl, int nsteps, int*
 
 /* sqrt(sum_e sum_q (u_h - u_exact)^2 |J| w) with the rule of degree 2(p+1)
  * (DGCell::densityErrorL2, DGError.cc:805-826) */
+/* The error family of DGError.cc (DGCell::L1exact :549, LinfError :567,
+ * L1exactPressure :601, entropyErrorL1_2D/3D :621-665, pressureErrorL2 :774,
+ * densityErrorL2 :805, entropyErrorL2_2D :687) in one place.  quantity >= 0:
+ * field `quantity`; -1: pressure (gamma - 1)(E - |m|^2 / 2 rho) with E at
+ * index 3 (and the 3D w-momentum at index 4); -2: entropy deviation
+ * (p / p_ex) / (rho / rho_ex)^gamma - 1.  gamma = 1.4 as those functions fix it.
+ * rule 0: the cell's volume rule of degree 2p (the L1 / Linf functions);
+ * rule 1: the rule of degree 2(p+1) (the L2 functions).  out: L1 = sum |d| |J| w,
+ * L2 = sqrt(sum d^2 |J| w), Linf = max |d| over the rule's points. */
+static double err_quantity(const or_solver* s, int quantity, const double* v) {
+  const double gamma = 1.4;
+  if (quantity >= 0) return v[quantity];
+  double m2 = v[1] * v[1] + v[2] * v[2];
+  if (s->dim == 3) m2 += v[4] * v[4];
+  const double p = (gamma - 1.) * (v[3] - 0.5 * m2 / v[0]);
+  return p; /* the entropy deviation needs both states: see or_error_norms */
+}
+
+int or_error_norms(const or_solver* s, double t, int quantity, int rule, double* out) {
+  const double gamma = 1.4;
+  if (quantity >= s->m || quantity < -2) return -1;
+  if (quantity < 0 && !(s->law == OR_EULER2D || s->law == OR_EULER3D)) return -1;
+  const double refm = (s->dim == 2) ? 0.5 : 1.0 / 6.0;
+  const dgp_q_rule* r = rule ? simplex_rule(s->dim, 2 * (s->order + 1)) : NULL;
+  if (rule && !r) return -1;
+  const int npts = rule ? r->npts : s->nq;
+  double l1 = 0.0, l2 = 0.0, li = 0.0;
+  for (int e = 0; e < s->E; ++e) {
+    const double* c = s->C + (size_t)e * s->m * s->Np;
+    for (int q = 0; q < npts; ++q) {
+      double xi[3] = {0, 0, 0}, x[3], fct[MAXNP], val[MAXM], ex[MAXM], w;
+      if (rule) {
+        for (int k = 0; k < s->dim; ++k) xi[k] = r->data[q * (s->dim + 1) + k];
+        w = refm * r->data[q * (s->dim + 1) + s->dim];
+        basis_eval(s, xi, fct);
+      } else {
+        for (int k = 0; k < s->dim; ++k) xi[k] = s->qp[q][k];
+        w = s->qw[q];
+        for (int k = 0; k < s->Np; ++k) fct[k] = s->phi[q][k];
+      }
+      interp(fct, c, s->m, s->Np, val);
+      phys_point(s, e, xi, x);
+      or_field_eval(s, x, t, ex);
+      double d;
+      if (quantity == -2) {
+        const double p = err_quantity(s, -1, val), pe = err_quantity(s, -1, ex);
+        d = (p / pe) / pow(val[0] / ex[0], gamma) - 1.;
+      } else {
+        d = err_quantity(s, quantity, val) - err_quantity(s, quantity, ex);
+      }
+      const double jw = s->det[e] * w;
+      l1 += fabs(d) * jw;
+      l2 += d * d * jw;
+      if (fabs(d) > li) li = fabs(d);
+    }
+  }
+  out[0] = l1;
+  out[1] = sqrt(l2);
+  out[2] = li;
+  return 0;
+}
+
 double or_l2_error(const or_solver* s, double t, int fi) {
   const dgp_q_rule* r = simplex_rule(s->dim, 2 * (s->order + 1));
   if (!r) return -1.0;

@@ -49,12 +49,18 @@ double or_cfl_dt(const or_solver* s, double cfl);
 double or_step(or_solver* s, double t, double dt);      /* SSP-RK3, returns resid */
 double or_run(or_solver* s, double t0, double tend, double cfl, int nsteps, int* steps_done);
 double or_l2_error(const or_solver* s, double t, int field_index); /* vs exact field */
+/* L1, L2, Linf of a field (quantity >= 0), the pressure (-1) or the entropy
+ * deviation (-2) against the exact field; rule 0: volume rule of degree 2p,
+ * 1: degree 2(p+1) (definitions in dg_oracle.c); returns -1 if not defined */
+int or_error_norms(const or_solver* s, double t, int quantity, int rule, double* out);
 void or_field_eval(const or_solver* s, const double* x, double t, double* q);
 unsigned int or_glibc_rand_first(unsigned int seed);   /* srand(seed); rand() */
-/* triangle moment limiter (definition in dg_oracle.c): applied after every
+/* limiters (definitions in dg_oracle.c), on = 1: triangle moment limiter,
+ * on = 2: Barth limiter (triangles and tets), 0: off.  Applied after every
  * SSP-RK3 stage by or_step when enabled; or_limit applies it once to the
- * current state and writes the per-cell trigger degree (0: untouched, file
- * order) when trig is not NULL; returns the number of triggered cells. */
+ * current state and writes the per-cell trigger (moment: lowest limited
+ * degree, Barth: 1 where a slope factor is below 1; 0: untouched, file order)
+ * when trig is not NULL; returns the number of triggered cells. */
 void or_set_limiter(or_solver* s, int on);
 int or_limit(or_solver* s, unsigned char* trig);
 /* P0 fallback of DGCell::setToZero for cells with a non-physical face trace */

@@ -15,6 +15,13 @@
 //   --state FILE   coefficients of every cell ([field][mode], file order) of
 //                  the projected initial state and after every --every steps.
 //   --log FILE     per step: dt, time, residual returned by advanceInTime.
+//   --barth FILE   after the steps: DGBarthLimiter::limit on every cell of the
+//                  state (means computed first, each cell's faces as its
+//                  allSubs list as DGAnalysis.cc:244-253 builds it), then the
+//                  coefficients of every cell ([field][mode], file order) and
+//                  the cell's per-field slope factors (details->limSlope).  The
+//                  limiter writes the coefficients in place; TimeIntegrator::
+//                  limit's copy of the unwritten second slot is not applied.
 //   --bench N      time N steps (after --warmup W untimed ones) (CFL dt + RungeKuttaTVD3::advanceInTime)
 //                  with --threads workers of the reference pthreads path
 //                  (parallel.cc, chunked as main.cc) and print one "BENCH ..."
@@ -57,6 +64,7 @@
 #include "EulerLaw.h"
 #include "Burgers.h"
 #include "FieldEvaluator.h"
+#include "DGLimiter.h"
 #include "mPoint.h"
 
 // Globals that the reference's threading code declares extern (main.cc owns
@@ -70,7 +78,7 @@ double timeRK = 0;
 static const double kPi = 3.14159265358979323846;
 
 struct Params {
-  std::string mesh, caseName = "gauss", flux = "exact", conn, rhs, state, log;
+  std::string mesh, caseName = "gauss", flux = "exact", conn, rhs, state, log, barth;
   int order = 2, steps = 0, every = 1, threads = 1, bench = 0, warmup = 0;
   double cfl = 0.1, tend = -1.0;
   // scalar
@@ -240,7 +248,7 @@ static double nowSec() {
 static void usage() {
   fprintf(stderr, "usage: ref_driver --mesh F.msh [--case gauss|vortex|pulse3d|sine|gauss3d] "
                   "[--flux exact|roe] [--order p] [--steps n | --tend T] [--cfl c] "
-                  "[--conn F] [--rhs F] [--state F --every k] [--log F] "
+                  "[--conn F] [--rhs F] [--state F --every k] [--log F] [--barth F] "
                   "[--threads k --bench n]\n");
   exit(1);
 }
@@ -265,6 +273,7 @@ int main(int argc, char** argv) {
     else if (a == "--rhs") P.rhs = v;
     else if (a == "--state") P.state = v;
     else if (a == "--log") P.log = v;
+    else if (a == "--barth") P.barth = v;
     else if (a == "--ax") P.ax = atof(v);
     else if (a == "--ay") P.ay = atof(v);
     else if (a == "--az") P.az = atof(v);
@@ -443,6 +452,27 @@ int main(int argc, char** argv) {
     if (fs && (step % P.every == 0)) Dump::state(fs, step, TACT, byFile, m, Np);
   }
   double elapsed = nowSec() - t0;
+  if (!P.barth.empty()) {
+    for (mMesh::iter it = mesh->begin(dim); it != mesh->end(dim); ++it) {
+      DGCell* cell = (DGCell*)(*it)->getCell();
+      cell->computeMean();
+      cell->details->allSubs.clear();
+      for (int k = 0; k < cell->theMeshEntity->size(dim - 1); ++k)
+        cell->details->allSubs.push_back(cell->theMeshEntity->get(dim - 1, k));
+    }
+    DGBarthLimiter barth;
+    for (mMesh::iter it = mesh->begin(dim); it != mesh->end(dim); ++it)
+      barth.limit((DGCell*)(*it)->getCell(), TACT);
+    FILE* f = fopen(P.barth.c_str(), "w");
+    fprintf(f, "%d %d %d\n", E, m, Np);
+    for (int e = 0; e < E; ++e) {
+      for (int i = 0; i < m; ++i)
+        for (int j = 0; j < Np; ++j) fprintf(f, "%.17g ", byFile[e]->theFieldsCoefficients->get(i, j));
+      for (int i = 0; i < m; ++i) fprintf(f, "%.17g ", byFile[e]->details->limSlope[i]);
+      fprintf(f, "\n");
+    }
+    fclose(f);
+  }
   if (fs) fclose(fs);
   if (fl) fclose(fl);
   if (P.bench > 0)

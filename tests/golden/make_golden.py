@@ -62,6 +62,39 @@ CASES = {
 }
 
 
+# Barth limiter fixtures: the reference's own DGBarthLimiter::limit applied to
+# every cell of the state after `steps` steps (ref_driver --barth); stored as
+# ``pre`` (the state handed to the limiter, [cell][field*mode]), ``post`` (the
+# limited coefficients) and ``slope`` (details->limSlope per cell and field).
+BARTH_CASES = {
+    "barth_scalar_tri_p1": ("tri", SQUARE, ["--case", "gauss", "--order", "1"], 2),
+    "barth_scalar_tri_p2": ("tri", SQUARE, ["--case", "gauss", "--order", "2"], 0),
+    "barth_scalar_tri12_p2": ("tri", dict(nx=12, ny=12, seed=1), ["--case", "gauss", "--order", "2",
+                                                                   "--s", "0.1"], 2),
+    "barth_euler_roe_p2": ("tri", VORTEX_BOX, ["--case", "vortex", "--flux", "roe", "--order", "2"], 2),
+    "barth_scalar_tet_p2": ("tet", dict(n=2, seed=3), ["--case", "gauss3d", "--order", "2", "--ax", "1",
+                                                        "--ay", "0.5", "--az", "0.25", "--cx", "0.5",
+                                                        "--cy", "0.5", "--cz", "0.5", "--s", "0.05"], 0),
+}
+
+
+def run_barth_case(name, kind, margs, dargs, steps):
+    mesh = build_mesh(kind, margs)
+    msh = os.path.join(HERE, name + ".msh")
+    meshgen.write_msh_v1(mesh, msh)
+    with tempfile.TemporaryDirectory() as td:
+        state, barth = os.path.join(td, "s"), os.path.join(td, "b")
+        cmd = [DRIVER, "--mesh", msh, "--steps", str(steps), "--cfl", "0.1", "--state", state,
+               "--every", str(max(steps, 1)), "--barth", barth] + dargs
+        subprocess.run(cmd, check=True, capture_output=True)
+        blocks = open(state).read().split("step ")[1:]
+        pre = np.array([list(map(float, ln.split())) for ln in blocks[-1].split("\n")[1:] if ln.strip()])
+        E, m, Np = map(int, open(barth).readline().split())
+        b = np.loadtxt(barth, skiprows=1, ndmin=2)
+    np.savez_compressed(os.path.join(HERE, name + ".npz"), pre=pre, post=b[:, :m * Np],
+                        slope=b[:, m * Np:], args=np.array(dargs), steps=steps)
+
+
 def build_mesh(kind, args):
     return meshgen.tri_square(**args) if kind == "tri" else meshgen.tet_cube(**args)
 
@@ -95,6 +128,11 @@ def main():
         if only and name not in only:
             continue
         run_case(name, kind, margs, dargs, steps)
+        print("wrote", name)
+    for name, (kind, margs, dargs, steps) in BARTH_CASES.items():
+        if only and name not in only:
+            continue
+        run_barth_case(name, kind, margs, dargs, steps)
         print("wrote", name)
 
 

@@ -50,6 +50,8 @@ def lib():
     L.or_run.restype = D
     L.or_l2_error.argtypes = [P, D, I]
     L.or_l2_error.restype = D
+    L.or_error_norms.argtypes = [P, D, I, I, ctypes.POINTER(ctypes.c_double)]
+    L.or_error_norms.restype = I
     pU8 = ctypes.POINTER(ctypes.c_uint8)
     L.or_set_limiter.argtypes = [P, I]
     L.or_limit.argtypes = [P, pU8]
@@ -114,8 +116,15 @@ class Oracle:
     def l2_error(self, t, field=0):
         return lib().or_l2_error(self.h, t, field)
 
+    def error_norms(self, t, quantity=0, rule=1):
+        out = np.zeros(3)
+        rc = lib().or_error_norms(self.h, t, quantity, rule, out.ctypes.data_as(ctypes.POINTER(ctypes.c_double)))
+        assert rc == 0
+        return out
+
     def set_limiter(self, on=True):
-        lib().or_set_limiter(self.h, 1 if on else 0)
+        """on: True / 1 triangle moment limiter, 2 Barth limiter, False / 0 off."""
+        lib().or_set_limiter(self.h, int(on) if not isinstance(on, bool) else (1 if on else 0))
 
     def set_p0_fallback(self, on=True):
         lib().or_set_p0_fallback(self.h, 1 if on else 0)
