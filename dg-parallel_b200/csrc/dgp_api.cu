@@ -537,11 +537,13 @@ extern "C" {
 const char* dgp_last_error(void) { return g_err.c_str(); }
 int dgp_version(void) { return 1; }
 
-int dgp_mesh_from_msh(const char* path, dgp_mesh* out) {
+int dgp_mesh_from_msh(const char* path, dgp_mesh* out) { return dgp_mesh_from_msh_ex(path, 0, out); }
+
+int dgp_mesh_from_msh_ex(const char* path, int gpu_faces, dgp_mesh* out) {
   if (!path || !out) return fail(DGP_ERR_INVALID, "null argument");
   auto* h = new dgp_mesh_s;
   std::string err;
-  int rc = read_msh_v1(path, h->m, err);
+  int rc = read_msh_v1(path, h->m, err, gpu_faces != 0);
   if (rc != DGP_OK) {
     delete h;
     return fail(rc, err);
@@ -553,11 +555,18 @@ int dgp_mesh_from_msh(const char* path, dgp_mesh* out) {
 int dgp_mesh_from_arrays(int dim, int nv, const double* xyz, const int* vertex_ids, int ncells,
                          const int* cells, int cell_tag, int nbfaces, const int* bfaces,
                          const int* btags, dgp_mesh* out) {
+  return dgp_mesh_from_arrays_ex(dim, nv, xyz, vertex_ids, ncells, cells, cell_tag, nbfaces, bfaces, btags, 0,
+                                 out);
+}
+
+int dgp_mesh_from_arrays_ex(int dim, int nv, const double* xyz, const int* vertex_ids, int ncells,
+                            const int* cells, int cell_tag, int nbfaces, const int* bfaces, const int* btags,
+                            int gpu_faces, dgp_mesh* out) {
   if (!out) return fail(DGP_ERR_INVALID, "null output handle");
   auto* h = new dgp_mesh_s;
   std::string err;
   int rc = mesh_from_arrays(dim, nv, xyz, vertex_ids, ncells, cells, cell_tag, nbfaces, bfaces, btags,
-                            h->m, err);
+                            h->m, err, gpu_faces != 0);
   if (rc != DGP_OK) {
     delete h;
     return fail(rc, err);

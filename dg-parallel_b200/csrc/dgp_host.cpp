@@ -87,6 +87,47 @@ int local_vertex(const HostMesh& m, int lf, int k) {
   return m.dim == 2 ? kTriFace[lf][k] : kTetFace[lf][k];
 }
 
+// classification of every face: a boundary face takes the tag of the boundary
+// element with its vertices, any other face the cells' tag
+void boundary_ids(HostMesh& m, const std::vector<FaceKey>& sorted_bkeys) {
+  m.bid.assign(m.F, m.ctag);
+  for (int f = 0; f < m.F; ++f) {
+    if (m.eR[f] >= 0) continue;
+    FaceKey k{{INT32_MAX, INT32_MAX, INT32_MAX}, 0, 0};
+    for (int j = 0; j < m.nfv; ++j) k.v[j] = m.vid[m.fv[static_cast<size_t>(f) * m.nfv + j]];
+    sort_small(k.v, m.nfv);
+    auto it = std::lower_bound(sorted_bkeys.begin(), sorted_bkeys.end(), k);
+    if (it != sorted_bkeys.end() && it->same(k)) m.bid[f] = it->cell;
+  }
+}
+
+void periodic_pairs(HostMesh& m) {
+  // periodic pairs (mMesh::setPeriodicBC, mMesh.cc:457-524): a boundary edge
+  // tagged 510 pairs with the first other 510 edge whose two vertices have the
+  // same y coordinates (within 1e-10, either order), 610 likewise with x
+  m.pface.assign(m.F, -1);
+  if (m.dim == 2) {
+    const double SN = 1.0e-10;
+    for (int f = 0; f < m.F; ++f) {
+      const int id = m.bid[f];
+      if (m.eR[f] >= 0 || (id != 510 && id != 610)) continue;
+      const int c = (id == 510) ? 1 : 0;
+      const double* v1 = &m.X[3 * m.fv[2 * f]];
+      const double* v2 = &m.X[3 * m.fv[2 * f + 1]];
+      for (int g = 0; g < m.F; ++g) {
+        if (g == f || m.eR[g] >= 0 || m.bid[g] != id) continue;
+        const double* a1 = &m.X[3 * m.fv[2 * g]];
+        const double* a2 = &m.X[3 * m.fv[2 * g + 1]];
+        if ((std::fabs(v1[c] - a1[c]) < SN && std::fabs(v2[c] - a2[c]) < SN) ||
+            (std::fabs(v1[c] - a2[c]) < SN && std::fabs(v2[c] - a1[c]) < SN)) {
+          m.pface[f] = g;
+          break;
+        }
+      }
+    }
+  }
+}
+
 int build_faces(HostMesh& m, const std::vector<FaceKey>& bkeys_in, std::string& err) {
   std::vector<FaceKey> bkeys = bkeys_in;
   std::sort(bkeys.begin(), bkeys.end());
@@ -112,7 +153,7 @@ int build_faces(HostMesh& m, const std::vector<FaceKey>& bkeys_in, std::string& 
       err = "non-manifold face shared by more than two cells";
       return DGP_ERR_IO;
     }
-    int a = keys[i].cell, la = keys[i].lf, b = -1, lb = -1, bid = m.ctag;
+    int a = keys[i].cell, la = keys[i].lf, b = -1, lb = -1;
     if (j - i == 2) {
       b = keys[i + 1].cell;
       lb = keys[i + 1].lf;
@@ -120,9 +161,6 @@ int build_faces(HostMesh& m, const std::vector<FaceKey>& bkeys_in, std::string& 
         std::swap(a, b);
         std::swap(la, lb);
       }
-    } else {
-      auto it = std::lower_bound(bkeys.begin(), bkeys.end(), keys[i]);
-      if (it != bkeys.end() && it->same(keys[i])) bid = it->cell;
     }
     int frame[3];
     for (int k = 0; k < m.nfv; ++k) frame[k] = m.cv[a * m.nvc + local_vertex(m, la, k)];
@@ -151,7 +189,6 @@ int build_faces(HostMesh& m, const std::vector<FaceKey>& bkeys_in, std::string& 
     m.eR.push_back(b);
     m.lfL.push_back(la);
     m.lfR.push_back(lb);
-    m.bid.push_back(bid);
     m.rperm.push_back(perm);
     m.F++;
     i = j;
@@ -194,30 +231,8 @@ int build_faces(HostMesh& m, const std::vector<FaceKey>& bkeys_in, std::string& 
     for (int k = 0; k < 3; ++k) m.fn[3 * f + k] = n[k];
     m.fmeas[f] = meas;
   }
-  // periodic pairs (mMesh::setPeriodicBC, mMesh.cc:457-524): a boundary edge
-  // tagged 510 pairs with the first other 510 edge whose two vertices have the
-  // same y coordinates (within 1e-10, either order), 610 likewise with x
-  m.pface.assign(m.F, -1);
-  if (m.dim == 2) {
-    const double SN = 1.0e-10;
-    for (int f = 0; f < m.F; ++f) {
-      const int id = m.bid[f];
-      if (m.eR[f] >= 0 || (id != 510 && id != 610)) continue;
-      const int c = (id == 510) ? 1 : 0;
-      const double* v1 = &m.X[3 * m.fv[2 * f]];
-      const double* v2 = &m.X[3 * m.fv[2 * f + 1]];
-      for (int g = 0; g < m.F; ++g) {
-        if (g == f || m.eR[g] >= 0 || m.bid[g] != id) continue;
-        const double* a1 = &m.X[3 * m.fv[2 * g]];
-        const double* a2 = &m.X[3 * m.fv[2 * g + 1]];
-        if ((std::fabs(v1[c] - a1[c]) < SN && std::fabs(v2[c] - a2[c]) < SN) ||
-            (std::fabs(v1[c] - a2[c]) < SN && std::fabs(v2[c] - a1[c]) < SN)) {
-          m.pface[f] = g;
-          break;
-        }
-      }
-    }
-  }
+  boundary_ids(m, bkeys);
+  periodic_pairs(m);
   return DGP_OK;
 }
 
@@ -253,7 +268,7 @@ struct Scanner {
 
 }  // namespace
 
-int read_msh_v1(const std::string& path, HostMesh& m, std::string& err) {
+int read_msh_v1(const std::string& path, HostMesh& m, std::string& err, bool gpu_faces) {
   std::ifstream in(path, std::ios::binary);
   if (!in) {
     err = "cannot open mesh file " + path;
@@ -348,12 +363,12 @@ int read_msh_v1(const std::string& path, HostMesh& m, std::string& err) {
   const int dim = is3d ? 3 : 2;
   return mesh_from_arrays(dim, static_cast<int>(ids.size()), X.data(), ids.data(),
                           static_cast<int>(ctags.size()), cells.data(), ctags.empty() ? 0 : ctags.back(),
-                          static_cast<int>(bt.size()), bf.data(), bt.data(), m, err);
+                          static_cast<int>(bt.size()), bf.data(), bt.data(), m, err, gpu_faces);
 }
 
 int mesh_from_arrays(int dim, int nv, const double* xyz, const int* vids, int ncells,
                      const int* cells, int cell_tag, int nbf, const int* bfaces,
-                     const int* btags, HostMesh& m, std::string& err) {
+                     const int* btags, HostMesh& m, std::string& err, bool gpu_faces) {
   if ((dim != 2 && dim != 3) || nv <= 0 || ncells <= 0 || !xyz || !cells) {
     err = "invalid mesh arrays";
     return DGP_ERR_INVALID;
@@ -397,6 +412,17 @@ int mesh_from_arrays(int dim, int nv, const double* xyz, const int* vids, int nc
       err = "degenerate cell " + std::to_string(e);
       return DGP_ERR_INVALID;
     }
+  }
+  if (gpu_faces) {
+    const int rc = build_faces_gpu(m, err);
+    if (rc == DGP_OK) {
+      std::sort(bkeys.begin(), bkeys.end());
+      boundary_ids(m, bkeys);
+      periodic_pairs(m);
+      return DGP_OK;
+    }
+    if (rc != DGP_ERR_UNSUPPORTED) return rc;
+    err.clear();
   }
   return build_faces(m, bkeys, err);
 }

@@ -32,11 +32,17 @@ struct HostMesh {
 };
 
 // Reads a Gmsh v1 file; returns 0 or a DGP_ERR_* code with `err` set.
-int read_msh_v1(const std::string& path, HostMesh& m, std::string& err);
+// gpu_faces: match the faces on the current CUDA device (build_faces_gpu).
+int read_msh_v1(const std::string& path, HostMesh& m, std::string& err, bool gpu_faces = false);
 // Builds from arrays (0-based indices); vertex ids default to 1..nv.
 int mesh_from_arrays(int dim, int nv, const double* xyz, const int* vids, int ncells,
                      const int* cells, int cell_tag, int nbf, const int* bfaces,
-                     const int* btags, HostMesh& m, std::string& err);
+                     const int* btags, HostMesh& m, std::string& err, bool gpu_faces = false);
+// Face matching on the GPU (dgp_meshprep.cu): fills F, fv, eL, eR, lfL, lfR,
+// rperm, fn, fmeas exactly as the host matching does (classification ids and
+// periodic pairs are added on the host).  DGP_ERR_UNSUPPORTED when the vertex
+// count does not fit the packed face keys (the caller then matches on the host).
+int build_faces_gpu(HostMesh& m, std::string& err);
 
 // glibc srand(seed); rand(): the TYPE_3 additive generator of the C library,
 // which DG-Parallel sums over vertex ids to order its entities

@@ -51,6 +51,8 @@ def lib() -> ctypes.CDLL:
         "dgp_version": ([], I),
         "dgp_mesh_from_msh": ([ctypes.c_char_p, pP], I),
         "dgp_mesh_from_arrays": ([I, I, pD, pI, I, pI, I, I, pI, pI, pP], I),
+        "dgp_mesh_from_msh_ex": ([ctypes.c_char_p, I, pP], I),
+        "dgp_mesh_from_arrays_ex": ([I, I, pD, pI, I, pI, I, I, pI, pI, I, pP], I),
         "dgp_mesh_info": ([P, pI, pI, pI, pI], I),
         "dgp_mesh_connectivity": ([P, pI], I),
         "dgp_mesh_face_geometry": ([P, pD], I),
@@ -151,14 +153,15 @@ class Mesh:
         self.dim, self.ncells, self.nfaces, self.nvertices = dim.value, e.value, f.value, v.value
 
     @classmethod
-    def from_msh(cls, path: str) -> "Mesh":
+    def from_msh(cls, path: str, gpu_faces: bool = False) -> "Mesh":
+        """gpu_faces: match the faces on the current CUDA device."""
         h = ctypes.c_void_p()
-        check(lib().dgp_mesh_from_msh(path.encode(), ctypes.byref(h)))
+        check(lib().dgp_mesh_from_msh_ex(path.encode(), 1 if gpu_faces else 0, ctypes.byref(h)))
         return cls(h)
 
     @classmethod
     def from_arrays(cls, dim, xyz, cells, cell_tag=100, bfaces=None, btags=None,
-                    vertex_ids=None) -> "Mesh":
+                    vertex_ids=None, gpu_faces: bool = False) -> "Mesh":
         xyz = np.ascontiguousarray(xyz, dtype=np.float64)
         cells = np.ascontiguousarray(cells, dtype=np.int32)
         nb = 0 if bfaces is None else len(bfaces)
@@ -166,9 +169,9 @@ class Mesh:
         bt = np.ascontiguousarray(btags if nb else np.zeros(1), dtype=np.int32)
         vids = None if vertex_ids is None else np.ascontiguousarray(vertex_ids, dtype=np.int32)
         h = ctypes.c_void_p()
-        check(lib().dgp_mesh_from_arrays(dim, xyz.shape[0], _dp(xyz), _ip(vids) if vids is not None else None,
-                                         cells.shape[0], _ip(cells), cell_tag, nb, _ip(bf), _ip(bt),
-                                         ctypes.byref(h)))
+        check(lib().dgp_mesh_from_arrays_ex(dim, xyz.shape[0], _dp(xyz), _ip(vids) if vids is not None else None,
+                                            cells.shape[0], _ip(cells), cell_tag, nb, _ip(bf), _ip(bt),
+                                            1 if gpu_faces else 0, ctypes.byref(h)))
         return cls(h)
 
     def connectivity(self) -> np.ndarray:

@@ -81,6 +81,15 @@ int dgp_mesh_from_msh(const char* path, dgp_mesh* out);
 int dgp_mesh_from_arrays(int dim, int nv, const double* xyz, const int* vertex_ids, int ncells,
                          const int* cells, int cell_tag, int nbfaces, const int* bfaces,
                          const int* btags, dgp_mesh* out);
+/* The same with the face matching on the current CUDA device when gpu_faces
+ * is nonzero (sort of packed face keys, left/right by the reference's entity
+ * order, frames, orientations, normals; the faces, normals and measures equal
+ * the host matching's, in another order); meshes whose vertex count does not
+ * fit the packed keys (tets: 2^21 vertices), or no device, match on the host. */
+int dgp_mesh_from_msh_ex(const char* path, int gpu_faces, dgp_mesh* out);
+int dgp_mesh_from_arrays_ex(int dim, int nv, const double* xyz, const int* vertex_ids, int ncells,
+                            const int* cells, int cell_tag, int nbfaces, const int* bfaces, const int* btags,
+                            int gpu_faces, dgp_mesh* out);
 int dgp_mesh_info(dgp_mesh m, int* dim, int* ncells, int* nfaces, int* nvertices);
 /* per face: dim sorted vertex ids, left cell, right cell (-1: boundary),
  * local face on each side (-1), classification id; (dim + 5) ints per face.

@@ -22,6 +22,13 @@
 //                  the cell's per-field slope factors (details->limSlope).  The
 //                  limiter writes the coefficients in place; TimeIntegrator::
 //                  limit's copy of the unwritten second slot is not applied.
+//   --ckpt-out F   after the steps: the data stream of DGAnalysis::write
+//                  (DGPref.cc:712-739) -- TACT, ITER, sizes, every cell's
+//                  writeMEntity + DGCell::write, every face's writeMEntity.
+//   --ckpt-in F    before the steps: the coefficients of every cell read the
+//                  way DGAnalysis::read does (DGPref.cc:741-766:
+//                  mMesh::readMEntity, the order, DGCell::read) in place of the
+//                  projection.
 //   --bench N      time N steps (after --warmup W untimed ones) (CFL dt + RungeKuttaTVD3::advanceInTime)
 //                  with --threads workers of the reference pthreads path
 //                  (parallel.cc, chunked as main.cc) and print one "BENCH ..."
@@ -47,6 +54,7 @@
 #include <string>
 #include <vector>
 #include <algorithm>
+#include <fstream>
 #include <unistd.h>
 
 #include "mImportExport.h"
@@ -78,7 +86,7 @@ double timeRK = 0;
 static const double kPi = 3.14159265358979323846;
 
 struct Params {
-  std::string mesh, caseName = "gauss", flux = "exact", conn, rhs, state, log, barth;
+  std::string mesh, caseName = "gauss", flux = "exact", conn, rhs, state, log, barth, ckptOut, ckptIn;
   int order = 2, steps = 0, every = 1, threads = 1, bench = 0, warmup = 0;
   double cfl = 0.1, tend = -1.0;
   // scalar
@@ -248,7 +256,7 @@ static double nowSec() {
 static void usage() {
   fprintf(stderr, "usage: ref_driver --mesh F.msh [--case gauss|vortex|pulse3d|sine|gauss3d] "
                   "[--flux exact|roe] [--order p] [--steps n | --tend T] [--cfl c] "
-                  "[--conn F] [--rhs F] [--state F --every k] [--log F] [--barth F] "
+                  "[--conn F] [--rhs F] [--state F --every k] [--log F] [--barth F] [--ckpt-in F] [--ckpt-out F] "
                   "[--threads k --bench n]\n");
   exit(1);
 }
@@ -274,6 +282,8 @@ int main(int argc, char** argv) {
     else if (a == "--state") P.state = v;
     else if (a == "--log") P.log = v;
     else if (a == "--barth") P.barth = v;
+    else if (a == "--ckpt-out") P.ckptOut = v;
+    else if (a == "--ckpt-in") P.ckptIn = v;
     else if (a == "--ax") P.ax = atof(v);
     else if (a == "--ay") P.ay = atof(v);
     else if (a == "--az") P.az = atof(v);
@@ -401,6 +411,20 @@ int main(int argc, char** argv) {
 
   RungeKuttaTVD3 rk(mesh, 0, m, DOF);
 
+  double TACT = 0.0;
+  if (!P.ckptIn.empty()) {
+    std::ifstream is(P.ckptIn.c_str());
+    int iter = 0, nd = 0, nvol = 0, nbnd = 0, order = 0;
+    is >> TACT >> iter >> nd >> nvol >> nbnd;
+    for (int i = 0; i < nvol; ++i) {
+      mEntity* ent = mesh->readMEntity(is);
+      is >> order;
+      DGCell* cell = (DGCell*)ent->getCell();
+      cell->read(is);
+      cell->computeMean();
+    }
+  }
+
   if (!P.rhs.empty()) {
     rk.assembleVolume(0.0);
     rk.assembleBoundary(0.0);
@@ -430,7 +454,6 @@ int main(int argc, char** argv) {
   if (fs) Dump::state(fs, 0, 0.0, byFile, m, Np);
 
   const int nsteps = P.bench > 0 ? P.bench + P.warmup : P.steps;
-  double TACT = 0.0;
   double t0 = nowSec();
   for (int step = 1; nsteps <= 0 || step <= nsteps; ++step) {
     if (P.bench > 0 && step == P.warmup + 1) t0 = nowSec();
@@ -452,6 +475,18 @@ int main(int argc, char** argv) {
     if (fs && (step % P.every == 0)) Dump::state(fs, step, TACT, byFile, m, Np);
   }
   double elapsed = nowSec() - t0;
+  if (!P.ckptOut.empty()) {
+    std::ofstream data(P.ckptOut.c_str());
+    data.precision(16);
+    data << TACT << "\n";
+    data << (nsteps > 0 ? nsteps : 0) << "\n";
+    data << dim << " " << mesh->size(dim) << " " << mesh->size(dim - 1) << "\n";
+    for (mMesh::iter it = mesh->begin(dim); it != mesh->end(dim); ++it) {
+      mesh->writeMEntity(data, *it);
+      ((DGCell*)(*it)->getCell())->write(data);
+    }
+    for (mMesh::iter it = mesh->begin(dim - 1); it != mesh->end(dim - 1); ++it) mesh->writeMEntity(data, *it);
+  }
   if (!P.barth.empty()) {
     for (mMesh::iter it = mesh->begin(dim); it != mesh->end(dim); ++it) {
       DGCell* cell = (DGCell*)(*it)->getCell();

@@ -95,6 +95,32 @@ def run_barth_case(name, kind, margs, dargs, steps):
                         slope=b[:, m * Np:], args=np.array(dargs), steps=steps)
 
 
+# Checkpoint fixture: the data stream of DGAnalysis::write after `steps` steps
+# (ref_driver --ckpt-out, the reference's own writeMEntity + DGCell::write at
+# 16 digits), stored as <name>.dat, with the same state at 17 digits in
+# <name>.npz (``state`` [cell][field*mode], ``t``, ``steps``).
+CKPT_CASES = {
+    "ckpt_euler_roe_p2": ("tri", VORTEX_BOX, ["--case", "vortex", "--flux", "roe", "--order", "2"], 2),
+}
+
+
+def run_ckpt_case(name, kind, margs, dargs, steps):
+    mesh = build_mesh(kind, margs)
+    msh = os.path.join(HERE, name + ".msh")
+    meshgen.write_msh_v1(mesh, msh)
+    dat = os.path.join(HERE, name + ".dat")
+    with tempfile.TemporaryDirectory() as td:
+        state, log = os.path.join(td, "s"), os.path.join(td, "l")
+        cmd = [DRIVER, "--mesh", msh, "--steps", str(steps), "--cfl", "0.1", "--state", state,
+               "--every", str(steps), "--log", log, "--ckpt-out", dat] + dargs
+        subprocess.run(cmd, check=True, capture_output=True)
+        blocks = open(state).read().split("step ")[1:]
+        st = np.array([list(map(float, ln.split())) for ln in blocks[-1].split("\n")[1:] if ln.strip()])
+        lg = np.loadtxt(log, ndmin=2)
+    np.savez_compressed(os.path.join(HERE, name + ".npz"), state=st, t=lg[-1, 2], steps=steps,
+                        args=np.array(dargs))
+
+
 def build_mesh(kind, args):
     return meshgen.tri_square(**args) if kind == "tri" else meshgen.tet_cube(**args)
 
@@ -128,6 +154,11 @@ def main():
         if only and name not in only:
             continue
         run_case(name, kind, margs, dargs, steps)
+        print("wrote", name)
+    for name, (kind, margs, dargs, steps) in CKPT_CASES.items():
+        if only and name not in only:
+            continue
+        run_ckpt_case(name, kind, margs, dargs, steps)
         print("wrote", name)
     for name, (kind, margs, dargs, steps) in BARTH_CASES.items():
         if only and name not in only:
