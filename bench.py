@@ -41,6 +41,56 @@ METRIC = "DOF-stage updates/s"
 REF_DRIVER = os.path.join(ROOT, "oracle", "_ref", "ref_driver")
 
 
+class Ranks:
+    """The N > 1 plumbing: one process per GPU (torchrun; NCCL) or CPU ranks
+    (gloo, for tests).  Without a process group every call is the identity."""
+
+    def __init__(self, backend: str = "nccl", timeout_s: int = 300):
+        self.world = int(os.environ.get("WORLD_SIZE", "1"))
+        self.rank = int(os.environ.get("RANK", "0"))
+        self.local = int(os.environ.get("LOCAL_RANK", "0"))
+        self.backend = backend
+        self.dist = None
+        if self.world > 1:
+            import torch.distributed as dist
+            from datetime import timedelta
+            dist.init_process_group(backend, timeout=timedelta(seconds=timeout_s))
+            self.dist = dist
+
+    def _reduce(self, x: float, op) -> float:
+        import torch
+        dev = "cuda" if self.backend == "nccl" else "cpu"
+        t = torch.tensor([x], device=dev, dtype=torch.float64)
+        self.dist.all_reduce(t, op=op)
+        return float(t.item())
+
+    def barrier(self):
+        if self.dist is not None:
+            self.dist.barrier()
+
+    def max(self, x: float) -> float:
+        return x if self.dist is None else self._reduce(x, self.dist.ReduceOp.MAX)
+
+    def sum(self, x: float) -> float:
+        return x if self.dist is None else self._reduce(x, self.dist.ReduceOp.SUM)
+
+    def close(self):
+        if self.dist is not None:
+            self.dist.destroy_process_group()
+            self.dist = None
+
+
+def shard(n: int, rank: int, world: int) -> list:
+    """Instances of a rank when n independent instances spread over world ranks
+    (round robin; every instance on exactly one rank)."""
+    return list(range(rank, n, world))
+
+
+def aggregate_rate(units_per_rank: float, seconds_max: float) -> float:
+    """Whole-job rate: the units all ranks processed over the slowest rank's time."""
+    return units_per_rank / seconds_max
+
+
 def load_peaks():
     try:
         with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as fh:
@@ -191,12 +241,14 @@ def main():
                     help="skip the untimed runs to t = 2 that state the density L2 errors")
     ap.add_argument("--ensemble", action="store_true",
                     help="only the batched-ensemble measurement (96 Burgers instances to t = 0.5, ~2 min)")
+    ap.add_argument("--ensemble-tend", type=float, default=0.5,
+                    help="--ensemble: end time of the instances (a short run for launch lists)")
     ap.add_argument("--adjoint", action="store_true",
                     help="only the discrete-adjoint measurement (Euler vortex 128x128x2 P2, 400 steps)")
     ap.add_argument("--configs", action="store_true",
                     help="only the other workloads: scalar P2 on 2048 triangles (200 steps) and "
                          "Maxwell P2 on 663552 tets (one TM110 period), both forms, ~2 min")
-    ap.add_argument("--profile-case", choices=["fp64", "mixed"], default=None,
+    ap.add_argument("--profile-case", choices=["fp64", "mixed", "maxwell"], default=None,
                     help="only set up the workload and run --warmup + --steps steps (for ncu)")
     ap.add_argument("--block", type=int, default=0, choices=[0, 64, 128, 256],
                     help="--profile-case: tile shape (threads) of the element and face kernels "
@@ -215,8 +267,12 @@ def main():
         return 0
     if args.ensemble:
         import torch
-        torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
-        print(json.dumps({"ensemble": ensemble_bench()}))
+        ranks = Ranks("nccl")
+        torch.cuda.set_device(ranks.local)
+        out = ensemble_bench(tend=args.ensemble_tend, ranks=ranks)
+        if ranks.rank == 0:
+            print(json.dumps({"ensemble": out}))
+        ranks.close()
         return 0
     if args.configs:
         import torch
@@ -228,15 +284,9 @@ def main():
     import torch
     import dgp
 
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
+    ranks = Ranks("nccl")
+    world, rank, local = ranks.world, ranks.rank, ranks.local
     torch.cuda.set_device(local)
-    dist = None
-    if world > 1:
-        import torch.distributed as dist
-        from datetime import timedelta
-        dist.init_process_group("nccl", timeout=timedelta(seconds=300))
 
     mesh_np = make_mesh()
     prm = vortex_params()
@@ -246,16 +296,11 @@ def main():
     units_per_step = E * 4 * 10 * 3
 
     def barrier():
-        if dist is not None:
-            dist.barrier()
+        ranks.barrier()
         torch.cuda.synchronize()
 
     def max_over_ranks(x):
-        if dist is None:
-            return x
-        t = torch.tensor([x], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+        return ranks.max(x)
 
     def timed_run(solver, steps, warmup, sampler=None):
         solver.project(0.0)
@@ -289,7 +334,7 @@ def main():
         err = s.l2_error(t_end, 0)
         kern = s.profile_kernels(20)
         launches = s.launches_per_step() * 8 * ((args.steps + 7) // 8) + 1  # graphs of 8 steps + first CFL
-        results[name] = {"seconds": sec, "value": units_per_step * args.steps * world / sec,
+        results[name] = {"seconds": sec, "value": aggregate_rate(units_per_step * args.steps * world, sec),
                          "gpu_launches": launches,
                          "t_end": t_end, "density_l2_vs_exact": err, "kernel_ms": kern.tolist(),
                          "solver": s}
@@ -366,6 +411,10 @@ def main():
                 cpu = {"value": r["value"], "unit": "DOF-stage/s", "cores": r["threads"], "kind": "reference",
                        "sample": "3 SSP-RK3 steps (after 1 warm-up) of the full 131072-cell workload, "
                                  "DG-Parallel pthreads path built from source, " + cpu_model()}
+                # the same path on one thread (1 step after 1 warm-up)
+                r1 = cpu_reference(mesh_np, 1, 1, 1)
+                if r1 is not None:
+                    cpu["value_1_thread"] = r1["value"]
         line = {
             "metric": METRIC, "value": fp64["value"], "unit": "DOF-stage/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_per_step,
@@ -402,12 +451,11 @@ def main():
         print(json.dumps(line))
     for r in results.values():
         r["solver"].close()
-    if dist is not None:
-        dist.destroy_process_group()
+    ranks.close()
     return 0
 
 
-def ensemble_bench(n=96, seed=6, tend=0.5):
+def ensemble_bench(n=96, seed=6, tend=0.5, ranks=None):
     """Batched ensemble: n independent Burgers2D instances (Lax-Friedrichs flux,
     far-field boundaries) on seeded jittered triangle meshes whose sizes are
     log-uniform in [2k, 128k] cells, orders uniform in P1-P4, initial state
@@ -415,21 +463,27 @@ def ensemble_bench(n=96, seed=6, tend=0.5):
     run to t = 0.5 (past shock formation) in the mixed form (FP32 right-hand
     side, FP64 state and conserved totals).  Tile shapes per group come from the
     autotuner.  The run is timed by the device clock from the common start to
-    each instance's last step."""
+    each instance's last step.  Under torchrun the instances spread over the
+    ranks round robin (no communication): the rate is the updates of all ranks
+    over the slowest rank's device time."""
     import numpy as np
     import dgp
     from dgp import meshgen
+    ranks = ranks or Ranks("nccl")
     rng = np.random.default_rng(seed)
     counts = np.exp(rng.uniform(np.log(2000.0), np.log(128000.0), n))
-    orders = rng.integers(1, 5, size=n)
+    orders_all = rng.integers(1, 5, size=n)
     amps = rng.uniform(0.5, 1.5, size=n)
+    mine = shard(n, ranks.rank, ranks.world)
+    orders = orders_all[mine]
     t_setup = time.time()
     meshes, laws = [], []
-    for i in range(n):
+    for i in mine:
         side = max(4, int(round(np.sqrt(counts[i] / 2.0))))
         m = meshgen.tri_square(side, side, 0.0, 1.0, 0.0, 1.0, jitter=0.15, seed=1000 + i)
         meshes.append(dgp.Mesh.from_arrays(2, m.vertices, m.cells, m.domain_tag, m.bfaces, m.btags))
         laws.append(dgp.Law(dgp.LAW_BURGERS2D, dgp.FLUX_LLF, dgp.FIELD_SINE, dgp.law_params(amplitude=amps[i])))
+    n_all, n = n, len(mine)
     setup_s = time.time() - t_setup
     t_tune = time.time()
     dgp.autotune_ensemble(meshes, laws, orders.tolist(), dgp.MIXED, dgp.LIMITER_MOMENT, iters=3)
@@ -445,6 +499,19 @@ def ensemble_bench(n=96, seed=6, tend=0.5):
     tot1 = np.array([ens.totals(i)[0] for i in range(n)])
     dofs = np.array([ens.shapes[i][0] * ens.shapes[i][1] * ens.shapes[i][2] for i in range(n)], dtype=np.float64)
     updates = float((dofs * 3 * steps).sum())
+    # whole-run algorithmic bytes by the per-element-stage formula (FP64 state
+    # coefficients, geometry, face data), every instance's cells x 3 stages x steps
+    stage_bytes = 0.0
+    for i in range(n):
+        stage_bytes += 3.0 * float(steps[i]) * stage_formula_bytes(meshes[i].ncells, meshes[i].nfaces,
+                                                                   ens.shapes[i][1], ens.shapes[i][2], 2)
+    peaks, peak_src = load_peaks()
+    # every rank's work over the slowest rank's device time
+    ranks.barrier()
+    total_ms = ranks.max(total_ms)
+    updates = ranks.sum(updates)
+    stage_bytes = ranks.sum(stage_bytes)
+    achieved = stage_bytes / (total_ms * 1e-3) / 1e9
     finite = all(np.isfinite(ens.get_state(i)).all() for i in range(n))
     groups = {}
     for g in sorted(set(ens.groups)):
@@ -453,8 +520,9 @@ def ensemble_bench(n=96, seed=6, tend=0.5):
         groups[f"P{int(orders[members[0]])}"] = {"instances": len(members), "block": b, "cells_per_tile": te,
                                                   "cells": int(sum(ens.shapes[i][0] for i in members))}
     out = {
-        "metric": "aggregate DOF-stage updates/s", "value": updates / (total_ms * 1e-3), "unit": "DOF-stage/s",
-        "instances": n, "cells_total": int(sum(ens.shapes[i][0] for i in range(n))),
+        "metric": "aggregate DOF-stage updates/s", "value": aggregate_rate(updates, total_ms * 1e-3),
+        "unit": "DOF-stage/s", "instances": n_all, "ranks": ranks.world, "instances_rank0": n,
+        "cells_total_rank0": int(sum(ens.shapes[i][0] for i in range(n))),
         "dofs_total": int(dofs.sum()), "steps_total": int(steps.sum()),
         "steps_min_max": [int(steps.min()), int(steps.max())],
         "device_ms_total": total_ms, "wall_s": wall_s,
@@ -462,6 +530,10 @@ def ensemble_bench(n=96, seed=6, tend=0.5):
         "all_reached_t_end": bool(np.allclose(t, tend, atol=1e-12)), "finite": bool(finite),
         "total_change_rel_max": float(np.max(np.abs(tot1 - tot0) / np.maximum(np.abs(tot0), 1e-300))),
         "groups": groups, "launches_per_step_all_groups": ens.launches_per_step(),
+        "roofline": {"bound": "hbm", "formula": "per-element-stage bytes (coefficients, geometry, faces) "
+                                                 "summed over every instance's stages, over the run's device time",
+                     "bytes": stage_bytes, "achieved": achieved, "peak": peaks.get("hbm_gbs"), "unit": "GB/s",
+                     "frac": achieved / peaks.get("hbm_gbs"), "peak_source": peak_src},
         "precision": "f32 RHS, f64 state, time and totals", "limiter": "triangle moment limiter",
         "flux": "Lax-Friedrichs, far-field boundaries", "setup_s": setup_s, "autotune_s": tune_s,
         "config": {"sizes": "log-uniform 2k-128k cells", "orders": "P1-P4 uniform", "A": "U[0.5,1.5]",
@@ -663,8 +735,20 @@ def adjoint_bench(n=128, order=2, nsteps=400, every=20, nrec=64, ndir=16, eps=1e
 
 
 def profile_case(args):
-    """The bench workload alone: setup, --warmup steps, then --steps steps."""
+    """The bench workload alone: setup, --warmup steps, then --steps steps
+    ("maxwell": the Maxwell P2 workload of --configs, FP64)."""
     import dgp
+    if args.profile_case == "maxwell":
+        from dgp import meshgen
+        m3 = meshgen.tet_cube(48, 0.0, 1.0, jitter=0.1, seed=3, boundary_tag=40000)
+        mesh3 = dgp.Mesh.from_arrays(3, m3.vertices, m3.cells, m3.domain_tag, m3.bfaces, m3.btags)
+        law3 = dgp.Law(dgp.LAW_MAXWELL3D, dgp.FLUX_UPWIND, dgp.FIELD_TM110, dgp.law_params(cavity=1.0))
+        s = dgp.Solver(mesh3, law3, 2, dgp.FP64)
+        t, _ = s.run(0.0, 0.0, 0.1, args.warmup)
+        t, n = s.run(t, 0.0, 0.1, args.steps)
+        s.synchronize()
+        print(f"profile case maxwell: {n} steps, t = {t:.6e}, block {s.block()[0]}")
+        return 0
     m = make_mesh()
     mesh = dgp.Mesh.from_arrays(2, m.vertices, m.cells, 100, m.bfaces, m.btags)
     law = dgp.Law(dgp.LAW_EULER2D, dgp.FLUX_ROE, dgp.FIELD_VORTEX, vortex_params())
