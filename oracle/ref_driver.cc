@@ -29,6 +29,9 @@
 //                  way DGAnalysis::read does (DGPref.cc:741-766:
 //                  mMesh::readMEntity, the order, DGCell::read) in place of the
 //                  projection.
+//   --gpu 1        (built as ref_driver_gpu only) step with GpuTimeIntegrator,
+//                  the shim of dg-parallel_b200/integration, on the reference's
+//                  own cells and CFL steps instead of RungeKuttaTVD3
 //   --bench N      time N steps (after --warmup W untimed ones) (CFL dt + RungeKuttaTVD3::advanceInTime)
 //                  with --threads workers of the reference pthreads path
 //                  (parallel.cc, chunked as main.cc) and print one "BENCH ..."
@@ -73,6 +76,9 @@
 #include "Burgers.h"
 #include "FieldEvaluator.h"
 #include "DGLimiter.h"
+#ifdef DGP_GPU_INTEGRATOR
+#include "GpuTimeIntegrator.h"
+#endif
 #include "mPoint.h"
 
 // Globals that the reference's threading code declares extern (main.cc owns
@@ -87,7 +93,7 @@ static const double kPi = 3.14159265358979323846;
 
 struct Params {
   std::string mesh, caseName = "gauss", flux = "exact", conn, rhs, state, log, barth, ckptOut, ckptIn;
-  int order = 2, steps = 0, every = 1, threads = 1, bench = 0, warmup = 0;
+  int order = 2, steps = 0, every = 1, threads = 1, bench = 0, warmup = 0, gpu = 0;
   double cfl = 0.1, tend = -1.0;
   // scalar
   double ax = 1.0, ay = 0.5, az = 0.0, cx = 0.3, cy = 0.3, cz = 0.3, s = 0.01;
@@ -284,6 +290,7 @@ int main(int argc, char** argv) {
     else if (a == "--barth") P.barth = v;
     else if (a == "--ckpt-out") P.ckptOut = v;
     else if (a == "--ckpt-in") P.ckptIn = v;
+    else if (a == "--gpu") P.gpu = atoi(v);
     else if (a == "--ax") P.ax = atof(v);
     else if (a == "--ay") P.ay = atof(v);
     else if (a == "--az") P.az = atof(v);
@@ -438,6 +445,34 @@ int main(int argc, char** argv) {
     for (int e = 0; e < E; ++e) byFile[e]->ZeroRHS();
   }
 
+#ifdef DGP_GPU_INTEGRATOR
+  GpuTimeIntegrator* gti = 0;
+  if (P.gpu) {
+    // the same case as the reference law, in the library's parameter layout
+    double prm[DGP_NPARAMS] = {0};
+    int kind = DGP_LAW_SCALAR, flux = DGP_FLUX_UPWIND, field = DGP_FIELD_GAUSS;
+    prm[0] = P.ax; prm[1] = P.ay; prm[2] = P.az;
+    prm[3] = P.cx; prm[4] = P.cy; prm[5] = P.cz;
+    prm[6] = P.s; prm[7] = P.gamma; prm[8] = P.beta; prm[9] = P.amp; prm[10] = 1.0;
+    if (P.caseName == "gauss3d") field = DGP_FIELD_GAUSS3D;
+    else if (P.caseName == "vortex") {
+      kind = DGP_LAW_EULER2D;
+      flux = P.flux == "roe" ? DGP_FLUX_ROE : DGP_FLUX_GODUNOV;
+      field = DGP_FIELD_VORTEX;
+      prm[0] = 1.0; prm[1] = 1.0; prm[2] = 0.0;
+      prm[3] = P.vx0; prm[4] = P.vy0; prm[5] = 0.0;
+    } else if (P.caseName == "pulse3d") {
+      kind = DGP_LAW_EULER3D;
+      flux = DGP_FLUX_GODUNOV;
+      field = DGP_FIELD_PULSE3D;
+    } else if (P.caseName == "sine") {
+      kind = DGP_LAW_BURGERS2D;
+      flux = DGP_FLUX_CENTRAL;
+      field = DGP_FIELD_SINE;
+    }
+    gti = new GpuTimeIntegrator(mesh, law, P.order, P.mesh.c_str(), byFile, kind, flux, field, prm);
+  }
+#endif
   FILE* fs = P.state.empty() ? 0 : fopen(P.state.c_str(), "w");
   FILE* fl = P.log.empty() ? 0 : fopen(P.log.c_str(), "w");
   if (fs) fprintf(fs, "%d %d %d\n", E, m, Np);
@@ -469,7 +504,11 @@ int main(int argc, char** argv) {
     }
     for (mMesh::iter it = mesh->begin(dim); it != mesh->end(dim); ++it)
       ((DGCell*)(*it)->getCell())->setTimeStep(dt);
+#ifdef DGP_GPU_INTEGRATOR
+    double resid = gti ? gti->advanceInTime(TACT, dt) : rk.advanceInTime(TACT, dt);
+#else
     double resid = rk.advanceInTime(TACT, dt);
+#endif
     TACT += dt;
     if (fl) fprintf(fl, "%d %.17g %.17g %.17g\n", step, dt, TACT, resid);
     if (fs && (step % P.every == 0)) Dump::state(fs, step, TACT, byFile, m, Np);
