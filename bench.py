@@ -248,7 +248,7 @@ def main():
     ap.add_argument("--configs", action="store_true",
                     help="only the other workloads: scalar P2 on 2048 triangles (200 steps) and "
                          "Maxwell P2 on 663552 tets (one TM110 period), both forms, ~2 min")
-    ap.add_argument("--profile-case", choices=["fp64", "mixed", "maxwell"], default=None,
+    ap.add_argument("--profile-case", choices=["fp64", "mixed", "maxwell", "limiter"], default=None,
                     help="only set up the workload and run --warmup + --steps steps (for ncu)")
     ap.add_argument("--block", type=int, default=0, choices=[0, 64, 128, 256],
                     help="--profile-case: tile shape (threads) of the element and face kernels "
@@ -738,6 +738,19 @@ def profile_case(args):
     """The bench workload alone: setup, --warmup steps, then --steps steps
     ("maxwell": the Maxwell P2 workload of --configs, FP64)."""
     import dgp
+    if args.profile_case == "limiter":
+        # Burgers P4, Lax-Friedrichs, 0.5 + sin(2 pi (x + y)) on 300x300x2
+        # triangles, mixed form, moment limiter after every stage
+        from dgp import meshgen
+        m = meshgen.tri_square(300, 300, 0.0, 1.0, 0.0, 1.0, jitter=0.15, seed=1000)
+        mesh = dgp.Mesh.from_arrays(2, m.vertices, m.cells, m.domain_tag, m.bfaces, m.btags)
+        law = dgp.Law(dgp.LAW_BURGERS2D, dgp.FLUX_LLF, dgp.FIELD_SINE, dgp.law_params(amplitude=1.0))
+        s = dgp.Solver(mesh, law, 4, dgp.MIXED, dgp.LIMITER_MOMENT)
+        s.project(0.0)
+        t, n = s.run(0.0, 0.0, 0.1, args.warmup + args.steps)
+        s.synchronize()
+        print(f"profile case limiter: {n} steps, t = {t:.6e}")
+        return 0
     if args.profile_case == "maxwell":
         from dgp import meshgen
         m3 = meshgen.tet_cube(48, 0.0, 1.0, jitter=0.1, seed=3, boundary_tag=40000)

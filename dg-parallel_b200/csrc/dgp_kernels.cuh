@@ -54,8 +54,9 @@ struct Cfg {
   // shared memory per cell of a tile: FP64 state and u_n, G rows, face slots,
   // geometry, CFL eigenvalues
   static constexpr int CELL_BYTES = 16 * MNP + (int)sizeof(T) * (M * LDK + NS * M) + 8 * (NV + DIM * DIM + 1);
-  // shared-memory budget of a tile: 768 bytes per thread, at most 110 KB
-  static constexpr int SMEM_BUDGET = BLOCK * 768 < 110 * 1024 ? BLOCK * 768 : 110 * 1024;
+  // shared-memory budget of a tile: 768 bytes per thread, at most 64 KB so
+  // that three tiles (with the table blob) share an SM whatever the order
+  static constexpr int SMEM_BUDGET = BLOCK * 768 < 64 * 1024 ? BLOCK * 768 : 64 * 1024;
   static constexpr int TE_SMEM = SMEM_BUDGET / CELL_BYTES;
   static constexpr int TE_ROWS = BLOCK / M;
   static constexpr int TE = TE_SMEM < TE_ROWS ? (TE_SMEM < 1 ? 1 : TE_SMEM) : TE_ROWS;
