@@ -65,7 +65,10 @@ struct Cfg {
   // face slots live tile-transposed, [tile][face point][row], so that the
   // element kernel reads them row-coalesced: slot(e, s, j) =
   // ((e / TE) * NS + s) * ROWS + (e % TE) * M + j
-  static constexpr int FACE_BLOCK = BLOCK;
+  // the face kernel's CTA does not depend on the tile shape (the slots are
+  // addressed per cell): 128 threads keep its register budget at the size
+  // that measured fastest
+  static constexpr int FACE_BLOCK = 128;
   static constexpr int FPB = FACE_BLOCK / NQF;  // faces per face-kernel CTA
   static constexpr int LDM = MNP | 1;           // staged coefficient row stride
 };
@@ -195,6 +198,25 @@ constexpr int pow2_div(int n) { return (n % 16 == 0) ? 16 : (n % 8 == 0) ? 8 : (
 
 // N values through the read-only path with loads of ALIGN bytes (p is
 // ALIGN-aligned)
+// N values to memory with stores of ALIGN bytes (p is ALIGN-aligned)
+template <typename T, int N, int ALIGN>
+__device__ __forceinline__ void st_vec(T* p, const T (&v)[N]) {
+  if constexpr (ALIGN == 16 && sizeof(T) == 8 && N % 2 == 0) {
+#pragma unroll
+    for (int i = 0; i < N / 2; ++i) reinterpret_cast<double2*>(p)[i] = make_double2(v[2 * i], v[2 * i + 1]);
+  } else if constexpr (ALIGN == 16 && sizeof(T) == 4 && N % 4 == 0) {
+#pragma unroll
+    for (int i = 0; i < N / 4; ++i)
+      reinterpret_cast<float4*>(p)[i] = make_float4(v[4 * i], v[4 * i + 1], v[4 * i + 2], v[4 * i + 3]);
+  } else if constexpr (ALIGN >= 8 && sizeof(T) == 4 && N % 2 == 0) {
+#pragma unroll
+    for (int i = 0; i < N / 2; ++i) reinterpret_cast<float2*>(p)[i] = make_float2(v[2 * i], v[2 * i + 1]);
+  } else {
+#pragma unroll
+    for (int i = 0; i < N; ++i) p[i] = v[i];
+  }
+}
+
 template <typename T, int N, int ALIGN>
 __device__ __forceinline__ void ldg_vec(const T* __restrict__ p, T (&out)[N]) {
   if constexpr (ALIGN == 16 && sizeof(T) == 8 && N % 2 == 0) {
@@ -330,13 +352,17 @@ __device__ __forceinline__ void face_finish(const StageArgs<typename K::T>& a, i
       boundary_flux<K::LAW, K::FLUX, DIM, T>(a.law, a.mesh.bbid[b], n, x, time, UL, flux);
     }
   }
-  T* sl = a.slots + slot_index<K>(eL, lfL * NQF + q, 0);
+  // the M values of a face point are contiguous in the slot layout: vector stores
+  constexpr int B = (int)(M * sizeof(T));
+  constexpr int ALIGN = pow2_div(B) < 16 ? pow2_div(B) : 16;
+  T v[M];
 #pragma unroll
-  for (int j = 0; j < M; ++j) sl[j] = -flux[j] * jw;
+  for (int j = 0; j < M; ++j) v[j] = -flux[j] * jw;
+  st_vec<T, M, ALIGN>(a.slots + slot_index<K>(eL, lfL * NQF + q, 0), v);
   if (eR >= 0) {
-    T* sr = a.slots + slot_index<K>(eR, lfR * NQF + qR, 0);
 #pragma unroll
-    for (int j = 0; j < M; ++j) sr[j] = flux[j] * jw;
+    for (int j = 0; j < M; ++j) v[j] = flux[j] * jw;
+    st_vec<T, M, ALIGN>(a.slots + slot_index<K>(eR, lfR * NQF + qR, 0), v);
   }
 }
 
