@@ -163,21 +163,38 @@ __device__ __forceinline__ void lim_row_moments(const double* __restrict__ row, 
 template <class K>
 __global__ void __launch_bounds__(128) limit_moments_kernel(LimArgs a) {
   constexpr int M = K::M, NP = K::NP, P = K::ORDER;
+  // the CTA's 128 rows are contiguous in the state and in the moments: both
+  // move through shared memory with coalesced loads and stores
+  __shared__ double s[128 * NP];
+  __shared__ unsigned char s_act[128];
   if (a.ctl && a.gctl->done) return;
   const size_t R = (size_t)a.E * M;
-  const size_t r = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
-  if (r >= R) return;
-  const int e = static_cast<int>(r / M);
-  if (lim_skip_cell(a, e)) return;
-  double gg[4];
+  const size_t r0 = blockIdx.x * (size_t)128;
+  const int nr = (int)(R - r0 < 128 ? R - r0 : 128);
+  const int t = threadIdx.x;
+  for (int i = t; i < nr * NP; i += 128) s[i] = a.C[r0 * NP + i];
+  __syncthreads();
+  const size_t r = r0 + t;
+  bool active = t < nr;
+  const int e = active ? static_cast<int>(r / M) : 0;
+  if (active && lim_skip_cell(a, e)) active = false;
+  s_act[t] = active ? 1 : 0;
+  if (active) {
+    double gg[4];
 #pragma unroll
-  for (int i = 0; i < 4; ++i) gg[i] = __ldg(a.geo + (size_t)e * kLimGeo + i);
-  double row[NP];
+    for (int i = 0; i < 4; ++i) gg[i] = __ldg(a.geo + (size_t)e * kLimGeo + i);
+    double row[NP], mo[NP];
 #pragma unroll
-  for (int k = 0; k < NP; ++k) row[k] = a.C[r * NP + k];
-  unsigned big = 0;
-  lim_row_moments<P, NP>(row, a.Dn, gg, a.Mo + r * NP, big);
-  a.big[r] = static_cast<unsigned char>(big);
+    for (int k = 0; k < NP; ++k) row[k] = s[t * NP + k];
+    unsigned big = 0;
+    lim_row_moments<P, NP>(row, a.Dn, gg, mo, big);
+#pragma unroll
+    for (int k = 0; k < NP; ++k) s[t * NP + k] = mo[k];  // the thread's own row
+    a.big[r] = static_cast<unsigned char>(big);
+  }
+  __syncthreads();
+  for (int i = t; i < nr * NP; i += 128)
+    if (s_act[i / NP]) a.Mo[r0 * NP + i] = s[i];
 }
 
 // one degree N of one row from the moments in registers (mo: the row's own,
