@@ -39,6 +39,7 @@ WORKLOAD = {"workload": "euler2d_isentropic_vortex_256x256x2_P3_roe", "cells": 1
             "rules": "12-pt volume, 4-pt Gauss-Legendre edges"}
 METRIC = "DOF-stage updates/s"
 REF_DRIVER = os.path.join(ROOT, "oracle", "_ref", "ref_driver")
+REF_DRIVER_LTS = os.path.join(ROOT, "oracle", "_ref", "ref_driver_lts")
 
 
 class Ranks:
@@ -248,7 +249,10 @@ def main():
     ap.add_argument("--configs", action="store_true",
                     help="only the other workloads: scalar P2 on 2048 triangles (200 steps) and "
                          "Maxwell P2 on 663552 tets (one TM110 period), both forms, ~2 min")
-    ap.add_argument("--profile-case", choices=["fp64", "mixed", "maxwell", "limiter"], default=None,
+    ap.add_argument("--lts", action="store_true",
+                    help="only the local time stepping measurement (Euler vortex P3 on 256x256x2 graded "
+                         "triangles, 4 size bins, against SSP-RK3 on the same mesh, ~1 min)")
+    ap.add_argument("--profile-case", choices=["fp64", "mixed", "maxwell", "limiter", "lts"], default=None,
                     help="only set up the workload and run --warmup + --steps steps (for ncu)")
     ap.add_argument("--block", type=int, default=0, choices=[0, 64, 128, 256],
                     help="--profile-case: tile shape (threads) of the element and face kernels "
@@ -278,6 +282,11 @@ def main():
         import torch
         torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
         print(json.dumps({"configs": configs_bench()}))
+        return 0
+    if args.lts:
+        import torch
+        torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+        print(json.dumps({"lts": lts_bench(steps=args.steps if args.steps != 300 else 16)}))
         return 0
 
     import numpy as np
@@ -635,6 +644,89 @@ def configs_bench(steps=200):
     return out
 
 
+def lts_mesh(n=256, ratio=1.0098):
+    """[0,10]^2 cut into n x n x 2 triangles with node lines spaced
+    geometrically (ratio 1.0098 per line: cell sizes span ~12x, 4 size bins,
+    every bin ~70 cells thick)."""
+    from dgp import meshgen
+    return meshgen.tri_graded(n, n, ratio, 0.0, 10.0, 0.0, 10.0)
+
+
+def lts_bench(n=256, ratio=1.0098, steps=16):
+    """Local time stepping (DGAnalysis mode 5: DGAnalysis::sortCellsBySize +
+    RungeKuttaTVD2adaptive) on the Euler vortex (beta 5 at (5, 5), Roe, P3,
+    FP64, exact-solution boundary) over lts_mesh(), CFL 0.1.  Timed with CUDA
+    events on the solver's stream: `steps` steps of DT (bin 0's step, the CFL
+    minimum times 2^(bins-1)) through dgp_run, then SSP-RK3 on the same mesh
+    from the same state to the same end time at the CFL step.  Units: a cell of
+    bin b takes 2^b sub-steps of two stages, M Np DOFs each (DOF-substage/s).
+    CPU: the reference's own binning and integrator (oracle/_ref/
+    ref_driver_lts, range helpers with the whole-mesh bodies) for one step on
+    one thread."""
+    import numpy as np
+    import torch
+    import dgp
+    m = lts_mesh(n, ratio)
+    mesh = dgp.Mesh.from_arrays(2, m.vertices, m.cells, 100, m.bfaces, m.btags)
+    law = dgp.Law(dgp.LAW_EULER2D, dgp.FLUX_ROE, dgp.FIELD_VORTEX, vortex_params())
+    M, NP = 4, 10
+
+    def timed_run(s, t0, tend, nmax):
+        stream = torch.cuda.ExternalStream(s.stream())
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record(stream)
+        t_end, k = s.run(t0, tend, 0.1, nmax)
+        e1.record(stream)
+        e1.synchronize()
+        return e0.elapsed_time(e1) / 1e3, t_end, k
+
+    s = dgp.Solver(mesh, law, 3, dgp.FP64)
+    nb = s.set_time_stepping(dgp.STEPPING_LOCAL)
+    bins, role = s.lts_bins()
+    E = mesh.ncells
+    units = float(np.sum(M * NP * 2 * (2.0 ** bins)))
+    t_w, _ = s.run(0.0, 0.0, 0.1, 3)  # warm-up (graph capture)
+    state_w = s.get_state()
+    DT = s.cfl_dt(0.1)
+    sec, t_end, k = timed_run(s, t_w, 0.0, steps)
+    launches = s.launches_per_step()
+    l2_lts = s.l2_error(t_end, 0)
+    rk = dgp.Solver(mesh, law, 3, dgp.FP64)
+    rk.set_state(state_w)
+    rk.run(t_w, 0.0, 0.1, 3)  # warm-up (graph capture), then back to the same state
+    rk.set_state(state_w)
+    dt_rk = rk.cfl_dt(0.1)
+    sec_rk, t_rk, k_rk = timed_run(rk, t_w, t_end, 0)
+    out = {"workload": f"Euler vortex P3 Roe FP64, {n}x{n}x2 graded triangles on [0,10]^2 "
+                       f"(node spacing ratio {ratio})", "cells": E, "bins": nb,
+           "cells_per_bin": np.bincount(bins, minlength=nb).tolist(),
+           "interface_cells": int(np.count_nonzero(role)),
+           "steps": k, "DT": DT, "t": [t_w, t_end], "ms_per_step": sec / k * 1e3,
+           "value": units * k / sec, "unit": "DOF-substage/s", "gpu_launches_per_step": launches,
+           "l2_density_vs_exact": l2_lts,
+           "ssprk3_same_mesh": {"steps": k_rk, "dt": dt_rk, "ms_per_step": sec_rk / k_rk * 1e3,
+                                "seconds_to_same_t": sec_rk, "l2_density_vs_exact": rk.l2_error(t_rk, 0)},
+           "seconds_to_same_t": sec, "speedup_over_ssprk3": sec_rk / sec}
+    rk.close()
+    s.close()
+    if os.path.exists(REF_DRIVER_LTS):
+        with tempfile.TemporaryDirectory() as td:
+            msh = os.path.join(td, "graded.msh")
+            from dgp import meshgen
+            meshgen.write_msh_v1(m, msh)
+            cmd = [REF_DRIVER_LTS, "--mesh", msh, "--lts", "1", "--case", "vortex", "--flux", "roe",
+                   "--order", "3", "--cfl", "0.1", "--bench", "1", "--warmup", "0"]
+            p = subprocess.run(cmd, capture_output=True, text=True, timeout=900)
+            line = next((ln for ln in p.stdout.splitlines() if ln.startswith("BENCH")), None)
+            if p.returncode == 0 and line:
+                kv = dict(tok.split("=") for tok in line.split()[1:])
+                out["cpu_baseline"] = {"value": units / float(kv["seconds"]), "unit": "DOF-substage/s",
+                                       "cores": 1, "kind": "reference",
+                                       "sample": "one step of the same mesh (ref_driver_lts, 1 thread)"}
+    return out
+
+
 def adjoint_bench(n=128, order=2, nsteps=400, every=20, nrec=64, ndir=16, eps=1e-3):
     """Discrete adjoint on the Euler vortex: 128x128x2 jittered triangles on
     [0,10]^2, P2, Roe flux, nsteps SSP-RK3 steps of a fixed dt (half the CFL
@@ -750,6 +842,17 @@ def profile_case(args):
         t, n = s.run(0.0, 0.0, 0.1, args.warmup + args.steps)
         s.synchronize()
         print(f"profile case limiter: {n} steps, t = {t:.6e}")
+        return 0
+    if args.profile_case == "lts":
+        # lts_bench's workload: local time stepping steps only
+        m = lts_mesh()
+        mesh = dgp.Mesh.from_arrays(2, m.vertices, m.cells, 100, m.bfaces, m.btags)
+        law = dgp.Law(dgp.LAW_EULER2D, dgp.FLUX_ROE, dgp.FIELD_VORTEX, vortex_params())
+        s = dgp.Solver(mesh, law, 3, dgp.FP64)
+        nb = s.set_time_stepping(dgp.STEPPING_LOCAL)
+        t, n = s.run(0.0, 0.0, 0.1, args.warmup + args.steps)
+        s.synchronize()
+        print(f"profile case lts: {nb} bins, {n} steps, t = {t:.6e}, {s.launches_per_step()} launches per step")
         return 0
     if args.profile_case == "maxwell":
         from dgp import meshgen

@@ -694,6 +694,7 @@ static int set_ctl(dgp_solver s, double t, double dt, double tend, double cfl, i
   c.tend = tend;
   c.cfl = cfl;
   c.max_steps = max_steps;
+  c.lts_shift = s->lts.on ? s->lts.nb - 1 : 0;  // mode-5 step: CFL minimum times 2^(bins-1)
   c.dtmin_bits = 0x7FF0000000000000ull;
   s->h_ctl[0] = c;
   DGP_CUDA(cudaMemcpyAsync(s->b.ctl, &s->h_ctl[0], sizeof(TimeCtl), cudaMemcpyHostToDevice, s->stream));
@@ -920,6 +921,11 @@ int dgp_cfl_dt(dgp_solver s, double cfl, double* dt) {
 // follows every stage and the next step's CFL reduction runs on the limited
 // state (instead of inside the last stage's element kernel)
 static void launch_step(dgp_solver s, int fuse_cfl) {
+  if (s->lts.on) {  // RungeKuttaTVD2adaptive::advanceInTime
+    dgp::launch_lts_step(s, fuse_cfl != 0);
+    if (!s->probes.empty()) launch_probe_recorders(s);
+    return;
+  }
   const bool lim = s->limiter != DGP_LIMITER_NONE && s->ops.limit;
   s->ops.stage(s->b, 1, 0.0, 0, s->stream);
   if (lim) s->ops.limit(s->b, 1, s->stream);
@@ -935,6 +941,10 @@ static void launch_step(dgp_solver s, int fuse_cfl) {
 
 int dgp_launches_per_step(dgp_solver s, int* n) {
   if (!s || !n) return fail(DGP_ERR_INVALID, "null argument");
+  if (s->lts.on) {
+    *n = dgp::launch_lts_step(s, true, true);
+    return DGP_OK;
+  }
   const bool lim = s->limiter != DGP_LIMITER_NONE && s->ops.limit;
   const int per_pass = s->limiter == DGP_LIMITER_BARTH ? 1 : 2;
   *n = 3 * (s->b.p0 ? 3 : 2) + (lim ? 3 * per_pass + 1 : 0);
@@ -1666,6 +1676,7 @@ static void step_keeping_stages(dgp_solver s, double* X, double* S, size_t ns) {
 }
 
 int dgp_forward_checkpointed(dgp_solver s, double t0, double dt, int nsteps, int every, double* J) {
+  if (s && s->lts.on) return fail(DGP_ERR_UNSUPPORTED, "the discrete adjoint follows SSP-RK3, not local time stepping");
   if (!s || !(dt > 0) || nsteps <= 0 || every < 0) return fail(DGP_ERR_INVALID, "bad argument");
   if (s->b.ninst) return fail(DGP_ERR_UNSUPPORTED, "the adjoint runs on a single solver");
   if (!s->ops.adj_stage) return fail(DGP_ERR_UNSUPPORTED, "no discrete adjoint for this law/flux");

@@ -62,6 +62,25 @@ struct AdjointState {
 
 struct dgp_probe_s;
 
+// Local time stepping (RungeKuttaTVD2adaptive on the size bins of
+// DGAnalysis::sortCellsBySize): bins and roles per internal cell, and device
+// lists of the integrator's cell groups and face classes.  Group (g, b): g = 0
+// inner cells of bin b, 1 large cells on interface b (bin b), 2 small cells on
+// interface b (bin b + 1).  Face class c < nb: faces of bin c; nb + c: faces
+// between bins c and c + 1.
+struct LtsState {
+  bool on = false;
+  int nb = 0;
+  std::vector<int> bin, role;        // internal cell order
+  int* lists = nullptr;              // all lists below, concatenated
+  int* fcls = nullptr;               // [F] class of each face
+  int* cface = nullptr;              // [E][NLF] face of each local face
+  double *c1 = nullptr, *save = nullptr, *racc = nullptr;  // copy slot, u_n, RHS accumulator
+  std::vector<int> goff, gn;         // group (g, b) at 3 * b + g: offset and length
+  std::vector<int> foff, fn;         // face class c: faces
+  std::vector<int> aoff, an;         // face class c: the cells that touch its faces
+};
+
 struct dgp_solver_s {
   AdjointState adj;
   dgp::PointLocator locator;            // built on first use (receivers, probes)
@@ -83,6 +102,7 @@ struct dgp_solver_s {
   cudaGraphExec_t graph1 = nullptr;  // one step (the tail of a run with a step limit)
   int graph_steps = 0;
   dgp::TimeCtl* h_ctl = nullptr;  // pinned, 2 entries
+  LtsState lts;                    // local time stepping (off unless enabled)
   void drop_graphs() {
     if (graph) cudaGraphExecDestroy(graph);
     if (graph1) cudaGraphExecDestroy(graph1);
@@ -157,6 +177,10 @@ int locate_points(dgp_solver s, int n, const double* points, std::vector<int>& c
 // probe recorders: launched at the end of every step; reset when a run starts
 void launch_probe_recorders(dgp_solver s);
 int reset_probe_recorders(dgp_solver s);
+// local time stepping (dgp_lts.cu): one advanceInTime of the current ctl->dt,
+// the step's end, and with next_dt the next step's CFL reduction; returns the
+// number of kernels launched (dry: count only)
+int launch_lts_step(dgp_solver s, bool next_dt, bool dry = false);
 }  // namespace dgp
 
 inline dgp_solver_s::~dgp_solver_s() {

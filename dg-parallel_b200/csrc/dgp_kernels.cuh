@@ -89,7 +89,7 @@ struct TimeCtl {
   int steps;         // steps completed
   int max_steps;     // <= 0: unbounded
   int done;          // set when tend or max_steps is reached
-  int pad;
+  int lts_shift;     // local time stepping: the step is the CFL minimum times 2^lts_shift
   unsigned long long dtmin_bits;  // atomicMin accumulator (positive double bits)
   unsigned int blocks_done;       // completion counter of the reducing kernel
   unsigned int pad2;
@@ -492,7 +492,7 @@ __device__ __forceinline__ double cell_dt(const StageArgs<typename K::T>& a, con
 
 __device__ __forceinline__ double ctl_finalize(TimeCtl* c, double dtmin) {
   bool done = (c->max_steps > 0 && c->steps >= c->max_steps) || (c->tend > 0 && c->t >= c->tend);
-  double dt = dtmin;
+  double dt = dtmin * (double)(1 << c->lts_shift);  // DGAnalysis.cc:590 (exact)
   if (c->tend > 0 && !done) {
     int N = (int)ceil((c->tend - c->t) / dt);
     dt = (c->tend - c->t) / N;

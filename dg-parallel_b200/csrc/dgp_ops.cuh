@@ -5,6 +5,7 @@
 #include "dgp_adjoint.cuh"
 #include "dgp_elem.cuh"
 #include "dgp_limiter.cuh"
+#include "dgp_lts.cuh"
 #include "dgp_solver.h"
 
 namespace dgp {
@@ -201,6 +202,33 @@ void ops_totals(const DeviceBuffers& b, double refm, int e_begin, int e_end, cud
 }
 
 template <class K>
+void ops_lts_vol(const DeviceBuffers& b, const int* cells, int n, double* racc, cudaStream_t st) {
+  const StageArgs<double> a = make_args<double>(b);
+  lts_vol_kernel<K><<<(n * K::M + 127) / 128, 128, 0, st>>>(a, cells, n, racc);
+}
+
+template <class K>
+void ops_lts_face(const DeviceBuffers& b, const int* faces, int n, double time_factor, cudaStream_t st) {
+  StageArgs<double> a = make_args<double>(b);
+  a.stage_time_factor = time_factor;
+  lts_face_kernel<K><<<(n + K::FPB - 1) / K::FPB, K::FACE_BLOCK, 0, st>>>(a, faces, n);
+}
+
+template <class K>
+void ops_lts_lift(const DeviceBuffers& b, const int* cells, int n, const int* cface, const int* fcls, int cls_a,
+                  int cls_b, double* racc, cudaStream_t st) {
+  const StageArgs<double> a = make_args<double>(b);
+  lts_lift_kernel<K><<<(n * K::M + 127) / 128, 128, 0, st>>>(a, cells, n, cface, fcls, cls_a, cls_b, racc);
+}
+
+template <class K>
+void ops_lts_update(const DeviceBuffers& b, const int* cells, int n, int op, double dt_factor, double* c1,
+                    double* save, double* racc, cudaStream_t st) {
+  const StageArgs<double> a = make_args<double>(b);
+  lts_update_kernel<K><<<(n * K::M + 127) / 128, 128, 0, st>>>(a, cells, n, op, dt_factor, c1, save, racc);
+}
+
+template <class K>
 Ops make_ops() {
   Ops o;
   o.M = K::M;
@@ -228,6 +256,12 @@ Ops make_ops() {
   o.limit = K::ORDER >= 1 ? &ops_limit<K> : nullptr;
   o.adj_stage = adjoint_built<K>() ? &ops_adj_stage<K> : nullptr;
   o.trace = &ops_trace<K>;
+  if constexpr (sizeof(typename K::T) == 8 && K::BLOCK == kDefaultBlock) {
+    o.lts_vol = &ops_lts_vol<K>;
+    o.lts_face = &ops_lts_face<K>;
+    o.lts_lift = &ops_lts_lift<K>;
+    o.lts_update = &ops_lts_update<K>;
+  }
   return o;
 }
 

@@ -183,6 +183,16 @@ struct Ops {
   void (*trace)(const DeviceBuffers&, const unsigned char* only, cudaStream_t) = nullptr;
   // discrete adjoint stage (nullptr where the adjoint is not built)
   void (*adj_stage)(const DeviceBuffers&, const AdjStage&, cudaStream_t) = nullptr;
+  // local time stepping (FP64, 128-thread tiles; nullptr elsewhere): volume
+  // term of listed cells into racc; face kernel over a face list (boundary
+  // time t + time_factor * dt); lift of face classes a / b into racc; one
+  // coefficient operation (LtsUpdateOp) with dt = ctl->dt * dt_factor
+  void (*lts_vol)(const DeviceBuffers&, const int* cells, int n, double* racc, cudaStream_t) = nullptr;
+  void (*lts_face)(const DeviceBuffers&, const int* faces, int n, double time_factor, cudaStream_t) = nullptr;
+  void (*lts_lift)(const DeviceBuffers&, const int* cells, int n, const int* cface, const int* fcls, int cls_a,
+                   int cls_b, double* racc, cudaStream_t) = nullptr;
+  void (*lts_update)(const DeviceBuffers&, const int* cells, int n, int op, double dt_factor, double* c1,
+                     double* save, double* racc, cudaStream_t) = nullptr;
 };
 
 // law, flux, dim, order, precision, block (tile variant: 64, 128 or 256 threads)

@@ -19,6 +19,7 @@ FLUX_UPWIND, FLUX_CENTRAL, FLUX_GODUNOV, FLUX_ROE, FLUX_LLF = range(5)
 FIELD_GAUSS, FIELD_VORTEX, FIELD_PULSE3D, FIELD_SINE, FIELD_GAUSS3D, FIELD_TM110 = range(6)
 FP64, MIXED = 0, 1
 LIMITER_NONE, LIMITER_MOMENT, LIMITER_BARTH = 0, 1, 2
+STEPPING_SSPRK3, STEPPING_LOCAL = 0, 5
 NPARAMS = 16
 
 ERRORS = {-1: "invalid argument", -2: "I/O", -3: "unsupported", -4: "CUDA", -5: "non-physical",
@@ -90,6 +91,8 @@ def lib() -> ctypes.CDLL:
         "dgp_limiter_triggers": ([P, ctypes.POINTER(ctypes.c_uint8)], I),
         "dgp_set_p0_fallback": ([P, I], I),
         "dgp_launches_per_step": ([P, pI], I),
+        "dgp_set_time_stepping": ([P, I, pI], I),
+        "dgp_lts_bins": ([P, pI, pI], I),
         "dgp_ensemble_create": ([I, pP, pP, pI, I, I, pP], I),
         "dgp_ensemble_destroy": ([P], I),
         "dgp_ensemble_info": ([P, I, pI, pI, pI, pI], I),
@@ -338,6 +341,23 @@ class Solver:
         n = ctypes.c_int()
         check(lib().dgp_launches_per_step(self.h, ctypes.byref(n)))
         return n.value
+
+    def set_time_stepping(self, mode: int = STEPPING_LOCAL) -> int:
+        """DGAnalysis's timeSteppingMode: STEPPING_LOCAL (5) bins the cells by
+        size and steps with RungeKuttaTVD2adaptive; STEPPING_SSPRK3 (0) goes
+        back to SSP-RK3.  Returns the number of size bins (0 for SSP-RK3)."""
+        n = ctypes.c_int()
+        check(lib().dgp_set_time_stepping(self.h, mode, ctypes.byref(n)))
+        return n.value
+
+    def lts_bins(self):
+        """(bin, role) per cell in file order; role 0 inner, 1 large and 2
+        small on an interface between bins."""
+        bins = np.zeros(self.ncells, dtype=np.int32)
+        role = np.zeros(self.ncells, dtype=np.int32)
+        pI = ctypes.POINTER(ctypes.c_int)
+        check(lib().dgp_lts_bins(self.h, bins.ctypes.data_as(pI), role.ctypes.data_as(pI)))
+        return bins, role
 
     def block(self) -> tuple[int, int]:
         """(threads, cells per element-kernel tile) of the tile shape in use."""

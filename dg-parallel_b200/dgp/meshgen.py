@@ -14,6 +14,9 @@ Meshes:
 * :func:`tri_square` -- an ``nx x ny`` grid of a rectangle, each cell split into
   two counter-clockwise triangles along the (i,j)-(i+1,j+1) diagonal, interior
   vertices jittered by a seeded uniform offset of +-``jitter*h`` per axis.
+* :func:`tri_graded` -- the same triangulation with node lines spaced
+  geometrically (ratio ``ratio`` between neighbouring spacings, per axis), so
+  that cell sizes span several factors of two (local time stepping bins).
 * :func:`tet_cube` -- an ``n^3`` grid of a box, each cube split into the six
   Kuhn tetrahedra around its main diagonal (conforming across cubes), interior
   vertices jittered the same way.
@@ -108,6 +111,25 @@ def tri_square(nx: int, ny: int, x0: float = 0.0, x1: float = 1.0, y0: float = 0
     bfaces = np.array(b, dtype=np.int64)
     btags = np.array(t, dtype=np.int64)
     return Mesh(2, verts, cells, bfaces, btags, domain_tag)
+
+
+def tri_graded(nx: int, ny: int, ratio: float = 1.08, x0: float = 0.0, x1: float = 1.0,
+               y0: float = 0.0, y1: float = 1.0, boundary_tag: int = 1, domain_tag: int = 100,
+               side_tags=None) -> Mesh:
+    """``tri_square`` (no jitter) with node line i at
+    ``x0 + (x1 - x0) (ratio^i - 1) / (ratio^nx - 1)`` (and likewise in y): the
+    cells shrink geometrically towards the (x0, y0) corner."""
+    m = tri_square(nx, ny, 0.0, 1.0, 0.0, 1.0, jitter=0.0, boundary_tag=boundary_tag,
+                   domain_tag=domain_tag, side_tags=side_tags)
+
+    def grade(u, n, lo, hi):
+        i = np.rint(u * n)
+        return lo + (hi - lo) * (ratio ** i - 1.0) / (ratio ** n - 1.0)
+
+    v = m.vertices.copy()
+    v[:, 0] = grade(v[:, 0], nx, x0, x1)
+    v[:, 1] = grade(v[:, 1], ny, y0, y1)
+    return Mesh(2, v, m.cells, m.bfaces, m.btags, domain_tag)
 
 
 def _kuhn_cube_tets() -> list[tuple[int, int, int, int]]:

@@ -119,9 +119,11 @@ int dgp_get_state_device(dgp_solver s, double* dev_state);
 /* assembled theRightHandSide of every cell for the current state at time t:
  * TimeIntegrator::assembleVolume + assembleBoundary (TimeIntegrator.cc:1332-1412) */
 int dgp_rhs(dgp_solver s, double t, double* host_rhs);
-/* min over cells of DGCell::adaptTimeStep (DGCell.cc:1155-1207) */
+/* min over cells of DGCell::adaptTimeStep (DGCell.cc:1155-1207); times
+ * 2^(bins - 1) with local time stepping (dgp_set_time_stepping) */
 int dgp_cfl_dt(dgp_solver s, double cfl, double* dt);
-/* RungeKuttaTVD3::advanceInTime(t, dt) (TimeIntegrator.cc:838-990); resid may be NULL */
+/* RungeKuttaTVD3::advanceInTime(t, dt) (TimeIntegrator.cc:838-990), or
+ * RungeKuttaTVD2adaptive::advanceInTime with local time stepping; resid may be NULL */
 int dgp_step(dgp_solver s, double t, double dt, double* resid);
 /* time loop of DGAnalysis::run (DGAnalysis.cc:480-731): CFL dt every step,
  * stretched to land on tend when tend > 0; at most max_steps when > 0.
@@ -129,8 +131,34 @@ int dgp_step(dgp_solver s, double t, double dt, double* resid);
 int dgp_run(dgp_solver s, double t0, double tend, double cfl, int max_steps, double* t_out,
             int* steps_out);
 /* kernels one step of dgp_run launches (face/element kernels per stage, the
- * P0 fallback's second face pass, limiter passes and the CFL reduction) */
+ * P0 fallback's second face pass, limiter passes and the CFL reduction; with
+ * local time stepping the kernels of one advanceInTime, the step's end and the
+ * CFL reduction) */
 int dgp_launches_per_step(dgp_solver s, int* n);
+
+/* ---- time stepping mode: DGAnalysis's timeSteppingMode (DGAnalysis.cc:229-242)
+ * DGP_STEPPING_SSPRK3: RungeKuttaTVD3 (the default).
+ * DGP_STEPPING_LOCAL: mode 5, local time stepping -- DGAnalysis::sortCellsBySize
+ *   (DGAnalysis.cc:749-890) bins the cells by size (bin b: sizes in
+ *   (max/2^(b+1), max/2^b], times 1.0001) and RungeKuttaTVD2adaptive
+ *   (TimeIntegrator.cc:442-836) advances bin b with dt / 2^b, interface cells
+ *   by the integrator's half steps.  dgp_step(t, dt) is then one
+ *   advanceInTime(t, dt) (dt for bin 0; resid 0 as the reference returns),
+ *   dgp_run and dgp_cfl_dt use the mode-5 step (CFL minimum times
+ *   2^(bins - 1), DGAnalysis.cc:590).  The reference ships the range helpers
+ *   this integrator calls (TimeIntegrator::assembleVolume/assembleBoundary(
+ *   begin, end, t), TimeIntegrator.cc:1438-1487) with empty bodies, so its own
+ *   mode 5 leaves the state unchanged; this library assembles what their
+ *   whole-mesh versions assemble on each range.  FP64, no limiter, single
+ *   solvers; meshes the reference rejects (fewer than 2 or more than 10 bins,
+ *   a cell in no bin or on two interfaces, neighbours more than one bin apart)
+ *   give DGP_ERR_INVALID.  nbins (may be NULL) receives the number of bins.
+ * dgp_lts_bins: per cell (file order) its bin and role (0 inner, 1 large on an
+ *   interface, 2 small on an interface); either pointer may be NULL. */
+#define DGP_STEPPING_SSPRK3 0
+#define DGP_STEPPING_LOCAL 5
+int dgp_set_time_stepping(dgp_solver s, int mode, int* nbins);
+int dgp_lts_bins(dgp_solver s, int* bin, int* role);
 /* Triangle moment limiter (DGP_LIMITER_MOMENT; replaces DGMomentLimiter::limit,
  * DGLimiter.cc:963-1133, which indexes the quadrilateral tensor basis and is
  * invalid on triangles).  The solver applies it after every SSP-RK3 stage

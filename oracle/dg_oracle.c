@@ -67,6 +67,10 @@ struct or_solver {
   unsigned char* trig; /* [E] trigger degree of the last limiter application */
   unsigned char* bad;  /* [E] P0 fallback marks */
   int* pcell;          /* [F] periodic partner's cell of a boundary face (-1: none) */
+  /* local time stepping (or_lts_setup) */
+  int lts_nb;          /* number of size bins, 0: off */
+  int *lts_bin, *lts_role, *lts_fcls; /* [E] bin, [E] role, [F] face class */
+  double *lts_c1, *lts_save, *lts_r;  /* copy slot, saved u_n, RHS accumulator */
 };
 
 static void build_limiter_tables(or_solver* s);
@@ -1109,6 +1113,8 @@ or_solver* or_create(const char* msh_path, int law, int flux, int order, int fie
 
 void or_destroy(or_solver* s) {
   if (!s) return;
+  free(s->lts_bin); free(s->lts_role); free(s->lts_fcls);
+  free(s->lts_c1); free(s->lts_save); free(s->lts_r);
   free(s->X); free(s->vid); free(s->cv); free(s->fv); free(s->eL); free(s->eR);
   free(s->lfL); free(s->lfR); free(s->bid); free(s->jac); free(s->jinv); free(s->det);
   free(s->csize); free(s->fn); free(s->fmeas); free(s->trL); free(s->trR); free(s->fx);
@@ -1190,63 +1196,70 @@ static void interp(const double* fct, const double* a, int m, int Np, double* fi
   }
 }
 
-/* assembly: DGCell::computeVolumeContribution (DGCell.cc:184-249) over all
- * cells, then DGBoundaryCell::computeBoundaryContributions (:639-732) over all
- * faces, accumulating into R (which is zeroed first). */
-static void assemble(or_solver* s, const double* C, double t, double* R) {
+/* DGCell::computeVolumeContribution (DGCell.cc:184-249) of cell e, added to R */
+static void vol_add(const or_solver* s, const double* C, int e, double* R) {
   const int m = s->m, Np = s->Np, d = s->dim;
-  memset(R, 0, (size_t)s->E * m * Np * sizeof(double));
-  for (int e = 0; e < s->E; ++e) {
-    const double* c = C + (size_t)e * m * Np;
-    double* r = R + (size_t)e * m * Np;
-    const double* Ji = s->jinv + 9 * e;
-    for (int q = 0; q < s->nq; ++q) {
-      double U[MAXM], F[MAXM][3], x[3];
-      interp(s->phi[q], c, m, Np, U);
-      phys_point(s, e, s->qp[q], x);
-      law_flux(s, x, U, F);
-      double jw = s->det[e] * s->qw[q];
-      for (int j = 0; j < m; ++j)
-        for (int k = 0; k < Np; ++k) {
-          double g[3];
-          for (int i = 0; i < 3; ++i) {
-            g[i] = 0.0;
-            for (int jj = 0; jj < 3; ++jj) g[i] += Ji[i * 3 + jj] * (jj < d ? s->dphi[q][jj][k] : 0.0);
-            g[i] *= jw;
-          }
-          r[j * Np + k] += F[j][0] * g[0] + F[j][1] * g[1] + F[j][2] * g[2];
+  const double* c = C + (size_t)e * m * Np;
+  double* r = R + (size_t)e * m * Np;
+  const double* Ji = s->jinv + 9 * e;
+  for (int q = 0; q < s->nq; ++q) {
+    double U[MAXM], F[MAXM][3], x[3];
+    interp(s->phi[q], c, m, Np, U);
+    phys_point(s, e, s->qp[q], x);
+    law_flux(s, x, U, F);
+    double jw = s->det[e] * s->qw[q];
+    for (int j = 0; j < m; ++j)
+      for (int k = 0; k < Np; ++k) {
+        double g[3];
+        for (int i = 0; i < 3; ++i) {
+          g[i] = 0.0;
+          for (int jj = 0; jj < 3; ++jj) g[i] += Ji[i * 3 + jj] * (jj < d ? s->dphi[q][jj][k] : 0.0);
+          g[i] *= jw;
         }
-    }
-  }
-  for (int f = 0; f < s->F; ++f) {
-    int eL = s->eL[f], eR = s->eR[f];
-    const double* n = s->fn + 3 * f;
-    for (int q = 0; q < s->nqf; ++q) {
-      const double* x = s->fx + (f * s->nqf + q) * 3;
-      const double* pl = s->trL + ((size_t)f * s->nqf + q) * Np;
-      const double* pr = s->trR + ((size_t)f * s->nqf + q) * Np;
-      double UL[MAXM], UR[MAXM], flux[MAXM];
-      interp(pl, C + (size_t)eL * m * Np, m, Np, UL);
-      if (eR >= 0) {
-        interp(pr, C + (size_t)eR * m * Np, m, Np, UR);
-        riemann_flux(s, n, x, UL, UR, flux);
-      } else if (s->pcell[f] >= 0) { /* periodic: the partner's trace (DGCell.cc:687-705) */
-        interp(pr, C + (size_t)s->pcell[f] * m * Np, m, Np, UR);
-        riemann_flux(s, n, x, UL, UR, flux);
-      } else {
-        boundary_flux(s, s->bid[f], n, x, t, UL, flux);
+        r[j * Np + k] += F[j][0] * g[0] + F[j][1] * g[1] + F[j][2] * g[2];
       }
-      double jw = s->fjw[f * s->nqf + q];
-      double* rl = R + (size_t)eL * m * Np;
+  }
+}
+
+/* DGBoundaryCell::computeBoundaryContributions (DGCell.cc:639-732) of face f
+ * at time t, added to R of both sides */
+static void face_add(const or_solver* s, const double* C, int f, double t, double* R) {
+  const int m = s->m, Np = s->Np;
+  int eL = s->eL[f], eR = s->eR[f];
+  const double* n = s->fn + 3 * f;
+  for (int q = 0; q < s->nqf; ++q) {
+    const double* x = s->fx + (f * s->nqf + q) * 3;
+    const double* pl = s->trL + ((size_t)f * s->nqf + q) * Np;
+    const double* pr = s->trR + ((size_t)f * s->nqf + q) * Np;
+    double UL[MAXM], UR[MAXM], flux[MAXM];
+    interp(pl, C + (size_t)eL * m * Np, m, Np, UL);
+    if (eR >= 0) {
+      interp(pr, C + (size_t)eR * m * Np, m, Np, UR);
+      riemann_flux(s, n, x, UL, UR, flux);
+    } else if (s->pcell[f] >= 0) { /* periodic: the partner's trace (DGCell.cc:687-705) */
+      interp(pr, C + (size_t)s->pcell[f] * m * Np, m, Np, UR);
+      riemann_flux(s, n, x, UL, UR, flux);
+    } else {
+      boundary_flux(s, s->bid[f], n, x, t, UL, flux);
+    }
+    double jw = s->fjw[f * s->nqf + q];
+    double* rl = R + (size_t)eL * m * Np;
+    for (int j = 0; j < m; ++j)
+      for (int k = 0; k < Np; ++k) rl[j * Np + k] -= flux[j] * pl[k] * jw;
+    if (eR >= 0) {
+      double* rr = R + (size_t)eR * m * Np;
       for (int j = 0; j < m; ++j)
-        for (int k = 0; k < Np; ++k) rl[j * Np + k] -= flux[j] * pl[k] * jw;
-      if (eR >= 0) {
-        double* rr = R + (size_t)eR * m * Np;
-        for (int j = 0; j < m; ++j)
-          for (int k = 0; k < Np; ++k) rr[j * Np + k] += flux[j] * pr[k] * jw;
-      }
+        for (int k = 0; k < Np; ++k) rr[j * Np + k] += flux[j] * pr[k] * jw;
     }
   }
+}
+
+/* assembly: the volume terms of all cells, then the face terms of all faces,
+ * accumulating into R (which is zeroed first). */
+static void assemble(or_solver* s, const double* C, double t, double* R) {
+  memset(R, 0, (size_t)s->E * s->m * s->Np * sizeof(double));
+  for (int e = 0; e < s->E; ++e) vol_add(s, C, e, R);
+  for (int f = 0; f < s->F; ++f) face_add(s, C, f, t, R);
 }
 
 void or_rhs(or_solver* s, double t, double* out) { assemble(s, s->C, t, out); }
@@ -1817,3 +1830,245 @@ double or_l2_error(const or_solver* s, double t, int fi) {
   }
   return sqrt(acc);
 }
+
+/* ------------------------------------------------------------------------ */
+/* Local time stepping: RungeKuttaTVD2adaptive (TimeIntegrator.cc:442-836)   */
+/* on the size bins of DGAnalysis::sortCellsBySize (DGAnalysis.cc:749-890).  */
+/* The reference's range helpers TimeIntegrator::assembleVolume/             */
+/* assembleBoundary(begin, end, t) (TimeIntegrator.cc:1438-1487) ship with   */
+/* their bodies commented out, which leaves its local time stepping without  */
+/* a right-hand side; here they do what the whole-mesh versions do           */
+/* (TimeIntegrator.cc:1332-1412) on their range.  The right-hand side of a   */
+/* cell accumulates across calls and is zeroed where the integrator calls   */
+/* ZeroRHS, as in the reference.  Roles: 0 inner cell of bin b, 1 large cell */
+/* on interface b (bin b), 2 small cell on interface b (bin b + 1).  Face   */
+/* classes: b for the faces of bin b (both cells in bin b, or a boundary    */
+/* face of a bin-b cell), nb + b for the faces between bins b and b + 1.    */
+/* No limiter and no P0 fallback on this path.                              */
+/* ------------------------------------------------------------------------ */
+#define LTS_MAXBINS 10 /* the integrator's per-bin arrays (TimeIntegrator.h:47-50) */
+
+int or_lts_setup(or_solver* s) {
+  const int E = s->E, F = s->F;
+  double maxS = 0.0, minS = 1.0; /* DGAnalysis.cc:756-766 (the minimum starts at 1) */
+  for (int e = 0; e < E; ++e) {
+    if (maxS < s->csize[e]) maxS = s->csize[e];
+    if (minS > s->csize[e]) minS = s->csize[e];
+  }
+  int nb = (int)ceil(log(maxS / minS) / log(2.));
+  if (nb < 2) return -1; /* no cell is binned: the reference stops ("cells were lost") */
+  if (nb > LTS_MAXBINS) return -2;
+  double B[LTS_MAXBINS + 1];
+  B[0] = maxS;
+  for (int i = 1; i <= nb; ++i) B[i] = B[i - 1] * 0.5;
+  int* bin = (int*)malloc(sizeof(int) * (size_t)E);
+  int* role = (int*)malloc(sizeof(int) * (size_t)E);
+  int* fcls = (int*)malloc(sizeof(int) * (size_t)(F > 0 ? F : 1));
+  int rc = 0;
+  for (int e = 0; e < E && !rc; ++e) {
+    bin[e] = -1;
+    role[e] = 0;
+    for (int i = 1; i <= nb; ++i)
+      if (s->csize[e] <= B[i - 1] * 1.0001 && s->csize[e] > B[i] * 1.0001) bin[e] = i - 1;
+    if (bin[e] < 0) rc = -3; /* below B_nb * 1.0001: lost */
+  }
+  for (int f = 0; f < F && !rc; ++f) {
+    const int eL = s->eL[f], eR = s->eR[f];
+    const int lb = bin[eL], rb = eR >= 0 ? bin[eR] : 0;
+    if (eR < 0 || lb == rb) {
+      fcls[f] = lb;
+    } else if (lb - rb == 1 || rb - lb == 1) {
+      const int lo = lb < rb ? lb : rb;
+      const int large = lb < rb ? eL : eR, small = lb < rb ? eR : eL;
+      fcls[f] = nb + lo;
+      if (role[large] == 2 || role[small] == 1) rc = -4; /* on two interfaces: counted twice */
+      role[large] = 1;
+      role[small] = 2;
+    } else {
+      rc = -5; /* "Too big a difference between elements" */
+    }
+  }
+  if (rc) {
+    free(bin); free(role); free(fcls);
+    return rc;
+  }
+  free(s->lts_bin); free(s->lts_role); free(s->lts_fcls);
+  free(s->lts_c1); free(s->lts_save); free(s->lts_r);
+  const size_t n = (size_t)E * s->m * s->Np;
+  s->lts_bin = bin;
+  s->lts_role = role;
+  s->lts_fcls = fcls;
+  s->lts_c1 = (double*)calloc(n, sizeof(double));
+  s->lts_save = (double*)calloc(n, sizeof(double));
+  s->lts_r = (double*)calloc(n, sizeof(double));
+  s->lts_nb = nb;
+  return nb;
+}
+
+void or_lts_bins(const or_solver* s, int* bin, int* role) {
+  memcpy(bin, s->lts_bin, sizeof(int) * (size_t)s->E);
+  memcpy(role, s->lts_role, sizeof(int) * (size_t)s->E);
+}
+
+/* group g of interface/bin index b: 0 inner cells of bin b, 1 large on
+ * interface b, 2 small on interface b */
+static int lts_in(const or_solver* s, int e, int g, int b) {
+  const int r = s->lts_role[e], bb = s->lts_bin[e];
+  return r == g && (g == 2 ? bb == b + 1 : bb == b);
+}
+
+static void lts_vol(or_solver* s, int g, int b) {
+  for (int e = 0; e < s->E; ++e)
+    if (lts_in(s, e, g, b)) vol_add(s, s->C, e, s->lts_r);
+}
+
+static void lts_bnd(or_solver* s, int cls, double t) {
+  for (int f = 0; f < s->F; ++f)
+    if (s->lts_fcls[f] == cls) face_add(s, s->C, f, t, s->lts_r);
+}
+
+/* the integrator's coefficient operations on one group (arithmetic in the
+ * reference's order, one rounding per operation) */
+enum { LU_EULER_IN, LU_TWO_HALF, LU_EULER, LU_SECOND, LU_SECOND_SWAP, LU_COPYBACK_ZERO, LU_LI_HALF,
+       LU_RESTORE, LU_FINAL_RESET };
+
+static void lts_update(or_solver* s, int g, int b, int op, double dt) {
+  const int dof = s->m * s->Np;
+  for (int e = 0; e < s->E; ++e) {
+    if (!lts_in(s, e, g, b)) continue;
+    const double det = s->det[e];
+    double* c = s->C + (size_t)e * dof;
+    double* c1 = s->lts_c1 + (size_t)e * dof;
+    double* sv = s->lts_save + (size_t)e * dof;
+    double* r = s->lts_r + (size_t)e * dof;
+    for (int i = 0; i < dof; ++i) {
+      switch (op) {
+        case LU_EULER_IN: /* TimeIntegrator.cc:486-490 */
+          sv[i] = c[i];
+          c[i] += r[i] / det * dt;
+          break;
+        case LU_TWO_HALF: /* :508-518, :560-571 */
+          sv[i] = c[i];
+          c[i] += r[i] * dt / det;
+          c1[i] = c[i];
+          c[i] += r[i] * dt / det;
+          break;
+        case LU_EULER: /* :537-541 */
+          sv[i] = c[i];
+          c[i] += r[i] * dt / det;
+          break;
+        case LU_SECOND: /* :647-653, :697-704 */
+        case LU_SECOND_SWAP: { /* :670-678, then DG_Dofs::swap */
+          const double cn = (c[i] + r[i] * dt / det + sv[i]) * 0.5;
+          if (op == LU_SECOND) {
+            c[i] = cn;
+          } else {
+            c[i] = c1[i];
+            c1[i] = cn;
+          }
+          break;
+        }
+        case LU_COPYBACK_ZERO: /* :615-621 */
+          c[i] = c1[i];
+          break;
+        case LU_LI_HALF: { /* :735-738 */
+          const double cn = sv[i] + (c[i] - sv[i]) + 0.25 * (c1[i] - 2. * c[i] + sv[i]);
+          c[i] = cn;
+          sv[i] = cn + 0.5 * (c1[i] - sv[i]);
+          break;
+        }
+        case LU_RESTORE: /* :759-760 */
+          c[i] = sv[i];
+          break;
+        case LU_FINAL_RESET: /* :777 */
+          c[i] = c1[i];
+          break;
+      }
+      if (op != LU_SECOND_SWAP && op != LU_LI_HALF && op != LU_RESTORE) r[i] = 0.0;
+    }
+  }
+}
+
+/* RungeKuttaTVD2adaptive::firstStage (TimeIntegrator.cc:442-591) */
+static void lts_first(or_solver* s, int from, int to, double t, double DT) {
+  const int nb = s->lts_nb;
+  double dt = DT / pow(2., from);
+  if (from) lts_vol(s, 2, from - 1);
+  for (int b = from; b < to; ++b) {
+    lts_vol(s, 0, b);
+    lts_vol(s, 1, b);
+    lts_vol(s, 2, b);
+    lts_bnd(s, b, t + dt);
+    lts_bnd(s, nb + b, t + dt);
+    dt *= 0.5;
+  }
+  if (from) lts_bnd(s, nb + from - 1, t + dt);
+  dt = DT / pow(2., from);
+  for (int b = from; b < to; ++b) {
+    lts_update(s, 0, b, LU_EULER_IN, dt);
+    dt *= 0.5;
+  }
+  dt = DT / pow(2., from);
+  for (int b = from; b < to - 1; ++b) {
+    dt *= 0.5;
+    lts_update(s, 1, b, LU_TWO_HALF, dt);
+  }
+  dt = DT / pow(2., from);
+  if (from) lts_update(s, 2, from - 1, LU_EULER, dt);
+  for (int b = from; b < to - 1; ++b) {
+    dt *= 0.5;
+    lts_update(s, 2, b, LU_TWO_HALF, dt);
+  }
+}
+
+/* RungeKuttaTVD2adaptive::secondStage (TimeIntegrator.cc:594-715) */
+static void lts_second(or_solver* s, int from, int to, double t, double DT) {
+  const int nb = s->lts_nb;
+  double dt = DT / pow(2., from);
+  for (int b = from; b < to; ++b) {
+    if (b > from) lts_update(s, 2, b - 1, LU_COPYBACK_ZERO, dt);
+    lts_vol(s, 0, b);
+    lts_vol(s, 1, b);
+    if (b > 0) lts_vol(s, 2, b - 1);
+    lts_bnd(s, b, t + dt);
+    lts_bnd(s, nb + b, t + dt);
+    if (b > 0) lts_bnd(s, nb + b - 1, t + dt);
+    lts_update(s, 0, b, LU_SECOND, dt);
+    lts_update(s, 1, b, LU_SECOND_SWAP, dt);
+    if (b > 0) lts_update(s, 2, b - 1, LU_SECOND, dt);
+    dt *= 0.5;
+  }
+}
+
+/* RungeKuttaTVD2adaptive::advanceInTime (TimeIntegrator.cc:784-836): one
+ * step of DT for bin 0, sub-cycled down to DT / 2^(nb-1) for the last bin.
+ * Returns 0 as the reference does. */
+double or_lts_step(or_solver* s, double t, double DT) {
+  const int nb = s->lts_nb;
+  int flat[LTS_MAXBINS];
+  if (nb < 2) return -1.0;
+  for (int i = 0; i < nb; ++i) flat[i] = 1;
+  lts_first(s, 0, nb, t, DT);
+  lts_second(s, 0, nb, t, DT);
+  for (int i = 1; i < nb; ++i) flat[i] = 0;
+  int i = nb - 1;
+  while (i > 0) {
+    for (i = nb - 1; i >= 1; i--)
+      if (!flat[i]) {
+        lts_update(s, 1, i - 1, LU_LI_HALF, 0.0);
+        lts_first(s, i, nb, t, DT);
+        lts_update(s, 1, i - 1, LU_RESTORE, 0.0);
+        lts_second(s, i, nb, t, DT);
+        lts_update(s, 1, i - 1, LU_FINAL_RESET, 0.0);
+        flat[i] = 1;
+        if (i != nb - 1)
+          for (int j = i + 1; j < nb; ++j) flat[j] = 0;
+        break;
+      }
+  }
+  return 0.0;
+}
+
+/* time step of DGAnalysis::run mode 5 (DGAnalysis.cc:514-593): the CFL
+ * minimum times 2^(bins - 1) */
+double or_lts_dt(const or_solver* s, double cfl) { return or_cfl_dt(s, cfl) * pow(2., s->lts_nb - 1); }

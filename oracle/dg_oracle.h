@@ -68,6 +68,18 @@ void or_set_p0_fallback(or_solver* s, int on);
 void or_bad_cells(const or_solver* s, unsigned char* out); /* marks of the last stage */
 void or_triggers(const or_solver* s, unsigned char* out);  /* of the last limiter pass */
 
+/* local time stepping (RungeKuttaTVD2adaptive on the size bins of
+ * DGAnalysis::sortCellsBySize; definitions in dg_oracle.c): or_lts_setup bins
+ * the cells and returns the number of bins, or < 0 where the reference stops
+ * (-1 fewer than 2 bins, -2 more than 10, -3 a cell in no bin, -4 a cell on
+ * two interfaces, -5 neighbours more than one bin apart); or_lts_bins: bin
+ * and role (0 inner, 1 large, 2 small on an interface) per cell, file order;
+ * or_lts_step: one step of dt for bin 0; or_lts_dt: the mode-5 step. */
+int or_lts_setup(or_solver* s);
+void or_lts_bins(const or_solver* s, int* bin, int* role);
+double or_lts_step(or_solver* s, double t, double dt);
+double or_lts_dt(const or_solver* s, double cfl);
+
 #ifdef __cplusplus
 }
 #endif

@@ -32,6 +32,22 @@
 //   --gpu 1        (built as ref_driver_gpu only) step with GpuTimeIntegrator,
 //                  the shim of dg-parallel_b200/integration, on the reference's
 //                  own cells and CFL steps instead of RungeKuttaTVD3
+//   --lts 1        (built as ref_driver_lts only) local time stepping: the
+//                  cells binned by size as DGAnalysis::sortCellsBySize does
+//                  (DGAnalysis.cc:749-890), the time step of mode 5
+//                  (DGAnalysis.cc:514-593: CFL minimum times 2^(bins-1)) and
+//                  RungeKuttaTVD2adaptive::advanceInTime (TimeIntegrator.cc:
+//                  442-836).  The reference ships the two range helpers that
+//                  integrator calls, TimeIntegrator::assembleVolume(begin, end,
+//                  t) and assembleBoundary(begin, end, t) (TimeIntegrator.cc:
+//                  1438-1487), with their bodies commented out, so its local
+//                  time stepping never assembles a right-hand side and leaves
+//                  the state unchanged.  This build defines them below with the
+//                  bodies of the whole-mesh versions (TimeIntegrator.cc:
+//                  1332-1412) restricted to the range, and links them ahead of
+//                  TimeIntegrator.cc compiled without inlining (oracle/Makefile).
+//   --bins FILE    (with --lts) per cell in file order: bin, role (0 inner,
+//                  1 large on an interface, 2 small on an interface).
 //   --bench N      time N steps (after --warmup W untimed ones) (CFL dt + RungeKuttaTVD3::advanceInTime)
 //                  with --threads workers of the reference pthreads path
 //                  (parallel.cc, chunked as main.cc) and print one "BENCH ..."
@@ -91,9 +107,94 @@ double timeRK = 0;
 
 static const double kPi = 3.14159265358979323846;
 
+#ifdef DGP_REF_LTS
+// The range helpers RungeKuttaTVD2adaptive calls, with the bodies of the
+// whole-mesh versions (TimeIntegrator.cc:1332-1412) on one thread.
+void TimeIntegrator::assembleVolume(const mMesh::iter begin, const mMesh::iter end, double t) {
+  for (mMesh::iter it = begin; it != end; ++it) ((DGCell*)(*it)->getCell())->computeVolumeContribution(t);
+}
+
+void TimeIntegrator::assembleBoundary(const mMesh::iter begin, const mMesh::iter end, double t) {
+  for (mMesh::iter it = begin; it != end; ++it) {
+    DGBoundaryCell* cell = (DGBoundaryCell*)(*it)->getCell();
+    switch (cell->computeBoundaryContributions(t)) {
+      case 0: break;
+      case 1: cell->getLeftCell()->setToZero(t); break;
+      case 2: cell->getRightCell()->setToZero(t); break;
+      default: cell->getLeftCell()->setToZero(t); cell->getRightCell()->setToZero(t); break;
+    }
+  }
+}
+
+// Size bins as DGAnalysis::sortCellsBySize (DGAnalysis.cc:749-890) forms them:
+// bins = ceil(log2(max size / min size)) (the minimum starts at 1.0), bin i
+// holds sizes in (B_{i+1} * 1.0001, B_i * 1.0001] with B_i = max / 2^i; a face
+// whose cells differ by one bin goes to the interface list of the larger bin,
+// its cells leave their bins for the large / small on-interface lists.
+// Returns the number of bins; exits as the reference does when cells are
+// lost or neighbours differ by more than one bin.
+static int ltsSortCells(mDGMesh* mesh, int n) {
+  double maxSize = 0.0, minSize = 1.0;
+  for (mMesh::iter it = mesh->begin(n); it != mesh->end(n); ++it) {
+    double sz = ((DGCell*)(*it)->getCell())->getSize();
+    if (maxSize < sz) maxSize = sz;
+    if (minSize > sz) minSize = sz;
+  }
+  const int nb = (int)ceil(log(maxSize / minSize) / log(2.));
+  mesh->setNbBins(nb);
+  std::vector<double> B(nb + 1);
+  B[0] = maxSize;
+  if (nb > 1) {
+    for (int i = 1; i <= nb; ++i) B[i] = B[i - 1] * 0.5;
+    for (mMesh::iter it = mesh->begin(n); it != mesh->end(n); ++it) {
+      DGCell* cell = (DGCell*)(*it)->getCell();
+      double sz = cell->getSize();
+      for (int i = 1; i <= nb; ++i)
+        if (sz <= B[i - 1] * 1.0001 && sz > B[i] * 1.0001) {
+          mesh->addToBin(i - 1, *it);
+          cell->setBinNb(i - 1);
+        }
+    }
+  }
+  for (mMesh::iter it = mesh->begin(n - 1); it != mesh->end(n - 1); ++it) {
+    DGBoundaryCell* bc = (DGBoundaryCell*)(*it)->getCell();
+    mEntity* left = bc->getLeft();
+    mEntity* right = bc->getRight();
+    int lb = ((DGCell*)left->getCell())->getBinNb();
+    int rb = right ? ((DGCell*)right->getCell())->getBinNb() : 0;
+    if (lb == rb || !right) {
+      mesh->addToBin(lb, *it);
+    } else if (lb - rb == 1 || rb - lb == 1) {
+      mesh->addToInterfaceBin(lb < rb ? lb : rb, *it);
+      if (lb < rb) {
+        mesh->addToLargeOnInterface(lb, left);
+        mesh->addToSmallOnInterface(lb, right);
+      } else {
+        mesh->addToLargeOnInterface(rb, right);
+        mesh->addToSmallOnInterface(rb, left);
+      }
+      mesh->delFromBin(lb, left);
+      mesh->delFromBin(rb, right);
+    } else {
+      printf("Too big a difference between elements\n");
+      exit(0);
+    }
+  }
+  int total = 0;
+  for (int i = 0; i < nb; ++i)
+    total += mesh->sizeOfBin(i, n) + mesh->sizeOfLargeOnInterface(i, n) + mesh->sizeOfSmallOnInterface(i, n);
+  if (total != mesh->size(n)) {
+    printf("Cells were lost in sorting!");
+    exit(0);
+  }
+  return nb;
+}
+#endif
+
 struct Params {
   std::string mesh, caseName = "gauss", flux = "exact", conn, rhs, state, log, barth, ckptOut, ckptIn;
-  int order = 2, steps = 0, every = 1, threads = 1, bench = 0, warmup = 0, gpu = 0;
+  int order = 2, steps = 0, every = 1, threads = 1, bench = 0, warmup = 0, gpu = 0, lts = 0;
+  std::string bins;
   double cfl = 0.1, tend = -1.0;
   // scalar
   double ax = 1.0, ay = 0.5, az = 0.0, cx = 0.3, cy = 0.3, cz = 0.3, s = 0.01;
@@ -291,6 +392,8 @@ int main(int argc, char** argv) {
     else if (a == "--ckpt-out") P.ckptOut = v;
     else if (a == "--ckpt-in") P.ckptIn = v;
     else if (a == "--gpu") P.gpu = atoi(v);
+    else if (a == "--lts") P.lts = atoi(v);
+    else if (a == "--bins") P.bins = v;
     else if (a == "--ax") P.ax = atof(v);
     else if (a == "--ay") P.ay = atof(v);
     else if (a == "--az") P.az = atof(v);
@@ -417,6 +520,29 @@ int main(int argc, char** argv) {
   }
 
   RungeKuttaTVD3 rk(mesh, 0, m, DOF);
+#ifdef DGP_REF_LTS
+  RungeKuttaTVD2adaptive* lts = 0;
+  int ltsBins = 0;
+  if (P.lts) {
+    ltsBins = ltsSortCells(mesh, dim);
+    lts = new RungeKuttaTVD2adaptive(mesh, 0, m, DOF);
+    if (!P.bins.empty()) {
+      std::vector<int> bin(E, -1), role(E, -1);
+      for (int b = 0; b < ltsBins; ++b) {
+        for (mMesh::iter it = mesh->beginBin(b, dim); it != mesh->endBin(b, dim); ++it)
+          bin[cellIndex(mc, *it)] = b, role[cellIndex(mc, *it)] = 0;
+        for (mMesh::iter it = mesh->beginLargeOnInterface(b, dim); it != mesh->endLargeOnInterface(b, dim); ++it)
+          bin[cellIndex(mc, *it)] = b, role[cellIndex(mc, *it)] = 1;
+        for (mMesh::iter it = mesh->beginSmallOnInterface(b, dim); it != mesh->endSmallOnInterface(b, dim); ++it)
+          bin[cellIndex(mc, *it)] = b + 1, role[cellIndex(mc, *it)] = 2;
+      }
+      FILE* f = fopen(P.bins.c_str(), "w");
+      fprintf(f, "%d %d\n", E, ltsBins);
+      for (int e = 0; e < E; ++e) fprintf(f, "%d %d\n", bin[e], role[e]);
+      fclose(f);
+    }
+  }
+#endif
 
   double TACT = 0.0;
   if (!P.ckptIn.empty()) {
@@ -498,14 +624,19 @@ int main(int argc, char** argv) {
     double dt = 500;
     for (mMesh::iter it = mesh->begin(dim); it != mesh->end(dim); ++it)
       ((DGCell*)(*it)->getCell())->adaptTimeStep(P.cfl, dt);
+#ifdef DGP_REF_LTS
+    if (lts) dt *= pow(2., ltsBins - 1);  // DGAnalysis.cc:590
+#endif
     if (P.tend > 0) {
       int N = (int)ceil((P.tend - TACT) / dt);
       dt = (P.tend - TACT) / N;
     }
     for (mMesh::iter it = mesh->begin(dim); it != mesh->end(dim); ++it)
       ((DGCell*)(*it)->getCell())->setTimeStep(dt);
-#ifdef DGP_GPU_INTEGRATOR
+#if defined(DGP_GPU_INTEGRATOR)
     double resid = gti ? gti->advanceInTime(TACT, dt) : rk.advanceInTime(TACT, dt);
+#elif defined(DGP_REF_LTS)
+    double resid = lts ? lts->advanceInTime(TACT, dt) : rk.advanceInTime(TACT, dt);
 #else
     double resid = rk.advanceInTime(TACT, dt);
 #endif

@@ -14,6 +14,7 @@ case, the mesh file and an .npz with:
 
 The reference run uses one worker thread so that stage times are honoured (see
 oracle/ref_driver.cc).  Usage: python tests/golden/make_golden.py [case ...]
+(the local time stepping cases need ``make -C oracle ref_lts``)
 """
 from __future__ import annotations
 
@@ -121,6 +122,40 @@ def run_ckpt_case(name, kind, margs, dargs, steps):
                         args=np.array(dargs))
 
 
+# Local time stepping fixtures: oracle/_ref/ref_driver_lts (the reference's
+# RungeKuttaTVD2adaptive with the range helpers TimeIntegrator::assembleVolume /
+# assembleBoundary(begin, end, t) given the bodies of their whole-mesh versions,
+# and the size bins of DGAnalysis::sortCellsBySize) on geometrically graded
+# meshes, the mode-5 step (CFL minimum times 2^(bins-1)); stored as ``bins``
+# (bin, role per cell), ``states`` (initial + every step) and ``log``.
+LTS_DRIVER = os.path.join(ROOT, "oracle", "_ref", "ref_driver_lts")
+GRADED = dict(nx=16, ny=16, ratio=1.15)
+GRADED_BOX = dict(nx=14, ny=14, ratio=1.15, x0=0.0, x1=10.0, y0=0.0, y1=10.0)
+LTS_CASES = {
+    "lts_scalar_graded_p2": ("graded", GRADED, ["--case", "gauss", "--order", "2"], 3),
+    "lts_euler_roe_graded_p2": ("graded", GRADED_BOX, ["--case", "vortex", "--flux", "roe", "--order", "2"], 2),
+}
+
+
+def run_lts_case(name, kind, margs, dargs, steps):
+    mesh = meshgen.tri_graded(**margs)
+    msh = os.path.join(HERE, name + ".msh")
+    meshgen.write_msh_v1(mesh, msh)
+    with tempfile.TemporaryDirectory() as td:
+        bins, state, log = (os.path.join(td, f) for f in ("b", "s", "l"))
+        cmd = [LTS_DRIVER, "--mesh", msh, "--lts", "1", "--steps", str(steps), "--cfl", "0.1",
+               "--bins", bins, "--state", state, "--log", log] + dargs
+        subprocess.run(cmd, check=True, capture_output=True)
+        b = np.loadtxt(bins, skiprows=1, dtype=np.int64, ndmin=2)
+        nb = int(open(bins).readline().split()[1])
+        blocks = open(state).read().split("step ")[1:]
+        states = np.array([[list(map(float, ln.split())) for ln in blk.split("\n")[1:] if ln.strip()]
+                           for blk in blocks])
+        lg = np.loadtxt(log, ndmin=2)
+    np.savez_compressed(os.path.join(HERE, name + ".npz"), bins=b, nbins=nb, states=states, log=lg,
+                        args=np.array(dargs), steps=steps)
+
+
 def build_mesh(kind, args):
     return meshgen.tri_square(**args) if kind == "tri" else meshgen.tet_cube(**args)
 
@@ -154,6 +189,11 @@ def main():
         if only and name not in only:
             continue
         run_case(name, kind, margs, dargs, steps)
+        print("wrote", name)
+    for name, (kind, margs, dargs, steps) in LTS_CASES.items():
+        if only and name not in only:
+            continue
+        run_lts_case(name, kind, margs, dargs, steps)
         print("wrote", name)
     for name, (kind, margs, dargs, steps) in CKPT_CASES.items():
         if only and name not in only:

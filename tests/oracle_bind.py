@@ -59,6 +59,13 @@ def lib():
     L.or_set_p0_fallback.argtypes = [P, I]
     L.or_bad_cells.argtypes = [P, pU8]
     L.or_triggers.argtypes = [P, pU8]
+    L.or_lts_setup.argtypes = [P]
+    L.or_lts_setup.restype = I
+    L.or_lts_bins.argtypes = [P, pI, pI]
+    L.or_lts_step.argtypes = [P, D, D]
+    L.or_lts_step.restype = D
+    L.or_lts_dt.argtypes = [P, D]
+    L.or_lts_dt.restype = D
     L.or_glibc_rand_first.argtypes = [ctypes.c_uint]
     L.or_glibc_rand_first.restype = ctypes.c_uint
     _lib = L
@@ -145,6 +152,23 @@ class Oracle:
         out = np.zeros(self.ncells, dtype=np.uint8)
         lib().or_bad_cells(self.h, out.ctypes.data_as(ctypes.POINTER(ctypes.c_uint8)))
         return out
+
+    def lts_setup(self):
+        """Size bins of DGAnalysis::sortCellsBySize; number of bins or < 0."""
+        return lib().or_lts_setup(self.h)
+
+    def lts_bins(self):
+        bins = np.zeros(self.ncells, dtype=np.int32)
+        role = np.zeros(self.ncells, dtype=np.int32)
+        pI = ctypes.POINTER(ctypes.c_int)
+        lib().or_lts_bins(self.h, bins.ctypes.data_as(pI), role.ctypes.data_as(pI))
+        return bins, role
+
+    def lts_step(self, t, dt):
+        return lib().or_lts_step(self.h, t, dt)
+
+    def lts_dt(self, cfl):
+        return lib().or_lts_dt(self.h, cfl)
 
     def close(self):
         if self.h:
