@@ -708,6 +708,16 @@ def lts_bench(n=256, ratio=1.0098, steps=16):
            "ssprk3_same_mesh": {"steps": k_rk, "dt": dt_rk, "ms_per_step": sec_rk / k_rk * 1e3,
                                 "seconds_to_same_t": sec_rk, "l2_density_vs_exact": rk.l2_error(t_rk, 0)},
            "seconds_to_same_t": sec, "speedup_over_ssprk3": sec_rk / sec}
+    # roofline by the per-element-stage formula, one element-stage per cell
+    # sub-stage (the accumulator, copy slot and saved state the integrator adds
+    # are not counted)
+    peaks, peak_src = load_peaks()
+    hbm = peaks.get("hbm_gbs")
+    sb = stage_formula_bytes(E, mesh.nfaces, M, NP, 2) / E * (units / (M * NP))
+    ach = sb / (sec / k) / 1e9
+    out["roofline"] = {"bound": "hbm", "basis": "per-element-stage formula x cell sub-stages per step",
+                       "algorithmic_bytes_per_step": sb, "achieved": ach, "peak": hbm, "unit": "GB/s",
+                       "frac": ach / hbm, "peak_source": peak_src}
     rk.close()
     s.close()
     if os.path.exists(REF_DRIVER_LTS):

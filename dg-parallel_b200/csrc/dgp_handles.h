@@ -4,7 +4,9 @@
 
 #include <cuda_runtime.h>
 
+#include <map>
 #include <string>
+#include <utility>
 #include <vector>
 
 #include "../../include/dgp.h"
@@ -78,7 +80,8 @@ struct LtsState {
   double *c1 = nullptr, *save = nullptr, *racc = nullptr;  // copy slot, u_n, RHS accumulator
   std::vector<int> goff, gn;         // group (g, b) at 3 * b + g: offset and length
   std::vector<int> foff, fn;         // face class c: faces
-  std::vector<int> aoff, an;         // face class c: the cells that touch its faces
+  std::map<unsigned, std::pair<int, int>> lift;  // class set (bit c) -> offset, length of
+                                                 // the cells touching its faces
 };
 
 struct dgp_solver_s {

@@ -319,7 +319,7 @@ template <class K, bool RERUN, bool ENS>
 __device__ __forceinline__ void face_finish(const StageArgs<typename K::T>& a, int f, int q, int eL, int eR,
                                             int inst, int lfL, int lfR, int qR, const typename K::T (&n)[K::DIM],
                                             typename K::T jw, const typename K::T (&UL)[K::M],
-                                            const typename K::T (&UR)[K::M]) {
+                                            const typename K::T (&UR)[K::M], double tfac = -1.0) {
   using T = typename K::T;
   constexpr int M = K::M, NP = K::NP, NQF = K::NQF, DIM = K::DIM, MNP = K::MNP;
   T flux[M];
@@ -348,7 +348,8 @@ __device__ __forceinline__ void face_finish(const StageArgs<typename K::T>& a, i
       const double time = __fma_rn(a.stage_time_factor, c->dt, c->t);
       boundary_flux<K::LAW, K::FLUX, DIM, T>(a.laws[inst], a.mesh.bbid[b], n, x, time, UL, flux);
     } else {
-      const double time = __fma_rn(a.stage_time_factor, a.ctl->dt, a.ctl->t);
+      // tfac >= 0: the caller's time factor (local time stepping's 2^-k)
+      const double time = __fma_rn(tfac < 0.0 ? a.stage_time_factor : tfac, a.ctl->dt, a.ctl->t);
       boundary_flux<K::LAW, K::FLUX, DIM, T>(a.law, a.mesh.bbid[b], n, x, time, UL, flux);
     }
   }
@@ -371,7 +372,7 @@ __device__ __forceinline__ void face_finish(const StageArgs<typename K::T>& a, i
 template <class K, bool RERUN, bool ENS>
 __device__ __forceinline__ void face_point(const StageArgs<typename K::T>& a, int f, int q,
                                            const typename K::T* s_phif, const typename K::T* s_fqw,
-                                           const int* s_qmap) {
+                                           const int* s_qmap, double tfac = -1.0) {
   using T = typename K::T;
   constexpr int M = K::M, NP = K::NP, NQF = K::NQF, DIM = K::DIM, MNP = K::MNP;
   const int eL = a.mesh.fel[2 * f], eR = a.mesh.fel[2 * f + 1];
@@ -399,7 +400,7 @@ __device__ __forceinline__ void face_point(const StageArgs<typename K::T>& a, in
     else
       load_trace<K>(a.tr, eR, lfR * NQF + qR, UR);
   }
-  face_finish<K, RERUN, ENS>(a, f, q, eL, eR, inst, lfL, lfR, qR, n, jw, UL, UR);
+  face_finish<K, RERUN, ENS>(a, f, q, eL, eR, inst, lfL, lfR, qR, n, jw, UL, UR, tfac);
 }
 
 template <class K>

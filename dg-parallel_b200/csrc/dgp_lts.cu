@@ -14,6 +14,8 @@
 #include <algorithm>
 #include <cmath>
 #include <string>
+#include <tuple>
+#include <utility>
 #include <vector>
 
 #include "../../include/dgp.h"
@@ -34,34 +36,107 @@ __global__ void lts_advance_kernel(TimeCtl* c) {
   c->resid = 0.0;
 }
 
+// The integrator's calls, batched: between two coefficient updates all
+// assembly calls commute (they read the state and add to accumulators), and
+// between two assembly calls the updates touch disjoint cell groups, so a run
+// of assembly calls is one volume launch (a segment per group), one face launch
+// (a segment per face class, each with its boundary time) and one lift over
+// the cells touching those classes, and a run of updates is one update launch
+// (a segment per group, each with its operation and dt).  A group or class
+// that repeats inside a run starts a new launch.
 struct Seq {
+  enum Mode { LAUNCH, COUNT, PLAN };
   dgp_solver s;
-  bool dry;
+  Mode mode;
+  std::vector<unsigned>* masks = nullptr;  // PLAN: the class sets of the lifts
   int launches = 0;
+  std::vector<int> vg;                          // pending volume groups (3 b + g)
+  std::vector<std::pair<int, int>> fc;          // pending face classes and their k
+  std::vector<std::tuple<int, int, int>> up;    // pending updates: group, op, k
   const LtsState& L() const { return s->lts; }
-  double fac(int k) const { return std::ldexp(1.0, -k); }
+  static double fac(int k) { return std::ldexp(1.0, -k); }
   // assembleVolume over group (g, b)
   void vol(int g, int b) {
-    const int i = 3 * b + g, n = L().gn[i];
-    if (n == 0) return;
-    ++launches;
-    if (!dry) s->ops.lts_vol(s->b, L().lists + L().goff[i], n, L().racc, s->stream);
+    flush_updates();
+    const int i = 3 * b + g;
+    if (L().gn[i] == 0) return;
+    if (std::find(vg.begin(), vg.end(), i) != vg.end() || static_cast<int>(vg.size()) == dgp::kLtsMaxSegs)
+      flush_assembly();
+    vg.push_back(i);
   }
   // assembleBoundary over face class c at t + DT * 2^-k
   void bnd(int c, int k) {
+    flush_updates();
     if (L().fn[c] == 0) return;
-    launches += 2;
-    if (dry) return;
-    s->ops.lts_face(s->b, L().lists + L().foff[c], L().fn[c], fac(k), s->stream);
-    s->ops.lts_lift(s->b, L().lists + L().aoff[c], L().an[c], L().cface, L().fcls, c, -1, L().racc, s->stream);
+    bool again = static_cast<int>(fc.size()) == dgp::kLtsMaxSegs;
+    for (const auto& p : fc) again |= p.first == c;
+    if (again) flush_assembly();
+    fc.push_back({c, k});
   }
   // a coefficient loop over group (g, b) with dt = DT * 2^-k
   void upd(int g, int b, int op, int k) {
-    const int i = 3 * b + g, n = L().gn[i];
-    if (n == 0) return;
+    flush_assembly();
+    const int i = 3 * b + g;
+    if (L().gn[i] == 0) return;
+    bool again = static_cast<int>(up.size()) == dgp::kLtsMaxSegs;
+    for (const auto& u : up) again |= std::get<0>(u) == i;
+    if (again) flush_updates();
+    up.push_back({i, op, k});
+  }
+  void flush_assembly() {
+    if (!vg.empty()) {
+      ++launches;
+      if (mode == LAUNCH) {
+        dgp::LtsSegs S{};
+        S.nseg = static_cast<int>(vg.size());
+        for (int j = 0; j < S.nseg; ++j) {
+          S.off[j] = L().goff[vg[j]];
+          S.cnt[j] = L().gn[vg[j]];
+        }
+        s->ops.lts_vol(s->b, L().lists, S, L().racc, s->stream);
+      }
+      vg.clear();
+    }
+    if (!fc.empty()) {
+      launches += 2;
+      unsigned mask = 0;
+      for (const auto& p : fc) mask |= 1u << p.first;
+      if (mode == PLAN) masks->push_back(mask);
+      if (mode == LAUNCH) {
+        dgp::LtsSegs S{};
+        S.nseg = static_cast<int>(fc.size());
+        for (int j = 0; j < S.nseg; ++j) {
+          S.off[j] = L().foff[fc[j].first];
+          S.cnt[j] = L().fn[fc[j].first];
+          S.fac[j] = fac(fc[j].second);
+        }
+        s->ops.lts_face(s->b, L().lists, S, s->stream);
+        const auto& u = L().lift.at(mask);
+        s->ops.lts_lift(s->b, L().lists + u.first, u.second, L().cface, L().fcls, mask, L().racc, s->stream);
+      }
+      fc.clear();
+    }
+  }
+  void flush_updates() {
+    if (up.empty()) return;
     ++launches;
-    if (!dry)
-      s->ops.lts_update(s->b, L().lists + L().goff[i], n, op, fac(k), L().c1, L().save, L().racc, s->stream);
+    if (mode == LAUNCH) {
+      dgp::LtsSegs S{};
+      S.nseg = static_cast<int>(up.size());
+      for (int j = 0; j < S.nseg; ++j) {
+        const int i = std::get<0>(up[j]);
+        S.off[j] = L().goff[i];
+        S.cnt[j] = L().gn[i];
+        S.op[j] = std::get<1>(up[j]);
+        S.fac[j] = fac(std::get<2>(up[j]));
+      }
+      s->ops.lts_update(s->b, L().lists, S, L().c1, L().save, L().racc, s->stream);
+    }
+    up.clear();
+  }
+  void finish() {
+    flush_assembly();
+    flush_updates();
   }
   // RungeKuttaTVD2adaptive::firstStage (TimeIntegrator.cc:442-591)
   void first(int from, int to) {
@@ -132,8 +207,9 @@ struct Seq {
 namespace dgp {
 
 int launch_lts_step(dgp_solver s, bool next_dt, bool dry) {
-  Seq q{s, dry};
+  Seq q{s, dry ? Seq::COUNT : Seq::LAUNCH};
   q.step();
+  q.finish();
   q.launches += 1 + (next_dt ? 1 : 0);
   if (!dry) {
     lts_advance_kernel<<<1, 1, 0, s->stream>>>(s->b.ctl);
@@ -195,7 +271,7 @@ static int lts_setup(dgp_solver s, int* nbins) {
       return fail(DGP_ERR_INVALID, "local time stepping: neighbouring cells more than one size bin apart");
     }
   }
-  // lists: groups (3 per bin), face classes (2 per bin), cells touching each class
+  // lists: groups (3 per bin), face classes (2 per bin)
   std::vector<int> all;
   L.goff.assign(3 * nb, 0);
   L.gn.assign(3 * nb, 0);
@@ -206,25 +282,38 @@ static int lts_setup(dgp_solver s, int* nbins) {
         if (role[e] == g && bin[e] == (g == 2 ? b + 1 : b)) all.push_back(e);
       L.gn[3 * b + g] = static_cast<int>(all.size()) - L.goff[3 * b + g];
     }
+  L.nb = nb;
   L.foff.assign(2 * nb, 0);
   L.fn.assign(2 * nb, 0);
-  L.aoff.assign(2 * nb, 0);
-  L.an.assign(2 * nb, 0);
   for (int c = 0; c < 2 * nb; ++c) {
     L.foff[c] = static_cast<int>(all.size());
-    std::vector<int> touch;
     for (int f = 0; f < F; ++f)
-      if (fcls[f] == c) {
-        all.push_back(f);
-        touch.push_back(fel[2 * f]);
-        if (fel[2 * f + 1] >= 0) touch.push_back(fel[2 * f + 1]);
-      }
+      if (fcls[f] == c) all.push_back(f);
     L.fn[c] = static_cast<int>(all.size()) - L.foff[c];
-    std::sort(touch.begin(), touch.end());
-    touch.erase(std::unique(touch.begin(), touch.end()), touch.end());
-    L.aoff[c] = static_cast<int>(all.size());
-    all.insert(all.end(), touch.begin(), touch.end());
-    L.an[c] = static_cast<int>(touch.size());
+  }
+  // the cells each batched lift covers: every cell touching a face of one of
+  // the classes of the run (found by walking the step once without launches)
+  {
+    std::vector<unsigned> masks;
+    Seq plan{s, Seq::PLAN};
+    plan.masks = &masks;
+    plan.step();
+    plan.finish();
+    std::sort(masks.begin(), masks.end());
+    masks.erase(std::unique(masks.begin(), masks.end()), masks.end());
+    L.lift.clear();
+    for (unsigned mask : masks) {
+      std::vector<int> touch;
+      for (int f = 0; f < F; ++f)
+        if ((mask >> fcls[f]) & 1u) {
+          touch.push_back(fel[2 * f]);
+          if (fel[2 * f + 1] >= 0) touch.push_back(fel[2 * f + 1]);
+        }
+      std::sort(touch.begin(), touch.end());
+      touch.erase(std::unique(touch.begin(), touch.end()), touch.end());
+      L.lift[mask] = {static_cast<int>(all.size()), static_cast<int>(touch.size())};
+      all.insert(all.end(), touch.begin(), touch.end());
+    }
   }
   if (!L.lists) {  // first setup: device buffers live as long as the solver
     const size_t n = s->state_count();
@@ -239,7 +328,6 @@ static int lts_setup(dgp_solver s, int* nbins) {
   }
   // the right-hand sides start at zero (DGCell::ZeroRHS after the projection)
   DGP_CUDA(cudaMemset(L.racc, 0, s->state_count() * sizeof(double)));
-  L.nb = nb;
   L.bin = bin;
   L.role = role;
   if (nbins) *nbins = nb;

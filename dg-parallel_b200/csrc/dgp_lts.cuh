@@ -11,11 +11,13 @@
 //   lts_vol_kernel   volume term of the listed cells, added to the accumulator;
 //   lts_face_kernel  the face kernel's face-point flux over a face list, into
 //                    the face slots of both sides;
-//   lts_lift_kernel  the slots of one or two face classes lifted into the
+//   lts_lift_kernel  the slots of a set of face classes lifted into the
 //                    accumulators of the cells that touch them (per cell, its
 //                    local faces in order: no atomics);
 // and every coefficient update is lts_update_kernel with one of the
 // integrator's operations, which also refreshes the row's face-point traces.
+// The cell kernels stage CPB listed cells per CTA in shared memory (LtsTile),
+// so that their global loads and stores are element-parallel and coalesced.
 // Every kernel returns at once when the run is done (ctl->done), so that a
 // step captured in a CUDA graph turns into no-ops past the end.
 #pragma once
@@ -38,26 +40,87 @@ enum LtsUpdateOp : int {
   LTS_FINAL_RESET = 8,   // c = c1; r = 0                          (:777)
 };
 
-// volume term of the listed cells: one thread per (cell, field) row,
-// r[j][k] += sum_q F_j(U_q) . J^-T grad phi_k |J| w_q
+// A launch covers several lists (segments): segment i is lists[off[i] ..
+// off[i] + cnt[i]), with its own update operation and 2^-k factor, and owns
+// CTAs block0[i] .. block0[i + 1] - 1.  Segments of one launch never share a
+// cell (cell kernels) or a face (face kernel).
+constexpr int kLtsMaxSegs = 32;
+struct LtsSegs {
+  int nseg;
+  int off[kLtsMaxSegs];
+  int cnt[kLtsMaxSegs];
+  int op[kLtsMaxSegs];
+  double fac[kLtsMaxSegs];
+  int block0[kLtsMaxSegs + 1];
+};
+
+// the segment of CTA blk and the CTA's index inside it
+__device__ __forceinline__ int lts_segment(const LtsSegs& S, int blk, int& local) {
+  int i = 0;
+  while (i + 1 < S.nseg && blk >= S.block0[i + 1]) ++i;
+  local = blk - S.block0[i];
+  return i;
+}
+
+// tile shape of the cell kernels: CPB listed cells per 128-thread CTA (one
+// (cell, field) row per thread at most), their coefficients and the volume
+// kernel's flux rows in at most 40 KB of shared memory
+template <class K>
+struct LtsTile {
+  static constexpr int M = K::M, MNP = K::MNP, KV = K::KV;
+  static constexpr int BYTES_PER_CELL = 8 * (MNP + M * KV);
+  static constexpr int BY_ROWS = 128 / M;
+  static constexpr int BY_SMEM = (40 * 1024) / BYTES_PER_CELL;
+  static constexpr int CPB = BY_ROWS < BY_SMEM ? BY_ROWS : (BY_SMEM < 1 ? 1 : BY_SMEM);
+  static int grid(int n) { return (n + CPB - 1) / CPB; }
+};
+
+// the tile's cells: s_e[i] = list[c0 + i], i < nc, for the CTA's tile `blk`
+template <int CPB>
+__device__ __forceinline__ int lts_tile_cells(const int* __restrict__ list, int n, int blk, int* s_e) {
+  const int c0 = blk * CPB;
+  const int nc = n - c0 < CPB ? n - c0 : CPB;
+  for (int i = threadIdx.x; i < nc; i += blockDim.x) s_e[i] = list[c0 + i];
+  __syncthreads();
+  return nc;
+}
+
+// racc[cell] += s_c[cell] for the tile's cells, element-parallel
+template <int MNP>
+__device__ __forceinline__ void lts_add_rows(const int* s_e, int nc, const double* s_c, double* racc) {
+  for (int x = threadIdx.x; x < nc * MNP; x += blockDim.x) {
+    const int i = x / MNP;
+    racc[(size_t)s_e[i] * MNP + (x - i * MNP)] += s_c[x];
+  }
+}
+
+// volume term of the listed cells, r[j][k] += sum_q F_j(U_q) . J^-T grad phi_k
+// |J| w_q: one thread per (cell, quadrature point) evaluates the flux once for
+// all fields into the rows G[(cell, j)][(q, r)]; one thread per (cell, field)
+// row contracts its G row with grad phi
 template <class K>
 __global__ void __launch_bounds__(128) lts_vol_kernel(const __grid_constant__ StageArgs<double> a,
-                                                       const int* __restrict__ list, int n,
+                                                       const int* __restrict__ lists,
+                                                       const __grid_constant__ LtsSegs S,
                                                        double* __restrict__ racc) {
-  constexpr int M = K::M, NP = K::NP, NQ = K::NQ, DIM = K::DIM, MNP = K::MNP;
+  constexpr int M = K::M, NP = K::NP, NQ = K::NQ, DIM = K::DIM, MNP = K::MNP, KV = K::KV;
+  constexpr int CPB = LtsTile<K>::CPB;
+  __shared__ double s_c[CPB * MNP];
+  __shared__ double s_g[CPB * M * KV];
+  __shared__ int s_e[CPB];
   if (a.gctl->done) return;
-  const int gid = blockIdx.x * blockDim.x + threadIdx.x;
-  if (gid >= n * M) return;
-  const int e = list[gid / M], j = gid - (gid / M) * M;
-  const double* c = a.C + (size_t)e * MNP;
-  double J[DIM * DIM];
-#pragma unroll
-  for (int i = 0; i < DIM * DIM; ++i) J[i] = a.mesh.jinv[(size_t)e * DIM * DIM + i];
-  const double det = a.mesh.detjd[e];
-  double acc[NP];
-#pragma unroll
-  for (int k = 0; k < NP; ++k) acc[k] = 0.0;
-  for (int q = 0; q < NQ; ++q) {
+  const int tid = threadIdx.x;
+  int blk;
+  const int sg = lts_segment(S, blockIdx.x, blk);
+  const int nc = lts_tile_cells<CPB>(lists + S.off[sg], S.cnt[sg], blk, s_e);
+  for (int x = tid; x < nc * MNP; x += 128) {
+    const int i = x / MNP;
+    s_c[x] = a.C[(size_t)s_e[i] * MNP + (x - i * MNP)];
+  }
+  __syncthreads();
+  for (int x = tid; x < nc * NQ; x += 128) {
+    const int i = x / NQ, q = x - i * NQ, e = s_e[i];
+    const double* c = s_c + i * MNP;
     double U[M];
 #pragma unroll
     for (int jj = 0; jj < M; ++jj) {
@@ -66,30 +129,47 @@ __global__ void __launch_bounds__(128) lts_vol_kernel(const __grid_constant__ St
       for (int k = 0; k < NP; ++k) u += a.tab.phi[q * NP + k] * c[jj * NP + k];
       U[jj] = u;
     }
-    if (j == 0 && !is_physical<K::LAW, double>(a.law, U)) flag_nonphysical(a.status, e);
+    if (!is_physical<K::LAW, double>(a.law, U)) flag_nonphysical(a.status, e);
     double F[M][DIM];
     volume_flux<K::LAW, DIM, double>(a.law, U, F);
-    const double jw = det * a.tab.qw[q];
+    double J[DIM * DIM];
 #pragma unroll
-    for (int r = 0; r < DIM; ++r) {
-      double g = 0.0;
+    for (int t = 0; t < DIM * DIM; ++t) J[t] = a.mesh.jinv[(size_t)e * DIM * DIM + t];
+    const double jw = a.mesh.detjd[e] * a.tab.qw[q];
 #pragma unroll
-      for (int i = 0; i < DIM; ++i) g += F[j][i] * J[i * DIM + r];
-      g *= jw;
+    for (int j = 0; j < M; ++j)
 #pragma unroll
-      for (int k = 0; k < NP; ++k) acc[k] += g * a.tab.dphi[(q * DIM + r) * NP + k];
-    }
+      for (int r = 0; r < DIM; ++r) {
+        double g = 0.0;
+#pragma unroll
+        for (int t = 0; t < DIM; ++t) g += F[j][t] * J[t * DIM + r];
+        s_g[(i * M + j) * KV + q * DIM + r] = g * jw;
+      }
   }
-  double* ro = racc + (size_t)e * MNP + j * NP;
+  __syncthreads();
+  for (int row = tid; row < nc * M; row += 128) {
+    double acc[NP];
 #pragma unroll
-  for (int k = 0; k < NP; ++k) ro[k] += acc[k];
+    for (int k = 0; k < NP; ++k) acc[k] = 0.0;
+    const double* g = s_g + row * KV;
+    for (int kk = 0; kk < KV; ++kk) {
+      const double gv = g[kk];
+#pragma unroll
+      for (int k = 0; k < NP; ++k) acc[k] += gv * a.tab.dphi[kk * NP + k];
+    }
+#pragma unroll
+    for (int k = 0; k < NP; ++k) s_c[row * NP + k] = acc[k];  // row < nc * M: own row only
+  }
+  __syncthreads();
+  lts_add_rows<MNP>(s_e, nc, s_c, racc);
 }
 
-// the face kernel over a face list: one thread per (listed face, face point);
-// the boundary data time is ctl->t + stage_time_factor * ctl->dt
+// the face kernel over face lists: one thread per (listed face, face point);
+// the boundary data time of segment i is ctl->t + fac[i] * ctl->dt
 template <class K>
 __global__ void __launch_bounds__(K::FACE_BLOCK) lts_face_kernel(const __grid_constant__ StageArgs<double> a,
-                                                                 const int* __restrict__ flist, int n) {
+                                                                 const int* __restrict__ lists,
+                                                                 const __grid_constant__ LtsSegs S) {
   if (a.gctl->done) return;
   __shared__ double s_fqw[K::NQF];
   __shared__ int s_qmap[K::NPERM * K::NQF];
@@ -97,128 +177,145 @@ __global__ void __launch_bounds__(K::FACE_BLOCK) lts_face_kernel(const __grid_co
   for (int i = tid; i < K::NQF; i += blockDim.x) s_fqw[i] = a.tab.fqw[i];
   for (int i = tid; i < K::NPERM * K::NQF; i += blockDim.x) s_qmap[i] = a.tab.qmap[i];
   __syncthreads();
+  int blk;
+  const int sg = lts_segment(S, blockIdx.x, blk);
   const int fl = tid / K::NQF, q = tid - (tid / K::NQF) * K::NQF;
-  const int i = blockIdx.x * K::FPB + fl;
-  if (fl >= K::FPB || i >= n) return;
-  face_point<K, false, false>(a, flist[i], q, nullptr, s_fqw, s_qmap);
+  const int i = blk * K::FPB + fl;
+  if (fl >= K::FPB || i >= S.cnt[sg]) return;
+  face_point<K, false, false>(a, lists[S.off[sg] + i], q, nullptr, s_fqw, s_qmap, S.fac[sg]);
 }
 
-// lift of the face slots of classes clsA / clsB into the accumulators of the
-// listed cells: one thread per (cell, field) row, local faces in order
+// lift of the face slots of the classes in `mask` (bit c: class c) into the
+// accumulators of the listed cells (every cell touching one of them, once):
+// one thread per (cell, field) row over the cell's local faces in order
+// (slots read row-coalesced), the sums added element-parallel
 template <class K>
 __global__ void __launch_bounds__(128) lts_lift_kernel(const __grid_constant__ StageArgs<double> a,
                                                         const int* __restrict__ list, int n,
                                                         const int* __restrict__ cface,
-                                                        const int* __restrict__ fcls, int clsA, int clsB,
+                                                        const int* __restrict__ fcls, unsigned mask,
                                                         double* __restrict__ racc) {
   constexpr int M = K::M, NP = K::NP, NQF = K::NQF, NLF = K::NLF, MNP = K::MNP;
+  constexpr int CPB = LtsTile<K>::CPB;
+  __shared__ double s_c[CPB * MNP];
+  __shared__ int s_e[CPB];
   if (a.gctl->done) return;
-  const int gid = blockIdx.x * blockDim.x + threadIdx.x;
-  if (gid >= n * M) return;
-  const int e = list[gid / M], j = gid - (gid / M) * M;
-  double acc[NP];
+  const int nc = lts_tile_cells<CPB>(list, n, blockIdx.x, s_e);
+  for (int row = threadIdx.x; row < nc * M; row += 128) {
+    const int i = row / M, j = row - i * M, e = s_e[i];
+    double acc[NP];
 #pragma unroll
-  for (int k = 0; k < NP; ++k) acc[k] = 0.0;
-  for (int lf = 0; lf < NLF; ++lf) {
-    const int f = cface[(size_t)e * NLF + lf];
-    if (f < 0) continue;
-    const int c = fcls[f];
-    if (c != clsA && c != clsB) continue;
-    for (int q = 0; q < NQF; ++q) {
-      const int s = lf * NQF + q;
-      const double sv = a.slots[slot_index<K>(e, s, j)];
+    for (int k = 0; k < NP; ++k) acc[k] = 0.0;
+    for (int lf = 0; lf < NLF; ++lf) {
+      const int f = cface[(size_t)e * NLF + lf];
+      if (f < 0) continue;
+      if (!((mask >> fcls[f]) & 1u)) continue;
+      for (int q = 0; q < NQF; ++q) {
+        const int s = lf * NQF + q;
+        const double sv = a.slots[slot_index<K>(e, s, j)];
 #pragma unroll
-      for (int k = 0; k < NP; ++k) acc[k] += sv * a.tab.phif[s * NP + k];
+        for (int k = 0; k < NP; ++k) acc[k] += sv * a.tab.phif[s * NP + k];
+      }
     }
-  }
-  double* ro = racc + (size_t)e * MNP + j * NP;
 #pragma unroll
-  for (int k = 0; k < NP; ++k) ro[k] += acc[k];
+    for (int k = 0; k < NP; ++k) s_c[row * NP + k] = acc[k];
+  }
+  __syncthreads();
+  lts_add_rows<MNP>(s_e, nc, s_c, racc);
 }
 
-// one of the integrator's coefficient operations on the listed cells, one
-// thread per (cell, field) row, each product, quotient and sum rounded once
-// in the reference's order (no contraction); then the row's face-point traces
+// one of the integrator's coefficient operations on the listed cells,
+// element-parallel (every product, quotient and sum rounded once, in the
+// reference's order: no contraction); then one thread per (cell, field) row
+// writes the row's face-point traces from the new coefficients
 template <class K>
 __global__ void __launch_bounds__(128) lts_update_kernel(const __grid_constant__ StageArgs<double> a,
-                                                          const int* __restrict__ list, int n, int op,
-                                                          double dt_factor, double* __restrict__ c1,
-                                                          double* __restrict__ save, double* __restrict__ racc) {
+                                                          const int* __restrict__ lists,
+                                                          const __grid_constant__ LtsSegs S,
+                                                          double* __restrict__ c1, double* __restrict__ save,
+                                                          double* __restrict__ racc) {
   constexpr int M = K::M, NP = K::NP, NS = K::NS, MNP = K::MNP;
+  constexpr int CPB = LtsTile<K>::CPB;
+  __shared__ double s_c[CPB * MNP];
+  __shared__ int s_e[CPB];
   if (a.gctl->done) return;
-  const int gid = blockIdx.x * blockDim.x + threadIdx.x;
-  if (gid >= n * M) return;
-  const int e = list[gid / M], j = gid - (gid / M) * M;
-  const double dt = __dmul_rn(a.ctl->dt, dt_factor);  // dt_factor = 2^-k: exact
-  const double det = a.mesh.detjd[e];
-  const size_t base = (size_t)e * MNP + j * NP;
-  double* c = a.Cout + base;
-  double* cc = c1 + base;
-  double* sv = save + base;
-  double* r = racc + base;
-  double o[NP];
-#pragma unroll
-  for (int k = 0; k < NP; ++k) {
-    double x = c[k];
+  const int tid = threadIdx.x;
+  int blk;
+  const int sg = lts_segment(S, blockIdx.x, blk);
+  const int nc = lts_tile_cells<CPB>(lists + S.off[sg], S.cnt[sg], blk, s_e);
+  const int op = S.op[sg];
+  const double dt = __dmul_rn(a.ctl->dt, S.fac[sg]);  // fac = 2^-k: exact
+  for (int xi = tid; xi < nc * MNP; xi += 128) {
+    const int i = xi / MNP, e = s_e[i];
+    const size_t g = (size_t)e * MNP + (xi - i * MNP);
+    const double det = a.mesh.detjd[e];
+    double x = a.Cout[g];
     switch (op) {
       case LTS_EULER_IN:
-        sv[k] = x;
-        x = __dadd_rn(x, __dmul_rn(__ddiv_rn(r[k], det), dt));
-        r[k] = 0.0;
+        save[g] = x;
+        x = __dadd_rn(x, __dmul_rn(__ddiv_rn(racc[g], det), dt));
+        racc[g] = 0.0;
         break;
       case LTS_TWO_HALF: {
-        sv[k] = x;
-        const double inc = __ddiv_rn(__dmul_rn(r[k], dt), det);
+        save[g] = x;
+        const double inc = __ddiv_rn(__dmul_rn(racc[g], dt), det);
         x = __dadd_rn(x, inc);
-        cc[k] = x;
+        c1[g] = x;
         x = __dadd_rn(x, inc);
-        r[k] = 0.0;
+        racc[g] = 0.0;
         break;
       }
       case LTS_EULER:
-        sv[k] = x;
-        x = __dadd_rn(x, __ddiv_rn(__dmul_rn(r[k], dt), det));
-        r[k] = 0.0;
+        save[g] = x;
+        x = __dadd_rn(x, __ddiv_rn(__dmul_rn(racc[g], dt), det));
+        racc[g] = 0.0;
         break;
       case LTS_SECOND:
       case LTS_SECOND_SWAP: {
-        const double xn = __dmul_rn(__dadd_rn(__dadd_rn(x, __ddiv_rn(__dmul_rn(r[k], dt), det)), sv[k]), 0.5);
+        const double xn =
+            __dmul_rn(__dadd_rn(__dadd_rn(x, __ddiv_rn(__dmul_rn(racc[g], dt), det)), save[g]), 0.5);
         if (op == LTS_SECOND) {
           x = xn;
-          r[k] = 0.0;
+          racc[g] = 0.0;
         } else {
-          x = cc[k];
-          cc[k] = xn;
+          x = c1[g];
+          c1[g] = xn;
         }
         break;
       }
       case LTS_COPYBACK_ZERO:
       case LTS_FINAL_RESET:
-        x = cc[k];
-        r[k] = 0.0;
+        x = c1[g];
+        racc[g] = 0.0;
         break;
       case LTS_LI_HALF: {
-        const double s0 = sv[k], x1 = cc[k];
+        const double s0 = save[g], x1 = c1[g];
         const double xn = __dadd_rn(__dadd_rn(s0, __dsub_rn(x, s0)),
                                     __dmul_rn(0.25, __dadd_rn(__dsub_rn(x1, __dmul_rn(2.0, x)), s0)));
-        sv[k] = __dadd_rn(xn, __dmul_rn(0.5, __dsub_rn(x1, s0)));
+        save[g] = __dadd_rn(xn, __dmul_rn(0.5, __dsub_rn(x1, s0)));
         x = xn;
         break;
       }
       default:  // LTS_RESTORE
-        x = sv[k];
+        x = save[g];
         break;
     }
-    c[k] = x;
-    o[k] = x;
+    a.Cout[g] = x;
+    s_c[xi] = x;
   }
-  // face-point traces of the new row for the face kernel
-#pragma unroll 4
-  for (int s = 0; s < NS; ++s) {
-    double t = 0.0;
+  __syncthreads();
+  for (int row = tid; row < nc * M; row += 128) {
+    const int i = row / M, j = row - i * M, e = s_e[i];
+    double o[NP];
 #pragma unroll
-    for (int k = 0; k < NP; ++k) t += a.tab.phif[s * NP + k] * o[k];
-    a.tr[slot_index<K>(e, s, j)] = t;
+    for (int k = 0; k < NP; ++k) o[k] = s_c[row * NP + k];
+#pragma unroll 4
+    for (int s = 0; s < NS; ++s) {
+      double t = 0.0;
+#pragma unroll
+      for (int k = 0; k < NP; ++k) t += a.tab.phif[s * NP + k] * o[k];
+      a.tr[slot_index<K>(e, s, j)] = t;
+    }
   }
 }
 

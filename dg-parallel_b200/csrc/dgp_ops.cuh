@@ -201,31 +201,48 @@ void ops_totals(const DeviceBuffers& b, double refm, int e_begin, int e_end, cud
   totals_kernel<K><<<(e_end - e_begin + 255) / 256, 256, 0, st>>>(a, refm, b.partials, e_begin, e_end);
 }
 
-template <class K>
-void ops_lts_vol(const DeviceBuffers& b, const int* cells, int n, double* racc, cudaStream_t st) {
-  const StageArgs<double> a = make_args<double>(b);
-  lts_vol_kernel<K><<<(n * K::M + 127) / 128, 128, 0, st>>>(a, cells, n, racc);
+// local time stepping launches over segment tables; S.block0 is filled here
+// from the segments' lengths and the kernels' cells (faces) per CTA
+inline int lts_fill_blocks(LtsSegs& S, int per_cta) {
+  int nb = 0;
+  for (int i = 0; i < S.nseg; ++i) {
+    S.block0[i] = nb;
+    nb += (S.cnt[i] + per_cta - 1) / per_cta;
+  }
+  S.block0[S.nseg] = nb;
+  return nb;
 }
 
 template <class K>
-void ops_lts_face(const DeviceBuffers& b, const int* faces, int n, double time_factor, cudaStream_t st) {
-  StageArgs<double> a = make_args<double>(b);
-  a.stage_time_factor = time_factor;
-  lts_face_kernel<K><<<(n + K::FPB - 1) / K::FPB, K::FACE_BLOCK, 0, st>>>(a, faces, n);
+void ops_lts_vol(const DeviceBuffers& b, const int* lists, const LtsSegs& segs, double* racc, cudaStream_t st) {
+  const StageArgs<double> a = make_args<double>(b);
+  LtsSegs S = segs;
+  const int grid = lts_fill_blocks(S, LtsTile<K>::CPB);
+  lts_vol_kernel<K><<<grid, 128, 0, st>>>(a, lists, S, racc);
 }
 
 template <class K>
-void ops_lts_lift(const DeviceBuffers& b, const int* cells, int n, const int* cface, const int* fcls, int cls_a,
-                  int cls_b, double* racc, cudaStream_t st) {
+void ops_lts_face(const DeviceBuffers& b, const int* lists, const LtsSegs& segs, cudaStream_t st) {
   const StageArgs<double> a = make_args<double>(b);
-  lts_lift_kernel<K><<<(n * K::M + 127) / 128, 128, 0, st>>>(a, cells, n, cface, fcls, cls_a, cls_b, racc);
+  LtsSegs S = segs;
+  const int grid = lts_fill_blocks(S, K::FPB);
+  lts_face_kernel<K><<<grid, K::FACE_BLOCK, 0, st>>>(a, lists, S);
 }
 
 template <class K>
-void ops_lts_update(const DeviceBuffers& b, const int* cells, int n, int op, double dt_factor, double* c1,
-                    double* save, double* racc, cudaStream_t st) {
+void ops_lts_lift(const DeviceBuffers& b, const int* cells, int n, const int* cface, const int* fcls, unsigned mask,
+                  double* racc, cudaStream_t st) {
   const StageArgs<double> a = make_args<double>(b);
-  lts_update_kernel<K><<<(n * K::M + 127) / 128, 128, 0, st>>>(a, cells, n, op, dt_factor, c1, save, racc);
+  lts_lift_kernel<K><<<LtsTile<K>::grid(n), 128, 0, st>>>(a, cells, n, cface, fcls, mask, racc);
+}
+
+template <class K>
+void ops_lts_update(const DeviceBuffers& b, const int* lists, const LtsSegs& segs, double* c1, double* save,
+                    double* racc, cudaStream_t st) {
+  const StageArgs<double> a = make_args<double>(b);
+  LtsSegs S = segs;
+  const int grid = lts_fill_blocks(S, LtsTile<K>::CPB);
+  lts_update_kernel<K><<<grid, 128, 0, st>>>(a, lists, S, c1, save, racc);
 }
 
 template <class K>
@@ -261,6 +278,8 @@ Ops make_ops() {
     o.lts_face = &ops_lts_face<K>;
     o.lts_lift = &ops_lts_lift<K>;
     o.lts_update = &ops_lts_update<K>;
+    o.lts_cpb = LtsTile<K>::CPB;
+    o.lts_fpb = K::FPB;
   }
   return o;
 }

@@ -11,6 +11,7 @@
 
 #include "dgp_host.h"
 #include "dgp_kernels.cuh"
+#include "dgp_lts.cuh"
 
 namespace dgp {
 
@@ -183,16 +184,19 @@ struct Ops {
   void (*trace)(const DeviceBuffers&, const unsigned char* only, cudaStream_t) = nullptr;
   // discrete adjoint stage (nullptr where the adjoint is not built)
   void (*adj_stage)(const DeviceBuffers&, const AdjStage&, cudaStream_t) = nullptr;
-  // local time stepping (FP64, 128-thread tiles; nullptr elsewhere): volume
-  // term of listed cells into racc; face kernel over a face list (boundary
-  // time t + time_factor * dt); lift of face classes a / b into racc; one
-  // coefficient operation (LtsUpdateOp) with dt = ctl->dt * dt_factor
-  void (*lts_vol)(const DeviceBuffers&, const int* cells, int n, double* racc, cudaStream_t) = nullptr;
-  void (*lts_face)(const DeviceBuffers&, const int* faces, int n, double time_factor, cudaStream_t) = nullptr;
-  void (*lts_lift)(const DeviceBuffers&, const int* cells, int n, const int* cface, const int* fcls, int cls_a,
-                   int cls_b, double* racc, cudaStream_t) = nullptr;
-  void (*lts_update)(const DeviceBuffers&, const int* cells, int n, int op, double dt_factor, double* c1,
-                     double* save, double* racc, cudaStream_t) = nullptr;
+  // local time stepping (FP64, 128-thread tiles; nullptr elsewhere), over
+  // segments of `lists` (LtsSegs): volume term of the cells into racc; face
+  // kernel over face lists (boundary time t + fac * dt); lift of the face
+  // classes in mask into racc over one cell list; coefficient operations
+  // (LtsUpdateOp) with dt = ctl->dt * fac
+  void (*lts_vol)(const DeviceBuffers&, const int* lists, const LtsSegs&, double* racc, cudaStream_t) = nullptr;
+  void (*lts_face)(const DeviceBuffers&, const int* lists, const LtsSegs&, cudaStream_t) = nullptr;
+  void (*lts_lift)(const DeviceBuffers&, const int* cells, int n, const int* cface, const int* fcls, unsigned mask,
+                   double* racc, cudaStream_t) = nullptr;
+  void (*lts_update)(const DeviceBuffers&, const int* lists, const LtsSegs&, double* c1, double* save,
+                     double* racc, cudaStream_t) = nullptr;
+  int lts_cpb = 0;  // cells per CTA of the cell kernels (LtsTile::CPB)
+  int lts_fpb = 0;  // faces per CTA of the face kernel
 };
 
 // law, flux, dim, order, precision, block (tile variant: 64, 128 or 256 threads)
