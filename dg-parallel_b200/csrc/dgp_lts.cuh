@@ -64,13 +64,19 @@ __device__ __forceinline__ int lts_segment(const LtsSegs& S, int blk, int& local
 
 // tile shape of the cell kernels: CPB listed cells per 128-thread CTA (one
 // (cell, field) row per thread at most), their coefficients and the volume
-// kernel's flux rows in at most 40 KB of shared memory
+// kernel's flux rows and tables in at most 40 KB of shared memory
 template <class K>
 struct LtsTile {
   static constexpr int M = K::M, MNP = K::MNP, KV = K::KV;
-  static constexpr int BYTES_PER_CELL = 8 * (MNP + M * KV);
+  static constexpr int KVP = KV | 1;  // row stride of the flux rows (odd: no bank conflicts)
+  // the volume kernel's tables (phi, grad phi, weights) in shared memory when
+  // they take at most 8 KB
+  static constexpr int TAB = K::NQ * K::NP + KV * K::NP + K::NQ;
+  static constexpr bool STAGE_TAB = TAB * 8 <= 8 * 1024;
+  static constexpr int TAB_SMEM = STAGE_TAB ? TAB : 1;
+  static constexpr int BYTES_PER_CELL = 8 * (MNP + M * KVP);
   static constexpr int BY_ROWS = 128 / M;
-  static constexpr int BY_SMEM = (40 * 1024) / BYTES_PER_CELL;
+  static constexpr int BY_SMEM = (40 * 1024 - 8 * TAB_SMEM) / BYTES_PER_CELL;
   static constexpr int CPB = BY_ROWS < BY_SMEM ? BY_ROWS : (BY_SMEM < 1 ? 1 : BY_SMEM);
   static int grid(int n) { return (n + CPB - 1) / CPB; }
 };
@@ -103,13 +109,26 @@ __global__ void __launch_bounds__(128) lts_vol_kernel(const __grid_constant__ St
                                                        const int* __restrict__ lists,
                                                        const __grid_constant__ LtsSegs S,
                                                        double* __restrict__ racc) {
+  using S_ = LtsTile<K>;
   constexpr int M = K::M, NP = K::NP, NQ = K::NQ, DIM = K::DIM, MNP = K::MNP, KV = K::KV;
-  constexpr int CPB = LtsTile<K>::CPB;
+  constexpr int CPB = S_::CPB, KVP = S_::KVP;
   __shared__ double s_c[CPB * MNP];
-  __shared__ double s_g[CPB * M * KV];
+  __shared__ double s_g[CPB * M * KVP];
+  __shared__ double s_tab[S_::TAB_SMEM];
   __shared__ int s_e[CPB];
   if (a.gctl->done) return;
   const int tid = threadIdx.x;
+  const double* phi = a.tab.phi;
+  const double* dphi = a.tab.dphi;
+  const double* qw = a.tab.qw;
+  if constexpr (S_::STAGE_TAB) {
+    for (int x = tid; x < NQ * NP; x += 128) s_tab[x] = a.tab.phi[x];
+    for (int x = tid; x < KV * NP; x += 128) s_tab[NQ * NP + x] = a.tab.dphi[x];
+    for (int x = tid; x < NQ; x += 128) s_tab[NQ * NP + KV * NP + x] = a.tab.qw[x];
+    phi = s_tab;
+    dphi = s_tab + NQ * NP;
+    qw = s_tab + NQ * NP + KV * NP;
+  }
   int blk;
   const int sg = lts_segment(S, blockIdx.x, blk);
   const int nc = lts_tile_cells<CPB>(lists + S.off[sg], S.cnt[sg], blk, s_e);
@@ -126,7 +145,7 @@ __global__ void __launch_bounds__(128) lts_vol_kernel(const __grid_constant__ St
     for (int jj = 0; jj < M; ++jj) {
       double u = 0.0;
 #pragma unroll
-      for (int k = 0; k < NP; ++k) u += a.tab.phi[q * NP + k] * c[jj * NP + k];
+      for (int k = 0; k < NP; ++k) u += phi[q * NP + k] * c[jj * NP + k];
       U[jj] = u;
     }
     if (!is_physical<K::LAW, double>(a.law, U)) flag_nonphysical(a.status, e);
@@ -135,7 +154,7 @@ __global__ void __launch_bounds__(128) lts_vol_kernel(const __grid_constant__ St
     double J[DIM * DIM];
 #pragma unroll
     for (int t = 0; t < DIM * DIM; ++t) J[t] = a.mesh.jinv[(size_t)e * DIM * DIM + t];
-    const double jw = a.mesh.detjd[e] * a.tab.qw[q];
+    const double jw = a.mesh.detjd[e] * qw[q];
 #pragma unroll
     for (int j = 0; j < M; ++j)
 #pragma unroll
@@ -143,7 +162,7 @@ __global__ void __launch_bounds__(128) lts_vol_kernel(const __grid_constant__ St
         double g = 0.0;
 #pragma unroll
         for (int t = 0; t < DIM; ++t) g += F[j][t] * J[t * DIM + r];
-        s_g[(i * M + j) * KV + q * DIM + r] = g * jw;
+        s_g[(i * M + j) * KVP + q * DIM + r] = g * jw;
       }
   }
   __syncthreads();
@@ -151,11 +170,11 @@ __global__ void __launch_bounds__(128) lts_vol_kernel(const __grid_constant__ St
     double acc[NP];
 #pragma unroll
     for (int k = 0; k < NP; ++k) acc[k] = 0.0;
-    const double* g = s_g + row * KV;
+    const double* g = s_g + row * KVP;
     for (int kk = 0; kk < KV; ++kk) {
       const double gv = g[kk];
 #pragma unroll
-      for (int k = 0; k < NP; ++k) acc[k] += gv * a.tab.dphi[kk * NP + k];
+      for (int k = 0; k < NP; ++k) acc[k] += gv * dphi[kk * NP + k];
     }
 #pragma unroll
     for (int k = 0; k < NP; ++k) s_c[row * NP + k] = acc[k];  // row < nc * M: own row only

@@ -17,6 +17,7 @@ Meshes:
 * :func:`tri_graded` -- the same triangulation with node lines spaced
   geometrically (ratio ``ratio`` between neighbouring spacings, per axis), so
   that cell sizes span several factors of two (local time stepping bins).
+* :func:`tet_graded` -- the same tets with node planes spaced geometrically.
 * :func:`tet_cube` -- an ``n^3`` grid of a box, each cube split into the six
   Kuhn tetrahedra around its main diagonal (conforming across cubes), interior
   vertices jittered the same way.
@@ -184,6 +185,19 @@ def tet_cube(n: int, x0: float = 0.0, x1: float = 1.0, jitter: float = 0.1, seed
     bfaces = faces[counts[inv.ravel()] == 1]
     btags = np.full(len(bfaces), boundary_tag, dtype=np.int64)
     return Mesh(3, coords, cells.astype(np.int64), bfaces.astype(np.int64), btags, domain_tag)
+
+
+def tet_graded(n: int, ratio: float = 1.2, x0: float = 0.0, x1: float = 1.0, boundary_tag: int = 1,
+               domain_tag: int = 100) -> Mesh:
+    """``tet_cube`` (no jitter) with node plane i at
+    ``x0 + (x1 - x0) (ratio^i - 1) / (ratio^n - 1)`` on every axis: the boxes,
+    and their six Kuhn tets, shrink geometrically towards the (x0, x0, x0)
+    corner (the monotone per-axis map keeps every tet's orientation)."""
+    m = tet_cube(n, 0.0, 1.0, jitter=0.0, boundary_tag=boundary_tag, domain_tag=domain_tag)
+    v = m.vertices.copy()
+    i = np.rint(v * n)
+    v = x0 + (x1 - x0) * (ratio ** i - 1.0) / (ratio ** n - 1.0)
+    return Mesh(3, v, m.cells, m.bfaces, m.btags, domain_tag)
 
 
 def write_msh_v1(mesh: Mesh, path: str) -> None:

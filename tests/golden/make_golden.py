@@ -134,11 +134,14 @@ GRADED_BOX = dict(nx=14, ny=14, ratio=1.15, x0=0.0, x1=10.0, y0=0.0, y1=10.0)
 LTS_CASES = {
     "lts_scalar_graded_p2": ("graded", GRADED, ["--case", "gauss", "--order", "2"], 3),
     "lts_euler_roe_graded_p2": ("graded", GRADED_BOX, ["--case", "vortex", "--flux", "roe", "--order", "2"], 2),
+    "lts_scalar_tet_graded_p2": ("tet_graded", dict(n=6, ratio=1.35),
+                                 ["--case", "gauss3d", "--order", "2", "--ax", "1", "--ay", "0.5", "--az", "0.25",
+                                  "--cx", "0.5", "--cy", "0.5", "--cz", "0.5", "--s", "0.05"], 2),
 }
 
 
 def run_lts_case(name, kind, margs, dargs, steps):
-    mesh = meshgen.tri_graded(**margs)
+    mesh = meshgen.tri_graded(**margs) if kind == "graded" else meshgen.tet_graded(**margs)
     msh = os.path.join(HERE, name + ".msh")
     meshgen.write_msh_v1(mesh, msh)
     with tempfile.TemporaryDirectory() as td:

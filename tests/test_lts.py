@@ -15,12 +15,13 @@ import pytest
 
 import dgp
 from dgp import meshgen
-from cases import REF_TOL, SCALAR2D, VORTEX, golden, rel
+from cases import REF_TOL, SCALAR2D, SCALAR3D, VORTEX, golden, rel
 from oracle_bind import Oracle
 
 LTS_CASES = {
     "lts_scalar_graded_p2": (dgp.LAW_SCALAR, dgp.FLUX_UPWIND, dgp.FIELD_GAUSS, 2, SCALAR2D),
     "lts_euler_roe_graded_p2": (dgp.LAW_EULER2D, dgp.FLUX_ROE, dgp.FIELD_VORTEX, 2, VORTEX),
+    "lts_scalar_tet_graded_p2": (dgp.LAW_SCALAR, dgp.FLUX_UPWIND, dgp.FIELD_GAUSS3D, 2, SCALAR3D),
 }
 ORACLE_IDS = {dgp.LAW_SCALAR: 0, dgp.LAW_EULER2D: 2}
 FP64_TOL = 1e-12
