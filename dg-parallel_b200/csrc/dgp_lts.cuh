@@ -264,64 +264,84 @@ __global__ void __launch_bounds__(128) lts_update_kernel(const __grid_constant__
   const int nc = lts_tile_cells<CPB>(lists + S.off[sg], S.cnt[sg], blk, s_e);
   const int op = S.op[sg];
   const double dt = __dmul_rn(a.ctl->dt, S.fac[sg]);  // fac = 2^-k: exact
-  for (int xi = tid; xi < nc * MNP; xi += 128) {
-    const int i = xi / MNP, e = s_e[i];
-    const size_t g = (size_t)e * MNP + (xi - i * MNP);
-    const double det = a.mesh.detjd[e];
-    double x = a.Cout[g];
-    switch (op) {
-      case LTS_EULER_IN:
+  const int ne = nc * MNP;
+  double* C = a.Cout;
+  // one loop per operation (the operation is uniform over the CTA), unrolled
+  // so that each thread has several independent loads in flight
+#define LTS_ELEMS(...)                                           \
+  _Pragma("unroll 4") for (int xi = tid; xi < ne; xi += 128) {   \
+    const int i = xi / MNP;                                      \
+    const size_t g = (size_t)s_e[i] * MNP + (xi - i * MNP);      \
+    const double det = a.mesh.detjd[s_e[i]];                     \
+    (void)det;                                                   \
+    double out;                                                  \
+    __VA_ARGS__                                                  \
+    C[g] = out;                                                  \
+    s_c[xi] = out;                                               \
+  }
+  switch (op) {
+    case LTS_EULER_IN:
+      LTS_ELEMS({
+        const double x = C[g], r = racc[g];
         save[g] = x;
-        x = __dadd_rn(x, __dmul_rn(__ddiv_rn(racc[g], det), dt));
+        out = __dadd_rn(x, __dmul_rn(__ddiv_rn(r, det), dt));
         racc[g] = 0.0;
-        break;
-      case LTS_TWO_HALF: {
+      })
+      break;
+    case LTS_TWO_HALF:
+      LTS_ELEMS({
+        const double x = C[g], r = racc[g];
         save[g] = x;
-        const double inc = __ddiv_rn(__dmul_rn(racc[g], dt), det);
-        x = __dadd_rn(x, inc);
-        c1[g] = x;
-        x = __dadd_rn(x, inc);
+        const double inc = __ddiv_rn(__dmul_rn(r, dt), det);
+        const double h = __dadd_rn(x, inc);
+        c1[g] = h;
+        out = __dadd_rn(h, inc);
         racc[g] = 0.0;
-        break;
-      }
-      case LTS_EULER:
+      })
+      break;
+    case LTS_EULER:
+      LTS_ELEMS({
+        const double x = C[g], r = racc[g];
         save[g] = x;
-        x = __dadd_rn(x, __ddiv_rn(__dmul_rn(racc[g], dt), det));
+        out = __dadd_rn(x, __ddiv_rn(__dmul_rn(r, dt), det));
         racc[g] = 0.0;
-        break;
-      case LTS_SECOND:
-      case LTS_SECOND_SWAP: {
-        const double xn =
-            __dmul_rn(__dadd_rn(__dadd_rn(x, __ddiv_rn(__dmul_rn(racc[g], dt), det)), save[g]), 0.5);
-        if (op == LTS_SECOND) {
-          x = xn;
-          racc[g] = 0.0;
-        } else {
-          x = c1[g];
-          c1[g] = xn;
-        }
-        break;
-      }
-      case LTS_COPYBACK_ZERO:
-      case LTS_FINAL_RESET:
-        x = c1[g];
+      })
+      break;
+    case LTS_SECOND:
+      LTS_ELEMS({
+        const double x = C[g], r = racc[g], s0 = save[g];
+        out = __dmul_rn(__dadd_rn(__dadd_rn(x, __ddiv_rn(__dmul_rn(r, dt), det)), s0), 0.5);
         racc[g] = 0.0;
-        break;
-      case LTS_LI_HALF: {
-        const double s0 = save[g], x1 = c1[g];
+      })
+      break;
+    case LTS_SECOND_SWAP:
+      LTS_ELEMS({
+        const double x = C[g], r = racc[g], s0 = save[g], x1 = c1[g];
+        c1[g] = __dmul_rn(__dadd_rn(__dadd_rn(x, __ddiv_rn(__dmul_rn(r, dt), det)), s0), 0.5);
+        out = x1;
+      })
+      break;
+    case LTS_COPYBACK_ZERO:
+    case LTS_FINAL_RESET:
+      LTS_ELEMS({
+        out = c1[g];
+        racc[g] = 0.0;
+      })
+      break;
+    case LTS_LI_HALF:
+      LTS_ELEMS({
+        const double x = C[g], s0 = save[g], x1 = c1[g];
         const double xn = __dadd_rn(__dadd_rn(s0, __dsub_rn(x, s0)),
                                     __dmul_rn(0.25, __dadd_rn(__dsub_rn(x1, __dmul_rn(2.0, x)), s0)));
         save[g] = __dadd_rn(xn, __dmul_rn(0.5, __dsub_rn(x1, s0)));
-        x = xn;
-        break;
-      }
-      default:  // LTS_RESTORE
-        x = save[g];
-        break;
-    }
-    a.Cout[g] = x;
-    s_c[xi] = x;
+        out = xn;
+      })
+      break;
+    default:  // LTS_RESTORE
+      LTS_ELEMS({ out = save[g]; })
+      break;
   }
+#undef LTS_ELEMS
   __syncthreads();
   for (int row = tid; row < nc * M; row += 128) {
     const int i = row / M, j = row - i * M, e = s_e[i];
