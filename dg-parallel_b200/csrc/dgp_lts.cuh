@@ -214,12 +214,20 @@ __global__ void __launch_bounds__(128) lts_lift_kernel(const __grid_constant__ S
                                                         const int* __restrict__ cface,
                                                         const int* __restrict__ fcls, unsigned mask,
                                                         double* __restrict__ racc) {
-  constexpr int M = K::M, NP = K::NP, NQF = K::NQF, NLF = K::NLF, MNP = K::MNP;
+  constexpr int M = K::M, NP = K::NP, NQF = K::NQF, NLF = K::NLF, MNP = K::MNP, NS = K::NS;
   constexpr int CPB = LtsTile<K>::CPB;
+  // the face-point basis in shared memory when it takes at most 8 KB
+  constexpr bool STAGE = NS * NP * 8 <= 8 * 1024;
   __shared__ double s_c[CPB * MNP];
+  __shared__ double s_phif[STAGE ? NS * NP : 1];
   __shared__ int s_e[CPB];
   if (a.gctl->done) return;
-  const int nc = lts_tile_cells<CPB>(list, n, blockIdx.x, s_e);
+  const double* phif = a.tab.phif;
+  if constexpr (STAGE) {
+    for (int x = threadIdx.x; x < NS * NP; x += 128) s_phif[x] = a.tab.phif[x];
+    phif = s_phif;
+  }
+  const int nc = lts_tile_cells<CPB>(list, n, blockIdx.x, s_e);  // its barrier covers s_phif
   for (int row = threadIdx.x; row < nc * M; row += 128) {
     const int i = row / M, j = row - i * M, e = s_e[i];
     double acc[NP];
@@ -233,7 +241,7 @@ __global__ void __launch_bounds__(128) lts_lift_kernel(const __grid_constant__ S
         const int s = lf * NQF + q;
         const double sv = a.slots[slot_index<K>(e, s, j)];
 #pragma unroll
-        for (int k = 0; k < NP; ++k) acc[k] += sv * a.tab.phif[s * NP + k];
+        for (int k = 0; k < NP; ++k) acc[k] += sv * phif[s * NP + k];
       }
     }
 #pragma unroll
