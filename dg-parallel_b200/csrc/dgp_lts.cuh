@@ -91,10 +91,12 @@ __device__ __forceinline__ int lts_tile_cells(const int* __restrict__ list, int 
   return nc;
 }
 
-// racc[cell] += s_c[cell] for the tile's cells, element-parallel
+// racc[cell] += s_c[cell] for the tile's cells, element-parallel (128-thread
+// CTAs; unrolled so that several loads are in flight)
 template <int MNP>
 __device__ __forceinline__ void lts_add_rows(const int* s_e, int nc, const double* s_c, double* racc) {
-  for (int x = threadIdx.x; x < nc * MNP; x += blockDim.x) {
+#pragma unroll 4
+  for (int x = threadIdx.x; x < nc * MNP; x += 128) {
     const int i = x / MNP;
     racc[(size_t)s_e[i] * MNP + (x - i * MNP)] += s_c[x];
   }
@@ -132,6 +134,7 @@ __global__ void __launch_bounds__(128) lts_vol_kernel(const __grid_constant__ St
   int blk;
   const int sg = lts_segment(S, blockIdx.x, blk);
   const int nc = lts_tile_cells<CPB>(lists + S.off[sg], S.cnt[sg], blk, s_e);
+#pragma unroll 4
   for (int x = tid; x < nc * MNP; x += 128) {
     const int i = x / MNP;
     s_c[x] = a.C[(size_t)s_e[i] * MNP + (x - i * MNP)];
