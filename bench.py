@@ -682,6 +682,7 @@ def lts_bench(n=256, ratio=1.0098, steps=16):
         return e0.elapsed_time(e1) / 1e3, t_end, k
 
     s = dgp.Solver(mesh, law, 3, dgp.FP64)
+    s.set_p0_fallback(False)  # local time stepping runs without the P0 fallback
     nb = s.set_time_stepping(dgp.STEPPING_LOCAL)
     bins, role = s.lts_bins()
     E = mesh.ncells
@@ -859,6 +860,7 @@ def profile_case(args):
         mesh = dgp.Mesh.from_arrays(2, m.vertices, m.cells, 100, m.bfaces, m.btags)
         law = dgp.Law(dgp.LAW_EULER2D, dgp.FLUX_ROE, dgp.FIELD_VORTEX, vortex_params())
         s = dgp.Solver(mesh, law, 3, dgp.FP64)
+        s.set_p0_fallback(False)
         nb = s.set_time_stepping(dgp.STEPPING_LOCAL)
         t, n = s.run(0.0, 0.0, 0.1, args.warmup + args.steps)
         s.synchronize()

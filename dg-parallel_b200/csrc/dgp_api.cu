@@ -240,6 +240,98 @@ static std::vector<int> morton_order(const HostMesh& m) {
   return order;
 }
 
+// Face records and halos of the fused stage kernel's tiles (TileMesh): for
+// tile t, every face with a side among its cells, in face order, with both
+// sides as local rows (own cells first, then the halo in order of first use)
+// and the face's FP64 normal and measure.  The fused kernel is left off (the
+// stages use the face and element kernels) if a tile's halo would not fit in
+// shared memory.
+static int build_tiles(dgp_solver s, int Etot, const std::vector<int>& fel, const std::vector<int>& fcode,
+                       const std::vector<double>& fnrm, const std::vector<double>& fj, const std::vector<int>& bpart,
+                       const std::vector<int>& cface) {
+  const int TE = s->ops.TE, nlf = s->tab.nlf, dim = s->b.dim;
+  const int ntiles = (Etot + TE - 1) / TE;
+  std::vector<int> tf_off(1, 0), tf_side, tf_code, tf_bnd, th_off(1, 0), th_cell;
+  std::vector<double> tf_nrm, tf_fj;
+  std::vector<int> flist, halo;
+  int nh_max = 0;
+  for (int t = 0; t < ntiles; ++t) {
+    const int e0 = t * TE, e1 = std::min(e0 + TE, Etot);
+    flist.clear();
+    halo.clear();
+    for (int e = e0; e < e1; ++e)
+      for (int lf = 0; lf < nlf; ++lf) {
+        const int k = cface[static_cast<size_t>(e) * nlf + lf];
+        if (k >= 0) flist.push_back(k);
+      }
+    std::sort(flist.begin(), flist.end());
+    flist.erase(std::unique(flist.begin(), flist.end()), flist.end());
+    auto local = [&](int e) {
+      if (e >= e0 && e < e1) return e - e0;
+      for (size_t h = 0; h < halo.size(); ++h)
+        if (halo[h] == e) return TE + static_cast<int>(h);
+      halo.push_back(e);
+      return TE + static_cast<int>(halo.size()) - 1;
+    };
+    for (int k : flist) {
+      const int eL = fel[2 * static_cast<size_t>(k)], eR = fel[2 * static_cast<size_t>(k) + 1];
+      const int lL = local(eL);
+      const int ownL = (eL >= e0 && eL < e1) ? 1 : 0;
+      int side = lL, ownR = 0, kind = 0, bnd = -1;
+      if (eR >= 0) {
+        side |= (local(eR) + 1) << 16;
+        ownR = (eR >= e0 && eR < e1) ? 1 : 0;
+      } else {
+        bnd = -eR - 1;
+        if (bpart[bnd] >= 0) {
+          kind = 2;
+          side |= (local(bpart[bnd]) + 1) << 16;
+        } else {
+          kind = 1;
+        }
+      }
+      tf_side.push_back(side);
+      tf_code.push_back((fcode[k] & 0xfff) | (ownL << 12) | (ownR << 13) | (kind << 14));
+      tf_bnd.push_back(bnd);
+      for (int c = 0; c < dim; ++c) tf_nrm.push_back(fnrm[static_cast<size_t>(k) * dim + c]);
+      tf_fj.push_back(fj[k]);
+    }
+    tf_off.push_back(static_cast<int>(tf_side.size()));
+    th_cell.insert(th_cell.end(), halo.begin(), halo.end());
+    th_off.push_back(static_cast<int>(th_cell.size()));
+    nh_max = std::max(nh_max, static_cast<int>(halo.size()));
+  }
+  s->fused = s->ops.fused != nullptr && nh_max <= TE * nlf && s->ops.fused_smem(nh_max) + 8 * 1024 <= 227 * 1024;
+  if (!s->fused) return DGP_OK;
+  TileMesh& tm = s->b.tm;
+  int rc = DGP_OK;
+  int *d_tf_off, *d_tf_side, *d_tf_code, *d_tf_bnd, *d_th_off, *d_th_cell;
+  double *d_tf_nrm, *d_tf_fj;
+  if (th_cell.empty()) th_cell.push_back(0);
+  if (tf_side.empty()) {
+    tf_side.push_back(0);
+    tf_code.push_back(0);
+    tf_bnd.push_back(-1);
+    tf_fj.push_back(0.0);
+    tf_nrm.resize(dim, 0.0);
+  }
+  if ((rc = s->upload(&d_tf_off, tf_off)) || (rc = s->upload(&d_tf_side, tf_side)) ||
+      (rc = s->upload(&d_tf_code, tf_code)) || (rc = s->upload(&d_tf_bnd, tf_bnd)) ||
+      (rc = s->upload(&d_tf_nrm, tf_nrm)) || (rc = s->upload(&d_tf_fj, tf_fj)) ||
+      (rc = s->upload(&d_th_off, th_off)) || (rc = s->upload(&d_th_cell, th_cell)))
+    return rc;
+  tm.tf_off = d_tf_off;
+  tm.tf_side = d_tf_side;
+  tm.tf_code = d_tf_code;
+  tm.tf_bnd = d_tf_bnd;
+  tm.tf_nrm = d_tf_nrm;
+  tm.tf_fj = d_tf_fj;
+  tm.th_off = d_th_off;
+  tm.th_cell = d_th_cell;
+  tm.nh_max = nh_max;
+  return DGP_OK;
+}
+
 // Builds the device state of a solver over the instances already in s->meshes
 // (one mesh for a single solver).  Instance i owns internal cells
 // [inst_off[i], inst_off[i] + E_i), each instance starting on an
@@ -387,6 +479,7 @@ static int build_solver(dgp_solver s, const std::vector<LawParams>& lps, int fie
   }
   b.F = Ftot;
   b.NB = nb;
+  if (int rc = build_tiles(s, Etot, fel, fcode, fnrm, fj, bpart, cface)) return rc;
   // per-cell geometry padded to whole tiles (the element kernel copies a
   // tile's J^{-1} and |J| in one piece)
   {
@@ -443,6 +536,14 @@ static int build_solver(dgp_solver s, const std::vector<LawParams>& lps, int fie
   DGP_CUDA(cudaMemset(tr, 0, nslot * ts));
   DGP_CUDA(cudaMemset(C, 0, nstate * 8 + 256));
   DGP_CUDA(cudaMemset(U0, 0, nstate * 8 + 256));
+  if (s->fused) {  // stage states u1, u2 (with the same tail as the state)
+    unsigned char *X1, *X2;
+    if ((rc = s->alloc(&X1, nstate * 8 + 256)) || (rc = s->alloc(&X2, nstate * 8 + 256))) return rc;
+    DGP_CUDA(cudaMemset(X1, 0, nstate * 8 + 256));
+    DGP_CUDA(cudaMemset(X2, 0, nstate * 8 + 256));
+    b.X1 = X1;
+    b.X2 = X2;
+  }
   b.C = C;
   b.U0 = U0;
   b.slots = slots;
@@ -899,7 +1000,12 @@ int dgp_rhs(dgp_solver s, double t, double* host_rhs) {
   if (!s || !host_rhs) return fail(DGP_ERR_INVALID, "null argument");
   DGP_CUDA(cudaSetDevice(s->device));
   if (int rc = set_ctl(s, t, 0.0, 0.0, 0.0, 0)) return rc;
-  s->ops.stage(s->b, 0, 0.0, 0, s->stream);
+  if (s->fused) {
+    const double* C = static_cast<const double*>(s->b.C);
+    s->ops.fused(s->b, C, C, static_cast<double*>(s->b.rhs), nullptr, 0, 0.0, 0, s->stream);
+  } else {
+    s->ops.stage(s->b, 0, 0.0, 0, s->stream);
+  }
   DGP_CUDA(cudaGetLastError());
   DGP_CUDA(cudaStreamSynchronize(s->stream));
   return state_to_host(s, s->b.rhs, host_rhs);
@@ -927,16 +1033,50 @@ static void launch_step(dgp_solver s, int fuse_cfl) {
     return;
   }
   const bool lim = s->limiter != DGP_LIMITER_NONE && s->ops.limit;
-  s->ops.stage(s->b, 1, 0.0, 0, s->stream);
-  if (lim) s->ops.limit(s->b, 1, s->stream);
-  s->ops.stage(s->b, 2, 1.0, 0, s->stream);
-  if (lim) s->ops.limit(s->b, 1, s->stream);
-  s->ops.stage(s->b, 3, 0.5, lim ? 0 : fuse_cfl, s->stream);
-  if (lim) {
-    s->ops.limit(s->b, 1, s->stream);
-    if (fuse_cfl) s->ops.cfl(s->b, s->stream);
+  if (s->fused) {
+    // u_n (C) -> u1 (X1) -> u2 (X2) -> u_n+1 (C, own rows in place); the
+    // limiter runs on each stage's output
+    DeviceBuffers& b = s->b;
+    double* C = static_cast<double*>(b.C);
+    double* X1 = static_cast<double*>(b.X1);
+    double* X2 = static_cast<double*>(b.X2);
+    DeviceBuffers bl = b;
+    s->ops.fused(b, C, C, X1, nullptr, 1, 0.0, 0, s->stream);
+    if (lim) {
+      bl.C = X1;
+      s->ops.limit(bl, 1, s->stream);
+    }
+    s->ops.fused(b, X1, C, X2, nullptr, 2, 1.0, 0, s->stream);
+    if (lim) {
+      bl.C = X2;
+      s->ops.limit(bl, 1, s->stream);
+    }
+    s->ops.fused(b, X2, C, C, nullptr, 3, 0.5, lim ? 0 : fuse_cfl, s->stream);
+    if (lim) {
+      s->ops.limit(b, 1, s->stream);
+      if (fuse_cfl) s->ops.cfl(b, s->stream);
+    }
+    s->tr_stale = true;
+  } else {
+    s->ops.stage(s->b, 1, 0.0, 0, s->stream);
+    if (lim) s->ops.limit(s->b, 1, s->stream);
+    s->ops.stage(s->b, 2, 1.0, 0, s->stream);
+    if (lim) s->ops.limit(s->b, 1, s->stream);
+    s->ops.stage(s->b, 3, 0.5, lim ? 0 : fuse_cfl, s->stream);
+    if (lim) {
+      s->ops.limit(s->b, 1, s->stream);
+      if (fuse_cfl) s->ops.cfl(s->b, s->stream);
+    }
   }
   if (!s->probes.empty()) launch_probe_recorders(s);
+}
+
+// the local time stepping kernels read the face-point traces, which the fused
+// stage kernel does not keep
+static void refresh_traces(dgp_solver s) {
+  if (!s->tr_stale) return;
+  s->ops.trace(s->b, nullptr, s->stream);
+  s->tr_stale = false;
 }
 
 int dgp_launches_per_step(dgp_solver s, int* n) {
@@ -947,7 +1087,7 @@ int dgp_launches_per_step(dgp_solver s, int* n) {
   }
   const bool lim = s->limiter != DGP_LIMITER_NONE && s->ops.limit;
   const int per_pass = s->limiter == DGP_LIMITER_BARTH ? 1 : 2;
-  *n = 3 * (s->b.p0 ? 3 : 2) + (lim ? 3 * per_pass + 1 : 0);
+  *n = 3 * (s->fused ? 1 : s->b.p0 ? 3 : 2) + (lim ? 3 * per_pass + 1 : 0);
   return DGP_OK;
 }
 
@@ -955,6 +1095,7 @@ int dgp_step(dgp_solver s, double t, double dt, double* resid) {
   if (!s || !(dt > 0)) return fail(DGP_ERR_INVALID, "bad argument");
   DGP_CUDA(cudaSetDevice(s->device));
   if (int rc = set_ctl(s, t, dt, 0.0, 0.0, 0)) return rc;
+  if (s->lts.on) refresh_traces(s);
   launch_step(s, 0);
   DGP_CUDA(cudaGetLastError());
   TimeCtl c;
@@ -986,6 +1127,7 @@ int dgp_run(dgp_solver s, double t0, double tend, double cfl, int max_steps, dou
     return DGP_OK;
   };
   const bool tail = max_steps > 0 && max_steps % K != 0;
+  if (s->lts.on) refresh_traces(s);
   if (!s->graph) {
     if (int rc = capture(K, &s->graph)) return rc;
     s->graph_steps = K;
@@ -1052,8 +1194,17 @@ int dgp_limiter_triggers(dgp_solver s, unsigned char* out) {
 
 int dgp_set_p0_fallback(dgp_solver s, int on) {
   if (!s) return fail(DGP_ERR_INVALID, "null solver");
+  if (on && s->lts.on)
+    return fail(DGP_ERR_UNSUPPORTED, "the P0 fallback is not built for local time stepping");
   s->drop_graphs();
   s->b.p0 = on ? 1 : 0;
+  return DGP_OK;
+}
+
+int dgp_set_copy_wait_limit(dgp_solver s, int polls) {
+  if (!s || polls < 0) return fail(DGP_ERR_INVALID, "bad argument");
+  s->drop_graphs();
+  s->b.mbar_polls = polls;
   return DGP_OK;
 }
 
@@ -1063,13 +1214,14 @@ int dgp_status(dgp_solver s, int* nonphysical, int* first_bad_cell) {
   Status st;
   DGP_CUDA(cudaMemcpyAsync(&st, s->b.status, sizeof(Status), cudaMemcpyDeviceToHost, s->stream));
   DGP_CUDA(cudaStreamSynchronize(s->stream));
+  // each call reports what happened since the previous one
+  Status st0{0, INT32_MAX};
+  DGP_CUDA(cudaMemcpy(s->b.status, &st0, sizeof(Status), cudaMemcpyHostToDevice));
   if (st.timeouts > 0)
     return fail(DGP_ERR_CUDA, "a bounded wait on a bulk copy gave up in " + std::to_string(st.timeouts) +
                                   " CTA(s); results of that launch are incomplete");
   if (nonphysical) *nonphysical = st.nonphysical;
   if (first_bad_cell) *first_bad_cell = st.nonphysical ? s->i2f[std::min(st.first_bad, s->b.E - 1)] : -1;
-  Status st0{0, INT32_MAX};
-  DGP_CUDA(cudaMemcpy(s->b.status, &st0, sizeof(Status), cudaMemcpyHostToDevice));
   return DGP_OK;
 }
 
@@ -1147,6 +1299,35 @@ int dgp_profile_kernels(dgp_solver s, int iters, float* ms) {
   if (int rc = set_ctl(s, 0.0, 0.0, 0.0, 0.1, 0)) return rc;
   cudaEvent_t ev[4];
   for (auto& e : ev) DGP_CUDA(cudaEventCreate(&e));
+  if (s->fused) {
+    // stage 1, stage 2 and the last stage with the CFL reduction, each reading
+    // the state and writing a stage buffer (the state is left as it is)
+    double* C = static_cast<double*>(s->b.C);
+    double* X1 = static_cast<double*>(s->b.X1);
+    double* X2 = static_cast<double*>(s->b.X2);
+    auto run = [&](int k) {
+      if (k == 0) s->ops.fused(s->b, C, C, X1, nullptr, 1, 0.0, 0, s->stream);
+      if (k == 1) s->ops.fused(s->b, C, C, X2, nullptr, 2, 1.0, 0, s->stream);
+      if (k == 2) s->ops.fused(s->b, C, C, X2, nullptr, 3, 0.5, 1, s->stream);
+    };
+    for (int k = 0; k < 3; ++k) run(k);  // warm-up
+    for (int k = 0; k < 3; ++k) {
+      DGP_CUDA(cudaEventRecord(ev[k], s->stream));
+      for (int i = 0; i < iters; ++i) run(k);
+    }
+    DGP_CUDA(cudaEventRecord(ev[3], s->stream));
+    DGP_CUDA(cudaGetLastError());
+    DGP_CUDA(cudaEventSynchronize(ev[3]));
+    for (int k = 0; k < 3; ++k) {
+      float t = 0;
+      DGP_CUDA(cudaEventElapsedTime(&t, ev[k], ev[k + 1]));
+      ms[k] = t / iters;
+    }
+    for (auto& e : ev) cudaEventDestroy(e);
+    DGP_CUDA(cudaMemcpyAsync(s->b.C, s->b.scratch, bytes, cudaMemcpyDeviceToDevice, s->stream));
+    DGP_CUDA(cudaStreamSynchronize(s->stream));
+    return DGP_OK;
+  }
   s->ops.face(s->b, 2, 1.0, s->stream);  // warm-up
   s->ops.elem(s->b, 2, 0, s->stream);
   s->ops.elem(s->b, 3, 1, s->stream);
@@ -1662,6 +1843,13 @@ int dgp_receiver_values(dgp_solver s, double* rho, double* J) {
 // one SSP-RK3 step from X back into X, keeping u_n, u1, u2 in S (three
 // consecutive states)
 static void step_keeping_stages(dgp_solver s, double* X, double* S, size_t ns) {
+  if (s->fused) {
+    s->ops.fused(s->b, X, X, S + ns, S, 1, 0.0, 0, s->stream);
+    s->ops.fused(s->b, S + ns, S, S + 2 * ns, nullptr, 2, 1.0, 0, s->stream);
+    s->ops.fused(s->b, S + 2 * ns, S, X, nullptr, 3, 0.5, 0, s->stream);
+    s->tr_stale = true;
+    return;
+  }
   DeviceBuffers b = s->b;
   b.U0 = S;
   b.C = X;

@@ -106,6 +106,9 @@ struct dgp_solver_s {
   int graph_steps = 0;
   dgp::TimeCtl* h_ctl = nullptr;  // pinned, 2 entries
   LtsState lts;                    // local time stepping (off unless enabled)
+  bool fused = false;              // stages run through the fused stage kernel
+  bool tr_stale = false;           // the face-point traces (tr) lag the state (the fused
+                                   // kernel keeps none; the local time stepping kernels read them)
   void drop_graphs() {
     if (graph) cudaGraphExecDestroy(graph);
     if (graph1) cudaGraphExecDestroy(graph1);

@@ -145,10 +145,30 @@ struct DevTables {
   double phi0;
 };
 
+// Per-tile face records and halo lists of the fused stage kernel.  Tile t
+// owns cells [t TE, (t + 1) TE); its faces are every face with a side in the
+// tile (a face between two tiles appears in both lists and is evaluated by
+// both, identically); a local row index l < TE is the own cell e0 + l, l >= TE
+// the halo cell th_cell[th_off[t] + l - TE].
+struct TileMesh {
+  const int* tf_off;     // [ntiles + 1] face records of each tile
+  const int* tf_side;    // lL | (lR + 1) << 16 (interior) or (partner + 1) << 16 (periodic), 0 above
+  const int* tf_code;    // lfL | lfR << 4 | perm << 8 | ownL << 12 | ownR << 13 | kind << 14
+                         // (kind 0 interior, 1 boundary, 2 periodic)
+  const int* tf_bnd;     // boundary face index of kinds 1 and 2
+  const double* tf_nrm;  // [NTF][DIM] unit normal out of the left cell (FP64)
+  const double* tf_fj;   // [NTF] |J_f| (FP64)
+  const int* th_off;     // [ntiles + 1] halo cells of each tile
+  const int* th_cell;    // internal cell index of each halo row
+  int nh_max;            // largest halo of a tile
+};
+
 template <typename T>
 struct StageArgs {
   DevMesh<T> mesh;
   DevTables<T> tab;
+  TileMesh tm;
+  int mbar_polls;  // bound of the first bulk-copy wait of the fused stage kernel (0: default)
   LawParams law;
   // the state is FP64 in both forms; T is the arithmetic of the RHS
   const double* C;   // state the stage reads

@@ -350,6 +350,9 @@ int dgp_set_time_stepping(dgp_solver s, int mode, int* nbins) {
   if (s->limiter != DGP_LIMITER_NONE)
     return fail(DGP_ERR_UNSUPPORTED, "local time stepping runs without a limiter");
   if (s->meshes.size() != 1) return fail(DGP_ERR_UNSUPPORTED, "local time stepping runs on single solvers");
+  if (s->b.p0)
+    return fail(DGP_ERR_UNSUPPORTED,
+                "local time stepping runs without the P0 fallback: turn it off first (dgp_set_p0_fallback(s, 0))");
   if (int rc = lts_setup(s, nbins)) return rc;
   s->lts.on = true;
   return DGP_OK;

@@ -44,7 +44,9 @@ static __device__ __align__(256) unsigned char g_scratch[kScratchBytes];
 std::mutex g_scratch_mutex;
 void* g_scratch_addr[kMaxDevices] = {};
 
-// device address of g_scratch on `device` (the current device)
+// device address of g_scratch on `device` (the current device), looked up once
+// per device; a device reset frees the module and with it this address, as it
+// frees every other device buffer the library's handles hold
 int scratch_address(int device, void** out) {
   if (device < 0 || device >= kMaxDevices) return fail(DGP_ERR_INVALID, "device index out of range");
   std::lock_guard<std::mutex> lock(g_scratch_mutex);
@@ -77,7 +79,10 @@ extern "C" int dgp_rhs_noalloc(dgp_solver s, const double* dev_state, double t, 
   DGP_CUDA(cudaSetDevice(s->device));
   const size_t tsize = s->ops.tsize;
   const int E = s->b.E, mnp = s->b.M * s->b.NP;
-  const size_t state_b = round256(s->state_count() * 8);  // FP64 state and RHS
+  // FP64 state and RHS, each with the 256-byte tail the solver's own state
+  // buffers carry: the element kernel's bulk copy of the last tile rounds its
+  // length up to 16 bytes and must stay inside the region
+  const size_t state_b = round256(s->state_count() * 8 + 256);
   const size_t ntiles = (static_cast<size_t>(E) + s->ops.TE - 1) / s->ops.TE;
   const size_t slot_b = round256(ntiles * s->ops.TE * s->tab.nlf * s->tab.nqf * s->b.M * tsize);
   const size_t need = 2 * state_b + 2 * slot_b;

@@ -7,6 +7,7 @@
 #include "dgp_limiter.cuh"
 #include "dgp_lts.cuh"
 #include "dgp_solver.h"
+#include "dgp_stage.cuh"
 
 namespace dgp {
 
@@ -17,8 +18,15 @@ constexpr bool adjoint_built() {
   return K::FLUX != DGP_FLUX_GODUNOV;
 }
 
+constexpr size_t kSmemPerCta = 227 * 1024;
+
+template <class K, bool ENS>
+cudaError_t fused_prepare();
+
 template <class K>
 cudaError_t ops_prepare() {
+  if (cudaError_t e = fused_prepare<K, false>()) return e;
+  if (cudaError_t e = fused_prepare<K, true>()) return e;
   const size_t smem = elem_kernel_smem<K>();
   if (smem > 48 * 1024) {
     cudaError_t e = cudaFuncSetAttribute(elem_kernel<K>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -33,6 +41,17 @@ cudaError_t ops_prepare() {
                                   static_cast<int>(as));
   }
   return cudaSuccess;
+}
+
+// dynamic shared memory of the fused stage kernel may use whatever the static
+// part leaves of the 227 KB a CTA can hold
+template <class K, bool ENS>
+cudaError_t fused_prepare() {
+  cudaFuncAttributes fa;
+  cudaError_t e = cudaFuncGetAttributes(&fa, stage_kernel<K, ENS>);
+  if (e != cudaSuccess) return e;
+  return cudaFuncSetAttribute(stage_kernel<K, ENS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              static_cast<int>(kSmemPerCta - fa.sharedSizeBytes));
 }
 
 template <class K>
@@ -85,6 +104,26 @@ void ops_stage(const DeviceBuffers& b, int stage, double time_factor, int fuse_c
   ops_face<K>(b, stage, time_factor, st);
   if (stage > 0 && b.p0) ops_face_rerun<K>(b, stage, time_factor, st);
   ops_elem<K>(b, stage, fuse_cfl, st);
+}
+
+template <class K>
+size_t ops_fused_smem(int nh_max) {
+  return FusedSmem<K>::bytes(nh_max);
+}
+
+template <class K>
+void ops_fused(const DeviceBuffers& b, const double* in, const double* u0, double* out, double* u0copy, int stage,
+               double time_factor, int fuse_cfl, cudaStream_t st) {
+  auto a = stage_args<K>(b, stage, time_factor, fuse_cfl);
+  a.C = in;
+  a.U0 = u0;
+  a.Cout = out;
+  a.U0out = u0copy;
+  const size_t smem = FusedSmem<K>::bytes(b.tm.nh_max);
+  if (b.cell_inst)
+    stage_kernel<K, true><<<ops_grid_elem<K>(b.E), K::BLOCK, smem, st>>>(a);
+  else
+    stage_kernel<K, false><<<ops_grid_elem<K>(b.E), K::BLOCK, smem, st>>>(a);
 }
 
 template <class K>
@@ -264,6 +303,8 @@ Ops make_ops() {
   o.stage = &ops_stage<K>;
   o.face = &ops_face<K>;
   o.elem = &ops_elem<K>;
+  o.fused = &ops_fused<K>;
+  o.fused_smem = &ops_fused_smem<K>;
   o.cfl = &ops_cfl<K>;
   o.project = &ops_project<K>;
   o.l2err = &ops_l2err<K>;

@@ -56,6 +56,10 @@ struct DeviceBuffers {
   void* tr = nullptr;     // face-point traces of C (slot layout)
   void* rhs = nullptr;    // assembled RHS for dgp_rhs
   void* scratch = nullptr;// state-sized staging for device-side set/get
+  void* X1 = nullptr;     // stage states u1, u2 of the fused stage kernel (the state C holds u_n)
+  void* X2 = nullptr;
+  TileMesh tm{};          // per-tile face records and halos of the fused stage kernel
+  int mbar_polls = 0;     // bound of the fused kernel's first bulk-copy wait (0: default)
   TimeCtl* ctl = nullptr;
   Status* status = nullptr;
   double* partials = nullptr;
@@ -121,6 +125,8 @@ inline StageArgs<T> make_args(const DeviceBuffers& b) {
   a.tab.ephi = b.ephi;
   a.tab.phi0 = b.phi0;
   a.law = b.law;
+  a.tm = b.tm;
+  a.mbar_polls = b.mbar_polls;
   a.C = static_cast<const double*>(b.C);
   a.U0 = static_cast<const double*>(b.U0);
   a.Cout = static_cast<double*>(b.Cout ? b.Cout : b.C);
@@ -169,6 +175,12 @@ struct Ops {
   void (*stage)(const DeviceBuffers&, int stage, double time_factor, int fuse_cfl, cudaStream_t) = nullptr;
   void (*face)(const DeviceBuffers&, int stage, double time_factor, cudaStream_t) = nullptr;
   void (*elem)(const DeviceBuffers&, int stage, int fuse_cfl, cudaStream_t) = nullptr;
+  // fused stage kernel: reads the stage input `in` (this tile's and its halo's
+  // rows) and u_n, writes `out` (stage 0: the RHS); u0copy, when set, receives
+  // the input rows in stage 1
+  void (*fused)(const DeviceBuffers&, const double* in, const double* u0, double* out, double* u0copy, int stage,
+                double time_factor, int fuse_cfl, cudaStream_t) = nullptr;
+  size_t (*fused_smem)(int nh_max) = nullptr;
   void (*cfl)(const DeviceBuffers&, cudaStream_t) = nullptr;
   void (*project)(const DeviceBuffers&, double t, cudaStream_t) = nullptr;
   // over cells [e_begin, e_end); lp: field parameters (nullptr: the solver's law)

@@ -1,0 +1,437 @@
+// Fused stage kernel: one CTA per tile of TE cells computes every face flux
+// that touches the tile, the volume term, the lift of the face slots, the
+// diagonal inverse mass and the SSP-RK3 stage combination, with the last
+// stage's residual and CFL reductions fused in.
+//
+// The tile reads the stage input rows of its own cells and of its halo (the
+// cells across its faces, periodic partners included), all staged into shared
+// memory by bulk copies on one mbarrier; face-point traces and face slots
+// live in shared memory only.  A face between two tiles is evaluated by both,
+// from identical inputs with identical arithmetic, so each side receives the
+// same flux it would get from a separate face pass.  The stage writes a
+// different buffer from the one it reads (u_n -> u1 -> u2 -> u_n in place,
+// own rows only), so no tile reads a row another tile is writing.
+//
+// Replaces DGBoundaryCell::computeBoundaryContributions (DGCell.cc:639-732),
+// DGCell::computeVolumeContribution (DGCell.cc:184-249) and the
+// RungeKuttaTVD3::advanceInTime update loops (TimeIntegrator.cc:838-990).
+//
+// P0 fallback (DGCell::setToZero, DGCell.cc:785-811; DGAnalysis.cc:392-417):
+// a cell is marked when its trace at any of its face points is not physical.
+// Each tile checks its own cells at their face points during the face pass
+// and its halo cells at all of theirs, so it knows every mark that reaches
+// its faces without a grid-wide pass; a tile that sees one zeroes the modes
+// k >= 1 of the marked rows (own and halo, in shared memory) and evaluates
+// its faces again.  Marks of stage 1 persist into u_n for stages 2 and 3
+// (bad[e]).
+#pragma once
+
+#include "dgp_elem.cuh"
+
+namespace dgp {
+
+template <class K>
+struct FusedSmem {
+  using T = typename K::T;
+  using L = ElemSmem<K>;
+  static constexpr size_t r16(size_t n) { return (n + 15) / 16 * 16; }
+  // table blob | own rows FP64 [TE][MNP] | face slots T [NS][ROWS] | geometry |
+  // union { halo rows FP64 [nh][MNP] (face pass), G T [ROWS][LDK] (volume) }
+  static constexpr size_t oC = r16(L::blob_bytes);
+  static constexpr size_t oS = oC + r16((size_t)K::TE * K::MNP * 8);
+  static constexpr size_t oJ = oS + r16((size_t)K::NS * K::ROWS * sizeof(T));
+  static constexpr size_t oX = oJ + r16(8 * ((size_t)K::TE * L::DD + (size_t)K::TE * K::NV));
+  static constexpr size_t g_bytes = r16((size_t)K::ROWS * K::LDK * sizeof(T));
+  static constexpr size_t bytes(int nh) {
+    return oX + (r16((size_t)nh * K::MNP * 8) > g_bytes ? r16((size_t)nh * K::MNP * 8) : g_bytes);
+  }
+  // rows can be bulk copied one by one when a row is a whole number of 16-byte units
+  static constexpr bool bulk_rows = (K::MNP * 8) % 16 == 0;
+  static constexpr int HMAX = K::TE * K::NLF;  // a tile's halo never exceeds one cell per own face
+};
+
+// trace of one FP64 row at a face point: U[j] = sum_k phi[k] row[j][k] in T,
+// in the order of the element kernel's volume interpolation
+template <class K>
+__device__ __forceinline__ void row_trace(const double* __restrict__ row, const typename K::T* phi,
+                                          typename K::T* U) {
+  using T = typename K::T;
+  constexpr int NP = K::NP;
+#pragma unroll
+  for (int j = 0; j < K::M; ++j) {
+    double cv[NP];
+    load_vec<double, NP>(row + j * NP, cv);
+    T acc = 0;
+#pragma unroll
+    for (int k = 0; k < NP; ++k) acc += phi[k] * (T)cv[k];
+    U[j] = acc;
+  }
+}
+
+// the periodic partner's trace, its basis values at the mirrored point read
+// from global memory
+template <class K>
+__device__ __forceinline__ void row_trace_g(const double* __restrict__ row, const typename K::T* __restrict__ phi,
+                                            typename K::T* U) {
+  using T = typename K::T;
+  constexpr int NP = K::NP;
+#pragma unroll
+  for (int j = 0; j < K::M; ++j) {
+    T acc = 0;
+#pragma unroll
+    for (int k = 0; k < NP; ++k) acc += __ldg(phi + k) * (T)row[j * NP + k];
+    U[j] = acc;
+  }
+}
+
+struct FusedTile {
+  int e0, ne, nh, f0, nf;
+};
+
+// One face point of a tile face: traces of both sides from the staged rows,
+// the law's numerical, periodic or boundary flux, and the slots of the own
+// sides.  CHECK: count non-physical own traces and, with the P0 fallback on,
+// mark their cells (returns true when it marked one).
+template <class K, bool ENS, bool CHECK>
+__device__ __forceinline__ bool fused_face_point(const StageArgs<typename K::T>& a, const TimeCtl* c, int inst,
+                                                 const FusedTile& ft, int tf, int q, const typename K::T* sPhif,
+                                                 const typename K::T* s_fqw, const int* s_qmap, const double* sC,
+                                                 const double* sH, typename K::T* sS, unsigned char* s_mark) {
+  using T = typename K::T;
+  using L = ElemSmem<K>;
+  constexpr int M = K::M, MNP = K::MNP, NQF = K::NQF, DIM = K::DIM, TE = K::TE, ROWS = K::ROWS;
+  constexpr int NPP = L::NPP;
+  const int side = a.tm.tf_side[tf], code = a.tm.tf_code[tf];
+  const int lL = side & 0xffff, hi = side >> 16;
+  const int lfL = code & 15, lfR = (code >> 4) & 15, perm = (code >> 8) & 15;
+  const bool ownL = (code >> 12) & 1, ownR = (code >> 13) & 1;
+  const int kind = (code >> 14) & 3;
+  auto rowp = [&](int l) -> const double* { return l < TE ? sC + l * MNP : sH + (l - TE) * MNP; };
+  T n[DIM];
+#pragma unroll
+  for (int i = 0; i < DIM; ++i) n[i] = (T)a.tm.tf_nrm[(size_t)tf * DIM + i];
+  const T jw = (T)a.tm.tf_fj[tf] * s_fqw[q];
+  bool marked = false;
+  T UL[M], UR[M], flux[M];
+  row_trace<K>(rowp(lL), sPhif + (lfL * NQF + q) * NPP, UL);
+  if (CHECK && ownL && !is_physical<K::LAW, T>(a.law, UL)) {
+    flag_nonphysical(a.status, ft.e0 + lL);
+    if (a.p0) {
+      s_mark[lL] = 1;
+      marked = true;
+    }
+  }
+  int qR = 0;
+  if (kind == 0) {
+    const int lR = hi - 1;
+    qR = s_qmap[perm * NQF + q];
+    row_trace<K>(rowp(lR), sPhif + (lfR * NQF + qR) * NPP, UR);
+    if (CHECK && ownR && !is_physical<K::LAW, T>(a.law, UR)) {
+      flag_nonphysical(a.status, ft.e0 + lR);
+      if (a.p0) {
+        s_mark[lR] = 1;
+        marked = true;
+      }
+    }
+    numerical_flux<K::LAW, K::FLUX, DIM, T>(a.law, n, UL, UR, flux);
+  } else if (kind == 2) {
+    // periodic edge (DGCell.cc:687-705): the partner cell's trace at the
+    // mirrored point through the numerical flux; only the left cell gets it
+    const int b = a.tm.tf_bnd[tf];
+    row_trace_g<K>(rowp(hi - 1), a.mesh.bpphi + ((size_t)b * NQF + q) * K::NP, UR);
+    numerical_flux<K::LAW, K::FLUX, DIM, T>(a.law, n, UL, UR, flux);
+  } else {
+    const int b = a.tm.tf_bnd[tf];
+    const double* x = a.mesh.bpts + ((size_t)b * NQF + q) * 3;
+    const double time = __fma_rn(a.stage_time_factor, c->dt, c->t);
+    if constexpr (ENS)
+      boundary_flux<K::LAW, K::FLUX, DIM, T>(a.laws[inst], a.mesh.bbid[b], n, x, time, UL, flux);
+    else
+      boundary_flux<K::LAW, K::FLUX, DIM, T>(a.law, a.mesh.bbid[b], n, x, time, UL, flux);
+  }
+  if (ownL) {
+    T* dst = sS + (lfL * NQF + q) * ROWS + lL * M;
+#pragma unroll
+    for (int j = 0; j < M; ++j) dst[j] = -flux[j] * jw;
+  }
+  if (kind == 0 && ownR) {
+    T* dst = sS + (lfR * NQF + qR) * ROWS + (hi - 1) * M;
+#pragma unroll
+    for (int j = 0; j < M; ++j) dst[j] = flux[j] * jw;
+  }
+  return marked;
+}
+
+template <class K, bool ENS, bool CHECK>
+__device__ __forceinline__ bool fused_face_pass(const StageArgs<typename K::T>& a, const TimeCtl* c, int inst,
+                                                const FusedTile& ft, const typename K::T* sPhif,
+                                                const typename K::T* s_fqw, const int* s_qmap, const double* sC,
+                                                const double* sH, typename K::T* sS, unsigned char* s_mark) {
+  constexpr int NQF = K::NQF;
+  bool mk = false;
+  for (int t = threadIdx.x; t < ft.nf * NQF; t += K::BLOCK) {
+    const int f = t / NQF, q = t - f * NQF;
+    mk |= fused_face_point<K, ENS, CHECK>(a, c, inst, ft, ft.f0 + f, q, sPhif, s_fqw, s_qmap, sC, sH, sS, s_mark);
+  }
+  return mk;
+}
+
+template <class K, bool ENS>
+__global__ void __launch_bounds__(K::BLOCK) stage_kernel(const __grid_constant__ StageArgs<typename K::T> a) {
+  using T = typename K::T;
+  using L = ElemSmem<K>;
+  using FS = FusedSmem<K>;
+  using G = GeoArea<K>;
+  constexpr int M = K::M, NP = K::NP, MNP = K::MNP, NQ = K::NQ, NS = K::NS, NQF = K::NQF, DIM = K::DIM;
+  constexpr int TE = K::TE, BLOCK = K::BLOCK, ROWS = K::ROWS, KV = K::KV, LDK = K::LDK, NPP = L::NPP;
+  if (a.gctl->done) return;
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  T* sT = reinterpret_cast<T*>(smem_raw);
+  const T* sDphi = sT + L::oDphi;
+  const T* sPhif = sT + L::oPhif;
+  const T* sPhi = sT + L::oPhi;
+  const T* sQw = sT + L::oQw;
+  double* sC = reinterpret_cast<double*>(smem_raw + FS::oC);
+  T* sS = reinterpret_cast<T*>(smem_raw + FS::oS);
+  double* sDet = reinterpret_cast<double*>(smem_raw + FS::oJ + G::oDet);
+  double* sEig = reinterpret_cast<double*>(smem_raw + FS::oJ + G::oEig);
+  T* sJi = reinterpret_cast<T*>(smem_raw + FS::oJ + G::oJi);
+  double* sH = reinterpret_cast<double*>(smem_raw + FS::oX);
+  T* sG = reinterpret_cast<T*>(smem_raw + FS::oX);
+  __shared__ __align__(8) uint64_t bar;
+  __shared__ double red[BLOCK / 32];
+  __shared__ int s_fail;
+  __shared__ T s_fqw[NQF];
+  __shared__ int s_qmap[K::NPERM * NQF];
+  __shared__ unsigned char s_mark[TE + FS::HMAX];
+  __shared__ double sPv[(K::NV - 1) * NP + 1];
+
+  const int tid = threadIdx.x;
+  const int tile = blockIdx.x;
+  FusedTile ft;
+  ft.e0 = tile * TE;
+  TimeCtl* c = a.ctl;
+  int inst = 0, eend = a.mesh.E;
+  if constexpr (ENS) {  // the tile belongs to one instance
+    inst = a.cell_inst[ft.e0];
+    c = a.ctl + inst;
+    eend = a.inst_end[inst];
+    if (c->done) {
+      if (a.stage == 3) {
+        elem_tile_tail<K>(a, c, tile, 0.0, false, nullptr, nullptr, 0, ft.e0, red, nullptr, 0.0);
+        elem_finish<K>(a, c, gridDim.x, red);
+      }
+      return;
+    }
+  }
+  ft.ne = min(TE, eend - ft.e0);
+  const int h0 = a.tm.th_off[tile];
+  ft.nh = a.tm.th_off[tile + 1] - h0;
+  ft.f0 = a.tm.tf_off[tile];
+  ft.nf = a.tm.tf_off[tile + 1] - ft.f0;
+  const uint32_t c_bytes = (uint32_t)(((size_t)ft.ne * MNP * 8 + 15) / 16 * 16);
+
+  if (tid == 0) {
+    s_fail = 0;
+    mbar_init(&bar, 1);
+  }
+  for (int i = tid; i < NQF; i += BLOCK) s_fqw[i] = a.tab.fqw[i];
+  for (int i = tid; i < K::NPERM * NQF; i += BLOCK) s_qmap[i] = a.tab.qmap[i];
+  for (int i = tid; i < TE + ft.nh; i += BLOCK) s_mark[i] = 0;
+  __syncthreads();
+  // one mbarrier for the tables, the tile's rows and the halo rows; lane 0
+  // announces every byte before any copy is issued
+  if (tid < 32) {
+    if (tid == 0) {
+      uint32_t tx = (uint32_t)L::blob_bytes;
+      if constexpr (FS::bulk_rows) tx += c_bytes + (uint32_t)ft.nh * MNP * 8;
+      mbar_arrive_expect_tx(&bar, tx);
+      bulk_g2s(sT, a.tab.blob, (uint32_t)L::blob_bytes, &bar);
+      if constexpr (FS::bulk_rows) bulk_g2s(sC, a.C + (size_t)ft.e0 * MNP, c_bytes, &bar);
+    }
+    __syncwarp();
+    if constexpr (FS::bulk_rows)
+      for (int h = tid; h < ft.nh; h += 32)
+        bulk_g2s(sH + (size_t)h * MNP, a.C + (size_t)a.tm.th_cell[h0 + h] * MNP, (uint32_t)(MNP * 8), &bar);
+    // a bound on the first wait counts its polls from the copies' issue
+    if (tid == 0 && a.mbar_polls > 0 && !mbar_test_polls(&bar, 0, a.mbar_polls)) s_fail = 1;
+  }
+  if constexpr (!FS::bulk_rows) {
+    const double* src = a.C + (size_t)ft.e0 * MNP;
+    for (int i = tid; i < ft.ne * MNP; i += BLOCK) sC[i] = src[i];
+    for (int i = tid; i < ft.nh * MNP; i += BLOCK) {
+      const int h = i / MNP;
+      sH[i] = a.C[(size_t)a.tm.th_cell[h0 + h] * MNP + (i - h * MNP)];
+    }
+  }
+  double csz = 0.0;
+  if (a.stage == 3 && a.fuse_cfl) {
+    if (tid < ft.ne) csz = a.mesh.csize[ft.e0 + tid];
+    for (int i = tid; i < (K::NV - 1) * NP; i += BLOCK) sPv[i] = a.tab.phiv[i];
+  }
+  for (int i = tid; i < ft.ne * DIM * DIM; i += BLOCK) sJi[i] = a.mesh.jinv[(size_t)ft.e0 * DIM * DIM + i];
+  for (int i = tid; i < ft.ne; i += BLOCK) sDet[i] = a.mesh.detjd[ft.e0 + i];
+  if (tid == 0 && (s_fail || !mbar_wait(&bar, 0, kMbarPolls))) {
+    // record the failure, then wait once more (bounded) for the copies this
+    // CTA issued before its shared memory is released
+    s_fail = 1;
+    atomicAdd(&a.status->timeouts, 1);
+    mbar_wait(&bar, 0, kMbarPolls);
+  }
+  __syncthreads();
+  if (s_fail) {
+    // the tile's output is not written; the last stage still joins the
+    // completion count so that the finalize runs and resets it
+    if (a.stage == 3) {
+      elem_tile_tail<K>(a, c, tile, 0.0, false, nullptr, nullptr, 0, ft.e0, red, nullptr, 0.0);
+      elem_finish<K>(a, c, gridDim.x, red);
+    }
+    return;
+  }
+
+  // ---- faces: every face point of the tile's faces into the slots --------
+  bool mk = fused_face_pass<K, ENS, true>(a, c, inst, ft, sPhif, s_fqw, s_qmap, sC, sH, sS, s_mark);
+  if (a.p0) {
+    // halo cells: marked when any of their face-point traces is not physical
+    for (int t = tid; t < ft.nh * NS; t += BLOCK) {
+      const int h = t / NS, s = t - h * NS;
+      T U[M];
+      row_trace<K>(sH + (size_t)h * MNP, sPhif + s * NPP, U);
+      if (!is_physical<K::LAW, T>(a.law, U)) {
+        s_mark[TE + h] = 1;
+        mk = true;
+      }
+    }
+    if (__syncthreads_or(mk)) {
+      // P0: marked rows drop to their means, then the faces again
+      for (int i = tid; i < (TE + ft.nh) * M; i += BLOCK) {
+        const int l = i / M, j = i - l * M;
+        if (l < TE && l >= ft.ne) continue;
+        if (!s_mark[l]) continue;
+        double* row = (l < TE ? sC + l * MNP : sH + (size_t)(l - TE) * MNP) + j * NP;
+        for (int k = 1; k < NP; ++k) row[k] = 0.0;
+      }
+      __syncthreads();
+      fused_face_pass<K, ENS, false>(a, c, inst, ft, sPhif, s_fqw, s_qmap, sC, sH, sS, s_mark);
+    }
+    // stage 1: the marks persist into u_n for stages 2 and 3
+    if (a.stage == 1)
+      for (int l = tid; l < ft.ne; l += BLOCK) a.bad[ft.e0 + l] = s_mark[l];
+  }
+  __syncthreads();  // halo rows are dead from here on: G takes their place
+
+  // ---- volume: thread (q, g) owns quadrature point q ------------------------
+  if (tid < K::EG * NQ) {
+    const int q = tid % NQ, g = tid / NQ;
+    T phi[NP];
+#pragma unroll
+    for (int k = 0; k < NP; ++k) phi[k] = sPhi[q * NPP + k];
+    const T w = sQw[q];
+    for (int e = g; e < ft.ne; e += K::EG) {
+      T U[M];
+#pragma unroll
+      for (int j = 0; j < M; ++j) {
+        double cv[NP];
+        load_vec<double, NP>(sC + (e * M + j) * NP, cv);
+        T acc = 0;
+#pragma unroll
+        for (int k = 0; k < NP; ++k) acc += phi[k] * (T)cv[k];
+        U[j] = acc;
+      }
+      if (!is_physical<K::LAW, T>(a.law, U)) flag_nonphysical(a.status, ft.e0 + e);
+      T F[M][DIM];
+      volume_flux<K::LAW, DIM, T>(a.law, U, F);
+      T J[DIM * DIM];
+#pragma unroll
+      for (int i = 0; i < DIM * DIM; ++i) J[i] = sJi[e * DIM * DIM + i];
+      const T jw = (T)sDet[e] * w;
+#pragma unroll
+      for (int j = 0; j < M; ++j)
+#pragma unroll
+        for (int r = 0; r < DIM; ++r) {
+          T acc = 0;
+#pragma unroll
+          for (int i = 0; i < DIM; ++i) acc += F[j][i] * J[i * DIM + r];
+          sG[(e * M + j) * LDK + q * DIM + r] = acc * jw;
+        }
+    }
+  }
+  // u_n of the row (stages 2 and 3) from global memory while the volume and
+  // contraction run; stage-1 P0 marks zero its modes k >= 1
+  const int row = tid;
+  const bool live = row < ft.ne * M;
+  const size_t gbase = ((size_t)ft.e0 * M + row) * NP;
+  constexpr int RALIGN = pow2_div(NP * 8) < 16 ? pow2_div(NP * 8) : 16;
+  double u0[NP];
+  if (live && a.stage >= 2) {
+    ldg_vec<double, NP, RALIGN>(a.U0 + gbase, u0);
+    if (a.p0 && a.bad[ft.e0 + row / M]) {
+#pragma unroll
+      for (int k = 1; k < NP; ++k) u0[k] = 0.0;
+    }
+  }
+  __syncthreads();
+
+  // ---- contraction + lift + inverse mass + stage combination ---------------
+  double rsum = 0.0;
+  if (live) {
+    T acc[NPP];
+#pragma unroll
+    for (int k = 0; k < NPP; ++k) acc[k] = 0;
+    const T* gr = sG + row * LDK;
+#pragma unroll 4
+    for (int kk = 0; kk < KV; ++kk) {
+      const T gv = gr[kk];
+      T d[NPP];
+      load_vec<T, NPP>(sDphi + kk * NPP, d);
+#pragma unroll
+      for (int k = 0; k < NPP; ++k) acc[k] += gv * d[k];
+    }
+#pragma unroll 4
+    for (int s = 0; s < NS; ++s) {
+      const T sv = sS[s * ROWS + row];
+      T p[NPP];
+      load_vec<T, NPP>(sPhif + s * NPP, p);
+#pragma unroll
+      for (int k = 0; k < NPP; ++k) acc[k] += sv * p[k];
+    }
+    if (a.stage == 0) {
+#pragma unroll
+      for (int k = 0; k < NP; ++k) a.Cout[gbase + k] = (double)acc[k];
+    } else {
+      const int e = row / M;
+      // FP64 update in the reference's operation order (dt/|J| in FP64)
+      const double dtj = c->dt / sDet[e];
+      double* crow = sC + row * NP;
+      double cv[NP];
+      load_vec<double, NP>(crow, cv);
+      if (a.stage == 1 && a.U0out) {
+#pragma unroll
+        for (int k = 0; k < NP; ++k) a.U0out[gbase + k] = cv[k];
+      }
+      double out[NP];
+#pragma unroll
+      for (int k = 0; k < NP; ++k) {
+        const double r = (double)acc[k];
+        if (a.stage == 1) {
+          out[k] = cv[k] + r * dtj;
+        } else if (a.stage == 2) {
+          out[k] = 0.25 * (cv[k] + r * dtj + 3. * u0[k]);
+        } else {
+          out[k] = (2.0 * (cv[k] + r * dtj) + u0[k]) / 3.0;
+          const double dd = out[k] - u0[k];
+          rsum += dd * dd;
+        }
+      }
+#pragma unroll
+      for (int k = 0; k < NP; ++k) crow[k] = out[k];
+      st_vec<double, NP, RALIGN>(a.Cout + gbase, out);
+    }
+  }
+  if (a.stage != 3) return;
+  __syncthreads();
+  elem_tile_tail<K>(a, c, tile, rsum, true, sC, sEig, ft.ne, ft.e0, red, sPv, csz);
+  elem_finish<K>(a, c, gridDim.x, red);
+}
+
+}  // namespace dgp

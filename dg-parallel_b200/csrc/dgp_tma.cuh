@@ -49,4 +49,17 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, int ma
   return ok != 0;
 }
 
+// polls phase `parity` of the barrier without suspending, at most `polls` times
+__device__ __forceinline__ bool mbar_test_polls(uint64_t* bar, uint32_t parity, int polls) {
+  uint32_t ok = 0;
+  for (int i = 0; i < polls && !ok; ++i) {
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.test_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+  }
+  return ok != 0;
+}
+
 }  // namespace dgp

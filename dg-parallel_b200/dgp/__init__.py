@@ -90,6 +90,7 @@ def lib() -> ctypes.CDLL:
         "dgp_limit": ([P, ctypes.POINTER(ctypes.c_uint8)], I),
         "dgp_limiter_triggers": ([P, ctypes.POINTER(ctypes.c_uint8)], I),
         "dgp_set_p0_fallback": ([P, I], I),
+        "dgp_set_copy_wait_limit": ([P, I], I),
         "dgp_launches_per_step": ([P, pI], I),
         "dgp_set_time_stepping": ([P, I, pI], I),
         "dgp_lts_bins": ([P, pI, pI], I),
@@ -336,6 +337,12 @@ class Solver:
 
     def set_p0_fallback(self, on: bool = True):
         check(lib().dgp_set_p0_fallback(self.h, 1 if on else 0))
+
+    def set_copy_wait_limit(self, polls: int = 0):
+        """Bound the fused stage kernel's first wait for its bulk copies, in
+        polls from the copies' issue (0: the default); a wait that gives up
+        surfaces as DGP_ERR_CUDA in the next status()."""
+        check(lib().dgp_set_copy_wait_limit(self.h, int(polls)))
 
     def launches_per_step(self) -> int:
         n = ctypes.c_int()

@@ -152,7 +152,11 @@ int dgp_launches_per_step(dgp_solver s, int* n);
  *   whole-mesh versions assemble on each range.  FP64, no limiter, single
  *   solvers; meshes the reference rejects (fewer than 2 or more than 10 bins,
  *   a cell in no bin or on two interfaces, neighbours more than one bin apart)
- *   give DGP_ERR_INVALID.  nbins (may be NULL) receives the number of bins.
+ *   give DGP_ERR_INVALID; so does a solver whose P0 fallback is on
+ *   (DGP_ERR_UNSUPPORTED: the local time stepping kernels have no P0 pass,
+ *   turn it off first with dgp_set_p0_fallback(s, 0); non-physical states are
+ *   still counted in dgp_status).  nbins (may be NULL) receives the number of
+ *   bins.
  * dgp_lts_bins: per cell (file order) its bin and role (0 inner, 1 large on an
  *   interface, 2 small on an interface); either pointer may be NULL. */
 #define DGP_STEPPING_SSPRK3 0
@@ -178,8 +182,16 @@ int dgp_limiter_triggers(dgp_solver s, unsigned char* out);
 /* P0 fallback of DGBoundaryCell::computeBoundaryContributions + DGCell::setToZero
  * (DGCell.cc:639-811): in every SSP-RK3 stage, cells with a non-physical trace
  * at a face point drop their modes k >= 1 and the stage is assembled again.
- * On by default for the Euler laws; 0 turns it off. */
+ * On by default for the Euler laws; 0 turns it off.  Turning it on while local
+ * time stepping is on returns DGP_ERR_UNSUPPORTED. */
 int dgp_set_p0_fallback(dgp_solver s, int on);
+/* Bound on the first wait of the fused stage kernel for its bulk copies, in
+ * polls counted from the copies' issue (0 restores the default wait, about 4
+ * million polls).  A CTA whose wait gives up waits again for its copies with
+ * the full bound, writes nothing and returns; the next dgp_status returns
+ * DGP_ERR_CUDA ("a bounded wait ... gave up") and that stage's output is
+ * incomplete.  For testing the error path; no counterpart in DG-Parallel. */
+int dgp_set_copy_wait_limit(dgp_solver s, int polls);
 /* non-physical states seen since the last call (isPhysical, EulerLaw.cc:1398) */
 int dgp_status(dgp_solver s, int* nonphysical, int* first_bad_cell);
 /* L2 error of one field against the law's exact field (DGCell::densityErrorL2,
@@ -228,9 +240,11 @@ int dgp_synchronize(dgp_solver s);
 /* the solver's CUDA stream (cudaStream_t) for callers that order their own
  * work or record CUDA events against the solver's launches */
 int dgp_solver_stream(dgp_solver s, void** stream);
-/* mean device time (CUDA events on the solver's stream) of the face kernel,
- * the element kernel of an inner stage and the element kernel of the last
- * stage (with the fused CFL reduction), over `iters` launches each: ms[3] */
+/* mean device time (CUDA events on the solver's stream) over `iters` launches
+ * each: ms[3] = the fused stage kernel of stage 1, of stage 2 and of the last
+ * stage with the fused CFL reduction (solvers whose tiles' halos do not fit
+ * the fused kernel: the face kernel, the element kernel of an inner stage and
+ * of the last stage).  Leaves the state unchanged; resets the time control. */
 int dgp_profile_kernels(dgp_solver s, int iters, float* ms);
 /* Assembled right-hand side that allocates no device memory; no counterpart in
  * DG-Parallel.  For callers that cannot call cudaMalloc when they need a RHS
@@ -241,7 +255,10 @@ int dgp_profile_kernels(dgp_solver s, int iters, float* ms);
  * the library holds until exit; meshes that need more return DGP_ERR_INVALID.
  * Calls share that array: calls that overlap on the GPU race.  The first call
  * on a device looks up the array's device address (host-side setup), so make
- * it before any stream capture.  Returns after the solver's stream is idle. */
+ * it before any stream capture.  Like dgp_rhs, the call resets the solver's
+ * time control (time t, step 0).  A device reset (cudaDeviceReset) invalidates
+ * every handle of this library on that device, the cached address of the
+ * static array included.  Returns after the solver's stream is idle. */
 int dgp_rhs_noalloc(dgp_solver s, const double* dev_state, double t, double* dev_rhs);
 
 /* ---- ensembles (no counterpart in DG-Parallel, which runs one DGAnalysis per

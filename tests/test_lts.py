@@ -68,9 +68,14 @@ def test_oracle_lts_rejects_meshes_the_reference_rejects(tmp_path):
         assert _oracle(p, dgp.LAW_SCALAR, dgp.FLUX_UPWIND, dgp.FIELD_GAUSS, 1, SCALAR2D).lts_setup() == code
 
 
-def _solver(msh, law, flux, field, order, prm, precision=dgp.FP64, limiter=dgp.LIMITER_NONE):
+def _solver(msh, law, flux, field, order, prm, precision=dgp.FP64, limiter=dgp.LIMITER_NONE, p0=False):
+    """Local time stepping runs without the P0 fallback (on by default for the
+    Euler laws): p0=False turns it off, as a caller must before enabling it."""
     mesh = dgp.Mesh.from_msh(msh)
-    return dgp.Solver(mesh, dgp.Law(law, flux, field, prm), order, precision, limiter)
+    s = dgp.Solver(mesh, dgp.Law(law, flux, field, prm), order, precision, limiter)
+    if not p0:
+        s.set_p0_fallback(False)
+    return s
 
 
 @pytest.mark.gpu
@@ -164,3 +169,18 @@ def test_gpu_lts_modes_and_errors(tmp_path):
     assert ei.value.code == -3
     with pytest.raises(dgp.DGPError):
         s.set_time_stepping(7)
+    # the P0 fallback (on by default for the Euler laws) and local time
+    # stepping exclude each other, whichever is asked for second
+    law_e, flux_e, field_e, order_e, prm_e = LTS_CASES["lts_euler_roe_graded_p2"]
+    msh_e, _ = golden("lts_euler_roe_graded_p2")
+    e = _solver(msh_e, law_e, flux_e, field_e, order_e, prm_e, p0=True)
+    with pytest.raises(dgp.DGPError) as ei:
+        e.set_time_stepping(dgp.STEPPING_LOCAL)
+    assert ei.value.code == -3 and "P0" in str(ei.value)
+    e.set_p0_fallback(False)
+    assert e.set_time_stepping(dgp.STEPPING_LOCAL) == 3
+    with pytest.raises(dgp.DGPError) as ei:
+        e.set_p0_fallback(True)
+    assert ei.value.code == -3
+    e.set_time_stepping(dgp.STEPPING_SSPRK3)
+    e.set_p0_fallback(True)
