@@ -22,6 +22,11 @@
 //                  the cell's per-field slope factors (details->limSlope).  The
 //                  limiter writes the coefficients in place; TimeIntegrator::
 //                  limit's copy of the unwritten second slot is not applied.
+//   --state-bin F  after the steps: the coefficients of every cell as raw
+//                  native doubles, [cell][field][mode] in file order.
+//   --l2 FILE      after the steps: DGAnalysis::densityErrorL2 (DGPref.cc:370-380)
+//                  at the final time, then every cell's DGCell::densityErrorL2
+//                  (DGError.cc:805-826; the squared error) in file order.
 //   --ckpt-out F   after the steps: the data stream of DGAnalysis::write
 //                  (DGPref.cc:712-739) -- TACT, ITER, sizes, every cell's
 //                  writeMEntity + DGCell::write, every face's writeMEntity.
@@ -192,7 +197,7 @@ static int ltsSortCells(mDGMesh* mesh, int n) {
 #endif
 
 struct Params {
-  std::string mesh, caseName = "gauss", flux = "exact", conn, rhs, state, log, barth, ckptOut, ckptIn;
+  std::string mesh, caseName = "gauss", flux = "exact", conn, rhs, state, log, barth, ckptOut, ckptIn, l2, stateBin;
   int order = 2, steps = 0, every = 1, threads = 1, bench = 0, warmup = 0, gpu = 0, lts = 0;
   std::string bins;
   double cfl = 0.1, tend = -1.0;
@@ -363,7 +368,7 @@ static double nowSec() {
 static void usage() {
   fprintf(stderr, "usage: ref_driver --mesh F.msh [--case gauss|vortex|pulse3d|sine|gauss3d] "
                   "[--flux exact|roe] [--order p] [--steps n | --tend T] [--cfl c] "
-                  "[--conn F] [--rhs F] [--state F --every k] [--log F] [--barth F] [--ckpt-in F] [--ckpt-out F] "
+                  "[--conn F] [--rhs F] [--state F --every k] [--log F] [--barth F] [--l2 F] [--state-bin F] [--ckpt-in F] [--ckpt-out F] "
                   "[--threads k --bench n]\n");
   exit(1);
 }
@@ -389,6 +394,8 @@ int main(int argc, char** argv) {
     else if (a == "--state") P.state = v;
     else if (a == "--log") P.log = v;
     else if (a == "--barth") P.barth = v;
+    else if (a == "--l2") P.l2 = v;
+    else if (a == "--state-bin") P.stateBin = v;
     else if (a == "--ckpt-out") P.ckptOut = v;
     else if (a == "--ckpt-in") P.ckptIn = v;
     else if (a == "--gpu") P.gpu = atoi(v);
@@ -656,6 +663,33 @@ int main(int argc, char** argv) {
       ((DGCell*)(*it)->getCell())->write(data);
     }
     for (mMesh::iter it = mesh->begin(dim - 1); it != mesh->end(dim - 1); ++it) mesh->writeMEntity(data, *it);
+  }
+  if (!P.stateBin.empty()) {
+    FILE* f = fopen(P.stateBin.c_str(), "wb");
+    std::vector<double> row(m * Np);
+    for (int e = 0; e < E; ++e) {
+      for (int i = 0; i < m; ++i)
+        for (int j = 0; j < Np; ++j) row[i * Np + j] = byFile[e]->theFieldsCoefficients->get(i, j);
+      fwrite(row.data(), sizeof(double), row.size(), f);
+    }
+    fclose(f);
+  }
+  if (!P.l2.empty()) {
+    // DGAnalysis::densityErrorL2 (DGPref.cc:370-380): sqrt of the sum over
+    // cells of DGCell::densityErrorL2 (DGError.cc:805-826) at the final time;
+    // the total first, then each cell's squared error in file order
+    double total = 0.0;
+    std::vector<double> per(E, 0.0);
+    for (mMesh::iter it = mesh->begin(dim); it != mesh->end(dim); ++it) {
+      DGCell* cell = (DGCell*)(*it)->getCell();
+      const double v = cell->densityErrorL2(TACT);
+      per[cellIndex(mc, *it)] = v;
+      total += v;
+    }
+    FILE* f = fopen(P.l2.c_str(), "w");
+    fprintf(f, "%.17g %.17g\n", TACT, sqrt(total));
+    for (int e = 0; e < E; ++e) fprintf(f, "%.17g\n", per[e]);
+    fclose(f);
   }
   if (!P.barth.empty()) {
     for (mMesh::iter it = mesh->begin(dim); it != mesh->end(dim); ++it) {

@@ -79,6 +79,62 @@ BARTH_CASES = {
 }
 
 
+# Workload-size fixtures.  ``config1_scalar_p2_32x32``: the scalar advection
+# workload as its definition states it -- the unit square cut into a 32x32 grid
+# of 2048 jittered triangles (seed 1, +-0.15h), P2, upwind flux, u0 =
+# exp(-((x-0.3)^2+(y-0.3)^2)/0.01), a = (1, 0.5), 200 SSP-RK3 steps at CFL 0.1
+# (the reference's own 6-point volume rule); stores the states at steps 0 and
+# 200, the per-step log, the connectivity and the RHS at t = 0.
+# ``l2_euler_roe_p3``: DGAnalysis::densityErrorL2 of the reference after five
+# steps of the P3 vortex (``l2`` the total, ``l2_cells`` each cell's squared
+# error, ``state`` the final state, ``t`` the final time).
+SIZE_CASES = {
+    "config1_scalar_p2_32x32": ("tri", dict(nx=32, ny=32, seed=1), ["--case", "gauss", "--order", "2"], 200),
+}
+L2_CASES = {
+    "l2_euler_roe_p3": ("tri", dict(nx=8, ny=8, x0=0.0, x1=10.0, y0=0.0, y1=10.0, seed=2),
+                        ["--case", "vortex", "--flux", "roe", "--order", "3"], 5),
+}
+
+
+def run_size_case(name, kind, margs, dargs, steps):
+    mesh = build_mesh(kind, margs)
+    msh = os.path.join(HERE, name + ".msh")
+    meshgen.write_msh_v1(mesh, msh)
+    with tempfile.TemporaryDirectory() as td:
+        conn, rhs, state, log = (os.path.join(td, f) for f in ("c", "r", "s", "l"))
+        cmd = [DRIVER, "--mesh", msh, "--steps", str(steps), "--cfl", "0.1", "--conn", conn, "--rhs", rhs,
+               "--state", state, "--every", str(steps), "--log", log] + dargs
+        subprocess.run(cmd, check=True, capture_output=True)
+        c = np.loadtxt(conn)
+        nf = 5 + (2 if kind == "tri" else 3)
+        r = np.loadtxt(rhs, skiprows=1)
+        blocks = open(state).read().split("step ")[1:]
+        states = np.array([[list(map(float, ln.split())) for ln in b.split("\n")[1:] if ln.strip()]
+                           for b in blocks])
+        lg = np.loadtxt(log, ndmin=2)
+    np.savez_compressed(os.path.join(HERE, name + ".npz"), conn=c[:, :nf].astype(np.int64),
+                        geom=c[:, nf:], states=states, rhs=np.atleast_2d(r), log=lg,
+                        args=np.array(dargs), steps=steps)
+
+
+def run_l2_case(name, kind, margs, dargs, steps):
+    mesh = build_mesh(kind, margs)
+    msh = os.path.join(HERE, name + ".msh")
+    meshgen.write_msh_v1(mesh, msh)
+    with tempfile.TemporaryDirectory() as td:
+        state, l2 = os.path.join(td, "s"), os.path.join(td, "e")
+        cmd = [DRIVER, "--mesh", msh, "--steps", str(steps), "--cfl", "0.1", "--state", state,
+               "--every", str(steps), "--l2", l2] + dargs
+        subprocess.run(cmd, check=True, capture_output=True)
+        blocks = open(state).read().split("step ")[1:]
+        st = np.array([list(map(float, ln.split())) for ln in blocks[-1].split("\n")[1:] if ln.strip()])
+        t, total = map(float, open(l2).readline().split())
+        cells = np.loadtxt(l2, skiprows=1)
+    np.savez_compressed(os.path.join(HERE, name + ".npz"), state=st, t=t, l2=total, l2_cells=cells,
+                        args=np.array(dargs), steps=steps)
+
+
 def run_barth_case(name, kind, margs, dargs, steps):
     mesh = build_mesh(kind, margs)
     msh = os.path.join(HERE, name + ".msh")
@@ -207,6 +263,16 @@ def main():
         if only and name not in only:
             continue
         run_barth_case(name, kind, margs, dargs, steps)
+        print("wrote", name)
+    for name, (kind, margs, dargs, steps) in SIZE_CASES.items():
+        if only and name not in only:
+            continue
+        run_size_case(name, kind, margs, dargs, steps)
+        print("wrote", name)
+    for name, (kind, margs, dargs, steps) in L2_CASES.items():
+        if only and name not in only:
+            continue
+        run_l2_case(name, kind, margs, dargs, steps)
         print("wrote", name)
 
 
