@@ -515,6 +515,8 @@ static int build_solver(dgp_solver s, const std::vector<LawParams>& lps, int fie
     std::vector<double> blob(s->ops.blob_elems);
     s->ops.fill_blob(t.dphi.data(), t.phif.data(), t.phi.data(), t.qw.data(), blob.data());
     if ((rc = s->upload_t(&b.blob, blob))) return rc;
+    s->ops.fill_fused_blob(t.dphi.data(), t.phif.data(), t.phi.data(), t.qw.data(), blob.data());
+    if ((rc = s->upload_t(&b.fblob, blob))) return rc;
     b.blob_bytes = static_cast<int>(s->ops.blob_elems * s->ops.tsize);
   }
   b.nqe = t.nqe;

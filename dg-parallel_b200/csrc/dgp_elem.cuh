@@ -134,11 +134,11 @@ constexpr int kMbarPolls = 1 << 22;  // bound of the bulk-copy wait
 // Last stage, per tile after the update: residual partial of the tile and
 // its contribution to the CFL step of the next step (fused).  Tiles of
 // finished ensemble instances join with active = false (partial 0).
-template <class K>
+template <class K, int LD = K::MNP>
 __device__ __forceinline__ void elem_tile_tail(const StageArgs<typename K::T>& a, TimeCtl* c, int tile,
                                                double rsum, bool active, const double* sC, double* sEig,
                                                int ne, int e0, double* red, const double* sPv, double csz) {
-  constexpr int M = K::M, NP = K::NP, MNP = K::MNP, NV = K::NV, BLOCK = K::BLOCK;
+  constexpr int M = K::M, NP = K::NP, NV = K::NV, BLOCK = K::BLOCK;
   const int tid = threadIdx.x;
   rsum = block_sum<BLOCK>(rsum, red);
   if (tid == 0) a.partials[tile] = rsum;
@@ -147,7 +147,7 @@ __device__ __forceinline__ void elem_tile_tail(const StageArgs<typename K::T>& a
     // reference vertices (DGCell::computeMAXEV, DGCell.cc:1155-1207)
     for (int it = tid; it < ne * NV; it += BLOCK) {
       const int e = it / NV, v = it - (it / NV) * NV;
-      const double* cc = sC + e * MNP;
+      const double* cc = sC + e * LD;
       double val[M];
       if (v == 0) {
 #pragma unroll

@@ -119,6 +119,7 @@ void ops_fused(const DeviceBuffers& b, const double* in, const double* u0, doubl
   a.U0 = u0;
   a.Cout = out;
   a.U0out = u0copy;
+  a.tab.blob = static_cast<const typename K::T*>(b.fblob);
   const size_t smem = FusedSmem<K>::bytes(b.tm.nh_max);
   if (b.cell_inst)
     stage_kernel<K, true><<<ops_grid_elem<K>(b.E), K::BLOCK, smem, st>>>(a);
@@ -298,6 +299,7 @@ Ops make_ops() {
   o.tsize = sizeof(typename K::T);
   o.blob_elems = ElemSmem<K>::blob_elems;
   o.fill_blob = &fill_table_blob<K>;
+  o.fill_fused_blob = &fill_fused_blob<K>;
   o.precision = sizeof(typename K::T) == 8 ? DGP_PRECISION_FP64 : DGP_PRECISION_MIXED;
   o.prepare = &ops_prepare<K>;
   o.stage = &ops_stage<K>;

@@ -33,6 +33,7 @@ struct DeviceBuffers {
   int* bpart = nullptr;
   void* bpphi = nullptr;
   void* blob = nullptr;   // element-kernel tables in shared-memory layout
+  void* fblob = nullptr;  // the fused stage kernel's tables (gradient rows in its G order)
   int blob_bytes = 0;
   void* phi = nullptr;
   void* dphi = nullptr;
@@ -170,6 +171,7 @@ struct Ops {
   // writes the element-kernel table blob (FP64) from dphi [KV][NP], phif [NS][NP],
   // phi [NQ][NP], qw [NQ]
   void (*fill_blob)(const double*, const double*, const double*, const double*, double*) = nullptr;
+  void (*fill_fused_blob)(const double*, const double*, const double*, const double*, double*) = nullptr;
   cudaError_t (*prepare)() = nullptr;
   // one SSP-RK3 stage (face kernel + element kernel); stage 0 writes the RHS
   void (*stage)(const DeviceBuffers&, int stage, double time_factor, int fuse_cfl, cudaStream_t) = nullptr;

@@ -30,40 +30,71 @@
 
 namespace dgp {
 
+// row stride (in elements) of staged rows: a whole, odd number of `unit`-byte
+// vectors, so that rows stay aligned for vector loads and threads reading
+// different rows hit different banks
+constexpr int padded_stride(int n, int esize, int unit) {
+  const int per = unit / esize;                  // elements per vector unit
+  const int s = (n + per - 1) / per * per;       // whole units
+  return ((s / per) % 2 == 1) ? s : s + per;     // odd number of units
+}
+
 template <class K>
 struct FusedSmem {
   using T = typename K::T;
   using L = ElemSmem<K>;
   static constexpr size_t r16(size_t n) { return (n + 15) / 16 * 16; }
-  // table blob | own rows FP64 [TE][MNP] | face slots T [NS][ROWS] | geometry |
-  // union { halo rows FP64 [nh][MNP] (face pass), G T [ROWS][LDK] (volume) }
+  static constexpr bool MIXED = sizeof(T) == 4;
+  // FP64 rows: 16-byte units (2 doubles); FP32 trace rows: 8-byte units (2 floats)
+  static constexpr int RS = padded_stride(K::MNP, 8, 16);
+  static constexpr int RSF = padded_stride(K::MNP, 4, 8);
+  static constexpr int RST = MIXED ? RSF : RS;  // stride of the rows the traces read
+  // table blob | own rows FP64 [TE][RS] | face slots T [NS][ROWS] | geometry |
+  // own rows FP32 [TE][RSF] (mixed) |
+  // union { halo rows FP64 [nh][RS] + FP32 [nh][RSF] (face pass), G T [ROWS][LDK] (volume) }
   static constexpr size_t oC = r16(L::blob_bytes);
-  static constexpr size_t oS = oC + r16((size_t)K::TE * K::MNP * 8);
+  static constexpr size_t oS = oC + r16((size_t)K::TE * RS * 8);
   static constexpr size_t oJ = oS + r16((size_t)K::NS * K::ROWS * sizeof(T));
-  static constexpr size_t oX = oJ + r16(8 * ((size_t)K::TE * L::DD + (size_t)K::TE * K::NV));
+  static constexpr size_t oCf = oJ + r16(8 * ((size_t)K::TE * L::DD + (size_t)K::TE * K::NV));
+  static constexpr size_t oX = oCf + (MIXED ? r16((size_t)K::TE * RSF * 4) : 0);
   static constexpr size_t g_bytes = r16((size_t)K::ROWS * K::LDK * sizeof(T));
-  static constexpr size_t bytes(int nh) {
-    return oX + (r16((size_t)nh * K::MNP * 8) > g_bytes ? r16((size_t)nh * K::MNP * 8) : g_bytes);
-  }
-  // rows can be bulk copied one by one when a row is a whole number of 16-byte units
+  static constexpr size_t halo_bytes(int nh) { return r16((size_t)nh * RS * 8) + (MIXED ? r16((size_t)nh * RSF * 4) : 0); }
+  static constexpr size_t bytes(int nh) { return oX + (halo_bytes(nh) > g_bytes ? halo_bytes(nh) : g_bytes); }
+  // rows are bulk copied one by one when a row is a whole number of 16-byte units
   static constexpr bool bulk_rows = (K::MNP * 8) % 16 == 0;
   static constexpr int HMAX = K::TE * K::NLF;  // a tile's halo never exceeds one cell per own face
+  // at most 128 registers a thread, so that 64k registers hold 512 threads
+  static constexpr int MIN_BLOCKS = 65536 / (K::BLOCK * 128) > 0 ? 65536 / (K::BLOCK * 128) : 1;
 };
 
-// trace of one FP64 row at a face point: U[j] = sum_k phi[k] row[j][k] in T,
-// in the order of the element kernel's volume interpolation
+// host-side table blob of the fused kernel: the element kernel's layout with
+// the reference-gradient rows in the order kk = r * NQ + q of its G rows
 template <class K>
-__device__ __forceinline__ void row_trace(const double* __restrict__ row, const typename K::T* phi,
+void fill_fused_blob(const double* dphi, const double* phif, const double* phi, const double* qw, double* blob) {
+  using L = ElemSmem<K>;
+  constexpr int NP = K::NP, NPP = L::NPP;
+  fill_table_blob<K>(dphi, phif, phi, qw, blob);
+  for (int q = 0; q < K::NQ; ++q)
+    for (int r = 0; r < K::DIM; ++r)
+      for (int k = 0; k < NP; ++k)
+        blob[L::oDphi + (size_t)(r * K::NQ + q) * NPP + k] = dphi[(q * K::DIM + r) * NP + k];
+}
+
+// trace of one row at a face point: U[j] = sum_k phi[k] row[j][k] in T, in the
+// order of the volume interpolation (the rows are the FP64 state, or its FP32
+// copy in the mixed form)
+template <class K>
+__device__ __forceinline__ void row_trace(const typename K::T* __restrict__ row, const typename K::T* phi,
                                           typename K::T* U) {
   using T = typename K::T;
   constexpr int NP = K::NP;
 #pragma unroll
   for (int j = 0; j < K::M; ++j) {
-    double cv[NP];
-    load_vec<double, NP>(row + j * NP, cv);
+    T cv[NP];
+    load_vec<T, NP>(row + j * NP, cv);
     T acc = 0;
 #pragma unroll
-    for (int k = 0; k < NP; ++k) acc += phi[k] * (T)cv[k];
+    for (int k = 0; k < NP; ++k) acc += phi[k] * cv[k];
     U[j] = acc;
   }
 }
@@ -71,15 +102,15 @@ __device__ __forceinline__ void row_trace(const double* __restrict__ row, const 
 // the periodic partner's trace, its basis values at the mirrored point read
 // from global memory
 template <class K>
-__device__ __forceinline__ void row_trace_g(const double* __restrict__ row, const typename K::T* __restrict__ phi,
-                                            typename K::T* U) {
+__device__ __forceinline__ void row_trace_g(const typename K::T* __restrict__ row,
+                                            const typename K::T* __restrict__ phi, typename K::T* U) {
   using T = typename K::T;
   constexpr int NP = K::NP;
 #pragma unroll
   for (int j = 0; j < K::M; ++j) {
     T acc = 0;
 #pragma unroll
-    for (int k = 0; k < NP; ++k) acc += __ldg(phi + k) * (T)row[j * NP + k];
+    for (int k = 0; k < NP; ++k) acc += __ldg(phi + k) * row[j * NP + k];
     U[j] = acc;
   }
 }
@@ -95,18 +126,19 @@ struct FusedTile {
 template <class K, bool ENS, bool CHECK>
 __device__ __forceinline__ bool fused_face_point(const StageArgs<typename K::T>& a, const TimeCtl* c, int inst,
                                                  const FusedTile& ft, int tf, int q, const typename K::T* sPhif,
-                                                 const typename K::T* s_fqw, const int* s_qmap, const double* sC,
-                                                 const double* sH, typename K::T* sS, unsigned char* s_mark) {
+                                                 const typename K::T* s_fqw, const int* s_qmap,
+                                                 const typename K::T* sC, const typename K::T* sH,
+                                                 typename K::T* sS, unsigned char* s_mark) {
   using T = typename K::T;
   using L = ElemSmem<K>;
-  constexpr int M = K::M, MNP = K::MNP, NQF = K::NQF, DIM = K::DIM, TE = K::TE, ROWS = K::ROWS;
-  constexpr int NPP = L::NPP;
+  constexpr int M = K::M, NQF = K::NQF, DIM = K::DIM, TE = K::TE, ROWS = K::ROWS;
+  constexpr int NPP = L::NPP, RST = FusedSmem<K>::RST;
   const int side = a.tm.tf_side[tf], code = a.tm.tf_code[tf];
   const int lL = side & 0xffff, hi = side >> 16;
   const int lfL = code & 15, lfR = (code >> 4) & 15, perm = (code >> 8) & 15;
   const bool ownL = (code >> 12) & 1, ownR = (code >> 13) & 1;
   const int kind = (code >> 14) & 3;
-  auto rowp = [&](int l) -> const double* { return l < TE ? sC + l * MNP : sH + (l - TE) * MNP; };
+  auto rowp = [&](int l) -> const T* { return l < TE ? sC + l * RST : sH + (l - TE) * RST; };
   T n[DIM];
 #pragma unroll
   for (int i = 0; i < DIM; ++i) n[i] = (T)a.tm.tf_nrm[(size_t)tf * DIM + i];
@@ -165,8 +197,9 @@ __device__ __forceinline__ bool fused_face_point(const StageArgs<typename K::T>&
 template <class K, bool ENS, bool CHECK>
 __device__ __forceinline__ bool fused_face_pass(const StageArgs<typename K::T>& a, const TimeCtl* c, int inst,
                                                 const FusedTile& ft, const typename K::T* sPhif,
-                                                const typename K::T* s_fqw, const int* s_qmap, const double* sC,
-                                                const double* sH, typename K::T* sS, unsigned char* s_mark) {
+                                                const typename K::T* s_fqw, const int* s_qmap,
+                                                const typename K::T* sC, const typename K::T* sH,
+                                                typename K::T* sS, unsigned char* s_mark) {
   constexpr int NQF = K::NQF;
   bool mk = false;
   for (int t = threadIdx.x; t < ft.nf * NQF; t += K::BLOCK) {
@@ -177,13 +210,15 @@ __device__ __forceinline__ bool fused_face_pass(const StageArgs<typename K::T>& 
 }
 
 template <class K, bool ENS>
-__global__ void __launch_bounds__(K::BLOCK) stage_kernel(const __grid_constant__ StageArgs<typename K::T> a) {
+__global__ void __launch_bounds__(K::BLOCK, FusedSmem<K>::MIN_BLOCKS)
+    stage_kernel(const __grid_constant__ StageArgs<typename K::T> a) {
   using T = typename K::T;
   using L = ElemSmem<K>;
   using FS = FusedSmem<K>;
   using G = GeoArea<K>;
   constexpr int M = K::M, NP = K::NP, MNP = K::MNP, NQ = K::NQ, NS = K::NS, NQF = K::NQF, DIM = K::DIM;
   constexpr int TE = K::TE, BLOCK = K::BLOCK, ROWS = K::ROWS, KV = K::KV, LDK = K::LDK, NPP = L::NPP;
+  constexpr int RS = FS::RS, RSF = FS::RSF, RST = FS::RST;
   if (a.gctl->done) return;
   extern __shared__ __align__(128) unsigned char smem_raw[];
   T* sT = reinterpret_cast<T*>(smem_raw);
@@ -218,7 +253,7 @@ __global__ void __launch_bounds__(K::BLOCK) stage_kernel(const __grid_constant__
     eend = a.inst_end[inst];
     if (c->done) {
       if (a.stage == 3) {
-        elem_tile_tail<K>(a, c, tile, 0.0, false, nullptr, nullptr, 0, ft.e0, red, nullptr, 0.0);
+        elem_tile_tail<K, RS>(a, c, tile, 0.0, false, nullptr, nullptr, 0, ft.e0, red, nullptr, 0.0);
         elem_finish<K>(a, c, gridDim.x, red);
       }
       return;
@@ -229,7 +264,17 @@ __global__ void __launch_bounds__(K::BLOCK) stage_kernel(const __grid_constant__
   ft.nh = a.tm.th_off[tile + 1] - h0;
   ft.f0 = a.tm.tf_off[tile];
   ft.nf = a.tm.tf_off[tile + 1] - ft.f0;
-  const uint32_t c_bytes = (uint32_t)(((size_t)ft.ne * MNP * 8 + 15) / 16 * 16);
+  // rows the traces and the volume interpolation read: the FP64 rows, or
+  // their FP32 copies (made once per tile) in the mixed form
+  T* sCt;
+  T* sHt;
+  if constexpr (FS::MIXED) {
+    sCt = reinterpret_cast<T*>(smem_raw + FS::oCf);
+    sHt = reinterpret_cast<T*>(smem_raw + FS::oX + FS::r16((size_t)ft.nh * RS * 8));
+  } else {
+    sCt = reinterpret_cast<T*>(sC);
+    sHt = reinterpret_cast<T*>(sH);
+  }
 
   if (tid == 0) {
     s_fail = 0;
@@ -239,29 +284,34 @@ __global__ void __launch_bounds__(K::BLOCK) stage_kernel(const __grid_constant__
   for (int i = tid; i < K::NPERM * NQF; i += BLOCK) s_qmap[i] = a.tab.qmap[i];
   for (int i = tid; i < TE + ft.nh; i += BLOCK) s_mark[i] = 0;
   __syncthreads();
-  // one mbarrier for the tables, the tile's rows and the halo rows; lane 0
-  // announces every byte before any copy is issued
+  // one mbarrier for the tables and every row (own and halo, one bulk copy a
+  // row at the padded stride); lane 0 announces every byte before any copy is
+  // issued
   if (tid < 32) {
     if (tid == 0) {
       uint32_t tx = (uint32_t)L::blob_bytes;
-      if constexpr (FS::bulk_rows) tx += c_bytes + (uint32_t)ft.nh * MNP * 8;
+      if constexpr (FS::bulk_rows) tx += (uint32_t)(ft.ne + ft.nh) * MNP * 8;
       mbar_arrive_expect_tx(&bar, tx);
       bulk_g2s(sT, a.tab.blob, (uint32_t)L::blob_bytes, &bar);
-      if constexpr (FS::bulk_rows) bulk_g2s(sC, a.C + (size_t)ft.e0 * MNP, c_bytes, &bar);
     }
     __syncwarp();
-    if constexpr (FS::bulk_rows)
+    if constexpr (FS::bulk_rows) {
+      for (int l = tid; l < ft.ne; l += 32)
+        bulk_g2s(sC + (size_t)l * RS, a.C + (size_t)(ft.e0 + l) * MNP, (uint32_t)(MNP * 8), &bar);
       for (int h = tid; h < ft.nh; h += 32)
-        bulk_g2s(sH + (size_t)h * MNP, a.C + (size_t)a.tm.th_cell[h0 + h] * MNP, (uint32_t)(MNP * 8), &bar);
+        bulk_g2s(sH + (size_t)h * RS, a.C + (size_t)a.tm.th_cell[h0 + h] * MNP, (uint32_t)(MNP * 8), &bar);
+    }
     // a bound on the first wait counts its polls from the copies' issue
     if (tid == 0 && a.mbar_polls > 0 && !mbar_test_polls(&bar, 0, a.mbar_polls)) s_fail = 1;
   }
   if constexpr (!FS::bulk_rows) {
-    const double* src = a.C + (size_t)ft.e0 * MNP;
-    for (int i = tid; i < ft.ne * MNP; i += BLOCK) sC[i] = src[i];
+    for (int i = tid; i < ft.ne * MNP; i += BLOCK) {
+      const int l = i / MNP;
+      sC[(size_t)l * RS + (i - l * MNP)] = a.C[(size_t)ft.e0 * MNP + i];
+    }
     for (int i = tid; i < ft.nh * MNP; i += BLOCK) {
       const int h = i / MNP;
-      sH[i] = a.C[(size_t)a.tm.th_cell[h0 + h] * MNP + (i - h * MNP)];
+      sH[(size_t)h * RS + (i - h * MNP)] = a.C[(size_t)a.tm.th_cell[h0 + h] * MNP + (i - h * MNP)];
     }
   }
   double csz = 0.0;
@@ -283,20 +333,31 @@ __global__ void __launch_bounds__(K::BLOCK) stage_kernel(const __grid_constant__
     // the tile's output is not written; the last stage still joins the
     // completion count so that the finalize runs and resets it
     if (a.stage == 3) {
-      elem_tile_tail<K>(a, c, tile, 0.0, false, nullptr, nullptr, 0, ft.e0, red, nullptr, 0.0);
+      elem_tile_tail<K, RS>(a, c, tile, 0.0, false, nullptr, nullptr, 0, ft.e0, red, nullptr, 0.0);
       elem_finish<K>(a, c, gridDim.x, red);
     }
     return;
   }
+  if constexpr (FS::MIXED) {
+    // one conversion of every staged row to the arithmetic type
+    for (int i = tid; i < (ft.ne + ft.nh) * MNP; i += BLOCK) {
+      const int l = i / MNP, k = i - l * MNP;
+      if (l < ft.ne)
+        sCt[(size_t)l * RSF + k] = (T)sC[(size_t)l * RS + k];
+      else
+        sHt[(size_t)(l - ft.ne) * RSF + k] = (T)sH[(size_t)(l - ft.ne) * RS + k];
+    }
+    __syncthreads();
+  }
 
   // ---- faces: every face point of the tile's faces into the slots --------
-  bool mk = fused_face_pass<K, ENS, true>(a, c, inst, ft, sPhif, s_fqw, s_qmap, sC, sH, sS, s_mark);
+  bool mk = fused_face_pass<K, ENS, true>(a, c, inst, ft, sPhif, s_fqw, s_qmap, sCt, sHt, sS, s_mark);
   if (a.p0) {
     // halo cells: marked when any of their face-point traces is not physical
     for (int t = tid; t < ft.nh * NS; t += BLOCK) {
       const int h = t / NS, s = t - h * NS;
       T U[M];
-      row_trace<K>(sH + (size_t)h * MNP, sPhif + s * NPP, U);
+      row_trace<K>(sHt + (size_t)h * RST, sPhif + s * NPP, U);
       if (!is_physical<K::LAW, T>(a.law, U)) {
         s_mark[TE + h] = 1;
         mk = true;
@@ -308,11 +369,15 @@ __global__ void __launch_bounds__(K::BLOCK) stage_kernel(const __grid_constant__
         const int l = i / M, j = i - l * M;
         if (l < TE && l >= ft.ne) continue;
         if (!s_mark[l]) continue;
-        double* row = (l < TE ? sC + l * MNP : sH + (size_t)(l - TE) * MNP) + j * NP;
-        for (int k = 1; k < NP; ++k) row[k] = 0.0;
+        T* row = (l < TE ? sCt + l * RST : sHt + (size_t)(l - TE) * RST) + j * NP;
+        for (int k = 1; k < NP; ++k) row[k] = (T)0;
+        if constexpr (FS::MIXED) {
+          if (l < TE)
+            for (int k = 1; k < NP; ++k) sC[(size_t)l * RS + j * NP + k] = 0.0;
+        }
       }
       __syncthreads();
-      fused_face_pass<K, ENS, false>(a, c, inst, ft, sPhif, s_fqw, s_qmap, sC, sH, sS, s_mark);
+      fused_face_pass<K, ENS, false>(a, c, inst, ft, sPhif, s_fqw, s_qmap, sCt, sHt, sS, s_mark);
     }
     // stage 1: the marks persist into u_n for stages 2 and 3
     if (a.stage == 1)
@@ -331,11 +396,11 @@ __global__ void __launch_bounds__(K::BLOCK) stage_kernel(const __grid_constant__
       T U[M];
 #pragma unroll
       for (int j = 0; j < M; ++j) {
-        double cv[NP];
-        load_vec<double, NP>(sC + (e * M + j) * NP, cv);
+        T cv[NP];
+        load_vec<T, NP>(sCt + e * RST + j * NP, cv);
         T acc = 0;
 #pragma unroll
-        for (int k = 0; k < NP; ++k) acc += phi[k] * (T)cv[k];
+        for (int k = 0; k < NP; ++k) acc += phi[k] * cv[k];
         U[j] = acc;
       }
       if (!is_physical<K::LAW, T>(a.law, U)) flag_nonphysical(a.status, ft.e0 + e);
@@ -345,6 +410,8 @@ __global__ void __launch_bounds__(K::BLOCK) stage_kernel(const __grid_constant__
 #pragma unroll
       for (int i = 0; i < DIM * DIM; ++i) J[i] = sJi[e * DIM * DIM + i];
       const T jw = (T)sDet[e] * w;
+      // G[(cell, field)][r * NQ + q]: consecutive points of a cell land in
+      // consecutive words
 #pragma unroll
       for (int j = 0; j < M; ++j)
 #pragma unroll
@@ -352,7 +419,7 @@ __global__ void __launch_bounds__(K::BLOCK) stage_kernel(const __grid_constant__
           T acc = 0;
 #pragma unroll
           for (int i = 0; i < DIM; ++i) acc += F[j][i] * J[i * DIM + r];
-          sG[(e * M + j) * LDK + q * DIM + r] = acc * jw;
+          sG[(e * M + j) * LDK + r * NQ + q] = acc * jw;
         }
     }
   }
@@ -395,14 +462,14 @@ __global__ void __launch_bounds__(K::BLOCK) stage_kernel(const __grid_constant__
 #pragma unroll
       for (int k = 0; k < NPP; ++k) acc[k] += sv * p[k];
     }
+    const int e = row / M, j = row - (row / M) * M;
+    double* crow = sC + (size_t)e * RS + j * NP;
     if (a.stage == 0) {
 #pragma unroll
       for (int k = 0; k < NP; ++k) a.Cout[gbase + k] = (double)acc[k];
     } else {
-      const int e = row / M;
       // FP64 update in the reference's operation order (dt/|J| in FP64)
       const double dtj = c->dt / sDet[e];
-      double* crow = sC + row * NP;
       double cv[NP];
       load_vec<double, NP>(crow, cv);
       if (a.stage == 1 && a.U0out) {
@@ -430,7 +497,7 @@ __global__ void __launch_bounds__(K::BLOCK) stage_kernel(const __grid_constant__
   }
   if (a.stage != 3) return;
   __syncthreads();
-  elem_tile_tail<K>(a, c, tile, rsum, true, sC, sEig, ft.ne, ft.e0, red, sPv, csz);
+  elem_tile_tail<K, RS>(a, c, tile, rsum, true, sC, sEig, ft.ne, ft.e0, red, sPv, csz);
   elem_finish<K>(a, c, gridDim.x, red);
 }
 
