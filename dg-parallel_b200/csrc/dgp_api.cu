@@ -1089,7 +1089,7 @@ int dgp_launches_per_step(dgp_solver s, int* n) {
   }
   const bool lim = s->limiter != DGP_LIMITER_NONE && s->ops.limit;
   const int per_pass = s->limiter == DGP_LIMITER_BARTH ? 1 : 2;
-  *n = 3 * (s->fused ? 1 : s->b.p0 ? 3 : 2) + (lim ? 3 * per_pass + 1 : 0);
+  *n = (s->fused ? 4 : 3 * (s->b.p0 ? 3 : 2)) + (lim ? 3 * per_pass + 1 : 0);
   return DGP_OK;
 }
 

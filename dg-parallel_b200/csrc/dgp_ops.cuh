@@ -125,6 +125,7 @@ void ops_fused(const DeviceBuffers& b, const double* in, const double* u0, doubl
     stage_kernel<K, true><<<ops_grid_elem<K>(b.E), K::BLOCK, smem, st>>>(a);
   else
     stage_kernel<K, false><<<ops_grid_elem<K>(b.E), K::BLOCK, smem, st>>>(a);
+  if (stage == 3) stage_finalize_kernel<K><<<1, kFinalizeThreads, 0, st>>>(a, ops_grid_elem<K>(b.E));
 }
 
 template <class K>

@@ -119,6 +119,66 @@ struct FusedTile {
   int e0, ne, nh, f0, nf;
 };
 
+constexpr int kFinalizeThreads = 1024;
+
+// Last stage, per tile: the residual partial of the tile and the smallest CFL
+// step of its cells (DGCell::computeMAXEV, DGCell.cc:1155-1207: eigenvalue at
+// the mean and, on triangles, at the three reference vertices), written to
+// partials[tile] and partials[ntiles + tile] for stage_finalize_kernel.
+template <class K, int LD>
+__device__ __forceinline__ void fused_tile_tail(const StageArgs<typename K::T>& a, const TimeCtl* c, int tile,
+                                                double rsum, const double* sC, double* sEig, int ne, double* red,
+                                                const double* sPv, double csz) {
+  constexpr int M = K::M, NP = K::NP, NV = K::NV, BLOCK = K::BLOCK;
+  const int tid = threadIdx.x;
+  const int ntiles = (a.mesh.E + K::TE - 1) / K::TE;
+  rsum = block_sum<BLOCK>(rsum, red);
+  if (tid == 0) a.partials[tile] = rsum;
+  if (!a.fuse_cfl) return;
+  for (int it = tid; it < ne * NV; it += BLOCK) {
+    const int e = it / NV, v = it - (it / NV) * NV;
+    const double* cc = sC + e * LD;
+    double val[M];
+    if (v == 0) {
+#pragma unroll
+      for (int j = 0; j < M; ++j) val[j] = cc[j * NP] * a.tab.phi0;
+    } else {
+      const double* pv = sPv + (v - 1) * NP;
+#pragma unroll
+      for (int j = 0; j < M; ++j) {
+        double acc = 0;
+#pragma unroll
+        for (int k = 0; k < NP; ++k) acc += pv[k] * cc[j * NP + k];
+        val[j] = acc;
+      }
+    }
+    sEig[it] = max_eigen<K::LAW, double>(a.law, val);
+  }
+  __syncthreads();
+  double dtl = 1e300;
+  if (tid < ne) {
+    double am = sEig[tid * NV];
+#pragma unroll
+    for (int v = 1; v < NV; ++v) {
+      const double b = sEig[tid * NV + v];
+      am = (b > am ? b : am);
+    }
+    dtl = csz * c->cfl / (am * (2. * K::ORDER + 1.0));
+  }
+  dtl = block_min<BLOCK>(dtl, red);
+  if (tid == 0) a.partials[ntiles + tile] = dtl;
+}
+
+// a tile that computes nothing in the last stage (its instance has finished,
+// or its copies gave up) leaves neutral partials
+template <class K>
+__device__ __forceinline__ void fused_tile_idle(const StageArgs<typename K::T>& a, int tile) {
+  if (a.stage != 3 || threadIdx.x != 0) return;
+  const int ntiles = (a.mesh.E + K::TE - 1) / K::TE;
+  a.partials[tile] = 0.0;
+  a.partials[ntiles + tile] = 1e300;
+}
+
 // One face point of a tile face: traces of both sides from the staged rows,
 // the law's numerical, periodic or boundary flux, and the slots of the own
 // sides.  CHECK: count non-physical own traces and, with the P0 fallback on,
@@ -253,8 +313,7 @@ __global__ void __launch_bounds__(K::BLOCK, FusedSmem<K>::MIN_BLOCKS)
     eend = a.inst_end[inst];
     if (c->done) {
       if (a.stage == 3) {
-        elem_tile_tail<K, RS>(a, c, tile, 0.0, false, nullptr, nullptr, 0, ft.e0, red, nullptr, 0.0);
-        elem_finish<K>(a, c, gridDim.x, red);
+        fused_tile_idle<K>(a, tile);
       }
       return;
     }
@@ -333,8 +392,7 @@ __global__ void __launch_bounds__(K::BLOCK, FusedSmem<K>::MIN_BLOCKS)
     // the tile's output is not written; the last stage still joins the
     // completion count so that the finalize runs and resets it
     if (a.stage == 3) {
-      elem_tile_tail<K, RS>(a, c, tile, 0.0, false, nullptr, nullptr, 0, ft.e0, red, nullptr, 0.0);
-      elem_finish<K>(a, c, gridDim.x, red);
+      fused_tile_idle<K>(a, tile);
     }
     return;
   }
@@ -497,8 +555,62 @@ __global__ void __launch_bounds__(K::BLOCK, FusedSmem<K>::MIN_BLOCKS)
   }
   if (a.stage != 3) return;
   __syncthreads();
-  elem_tile_tail<K, RS>(a, c, tile, rsum, true, sC, sEig, ft.ne, ft.e0, red, sPv, csz);
-  elem_finish<K>(a, c, gridDim.x, red);
+  fused_tile_tail<K, RS>(a, c, tile, rsum, sC, sEig, ft.ne, red, sPv, csz);
+}
+
+// After the last stage: one CTA sums the tiles' residual partials in tile
+// order, takes the minimum of their CFL steps, advances the time and, with the
+// fused CFL, finalizes the next step (per instance for ensembles).  Keeping
+// this out of the stage kernel spares every tile a fence and an atomic round
+// trip on one address.
+template <class K>
+__global__ void __launch_bounds__(kFinalizeThreads) stage_finalize_kernel(
+    const __grid_constant__ StageArgs<typename K::T> a, int ntiles) {
+  constexpr int NT = kFinalizeThreads;
+  __shared__ double red[NT / 32];
+  if (a.gctl->done) return;
+  const double* part = a.partials;
+  const double* dtp = a.partials + ntiles;
+  const int tid = threadIdx.x;
+  if (a.cell_inst) {
+    for (int i = tid; i < a.ninst; i += NT) {
+      TimeCtl* c = a.ctl + i;
+      if (c->done) continue;
+      double r = 0.0, d = 1e300;
+      for (int b = a.tile_first[i]; b < a.tile_first[i + 1]; ++b) {
+        r += part[b];
+        d = fmin(d, dtp[b]);
+      }
+      c->resid = r;
+      c->t = c->t + c->dt;
+      c->steps += 1;
+      if (a.fuse_cfl) {
+        ctl_finalize(c, d);
+        if (c->done) c->t_mark_ns = device_clock_ns();
+      }
+    }
+    __syncthreads();
+    if (tid == 0) {
+      int all = 1;
+      for (int i = 0; i < a.ninst; ++i) all &= (*(volatile int*)&a.ctl[i].done) != 0;
+      a.gctl->done = all;
+    }
+    return;
+  }
+  double r = 0.0, d = 1e300;
+  for (int b = tid; b < ntiles; b += NT) {
+    r += part[b];
+    d = fmin(d, dtp[b]);
+  }
+  r = block_sum<NT>(r, red);
+  d = block_min<NT>(d, red);
+  if (tid == 0) {
+    TimeCtl* c = a.ctl;
+    c->resid = r;
+    c->t = c->t + c->dt;
+    c->steps += 1;
+    if (a.fuse_cfl) ctl_finalize(c, d);
+  }
 }
 
 }  // namespace dgp
