@@ -22,7 +22,10 @@ LIB = os.path.join(HERE, "lib", "libdgp.so")
 INCLUDE = os.path.join(os.path.dirname(HERE), "include")
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+# FP32 division and square root by their fast approximations (the mixed form's
+# right-hand side; FP64 arithmetic is not affected)
 CUFLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC,-O3", "--expt-relaxed-constexpr",
+           "--prec-div=false", "--prec-sqrt=false",
            "-I" + CSRC, "-I" + INCLUDE]
 
 

@@ -515,8 +515,9 @@ static int build_solver(dgp_solver s, const std::vector<LawParams>& lps, int fie
     std::vector<double> blob(s->ops.blob_elems);
     s->ops.fill_blob(t.dphi.data(), t.phif.data(), t.phi.data(), t.qw.data(), blob.data());
     if ((rc = s->upload_t(&b.blob, blob))) return rc;
-    s->ops.fill_fused_blob(t.dphi.data(), t.phif.data(), t.phi.data(), t.qw.data(), blob.data());
-    if ((rc = s->upload_t(&b.fblob, blob))) return rc;
+    std::vector<double> fblob(s->ops.fused_blob_elems, 0.0);
+    s->ops.fill_fused_blob(t.dphi.data(), t.phif.data(), t.phi.data(), t.qw.data(), fblob.data());
+    if ((rc = s->upload_t(&b.fblob, fblob))) return rc;
     b.blob_bytes = static_cast<int>(s->ops.blob_elems * s->ops.tsize);
   }
   b.nqe = t.nqe;

@@ -301,6 +301,7 @@ Ops make_ops() {
   o.blob_elems = ElemSmem<K>::blob_elems;
   o.fill_blob = &fill_table_blob<K>;
   o.fill_fused_blob = &fill_fused_blob<K>;
+  o.fused_blob_elems = FusedSmem<K>::fblob_elems;
   o.precision = sizeof(typename K::T) == 8 ? DGP_PRECISION_FP64 : DGP_PRECISION_MIXED;
   o.prepare = &ops_prepare<K>;
   o.stage = &ops_stage<K>;

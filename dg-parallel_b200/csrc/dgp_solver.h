@@ -172,6 +172,7 @@ struct Ops {
   // phi [NQ][NP], qw [NQ]
   void (*fill_blob)(const double*, const double*, const double*, const double*, double*) = nullptr;
   void (*fill_fused_blob)(const double*, const double*, const double*, const double*, double*) = nullptr;
+  size_t fused_blob_elems = 0;
   cudaError_t (*prepare)() = nullptr;
   // one SSP-RK3 stage (face kernel + element kernel); stage 0 writes the RHS
   void (*stage)(const DeviceBuffers&, int stage, double time_factor, int fuse_cfl, cudaStream_t) = nullptr;

@@ -27,6 +27,7 @@
 #pragma once
 
 #include "dgp_elem.cuh"
+#include "dgp_umma.cuh"
 
 namespace dgp {
 
@@ -49,15 +50,30 @@ struct FusedSmem {
   static constexpr int RS = padded_stride(K::MNP, 8, 16);
   static constexpr int RSF = padded_stride(K::MNP, 4, 8);
   static constexpr int RST = MIXED ? RSF : RS;  // stride of the rows the traces read
+  // The mixed form's volume contraction on the tensor cores (tcgen05, TF32
+  // with split operands): one M = 128 MMA tile covers the tile's rows, N = 16
+  // the modes, K = KPAD the (direction, point) pairs padded to whole k-steps.
+  static constexpr bool UMMA = MIXED && K::BLOCK == 128 && K::ROWS <= 128 && K::NP <= 16;
+  static constexpr int KPAD = (K::KV + 7) / 8 * 8;
+  static constexpr int UN = 16;
+  static constexpr size_t a_bytes = (size_t)128 * KPAD * 4;  // one split part of A
+  static constexpr size_t b_bytes = (size_t)UN * KPAD * 4;   // one split part of B
+  // the fused kernel's table blob: the element kernel's tables, then (tensor
+  // cores) B = the reference gradients as TF32 high and low parts in the MMA layout
+  static constexpr size_t oBhi = L::blob_bytes;
+  static constexpr size_t oBlo = oBhi + b_bytes;
+  static constexpr size_t fblob_bytes = L::blob_bytes + (UMMA ? 2 * b_bytes : 0);
+  static constexpr size_t fblob_elems = fblob_bytes / sizeof(T);
   // table blob | own rows FP64 [TE][RS] | face slots T [NS][ROWS] | geometry |
   // own rows FP32 [TE][RSF] (mixed) |
-  // union { halo rows FP64 [nh][RS] + FP32 [nh][RSF] (face pass), G T [ROWS][LDK] (volume) }
-  static constexpr size_t oC = r16(L::blob_bytes);
+  // union { halo rows FP64 [nh][RS] + FP32 [nh][RSF] (face pass),
+  //         G T [ROWS][LDK] or the MMA's A high and low parts (volume) }
+  static constexpr size_t oC = r16(fblob_bytes);
   static constexpr size_t oS = oC + r16((size_t)K::TE * RS * 8);
   static constexpr size_t oJ = oS + r16((size_t)K::NS * K::ROWS * sizeof(T));
   static constexpr size_t oCf = oJ + r16(8 * ((size_t)K::TE * L::DD + (size_t)K::TE * K::NV));
   static constexpr size_t oX = oCf + (MIXED ? r16((size_t)K::TE * RSF * 4) : 0);
-  static constexpr size_t g_bytes = r16((size_t)K::ROWS * K::LDK * sizeof(T));
+  static constexpr size_t g_bytes = UMMA ? 2 * a_bytes : r16((size_t)K::ROWS * K::LDK * sizeof(T));
   static constexpr size_t halo_bytes(int nh) { return r16((size_t)nh * RS * 8) + (MIXED ? r16((size_t)nh * RSF * 4) : 0); }
   static constexpr size_t bytes(int nh) { return oX + (halo_bytes(nh) > g_bytes ? halo_bytes(nh) : g_bytes); }
   // rows are bulk copied one by one when a row is a whole number of 16-byte units
@@ -73,11 +89,30 @@ template <class K>
 void fill_fused_blob(const double* dphi, const double* phif, const double* phi, const double* qw, double* blob) {
   using L = ElemSmem<K>;
   constexpr int NP = K::NP, NPP = L::NPP;
+  using FS = FusedSmem<K>;
   fill_table_blob<K>(dphi, phif, phi, qw, blob);
   for (int q = 0; q < K::NQ; ++q)
     for (int r = 0; r < K::DIM; ++r)
       for (int k = 0; k < NP; ++k)
         blob[L::oDphi + (size_t)(r * K::NQ + q) * NPP + k] = dphi[(q * K::DIM + r) * NP + k];
+  if constexpr (FS::UMMA) {
+    // B[n][kk] = dphi of row kk = r * NQ + q at mode n, as FP32 split into
+    // TF32 high and low parts, zero beyond the modes and the rows
+    double* bhi = blob + FS::oBhi / 4;
+    double* blo = blob + FS::oBlo / 4;
+    for (int n = 0; n < FS::UN; ++n)
+      for (int kk = 0; kk < FS::KPAD; ++kk) {
+        float v = 0.0f;
+        if (kk < K::KV && n < NP) {
+          const int r = kk / K::NQ, q = kk - r * K::NQ;
+          v = (float)dphi[(q * K::DIM + r) * NP + n];
+        }
+        const float hi = host_tf32(v), lo = host_tf32(v - hi);
+        const uint32_t o = umma_off(n, kk, FS::KPAD) / 4;
+        bhi[o] = hi;
+        blo[o] = lo;
+      }
+  }
 }
 
 // trace of one row at a face point: U[j] = sum_k phi[k] row[j][k] in T, in the
@@ -300,6 +335,8 @@ __global__ void __launch_bounds__(K::BLOCK, FusedSmem<K>::MIN_BLOCKS)
   __shared__ int s_qmap[K::NPERM * NQF];
   __shared__ unsigned char s_mark[TE + FS::HMAX];
   __shared__ double sPv[(K::NV - 1) * NP + 1];
+  __shared__ __align__(8) uint64_t mma_bar;
+  __shared__ uint32_t s_tmem;
 
   const int tid = threadIdx.x;
   const int tile = blockIdx.x;
@@ -338,6 +375,7 @@ __global__ void __launch_bounds__(K::BLOCK, FusedSmem<K>::MIN_BLOCKS)
   if (tid == 0) {
     s_fail = 0;
     mbar_init(&bar, 1);
+    if constexpr (FS::UMMA) mbar_init(&mma_bar, 1);
   }
   for (int i = tid; i < NQF; i += BLOCK) s_fqw[i] = a.tab.fqw[i];
   for (int i = tid; i < K::NPERM * NQF; i += BLOCK) s_qmap[i] = a.tab.qmap[i];
@@ -348,10 +386,10 @@ __global__ void __launch_bounds__(K::BLOCK, FusedSmem<K>::MIN_BLOCKS)
   // issued
   if (tid < 32) {
     if (tid == 0) {
-      uint32_t tx = (uint32_t)L::blob_bytes;
+      uint32_t tx = (uint32_t)FS::fblob_bytes;
       if constexpr (FS::bulk_rows) tx += (uint32_t)(ft.ne + ft.nh) * MNP * 8;
       mbar_arrive_expect_tx(&bar, tx);
-      bulk_g2s(sT, a.tab.blob, (uint32_t)L::blob_bytes, &bar);
+      bulk_g2s(sT, a.tab.blob, (uint32_t)FS::fblob_bytes, &bar);
     }
     __syncwarp();
     if constexpr (FS::bulk_rows) {
@@ -395,6 +433,11 @@ __global__ void __launch_bounds__(K::BLOCK, FusedSmem<K>::MIN_BLOCKS)
       fused_tile_idle<K>(a, tile);
     }
     return;
+  }
+  if constexpr (FS::UMMA) {
+    // 32 columns of tensor memory for D (freed before the kernel returns)
+    if (tid < 32) tmem_alloc(&s_tmem, 32);
+    tc_fence_before();
   }
   if constexpr (FS::MIXED) {
     // one conversion of every staged row to the arithmetic type
@@ -477,9 +520,31 @@ __global__ void __launch_bounds__(K::BLOCK, FusedSmem<K>::MIN_BLOCKS)
           T acc = 0;
 #pragma unroll
           for (int i = 0; i < DIM; ++i) acc += F[j][i] * J[i * DIM + r];
-          sG[(e * M + j) * LDK + r * NQ + q] = acc * jw;
+          if constexpr (FS::UMMA) {
+            // A[(cell, field)][r * NQ + q] as TF32 high and low parts
+            uint32_t hi, lo;
+            tf32_split((float)(acc * jw), hi, lo);
+            const uint32_t o = umma_off(e * M + j, r * NQ + q, FS::KPAD);
+            *reinterpret_cast<uint32_t*>(smem_raw + FS::oX + o) = hi;
+            *reinterpret_cast<uint32_t*>(smem_raw + FS::oX + FS::a_bytes + o) = lo;
+          } else {
+            sG[(e * M + j) * LDK + r * NQ + q] = acc * jw;
+          }
         }
     }
+  }
+  if constexpr (FS::UMMA) {
+    // the padding columns of A are zero (the padding rows of B are): then the
+    // generic writes of A are ordered before the tensor cores read it
+    constexpr int NPAD = FS::KPAD - KV;
+    if constexpr (NPAD > 0) {
+      for (int i = tid; i < 128 * NPAD; i += BLOCK) {
+        const uint32_t o = umma_off(i / NPAD, KV + i % NPAD, FS::KPAD);
+        *reinterpret_cast<uint32_t*>(smem_raw + FS::oX + o) = 0u;
+        *reinterpret_cast<uint32_t*>(smem_raw + FS::oX + FS::a_bytes + o) = 0u;
+      }
+    }
+    fence_proxy_async_smem();
   }
   // u_n of the row (stages 2 and 3) from global memory while the volume and
   // contraction run; stage-1 P0 marks zero its modes k >= 1
@@ -498,19 +563,60 @@ __global__ void __launch_bounds__(K::BLOCK, FusedSmem<K>::MIN_BLOCKS)
   __syncthreads();
 
   // ---- contraction + lift + inverse mass + stage combination ---------------
+  float dv[16];  // the volume contraction of this row from the tensor cores
+  if constexpr (FS::UMMA) {
+    // D[row][mode] = sum over K of A B: per k-step of 8, the products
+    // hi hi + hi lo + lo hi (TF32), accumulated in FP32 in tensor memory
+    tc_fence_after();
+    const uint32_t tmem = s_tmem;
+    if (tid == 0) {
+      constexpr uint32_t idesc = umma_idesc_tf32(128, FS::UN);
+      constexpr uint32_t SBO_A = (FS::KPAD / 4) * 128, SBO_B = SBO_A;
+      const unsigned char* A = smem_raw + FS::oX;
+      const unsigned char* B = smem_raw + FS::oBhi;
+      uint32_t accum = 0;
+#pragma unroll
+      for (int kb = 0; kb < FS::KPAD / 8; ++kb) {
+        const uint32_t ko = (uint32_t)kb * 256;
+        const uint64_t ahi = umma_desc(A + ko, 128, SBO_A), alo = umma_desc(A + FS::a_bytes + ko, 128, SBO_A);
+        const uint64_t bhi = umma_desc(B + ko, 128, SBO_B), blo = umma_desc(B + FS::b_bytes + ko, 128, SBO_B);
+        umma_tf32(tmem, ahi, bhi, idesc, accum);
+        accum = 1;
+        umma_tf32(tmem, ahi, blo, idesc, 1);
+        umma_tf32(tmem, alo, bhi, idesc, 1);
+      }
+      umma_commit(&mma_bar);
+    }
+    if (!mbar_wait(&mma_bar, 0, kMbarPolls)) {
+      // never expected: record it, then wait once more (bounded) so that the
+      // tensor memory is not freed under a running MMA
+      if (tid == 0) atomicAdd(&a.status->timeouts, 1);
+      mbar_wait(&mma_bar, 0, kMbarPolls);
+    }
+    tc_fence_after();
+    tmem_ld16(tmem + ((uint32_t)(tid & ~31) << 16), dv);
+    tc_fence_before();
+    __syncthreads();
+    if (tid < 32) tmem_dealloc(tmem, 32);
+  }
   double rsum = 0.0;
   if (live) {
     T acc[NPP];
 #pragma unroll
     for (int k = 0; k < NPP; ++k) acc[k] = 0;
-    const T* gr = sG + row * LDK;
-#pragma unroll 4
-    for (int kk = 0; kk < KV; ++kk) {
-      const T gv = gr[kk];
-      T d[NPP];
-      load_vec<T, NPP>(sDphi + kk * NPP, d);
+    if constexpr (FS::UMMA) {
 #pragma unroll
-      for (int k = 0; k < NPP; ++k) acc[k] += gv * d[k];
+      for (int k = 0; k < NPP; ++k) acc[k] = k < 16 ? dv[k < 16 ? k : 0] : (T)0;
+    } else {
+      const T* gr = sG + row * LDK;
+#pragma unroll 4
+      for (int kk = 0; kk < KV; ++kk) {
+        const T gv = gr[kk];
+        T d[NPP];
+        load_vec<T, NPP>(sDphi + kk * NPP, d);
+#pragma unroll
+        for (int k = 0; k < NPP; ++k) acc[k] += gv * d[k];
+      }
     }
 #pragma unroll 4
     for (int s = 0; s < NS; ++s) {
