@@ -177,13 +177,13 @@ def cpu_reference(mesh, steps: int, warmup: int, threads: int):
             "steps": int(kv["steps"]), "threads": int(kv["threads"])}
 
 
-def elem_kernel_bytes(E, M, NP, NS, DIM, tsize):
-    """Bytes one element-kernel launch must move: state read, u_n read (stage 1
-    writes it instead), new state written (FP64), face slots read and face-point
-    traces written (right-hand-side type), J^{-1} (right-hand-side type) and
-    |J| (FP64) per cell."""
+def fused_kernel_bytes(E, M, NP, DIM, tsize, with_u0):
+    """Bytes one fused stage-kernel launch must move from and to device memory:
+    the stage input read, u_n read (stages 2 and 3), the output written (FP64
+    state), J^{-1} (right-hand-side type) and |J| (FP64) per cell; the halo
+    rows are neighbours' rows of the same input (counted once)."""
     state = E * M * NP * 8
-    return 3 * state + 2 * E * NS * M * tsize + E * (DIM * DIM * tsize + 8)
+    return (3 if with_u0 else 2) * state + E * (DIM * DIM * tsize + 8)
 
 
 def stage_formula_bytes(E, F, M, NP, DIM):
@@ -218,7 +218,8 @@ def run_reference_arm(args):
             "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": 1e3 * r["seconds"] / r["steps"], "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": dict(WORKLOAD, threads=threads, cpu=cpu_model()),
+            "config": dict(WORKLOAD),
+            "run": {"threads": threads, "cpu": cpu_model()},
             "cpu_baseline": {"value": r["value"], "unit": "DOF-stage/s", "cores": threads,
                              "kind": "reference",
                              "sample": f"{args.steps} SSP-RK3 steps of the full workload after "
@@ -238,6 +239,8 @@ def main():
     ap.add_argument("--impl", default="dgp", choices=["dgp", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--e2e-steps", type=int, default=20)
+    ap.add_argument("--no-adjoint", action="store_true",
+                    help="leave the discrete-adjoint measurement out of the line")
     ap.add_argument("--no-accuracy", action="store_true",
                     help="skip the untimed runs to t = 2 that state the density L2 errors")
     ap.add_argument("--ensemble", action="store_true",
@@ -329,12 +332,19 @@ def main():
     results = {}
     clocks = None
     tiles = {}
-    for name, prec in (("fp64", dgp.FP64), ("mixed", dgp.MIXED)):
-        # tile shape of the element and face kernels from the autotuner
-        # (untimed; a few steps of each built shape on this mesh)
-        best, cand = dgp.autotune(mesh, law, 3, prec, 0, iters=5)
-        tiles[name] = {"block": best, "ms_per_step_64_128_256": cand}
+    for name, prec, tc in (("fp64", dgp.FP64, False), ("mixed", dgp.MIXED, False),
+                           ("mixed_tc", dgp.MIXED, True)):
+        # tile shape of the stage kernel from the autotuner (untimed; a few
+        # steps of each built shape on this mesh); the tensor-core variant of
+        # the mixed form has 128-thread tiles
+        if tc:
+            dgp.tune_set(dgp.LAW_EULER2D, dgp.FLUX_ROE, 2, 3, prec, E, 128)
+        else:
+            best, cand = dgp.autotune(mesh, law, 3, prec, 0, iters=5)
+            tiles[name] = {"block": best, "ms_per_step_64_128_256": cand}
         s = dgp.Solver(mesh, law, 3, prec)
+        if tc:
+            s.set_tensor_cores(True)
         sampler = ClockSampler(local) if (name == "fp64" and rank == 0) else None
         sec, t_end, n = timed_run(s, args.steps, args.warmup, sampler)
         if sampler is not None:
@@ -347,7 +357,7 @@ def main():
                          "gpu_launches": launches,
                          "t_end": t_end, "density_l2_vs_exact": err, "kernel_ms": kern.tolist(),
                          "solver": s}
-    fp64, mixed = results["fp64"], results["mixed"]
+    fp64, mixed, mixed_tc = results["fp64"], results["mixed"], results["mixed_tc"]
     # mixed vs FP64 at the same time: density L2 difference
     c64 = fp64["solver"].get_state()
     c32 = mixed["solver"].get_state()
@@ -357,7 +367,7 @@ def main():
     accuracy = None
     if not args.no_accuracy:
         accuracy = {}
-        for name in ("fp64", "mixed"):
+        for name in ("fp64", "mixed", "mixed_tc"):
             s = results[name]["solver"]
             s.project(0.0)
             w0 = time.perf_counter()
@@ -366,6 +376,8 @@ def main():
                               "wall_s": time.perf_counter() - w0}
         accuracy["mixed_over_fp64_l2"] = (accuracy["mixed"]["density_l2_vs_exact"] /
                                           accuracy["fp64"]["density_l2_vs_exact"])
+        accuracy["mixed_tc_over_fp64_l2"] = (accuracy["mixed_tc"]["density_l2_vs_exact"] /
+                                             accuracy["fp64"]["density_l2_vs_exact"])
         c64 = results["fp64"]["solver"].get_state()
         c32 = results["mixed"]["solver"].get_state()
         accuracy["mixed_density_coeff_rel_diff_vs_fp64"] = float(
@@ -388,30 +400,33 @@ def main():
     e2e_sec = max_over_ranks(time.perf_counter() - w0)
     e2e_value = units_per_step * args.e2e_steps * world / e2e_sec
 
+    # the adjoint of the discrete operator on its own workload (untimed here;
+    # its own CUDA-event times): gradient cost against a forward solve
+    adjoint = None
+    if not args.no_adjoint:
+        adjoint = adjoint_bench()
+
     if rank == 0:
         peaks, peak_src = load_peaks()
-        # dominant kernel per stage and its algorithmic bytes per launch
-        face_ms, elem_ms, elem3_ms = fp64["kernel_ms"]
-        M, NP, NQF, NLF = 4, 10, 4, 3
+        # the fused stage kernel (one launch a stage): stage 1, stage 2 and
+        # the last stage with its CFL reduction (and the one-CTA finalize)
+        s1_ms, s2_ms, s3_ms = fp64["kernel_ms"]
+        stage_ms = (s1_ms + s2_ms + s3_ms) / 3.0
+        M, NP = 4, 10
         F = mesh.nfaces
-        slot_b = E * NLF * NQF * M * 8
-        geo_f = F * (2 * 8 + 8 + 8 + 4)
-        elem_bytes = elem_kernel_bytes(E, M, NP, NLF * NQF, 2, 8)
-        face_bytes = 2 * slot_b + geo_f               # read both sides' traces, write slots, geometry
-        if elem_ms >= face_ms:
-            kname, kms, kbytes = "elem_kernel (volume + lift + RK3 stage)", elem_ms, elem_bytes
-        else:
-            kname, kms, kbytes = "face_kernel (traces + Roe flux + slot scatter)", face_ms, face_bytes
-        achieved = kbytes / (kms * 1e-3) / 1e9
-        # the whole stage (face + element kernel) against the per-element-stage
-        # formula (coefficients, geometry and face data, no intermediates)
+        # algorithmic bytes of a stage by the workload's per-element-stage
+        # formula (coefficients (2 + 2/3) m Np 8, geometry, face data): the
+        # roofline's numerator
         st_bytes = stage_formula_bytes(E, F, M, NP, 2)
-        st_ach = st_bytes / ((face_ms + elem_ms) * 1e-3) / 1e9
+        achieved = st_bytes / (stage_ms * 1e-3) / 1e9
+        kname = "stage_kernel (faces + volume + lift + SSP-RK3 stage, fused; mean of the three stages)"
+        # the bytes the fused kernel itself moves per launch (secondary)
+        own_bytes = (fused_kernel_bytes(E, M, NP, 2, 8, False) + 2 * fused_kernel_bytes(E, M, NP, 2, 8, True)) / 3.0
         traffic = None
         tfile = os.path.join(ROOT, "profiles", "traffic.json")
         if os.path.exists(tfile):
             tr = json.load(open(tfile))
-            traffic = tr.get(kname.split()[0])
+            traffic = tr.get("stage_kernel")
         ms_per_step = fp64["seconds"] / args.steps * 1e3
         cpu = None
         if not args.no_cpu_baseline:
@@ -429,27 +444,33 @@ def main():
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_per_step,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic",
-            "config": dict(WORKLOAD, parallelism=f"replicas{world}",
-                           l2="working set 290 MB > 126 MB L2; each step streams ~1 GB",
-                           tiles=tiles),
+            "config": dict(WORKLOAD),
+            "run": {"parallelism": f"replicas{world}", "tiles": tiles,
+                    "l2": "working set 290 MB > 126 MB L2; each step streams ~1 GB"},
             "mixed": {"value": mixed["value"],
                       "dtype": "f32 RHS (traces, fluxes, contractions, face slots); f64 state, "
                                "RK update, inverse mass, time, totals",
                       "speedup_vs_fp64": mixed["value"] / fp64["value"],
                       "density_l2_vs_exact": mixed["density_l2_vs_exact"],
                       "density_coeff_rel_diff_vs_fp64": mixed["density_coeff_rel_diff_vs_fp64"],
-                      "kernel_ms": mixed["kernel_ms"]},
+                      "kernel_ms": mixed["kernel_ms"],
+                      "tensor_cores": {"value": mixed_tc["value"],
+                                       "contraction": "tcgen05.mma kind::tf32, split high/low operands",
+                                       "speedup_vs_fp64": mixed_tc["value"] / fp64["value"],
+                                       "density_l2_vs_exact": mixed_tc["density_l2_vs_exact"],
+                                       "kernel_ms": mixed_tc["kernel_ms"]}},
             "fp64_density_l2_vs_exact": fp64["density_l2_vs_exact"],
             "accuracy_t2": accuracy,
-            "kernel_ms": {"face": face_ms, "elem": elem_ms, "elem_last_stage_cfl": elem3_ms},
+            "kernel_ms": {"stage1": s1_ms, "stage2": s2_ms, "stage3_cfl": s3_ms},
             "roofline": {"kernel": kname, "bound": "hbm", "achieved": achieved,
                          "peak": peaks.get("hbm_gbs"), "unit": "GB/s",
                          "frac": achieved / peaks.get("hbm_gbs"), "traffic": traffic,
-                         "peak_source": peak_src, "algorithmic_bytes_per_launch": kbytes,
-                         "stage_formula": {"bytes_per_dof_stage": st_bytes / (E * M * NP),
-                                           "bytes_per_stage": st_bytes,
-                                           "stage_ms": face_ms + elem_ms, "achieved": st_ach,
-                                           "frac": st_ach / peaks.get("hbm_gbs")}},
+                         "peak_source": peak_src,
+                         "algorithmic_bytes_per_launch": st_bytes,
+                         "bytes_per_dof_stage": st_bytes / (E * M * NP),
+                         "kernel_own_bytes_per_launch": own_bytes,
+                         "kernel_own_frac": own_bytes / (stage_ms * 1e-3) / 1e9 / peaks.get("hbm_gbs")},
+            "adjoint": adjoint,
             "cpu_baseline": cpu,
             "e2e": {"value": e2e_value, "unit": "DOF-stage/s", "h2d_bytes_per_step": nbytes,
                     "d2h_bytes_per_step": nbytes, "steps": args.e2e_steps,

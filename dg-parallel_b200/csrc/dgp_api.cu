@@ -1204,6 +1204,16 @@ int dgp_set_p0_fallback(dgp_solver s, int on) {
   return DGP_OK;
 }
 
+int dgp_set_tensor_cores(dgp_solver s, int on) {
+  if (!s) return fail(DGP_ERR_INVALID, "null solver");
+  if (on && !(s->fused && s->ops.tensor_cores_ok))
+    return fail(DGP_ERR_UNSUPPORTED,
+                "no tensor-core contraction for this solver (mixed form, 128-thread tiles, at most 16 modes)");
+  s->drop_graphs();
+  s->b.tensor_cores = on ? 1 : 0;
+  return DGP_OK;
+}
+
 int dgp_set_copy_wait_limit(dgp_solver s, int polls) {
   if (!s || polls < 0) return fail(DGP_ERR_INVALID, "bad argument");
   s->drop_graphs();

@@ -45,13 +45,20 @@ cudaError_t ops_prepare() {
 
 // dynamic shared memory of the fused stage kernel may use whatever the static
 // part leaves of the 227 KB a CTA can hold
+template <class K, bool ENS, bool TC>
+cudaError_t fused_prepare_one() {
+  cudaFuncAttributes fa;
+  cudaError_t e = cudaFuncGetAttributes(&fa, stage_kernel<K, ENS, TC>);
+  if (e != cudaSuccess) return e;
+  return cudaFuncSetAttribute(stage_kernel<K, ENS, TC>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              static_cast<int>(kSmemPerCta - fa.sharedSizeBytes));
+}
+
 template <class K, bool ENS>
 cudaError_t fused_prepare() {
-  cudaFuncAttributes fa;
-  cudaError_t e = cudaFuncGetAttributes(&fa, stage_kernel<K, ENS>);
-  if (e != cudaSuccess) return e;
-  return cudaFuncSetAttribute(stage_kernel<K, ENS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                              static_cast<int>(kSmemPerCta - fa.sharedSizeBytes));
+  if constexpr (FusedSmem<K>::UMMA_OK)
+    if (cudaError_t e = fused_prepare_one<K, ENS, true>()) return e;
+  return fused_prepare_one<K, ENS, false>();
 }
 
 template <class K>
@@ -108,7 +115,8 @@ void ops_stage(const DeviceBuffers& b, int stage, double time_factor, int fuse_c
 
 template <class K>
 size_t ops_fused_smem(int nh_max) {
-  return FusedSmem<K>::bytes(nh_max);
+  const size_t a = FusedSmem<K, false>::bytes(nh_max), b = FusedSmem<K, true>::bytes(nh_max);
+  return a > b ? a : b;
 }
 
 template <class K>
@@ -120,11 +128,24 @@ void ops_fused(const DeviceBuffers& b, const double* in, const double* u0, doubl
   a.Cout = out;
   a.U0out = u0copy;
   a.tab.blob = static_cast<const typename K::T*>(b.fblob);
-  const size_t smem = FusedSmem<K>::bytes(b.tm.nh_max);
-  if (b.cell_inst)
-    stage_kernel<K, true><<<ops_grid_elem<K>(b.E), K::BLOCK, smem, st>>>(a);
-  else
-    stage_kernel<K, false><<<ops_grid_elem<K>(b.E), K::BLOCK, smem, st>>>(a);
+  const int grid = ops_grid_elem<K>(b.E);
+  bool tc = false;
+  if constexpr (FusedSmem<K>::UMMA_OK) tc = b.tensor_cores != 0;
+  if (tc) {
+    if constexpr (FusedSmem<K>::UMMA_OK) {
+      const size_t smem = FusedSmem<K, true>::bytes(b.tm.nh_max);
+      if (b.cell_inst)
+        stage_kernel<K, true, true><<<grid, K::BLOCK, smem, st>>>(a);
+      else
+        stage_kernel<K, false, true><<<grid, K::BLOCK, smem, st>>>(a);
+    }
+  } else {
+    const size_t smem = FusedSmem<K, false>::bytes(b.tm.nh_max);
+    if (b.cell_inst)
+      stage_kernel<K, true, false><<<grid, K::BLOCK, smem, st>>>(a);
+    else
+      stage_kernel<K, false, false><<<grid, K::BLOCK, smem, st>>>(a);
+  }
   if (stage == 3) stage_finalize_kernel<K><<<1, kFinalizeThreads, 0, st>>>(a, ops_grid_elem<K>(b.E));
 }
 
@@ -302,6 +323,7 @@ Ops make_ops() {
   o.fill_blob = &fill_table_blob<K>;
   o.fill_fused_blob = &fill_fused_blob<K>;
   o.fused_blob_elems = FusedSmem<K>::fblob_elems;
+  o.tensor_cores_ok = FusedSmem<K>::UMMA_OK;
   o.precision = sizeof(typename K::T) == 8 ? DGP_PRECISION_FP64 : DGP_PRECISION_MIXED;
   o.prepare = &ops_prepare<K>;
   o.stage = &ops_stage<K>;

@@ -61,6 +61,7 @@ struct DeviceBuffers {
   void* X2 = nullptr;
   TileMesh tm{};          // per-tile face records and halos of the fused stage kernel
   int mbar_polls = 0;     // bound of the fused kernel's first bulk-copy wait (0: default)
+  int tensor_cores = 0;   // mixed form: volume contraction on the tensor cores (tcgen05)
   TimeCtl* ctl = nullptr;
   Status* status = nullptr;
   double* partials = nullptr;
@@ -173,6 +174,7 @@ struct Ops {
   void (*fill_blob)(const double*, const double*, const double*, const double*, double*) = nullptr;
   void (*fill_fused_blob)(const double*, const double*, const double*, const double*, double*) = nullptr;
   size_t fused_blob_elems = 0;
+  bool tensor_cores_ok = false;  // the fused kernel has a tensor-core contraction for this shape
   cudaError_t (*prepare)() = nullptr;
   // one SSP-RK3 stage (face kernel + element kernel); stage 0 writes the RHS
   void (*stage)(const DeviceBuffers&, int stage, double time_factor, int fuse_cfl, cudaStream_t) = nullptr;

@@ -4,9 +4,9 @@
 // stage's residual and CFL reductions fused in.
 //
 // The tile reads the stage input rows of its own cells and of its halo (the
-// cells across its faces, periodic partners included), all staged into shared
-// memory by bulk copies on one mbarrier; face-point traces and face slots
-// live in shared memory only.  A face between two tiles is evaluated by both,
+// cells across its faces, periodic partners included), staged into shared
+// memory by 16-byte asynchronous copies (the tables by one bulk copy on an
+// mbarrier); face-point traces and face slots live in shared memory only.  A face between two tiles is evaluated by both,
 // from identical inputs with identical arithmetic, so each side receives the
 // same flux it would get from a separate face pass.  The stage writes a
 // different buffer from the one it reads (u_n -> u1 -> u2 -> u_n in place,
@@ -40,7 +40,7 @@ constexpr int padded_stride(int n, int esize, int unit) {
   return ((s / per) % 2 == 1) ? s : s + per;     // odd number of units
 }
 
-template <class K>
+template <class K, bool TC = false>
 struct FusedSmem {
   using T = typename K::T;
   using L = ElemSmem<K>;
@@ -51,9 +51,11 @@ struct FusedSmem {
   static constexpr int RSF = padded_stride(K::MNP, 4, 8);
   static constexpr int RST = MIXED ? RSF : RS;  // stride of the rows the traces read
   // The mixed form's volume contraction on the tensor cores (tcgen05, TF32
-  // with split operands): one M = 128 MMA tile covers the tile's rows, N = 16
-  // the modes, K = KPAD the (direction, point) pairs padded to whole k-steps.
-  static constexpr bool UMMA = MIXED && K::BLOCK == 128 && K::ROWS <= 128 && K::NP <= 16;
+  // with split operands) where TC asks for it: one M = 128 MMA tile covers
+  // the tile's rows, N = 16 the modes, K = KPAD the (direction, point) pairs
+  // padded to whole k-steps.  UMMA_OK: the shape allows it.
+  static constexpr bool UMMA_OK = MIXED && K::BLOCK == 128 && K::ROWS <= 128 && K::NP <= 16;
+  static constexpr bool UMMA = UMMA_OK && TC;
   static constexpr int KPAD = (K::KV + 7) / 8 * 8;
   static constexpr int UN = 16;
   static constexpr size_t a_bytes = (size_t)128 * KPAD * 4;  // one split part of A
@@ -62,7 +64,7 @@ struct FusedSmem {
   // cores) B = the reference gradients as TF32 high and low parts in the MMA layout
   static constexpr size_t oBhi = L::blob_bytes;
   static constexpr size_t oBlo = oBhi + b_bytes;
-  static constexpr size_t fblob_bytes = L::blob_bytes + (UMMA ? 2 * b_bytes : 0);
+  static constexpr size_t fblob_bytes = L::blob_bytes + (UMMA_OK ? 2 * b_bytes : 0);
   static constexpr size_t fblob_elems = fblob_bytes / sizeof(T);
   // table blob | own rows FP64 [TE][RS] | face slots T [NS][ROWS] | geometry |
   // own rows FP32 [TE][RSF] (mixed) |
@@ -95,7 +97,7 @@ void fill_fused_blob(const double* dphi, const double* phif, const double* phi, 
     for (int r = 0; r < K::DIM; ++r)
       for (int k = 0; k < NP; ++k)
         blob[L::oDphi + (size_t)(r * K::NQ + q) * NPP + k] = dphi[(q * K::DIM + r) * NP + k];
-  if constexpr (FS::UMMA) {
+  if constexpr (FS::UMMA_OK) {
     // B[n][kk] = dphi of row kk = r * NQ + q at mode n, as FP32 split into
     // TF32 high and low parts, zero beyond the modes and the rows
     double* bhi = blob + FS::oBhi / 4;
@@ -304,12 +306,12 @@ __device__ __forceinline__ bool fused_face_pass(const StageArgs<typename K::T>& 
   return mk;
 }
 
-template <class K, bool ENS>
+template <class K, bool ENS, bool TC = false>
 __global__ void __launch_bounds__(K::BLOCK, FusedSmem<K>::MIN_BLOCKS)
     stage_kernel(const __grid_constant__ StageArgs<typename K::T> a) {
   using T = typename K::T;
   using L = ElemSmem<K>;
-  using FS = FusedSmem<K>;
+  using FS = FusedSmem<K, TC>;
   using G = GeoArea<K>;
   constexpr int M = K::M, NP = K::NP, MNP = K::MNP, NQ = K::NQ, NS = K::NS, NQF = K::NQF, DIM = K::DIM;
   constexpr int TE = K::TE, BLOCK = K::BLOCK, ROWS = K::ROWS, KV = K::KV, LDK = K::LDK, NPP = L::NPP;
@@ -380,26 +382,32 @@ __global__ void __launch_bounds__(K::BLOCK, FusedSmem<K>::MIN_BLOCKS)
   for (int i = tid; i < NQF; i += BLOCK) s_fqw[i] = a.tab.fqw[i];
   for (int i = tid; i < K::NPERM * NQF; i += BLOCK) s_qmap[i] = a.tab.qmap[i];
   for (int i = tid; i < TE + ft.nh; i += BLOCK) s_mark[i] = 0;
+  if constexpr (FS::UMMA) {
+    // 32 columns of tensor memory for D, allocated while the copies fly and
+    // freed on every way out of the kernel
+    if (tid < 32) tmem_alloc(&s_tmem, 32);
+    tc_fence_before();
+  }
   __syncthreads();
-  // one mbarrier for the tables and every row (own and halo, one bulk copy a
-  // row at the padded stride); lane 0 announces every byte before any copy is
-  // issued
-  if (tid < 32) {
-    if (tid == 0) {
-      uint32_t tx = (uint32_t)FS::fblob_bytes;
-      if constexpr (FS::bulk_rows) tx += (uint32_t)(ft.ne + ft.nh) * MNP * 8;
-      mbar_arrive_expect_tx(&bar, tx);
-      bulk_g2s(sT, a.tab.blob, (uint32_t)FS::fblob_bytes, &bar);
+  // the tables: one bulk copy on the mbarrier (a bound on its first wait
+  // counts the polls from the copy's issue)
+  if (tid == 0) {
+    mbar_arrive_expect_tx(&bar, (uint32_t)FS::fblob_bytes);
+    bulk_g2s(sT, a.tab.blob, (uint32_t)FS::fblob_bytes, &bar);
+    if (a.mbar_polls > 0 && !mbar_test_polls(&bar, 0, a.mbar_polls)) s_fail = 1;
+  }
+  // the rows (own, then halo) at the padded stride: 16-byte asynchronous
+  // copies spread over every thread, all in flight at once (many small bulk
+  // copies would queue on the SM's one bulk-copy engine)
+  if constexpr (FS::bulk_rows) {
+    constexpr int CH = MNP * 8 / 16;  // 16-byte chunks a row
+    for (int i = tid; i < (ft.ne + ft.nh) * CH; i += BLOCK) {
+      const int l = i / CH, w = i - l * CH;
+      const double* src = (l < ft.ne ? a.C + (size_t)(ft.e0 + l) * MNP
+                                     : a.C + (size_t)a.tm.th_cell[h0 + l - ft.ne] * MNP) + 2 * w;
+      double* dst = (l < ft.ne ? sC + (size_t)l * RS : sH + (size_t)(l - ft.ne) * RS) + 2 * w;
+      cp_async16(dst, src);
     }
-    __syncwarp();
-    if constexpr (FS::bulk_rows) {
-      for (int l = tid; l < ft.ne; l += 32)
-        bulk_g2s(sC + (size_t)l * RS, a.C + (size_t)(ft.e0 + l) * MNP, (uint32_t)(MNP * 8), &bar);
-      for (int h = tid; h < ft.nh; h += 32)
-        bulk_g2s(sH + (size_t)h * RS, a.C + (size_t)a.tm.th_cell[h0 + h] * MNP, (uint32_t)(MNP * 8), &bar);
-    }
-    // a bound on the first wait counts its polls from the copies' issue
-    if (tid == 0 && a.mbar_polls > 0 && !mbar_test_polls(&bar, 0, a.mbar_polls)) s_fail = 1;
   }
   if constexpr (!FS::bulk_rows) {
     for (int i = tid; i < ft.ne * MNP; i += BLOCK) {
@@ -418,6 +426,7 @@ __global__ void __launch_bounds__(K::BLOCK, FusedSmem<K>::MIN_BLOCKS)
   }
   for (int i = tid; i < ft.ne * DIM * DIM; i += BLOCK) sJi[i] = a.mesh.jinv[(size_t)ft.e0 * DIM * DIM + i];
   for (int i = tid; i < ft.ne; i += BLOCK) sDet[i] = a.mesh.detjd[ft.e0 + i];
+  if constexpr (FS::bulk_rows) cp_async_wait_all();
   if (tid == 0 && (s_fail || !mbar_wait(&bar, 0, kMbarPolls))) {
     // record the failure, then wait once more (bounded) for the copies this
     // CTA issued before its shared memory is released
@@ -427,17 +436,16 @@ __global__ void __launch_bounds__(K::BLOCK, FusedSmem<K>::MIN_BLOCKS)
   }
   __syncthreads();
   if (s_fail) {
-    // the tile's output is not written; the last stage still joins the
-    // completion count so that the finalize runs and resets it
+    // the tile's output is not written; the last stage still leaves neutral
+    // partials for the finalize
     if (a.stage == 3) {
       fused_tile_idle<K>(a, tile);
     }
+    if constexpr (FS::UMMA) {
+      tc_fence_after();
+      if (tid < 32) tmem_dealloc(s_tmem, 32);
+    }
     return;
-  }
-  if constexpr (FS::UMMA) {
-    // 32 columns of tensor memory for D (freed before the kernel returns)
-    if (tid < 32) tmem_alloc(&s_tmem, 32);
-    tc_fence_before();
   }
   if constexpr (FS::MIXED) {
     // one conversion of every staged row to the arithmetic type
@@ -563,12 +571,11 @@ __global__ void __launch_bounds__(K::BLOCK, FusedSmem<K>::MIN_BLOCKS)
   __syncthreads();
 
   // ---- contraction + lift + inverse mass + stage combination ---------------
-  float dv[16];  // the volume contraction of this row from the tensor cores
   if constexpr (FS::UMMA) {
     // D[row][mode] = sum over K of A B: per k-step of 8, the products
-    // hi hi + hi lo + lo hi (TF32), accumulated in FP32 in tensor memory
+    // hi hi + hi lo + lo hi (TF32), accumulated in FP32 in tensor memory; the
+    // CUDA cores lift the face slots meanwhile
     tc_fence_after();
-    const uint32_t tmem = s_tmem;
     if (tid == 0) {
       constexpr uint32_t idesc = umma_idesc_tf32(128, FS::UN);
       constexpr uint32_t SBO_A = (FS::KPAD / 4) * 128, SBO_B = SBO_A;
@@ -580,34 +587,20 @@ __global__ void __launch_bounds__(K::BLOCK, FusedSmem<K>::MIN_BLOCKS)
         const uint32_t ko = (uint32_t)kb * 256;
         const uint64_t ahi = umma_desc(A + ko, 128, SBO_A), alo = umma_desc(A + FS::a_bytes + ko, 128, SBO_A);
         const uint64_t bhi = umma_desc(B + ko, 128, SBO_B), blo = umma_desc(B + FS::b_bytes + ko, 128, SBO_B);
-        umma_tf32(tmem, ahi, bhi, idesc, accum);
+        umma_tf32(s_tmem, ahi, bhi, idesc, accum);
         accum = 1;
-        umma_tf32(tmem, ahi, blo, idesc, 1);
-        umma_tf32(tmem, alo, bhi, idesc, 1);
+        umma_tf32(s_tmem, ahi, blo, idesc, 1);
+        umma_tf32(s_tmem, alo, bhi, idesc, 1);
       }
       umma_commit(&mma_bar);
     }
-    if (!mbar_wait(&mma_bar, 0, kMbarPolls)) {
-      // never expected: record it, then wait once more (bounded) so that the
-      // tensor memory is not freed under a running MMA
-      if (tid == 0) atomicAdd(&a.status->timeouts, 1);
-      mbar_wait(&mma_bar, 0, kMbarPolls);
-    }
-    tc_fence_after();
-    tmem_ld16(tmem + ((uint32_t)(tid & ~31) << 16), dv);
-    tc_fence_before();
-    __syncthreads();
-    if (tid < 32) tmem_dealloc(tmem, 32);
   }
   double rsum = 0.0;
+  T acc[NPP];
+#pragma unroll
+  for (int k = 0; k < NPP; ++k) acc[k] = 0;
   if (live) {
-    T acc[NPP];
-#pragma unroll
-    for (int k = 0; k < NPP; ++k) acc[k] = 0;
-    if constexpr (FS::UMMA) {
-#pragma unroll
-      for (int k = 0; k < NPP; ++k) acc[k] = k < 16 ? dv[k < 16 ? k : 0] : (T)0;
-    } else {
+    if constexpr (!FS::UMMA) {
       const T* gr = sG + row * LDK;
 #pragma unroll 4
       for (int kk = 0; kk < KV; ++kk) {
@@ -626,6 +619,21 @@ __global__ void __launch_bounds__(K::BLOCK, FusedSmem<K>::MIN_BLOCKS)
 #pragma unroll
       for (int k = 0; k < NPP; ++k) acc[k] += sv * p[k];
     }
+  }
+  if constexpr (FS::UMMA) {
+    if (!mbar_wait(&mma_bar, 0, kMbarPolls)) {
+      // never expected: record it, then wait once more (bounded) so that the
+      // tensor memory is not read or freed under a running MMA
+      if (tid == 0) atomicAdd(&a.status->timeouts, 1);
+      mbar_wait(&mma_bar, 0, kMbarPolls);
+    }
+    tc_fence_after();
+    float dv[16];
+    tmem_ld16(s_tmem + ((uint32_t)(tid & ~31) << 16), dv);
+#pragma unroll
+    for (int k = 0; k < NPP; ++k) acc[k] += (k < 16 ? dv[k < 16 ? k : 0] : (T)0);
+  }
+  if (live) {
     const int e = row / M, j = row - (row / M) * M;
     double* crow = sC + (size_t)e * RS + j * NP;
     if (a.stage == 0) {
@@ -658,6 +666,11 @@ __global__ void __launch_bounds__(K::BLOCK, FusedSmem<K>::MIN_BLOCKS)
       for (int k = 0; k < NP; ++k) crow[k] = out[k];
       st_vec<double, NP, RALIGN>(a.Cout + gbase, out);
     }
+  }
+  if constexpr (FS::UMMA) {
+    tc_fence_before();
+    __syncthreads();
+    if (tid < 32) tmem_dealloc(s_tmem, 32);
   }
   if (a.stage != 3) return;
   __syncthreads();

@@ -49,6 +49,16 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, int ma
   return ok != 0;
 }
 
+// 16 bytes global -> shared without passing through registers (L2 only);
+// dst and src 16-byte aligned.  Completion: cp_async_wait_all().
+__device__ __forceinline__ void cp_async16(void* dst, const void* src) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smem_u32(dst)), "l"(src) : "memory");
+}
+
+__device__ __forceinline__ void cp_async_wait_all() {
+  asm volatile("cp.async.commit_group;\n cp.async.wait_all;" ::: "memory");
+}
+
 // polls phase `parity` of the barrier without suspending, at most `polls` times
 __device__ __forceinline__ bool mbar_test_polls(uint64_t* bar, uint32_t parity, int polls) {
   uint32_t ok = 0;

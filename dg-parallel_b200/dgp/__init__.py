@@ -91,6 +91,7 @@ def lib() -> ctypes.CDLL:
         "dgp_limiter_triggers": ([P, ctypes.POINTER(ctypes.c_uint8)], I),
         "dgp_set_p0_fallback": ([P, I], I),
         "dgp_set_copy_wait_limit": ([P, I], I),
+        "dgp_set_tensor_cores": ([P, I], I),
         "dgp_launches_per_step": ([P, pI], I),
         "dgp_set_time_stepping": ([P, I, pI], I),
         "dgp_lts_bins": ([P, pI, pI], I),
@@ -337,6 +338,11 @@ class Solver:
 
     def set_p0_fallback(self, on: bool = True):
         check(lib().dgp_set_p0_fallback(self.h, 1 if on else 0))
+
+    def set_tensor_cores(self, on: bool = True):
+        """Mixed form: run the volume contraction on the tcgen05 tensor cores
+        (TF32 with split operands) instead of FP32 FMAs."""
+        check(lib().dgp_set_tensor_cores(self.h, 1 if on else 0))
 
     def set_copy_wait_limit(self, polls: int = 0):
         """Bound the fused stage kernel's first wait for its bulk copies, in

@@ -185,6 +185,14 @@ int dgp_limiter_triggers(dgp_solver s, unsigned char* out);
  * On by default for the Euler laws; 0 turns it off.  Turning it on while local
  * time stepping is on returns DGP_ERR_UNSUPPORTED. */
 int dgp_set_p0_fallback(dgp_solver s, int on);
+/* Mixed form: the volume contraction of the fused stage kernel on the
+ * 5th-generation tensor cores (tcgen05.mma kind::tf32, operands split into
+ * TF32 high and low parts, three products accumulated in FP32 in tensor
+ * memory) instead of FP32 FMAs on the CUDA cores; off by default (it measured
+ * slower on the P3 Euler vortex: a 128-row tile's MMA is too small to hide its
+ * fixed latency).  DGP_ERR_UNSUPPORTED unless the solver is mixed, with
+ * 128-thread tiles and at most 16 modes.  No counterpart in DG-Parallel. */
+int dgp_set_tensor_cores(dgp_solver s, int on);
 /* Bound on the first wait of the fused stage kernel for its bulk copies, in
  * polls counted from the copies' issue (0 restores the default wait, about 4
  * million polls).  A CTA whose wait gives up waits again for its copies with

@@ -125,10 +125,14 @@ def test_run_device_loop_matches_oracle(tmp_path):
     assert rel(s.get_state(), o.state()) < 1e-11
 
 
-def test_mixed_precision_tracks_fp64(tmp_path):
+@pytest.mark.parametrize("tensor_cores", [False, True])
+def test_mixed_precision_tracks_fp64(tmp_path, tensor_cores):
+    """The mixed form (FP32 right-hand side; with tensor_cores, its volume
+    contraction on tcgen05 as split TF32) against the FP64 oracle."""
     msh = _tri(tmp_path, 8, box=(0.0, 10.0), seed=2)
     o = Oracle(msh, dgp.LAW_EULER2D, dgp.FLUX_ROE, 3, dgp.FIELD_VORTEX, VORTEX)
     s = solver_for(msh, dgp.LAW_EULER2D, dgp.FLUX_ROE, dgp.FIELD_VORTEX, 3, VORTEX, dgp.MIXED)
+    s.set_tensor_cores(tensor_cores)
     assert rel(s.get_state(), o.state()) < 1e-6
     t = 0.0
     for _ in range(5):
@@ -137,6 +141,15 @@ def test_mixed_precision_tracks_fp64(tmp_path):
         o.step(t, dt)
         t += dt
     assert rel(s.get_state(), o.state()) < 2e-5
+
+
+def test_tensor_cores_refused_where_not_built(tmp_path):
+    msh = _tri(tmp_path, 4, box=(0.0, 10.0), seed=2)
+    s = solver_for(msh, dgp.LAW_EULER2D, dgp.FLUX_ROE, dgp.FIELD_VORTEX, 3, VORTEX, dgp.FP64)
+    with pytest.raises(dgp.DGPError) as ei:
+        s.set_tensor_cores(True)
+    assert ei.value.code == -3
+    s.set_tensor_cores(False)
 
 
 def test_state_roundtrip_and_totals(tmp_path):
