@@ -249,6 +249,9 @@ def main():
                     help="--ensemble: end time of the instances (a short run for launch lists)")
     ap.add_argument("--adjoint", action="store_true",
                     help="only the discrete-adjoint measurement (Euler vortex 128x128x2 P2, 400 steps)")
+    ap.add_argument("--decompose", action="store_true",
+                    help="only the error decomposition of the mixed form (the vortex to t = 2 with "
+                         "groups of terms rounded to FP32, ~3 min)")
     ap.add_argument("--configs", action="store_true",
                     help="only the other workloads: scalar P2 on 2048 triangles (200 steps) and "
                          "Maxwell P2 on 663552 tets (one TM110 period), both forms, ~2 min")
@@ -280,6 +283,11 @@ def main():
         if ranks.rank == 0:
             print(json.dumps({"ensemble": out}))
         ranks.close()
+        return 0
+    if args.decompose:
+        import torch
+        torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+        print(json.dumps({"decompose": decompose_bench()}))
         return 0
     if args.configs:
         import torch
@@ -483,6 +491,40 @@ def main():
         r["solver"].close()
     ranks.close()
     return 0
+
+
+def decompose_bench(tend=2.0):
+    """Error decomposition of the mixed form on the bench workload (the vortex
+    to t = 2): the FP64 solver with one group of terms rounded to FP32 at a
+    time (dgp_set_rounding_probe), every group together, and the mixed form
+    itself; density L2 error against the exact vortex for each."""
+    import dgp
+    m = make_mesh()
+    mesh = dgp.Mesh.from_arrays(2, m.vertices, m.cells, 100, m.bfaces, m.btags)
+    law = dgp.Law(dgp.LAW_EULER2D, dgp.FLUX_ROE, dgp.FIELD_VORTEX, vortex_params())
+    dgp.tune_set(dgp.LAW_EULER2D, dgp.FLUX_ROE, 2, 3, dgp.FP64, m.cells.shape[0], 128)
+    names = {0: "fp64", 1: "geometry", 2: "face traces", 4: "volume values", 8: "volume flux products",
+             16: "face slots", 32: "contraction result", 64: "tables", 127: "all of the above"}
+    rows = []
+    for mask, name in names.items():
+        s = dgp.Solver(mesh, law, 3, dgp.FP64)
+        s.set_rounding_probe(mask)
+        s.project(0.0)
+        t, n = s.run(0.0, tend, 0.1)
+        rows.append({"rounded_to_fp32": name, "mask": mask, "steps": n, "density_l2_vs_exact": s.l2_error(t, 0)})
+        s.close()
+    for name, tc in (("mixed form (FP32 right-hand side)", False), ("mixed form, tensor-core contraction", True)):
+        s = dgp.Solver(mesh, law, 3, dgp.MIXED)
+        if tc:
+            s.set_tensor_cores(True)
+        s.project(0.0)
+        t, n = s.run(0.0, tend, 0.1)
+        rows.append({"rounded_to_fp32": name, "steps": n, "density_l2_vs_exact": s.l2_error(t, 0)})
+        s.close()
+    base = rows[0]["density_l2_vs_exact"]
+    for r in rows:
+        r["over_fp64"] = r["density_l2_vs_exact"] / base
+    return {"workload": WORKLOAD["workload"], "t": tend, "rows": rows}
 
 
 def ensemble_bench(n=96, seed=6, tend=0.5, ranks=None):

@@ -1214,6 +1214,16 @@ int dgp_set_tensor_cores(dgp_solver s, int on) {
   return DGP_OK;
 }
 
+int dgp_set_rounding_probe(dgp_solver s, int mask) {
+  if (!s || mask < 0 || mask > 127) return fail(DGP_ERR_INVALID, "bad argument");
+  if (mask && !(s->fused && s->ops.probe_ok && s->meshes.size() == 1))
+    return fail(DGP_ERR_UNSUPPORTED, "the rounding probe is built for the FP64 P3 Euler (Roe) solver "
+                                     "with 128-thread tiles");
+  s->drop_graphs();
+  s->b.round_mask = mask;
+  return DGP_OK;
+}
+
 int dgp_set_copy_wait_limit(dgp_solver s, int polls) {
   if (!s || polls < 0) return fail(DGP_ERR_INVALID, "bad argument");
   s->drop_graphs();

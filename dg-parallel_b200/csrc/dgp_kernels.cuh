@@ -169,6 +169,7 @@ struct StageArgs {
   DevTables<T> tab;
   TileMesh tm;
   int mbar_polls;  // bound of the first bulk-copy wait of the fused stage kernel (0: default)
+  int round_mask;  // rounding probe of the fused stage kernel (0: off)
   LawParams law;
   // the state is FP64 in both forms; T is the arithmetic of the RHS
   const double* C;   // state the stage reads

@@ -58,6 +58,14 @@ template <class K, bool ENS>
 cudaError_t fused_prepare() {
   if constexpr (FusedSmem<K>::UMMA_OK)
     if (cudaError_t e = fused_prepare_one<K, ENS, true>()) return e;
+  if constexpr (probe_built<K>() && !ENS) {
+    cudaFuncAttributes fa;
+    cudaError_t e = cudaFuncGetAttributes(&fa, stage_kernel<K, false, false, true>);
+    if (e != cudaSuccess) return e;
+    e = cudaFuncSetAttribute(stage_kernel<K, false, false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             static_cast<int>(kSmemPerCta - fa.sharedSizeBytes));
+    if (e != cudaSuccess) return e;
+  }
   return fused_prepare_one<K, ENS, false>();
 }
 
@@ -129,6 +137,13 @@ void ops_fused(const DeviceBuffers& b, const double* in, const double* u0, doubl
   a.U0out = u0copy;
   a.tab.blob = static_cast<const typename K::T*>(b.fblob);
   const int grid = ops_grid_elem<K>(b.E);
+  if constexpr (probe_built<K>()) {
+    if (b.round_mask && !b.cell_inst) {
+      stage_kernel<K, false, false, true><<<grid, K::BLOCK, FusedSmem<K, false>::bytes(b.tm.nh_max), st>>>(a);
+      if (stage == 3) stage_finalize_kernel<K><<<1, kFinalizeThreads, 0, st>>>(a, grid);
+      return;
+    }
+  }
   bool tc = false;
   if constexpr (FusedSmem<K>::UMMA_OK) tc = b.tensor_cores != 0;
   if (tc) {
@@ -324,6 +339,7 @@ Ops make_ops() {
   o.fill_fused_blob = &fill_fused_blob<K>;
   o.fused_blob_elems = FusedSmem<K>::fblob_elems;
   o.tensor_cores_ok = FusedSmem<K>::UMMA_OK;
+  o.probe_ok = probe_built<K>();
   o.precision = sizeof(typename K::T) == 8 ? DGP_PRECISION_FP64 : DGP_PRECISION_MIXED;
   o.prepare = &ops_prepare<K>;
   o.stage = &ops_stage<K>;

@@ -62,6 +62,7 @@ struct DeviceBuffers {
   TileMesh tm{};          // per-tile face records and halos of the fused stage kernel
   int mbar_polls = 0;     // bound of the fused kernel's first bulk-copy wait (0: default)
   int tensor_cores = 0;   // mixed form: volume contraction on the tensor cores (tcgen05)
+  int round_mask = 0;     // FP64 rounding probe of the fused kernel (error decomposition; 0: off)
   TimeCtl* ctl = nullptr;
   Status* status = nullptr;
   double* partials = nullptr;
@@ -129,6 +130,7 @@ inline StageArgs<T> make_args(const DeviceBuffers& b) {
   a.law = b.law;
   a.tm = b.tm;
   a.mbar_polls = b.mbar_polls;
+  a.round_mask = b.round_mask;
   a.C = static_cast<const double*>(b.C);
   a.U0 = static_cast<const double*>(b.U0);
   a.Cout = static_cast<double*>(b.Cout ? b.Cout : b.C);
@@ -175,6 +177,7 @@ struct Ops {
   void (*fill_fused_blob)(const double*, const double*, const double*, const double*, double*) = nullptr;
   size_t fused_blob_elems = 0;
   bool tensor_cores_ok = false;  // the fused kernel has a tensor-core contraction for this shape
+  bool probe_ok = false;         // the fused kernel has the rounding probe for this configuration
   cudaError_t (*prepare)() = nullptr;
   // one SSP-RK3 stage (face kernel + element kernel); stage 0 writes the RHS
   void (*stage)(const DeviceBuffers&, int stage, double time_factor, int fuse_cfl, cudaStream_t) = nullptr;

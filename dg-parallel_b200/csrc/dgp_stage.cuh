@@ -156,6 +156,32 @@ struct FusedTile {
   int e0, ne, nh, f0, nf;
 };
 
+// Rounding probe (error decomposition of the mixed form): with RND, the terms
+// whose bit is set in the mask are rounded to FP32 inside the FP64 kernel.
+// Bits: geometry (J^{-1}, |J| w, face normals, |J_f| w), face-point traces,
+// volume-point values, volume flux products G, face slots, the contraction's
+// result, the reference tables.
+enum : int {
+  kRndGeometry = 1, kRndTraces = 2, kRndVolumeValues = 4, kRndVolumeFlux = 8, kRndSlots = 16,
+  kRndContraction = 32, kRndTables = 64
+};
+
+template <bool RND, typename T>
+__device__ __forceinline__ T probe(T x, int mask, int bit) {
+  if constexpr (RND) {
+    if (mask & bit) return (T)(float)x;
+  }
+  return x;
+}
+
+// the one configuration the probe is built for: the FP64 P3 Euler vortex
+// workload with Roe flux and 128-thread tiles
+template <class K>
+constexpr bool probe_built() {
+  return sizeof(typename K::T) == 8 && K::LAW == DGP_LAW_EULER2D && K::FLUX == DGP_FLUX_ROE && K::DIM == 2 &&
+         K::ORDER == 3 && K::BLOCK == 128;
+}
+
 constexpr int kFinalizeThreads = 1024;
 
 // Last stage, per tile: the residual partial of the tile and the smallest CFL
@@ -220,7 +246,7 @@ __device__ __forceinline__ void fused_tile_idle(const StageArgs<typename K::T>& 
 // the law's numerical, periodic or boundary flux, and the slots of the own
 // sides.  CHECK: count non-physical own traces and, with the P0 fallback on,
 // mark their cells (returns true when it marked one).
-template <class K, bool ENS, bool CHECK>
+template <class K, bool ENS, bool CHECK, bool RND = false>
 __device__ __forceinline__ bool fused_face_point(const StageArgs<typename K::T>& a, const TimeCtl* c, int inst,
                                                  const FusedTile& ft, int tf, int q, const typename K::T* sPhif,
                                                  const typename K::T* s_fqw, const int* s_qmap,
@@ -238,11 +264,15 @@ __device__ __forceinline__ bool fused_face_point(const StageArgs<typename K::T>&
   auto rowp = [&](int l) -> const T* { return l < TE ? sC + l * RST : sH + (l - TE) * RST; };
   T n[DIM];
 #pragma unroll
-  for (int i = 0; i < DIM; ++i) n[i] = (T)a.tm.tf_nrm[(size_t)tf * DIM + i];
-  const T jw = (T)a.tm.tf_fj[tf] * s_fqw[q];
+  for (int i = 0; i < DIM; ++i) n[i] = probe<RND, T>((T)a.tm.tf_nrm[(size_t)tf * DIM + i], a.round_mask, kRndGeometry);
+  const T jw = probe<RND, T>((T)a.tm.tf_fj[tf] * s_fqw[q], a.round_mask, kRndGeometry);
   bool marked = false;
   T UL[M], UR[M], flux[M];
   row_trace<K>(rowp(lL), sPhif + (lfL * NQF + q) * NPP, UL);
+  if constexpr (RND) {
+#pragma unroll
+    for (int j = 0; j < M; ++j) UL[j] = probe<RND, T>(UL[j], a.round_mask, kRndTraces);
+  }
   if (CHECK && ownL && !is_physical<K::LAW, T>(a.law, UL)) {
     flag_nonphysical(a.status, ft.e0 + lL);
     if (a.p0) {
@@ -255,6 +285,10 @@ __device__ __forceinline__ bool fused_face_point(const StageArgs<typename K::T>&
     const int lR = hi - 1;
     qR = s_qmap[perm * NQF + q];
     row_trace<K>(rowp(lR), sPhif + (lfR * NQF + qR) * NPP, UR);
+    if constexpr (RND) {
+#pragma unroll
+      for (int j = 0; j < M; ++j) UR[j] = probe<RND, T>(UR[j], a.round_mask, kRndTraces);
+    }
     if (CHECK && ownR && !is_physical<K::LAW, T>(a.law, UR)) {
       flag_nonphysical(a.status, ft.e0 + lR);
       if (a.p0) {
@@ -281,17 +315,17 @@ __device__ __forceinline__ bool fused_face_point(const StageArgs<typename K::T>&
   if (ownL) {
     T* dst = sS + (lfL * NQF + q) * ROWS + lL * M;
 #pragma unroll
-    for (int j = 0; j < M; ++j) dst[j] = -flux[j] * jw;
+    for (int j = 0; j < M; ++j) dst[j] = probe<RND, T>(-flux[j] * jw, a.round_mask, kRndSlots);
   }
   if (kind == 0 && ownR) {
     T* dst = sS + (lfR * NQF + qR) * ROWS + (hi - 1) * M;
 #pragma unroll
-    for (int j = 0; j < M; ++j) dst[j] = flux[j] * jw;
+    for (int j = 0; j < M; ++j) dst[j] = probe<RND, T>(flux[j] * jw, a.round_mask, kRndSlots);
   }
   return marked;
 }
 
-template <class K, bool ENS, bool CHECK>
+template <class K, bool ENS, bool CHECK, bool RND = false>
 __device__ __forceinline__ bool fused_face_pass(const StageArgs<typename K::T>& a, const TimeCtl* c, int inst,
                                                 const FusedTile& ft, const typename K::T* sPhif,
                                                 const typename K::T* s_fqw, const int* s_qmap,
@@ -301,12 +335,12 @@ __device__ __forceinline__ bool fused_face_pass(const StageArgs<typename K::T>& 
   bool mk = false;
   for (int t = threadIdx.x; t < ft.nf * NQF; t += K::BLOCK) {
     const int f = t / NQF, q = t - f * NQF;
-    mk |= fused_face_point<K, ENS, CHECK>(a, c, inst, ft, ft.f0 + f, q, sPhif, s_fqw, s_qmap, sC, sH, sS, s_mark);
+    mk |= fused_face_point<K, ENS, CHECK, RND>(a, c, inst, ft, ft.f0 + f, q, sPhif, s_fqw, s_qmap, sC, sH, sS, s_mark);
   }
   return mk;
 }
 
-template <class K, bool ENS, bool TC = false>
+template <class K, bool ENS, bool TC = false, bool RND = false>
 __global__ void __launch_bounds__(K::BLOCK, FusedSmem<K>::MIN_BLOCKS)
     stage_kernel(const __grid_constant__ StageArgs<typename K::T> a) {
   using T = typename K::T;
@@ -460,7 +494,13 @@ __global__ void __launch_bounds__(K::BLOCK, FusedSmem<K>::MIN_BLOCKS)
   }
 
   // ---- faces: every face point of the tile's faces into the slots --------
-  bool mk = fused_face_pass<K, ENS, true>(a, c, inst, ft, sPhif, s_fqw, s_qmap, sCt, sHt, sS, s_mark);
+  if constexpr (RND) {
+    if (a.round_mask & kRndTables) {
+      for (int i = tid; i < (int)(L::blob_bytes / sizeof(T)); i += BLOCK) sT[i] = (T)(float)sT[i];
+      __syncthreads();
+    }
+  }
+  bool mk = fused_face_pass<K, ENS, true, RND>(a, c, inst, ft, sPhif, s_fqw, s_qmap, sCt, sHt, sS, s_mark);
   if (a.p0) {
     // halo cells: marked when any of their face-point traces is not physical
     for (int t = tid; t < ft.nh * NS; t += BLOCK) {
@@ -486,7 +526,7 @@ __global__ void __launch_bounds__(K::BLOCK, FusedSmem<K>::MIN_BLOCKS)
         }
       }
       __syncthreads();
-      fused_face_pass<K, ENS, false>(a, c, inst, ft, sPhif, s_fqw, s_qmap, sCt, sHt, sS, s_mark);
+      fused_face_pass<K, ENS, false, RND>(a, c, inst, ft, sPhif, s_fqw, s_qmap, sCt, sHt, sS, s_mark);
     }
     // stage 1: the marks persist into u_n for stages 2 and 3
     if (a.stage == 1)
@@ -512,13 +552,17 @@ __global__ void __launch_bounds__(K::BLOCK, FusedSmem<K>::MIN_BLOCKS)
         for (int k = 0; k < NP; ++k) acc += phi[k] * cv[k];
         U[j] = acc;
       }
+      if constexpr (RND) {
+#pragma unroll
+        for (int j = 0; j < M; ++j) U[j] = probe<RND, T>(U[j], a.round_mask, kRndVolumeValues);
+      }
       if (!is_physical<K::LAW, T>(a.law, U)) flag_nonphysical(a.status, ft.e0 + e);
       T F[M][DIM];
       volume_flux<K::LAW, DIM, T>(a.law, U, F);
       T J[DIM * DIM];
 #pragma unroll
-      for (int i = 0; i < DIM * DIM; ++i) J[i] = sJi[e * DIM * DIM + i];
-      const T jw = (T)sDet[e] * w;
+      for (int i = 0; i < DIM * DIM; ++i) J[i] = probe<RND, T>(sJi[e * DIM * DIM + i], a.round_mask, kRndGeometry);
+      const T jw = probe<RND, T>((T)sDet[e] * w, a.round_mask, kRndGeometry);
       // G[(cell, field)][r * NQ + q]: consecutive points of a cell land in
       // consecutive words
 #pragma unroll
@@ -536,7 +580,7 @@ __global__ void __launch_bounds__(K::BLOCK, FusedSmem<K>::MIN_BLOCKS)
             *reinterpret_cast<uint32_t*>(smem_raw + FS::oX + o) = hi;
             *reinterpret_cast<uint32_t*>(smem_raw + FS::oX + FS::a_bytes + o) = lo;
           } else {
-            sG[(e * M + j) * LDK + r * NQ + q] = acc * jw;
+            sG[(e * M + j) * LDK + r * NQ + q] = probe<RND, T>(acc * jw, a.round_mask, kRndVolumeFlux);
           }
         }
     }
@@ -651,7 +695,7 @@ __global__ void __launch_bounds__(K::BLOCK, FusedSmem<K>::MIN_BLOCKS)
       double out[NP];
 #pragma unroll
       for (int k = 0; k < NP; ++k) {
-        const double r = (double)acc[k];
+        const double r = probe<RND, double>((double)acc[k], a.round_mask, kRndContraction);
         if (a.stage == 1) {
           out[k] = cv[k] + r * dtj;
         } else if (a.stage == 2) {

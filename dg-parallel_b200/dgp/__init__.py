@@ -92,6 +92,7 @@ def lib() -> ctypes.CDLL:
         "dgp_set_p0_fallback": ([P, I], I),
         "dgp_set_copy_wait_limit": ([P, I], I),
         "dgp_set_tensor_cores": ([P, I], I),
+        "dgp_set_rounding_probe": ([P, I], I),
         "dgp_launches_per_step": ([P, pI], I),
         "dgp_set_time_stepping": ([P, I, pI], I),
         "dgp_lts_bins": ([P, pI, pI], I),
@@ -343,6 +344,12 @@ class Solver:
         """Mixed form: run the volume contraction on the tcgen05 tensor cores
         (TF32 with split operands) instead of FP32 FMAs."""
         check(lib().dgp_set_tensor_cores(self.h, 1 if on else 0))
+
+    def set_rounding_probe(self, mask: int = 0):
+        """FP64 solver: round the terms selected by mask to FP32 (1 geometry,
+        2 face traces, 4 volume values, 8 volume flux products, 16 face slots,
+        32 contraction result, 64 tables) -- the mixed form's error, term by term."""
+        check(lib().dgp_set_rounding_probe(self.h, int(mask)))
 
     def set_copy_wait_limit(self, polls: int = 0):
         """Bound the fused stage kernel's first wait for its bulk copies, in

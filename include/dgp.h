@@ -193,6 +193,14 @@ int dgp_set_p0_fallback(dgp_solver s, int on);
  * fixed latency).  DGP_ERR_UNSUPPORTED unless the solver is mixed, with
  * 128-thread tiles and at most 16 modes.  No counterpart in DG-Parallel. */
 int dgp_set_tensor_cores(dgp_solver s, int on);
+/* Rounding probe for the error decomposition of the mixed form: in the FP64
+ * fused stage kernel, the terms selected by mask are rounded to FP32 (1 the
+ * geometry: J^{-1}, |J| w, face normals, |J_f| w; 2 the face-point traces; 4
+ * the volume-point values; 8 the volume flux products; 16 the face slots; 32
+ * the contraction's result; 64 the reference tables); 0 turns it off.  Built
+ * for the FP64 P3 Euler (Roe) solver with 128-thread tiles
+ * (DGP_ERR_UNSUPPORTED elsewhere).  No counterpart in DG-Parallel. */
+int dgp_set_rounding_probe(dgp_solver s, int mask);
 /* Bound on the first wait of the fused stage kernel for its bulk copies, in
  * polls counted from the copies' issue (0 restores the default wait, about 4
  * million polls).  A CTA whose wait gives up waits again for its copies with

@@ -143,6 +143,36 @@ def test_mixed_precision_tracks_fp64(tmp_path, tensor_cores):
     assert rel(s.get_state(), o.state()) < 2e-5
 
 
+def test_rounding_probe_perturbs_at_fp32_level(tmp_path):
+    """The FP64 kernel with terms rounded to FP32: no mask leaves the FP64
+    result; each mask moves it by FP32 rounding, never more than the mixed form."""
+    msh = _tri(tmp_path, 8, box=(0.0, 10.0), seed=2)
+    o = Oracle(msh, dgp.LAW_EULER2D, dgp.FLUX_ROE, 3, dgp.FIELD_VORTEX, VORTEX)
+    dts = []
+    t = 0.0
+    for _ in range(3):
+        dts.append(o.cfl_dt(0.1))
+        o.step(t, dts[-1])
+        t += dts[-1]
+    ref = o.state()
+    for mask in (0, 1, 2, 4, 8, 16, 32, 64, 127):
+        s = solver_for(msh, dgp.LAW_EULER2D, dgp.FLUX_ROE, dgp.FIELD_VORTEX, 3, VORTEX)
+        s.set_rounding_probe(mask)
+        t = 0.0
+        for dt in dts:
+            s.step(t, dt)
+            t += dt
+        err = rel(s.get_state(), ref)
+        if mask == 0:
+            assert err < FP64_TOL
+        else:
+            assert 1e-12 < err < 2e-5, (mask, err)
+    u = solver_for(msh, dgp.LAW_SCALAR, dgp.FLUX_UPWIND, dgp.FIELD_GAUSS, 2, SCALAR2D)
+    with pytest.raises(dgp.DGPError) as ei:
+        u.set_rounding_probe(2)
+    assert ei.value.code == -3
+
+
 def test_tensor_cores_refused_where_not_built(tmp_path):
     msh = _tri(tmp_path, 4, box=(0.0, 10.0), seed=2)
     s = solver_for(msh, dgp.LAW_EULER2D, dgp.FLUX_ROE, dgp.FIELD_VORTEX, 3, VORTEX, dgp.FP64)
