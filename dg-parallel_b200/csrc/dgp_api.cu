@@ -47,6 +47,7 @@ void ensure_registry() {
     register_euler2d_llf_ops();
     register_euler3d_ops();
     register_maxwell3d_ops();
+    register_maxwell2d_ops();
     register_burgers_tile_ops();
     register_euler2d_roe_tile_ops();
   });
@@ -723,9 +724,9 @@ int dgp_mesh_destroy(dgp_mesh m) {
 
 int dgp_law_create(int kind, int flux, int field, const double* params, dgp_law* out) {
   if (!out) return fail(DGP_ERR_INVALID, "null output handle");
-  if (kind < DGP_LAW_SCALAR || kind > DGP_LAW_MAXWELL3D) return fail(DGP_ERR_INVALID, "unknown law");
+  if (kind < DGP_LAW_SCALAR || kind > DGP_LAW_MAXWELL2D) return fail(DGP_ERR_INVALID, "unknown law");
   if (flux < DGP_FLUX_UPWIND || flux > DGP_FLUX_LLF) return fail(DGP_ERR_INVALID, "unknown flux");
-  if (field < DGP_FIELD_GAUSS || field > DGP_FIELD_TM110) return fail(DGP_ERR_INVALID, "unknown field");
+  if (field < DGP_FIELD_GAUSS || field > DGP_FIELD_TM2D) return fail(DGP_ERR_INVALID, "unknown field");
   auto* l = new dgp_law_s;
   l->kind = kind;
   l->flux = flux;
@@ -751,7 +752,8 @@ int dgp_solver_create(dgp_mesh mh, dgp_law law, int order, int precision, int li
   const HostMesh& m = mh->m;
   if (limiter == DGP_LIMITER_MOMENT && m.dim != 2)
     return fail(DGP_ERR_UNSUPPORTED, "the moment limiter is built for triangles only");
-  if ((law->kind == DGP_LAW_EULER2D || law->kind == DGP_LAW_BURGERS2D) && m.dim != 2)
+  if ((law->kind == DGP_LAW_EULER2D || law->kind == DGP_LAW_BURGERS2D || law->kind == DGP_LAW_MAXWELL2D) &&
+      m.dim != 2)
     return fail(DGP_ERR_UNSUPPORTED, "2D law on a 3D mesh");
   if ((law->kind == DGP_LAW_EULER3D || law->kind == DGP_LAW_MAXWELL3D) && m.dim != 3)
     return fail(DGP_ERR_UNSUPPORTED, "3D law on a 2D mesh");
@@ -1403,7 +1405,8 @@ int dgp_ensemble_create(int n, const dgp_mesh* meshes, const dgp_law* laws, cons
     if (!meshes[i] || !laws[i]) return fail(DGP_ERR_INVALID, "null mesh or law");
     const HostMesh& m = meshes[i]->m;
     const dgp_law_s* l = laws[i];
-    if ((l->kind == DGP_LAW_EULER2D || l->kind == DGP_LAW_BURGERS2D) && m.dim != 2)
+    if ((l->kind == DGP_LAW_EULER2D || l->kind == DGP_LAW_BURGERS2D || l->kind == DGP_LAW_MAXWELL2D) &&
+        m.dim != 2)
       return fail(DGP_ERR_UNSUPPORTED, "2D law on a 3D mesh");
     if ((l->kind == DGP_LAW_EULER3D || l->kind == DGP_LAW_MAXWELL3D) && m.dim != 3)
       return fail(DGP_ERR_UNSUPPORTED, "3D law on a 2D mesh");

@@ -23,6 +23,8 @@ template <>
 struct LawTraits<DGP_LAW_EULER3D> { static constexpr int M = 5; };
 template <>
 struct LawTraits<DGP_LAW_MAXWELL3D> { static constexpr int M = 6; };
+template <>
+struct LawTraits<DGP_LAW_MAXWELL2D> { static constexpr int M = 3; };
 
 // Law parameters as they reach the device (DGP_NPARAMS doubles, see dgp.h)
 struct LawParams {
@@ -76,6 +78,15 @@ __device__ __forceinline__ void field_eval(const LawParams& lp, const double* x,
     case DGP_FIELD_SINE:
       q[0] = (T)(0.5 + p[9] * sin(2.0 * kPi * (x[0] + x[1])));
       break;
+    case DGP_FIELD_TM2D: {  // the same mode in Maxwell2d's field order (Hx, Hy, Ez)
+      double L = p[10] > 0 ? p[10] : 1.0;
+      double k = kPi / L, w = kPi * sqrt(2.0) / L;
+      double sx = sin(k * x[0]), cx = cos(k * x[0]), sy = sin(k * x[1]), cy = cos(k * x[1]);
+      q[0] = (T)(-(k / w) * sx * cy * sin(w * t));
+      q[1] = (T)((k / w) * cx * sy * sin(w * t));
+      q[2] = (T)(sx * sy * cos(w * t));
+      break;
+    }
     case DGP_FIELD_TM110: {
       double L = p[10] > 0 ? p[10] : 1.0;
       double k = kPi / L, w = kPi * sqrt(2.0) / L;
@@ -124,6 +135,10 @@ __device__ __forceinline__ void volume_flux(const LawParams& lp, const T* Q, T (
     F[4][0] = q14; F[4][1] = q24; F[4][2] = q44 + p;
     T qq = invrho * (Q[3] + p);
     F[3][0] = Q[1] * qq; F[3][1] = Q[2] * qq; F[3][2] = Q[4] * qq;
+  } else if constexpr (LAW == DGP_LAW_MAXWELL2D) {  // Maxwell2d::Fi, MaxwellLaw.cc:21-37, Q = (Hx, Hy, Ez)
+    F[0][0] = 0;     F[0][1] = Q[2];
+    F[1][0] = -Q[2]; F[1][1] = 0;
+    F[2][0] = -Q[1]; F[2][1] = Q[0];
   } else {  // 3D Maxwell, eps = mu = 1: dE/dt = curl H, dH/dt = -curl E, so
             // F_E e_i = -(e_i x H) and F_H e_i = e_i x E
     const T *E = Q, *H = Q + 3;
@@ -357,6 +372,21 @@ __device__ __forceinline__ void numerical_flux(const LawParams& lp, const T* n, 
     flux[2] = flux[0] * (n1 * vnav + t[1] * vtav + sv[1] * vsav) + pav * n1;
     flux[4] = flux[0] * (n2 * vnav + t[2] * vtav + sv[2] * vsav) + pav * n2;
     flux[3] = vnav * (pav / (g - (T)1) + pav + (T)0.5 * rhoav * (vnav * vnav + vtav * vtav + vsav * vsav));
+  } else if constexpr (LAW == DGP_LAW_MAXWELL2D) {
+    // Maxwell2d::riemannSolver (MaxwellLaw.cc:137-195): the interface state
+    // uR2 of its characteristic split, written as the reference condenses it,
+    // then Maxwell2d::Fi(uR2) . n
+    const T nx = n[0], ny = n[1];
+    T uR2[3];
+    uR2[0] = (u0[0] + u1[0]) * (nx * ny / (T)2 + ny * ny / (T)2) + (u0[1] + u1[1]) * (nx * nx / (T)2 - nx * ny / (T)2) +
+             (u0[2] - u1[2]) * ny / (T)2;
+    uR2[1] = (u0[0] + u1[0]) * (-nx * ny / (T)2 + ny * ny / (T)2) +
+             (u0[1] + u1[1]) * (nx * nx / (T)2 + nx * ny / (T)2) + (u0[2] - u1[2]) * (-nx) / (T)2;
+    uR2[2] = ny * (u0[0] - u1[0]) / (T)2 + nx * (u1[1] - u0[1]) / (T)2 + (u0[2] + u1[2]) / (T)2;
+    T f[M][DIM];
+    volume_flux<LAW, DIM, T>(lp, uR2, f);
+#pragma unroll
+    for (int i = 0; i < 3; ++i) flux[i] = f[i][0] * nx + f[i][1] * ny;
   } else {  // Maxwell upwind: F*_E = -n x {H} + n x (n x [E])/2, F*_H = n x {E} + n x (n x [H])/2
     T Ea[3], Ha[3], dE[3], dH[3];
 #pragma unroll
@@ -427,6 +457,19 @@ __device__ __forceinline__ void boundary_flux(const LawParams& lp, int bid, cons
     numerical_flux<LAW, FLUX, DIM, T>(lp, n, Q, f, flux);
   } else if constexpr (LAW == DGP_LAW_EULER3D) {
     field_eval<T>(lp, x, time, f);
+    numerical_flux<LAW, FLUX, DIM, T>(lp, n, Q, f, flux);
+  } else if constexpr (LAW == DGP_LAW_MAXWELL2D) {
+    // Maxwell2d::boundaryFlux (MaxwellLaw.cc:113-133): reflection on 40000
+    // (H mirrored about the face, Ez kept), far field elsewhere, both through
+    // the Riemann solver
+    if (bid == 40000) {
+      const T Hdotn = Q[0] * n[0] + Q[1] * n[1];
+      f[0] = -Q[0] + (T)2 * n[0] * Hdotn;
+      f[1] = -Q[1] + (T)2 * n[1] * Hdotn;
+      f[2] = Q[2];
+    } else {
+      field_eval<T>(lp, x, time, f);
+    }
     numerical_flux<LAW, FLUX, DIM, T>(lp, n, Q, f, flux);
   } else {  // Maxwell: PEC ghost (E -> -E, H -> H) on 40000, far field elsewhere
     if (bid == 40000) {

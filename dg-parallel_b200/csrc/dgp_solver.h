@@ -230,6 +230,7 @@ void register_euler2d_roe_ops();
 void register_euler2d_llf_ops();
 void register_euler3d_ops();
 void register_maxwell3d_ops();
+void register_maxwell2d_ops();
 void register_burgers_tile_ops();
 void register_euler2d_roe_tile_ops();
 

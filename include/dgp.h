@@ -30,6 +30,8 @@ extern "C" {
 #define DGP_LAW_EULER2D 2   /* Euler2d / Euler2dRoe (EulerLaw.cc) */
 #define DGP_LAW_EULER3D 3   /* Euler3d (EulerLaw.cc) */
 #define DGP_LAW_MAXWELL3D 4 /* 3D Maxwell on tets (no counterpart; Maxwell2d is 2D only) */
+#define DGP_LAW_MAXWELL2D 5 /* Maxwell2d (MaxwellLaw.cc): fields Hx, Hy, Ez; its riemannSolver
+                             * (MaxwellLaw.cc:137-195) whatever flux id is given */
 
 /* numerical fluxes (ConservationLaw::riemannSolver overrides) */
 #define DGP_FLUX_UPWIND 0  /* ScalarLaw::riemannSolver, Maxwell upwind */
@@ -48,6 +50,8 @@ extern "C" {
 #define DGP_FIELD_SINE 3    /* 0.5 + A sin(2 pi (x + y)) */
 #define DGP_FIELD_GAUSS3D 4 /* exp(-|x - c - a t|^2 / s), 3D */
 #define DGP_FIELD_TM110 5   /* TM110 mode of the PEC cube [0,L]^3 */
+#define DGP_FIELD_TM2D 6    /* (Hx, Hy, Ez) of the mode Ez = sin(pi x/L) sin(pi y/L) cos(w t),
+                             * w = pi sqrt(2)/L, of Maxwell2d's equations on [0,L]^2 */
 
 /* law / field parameters: double[16]
  *  [0..2] advection velocity a   [3..5] centre c   [6] width s

@@ -234,6 +234,17 @@ void or_field_eval(const or_solver* s, const double* x, double t, double* q) {
     case OR_FIELD_SINE:
       q[0] = 0.5 + p[9] * sin(2.0 * kPi * (x[0] + x[1]));
       break;
+    case OR_FIELD_TM2D: {
+      /* the TM mode Ez = sin(pi x/L) sin(pi y/L) cos(w t) of Maxwell2d's
+       * equations, fields (Hx, Hy, Ez) */
+      double L = p[10] > 0 ? p[10] : 1.0;
+      double k = kPi / L, w = kPi * sqrt(2.0) / L;
+      double sx = sin(k * x[0]), cx = cos(k * x[0]), sy = sin(k * x[1]), cy = cos(k * x[1]);
+      q[0] = -(k / w) * sx * cy * sin(w * t);
+      q[1] = (k / w) * cx * sy * sin(w * t);
+      q[2] = sx * sy * cos(w * t);
+      break;
+    }
     case OR_FIELD_TM110: {
       /* TM110 mode of the PEC cube [0,L]^3: fields (Ex,Ey,Ez,Hx,Hy,Hz) */
       double L = p[10] > 0 ? p[10] : 1.0;
@@ -292,6 +303,11 @@ static void law_flux(const or_solver* s, const double* x, const double* Q, doubl
       F[3][0] = Q[1] * qq; F[3][1] = Q[2] * qq; F[3][2] = Q[4] * qq;
       break;
     }
+    case OR_MAXWELL2D: /* Maxwell2d::Fi, MaxwellLaw.cc:21-37, Q = (Hx, Hy, Ez) */
+      F[0][0] = 0.0;   F[0][1] = Q[2];  F[0][2] = 0.0;
+      F[1][0] = -Q[2]; F[1][1] = 0.0;   F[1][2] = 0.0;
+      F[2][0] = -Q[1]; F[2][1] = Q[0];  F[2][2] = 0.0;
+      break;
     case OR_MAXWELL3D: {
       /* dE/dt - curl H = 0, dH/dt + curl E = 0 (eps = mu = 1):
        * F_E . n = -(n x H), F_H . n = n x E */
@@ -547,6 +563,21 @@ static void riemann_flux(const or_solver* s, const double* n, const double* x, c
       flux[3] = vnav * (pav / (g - 1.) + pav + 0.5 * rhoav * (vnav * vnav + vtav * vtav + vsav * vsav));
       break;
     }
+    case OR_MAXWELL2D: {
+      /* Maxwell2d::riemannSolver, MaxwellLaw.cc:137-195: the interface state of
+       * its characteristic split in the reference's condensed form, then
+       * Maxwell2d::Fi(uR2) . n */
+      const double nx = n[0], ny = n[1];
+      double uR2[3], F2[MAXM][3];
+      uR2[0] = (u0[0] + u1[0]) * (nx * ny / 2 + ny * ny / 2) + (u0[1] + u1[1]) * (nx * nx / 2 - nx * ny / 2) +
+               (u0[2] - u1[2]) * ny / 2;
+      uR2[1] = (u0[0] + u1[0]) * (-nx * ny / 2 + ny * ny / 2) + (u0[1] + u1[1]) * (nx * nx / 2 + nx * ny / 2) +
+               (u0[2] - u1[2]) * (-nx) / 2;
+      uR2[2] = ny * (u0[0] - u1[0]) / 2 + nx * (u1[1] - u0[1]) / 2 + (u0[2] + u1[2]) / 2;
+      law_flux(s, x, uR2, F2);
+      for (int i = 0; i < 3; ++i) flux[i] = dot3(F2[i], n);
+      break;
+    }
     case OR_MAXWELL3D: {
       /* upwind flux (eps = mu = 1): F*_E = -n x {H} + 1/2 n x (n x [E]),
        *                             F*_H =  n x {E} + 1/2 n x (n x [H]),
@@ -626,6 +657,17 @@ static void boundary_flux(const or_solver* s, int bid, const double* n, const do
       or_field_eval(s, x, T, f);
       riemann_flux(s, n, x, Q, f, flux);
       return;
+    case OR_MAXWELL2D:
+      if (bid == 40000) { /* Maxwell2d::boundaryFlux reflection, MaxwellLaw.cc:113-125 */
+        double Hdotn = Q[0] * n[0] + Q[1] * n[1];
+        f[0] = -Q[0] + 2 * n[0] * Hdotn;
+        f[1] = -Q[1] + 2 * n[1] * Hdotn;
+        f[2] = Q[2];
+      } else { /* far field, MaxwellLaw.cc:126-131 */
+        or_field_eval(s, x, T, f);
+      }
+      riemann_flux(s, n, x, Q, f, flux);
+      return;
     case OR_MAXWELL3D:
       if (bid == 40000) { /* perfect electric conductor: ghost E = -E, H = H */
         for (int i = 0; i < 3; ++i) {
@@ -660,6 +702,7 @@ static double max_eigen(const or_solver* s, const double* Q) {
       return c + sqrt(v2);
     }
     case OR_MAXWELL3D: return 1.0;
+    case OR_MAXWELL2D: return 1.0; /* Maxwell2d::maximumEigenValue, MaxwellLaw.cc:197-200 */
   }
   return 1.0;
 }
@@ -1056,6 +1099,7 @@ or_solver* or_create(const char* msh_path, int law, int flux, int order, int fie
     case OR_SCALAR: case OR_BURGERS2D: s->m = 1; break;
     case OR_EULER2D: s->m = 4; break;
     case OR_EULER3D: s->m = 5; break;
+    case OR_MAXWELL2D: s->m = 3; break;
     default: s->m = 6;
   }
   /* rules need the dimension: read the mesh first */

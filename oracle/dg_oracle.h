@@ -18,12 +18,12 @@
 extern "C" {
 #endif
 
-enum { OR_SCALAR = 0, OR_BURGERS2D = 1, OR_EULER2D = 2, OR_EULER3D = 3, OR_MAXWELL3D = 4 };
+enum { OR_SCALAR = 0, OR_BURGERS2D = 1, OR_EULER2D = 2, OR_EULER3D = 3, OR_MAXWELL3D = 4, OR_MAXWELL2D = 5 };
 enum { OR_FLUX_UPWIND = 0, OR_FLUX_CENTRAL = 1, OR_FLUX_GODUNOV = 2, OR_FLUX_ROE = 3,
        OR_FLUX_LLF = 4 };
 /* analytic fields used as initial condition, far field and exact solution */
 enum { OR_FIELD_GAUSS = 0, OR_FIELD_VORTEX = 1, OR_FIELD_PULSE3D = 2, OR_FIELD_SINE = 3,
-       OR_FIELD_GAUSS3D = 4, OR_FIELD_TM110 = 5 };
+       OR_FIELD_GAUSS3D = 4, OR_FIELD_TM110 = 5, OR_FIELD_TM2D = 6 };
 
 /* field parameters (16 doubles):
  *  [0..2] advection velocity a      [3..5] centre c       [6] width s

@@ -67,6 +67,8 @@
 //             Euler2dRoe with --flux roe); exact solution as far field.
 //   pulse3d   3D Euler (Euler3d) density pulse advected by a uniform flow.
 //   sine      Burgers2D with u0 = 0.5 + A sin(2 pi (x+y)) as far field.
+//   tm2d      Maxwell2d (MaxwellLaw.cc) with a TM cavity mode (TM2DField) as
+//             initial state and far field; faces tagged 40000 reflect.
 //   gauss3d   scalar advection on tets, 3D Gaussian.
 #include <cmath>
 #include <cstdio>
@@ -94,6 +96,7 @@
 #include "TimeIntegrator.h"
 #include "ScalarLaw.h"
 #include "EulerLaw.h"
+#include "MaxwellLaw.h"
 #include "Burgers.h"
 #include "FieldEvaluator.h"
 #include "DGLimiter.h"
@@ -207,6 +210,7 @@ struct Params {
   double gamma = 1.4, beta = 5.0, vx0 = 5.0, vy0 = 5.0;
   // burgers
   double amp = 1.0;
+  double L = 1.0;  // tm2d cavity side
 };
 static Params P;
 
@@ -272,6 +276,23 @@ class Pulse3DField : public FieldEvaluator {
     q[2] = rho * P.ay;
     q[4] = rho * P.az;
     q[3] = pr / (P.gamma - 1.0) + 0.5 * rho * (P.ax * P.ax + P.ay * P.ay + P.az * P.az);
+  }
+  int order() const { return 0; }
+};
+
+// the TM mode Ez = sin(pi x/L) sin(pi y/L) cos(w t), w = pi sqrt(2)/L, of
+// Maxwell2d's equations (dHx/dt = -dEz/dy, dHy/dt = dEz/dx, dEz/dt = dHy/dx -
+// dHx/dy), fields (Hx, Hy, Ez); L = --L (default 1)
+class TM2DField : public FieldEvaluator {
+ public:
+  void eval(const mPoint& x, double t, double* v) const {
+    mPoint& p = const_cast<mPoint&>(x);
+    const double L = P.L > 0 ? P.L : 1.0;
+    const double k = kPi / L, w = kPi * sqrt(2.0) / L;
+    const double sx = sin(k * p(0)), cx = cos(k * p(0)), sy = sin(k * p(1)), cy = cos(k * p(1));
+    v[0] = -(k / w) * sx * cy * sin(w * t);
+    v[1] = (k / w) * cx * sy * sin(w * t);
+    v[2] = sx * sy * cos(w * t);
   }
   int order() const { return 0; }
 };
@@ -412,6 +433,7 @@ int main(int argc, char** argv) {
     else if (a == "--x0") P.vx0 = atof(v);
     else if (a == "--y0") P.vy0 = atof(v);
     else if (a == "--amp") P.amp = atof(v);
+    else if (a == "--L") P.L = atof(v);
     else usage();
     ++i;
   }
@@ -460,6 +482,7 @@ int main(int argc, char** argv) {
   VortexField vortex;
   Pulse3DField pulse;
   SineField sine;
+  TM2DField tm2d;
   std::set<int> walls;
   ConservationLaw* law = 0;
   if (P.caseName == "gauss") law = new ScalarLaw(&gauss, &vel, &gauss);
@@ -469,6 +492,7 @@ int main(int argc, char** argv) {
     else law = new Euler2d(walls, &vortex, P.gamma);
   } else if (P.caseName == "pulse3d") law = new Euler3d(walls, &pulse, P.gamma);
   else if (P.caseName == "sine") law = new Burgers2D(&sine, &sine);
+  else if (P.caseName == "tm2d") law = new Maxwell2d(walls, &tm2d);
   else usage();
   const int m = law->getNbFields();
 

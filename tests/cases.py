@@ -44,6 +44,11 @@ GOLDEN_CASES = {
     # periodic edges (510 left/right, 610 bottom/top) on [-1,1]^2
     "scalar_periodic_p2": (dgp.LAW_SCALAR, dgp.FLUX_UPWIND, dgp.FIELD_GAUSS, 2, SCALAR_PERIODIC),
     "burgers_periodic_p3": (dgp.LAW_BURGERS2D, dgp.FLUX_CENTRAL, dgp.FIELD_SINE, 3, SINE),
+    # Maxwell2d, TM cavity mode (far field; reflection on 40000)
+    "maxwell2d_p1": (dgp.LAW_MAXWELL2D, dgp.FLUX_UPWIND, dgp.FIELD_TM2D, 1, TM110),
+    "maxwell2d_p2": (dgp.LAW_MAXWELL2D, dgp.FLUX_UPWIND, dgp.FIELD_TM2D, 2, TM110),
+    "maxwell2d_p3": (dgp.LAW_MAXWELL2D, dgp.FLUX_UPWIND, dgp.FIELD_TM2D, 3, TM110),
+    "maxwell2d_wall_p2": (dgp.LAW_MAXWELL2D, dgp.FLUX_UPWIND, dgp.FIELD_TM2D, 2, TM110),
 }
 
 # Relative tolerance (max abs difference / max abs value) of the oracle -- exact

@@ -60,6 +60,12 @@ CASES = {
     "scalar_periodic_p2": ("tri", PERIODIC_BOX, ["--case", "gauss", "--order", "2", "--cx", "0.2",
                                                   "--cy", "-0.1", "--s", "0.1"], 4),
     "burgers_periodic_p3": ("tri", PERIODIC_BOX, ["--case", "sine", "--order", "3", "--amp", "0.25"], 4),
+    # Maxwell2d (MaxwellLaw.cc) with a TM cavity mode: far field, and the
+    # reflection of faces tagged 40000
+    "maxwell2d_p1": ("tri", SQUARE, ["--case", "tm2d", "--order", "1"], 3),
+    "maxwell2d_p2": ("tri", SQUARE, ["--case", "tm2d", "--order", "2"], 3),
+    "maxwell2d_p3": ("tri", SQUARE, ["--case", "tm2d", "--order", "3"], 3),
+    "maxwell2d_wall_p2": ("tri", dict(SQUARE, boundary_tag=40000), ["--case", "tm2d", "--order", "2"], 3),
 }
 
 
