@@ -737,6 +737,25 @@ int dgp_law_create(int kind, int flux, int field, const double* params, dgp_law*
   return DGP_OK;
 }
 
+int dgp_law_set_bc(dgp_law l, int boundary_id, int bc_kind) {
+  if (!l) return fail(DGP_ERR_INVALID, "null law");
+  if (bc_kind < DGP_BC_DEFAULT || bc_kind > DGP_BC_WALL) return fail(DGP_ERR_INVALID, "unknown boundary condition");
+  if (boundary_id == 510 || boundary_id == 610)
+    return fail(DGP_ERR_INVALID, "510 and 610 are periodic edges, not boundary conditions");
+  if (bc_kind == DGP_BC_WALL && (l->kind == DGP_LAW_SCALAR || l->kind == DGP_LAW_BURGERS2D))
+    return fail(DGP_ERR_UNSUPPORTED, "no wall condition for the scalar laws");
+  for (int i = 0; i < l->nbc; ++i)
+    if (l->bc_id[i] == boundary_id) {
+      l->bc_kind[i] = bc_kind;
+      return DGP_OK;
+    }
+  if (l->nbc == DGP_MAX_BC) return fail(DGP_ERR_INVALID, "too many boundary settings on one law");
+  l->bc_id[l->nbc] = boundary_id;
+  l->bc_kind[l->nbc] = bc_kind;
+  ++l->nbc;
+  return DGP_OK;
+}
+
 int dgp_law_destroy(dgp_law l) {
   delete l;
   return DGP_OK;
@@ -764,9 +783,7 @@ int dgp_solver_create(dgp_mesh mh, dgp_law law, int order, int precision, int li
     return rc;
   }
   s->meshes.push_back(m);
-  LawParams lp{};
-  lp.field = law->field;
-  for (int i = 0; i < DGP_NPARAMS; ++i) lp.p[i] = law->p[i];
+  const LawParams lp = law->params();
   if (int rc = build_solver(s, {lp}, law->field, false)) {
     delete s;
     return rc;
@@ -1440,10 +1457,7 @@ int dgp_ensemble_create(int n, const dgp_mesh* meshes, const dgp_law* laws, cons
     for (size_t k = 0; k < members.size(); ++k) {
       const int i = members[k];
       s->meshes.push_back(meshes[i]->m);
-      LawParams lp{};
-      lp.field = laws[i]->field;
-      for (int q = 0; q < DGP_NPARAMS; ++q) lp.p[q] = laws[i]->p[q];
-      lps.push_back(lp);
+      lps.push_back(laws[i]->params());
       e->inst_group[i] = static_cast<int>(e->groups.size());
       e->inst_index[i] = static_cast<int>(k);
     }

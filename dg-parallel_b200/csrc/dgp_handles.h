@@ -34,6 +34,21 @@ struct dgp_mesh_s {
 struct dgp_law_s {
   int kind, flux, field;
   double p[DGP_NPARAMS];
+  int nbc = 0;
+  int bc_id[DGP_MAX_BC] = {};
+  int bc_kind[DGP_MAX_BC] = {};
+  // the device view of the law: parameters, field and boundary settings
+  dgp::LawParams params() const {
+    dgp::LawParams lp{};
+    lp.field = field;
+    for (int i = 0; i < DGP_NPARAMS; ++i) lp.p[i] = p[i];
+    lp.nbc = nbc;
+    for (int i = 0; i < nbc; ++i) {
+      lp.bc_id[i] = bc_id[i];
+      lp.bc_kind[i] = bc_kind[i];
+    }
+    return lp;
+  }
 };
 
 // Discrete adjoint bookkeeping of a solver: checkpoints of the last

@@ -30,7 +30,21 @@ struct LawTraits<DGP_LAW_MAXWELL2D> { static constexpr int M = 3; };
 struct LawParams {
   double p[DGP_NPARAMS];
   int field;
+  int nbc;                   // boundary ids remapped by dgp_law_set_bc
+  int bc_id[DGP_MAX_BC];
+  int bc_kind[DGP_MAX_BC];   // DGP_BC_*
 };
+
+// the classification id a boundary face is treated as: a wall is the law's
+// 40000, the far field any other id; ids without a setting keep their own rule
+__host__ __device__ inline int bc_effective_id(const LawParams& lp, int bid) {
+  for (int i = 0; i < lp.nbc; ++i)
+    if (lp.bc_id[i] == bid) {
+      if (lp.bc_kind[i] == DGP_BC_WALL) return 40000;
+      if (lp.bc_kind[i] == DGP_BC_FARFIELD) return bid == 40000 ? 1 : bid;
+    }
+  return bid;
+}
 
 constexpr double kPi = 3.14159265358979323846;
 
@@ -418,9 +432,10 @@ __device__ __forceinline__ void numerical_flux(const LawParams& lp, const T* n, 
 
 // ---- boundary flux for faces without a right cell (DGCell.cc:696-705) -------
 template <int LAW, int FLUX, int DIM, typename T>
-__device__ __forceinline__ void boundary_flux(const LawParams& lp, int bid, const T* n,
+__device__ __forceinline__ void boundary_flux(const LawParams& lp, int bid_in, const T* n,
                                               const double* x, double time, const T* Q, T* flux) {
   constexpr int M = LawTraits<LAW>::M;
+  const int bid = bc_effective_id(lp, bid_in);
   T f[M];
   if constexpr (LAW == DGP_LAW_SCALAR) {  // ScalarLaw::boundaryFlux, ScalarLaw.cc:85-105
     T nv = 0;

@@ -17,6 +17,7 @@ LIB_PATH = os.path.join(os.path.dirname(_HERE), "lib", "libdgp.so")
 LAW_SCALAR, LAW_BURGERS2D, LAW_EULER2D, LAW_EULER3D, LAW_MAXWELL3D, LAW_MAXWELL2D = range(6)
 FLUX_UPWIND, FLUX_CENTRAL, FLUX_GODUNOV, FLUX_ROE, FLUX_LLF = range(5)
 FIELD_GAUSS, FIELD_VORTEX, FIELD_PULSE3D, FIELD_SINE, FIELD_GAUSS3D, FIELD_TM110, FIELD_TM2D = range(7)
+BC_DEFAULT, BC_FARFIELD, BC_WALL = range(3)
 FP64, MIXED = 0, 1
 LIMITER_NONE, LIMITER_MOMENT, LIMITER_BARTH = 0, 1, 2
 STEPPING_SSPRK3, STEPPING_LOCAL = 0, 5
@@ -59,6 +60,7 @@ def lib() -> ctypes.CDLL:
         "dgp_mesh_face_geometry": ([P, pD], I),
         "dgp_mesh_destroy": ([P], I),
         "dgp_law_create": ([I, I, I, pD, pP], I),
+        "dgp_law_set_bc": ([P, I, I], I),
         "dgp_law_destroy": ([P], I),
         "dgp_solver_create": ([P, P, I, I, I, pP], I),
         "dgp_solver_destroy": ([P], I),
@@ -209,6 +211,11 @@ class Law:
         self.h = ctypes.c_void_p()
         self.kind, self.flux, self.field = kind, flux, field
         check(lib().dgp_law_create(kind, flux, field, _dp(p), ctypes.byref(self.h)))
+
+    def set_bc(self, boundary_id: int, kind: int):
+        """Boundary condition of the faces classified boundary_id (BC_DEFAULT,
+        BC_FARFIELD, BC_WALL) for solvers created from this law afterwards."""
+        check(lib().dgp_law_set_bc(self.h, int(boundary_id), int(kind)))
 
     def close(self):
         if self.h:

@@ -8,12 +8,52 @@
 #ifndef DGP_GPU_TIME_INTEGRATOR_H
 #define DGP_GPU_TIME_INTEGRATOR_H
 
+#include <typeinfo>
 #include <vector>
 
+#include "Burgers.h"
 #include "DGCell.h"
+#include "EulerLaw.h"
+#include "MaxwellLaw.h"
+#include "ScalarLaw.h"
 #include "TimeIntegrator.h"
 #include "dgp.h"
 #include "mException.h"
+
+// GpuConservationLaw: the library's law and numerical-flux ids of a
+// DG-Parallel law object (ConservationLaw.h:12-60), by its dynamic type: each
+// class whose riemannSolver the library has kernels for maps to one pair.
+// Subclasses with other Riemann solvers (EulervanLeer, Euler2dHLLC,
+// Euler2dExactRiemann, Euler3dRoe, ...) have none and are refused.
+struct GpuConservationLaw {
+  static bool map(const ConservationLaw* law, int* kind, int* flux) {
+    const std::type_info& t = typeid(*law);
+    if (t == typeid(Euler2dRoe)) return set(DGP_LAW_EULER2D, DGP_FLUX_ROE, kind, flux);
+    if (t == typeid(Euler2d)) return set(DGP_LAW_EULER2D, DGP_FLUX_GODUNOV, kind, flux);
+    if (t == typeid(Euler3d)) return set(DGP_LAW_EULER3D, DGP_FLUX_GODUNOV, kind, flux);
+    if (t == typeid(ScalarLaw)) return set(DGP_LAW_SCALAR, DGP_FLUX_UPWIND, kind, flux);
+    if (t == typeid(Burgers2D)) return set(DGP_LAW_BURGERS2D, DGP_FLUX_CENTRAL, kind, flux);
+    if (t == typeid(Maxwell2d)) return set(DGP_LAW_MAXWELL2D, DGP_FLUX_UPWIND, kind, flux);
+    return false;
+  }
+  static int kind(const ConservationLaw* law) {
+    int k, f;
+    if (!map(law, &k, &f)) throw new mException(__LINE__, __FILE__, (char*)"no GPU kernels for this ConservationLaw");
+    return k;
+  }
+  static int flux(const ConservationLaw* law) {
+    int k, f;
+    if (!map(law, &k, &f)) throw new mException(__LINE__, __FILE__, (char*)"no GPU kernels for this ConservationLaw");
+    return f;
+  }
+
+ private:
+  static bool set(int k, int f, int* kind, int* flux) {
+    *kind = k;
+    *flux = f;
+    return true;
+  }
+};
 
 class GpuTimeIntegrator : public TimeIntegrator {
  public:
@@ -31,6 +71,13 @@ class GpuTimeIntegrator : public TimeIntegrator {
     dof_ = nf * np;
     buf_.resize((size_t)e * dof_);
   }
+  // the same, with the law and flux ids read off the reference law object;
+  // the field evaluator (a host callback) is named by id
+  GpuTimeIntegrator(mDGMesh* m, ConservationLaw* law, int order, const char* msh,
+                    const std::vector<DGCell*>& cells, int field, const double* params,
+                    int precision = DGP_PRECISION_FP64)
+      : GpuTimeIntegrator(m, law, order, msh, cells, GpuConservationLaw::kind(law), GpuConservationLaw::flux(law),
+                          field, params, precision) {}
   ~GpuTimeIntegrator() {
     dgp_solver_destroy(s_);
     dgp_law_destroy(law_);

@@ -59,6 +59,15 @@ extern "C" {
  *  [9] amplitude A               [10] cavity side L */
 #define DGP_NPARAMS 16
 
+/* boundary conditions by classification id (ConservationLaw::boundaryFlux's
+ * dispatch on BoundaryId, ConservationLaw.h:31-40; EulerLaw.cc:280-295,
+ * MaxwellLaw.cc:113-131): */
+#define DGP_BC_DEFAULT 0  /* the law's own rule for the id (40000 a wall, other ids the far field) */
+#define DGP_BC_FARFIELD 1 /* the law's field through its boundary / Riemann flux */
+#define DGP_BC_WALL 2     /* the law's wall: Euler slip mirror state, Maxwell2d reflection,
+                           * Maxwell3d perfect conductor (not defined for the scalar laws) */
+#define DGP_MAX_BC 8      /* ids a law can remap */
+
 #define DGP_PRECISION_FP64 0  /* plain FP64 drop-in form */
 #define DGP_PRECISION_MIXED 1 /* FP32 bulk arithmetic, FP64 geometry/totals/time */
 
@@ -107,6 +116,11 @@ int dgp_mesh_destroy(dgp_mesh m);
 /* ---- law: replaces the ConservationLaw + FieldEvaluator objects */
 int dgp_law_create(int kind, int flux, int field, const double* params, dgp_law* out);
 int dgp_law_destroy(dgp_law law);
+/* Boundary condition of the faces classified boundary_id: bc_kind one of
+ * DGP_BC_*.  Applies to solvers and ensembles created from the law afterwards;
+ * periodic ids (510, 610) are paired edges, not boundary conditions.  At most
+ * DGP_MAX_BC ids per law; DGP_ERR_UNSUPPORTED for a wall on a scalar law. */
+int dgp_law_set_bc(dgp_law law, int boundary_id, int bc_kind);
 
 /* ---- solver: DGAnalysis setup (DGAnalysis.cc:133-302) + TimeIntegrator */
 int dgp_solver_create(dgp_mesh m, dgp_law law, int order, int precision, int limiter,

@@ -626,8 +626,21 @@ int main(int argc, char** argv) {
       kind = DGP_LAW_BURGERS2D;
       flux = DGP_FLUX_CENTRAL;
       field = DGP_FIELD_SINE;
+    } else if (P.caseName == "tm2d") {
+      kind = DGP_LAW_MAXWELL2D;
+      flux = DGP_FLUX_UPWIND;
+      field = DGP_FIELD_TM2D;
+      prm[10] = P.L;
     }
-    gti = new GpuTimeIntegrator(mesh, law, P.order, P.mesh.c_str(), byFile, kind, flux, field, prm);
+    // the law and flux ids come from the reference law object itself
+    // (GpuConservationLaw); they must agree with this driver's case table
+    int mk = -1, mf = -1;
+    if (!GpuConservationLaw::map(law, &mk, &mf) || mk != kind || mf != flux) {
+      fprintf(stderr, "GpuConservationLaw maps this law to (%d, %d), the case table says (%d, %d)\n", mk, mf,
+              kind, flux);
+      return 2;
+    }
+    gti = new GpuTimeIntegrator(mesh, law, P.order, P.mesh.c_str(), byFile, field, prm);
   }
 #endif
   FILE* fs = P.state.empty() ? 0 : fopen(P.state.c_str(), "w");

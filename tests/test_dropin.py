@@ -2,7 +2,9 @@
 DGCell projection, CFL reduction, output) steps its cells through the
 reference-side shim dg-parallel_b200/integration/GpuTimeIntegrator.h
 (oracle/_ref/ref_driver_gpu --gpu 1) instead of its RungeKuttaTVD3, and the
-states match the reference's own integration step by step."""
+states match the reference's own integration step by step.  The shim reads
+the library's law and flux ids off the reference's law object
+(GpuConservationLaw)."""
 import os
 import subprocess
 
@@ -19,6 +21,7 @@ CASES = {
     "euler_roe_p3": ["--case", "vortex", "--flux", "roe", "--order", "3"],
     "euler_godunov_p2": ["--case", "vortex", "--flux", "exact", "--order", "2"],
     "burgers_p2": ["--case", "sine", "--order", "2", "--amp", "0.25"],
+    "maxwell2d_wall_p2": ["--case", "tm2d", "--order", "2"],
     "scalar_tet_p2": ["--case", "gauss3d", "--order", "2", "--ax", "1", "--ay", "0.5", "--az", "0.25",
                       "--cx", "0.5", "--cy", "0.5", "--cz", "0.5", "--s", "0.05"],
 }

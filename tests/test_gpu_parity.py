@@ -226,3 +226,36 @@ def test_unsupported_and_invalid(tmp_path):
     with pytest.raises(dgp.DGPError) as e:
         dgp.Solver(mesh, dgp.Law(dgp.LAW_SCALAR, dgp.FLUX_UPWIND, dgp.FIELD_GAUSS, SCALAR2D), 7)
     assert e.value.code == -3
+
+
+@pytest.mark.parametrize("law_id, flux, field, prm", [
+    (dgp.LAW_EULER2D, dgp.FLUX_ROE, dgp.FIELD_VORTEX, VORTEX),
+    (dgp.LAW_MAXWELL2D, dgp.FLUX_UPWIND, dgp.FIELD_TM2D, TM110),
+])
+def test_law_set_bc_equals_retagged_mesh(tmp_path, law_id, flux, field, prm):
+    """dgp_law_set_bc: faces tagged 1 declared walls step exactly as the same
+    mesh tagged 40000 with the default rule, and 40000 declared far field as
+    the mesh tagged 1."""
+    box = (0.0, 10.0) if law_id == dgp.LAW_EULER2D else (0.0, 1.0)
+    far = _tri(tmp_path, 6, box=box, seed=2, tag=1)
+    wall = _tri(tmp_path, 6, box=box, seed=2, tag=40000)
+
+    def run(msh, bcs):
+        law = dgp.Law(law_id, flux, field, prm)
+        for bid, kind in bcs:
+            law.set_bc(bid, kind)
+        s = dgp.Solver(dgp.Mesh.from_msh(msh), law, 2)
+        t = 0.0
+        for _ in range(3):
+            dt = 0.5 * s.cfl_dt(0.1) if law_id == dgp.LAW_EULER2D else 0.005
+            s.step(t, dt)
+            t += dt
+        return s.get_state()
+
+    a = run(far, [(1, dgp.BC_WALL)])
+    b = run(wall, [])
+    assert np.array_equal(a, b)
+    c = run(wall, [(40000, dgp.BC_FARFIELD)])
+    d = run(far, [])
+    assert np.array_equal(c, d)
+    assert not np.array_equal(a, d)

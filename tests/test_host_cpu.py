@@ -91,3 +91,28 @@ def test_tet_mesh_faces_and_orientation():
         fc = np.mean([v[ids[x]] for x in row[:3]], axis=0)
         cc = v[cells[row[n]]].mean(axis=0)
         assert np.dot(gg[:3], fc - cc) > 0
+
+
+def test_law_boundary_settings_are_checked():
+    """dgp_law_set_bc (no GPU needed): periodic ids are not boundary
+    conditions, the scalar laws have no wall, at most DGP_MAX_BC ids a law."""
+    import dgp
+    e = dgp.Law(dgp.LAW_EULER2D, dgp.FLUX_ROE, dgp.FIELD_VORTEX, dgp.law_params())
+    e.set_bc(1, dgp.BC_WALL)
+    e.set_bc(1, dgp.BC_FARFIELD)  # a second setting of the same id replaces the first
+    with pytest.raises(dgp.DGPError) as ei:
+        e.set_bc(510, dgp.BC_WALL)
+    assert ei.value.code == -1
+    with pytest.raises(dgp.DGPError) as ei:
+        e.set_bc(2, 7)
+    assert ei.value.code == -1
+    for bid in range(2, 9):
+        e.set_bc(bid, dgp.BC_WALL)
+    with pytest.raises(dgp.DGPError) as ei:
+        e.set_bc(99, dgp.BC_WALL)
+    assert ei.value.code == -1
+    s = dgp.Law(dgp.LAW_SCALAR, dgp.FLUX_UPWIND, dgp.FIELD_GAUSS, dgp.law_params())
+    with pytest.raises(dgp.DGPError) as ei:
+        s.set_bc(1, dgp.BC_WALL)
+    assert ei.value.code == -3
+    s.set_bc(1, dgp.BC_FARFIELD)
