@@ -103,6 +103,16 @@ __device__ __forceinline__ Dual<T, N> sqrt(const Dual<T, N>& a) {
 }
 
 template <typename T, int N>
+__device__ __forceinline__ Dual<T, N> rsqrt(const Dual<T, N>& a) {
+  Dual<T, N> r;
+  r.v = ::rsqrt(a.v);
+  const T dr = (T)-0.5 * r.v * r.v * r.v;  // d/dx x^(-1/2)
+#pragma unroll
+  for (int k = 0; k < N; ++k) r.d[k] = dr * a.d[k];
+  return r;
+}
+
+template <typename T, int N>
 __device__ __forceinline__ Dual<T, N> fabs(const Dual<T, N>& a) {
   return a.v < (T)0 ? -a : a;
 }

@@ -118,6 +118,19 @@ __device__ __forceinline__ void field_eval(const LawParams& lp, const double* x,
   }
 }
 
+// Euler2d::Fi (EulerLaw.cc:47-69) with 1/rho given
+template <typename T>
+__device__ __forceinline__ void euler2d_flux_inv(T g, const T* Q, T invrho, T (*F)[2]) {
+  T Q1 = Q[1], Q2 = Q[2];
+  T q12 = Q1 * Q2 * invrho, q11 = Q1 * Q1 * invrho, q22 = Q2 * Q2 * invrho;
+  T p = (g - (T)1) * (Q[3] - (T)0.5 * (q11 + q22));
+  T qq = invrho * (Q[3] + p);
+  F[0][0] = Q1; F[0][1] = Q2;
+  F[1][0] = q11 + p; F[1][1] = q12;
+  F[2][0] = q12; F[2][1] = q22 + p;
+  F[3][0] = Q1 * qq; F[3][1] = Q2 * qq;
+}
+
 // ---- volume flux F[j][i] (ConservationLaw::Fi) ------------------------------
 template <int LAW, int DIM, typename T>
 __device__ __forceinline__ void volume_flux(const LawParams& lp, const T* Q, T (*F)[DIM]) {
@@ -167,6 +180,13 @@ __device__ __forceinline__ void volume_flux(const LawParams& lp, const T* Q, T (
 
 template <typename T>
 __device__ __forceinline__ T tmax(T a, T b) { return a > b ? a : b; }
+
+// 1 / sqrt(x) (the hardware reciprocal square root with its refinement; the
+// adjoint's dual numbers bring their own rsqrt)
+__device__ __forceinline__ double inv_sqrt(double x) { return ::rsqrt(x); }
+__device__ __forceinline__ float inv_sqrt(float x) { return ::rsqrtf(x); }
+template <typename T>
+__device__ __forceinline__ T inv_sqrt(const T& x) { return rsqrt(x); }
 
 // Euler::riemann, EulerLaw.cc:610-810: exact Riemann solver, Newton on p*
 // from the two-shock guess, <= 12 iterations to relative 1e-14.
@@ -280,10 +300,16 @@ __device__ __forceinline__ void numerical_flux(const LawParams& lp, const T* n, 
   } else if constexpr (LAW == DGP_LAW_EULER2D) {
     const T g = (T)lp.p[7];
     if constexpr (FLUX == DGP_FLUX_ROE) {  // Euler2dRoe::riemannSolver, EulerLaw.cc:913-1010
+      // the reference's arithmetic, with its square roots and reciprocals of
+      // the densities and of the sound speed taken from reciprocal square
+      // roots (one hardware operation each instead of a square root and a
+      // division): results agree to a few ulps
       T rho_0 = u0[0], rho_1 = u1[0];
-      T sqrt_rho_0 = sqrt(rho_0), sqrt_rho_1 = sqrt(rho_1);
-      T inv_rho_0 = (T)1 / rho_0, inv_rho_1 = (T)1 / rho_1;
+      const T is0 = inv_sqrt(rho_0), is1 = inv_sqrt(rho_1);
+      T sqrt_rho_0 = rho_0 * is0, sqrt_rho_1 = rho_1 * is1;
+      T inv_rho_0 = is0 * is0, inv_rho_1 = is1 * is1;
       T rho_A = sqrt_rho_0 * sqrt_rho_1;
+      const T inv_rho_A = is0 * is1;
       T inv_denom = (T)1 / (sqrt_rho_0 + sqrt_rho_1);
       T u_0 = u0[1] * inv_rho_0, u_1 = u1[1] * inv_rho_1;
       T u_A = (u_0 * sqrt_rho_0 + u_1 * sqrt_rho_1) * inv_denom;
@@ -296,28 +322,30 @@ __device__ __forceinline__ void numerical_flux(const LawParams& lp, const T* n, 
       T qq = H_A - (T)0.5 * (u_A * u_A + v_A * v_A);
       T roe[4] = {0, 0, 0, 0};
       if (qq > 0) {
-        T c_A = sqrt((g - (T)1) * qq);
+        const T c2 = (g - (T)1) * qq;
+        T inv_c_A = inv_sqrt(c2);
+        T c_A = c2 * inv_c_A;
         T vn = u_A * n[0] + v_A * n[1];
         T ev[4] = {fabs(vn), fabs(vn), fabs(vn + c_A), fabs(vn - c_A)};
-        T k = (T)0.5 * rho_A / c_A;
+        T k = (T)0.5 * rho_A * inv_c_A;
         T evec[4][4] = {
             {(T)1, u_A, v_A, (T)0.5 * (u_A * u_A + v_A * v_A)},
             {(T)0, n[1] * rho_A, -n[0] * rho_A, rho_A * (u_A * n[1] - v_A * n[0])},
             {k, k * (u_A + c_A * n[0]), k * (v_A + c_A * n[1]), k * (H_A + c_A * vn)},
             {k, k * (u_A - c_A * n[0]), k * (v_A - c_A * n[1]), k * (H_A - c_A * vn)}};
-        T inv_c_A = (T)1 / c_A;
         T drho = rho_1 - rho_0, dp = p_1 - p_0, du = u_1 - u_0, dv = v_1 - v_0;
+        const T dpc = dp * inv_rho_A * inv_c_A;
         T charv[4] = {drho - dp * inv_c_A * inv_c_A, n[1] * du - n[0] * dv,
-                      n[0] * du + n[1] * dv + dp / rho_A * inv_c_A,
-                      -n[0] * du - n[1] * dv + dp / rho_A * inv_c_A};
+                      n[0] * du + n[1] * dv + dpc, -n[0] * du - n[1] * dv + dpc};
 #pragma unroll
         for (int i = 0; i < 4; i++)
 #pragma unroll
           for (int j = 0; j < 4; j++) roe[j] += ev[i] * charv[i] * evec[i][j];
       }
+      // Euler2d::Fi of both states with the reciprocals above
       T f1[M][DIM], f2[M][DIM];
-      volume_flux<LAW, DIM, T>(lp, u0, f1);
-      volume_flux<LAW, DIM, T>(lp, u1, f2);
+      euler2d_flux_inv<T>(g, u0, inv_rho_0, f1);
+      euler2d_flux_inv<T>(g, u1, inv_rho_1, f2);
 #pragma unroll
       for (int i = 0; i < 4; i++)
         flux[i] = (T)0.5 * ((f1[i][0] + f2[i][0]) * n[0] + (f1[i][1] + f2[i][1]) * n[1] - roe[i]);
