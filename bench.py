@@ -260,6 +260,8 @@ def main():
                          "triangles, 4 size bins, against SSP-RK3 on the same mesh, ~1 min)")
     ap.add_argument("--profile-case", choices=["fp64", "mixed", "maxwell", "limiter", "lts"], default=None,
                     help="only set up the workload and run --warmup + --steps steps (for ncu)")
+    ap.add_argument("--tensor-cores", action="store_true",
+                    help="--profile-case mixed: the volume contraction on the tensor cores")
     ap.add_argument("--block", type=int, default=0, choices=[0, 64, 128, 256],
                     help="--profile-case: tile shape (threads) of the element and face kernels "
                          "(0: the autotuner's pick, as the bench line)")
@@ -949,6 +951,8 @@ def profile_case(args):
     else:
         dgp.autotune(mesh, law, 3, prec, 0, iters=5)
     s = dgp.Solver(mesh, law, 3, prec)
+    if args.tensor_cores:
+        s.set_tensor_cores(True)
     t, _ = s.run(0.0, 0.0, 0.1, args.warmup)
     t, n = s.run(t, 0.0, 0.1, args.steps)
     s.synchronize()
