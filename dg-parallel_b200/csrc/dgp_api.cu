@@ -1812,6 +1812,12 @@ int dgp_solver_block(dgp_solver s, int* block, int* cells_per_tile) {
   return DGP_OK;
 }
 
+int dgp_solver_fused(dgp_solver s, int* fused) {
+  if (!s || !fused) return fail(DGP_ERR_INVALID, "null argument");
+  *fused = s->fused ? 1 : 0;
+  return DGP_OK;
+}
+
 int dgp_ensemble_group_block(dgp_ensemble e, int group, int* block, int* cells_per_tile) {
   if (!e || group < 0 || group >= static_cast<int>(e->groups.size())) return fail(DGP_ERR_INVALID, "bad group");
   return dgp_solver_block(e->groups[group], block, cells_per_tile);

@@ -116,6 +116,7 @@ def lib() -> ctypes.CDLL:
         "dgp_forward_checkpointed": ([P, D, D, I, I, pD], I),
         "dgp_backward": ([P, pD, pD], I),
         "dgp_solver_block": ([P, pI, pI], I),
+        "dgp_solver_fused": ([P, pI], I),
         "dgp_ensemble_group_block": ([P, I, pI, pI], I),
     }
     for name, (args, res) in sig.items():
@@ -326,8 +327,10 @@ class Solver:
         return h.value or 0
 
     def profile_kernels(self, iters: int = 20) -> np.ndarray:
-        """Mean ms of [face kernel, element kernel (inner stage), element kernel
-        (last stage with the fused CFL reduction)]."""
+        """Mean ms of [stage 1, stage 2, last stage with the CFL reduction] of
+        the fused stage kernel; for solvers that are not fused (see `fused`):
+        [face kernel, element kernel (inner stage), element kernel (last
+        stage with the CFL reduction)]."""
         out = (ctypes.c_float * 3)()
         check(lib().dgp_profile_kernels(self.h, iters, out))
         return np.array(out[:], dtype=np.float64)
@@ -343,6 +346,13 @@ class Solver:
         out = np.zeros(self.ncells, dtype=np.uint8)
         check(lib().dgp_limiter_triggers(self.h, out.ctypes.data_as(ctypes.POINTER(ctypes.c_uint8))))
         return out
+
+    @property
+    def fused(self) -> bool:
+        """True when each stage runs as one fused stage kernel."""
+        f = ctypes.c_int()
+        check(lib().dgp_solver_fused(self.h, ctypes.byref(f)))
+        return bool(f.value)
 
     def set_p0_fallback(self, on: bool = True):
         check(lib().dgp_set_p0_fallback(self.h, 1 if on else 0))

@@ -280,6 +280,10 @@ int dgp_solver_stream(dgp_solver s, void** stream);
  * the fused kernel: the face kernel, the element kernel of an inner stage and
  * of the last stage).  Leaves the state unchanged; resets the time control. */
 int dgp_profile_kernels(dgp_solver s, int iters, float* ms);
+/* *fused = 1 when each stage runs as one fused stage kernel (faces, volume,
+ * lift and the SSP-RK3 update of a tile of cells), 0 when it runs as the face
+ * and element kernels (a tile's halo too large for shared memory) */
+int dgp_solver_fused(dgp_solver s, int* fused);
 /* Assembled right-hand side that allocates no device memory; no counterpart in
  * DG-Parallel.  For callers that cannot call cudaMalloc when they need a RHS
  * (device memory owned by another allocator, or no tolerance for the

@@ -114,6 +114,7 @@ def test_run_device_loop_matches_oracle(tmp_path):
     msh = _tri(tmp_path, 12, box=(0.0, 10.0), seed=2)
     o = Oracle(msh, dgp.LAW_EULER2D, dgp.FLUX_ROE, 3, dgp.FIELD_VORTEX, VORTEX)
     s = solver_for(msh, dgp.LAW_EULER2D, dgp.FLUX_ROE, dgp.FIELD_VORTEX, 3, VORTEX)
+    assert s.fused and s.launches_per_step() == 4  # 3 stage launches + the finalize
     tg, ng = s.run(0.0, 0.05, 0.1)
     to, no = o.run(0.0, 0.05, 0.1, 0)
     assert ng == no and tg == to
