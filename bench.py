@@ -186,6 +186,15 @@ def fused_kernel_bytes(E, M, NP, DIM, tsize, with_u0):
     return (3 if with_u0 else 2) * state + E * (DIM * DIM * tsize + 8)
 
 
+def elem_kernel_bytes(E, M, NP, NS, DIM, tsize):
+    """Bytes one element-kernel launch must move (solvers whose tiles do not
+    fit the fused kernel): state read, u_n read, new state written (FP64), face
+    slots read and face-point traces written (right-hand-side type), J^{-1}
+    (right-hand-side type) and |J| (FP64) per cell."""
+    state = E * M * NP * 8
+    return 3 * state + 2 * E * NS * M * tsize + E * (DIM * DIM * tsize + 8)
+
+
 def stage_formula_bytes(E, F, M, NP, DIM):
     """Algorithmic bytes of one whole stage by the per-element-stage formula of
     the workload's roofline definition: coefficients (2 + 2/3) m Np 8 (FP64

@@ -513,6 +513,14 @@ static int build_solver(dgp_solver s, const std::vector<LawParams>& lps, int fie
       (rc = s->upload(&s->d_f2i, s->f2i)))
     return rc;
   {
+    // largest |phi_k| over the volume points and every local face's points
+    const size_t np = static_cast<size_t>(t.Np);
+    std::vector<double> phimax(np, 0.0);
+    for (size_t i = 0; i < t.phi.size(); ++i) phimax[i % np] = std::max(phimax[i % np], std::fabs(t.phi[i]));
+    for (size_t i = 0; i < t.phif.size(); ++i) phimax[i % np] = std::max(phimax[i % np], std::fabs(t.phif[i]));
+    if ((rc = s->upload_t(&b.phimax, phimax))) return rc;
+  }
+  {
     std::vector<double> blob(s->ops.blob_elems);
     s->ops.fill_blob(t.dphi.data(), t.phif.data(), t.phi.data(), t.qw.data(), blob.data());
     if ((rc = s->upload_t(&b.blob, blob))) return rc;
@@ -1026,7 +1034,14 @@ int dgp_rhs(dgp_solver s, double t, double* host_rhs) {
     const double* C = static_cast<const double*>(s->b.C);
     s->ops.fused(s->b, C, C, static_cast<double*>(s->b.rhs), nullptr, 0, 0.0, 0, s->stream);
   } else {
+    // the P0 fallback's second face pass zeroes the marked cells' modes in
+    // the state: the assembly runs on a copy, the state stays as it was
+    const size_t bytes = s->state_count() * 8;
+    if (s->b.p0)
+      DGP_CUDA(cudaMemcpyAsync(s->b.scratch, s->b.C, bytes, cudaMemcpyDeviceToDevice, s->stream));
     s->ops.stage(s->b, 0, 0.0, 0, s->stream);
+    if (s->b.p0)
+      DGP_CUDA(cudaMemcpyAsync(s->b.C, s->b.scratch, bytes, cudaMemcpyDeviceToDevice, s->stream));
   }
   DGP_CUDA(cudaGetLastError());
   DGP_CUDA(cudaStreamSynchronize(s->stream));
@@ -1109,7 +1124,7 @@ int dgp_launches_per_step(dgp_solver s, int* n) {
   }
   const bool lim = s->limiter != DGP_LIMITER_NONE && s->ops.limit;
   const int per_pass = s->limiter == DGP_LIMITER_BARTH ? 1 : 2;
-  *n = (s->fused ? 4 : 3 * (s->b.p0 ? 3 : 2)) + (lim ? 3 * per_pass + 1 : 0);
+  *n = (s->fused ? 4 : 3 * (s->b.p0 ? 4 : 2)) + (lim ? 3 * per_pass + 1 : 0);
   return DGP_OK;
 }
 

@@ -135,6 +135,7 @@ struct DevTables {
   const T* fqw;     // NQF
   const int* qmap;  // NPERM x NQF
   const double* phiv;  // (DIM+1) x NP  (FP64, CFL)
+  const T* phimax;     // NP: largest |phi_k| over the volume and face points (P0 check)
   const double* phiq;  // NQ x NP (FP64, projection)
   const double* qwd;   // NQ (FP64)
   const double* qpd;   // NQ x 3 (FP64)
@@ -480,6 +481,32 @@ __global__ void __launch_bounds__(K::FACE_BLOCK) face_rerun_kernel(const __grid_
   for (int vb = blockIdx.x; vb * K::FPB < a.mesh.F; vb += gridDim.x) {
     const int f = vb * K::FPB + fl;
     if (f < a.mesh.F) face_point<K, true, ENS>(a, f, q, s_phif, s_fqw, s_qmap);
+  }
+}
+
+// First check of the P0 fallback, thread per (cell, volume quadrature point):
+// a cell with a non-physical value at one of its volume points is marked (the
+// correction inside DGCell::computeVolumeContribution, DGCell.cc:197-221);
+// the face kernel marks the cells with a non-physical face-point trace, and
+// face_rerun_kernel drops every marked cell to its mean.
+template <class K, bool ENS>
+__global__ void __launch_bounds__(128) p0_volume_kernel(const __grid_constant__ StageArgs<typename K::T> a) {
+  using T = typename K::T;
+  if (a.gctl->done) return;
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= (long long)a.mesh.E * K::NQ) return;
+  const int e = (int)(i / K::NQ), q = (int)(i - (long long)e * K::NQ);
+  const LawParams* lp = &a.law;
+  if constexpr (ENS) {
+    const int inst = a.cell_inst[e];
+    if (inst < 0 || a.ctl[inst].done) return;
+    lp = a.laws + inst;
+  }
+  T U[K::M];
+  cell_trace<K>(a.C + (size_t)e * K::MNP, a.tab.phi + q * K::NP, U);
+  if (!is_physical<K::LAW, T>(*lp, U)) {
+    flag_nonphysical(a.status, e);
+    mark_p0(a, e);
   }
 }
 

@@ -570,4 +570,28 @@ __device__ __forceinline__ bool is_physical(const LawParams& lp, const T* Q) {
   }
 }
 
+// A sufficient condition for isPhysical at every point of a cell: each field
+// stays within B[j] of mean[j] (B from the modes k >= 1 and the largest basis
+// values), and density and pressure keep a relative margin far above the
+// rounding of a value evaluated point by point.  False means "evaluate the
+// points"; laws without a physical range always pass.
+template <int LAW, typename T>
+__device__ __forceinline__ bool physical_bound(const LawParams& lp, const T* mean, const T* B) {
+  if constexpr (LAW == DGP_LAW_EULER2D || LAW == DGP_LAW_EULER3D) {
+    constexpr T tol = sizeof(T) == 8 ? (T)1e-9 : (T)1e-3;
+    const T rho = mean[0] - B[0] - tol * (fabs(mean[0]) + B[0]);
+    if (!(rho > (T)0)) return false;
+    const T m1 = fabs(mean[1]) + B[1], m2 = fabs(mean[2]) + B[2];
+    T mm = m1 * m1 + m2 * m2;
+    if constexpr (LAW == DGP_LAW_EULER3D) {
+      const T m3 = fabs(mean[4]) + B[4];
+      mm += m3 * m3;
+    }
+    const T e = mean[3] - B[3] - tol * (fabs(mean[3]) + B[3]);
+    return e - (T)0.5 * mm / rho * ((T)1 + tol) > (T)0;
+  } else {
+    return true;
+  }
+}
+
 }  // namespace dgp

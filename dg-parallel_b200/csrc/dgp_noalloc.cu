@@ -94,6 +94,7 @@ extern "C" int dgp_rhs_noalloc(dgp_solver s, const double* dev_state, double t, 
   if (int rc = scratch_address(s->device, &base)) return rc;
   unsigned char* p = static_cast<unsigned char*>(base);
   dgp::DeviceBuffers b = s->b;  // geometry and tables of the solver, intermediates in scratch
+  b.p0 = 0;  // the P0 fallback's second pass would zero modes of the caller's state
   b.C = p;
   b.slots = p + state_b;
   b.rhs = p + state_b + slot_b;

@@ -81,7 +81,7 @@ StageArgs<typename K::T> stage_args(const DeviceBuffers& b, int stage, double ti
   a.stage = stage;
   a.stage_time_factor = time_factor;
   a.fuse_cfl = fuse_cfl;
-  a.p0 = (stage > 0 && b.p0) ? 1 : 0;
+  a.p0 = b.p0;
   if (stage == 0) a.Cout = static_cast<double*>(b.rhs);
   return a;
 }
@@ -108,6 +108,18 @@ void ops_face_rerun(const DeviceBuffers& b, int stage, double time_factor, cudaS
     face_rerun_kernel<K, false><<<g, K::FACE_BLOCK, 0, st>>>(a);
 }
 
+// volume-point check of the P0 fallback (marks only)
+template <class K>
+void ops_p0_volume(const DeviceBuffers& b, int stage, cudaStream_t st) {
+  auto a = stage_args<K>(b, stage, 0.0, 0);
+  const long long n = (long long)b.E * K::NQ;
+  const int g = (int)((n + 127) / 128);
+  if (b.cell_inst)
+    p0_volume_kernel<K, true><<<g, 128, 0, st>>>(a);
+  else
+    p0_volume_kernel<K, false><<<g, 128, 0, st>>>(a);
+}
+
 template <class K>
 void ops_elem(const DeviceBuffers& b, int stage, int fuse_cfl, cudaStream_t st) {
   auto a = stage_args<K>(b, stage, 0.0, fuse_cfl);
@@ -116,8 +128,9 @@ void ops_elem(const DeviceBuffers& b, int stage, int fuse_cfl, cudaStream_t st) 
 
 template <class K>
 void ops_stage(const DeviceBuffers& b, int stage, double time_factor, int fuse_cfl, cudaStream_t st) {
+  if (b.p0) ops_p0_volume<K>(b, stage, st);
   ops_face<K>(b, stage, time_factor, st);
-  if (stage > 0 && b.p0) ops_face_rerun<K>(b, stage, time_factor, st);
+  if (b.p0) ops_face_rerun<K>(b, stage, time_factor, st);
   ops_elem<K>(b, stage, fuse_cfl, st);
 }
 

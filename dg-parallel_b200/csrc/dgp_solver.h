@@ -42,6 +42,7 @@ struct DeviceBuffers {
   void* fqw = nullptr;
   int* qmap = nullptr;
   double* phiv = nullptr;
+  void* phimax = nullptr;  // largest |phi_k| over volume and face points
   double* phiq = nullptr;
   double* qwd = nullptr;
   double* qpd = nullptr;
@@ -119,6 +120,7 @@ inline StageArgs<T> make_args(const DeviceBuffers& b) {
   a.tab.fqw = static_cast<const T*>(b.fqw);
   a.tab.qmap = b.qmap;
   a.tab.phiv = b.phiv;
+  a.tab.phimax = static_cast<const T*>(b.phimax);
   a.tab.phiq = b.phiq;
   a.tab.qwd = b.qwd;
   a.tab.qpd = b.qpd;

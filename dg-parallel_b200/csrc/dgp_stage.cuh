@@ -16,14 +16,16 @@
 // DGCell::computeVolumeContribution (DGCell.cc:184-249) and the
 // RungeKuttaTVD3::advanceInTime update loops (TimeIntegrator.cc:838-990).
 //
-// P0 fallback (DGCell::setToZero, DGCell.cc:785-811; DGAnalysis.cc:392-417):
-// a cell is marked when its trace at any of its face points is not physical.
-// Each tile checks its own cells at their face points during the face pass
-// and its halo cells at all of theirs, so it knows every mark that reaches
-// its faces without a grid-wide pass; a tile that sees one zeroes the modes
-// k >= 1 of the marked rows (own and halo, in shared memory) and evaluates
-// its faces again.  Marks of stage 1 persist into u_n for stages 2 and 3
-// (bad[e]).
+// P0 fallback (DGCell::setToZero, DGCell.cc:785-811; DGAnalysis.cc:392-417,
+// and the correction inside DGCell::computeVolumeContribution,
+// DGCell.cc:197-221): a cell is marked when its value at any of its volume
+// quadrature points or its trace at any of its face points is not physical.
+// Each tile checks its own cells at their face points during the face pass,
+// at their volume points after it, and its halo cells at all of theirs, so it
+// knows every mark that reaches its faces without a grid-wide pass; a tile
+// that sees one zeroes the modes k >= 1 of the marked rows (own and halo, in
+// shared memory) and evaluates its faces again.  Marks of stage 1 persist
+// into u_n for stages 2 and 3 (bad[e]).
 #pragma once
 
 #include "dgp_elem.cuh"
@@ -340,6 +342,43 @@ __device__ __forceinline__ bool fused_face_pass(const StageArgs<typename K::T>& 
   return mk;
 }
 
+// The P0 check of one staged cell: true when its value at a volume
+// quadrature point or (halo cell, e < 0) its trace at a face point is not
+// physical; an own cell's non-physical volume points are counted.  A cell
+// whose modes k >= 1 cannot move a field past the limit anywhere
+// (physical_bound, from the largest basis values phimax, in shared memory) is
+// cleared without evaluating its points.
+template <class K>
+__device__ __forceinline__ bool p0_cell_bad(const StageArgs<typename K::T>& a, const typename K::T* row,
+                                            const typename K::T* sPhi, const typename K::T* sPhif,
+                                            const typename K::T* phimax, int e) {
+  using T = typename K::T;
+  constexpr int M = K::M, NP = K::NP;
+  constexpr int NPP = ElemSmem<K>::NPP;
+  T mean[M], B[M];
+#pragma unroll
+  for (int j = 0; j < M; ++j) {
+    mean[j] = row[j * NP] * sPhi[0];
+    T b = 0;
+#pragma unroll
+    for (int k = 1; k < NP; ++k) b += fabs(row[j * NP + k]) * phimax[k];
+    B[j] = b;
+  }
+  if (physical_bound<K::LAW, T>(a.law, mean, B)) return false;
+  bool bad = false;
+  const int np = e >= 0 ? K::NQ : K::NQ + K::NS;
+#pragma unroll 1
+  for (int p = 0; p < np; ++p) {
+    T U[M];
+    row_trace<K>(row, p < K::NQ ? sPhi + p * NPP : sPhif + (p - K::NQ) * NPP, U);
+    if (!is_physical<K::LAW, T>(a.law, U)) {
+      bad = true;
+      if (e >= 0) flag_nonphysical(a.status, e);
+    }
+  }
+  return bad;
+}
+
 template <class K, bool ENS, bool TC = false, bool RND = false>
 __global__ void __launch_bounds__(K::BLOCK, FusedSmem<K>::MIN_BLOCKS)
     stage_kernel(const __grid_constant__ StageArgs<typename K::T> a) {
@@ -370,6 +409,7 @@ __global__ void __launch_bounds__(K::BLOCK, FusedSmem<K>::MIN_BLOCKS)
   __shared__ T s_fqw[NQF];
   __shared__ int s_qmap[K::NPERM * NQF];
   __shared__ unsigned char s_mark[TE + FS::HMAX];
+  __shared__ T s_phimax[NP];
   __shared__ double sPv[(K::NV - 1) * NP + 1];
   __shared__ __align__(8) uint64_t mma_bar;
   __shared__ uint32_t s_tmem;
@@ -414,6 +454,8 @@ __global__ void __launch_bounds__(K::BLOCK, FusedSmem<K>::MIN_BLOCKS)
     if constexpr (FS::UMMA) mbar_init(&mma_bar, 1);
   }
   for (int i = tid; i < NQF; i += BLOCK) s_fqw[i] = a.tab.fqw[i];
+  if (a.p0)
+    for (int i = tid; i < NP; i += BLOCK) s_phimax[i] = a.tab.phimax[i];
   for (int i = tid; i < K::NPERM * NQF; i += BLOCK) s_qmap[i] = a.tab.qmap[i];
   for (int i = tid; i < TE + ft.nh; i += BLOCK) s_mark[i] = 0;
   if constexpr (FS::UMMA) {
@@ -502,13 +544,16 @@ __global__ void __launch_bounds__(K::BLOCK, FusedSmem<K>::MIN_BLOCKS)
   }
   bool mk = fused_face_pass<K, ENS, true, RND>(a, c, inst, ft, sPhif, s_fqw, s_qmap, sCt, sHt, sS, s_mark);
   if (a.p0) {
-    // halo cells: marked when any of their face-point traces is not physical
-    for (int t = tid; t < ft.nh * NS; t += BLOCK) {
-      const int h = t / NS, s = t - h * NS;
-      T U[M];
-      row_trace<K>(sHt + (size_t)h * RST, sPhif + s * NPP, U);
-      if (!is_physical<K::LAW, T>(a.law, U)) {
-        s_mark[TE + h] = 1;
+    // the face pass marked the own cells with a non-physical trace; also
+    // marked: own cells with a non-physical value at a volume quadrature
+    // point (the correction inside DGCell::computeVolumeContribution,
+    // DGCell.cc:197-221) and halo cells with one at a volume or a face point
+    // (what their own tiles find)
+    for (int l = tid; l < TE + ft.nh; l += BLOCK) {
+      if (l >= ft.ne && l < TE) continue;
+      const T* row = l < TE ? sCt + l * RST : sHt + (size_t)(l - TE) * RST;
+      if (p0_cell_bad<K>(a, row, sPhi, sPhif, s_phimax, l < TE ? ft.e0 + l : -1)) {
+        s_mark[l] = 1;
         mk = true;
       }
     }

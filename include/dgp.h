@@ -148,8 +148,10 @@ int dgp_step(dgp_solver s, double t, double dt, double* resid);
  * Runs device-resident (CUDA graphs), no host sync per step. */
 int dgp_run(dgp_solver s, double t0, double tend, double cfl, int max_steps, double* t_out,
             int* steps_out);
-/* kernels one step of dgp_run launches (face/element kernels per stage, the
- * P0 fallback's second face pass, limiter passes and the CFL reduction; with
+/* kernels one step of dgp_run launches (the fused stage kernel per stage and
+ * the finalize of the last; or face/element kernels per stage with the P0
+ * fallback's volume check and second face pass), limiter passes and the CFL
+ * reduction; with
  * local time stepping the kernels of one advanceInTime, the step's end and the
  * CFL reduction) */
 int dgp_launches_per_step(dgp_solver s, int* n);

@@ -1696,16 +1696,27 @@ static int or_is_physical(const or_solver* s, const double* Q) {
   return 1;
 }
 
-/* assembly of one stage with the P0 fallback of DGAnalysis.cc:392-417 and
- * DGCell::setToZero (DGCell.cc:785-811): cells with a non-physical trace at
- * a face point drop their modes k >= 1, then the RHS is assembled again.  All
- * marked cells are zeroed before the second assembly. */
+/* assembly of one stage with the P0 fallback: a cell with a non-physical
+ * value at a volume quadrature point (the correction inside
+ * DGCell::computeVolumeContribution, DGCell.cc:197-221, which runs before the
+ * faces) or with a non-physical trace at a face point (the code of
+ * computeBoundaryContributions, DGCell.cc:639-732, then DGCell::setToZero,
+ * DGCell.cc:785-811, in the serial order of DGAnalysis.cc:392-417) drops its
+ * modes k >= 1, and the RHS is assembled again.  The volume correction leaves
+ * the zeroed cells with physical means, so the face check sees the same
+ * cells either way: all marked cells are zeroed before the second assembly. */
 static int assemble_stage(or_solver* s, double t, double* R) {
   assemble(s, s->C, t, R);
   if (!s->p0) return 0;
   const int m = s->m, Np = s->Np;
   int nbad = 0;
   memset(s->bad, 0, (size_t)s->E);
+  for (int e = 0; e < s->E; ++e)
+    for (int q = 0; q < s->nq; ++q) {
+      double U[MAXM];
+      interp(s->phi[q], s->C + (size_t)e * m * Np, m, Np, U);
+      if (!or_is_physical(s, U)) s->bad[e] = 1;
+    }
   for (int f = 0; f < s->F; ++f)
     for (int q = 0; q < s->nqf; ++q) {
       double U[MAXM];
@@ -1727,6 +1738,11 @@ static int assemble_stage(or_solver* s, double t, double* R) {
 }
 
 void or_bad_cells(const or_solver* s, unsigned char* out) { memcpy(out, s->bad, (size_t)s->E); }
+
+/* the right-hand side of one assembly with the P0 fallback (when on): the
+ * marked cells' modes k >= 1 are zeroed in the state, as setToZero does;
+ * returns the number of marked cells */
+int or_rhs_p0(or_solver* s, double t, double* out) { return assemble_stage(s, t, out); }
 
 void or_triggers(const or_solver* s, unsigned char* out) { memcpy(out, s->trig, (size_t)s->E); }
 

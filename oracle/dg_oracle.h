@@ -45,6 +45,7 @@ void or_get_state(const or_solver* s, double* out);    /* [E][m][Np] file order 
 void or_set_state(or_solver* s, const double* in);
 void or_project(or_solver* s, double t);                /* L2 projection of the field */
 void or_rhs(or_solver* s, double t, double* out);       /* assembled RHS, not scaled */
+int or_rhs_p0(or_solver* s, double t, double* out);
 double or_cfl_dt(const or_solver* s, double cfl);
 double or_step(or_solver* s, double t, double dt);      /* SSP-RK3, returns resid */
 double or_run(or_solver* s, double t0, double tend, double cfl, int nsteps, int* steps_done);

@@ -201,6 +201,8 @@ static int ltsSortCells(mDGMesh* mesh, int n) {
 
 struct Params {
   std::string mesh, caseName = "gauss", flux = "exact", conn, rhs, state, log, barth, ckptOut, ckptIn, l2, stateBin;
+  std::string p0rhs, p0cells;  // P0 fallback fixture: output file, perturbed cells
+  double p0amp = 3.0;
   int order = 2, steps = 0, every = 1, threads = 1, bench = 0, warmup = 0, gpu = 0, lts = 0;
   std::string bins;
   double cfl = 0.1, tend = -1.0;
@@ -390,6 +392,7 @@ static void usage() {
   fprintf(stderr, "usage: ref_driver --mesh F.msh [--case gauss|vortex|pulse3d|sine|gauss3d] "
                   "[--flux exact|roe] [--order p] [--steps n | --tend T] [--cfl c] "
                   "[--conn F] [--rhs F] [--state F --every k] [--log F] [--barth F] [--l2 F] [--state-bin F] [--ckpt-in F] [--ckpt-out F] "
+                  "[--p0-rhs F --p0-cells e,e,... [--p0-amp a]] "
                   "[--threads k --bench n]\n");
   exit(1);
 }
@@ -417,6 +420,9 @@ int main(int argc, char** argv) {
     else if (a == "--barth") P.barth = v;
     else if (a == "--l2") P.l2 = v;
     else if (a == "--state-bin") P.stateBin = v;
+    else if (a == "--p0-rhs") P.p0rhs = v;
+    else if (a == "--p0-cells") P.p0cells = v;
+    else if (a == "--p0-amp") P.p0amp = atof(v);
     else if (a == "--ckpt-out") P.ckptOut = v;
     else if (a == "--ckpt-in") P.ckptIn = v;
     else if (a == "--gpu") P.gpu = atoi(v);
@@ -587,6 +593,63 @@ int main(int argc, char** argv) {
       cell->read(is);
       cell->computeMean();
     }
+  }
+
+  // The P0 fallback as DGAnalysis's serial assembly applies it
+  // (DGAnalysis.cc:392-417): every volume and face contribution first,
+  // collecting the cells with a non-physical trace, then DGCell::setToZero on
+  // each of them.  The state: the projection with the listed cells' first
+  // field pushed away from its mean (modes k >= 1 += a|c_0|, the sign
+  // alternating over the list).  Writes "E m Np n", the n zeroed cells (file
+  // order, as listed), the perturbed state, the state after the fallback
+  // (the volume correction zeroes cells too) and the right-hand side.
+  if (!P.p0rhs.empty()) {
+    std::vector<int> pert;
+    for (const char* c = P.p0cells.c_str(); *c;) {
+      pert.push_back(atoi(c));
+      while (*c && *c != ',') ++c;
+      if (*c == ',') ++c;
+    }
+    for (size_t k = 0; k < pert.size(); ++k) {
+      DGCell* cell = byFile[pert[k]];
+      const double a = (k % 2 ? -1.0 : 1.0) * P.p0amp * fabs(cell->theFieldsCoefficients->get(0, 0));
+      for (int j = 1; j < Np; ++j) cell->theFieldsCoefficients->get(0, j) += a;
+      cell->computeMean();
+    }
+    std::vector<double> perturbed((size_t)E * m * Np);
+    for (int e = 0; e < E; ++e)
+      for (int i = 0; i < m; ++i)
+        for (int j = 0; j < Np; ++j) perturbed[((size_t)e * m + i) * Np + j] = byFile[e]->theFieldsCoefficients->get(i, j);
+    for (int e = 0; e < E; ++e) byFile[e]->ZeroRHS();
+    for (mMesh::iter it = mesh->begin(dim); it != mesh->end(dim); ++it)
+      ((DGCell*)(*it)->getCell())->computeVolumeContribution(0.0);
+    std::vector<DGCell*> zero;
+    for (mMesh::iter it = mesh->begin(dim - 1); it != mesh->end(dim - 1); ++it) {
+      DGBoundaryCell* bc = (DGBoundaryCell*)(*it)->getCell();
+      const int np = bc->computeBoundaryContributions(0.0);
+      if (np == 1 || np == 3) zero.push_back((DGCell*)bc->getLeftCell());
+      if (np == 2 || np == 3) zero.push_back((DGCell*)bc->getRightCell());
+    }
+    for (size_t k = 0; k < zero.size(); ++k) zero[k]->setToZero(0.0);
+    FILE* f = fopen(P.p0rhs.c_str(), "w");
+    fprintf(f, "%d %d %d %d\n", E, m, Np, (int)zero.size());
+    for (size_t k = 0; k < zero.size(); ++k) fprintf(f, "%d ", cellIndex(mc, zero[k]->getMeshEntity()));
+    fprintf(f, "\n");
+    for (int e = 0; e < E; ++e) {
+      for (int j = 0; j < m * Np; ++j) fprintf(f, "%.17g ", perturbed[(size_t)e * m * Np + j]);
+      fprintf(f, "\n");
+    }
+    for (int e = 0; e < E; ++e) {
+      for (int i = 0; i < m; ++i)
+        for (int j = 0; j < Np; ++j) fprintf(f, "%.17g ", byFile[e]->theFieldsCoefficients->get(i, j));
+      fprintf(f, "\n");
+    }
+    for (int e = 0; e < E; ++e) {
+      for (int j = 0; j < m * Np; ++j) fprintf(f, "%.17g ", byFile[e]->theRightHandSide[j]);
+      fprintf(f, "\n");
+    }
+    fclose(f);
+    return 0;
   }
 
   if (!P.rhs.empty()) {

@@ -12,6 +12,8 @@ case, the mesh file and an .npz with:
 * ``rhs``    assembled right-hand side of the projected state at t = 0
 * ``log``    per step: dt, time, residual
 
+(further case tables below store what their comment names)
+
 The reference run uses one worker thread so that stage times are honoured (see
 oracle/ref_driver.cc).  Usage: python tests/golden/make_golden.py [case ...]
 (the local time stepping cases need ``make -C oracle ref_lts``)
@@ -101,6 +103,45 @@ L2_CASES = {
     "l2_euler_roe_p3": ("tri", dict(nx=8, ny=8, x0=0.0, x1=10.0, y0=0.0, y1=10.0, seed=2),
                         ["--case", "vortex", "--flux", "roe", "--order", "3"], 5),
 }
+
+# The P0 fallback (DGCell::setToZero) as the reference's serial assembly
+# applies it (DGAnalysis.cc:392-417): the projected vortex with the listed
+# cells' density pushed away from its mean by a|c_0| (ref_driver --p0-rhs;
+# cell 34 shares an edge with cell 37).  ``state`` the perturbed state,
+# ``after`` the state after the fallback, ``rhs`` the right-hand side,
+# ``dropped`` the cells whose modes k >= 1 were zeroed (by the volume
+# correction of computeVolumeContribution or by the faces), ``zeroed_by_faces``
+# the setToZero calls of the face pass (file order, repeats kept).  The cases
+# reach the volume correction alone, the face pass alone, and both.
+P0_BOX = dict(nx=10, ny=10, x0=0.0, x1=10.0, y0=0.0, y1=10.0, jitter=0.15, seed=2)
+P0_VORTEX = ["--case", "vortex", "--flux", "roe"]
+P0_CASES = {
+    "p0_euler_roe_p2_volume": ("tri", P0_BOX, P0_VORTEX + ["--order", "2"], [37, 80], 3.0),
+    "p0_euler_roe_p1_faces": ("tri", P0_BOX, P0_VORTEX + ["--order", "1"], [37, 34, 120, 80], 0.3),
+    "p0_euler_roe_p1_both": ("tri", P0_BOX, P0_VORTEX + ["--order", "1"], [37, 34, 120, 80], 0.4),
+    "p0_euler_roe_p3_both": ("tri", P0_BOX, P0_VORTEX + ["--order", "3"], [37, 34, 120, 80], 0.2),
+}
+
+
+def run_p0_case(name, kind, margs, dargs, cells, amp):
+    mesh = build_mesh(kind, margs)
+    msh = os.path.join(HERE, name + ".msh")
+    meshgen.write_msh_v1(mesh, msh)
+    with tempfile.TemporaryDirectory() as td:
+        out = os.path.join(td, "p0")
+        cmd = [DRIVER, "--mesh", msh, "--p0-rhs", out, "--p0-cells", ",".join(map(str, cells)),
+               "--p0-amp", repr(amp)] + dargs
+        subprocess.run(cmd, check=True, capture_output=True)
+        lines = open(out).read().split("\n")
+        E, m, Np, nz = map(int, lines[0].split())
+        zeroed = np.array(list(map(int, lines[1].split())), dtype=np.int64)
+        rows = np.array([list(map(float, ln.split())) for ln in lines[2:2 + 3 * E]])
+    state, after = rows[:E].reshape(E, m, Np), rows[E:2 * E].reshape(E, m, Np)
+    dropped = np.nonzero((after != state).any(axis=(1, 2)))[0]
+    assert len(dropped) > 0, "no cell became non-physical"
+    np.savez_compressed(os.path.join(HERE, name + ".npz"), state=state, after=after,
+                        rhs=rows[2 * E:].reshape(E, m, Np), zeroed_by_faces=zeroed, dropped=dropped,
+                        cells=np.array(cells), amp=amp, args=np.array(dargs))
 
 
 def run_size_case(name, kind, margs, dargs, steps):
@@ -279,6 +320,11 @@ def main():
         if only and name not in only:
             continue
         run_l2_case(name, kind, margs, dargs, steps)
+        print("wrote", name)
+    for name, (kind, margs, dargs, cells, amp) in P0_CASES.items():
+        if only and name not in only:
+            continue
+        run_p0_case(name, kind, margs, dargs, cells, amp)
         print("wrote", name)
 
 

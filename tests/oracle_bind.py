@@ -42,6 +42,8 @@ def lib():
     L.or_set_state.argtypes = [P, pD]
     L.or_project.argtypes = [P, D]
     L.or_rhs.argtypes = [P, D, pD]
+    L.or_rhs_p0.argtypes = [P, D, pD]
+    L.or_rhs_p0.restype = I
     L.or_cfl_dt.argtypes = [P, D]
     L.or_cfl_dt.restype = D
     L.or_step.argtypes = [P, D, D]
@@ -108,6 +110,13 @@ class Oracle:
         out = np.zeros(self.shape)
         lib().or_rhs(self.h, t, _dp(out))
         return out
+
+    def rhs_p0(self, t):
+        """RHS of one assembly with the P0 fallback (when on); the marked
+        cells' modes k >= 1 are zeroed in the state.  (rhs, marked cells)"""
+        out = np.zeros(self.shape)
+        n = lib().or_rhs_p0(self.h, t, _dp(out))
+        return out, n
 
     def cfl_dt(self, cfl):
         return lib().or_cfl_dt(self.h, cfl)
