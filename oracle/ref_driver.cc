@@ -202,6 +202,7 @@ static int ltsSortCells(mDGMesh* mesh, int n) {
 struct Params {
   std::string mesh, caseName = "gauss", flux = "exact", conn, rhs, state, log, barth, ckptOut, ckptIn, l2, stateBin;
   std::string p0rhs, p0cells;  // P0 fallback fixture: output file, perturbed cells
+  std::string probeOut, probePts;  // point sensors: output file, "x,y,z;x,y,z;..."
   double p0amp = 3.0;
   int order = 2, steps = 0, every = 1, threads = 1, bench = 0, warmup = 0, gpu = 0, lts = 0;
   std::string bins;
@@ -392,7 +393,7 @@ static void usage() {
   fprintf(stderr, "usage: ref_driver --mesh F.msh [--case gauss|vortex|pulse3d|sine|gauss3d] "
                   "[--flux exact|roe] [--order p] [--steps n | --tend T] [--cfl c] "
                   "[--conn F] [--rhs F] [--state F --every k] [--log F] [--barth F] [--l2 F] [--state-bin F] [--ckpt-in F] [--ckpt-out F] "
-                  "[--p0-rhs F --p0-cells e,e,... [--p0-amp a]] "
+                  "[--p0-rhs F --p0-cells e,e,... [--p0-amp a]] [--probe-out F --probe-pts x,y,z;...] "
                   "[--threads k --bench n]\n");
   exit(1);
 }
@@ -423,6 +424,8 @@ int main(int argc, char** argv) {
     else if (a == "--p0-rhs") P.p0rhs = v;
     else if (a == "--p0-cells") P.p0cells = v;
     else if (a == "--p0-amp") P.p0amp = atof(v);
+    else if (a == "--probe-out") P.probeOut = v;
+    else if (a == "--probe-pts") P.probePts = v;
     else if (a == "--ckpt-out") P.ckptOut = v;
     else if (a == "--ckpt-in") P.ckptIn = v;
     else if (a == "--gpu") P.gpu = atoi(v);
@@ -771,6 +774,32 @@ int main(int argc, char** argv) {
       for (int i = 0; i < m; ++i)
         for (int j = 0; j < Np; ++j) row[i * Np + j] = byFile[e]->theFieldsCoefficients->get(i, j);
       fwrite(row.data(), sizeof(double), row.size(), f);
+    }
+    fclose(f);
+  }
+  if (!P.probeOut.empty()) {
+    // DGPointSensor::eval (DGSensor.cc:170-186) at the final time: the field
+    // values at each point from DGCell::inCell (DGCell.cc:1499-1521) of the
+    // first cell (file order) that contains it; "i cell v_0 .. v_m-1", cell -1
+    // (and no values) for a point outside the mesh
+    FILE* f = fopen(P.probeOut.c_str(), "w");
+    int i = 0;
+    for (const char* c = P.probePts.c_str(); *c; ++i) {
+      double x[3] = {0.0, 0.0, 0.0};
+      for (int k = 0; k < 3 && *c; ++k) {
+        x[k] = atof(c);
+        while (*c && *c != ',' && *c != ';') ++c;
+        if (*c == ',') ++c;
+      }
+      if (*c == ';') ++c;
+      double val[MaxNbEqn];
+      int found = -1;
+      for (int e = 0; e < E && found < 0; ++e)
+        if (byFile[e]->inCell(mPoint(x[0], x[1], x[2]), val)) found = e;
+      fprintf(f, "%d %d", i, found);
+      if (found >= 0)
+        for (int k = 0; k < m; ++k) fprintf(f, " %.17g", val[k]);
+      fprintf(f, "\n");
     }
     fclose(f);
   }

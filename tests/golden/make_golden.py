@@ -143,6 +143,55 @@ def run_p0_case(name, kind, margs, dargs, cells, amp):
                         rhs=rows[2 * E:].reshape(E, m, Np), zeroed_by_faces=zeroed, dropped=dropped,
                         cells=np.array(cells), amp=amp, args=np.array(dargs))
 
+# Point sensors (DGPointSensor, DGCell::inCell) after a few steps, at seeded
+# points inside the domain and one outside it (ref_driver --probe-out):
+# ``points``, ``cell`` (-1 outside), ``values`` [point][field] (NaN outside),
+# ``state`` the final state.
+def probe_points(kind, seed, n):
+    rng = np.random.default_rng(seed)
+    if kind == "tri":
+        p = np.zeros((n + 1, 3))
+        p[:n, :2] = rng.uniform(0.3, 9.7, size=(n, 2))
+        p[n, :2] = (12.0, 5.0)
+    else:
+        p = rng.uniform(0.05, 0.95, size=(n + 1, 3))
+        p[n] = (1.5, 0.5, 0.5)
+    return p
+
+
+PROBE_CASES = {
+    "probes_euler_roe_p2": ("tri", dict(nx=6, ny=6, x0=0.0, x1=10.0, y0=0.0, y1=10.0, seed=2),
+                            ["--case", "vortex", "--flux", "roe", "--order", "2"], 3, 16),
+    "probes_scalar_tet_p2": ("tet", dict(n=2, seed=3),
+                             ["--case", "gauss3d", "--order", "2", "--ax", "1", "--ay", "0.5", "--az", "0.25",
+                              "--cx", "0.5", "--cy", "0.5", "--cz", "0.5", "--s", "0.05"], 3, 12),
+}
+
+
+def run_probe_case(name, kind, margs, dargs, steps, npts):
+    mesh = build_mesh(kind, margs)
+    msh = os.path.join(HERE, name + ".msh")
+    meshgen.write_msh_v1(mesh, msh)
+    pts = probe_points(kind, 11, npts)
+    with tempfile.TemporaryDirectory() as td:
+        out, state = os.path.join(td, "p"), os.path.join(td, "s")
+        cmd = [DRIVER, "--mesh", msh, "--steps", str(steps), "--cfl", "0.1", "--state", state,
+               "--every", str(steps), "--probe-out", out,
+               "--probe-pts", ";".join(",".join(repr(float(v)) for v in p) for p in pts)] + dargs
+        subprocess.run(cmd, check=True, capture_output=True)
+        rows = [list(map(float, ln.split())) for ln in open(out) if ln.strip()]
+        blocks = open(state).read().split("step ")[1:]
+        st = np.array([list(map(float, ln.split())) for ln in blocks[-1].split("\n")[1:] if ln.strip()])
+    m = max(len(r) for r in rows) - 2
+    cell = np.array([int(r[1]) for r in rows], dtype=np.int64)
+    vals = np.full((len(rows), m), np.nan)
+    for i, r in enumerate(rows):
+        if r[1] >= 0:
+            vals[i] = r[2:]
+    assert (cell >= 0).sum() == npts and cell[-1] == -1
+    np.savez_compressed(os.path.join(HERE, name + ".npz"), points=pts, cell=cell, values=vals, state=st,
+                        args=np.array(dargs), steps=steps)
+
 
 def run_size_case(name, kind, margs, dargs, steps):
     mesh = build_mesh(kind, margs)
@@ -320,6 +369,11 @@ def main():
         if only and name not in only:
             continue
         run_l2_case(name, kind, margs, dargs, steps)
+        print("wrote", name)
+    for name, (kind, margs, dargs, steps, npts) in PROBE_CASES.items():
+        if only and name not in only:
+            continue
+        run_probe_case(name, kind, margs, dargs, steps, npts)
         print("wrote", name)
     for name, (kind, margs, dargs, cells, amp) in P0_CASES.items():
         if only and name not in only:

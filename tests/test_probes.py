@@ -5,7 +5,7 @@ import pytest
 
 import dgp
 from dgp import meshgen
-from cases import VORTEX
+from cases import REF_TOL, SCALAR3D, VORTEX, golden, rel
 
 
 def test_line_points_match_the_line_sensor_samples():
@@ -102,3 +102,26 @@ def test_gpu_probe_records_inside_the_run(prec):
     pr.close()
     s.close()
     s2.close()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name,law,flux,field,prm", [
+    ("probes_euler_roe_p2", dgp.LAW_EULER2D, dgp.FLUX_ROE, dgp.FIELD_VORTEX, VORTEX),
+    ("probes_scalar_tet_p2", dgp.LAW_SCALAR, dgp.FLUX_UPWIND, dgp.FIELD_GAUSS3D, SCALAR3D),
+])
+def test_gpu_probes_match_reference_point_sensor(name, law, flux, field, prm):
+    """Pinned against DG-Parallel's own point evaluation (DGPointSensor through
+    DGCell::inCell) on the reference's state after three steps: the same points
+    found, the same values to the basis-table floor."""
+    msh, g = golden(name)
+    order = int(list(g["args"])[list(g["args"]).index("--order") + 1])
+    s = dgp.Solver(dgp.Mesh.from_msh(msh), dgp.Law(law, flux, field, prm), order, dgp.FP64)
+    E = s.ncells
+    s.set_state(g["state"].reshape(E, s.nfields, -1))
+    pts = g["points"][:, : (2 if "tet" not in name else 3)]
+    pr = dgp.Probe(s, pts)
+    assert np.array_equal(pr.found, g["cell"] >= 0)
+    v = pr.eval()
+    ok = g["cell"] >= 0
+    assert np.isnan(v[~ok]).all()
+    assert rel(v[ok], g["values"][ok]) < REF_TOL[order]
