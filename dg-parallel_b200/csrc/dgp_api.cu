@@ -77,6 +77,37 @@ void set_tuned_block(int law, int flux, int dim, int order, int precision, long 
   g_tune[std::make_tuple(law, flux, dim, order, precision, size_bucket(cells))] = block;
 }
 
+// Fused stage kernel or separate face and element kernels, per (law, flux,
+// element, order, precision, size bucket): the autotuner's measurement where
+// there is one, else the default below.  The default follows measurements on
+// B200 (128-thread tiles, 131k-180k triangles, 196k-663k tets; step time of
+// the separate kernels over the fused one): the fused kernel wins for the 2D
+// Euler (Roe, LLF), scalar and Maxwell laws at P2-P3 (1.10-1.45x), Euler P1
+// (1.08x) and P1 on tets (scalar P2: 1.11x, 1.21-1.38x); the separate kernels
+// win for Burgers (up to 1.56x), the exact Godunov flux, P4 on triangles (up to
+// 2x), the 3D Euler law and tets of higher order (1.07-1.43x), where the fused
+// tile's halo (rows read and faces evaluated by two tiles) and its larger
+// shared memory cost more than the face data the separate kernels pass
+// through device memory.
+std::map<std::tuple<int, int, int, int, int, int>, int> g_tune_fused;
+
+bool fused_default(int law, int flux, int dim, int order) {
+  if (law == DGP_LAW_BURGERS2D || law == DGP_LAW_EULER3D || flux == DGP_FLUX_GODUNOV) return false;
+  if (dim == 2) return order == 2 || order == 3 || (order == 1 && law == DGP_LAW_EULER2D);
+  return order == 1 || (law == DGP_LAW_SCALAR && order == 2);
+}
+
+bool tuned_fused(int law, int flux, int dim, int order, int precision, long long cells) {
+  std::lock_guard<std::mutex> lock(g_tune_mutex);
+  auto it = g_tune_fused.find(std::make_tuple(law, flux, dim, order, precision, size_bucket(cells)));
+  return it == g_tune_fused.end() ? fused_default(law, flux, dim, order) : it->second != 0;
+}
+
+void set_tuned_fused(int law, int flux, int dim, int order, int precision, long long cells, bool fused) {
+  std::lock_guard<std::mutex> lock(g_tune_mutex);
+  g_tune_fused[std::make_tuple(law, flux, dim, order, precision, size_bucket(cells))] = fused ? 1 : 0;
+}
+
 bool has_block(int law, int flux, int dim, int order, int precision, int block) {
   ensure_registry();
   return ops_registry().count(OpsKey(law, flux, dim, order, precision, block)) != 0;
@@ -302,8 +333,11 @@ static int build_tiles(dgp_solver s, int Etot, const std::vector<int>& fel, cons
     th_off.push_back(static_cast<int>(th_cell.size()));
     nh_max = std::max(nh_max, static_cast<int>(halo.size()));
   }
-  s->fused = s->ops.fused != nullptr && nh_max <= TE * nlf && s->ops.fused_smem(nh_max) + 8 * 1024 <= 227 * 1024;
-  if (!s->fused) return DGP_OK;
+  s->fused_ok = s->ops.fused != nullptr && nh_max <= TE * nlf && s->ops.fused_smem(nh_max) + 8 * 1024 <= 227 * 1024;
+  long long cells = 0;
+  for (const auto& hm : s->meshes) cells += hm.E;
+  s->fused = s->fused_ok && tuned_fused(s->law, s->flux, dim, s->order, s->precision, cells);
+  if (!s->fused_ok) return DGP_OK;
   TileMesh& tm = s->b.tm;
   int rc = DGP_OK;
   int *d_tf_off, *d_tf_side, *d_tf_code, *d_tf_bnd, *d_th_off, *d_th_cell;
@@ -548,7 +582,7 @@ static int build_solver(dgp_solver s, const std::vector<LawParams>& lps, int fie
   DGP_CUDA(cudaMemset(tr, 0, nslot * ts));
   DGP_CUDA(cudaMemset(C, 0, nstate * 8 + 256));
   DGP_CUDA(cudaMemset(U0, 0, nstate * 8 + 256));
-  if (s->fused) {  // stage states u1, u2 (with the same tail as the state)
+  if (s->fused_ok) {  // stage states u1, u2 (with the same tail as the state)
     unsigned char *X1, *X2;
     if ((rc = s->alloc(&X1, nstate * 8 + 256)) || (rc = s->alloc(&X2, nstate * 8 + 256))) return rc;
     DGP_CUDA(cudaMemset(X1, 0, nstate * 8 + 256));
@@ -1745,6 +1779,7 @@ int dgp_autotune(dgp_mesh mh, dgp_law law, int order, int precision, int limiter
   const HostMesh& m = mh->m;
   int best = 0;
   float best_ms = 0;
+  bool best_fused = false;
   for (int v = 0; v < 3; ++v) {
     if (ms_per_step) ms_per_step[v] = -1.0f;
     const int block = kTileBlocks[v];
@@ -1752,18 +1787,31 @@ int dgp_autotune(dgp_mesh mh, dgp_law law, int order, int precision, int limiter
     set_tuned_block(law->kind, law->flux, m.dim, order, precision, m.E, block);
     dgp_solver s = nullptr;
     if (int rc = dgp_solver_create(mh, law, order, precision, limiter, &s)) return rc;
+    // both stage forms where the fused kernel is built
     float ms = 0;
-    int rc = time_steps(s, iters, &ms);
+    bool fused = false;
+    int rc = DGP_OK;
+    for (int f = 0; f < (s->fused_ok ? 2 : 1) && !rc; ++f) {
+      if (s->fused_ok) rc = dgp_set_fused(s, f);
+      float t = 0;
+      if (!rc) rc = time_steps(s, iters, &t);
+      if (!rc && (f == 0 || t < ms)) {
+        ms = t;
+        fused = f == 1;
+      }
+    }
     dgp_solver_destroy(s);
     if (rc) return rc;
     if (ms_per_step) ms_per_step[v] = ms;
     if (!best || ms < best_ms) {
       best = block;
       best_ms = ms;
+      best_fused = fused;
     }
   }
   if (!best) return fail(DGP_ERR_UNSUPPORTED, "no kernels for this law/flux/element/order/precision");
   set_tuned_block(law->kind, law->flux, m.dim, order, precision, m.E, best);
+  set_tuned_fused(law->kind, law->flux, m.dim, order, precision, m.E, best_fused);
   if (best_block) *best_block = best;
   return DGP_OK;
 }
@@ -1792,6 +1840,7 @@ int dgp_autotune_ensemble(int n, const dgp_mesh* meshes, const dgp_law* laws, co
     }
     int best = 0;
     float best_ms = 0;
+    bool best_fused = false;
     for (int block : kTileBlocks) {
       if (!has_block(law, flux, dim, order, precision, block)) continue;
       set_tuned_block(law, flux, dim, order, precision, cells, block);
@@ -1799,16 +1848,25 @@ int dgp_autotune_ensemble(int n, const dgp_mesh* meshes, const dgp_law* laws, co
       if (int rc = dgp_ensemble_create(static_cast<int>(ms.size()), ms.data(), ls.data(), os.data(), precision,
                                        limiter, &e))
         return rc;
-      float t = 0;
-      int rc = time_steps(e->groups[0], iters, &t);
+      dgp_solver g = e->groups[0];
+      int rc = DGP_OK;
+      for (int f = 0; f < (g->fused_ok ? 2 : 1) && !rc; ++f) {
+        if (g->fused_ok) rc = dgp_set_fused(g, f);
+        float t = 0;
+        if (!rc) rc = time_steps(g, iters, &t);
+        if (!rc && (!best || t < best_ms)) {
+          best = block;
+          best_ms = t;
+          best_fused = g->fused_ok && f == 1;
+        }
+      }
       dgp_ensemble_destroy(e);
       if (rc) return rc;
-      if (!best || t < best_ms) {
-        best = block;
-        best_ms = t;
-      }
     }
-    if (best) set_tuned_block(law, flux, dim, order, precision, cells, best);
+    if (best) {
+      set_tuned_block(law, flux, dim, order, precision, cells, best);
+      set_tuned_fused(law, flux, dim, order, precision, cells, best_fused);
+    }
   }
   return DGP_OK;
 }
@@ -1830,6 +1888,25 @@ int dgp_solver_block(dgp_solver s, int* block, int* cells_per_tile) {
 int dgp_solver_fused(dgp_solver s, int* fused) {
   if (!s || !fused) return fail(DGP_ERR_INVALID, "null argument");
   *fused = s->fused ? 1 : 0;
+  return DGP_OK;
+}
+
+int dgp_set_fused(dgp_solver s, int on) {
+  if (!s) return fail(DGP_ERR_INVALID, "null solver");
+  if (on && !s->fused_ok)
+    return fail(DGP_ERR_UNSUPPORTED, "no fused stage kernel for this solver (a tile's halo does not fit)");
+  if (on == (s->fused ? 1 : 0)) return DGP_OK;
+  DGP_CUDA(cudaSetDevice(s->device));
+  s->drop_graphs();
+  if (!on) {
+    // the face kernel reads the face-point traces, which fused stages do not keep
+    s->ops.trace(s->b, nullptr, s->stream);
+    DGP_CUDA(cudaGetLastError());
+    s->tr_stale = false;
+    s->b.tensor_cores = 0;
+    s->b.round_mask = 0;
+  }
+  s->fused = on != 0;
   return DGP_OK;
 }
 

@@ -122,6 +122,7 @@ struct dgp_solver_s {
   dgp::TimeCtl* h_ctl = nullptr;  // pinned, 2 entries
   LtsState lts;                    // local time stepping (off unless enabled)
   bool fused = false;              // stages run through the fused stage kernel
+  bool fused_ok = false;           // the fused stage kernel is built for this solver
   bool tr_stale = false;           // the face-point traces (tr) lag the state (the fused
                                    // kernel keeps none; the local time stepping kernels read them)
   void drop_graphs() {

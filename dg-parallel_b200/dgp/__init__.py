@@ -117,6 +117,7 @@ def lib() -> ctypes.CDLL:
         "dgp_backward": ([P, pD, pD], I),
         "dgp_solver_block": ([P, pI, pI], I),
         "dgp_solver_fused": ([P, pI], I),
+        "dgp_set_fused": ([P, I], I),
         "dgp_ensemble_group_block": ([P, I, pI, pI], I),
     }
     for name, (args, res) in sig.items():
@@ -353,6 +354,11 @@ class Solver:
         f = ctypes.c_int()
         check(lib().dgp_solver_fused(self.h, ctypes.byref(f)))
         return bool(f.value)
+
+    def set_fused(self, on: bool = True):
+        """Stages as the fused stage kernel (True) or as the separate face and
+        element kernels (False)."""
+        check(lib().dgp_set_fused(self.h, 1 if on else 0))
 
     def set_p0_fallback(self, on: bool = True):
         check(lib().dgp_set_p0_fallback(self.h, 1 if on else 0))

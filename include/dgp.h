@@ -286,6 +286,12 @@ int dgp_profile_kernels(dgp_solver s, int iters, float* ms);
  * lift and the SSP-RK3 update of a tile of cells), 0 when it runs as the face
  * and element kernels (a tile's halo too large for shared memory) */
 int dgp_solver_fused(dgp_solver s, int* fused);
+/* run the stages as the fused stage kernel (on = 1, the default where it is
+ * built) or as the separate face and element kernels (on = 0; also turns off
+ * the tensor-core contraction and the rounding probe, which only the fused
+ * kernel has); DGP_ERR_UNSUPPORTED when on = 1 and the fused kernel is not
+ * built for the solver */
+int dgp_set_fused(dgp_solver s, int on);
 /* Assembled right-hand side that allocates no device memory; no counterpart in
  * DG-Parallel.  For callers that cannot call cudaMalloc when they need a RHS
  * (device memory owned by another allocator, or no tolerance for the
@@ -353,8 +359,14 @@ int dgp_backward(dgp_solver s, const double* dJ_duT, double* dJ_du0);
  * problem size.  Each candidate is timed over `iters` SSP-RK3 steps with CUDA
  * events; the winner is recorded in a process-wide table keyed by (law, flux,
  * element, order, precision, floor(log2 cells)) that dgp_solver_create and
- * dgp_ensemble_create consult (128 threads when nothing is recorded).
- * ms_per_step[3] (may be NULL) gets each candidate's time, -1 where not built. */
+ * dgp_ensemble_create consult (128 threads when nothing is recorded).  For
+ * each shape both stage forms are timed where the fused stage kernel is built
+ * (dgp_set_fused), and the faster is recorded with it (without a record, a
+ * default measured on B200 decides: fused for the 2D Euler (Roe, LLF), scalar
+ * and Maxwell laws at P2-P3, 2D Euler P1 and P1 on tets (scalar: P2); the
+ * separate kernels for Burgers, the exact Godunov flux, 2D P4, the 3D Euler law
+ * and tets of higher order).  ms_per_step[3] (may be NULL) gets each shape's best time, -1
+ * where not built. */
 int dgp_autotune(dgp_mesh m, dgp_law law, int order, int precision, int limiter, int iters, int* best_block,
                  float* ms_per_step);
 /* the same for every (law, flux, element, order) group of an ensemble */

@@ -82,8 +82,12 @@ ORACLE_CASES = [
 PARAMS = [(c[0], o) for c in ORACLE_CASES for o in c[7]]
 
 
+@pytest.mark.parametrize("form", ["fused", "separate"])
 @pytest.mark.parametrize("cid,order", PARAMS)
-def test_gpu_matches_oracle(tmp_path, cid, order):
+def test_gpu_matches_oracle(tmp_path, cid, order, form):
+    """Both stage forms: the fused stage kernel and the separate face and
+    element kernels (whichever the solver picks by default, the other by
+    dgp_set_fused)."""
     case = next(c for c in ORACLE_CASES if c[0] == cid)
     _, kind, n, law, flux, field, prm, _, tag = case
     if kind == "tri":
@@ -94,6 +98,12 @@ def test_gpu_matches_oracle(tmp_path, cid, order):
         msh = _tet(tmp_path, n, tag=tag)
     o = Oracle(msh, law, flux, order, field, prm)
     s = solver_for(msh, law, flux, field, order, prm)
+    try:
+        s.set_fused(form == "fused")
+    except dgp.DGPError as e:
+        assert e.code == -3 and form == "fused"
+        pytest.skip("no fused stage kernel for this solver")
+    assert s.fused == (form == "fused")
     E = s.ncells
     assert rel(s.get_state(), o.state()) < FP64_TOL
     assert rel(s.rhs(0.0), o.rhs(0.0)) < RHS_TOL
