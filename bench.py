@@ -661,11 +661,12 @@ def configs_bench(steps=200):
         e1.synchronize()
         return e0.elapsed_time(e1) / 1e3, t_end, n
 
-    def measure(mesh, law, order, M, NP, NS, DIM, field, t_full=None):
+    def measure(mesh, law, order, M, NP, NS, DIM, field, t_full=None, rule=0):
         E, F = mesh.ncells, mesh.nfaces
-        res = {"cells": E, "faces": F, "dofs": E * M * NP}
+        res = {"cells": E, "faces": F, "dofs": E * M * NP,
+               "quadrature": "the workloads' point counts" if rule else "DG-Parallel's rules"}
         for name, prec, tsize in (("fp64", dgp.FP64, 8), ("mixed", dgp.MIXED, 4)):
-            s = dgp.Solver(mesh, law, order, prec)
+            s = dgp.Solver(mesh, law, order, prec, rule=rule)
             sec, t_end, n = timed(s, steps)
             kern = s.profile_kernels(10)
             sb = stage_formula_bytes(E, F, M, NP, DIM)
@@ -709,6 +710,8 @@ def configs_bench(steps=200):
                    dgp.law_params(velocity=(1.0, 0.5, 0.0), center=(0.3, 0.3, 0.0), width=0.01))
     out["scalar_p2_2048tri"] = measure(mesh1, law1, 2, 1, 6, 3 * 3, 2, 0)
     out["scalar_p2_2048tri"]["note"] = "launch/latency bound (12288 DOFs); not roofline-graded"
+    # the workload's stated quadrature: 7-point volume rule (degree 5)
+    out["scalar_p2_2048tri_7pt"] = measure(mesh1, law1, 2, 1, 6, 3 * 3, 2, 0, rule=dgp.RULE_WORKLOAD)
     if os.path.exists(REF_DRIVER):
         cpu = {}
         with tempfile.TemporaryDirectory() as td:
@@ -728,6 +731,9 @@ def configs_bench(steps=200):
     mesh3 = dgp.Mesh.from_arrays(3, m3.vertices, m3.cells, m3.domain_tag, m3.bfaces, m3.btags)
     law3 = dgp.Law(dgp.LAW_MAXWELL3D, dgp.FLUX_UPWIND, dgp.FIELD_TM110, dgp.law_params(cavity=1.0))
     out["maxwell3d_p2_663552tet"] = measure(mesh3, law3, 2, 6, 10, 4 * 7, 3, 2, t_full=np.sqrt(2.0))
+    # the workload's stated quadrature: 11-point volume, 6-point face rules
+    out["maxwell3d_p2_663552tet_11pt"] = measure(mesh3, law3, 2, 6, 10, 4 * 6, 3, 2, t_full=np.sqrt(2.0),
+                                                 rule=dgp.RULE_WORKLOAD)
     return out
 
 

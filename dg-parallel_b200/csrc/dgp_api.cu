@@ -110,7 +110,7 @@ void set_tuned_fused(int law, int flux, int dim, int order, int precision, long 
 
 bool has_block(int law, int flux, int dim, int order, int precision, int block) {
   ensure_registry();
-  return ops_registry().count(OpsKey(law, flux, dim, order, precision, block)) != 0;
+  return ops_registry().count(OpsKey(law, flux, dim, order, precision, block, DGP_RULE_REFERENCE)) != 0;
 }
 
 // gather cells by `perm` and convert the arithmetic type
@@ -652,11 +652,13 @@ static int build_solver(dgp_solver s, const std::vector<LawParams>& lps, int fie
 
 // common part of solver and ensemble-group creation: kernels, tables, stream
 static int solver_begin(dgp_solver s, int law, int flux, int dim, int order, int precision, int limiter,
-                        int block) {
+                        int block, int rule = DGP_RULE_REFERENCE) {
   ensure_registry();
-  auto it = ops_registry().find(OpsKey(law, flux, dim, order, precision, block));
+  auto it = ops_registry().find(OpsKey(law, flux, dim, order, precision, block, rule));
   if (it == ops_registry().end())
-    return fail(DGP_ERR_UNSUPPORTED, "no kernels for this law/flux/element/order/precision");
+    return fail(DGP_ERR_UNSUPPORTED, rule == DGP_RULE_REFERENCE
+                                         ? "no kernels for this law/flux/element/order/precision"
+                                         : "no kernels with this quadrature rule for this configuration");
   int ndev = 0;
   if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
     return fail(DGP_ERR_CUDA, "no CUDA device available");
@@ -668,7 +670,8 @@ static int solver_begin(dgp_solver s, int law, int flux, int dim, int order, int
   s->limiter = limiter;
   cudaGetDevice(&s->device);
   std::string err;
-  if (int rc = build_tables(dim, order, s->tab, err)) return fail(rc, err);
+  s->rule = rule;
+  if (int rc = build_tables(dim, order, s->tab, err, rule)) return fail(rc, err);
   const RefTables& t = s->tab;
   if (t.nq != s->ops.NQ || t.nqf != s->ops.NQF || t.Np != s->ops.NP)
     return fail(DGP_ERR_UNSUPPORTED, "table/kernel shape mismatch");
@@ -805,7 +808,13 @@ int dgp_law_destroy(dgp_law l) {
 
 int dgp_solver_create(dgp_mesh mh, dgp_law law, int order, int precision, int limiter,
                       dgp_solver* out) {
+  return dgp_solver_create_ex(mh, law, order, precision, limiter, DGP_RULE_REFERENCE, out);
+}
+
+int dgp_solver_create_ex(dgp_mesh mh, dgp_law law, int order, int precision, int limiter, int rule,
+                         dgp_solver* out) {
   if (!mh || !law || !out) return fail(DGP_ERR_INVALID, "null argument");
+  if (rule != DGP_RULE_REFERENCE && rule != DGP_RULE_WORKLOAD) return fail(DGP_ERR_INVALID, "unknown rule");
   if (precision != DGP_PRECISION_FP64 && precision != DGP_PRECISION_MIXED)
     return fail(DGP_ERR_INVALID, "unknown precision");
   if (limiter != DGP_LIMITER_NONE && limiter != DGP_LIMITER_MOMENT && limiter != DGP_LIMITER_BARTH)
@@ -819,8 +828,10 @@ int dgp_solver_create(dgp_mesh mh, dgp_law law, int order, int precision, int li
   if ((law->kind == DGP_LAW_EULER3D || law->kind == DGP_LAW_MAXWELL3D) && m.dim != 3)
     return fail(DGP_ERR_UNSUPPORTED, "3D law on a 2D mesh");
   auto s = new dgp_solver_s;
-  const int block = tuned_block(law->kind, law->flux, m.dim, order, precision, m.E);
-  if (int rc = solver_begin(s, law->kind, law->flux, m.dim, order, precision, limiter, block)) {
+  // the other rule is built for the default tile shape only
+  const int block = rule == DGP_RULE_REFERENCE ? tuned_block(law->kind, law->flux, m.dim, order, precision, m.E)
+                                               : kDefaultBlock;
+  if (int rc = solver_begin(s, law->kind, law->flux, m.dim, order, precision, limiter, block, rule)) {
     delete s;
     return rc;
   }

@@ -111,6 +111,7 @@ struct dgp_solver_s {
   dgp::Ops ops;
   dgp::DeviceBuffers b;
   int law = 0, flux = 0, order = 0, precision = 0, limiter = 0, device = 0;
+  int rule = 0;  // quadrature rule option (DGP_RULE_*)
   cudaStream_t stream = nullptr;
   std::vector<int> i2f, f2i;  // internal <-> file cell order
   int* d_i2f = nullptr;

@@ -642,7 +642,7 @@ void build_limiter_tables(const RefTables& t, std::vector<double>& D, std::vecto
   }
 }
 
-int build_tables(int dim, int order, RefTables& t, std::string& err) {
+int build_tables(int dim, int order, RefTables& t, std::string& err, int rule) {
   t = RefTables();
   t.dim = dim;
   t.order = order;
@@ -687,7 +687,8 @@ int build_tables(int dim, int order, RefTables& t, std::string& err) {
   t.phi0 = t.G[0][0];
 
   const double refm = dim == 2 ? 0.5 : 1.0 / 6.0;
-  const dgp_q_rule* vr = find_rule(dim, 2 * order);
+  const bool alt = rule == 1 && order == 2;
+  const dgp_q_rule* vr = !alt ? find_rule(dim, 2 * order) : dim == 2 ? find_rule(2, 5) : &dgp_q_tet_alt_rules[0];
   const dgp_q_rule* er = find_rule(dim, 2 * (order + 1));
   if (!vr || !er) {
     err = "no quadrature rule for this order";
@@ -733,7 +734,7 @@ int build_tables(int dim, int order, RefTables& t, std::string& err) {
       t.fqw[q] = gl[2 * q + 1];
     }
   } else {
-    const dgp_q_rule* fr = find_rule(2, 2 * order + 1);
+    const dgp_q_rule* fr = find_rule(2, alt ? 4 : 2 * order + 1);
     if (!fr) {
       err = "no face rule";
       return DGP_ERR_UNSUPPORTED;

@@ -70,7 +70,10 @@ struct RefTables {
   std::vector<double> eqp, eqw, ephi;
 };
 
-int build_tables(int dim, int order, RefTables& t, std::string& err);
+// rule 0: DG-Parallel's quadrature (volume degree 2p, tet faces degree 2p + 1);
+// rule 1: at P2 the workloads' point counts (triangle volume: the 7-point rule
+// of degree 5; tets: the 11-point volume and 6-point face rules of degree 4)
+int build_tables(int dim, int order, RefTables& t, std::string& err, int rule = 0);
 void basis_eval(const RefTables& t, const double* xi, double* out);
 // triangle moment limiter tables, per degree n a (n+1)^2 block at
 // n(n+1)(2n+1)/6: D[i][m] = d^n phi_(n,m) / du^(n-i) dv^i (constant on the

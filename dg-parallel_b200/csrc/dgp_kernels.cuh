@@ -25,22 +25,34 @@
 namespace dgp {
 
 // ---- compile-time shape of one (law, flux, dim, order, precision) ----------
-constexpr int tri_vol_points(int p) { return p == 0 ? 1 : p == 1 ? 3 : p == 2 ? 6 : p == 3 ? 12 : 16; }
-constexpr int tet_vol_points(int p) { return p == 0 ? 1 : p == 1 ? 4 : p == 2 ? 14 : 24; }
-constexpr int tet_face_points(int p) { return p == 0 ? 1 : p == 1 ? 4 : p == 2 ? 7 : 13; }
+// Quadrature points.  Rule 0: DG-Parallel's rules (volume degree 2p, tet faces
+// 2p+1, edges p+1 Gauss points).  Rule 1 (DGP_RULE_WORKLOAD): the point counts
+// the workloads state at P2 -- triangles the 7-point volume rule of degree 5,
+// tets the 11-point volume rule and the 6-point face rule of degree 4; every
+// other order as rule 0.
+constexpr int tri_vol_points(int p, int rule = 0) {
+  return rule == 1 && p == 2 ? 7 : p == 0 ? 1 : p == 1 ? 3 : p == 2 ? 6 : p == 3 ? 12 : 16;
+}
+constexpr int tet_vol_points(int p, int rule = 0) {
+  return rule == 1 && p == 2 ? 11 : p == 0 ? 1 : p == 1 ? 4 : p == 2 ? 14 : 24;
+}
+constexpr int tet_face_points(int p, int rule = 0) {
+  return rule == 1 && p == 2 ? 6 : p == 0 ? 1 : p == 1 ? 4 : p == 2 ? 7 : 13;
+}
 
 // BLOCK_: threads of the element and face kernels; it sets the cells per
 // element-kernel tile (TE) and the faces per face-kernel CTA, the shapes the
 // autotuner chooses among (64, 128, 256).
-template <int LAW_, int FLUX_, int DIM_, int ORDER_, typename T_, int BLOCK_ = 128>
+// RULE_: the quadrature rule option (see tri_vol_points).
+template <int LAW_, int FLUX_, int DIM_, int ORDER_, typename T_, int BLOCK_ = 128, int RULE_ = 0>
 struct Cfg {
   using T = T_;
-  static constexpr int LAW = LAW_, FLUX = FLUX_, DIM = DIM_, ORDER = ORDER_;
+  static constexpr int LAW = LAW_, FLUX = FLUX_, DIM = DIM_, ORDER = ORDER_, RULE = RULE_;
   static constexpr int M = LawTraits<LAW>::M;
   static constexpr int NP = DIM == 2 ? (ORDER + 1) * (ORDER + 2) / 2
                                      : (ORDER + 1) * (ORDER + 2) * (ORDER + 3) / 6;
-  static constexpr int NQ = DIM == 2 ? tri_vol_points(ORDER) : tet_vol_points(ORDER);
-  static constexpr int NQF = DIM == 2 ? ORDER + 1 : tet_face_points(ORDER);
+  static constexpr int NQ = DIM == 2 ? tri_vol_points(ORDER, RULE) : tet_vol_points(ORDER, RULE);
+  static constexpr int NQF = DIM == 2 ? ORDER + 1 : tet_face_points(ORDER, RULE);
   static constexpr int NLF = DIM + 1;
   static constexpr int NPERM = DIM == 2 ? 2 : 6;
   static constexpr int MNP = M * NP;

@@ -367,9 +367,10 @@ Ops make_ops() {
   o.totals = &ops_totals<K>;
   o.grid_elem = &ops_grid_elem<K>;
   o.limit = K::ORDER >= 1 ? &ops_limit<K> : nullptr;
-  o.adj_stage = adjoint_built<K>() ? &ops_adj_stage<K> : nullptr;
+  // the adjoint and local time stepping are built for the reference rule
+  if constexpr (K::RULE == 0) o.adj_stage = adjoint_built<K>() ? &ops_adj_stage<K> : nullptr;
   o.trace = &ops_trace<K>;
-  if constexpr (sizeof(typename K::T) == 8 && K::BLOCK == kDefaultBlock) {
+  if constexpr (sizeof(typename K::T) == 8 && K::BLOCK == kDefaultBlock && K::RULE == 0) {
     o.lts_vol = &ops_lts_vol<K>;
     o.lts_face = &ops_lts_face<K>;
     o.lts_lift = &ops_lts_lift<K>;
@@ -380,12 +381,12 @@ Ops make_ops() {
   return o;
 }
 
-template <int LAW, int FLUX, int DIM, int ORDER, int BLOCK = kDefaultBlock>
+template <int LAW, int FLUX, int DIM, int ORDER, int BLOCK = kDefaultBlock, int RULE = 0>
 void add_ops() {
-  ops_registry()[OpsKey(LAW, FLUX, DIM, ORDER, DGP_PRECISION_FP64, BLOCK)] =
-      make_ops<Cfg<LAW, FLUX, DIM, ORDER, double, BLOCK>>();
-  ops_registry()[OpsKey(LAW, FLUX, DIM, ORDER, DGP_PRECISION_MIXED, BLOCK)] =
-      make_ops<Cfg<LAW, FLUX, DIM, ORDER, float, BLOCK>>();
+  ops_registry()[OpsKey(LAW, FLUX, DIM, ORDER, DGP_PRECISION_FP64, BLOCK, RULE)] =
+      make_ops<Cfg<LAW, FLUX, DIM, ORDER, double, BLOCK, RULE>>();
+  ops_registry()[OpsKey(LAW, FLUX, DIM, ORDER, DGP_PRECISION_MIXED, BLOCK, RULE)] =
+      make_ops<Cfg<LAW, FLUX, DIM, ORDER, float, BLOCK, RULE>>();
 }
 
 // the other tile shapes the autotuner chooses among

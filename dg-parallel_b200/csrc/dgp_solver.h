@@ -222,7 +222,8 @@ struct Ops {
 };
 
 // law, flux, dim, order, precision, block (tile variant: 64, 128 or 256 threads)
-using OpsKey = std::tuple<int, int, int, int, int, int>;
+// (law, flux, dim, order, precision, block, quadrature rule)
+using OpsKey = std::tuple<int, int, int, int, int, int, int>;
 constexpr int kDefaultBlock = 128;
 std::map<OpsKey, Ops>& ops_registry();
 void register_scalar_ops();

@@ -12,7 +12,10 @@ volume and face integrals at the truncation-error level).  DG-Parallel selects
   points (``GaussQuadratureTet.cc:349-380``, weights scaled by 1/6 in
   ``Integrator.cc:92-97``),
 * edges: Gauss-Legendre with ``n = floor(order/2)+1`` points on [-1,1]
-  (``GaussLegendre1D.cc:271-274``).
+  (``GaussLegendre1D.cc:271-274``),
+
+and, for the solver's alternative rule option, Keast's 11-point tet rule of
+degree 4 (the triangle alternatives are rules of the table above).
 
 Each rule is written here as its orbit structure (barycentric symmetry classes)
 with a low-precision seed for every orbit parameter and weight; the seed only
@@ -75,6 +78,12 @@ TET_RULES = {
     8: [("S4", -0.235962), ("S31", 0.127471, 0.024488), ("S31", 0.032079, 0.003949),
         ("S22", 0.049777, 0.026306), ("S22", 0.18373, 0.08298),
         ("S211", 0.231901, 0.022918, 0.025443), ("S211", 0.03797, 0.193746, 0.013432)],
+}
+# Alternative tet rules offered besides DG-Parallel's (the solver's rule option
+# for workloads stated with other point counts): Keast's 11-point rule of
+# degree 4 (a negative centroid weight).
+TET_ALT_RULES = {
+    4: [("S4", -0.078933), ("S31", 0.071429, 0.045733), ("S22", 0.100596, 0.149333)],
 }
 # parameters that define a rule exactly and are kept fixed (the edge-midpoint
 # orbit of the 14-point tet rule sits at a = 0).
@@ -164,6 +173,7 @@ def residual(dim, orbits, params, mom):
 
 
 def solve(kind, order, orbits):
+    """kind: TRI, TET or TETALT (an alternative tet rule: no fixed parameters)."""
     dim = 2 if kind == "TRI" else 3
     params = []
     fixed = []
@@ -243,6 +253,15 @@ def main():
                 out.write("  {" + ", ".join(fmt(x) for x in bary[1:]) + ", " + fmt(w) + "},\n")
             out.write("};\n")
             index.append((kind, order, len(pts), name))
+    for order, orbits in sorted(TET_ALT_RULES.items()):
+        pts, err = solve("TETALT", order, orbits)
+        name = f"dgp_q_tet{order}_{len(pts)}"
+        out.write(f"// TET degree {order} (alternative): {len(pts)} points, max moment residual {err:.1e}\n")
+        out.write(f"static const double {name}[{len(pts)}][4] = {{\n")
+        for bary, w in pts:
+            out.write("  {" + ", ".join(fmt(x) for x in bary[1:]) + ", " + fmt(w) + "},\n")
+        out.write("};\n")
+        index.append(("TETALT", order, len(pts), name))
     out.write("\n")
     for n in range(1, 11):
         x, w = gauss_legendre(n)
@@ -258,6 +277,10 @@ def main():
     out.write("};\nstatic const dgp_q_rule dgp_q_tet_rules[] = {\n")
     for kind, order, n, name in index:
         if kind == "TET":
+            out.write(f"  {{3, {order}, {n}, &{name}[0][0]}},\n")
+    out.write("};\nstatic const dgp_q_rule dgp_q_tet_alt_rules[] = {\n")
+    for kind, order, n, name in index:
+        if kind == "TETALT":
             out.write(f"  {{3, {order}, {n}, &{name}[0][0]}},\n")
     out.write("};\nstatic const double* const dgp_q_gauss_legendre[11] = {0")
     for n in range(1, 11):

@@ -18,6 +18,7 @@ LAW_SCALAR, LAW_BURGERS2D, LAW_EULER2D, LAW_EULER3D, LAW_MAXWELL3D, LAW_MAXWELL2
 FLUX_UPWIND, FLUX_CENTRAL, FLUX_GODUNOV, FLUX_ROE, FLUX_LLF = range(5)
 FIELD_GAUSS, FIELD_VORTEX, FIELD_PULSE3D, FIELD_SINE, FIELD_GAUSS3D, FIELD_TM110, FIELD_TM2D = range(7)
 BC_DEFAULT, BC_FARFIELD, BC_WALL = range(3)
+RULE_REFERENCE, RULE_WORKLOAD = range(2)  # quadrature: DG-Parallel's, the workloads' P2 point counts
 FP64, MIXED = 0, 1
 LIMITER_NONE, LIMITER_MOMENT, LIMITER_BARTH = 0, 1, 2
 STEPPING_SSPRK3, STEPPING_LOCAL = 0, 5
@@ -63,6 +64,7 @@ def lib() -> ctypes.CDLL:
         "dgp_law_set_bc": ([P, I, I], I),
         "dgp_law_destroy": ([P], I),
         "dgp_solver_create": ([P, P, I, I, I, pP], I),
+        "dgp_solver_create_ex": ([P, P, I, I, I, I, pP], I),
         "dgp_solver_destroy": ([P], I),
         "dgp_solver_info": ([P, pI, pI, pI, pI], I),
         "dgp_project": ([P, D], I),
@@ -234,10 +236,11 @@ class Law:
 class Solver:
     """TimeIntegrator-style driver of one mesh + law on the current CUDA device."""
 
-    def __init__(self, mesh: Mesh, law: Law, order: int, precision: int = FP64, limiter: int = 0):
+    def __init__(self, mesh: Mesh, law: Law, order: int, precision: int = FP64, limiter: int = 0,
+                 rule: int = 0):
         self.mesh, self.law = mesh, law
         self.h = ctypes.c_void_p()
-        check(lib().dgp_solver_create(mesh.h, law.h, order, precision, limiter, ctypes.byref(self.h)))
+        check(lib().dgp_solver_create_ex(mesh.h, law.h, order, precision, limiter, rule, ctypes.byref(self.h)))
         m, n, e, f = (ctypes.c_int() for _ in range(4))
         check(lib().dgp_solver_info(self.h, ctypes.byref(m), ctypes.byref(n), ctypes.byref(e),
                                     ctypes.byref(f)))

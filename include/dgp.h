@@ -71,6 +71,8 @@ extern "C" {
 #define DGP_PRECISION_FP64 0  /* plain FP64 drop-in form */
 #define DGP_PRECISION_MIXED 1 /* FP32 bulk arithmetic, FP64 geometry/totals/time */
 
+#define DGP_RULE_REFERENCE 0
+#define DGP_RULE_WORKLOAD 1
 #define DGP_LIMITER_NONE 0
 #define DGP_LIMITER_MOMENT 1
 #define DGP_LIMITER_BARTH 2
@@ -125,6 +127,14 @@ int dgp_law_set_bc(dgp_law law, int boundary_id, int bc_kind);
 /* ---- solver: DGAnalysis setup (DGAnalysis.cc:133-302) + TimeIntegrator */
 int dgp_solver_create(dgp_mesh m, dgp_law law, int order, int precision, int limiter,
                       dgp_solver* out);
+/* quadrature rule: DGP_RULE_REFERENCE (DG-Parallel's: volume degree 2p, tet
+ * faces degree 2p + 1, edges p + 1 Gauss points) or DGP_RULE_WORKLOAD (at P2
+ * the point counts the workloads state: triangles the 7-point volume rule of
+ * degree 5, tets the 11-point volume and 6-point face rules of degree 4; built
+ * for ScalarLaw on triangles and tets and 3D Maxwell on tets, 128-thread tiles;
+ * DGP_ERR_UNSUPPORTED elsewhere).  dgp_solver_create uses the reference rule. */
+int dgp_solver_create_ex(dgp_mesh m, dgp_law law, int order, int precision, int limiter, int rule,
+                         dgp_solver* out);
 int dgp_solver_destroy(dgp_solver s);
 int dgp_solver_info(dgp_solver s, int* nfields, int* nmodes, int* ncells, int* nfaces);
 /* DGCell::L2ProjInitial (DGCell.cc:1458-1483) of the law's field at time t */

@@ -1088,6 +1088,14 @@ static const dgp_q_rule* simplex_rule(int dim, int degree) {
 
 or_solver* or_create(const char* msh_path, int law, int flux, int order, int field,
                      const double* params) {
+  return or_create_rule(msh_path, law, flux, order, field, params, 0);
+}
+
+/* rule 1: at P2 the workloads' quadrature point counts -- triangles the
+ * 7-point volume rule of degree 5, tets the 11-point volume rule and the
+ * 6-point face rule of degree 4; every other order as rule 0 (DG-Parallel's) */
+or_solver* or_create_rule(const char* msh_path, int law, int flux, int order, int field,
+                          const double* params, int rule) {
   or_solver* s = calloc(1, sizeof(or_solver));
   s->law = law;
   s->flux = flux;
@@ -1111,7 +1119,9 @@ or_solver* or_create(const char* msh_path, int law, int flux, int order, int fie
   if (s->Np > MAXNP) { or_destroy(s); return NULL; }
   build_basis(s);
   s->phi0 = s->G[0][0];
-  const dgp_q_rule* vr = simplex_rule(s->dim, 2 * order);
+  const int alt = rule == 1 && order == 2;
+  const dgp_q_rule* vr = !alt ? simplex_rule(s->dim, 2 * order)
+                              : s->dim == 2 ? simplex_rule(2, 5) : &dgp_q_tet_alt_rules[0];
   if (!vr) { or_destroy(s); return NULL; }
   s->nq = vr->npts;
   double refm = (s->dim == 2) ? 0.5 : 1.0 / 6.0;
@@ -1130,7 +1140,7 @@ or_solver* or_create(const char* msh_path, int law, int flux, int order, int fie
       s->fqw[q] = gl[2 * q + 1];
     }
   } else {
-    const dgp_q_rule* fr = simplex_rule(2, 2 * order + 1);
+    const dgp_q_rule* fr = simplex_rule(2, alt ? 4 : 2 * order + 1);
     s->nqf = fr->npts;
     for (int q = 0; q < s->nqf; ++q) {
       s->fqp[q][0] = fr->data[q * 3];

@@ -32,6 +32,10 @@ typedef struct or_solver or_solver;
 
 or_solver* or_create(const char* msh_path, int law, int flux, int order, int field,
                      const double* params);
+/* the same with a quadrature rule option: 0 DG-Parallel's, 1 the workloads'
+ * point counts at P2 (the solver's DGP_RULE_WORKLOAD) */
+or_solver* or_create_rule(const char* msh_path, int law, int flux, int order, int field,
+                          const double* params, int rule);
 void or_destroy(or_solver* s);
 int or_num_cells(const or_solver* s);
 int or_num_faces(const or_solver* s);

@@ -31,6 +31,8 @@ def lib():
     pI = ctypes.POINTER(ctypes.c_int)
     L.or_create.restype = P
     L.or_create.argtypes = [ctypes.c_char_p, I, I, I, I, pD]
+    L.or_create_rule.restype = P
+    L.or_create_rule.argtypes = [ctypes.c_char_p, I, I, I, I, pD, I]
     for f in ("or_num_cells", "or_num_faces", "or_num_fields", "or_num_modes"):
         getattr(L, f).argtypes = [P]
         getattr(L, f).restype = I
@@ -79,9 +81,9 @@ def _dp(a):
 
 
 class Oracle:
-    def __init__(self, msh: str, law: int, flux: int, order: int, field: int, params):
+    def __init__(self, msh: str, law: int, flux: int, order: int, field: int, params, rule: int = 0):
         p = np.ascontiguousarray(params, dtype=np.float64)
-        self.h = lib().or_create(msh.encode(), law, flux, order, field, _dp(p))
+        self.h = lib().or_create_rule(msh.encode(), law, flux, order, field, _dp(p), rule)
         if not self.h:
             raise RuntimeError(f"oracle could not load {msh}")
         L = lib()
