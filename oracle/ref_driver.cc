@@ -203,6 +203,7 @@ struct Params {
   std::string mesh, caseName = "gauss", flux = "exact", conn, rhs, state, log, barth, ckptOut, ckptIn, l2, stateBin;
   std::string p0rhs, p0cells;  // P0 fallback fixture: output file, perturbed cells
   std::string probeOut, probePts;  // point sensors: output file, "x,y,z;x,y,z;..."
+  std::string norms;  // the DGError.cc error norms at the final time
   double p0amp = 3.0;
   int order = 2, steps = 0, every = 1, threads = 1, bench = 0, warmup = 0, gpu = 0, lts = 0;
   std::string bins;
@@ -393,7 +394,7 @@ static void usage() {
   fprintf(stderr, "usage: ref_driver --mesh F.msh [--case gauss|vortex|pulse3d|sine|gauss3d] "
                   "[--flux exact|roe] [--order p] [--steps n | --tend T] [--cfl c] "
                   "[--conn F] [--rhs F] [--state F --every k] [--log F] [--barth F] [--l2 F] [--state-bin F] [--ckpt-in F] [--ckpt-out F] "
-                  "[--p0-rhs F --p0-cells e,e,... [--p0-amp a]] [--probe-out F --probe-pts x,y,z;...] "
+                  "[--p0-rhs F --p0-cells e,e,... [--p0-amp a]] [--probe-out F --probe-pts x,y,z;...] [--norms F] "
                   "[--threads k --bench n]\n");
   exit(1);
 }
@@ -425,6 +426,7 @@ int main(int argc, char** argv) {
     else if (a == "--p0-cells") P.p0cells = v;
     else if (a == "--p0-amp") P.p0amp = atof(v);
     else if (a == "--probe-out") P.probeOut = v;
+    else if (a == "--norms") P.norms = v;
     else if (a == "--probe-pts") P.probePts = v;
     else if (a == "--ckpt-out") P.ckptOut = v;
     else if (a == "--ckpt-in") P.ckptIn = v;
@@ -775,6 +777,33 @@ int main(int argc, char** argv) {
         for (int j = 0; j < Np; ++j) row[i * Np + j] = byFile[e]->theFieldsCoefficients->get(i, j);
       fwrite(row.data(), sizeof(double), row.size(), f);
     }
+    fclose(f);
+  }
+  if (!P.norms.empty()) {
+    // DGAnalysis::ExactError, LinfError, PressureError, entropyErrorL1,
+    // pressureErrorL2, densityErrorL2, entropyErrorL2 (DGPref.cc:249-381) at
+    // the final time, summed over the cells as there (one thread); the
+    // pressure and entropy norms for the 2D Euler case only
+    double l1 = 0.0, linf = 0.0, pl1 = 0.0, el1 = 0.0, pl2 = 0.0, dl2 = 0.0, el2 = 0.0;
+    const bool euler = P.caseName == "vortex";
+    for (mMesh::iter it = mesh->begin(dim); it != mesh->end(dim); ++it) {
+      DGCell* cell = (DGCell*)(*it)->getCell();
+      l1 += cell->L1exact(TACT);
+      const double li = cell->LinfError(TACT);
+      if (linf < li) linf = li;
+      dl2 += cell->densityErrorL2(TACT);
+      if (euler) {
+        pl1 += cell->L1exactPressure(TACT);
+        el1 += cell->entropyErrorL1_2D(TACT);
+        pl2 += cell->pressureErrorL2(TACT);
+        el2 += cell->entropyErrorL2_2D(TACT);
+      }
+    }
+    FILE* f = fopen(P.norms.c_str(), "w");
+    fprintf(f, "t %.17g\nExactError %.17g\nLinfError %.17g\ndensityErrorL2 %.17g\n", TACT, l1, linf, sqrt(dl2));
+    if (euler)
+      fprintf(f, "PressureError %.17g\nentropyErrorL1 %.17g\npressureErrorL2 %.17g\nentropyErrorL2 %.17g\n", pl1,
+              el1, sqrt(pl2), sqrt(el2));
     fclose(f);
   }
   if (!P.probeOut.empty()) {

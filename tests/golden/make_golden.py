@@ -192,6 +192,31 @@ def run_probe_case(name, kind, margs, dargs, steps, npts):
     np.savez_compressed(os.path.join(HERE, name + ".npz"), points=pts, cell=cell, values=vals, state=st,
                         args=np.array(dargs), steps=steps)
 
+# The DGError.cc error norms summed as DGAnalysis does (DGPref.cc:249-381)
+# after a few steps (ref_driver --norms): ``t``, ``state`` and one entry per
+# norm (ExactError, LinfError, densityErrorL2; for the vortex also
+# PressureError, entropyErrorL1, pressureErrorL2, entropyErrorL2).
+NORM_CASES = {
+    "norms_euler_roe_p3": ("tri", dict(nx=8, ny=8, x0=0.0, x1=10.0, y0=0.0, y1=10.0, seed=2),
+                           ["--case", "vortex", "--flux", "roe", "--order", "3"], 5),
+    "norms_scalar_p2": ("tri", SQUARE, ["--case", "gauss", "--order", "2"], 5),
+}
+
+
+def run_norm_case(name, kind, margs, dargs, steps):
+    mesh = build_mesh(kind, margs)
+    msh = os.path.join(HERE, name + ".msh")
+    meshgen.write_msh_v1(mesh, msh)
+    with tempfile.TemporaryDirectory() as td:
+        state, nf = os.path.join(td, "s"), os.path.join(td, "n")
+        cmd = [DRIVER, "--mesh", msh, "--steps", str(steps), "--cfl", "0.1", "--state", state,
+               "--every", str(steps), "--norms", nf] + dargs
+        subprocess.run(cmd, check=True, capture_output=True)
+        blocks = open(state).read().split("step ")[1:]
+        st = np.array([list(map(float, ln.split())) for ln in blocks[-1].split("\n")[1:] if ln.strip()])
+        vals = {ln.split()[0]: float(ln.split()[1]) for ln in open(nf) if ln.strip()}
+    np.savez_compressed(os.path.join(HERE, name + ".npz"), state=st, args=np.array(dargs), steps=steps, **vals)
+
 
 def run_size_case(name, kind, margs, dargs, steps):
     mesh = build_mesh(kind, margs)
@@ -369,6 +394,11 @@ def main():
         if only and name not in only:
             continue
         run_l2_case(name, kind, margs, dargs, steps)
+        print("wrote", name)
+    for name, (kind, margs, dargs, steps) in NORM_CASES.items():
+        if only and name not in only:
+            continue
+        run_norm_case(name, kind, margs, dargs, steps)
         print("wrote", name)
     for name, (kind, margs, dargs, steps, npts) in PROBE_CASES.items():
         if only and name not in only:

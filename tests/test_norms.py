@@ -1,16 +1,17 @@
 """Error norms of DGError.cc (field, pressure and entropy errors; L1, L2, Linf;
 the volume rule of degree 2p or the rule of degree 2(p+1)).
 
-CPU: the oracle's restatement against its own L2 density error and against
-hand-made states with known errors.  GPU: the CUDA reduction against the oracle
-on the same state.
+CPU: the oracle's restatement against its own L2 density error, against
+hand-made states with known errors, and against the norms DG-Parallel itself
+computes (fixtures).  GPU: the CUDA reduction against the oracle on the same
+state and against the same fixtures.
 """
 import numpy as np
 import pytest
 
 import dgp
 from dgp import meshgen
-from cases import VORTEX, SCALAR2D
+from cases import VORTEX, SCALAR2D, golden
 from oracle_bind import Oracle
 
 
@@ -84,3 +85,54 @@ def test_gpu_norms_match_oracle(tmp_path, order):
     assert abs(s.error_norms(t, 0, 1)[1] - s.l2_error(t, 0)) <= 1e-13 * s.l2_error(t, 0)
     s.close()
     o.close()
+
+
+# DGAnalysis's norms (DGPref.cc:249-381) as the reference computes them on its
+# own state after five steps (tests/golden/norms_*.npz, ref_driver --norms):
+# name -> (quantity, rule, index into (L1, L2, Linf))
+REFERENCE_NORMS = {
+    "ExactError": (0, 0, 0),
+    "LinfError": (0, 0, 2),
+    "densityErrorL2": (0, 1, 1),
+    "PressureError": (-1, 0, 0),
+    "entropyErrorL1": (-2, 0, 0),
+    "pressureErrorL2": (-1, 1, 1),
+    "entropyErrorL2": (-2, 1, 1),
+}
+NORM_CASES = [
+    ("norms_euler_roe_p3", dgp.LAW_EULER2D, dgp.FLUX_ROE, dgp.FIELD_VORTEX, VORTEX, 3),
+    ("norms_scalar_p2", dgp.LAW_SCALAR, dgp.FLUX_UPWIND, dgp.FIELD_GAUSS, SCALAR2D, 2),
+]
+# the reference's basis tables (decimal, ~1e-11 at P3) set the floor
+NORM_TOL = 1e-10
+
+
+def _reference_norms(g):
+    return {k: float(g[k]) for k in REFERENCE_NORMS if k in g.files}
+
+
+@pytest.mark.parametrize("name,law,flux,field,prm,order", NORM_CASES)
+def test_oracle_norms_match_reference(name, law, flux, field, prm, order):
+    msh, g = golden(name)
+    o = Oracle(msh, law, flux, order, field, prm)
+    o.set_state(g["state"].reshape(o.shape))
+    t = float(g["t"])
+    for k, ref in _reference_norms(g).items():
+        q, rule, i = REFERENCE_NORMS[k]
+        got = o.error_norms(t, q, rule)[i]
+        assert abs(got - ref) <= NORM_TOL * ref, (k, got, ref)
+    o.close()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name,law,flux,field,prm,order", NORM_CASES)
+def test_gpu_norms_match_reference(name, law, flux, field, prm, order):
+    msh, g = golden(name)
+    s = dgp.Solver(dgp.Mesh.from_msh(msh), dgp.Law(law, flux, field, prm), order, dgp.FP64)
+    s.set_state(g["state"].reshape(s.shape))
+    t = float(g["t"])
+    for k, ref in _reference_norms(g).items():
+        q, rule, i = REFERENCE_NORMS[k]
+        got = s.error_norms(t, q, rule)[i]
+        assert abs(got - ref) <= NORM_TOL * ref, (k, got, ref)
+    s.close()
