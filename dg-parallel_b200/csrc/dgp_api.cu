@@ -1944,6 +1944,28 @@ static int adj_buffer(dgp_solver s, double** p, size_t* have, size_t states) {
   return DGP_OK;
 }
 
+// the Barth slope factors of `stages` stages ([stage][E][M] doubles)
+static int adj_slopes(dgp_solver s, size_t stages) {
+  AdjointState& a = s->adj;
+  const size_t n = stages * static_cast<size_t>(s->b.E) * s->b.M;
+  if (a.slopes && a.slopes_n >= n) return DGP_OK;
+  if (a.slopes) {
+    cudaFree(a.slopes);
+    s->allocs.erase(std::remove(s->allocs.begin(), s->allocs.end(), static_cast<void*>(a.slopes)), s->allocs.end());
+    a.slopes = nullptr;
+  }
+  if (int rc = s->alloc(&a.slopes, n)) return rc;
+  a.slopes_n = n;
+  return DGP_OK;
+}
+
+int dgp_adjoint_freeze_limiter(dgp_solver s, int on) {
+  if (!s) return fail(DGP_ERR_INVALID, "null solver");
+  if (on && s->limiter != DGP_LIMITER_BARTH) return fail(DGP_ERR_UNSUPPORTED, "no Barth limiter to freeze");
+  s->adj.freeze = on != 0;
+  return DGP_OK;
+}
+
 int dgp_adjoint_set_receivers(dgp_solver s, int n, const double* points, const double* observed) {
   if (!s || n <= 0 || !points || !observed) return fail(DGP_ERR_INVALID, "bad argument");
   if (s->b.ninst) return fail(DGP_ERR_UNSUPPORTED, "receivers are set on a single solver");
@@ -1990,26 +2012,54 @@ int dgp_receiver_values(dgp_solver s, double* rho, double* J) {
 }
 
 // one SSP-RK3 step from X back into X, keeping u_n, u1, u2 in S (three
-// consecutive states)
-static void step_keeping_stages(dgp_solver s, double* X, double* S, size_t ns) {
+// consecutive states).  With the Barth limiter it follows every stage, its
+// slope factors going to slopes[3][E][M] (replay: applied from there).
+static void step_keeping_stages(dgp_solver s, double* X, double* S, size_t ns, double* slopes = nullptr,
+                                bool replay = false) {
+  const bool lim = s->limiter == DGP_LIMITER_BARTH && s->ops.limit;
+  const size_t em = static_cast<size_t>(s->b.E) * s->b.M;
+  auto limit = [&](double* u, int k) {
+    if (!lim) return;
+    DeviceBuffers bl = s->b;
+    bl.C = u;
+    bl.lim_slope = slopes ? slopes + static_cast<size_t>(k) * em : nullptr;
+    bl.lim_replay = replay ? 1 : 0;
+    s->ops.limit(bl, 0, s->stream);
+  };
   if (s->fused) {
     s->ops.fused(s->b, X, X, S + ns, S, 1, 0.0, 0, s->stream);
+    limit(S + ns, 0);
     s->ops.fused(s->b, S + ns, S, S + 2 * ns, nullptr, 2, 1.0, 0, s->stream);
+    limit(S + 2 * ns, 1);
     s->ops.fused(s->b, S + 2 * ns, S, X, nullptr, 3, 0.5, 0, s->stream);
+    limit(X, 2);
     s->tr_stale = true;
     return;
   }
+  // the separate kernels read the face-point traces of each stage's input
+  auto traces = [&](double* u) {
+    if (!replay) return;  // the limiter pass refreshed the traces of the cells it changed
+    DeviceBuffers bt = s->b;
+    bt.C = u;
+    s->ops.trace(bt, nullptr, s->stream);
+  };
   DeviceBuffers b = s->b;
   b.U0 = S;
   b.C = X;
   b.Cout = S + ns;
   s->ops.stage(b, 1, 0.0, 0, s->stream);
+  limit(S + ns, 0);
+  if (lim) traces(S + ns);
   b.C = S + ns;
   b.Cout = S + 2 * ns;
   s->ops.stage(b, 2, 1.0, 0, s->stream);
+  limit(S + 2 * ns, 1);
+  if (lim) traces(S + 2 * ns);
   b.C = S + 2 * ns;
   b.Cout = X;
   s->ops.stage(b, 3, 0.5, 0, s->stream);
+  limit(X, 2);
+  if (lim) traces(X);
 }
 
 int dgp_forward_checkpointed(dgp_solver s, double t0, double dt, int nsteps, int every, double* J) {
@@ -2017,7 +2067,8 @@ int dgp_forward_checkpointed(dgp_solver s, double t0, double dt, int nsteps, int
   if (!s || !(dt > 0) || nsteps <= 0 || every < 0) return fail(DGP_ERR_INVALID, "bad argument");
   if (s->b.ninst) return fail(DGP_ERR_UNSUPPORTED, "the adjoint runs on a single solver");
   if (!s->ops.adj_stage) return fail(DGP_ERR_UNSUPPORTED, "no discrete adjoint for this law/flux");
-  if (s->limiter != DGP_LIMITER_NONE) return fail(DGP_ERR_UNSUPPORTED, "adjoint with the limiter on");
+  if (s->limiter == DGP_LIMITER_MOMENT)
+    return fail(DGP_ERR_UNSUPPORTED, "the adjoint's frozen limiter is built for the Barth limiter");
   for (const HostMesh& hm : s->meshes)
     for (int pf : hm.pface)
       if (pf >= 0) return fail(DGP_ERR_UNSUPPORTED, "adjoint on a mesh with periodic edges");
@@ -2025,11 +2076,16 @@ int dgp_forward_checkpointed(dgp_solver s, double t0, double dt, int nsteps, int
   AdjointState& a = s->adj;
   // every == 0: one segment whose stage states are all kept (no recompute)
   const bool record = every == 0;
+  const bool lim = s->limiter == DGP_LIMITER_BARTH;
+  if (a.freeze && !(record && lim && a.slopes && a.slopes_n >= static_cast<size_t>(3) * nsteps * s->b.E * s->b.M))
+    return fail(DGP_ERR_INVALID, "a frozen limiter replays the factors of a recorded pass (every = 0) of as many steps");
   if (record) every = nsteps;
   const int nseg = (nsteps + every - 1) / every;
   if (int rc = adj_buffer(s, &a.ckpt, &a.ckpt_states, static_cast<size_t>(nseg) + 1)) return rc;
   if (record)
     if (int rc = adj_buffer(s, &a.store, &a.store_states, static_cast<size_t>(3) * nsteps)) return rc;
+  if (record && lim && !a.freeze)
+    if (int rc = adj_slopes(s, static_cast<size_t>(3) * nsteps)) return rc;
   a.recorded = record;
   if (!a.t_seg && (s->alloc(&a.t_seg, 1) != DGP_OK)) return DGP_ERR_NOMEM;
   a.nsteps = nsteps;
@@ -2038,6 +2094,7 @@ int dgp_forward_checkpointed(dgp_solver s, double t0, double dt, int nsteps, int
   a.t0 = t0;
   a.dt = dt;
   const size_t ns = s->state_count(), bytes = ns * 8;
+  const size_t em = static_cast<size_t>(s->b.E) * s->b.M;
   const int p0 = s->b.p0;
   s->b.p0 = 0;  // the adjoint differentiates the plain operator
   for (int seg = 0; seg < nseg; ++seg) {
@@ -2049,7 +2106,8 @@ int dgp_forward_checkpointed(dgp_solver s, double t0, double dt, int nsteps, int
       const double tk = t0 + static_cast<double>(seg * every + k) * dt;
       set_segment_time<<<1, 1, 0, s->stream>>>(s->b.ctl, tk, dt, a.t_seg);
       if (record)
-        step_keeping_stages(s, X, a.store + static_cast<size_t>(k) * 3 * ns, ns);
+        step_keeping_stages(s, X, a.store + static_cast<size_t>(k) * 3 * ns, ns,
+                            lim ? a.slopes + static_cast<size_t>(k) * 3 * em : nullptr, a.freeze);
       else
         launch_step(s, 0);
     }
@@ -2073,6 +2131,22 @@ int dgp_backward(dgp_solver s, const double* dJ_duT, double* dJ_du0) {
   DGP_CUDA(cudaSetDevice(s->device));
   const size_t ns = s->state_count(), bytes = ns * 8;
   if (int rc = adj_buffer(s, &a.store, &a.store_states, static_cast<size_t>(3) * a.every)) return rc;
+  const bool lim = s->limiter == DGP_LIMITER_BARTH;
+  const size_t em = static_cast<size_t>(s->b.E) * s->b.M;
+  if (lim && !a.recorded)
+    if (int rc = adj_slopes(s, static_cast<size_t>(3) * a.every)) return rc;
+  // the frozen limiter of stage k of step j: its recorded linear map (diagonal
+  // in the modes) applied to the cotangent of the stage's limited output
+  auto frozen = [&](double* mu, int j, int k) {
+    if (!lim) return;
+    DeviceBuffers bl = s->b;
+    bl.C = mu;
+    bl.tr = nullptr;
+    bl.trig = nullptr;
+    bl.lim_slope = a.slopes + (static_cast<size_t>(j) * 3 + k) * em;
+    bl.lim_replay = 1;
+    s->ops.limit(bl, 0, s->stream);
+  };
   if (!a.lam) {
     size_t one = 0;
     if (int rc = adj_buffer(s, &a.lam, &one, 1)) return rc;
@@ -2105,7 +2179,8 @@ int dgp_backward(dgp_solver s, const double* dJ_duT, double* dJ_du0) {
       s->ops.trace(s->b, nullptr, s->stream);
       for (int j = 0; j < len; ++j) {
         set_segment_time<<<1, 1, 0, s->stream>>>(s->b.ctl, step_time(j), a.dt, a.t_seg);
-        step_keeping_stages(s, X, a.store + static_cast<size_t>(j) * 3 * ns, ns);
+        step_keeping_stages(s, X, a.store + static_cast<size_t>(j) * 3 * ns, ns,
+                            lim ? a.slopes + static_cast<size_t>(j) * 3 * em : nullptr);
       }
     }
     // reversed steps
@@ -2117,6 +2192,7 @@ int dgp_backward(dgp_solver s, const double* dJ_duT, double* dJ_du0) {
       g.t_seg = a.t_seg;
       // u3 = (2 (u2 + dt L(u2)) + u) / 3
       b.C = a.store + (static_cast<size_t>(j) * 3 + 2) * ns;
+      frozen(a.lam, j, 2);
       g.mu = a.lam;
       g.out = a.lam2;
       g.acc = a.acc;
@@ -2129,6 +2205,7 @@ int dgp_backward(dgp_solver s, const double* dJ_duT, double* dJ_du0) {
       s->ops.adj_stage(b, g, s->stream);
       // u2 = (u1 + dt L(u1) + 3 u) / 4
       b.C = a.store + (static_cast<size_t>(j) * 3 + 1) * ns;
+      frozen(a.lam2, j, 1);
       g.mu = a.lam2;
       g.out = a.lam1;
       g.ca = 0.25;
@@ -2140,6 +2217,7 @@ int dgp_backward(dgp_solver s, const double* dJ_duT, double* dJ_du0) {
       s->ops.adj_stage(b, g, s->stream);
       // u1 = u + dt L(u)
       b.C = a.store + (static_cast<size_t>(j) * 3 + 0) * ns;
+      frozen(a.lam1, j, 0);
       g.mu = a.lam1;
       g.out = a.lam;
       g.ca = 1.0;

@@ -66,6 +66,11 @@ struct AdjointState {
   double* lam1 = nullptr;
   double* acc = nullptr;
   double* t_seg = nullptr;  // device scalar
+  // Barth limiter: its slope factors per (step, stage, cell, field) of the
+  // steps whose stage states are kept (the frozen active set)
+  double* slopes = nullptr;
+  size_t slopes_n = 0;
+  bool freeze = false;      // forward passes replay the recorded factors
   bool ready = false;       // a forward pass is recorded
   bool recorded = false;    // every stage state of the forward pass is kept (no recompute)
   // receivers: J = sum_r (rho(x_r) - obs_r)^2

@@ -389,6 +389,11 @@ struct BarthArgs {
   const TimeCtl* gctl;
   const int* cell_inst;
   int E;
+  // the pass's slope factors per (cell, field): written when not null, or,
+  // with replay, applied as recorded (the limiter frozen to a fixed linear
+  // map, as the discrete adjoint linearises it); trig, tr may then be null
+  double* slope;
+  int replay;
 };
 
 template <class K>
@@ -402,6 +407,20 @@ __global__ void __launch_bounds__(128) barth_kernel(BarthArgs a) {
   if (a.cell_inst) {
     const int i = a.cell_inst[e];
     if (i < 0 || (a.ctl && a.ctl[i].done)) return;
+  }
+  if (a.replay) {
+    // the recorded factors: degree 1 scaled, degrees >= 2 dropped below 0.9
+    double* c = a.C + (size_t)e * M * NP;
+#pragma unroll
+    for (int j = 0; j < M; ++j) {
+      const double sl = a.slope[(size_t)e * M + j];
+      if (!(sl < 1.0)) continue;
+      if (sl < 0.9)
+        for (int k = S1; k < NP; ++k) c[j * NP + k] = 0.0;
+#pragma unroll
+      for (int k = 1; k < S1; ++k) c[j * NP + k] = __dmul_rn(c[j * NP + k], sl);
+    }
+    return;
   }
   int fc[NLF];
 #pragma unroll
@@ -457,6 +476,9 @@ __global__ void __launch_bounds__(128) barth_kernel(BarthArgs a) {
         }
       }
     }
+    if (a.slope)
+#pragma unroll
+      for (int j = 0; j < M; ++j) a.slope[(size_t)e * M + j] = slope[j];
 #pragma unroll
     for (int j = 0; j < M; ++j) {
       if (!(slope[j] < 1.0)) continue;
@@ -483,6 +505,10 @@ __global__ void __launch_bounds__(128) barth_kernel(BarthArgs a) {
         }
       }
     }
+  }
+  else if (a.slope) {
+#pragma unroll
+    for (int j = 0; j < M; ++j) a.slope[(size_t)e * M + j] = 1.0;
   }
 #pragma unroll
   for (int j = 0; j < M; ++j) a.trig[(size_t)e * M + j] = trig;

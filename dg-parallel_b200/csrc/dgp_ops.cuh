@@ -204,6 +204,8 @@ void ops_limit(const DeviceBuffers& b, int check_done, cudaStream_t st) {
       a.gctl = b.gctl;
       a.cell_inst = b.cell_inst;
       a.E = b.E;
+      a.slope = b.lim_slope;
+      a.replay = b.lim_replay;
       barth_kernel<K><<<(b.E + 127) / 128, 128, 0, st>>>(a);
       return;
     }

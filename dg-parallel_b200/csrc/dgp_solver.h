@@ -76,6 +76,8 @@ struct DeviceBuffers {
   int* cface = nullptr;           // Barth: [E][NLF] face of each local face
   double* bphif = nullptr;        // Barth: FP64 face-point basis values [NLF * NQF][NP]
   unsigned char* trig = nullptr;  // [E * M] trigger degree of each row in the last limiter pass
+  double* lim_slope = nullptr;    // Barth: [E][M] slope factors of the pass (written; read when replayed)
+  int lim_replay = 0;             // Barth: 1 applies lim_slope instead of computing the factors
   unsigned char* lbig = nullptr;  // [E * M] degrees with a mode above the limiter's threshold
   double* lmo = nullptr;          // [E * M][NP] moments of every degree of each row
   int* nb = nullptr;              // [E][4] left, right, bottom, top

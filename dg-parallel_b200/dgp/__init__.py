@@ -116,6 +116,7 @@ def lib() -> ctypes.CDLL:
         "dgp_adjoint_set_receivers": ([P, I, pD, pD], I),
         "dgp_receiver_values": ([P, pD, pD], I),
         "dgp_forward_checkpointed": ([P, D, D, I, I, pD], I),
+        "dgp_adjoint_freeze_limiter": ([P, I], I),
         "dgp_backward": ([P, pD, pD], I),
         "dgp_solver_block": ([P, pI, pI], I),
         "dgp_solver_fused": ([P, pI], I),
@@ -424,6 +425,11 @@ class Solver:
         J = ctypes.c_double()
         check(lib().dgp_receiver_values(self.h, _dp(rho), ctypes.byref(J)))
         return rho, J.value
+
+    def adjoint_freeze_limiter(self, on: bool = True):
+        """Later recorded forward passes replay the Barth slope factors of the
+        last one (the frozen map the backward pass linearises)."""
+        check(lib().dgp_adjoint_freeze_limiter(self.h, 1 if on else 0))
 
     def forward_checkpointed(self, t0: float, dt: float, nsteps: int, every: int) -> float:
         J = ctypes.c_double()

@@ -349,7 +349,11 @@ int dgp_ensemble_launches_per_step(dgp_ensemble e, int* n);
  * recompute.  The backward pass runs the transposed linearised operator
  * (transposed volume contraction and lift, Jacobians of the numerical and
  * boundary fluxes, reversed stage combination) on the device.  Built for the
- * closed-form fluxes (not the exact Riemann solver), without the limiter.
+ * closed-form fluxes (not the exact Riemann solver).  With the Barth limiter
+ * the limiter is linearised with its active set frozen: the forward pass
+ * records each pass's slope factors per (cell, field), and the backward pass
+ * applies that fixed linear map (degree 1 scaled, degrees >= 2 dropped below
+ * 0.9) to the cotangents; the moment limiter is refused.
  * Receivers define J = sum_r (u_0(x_r, T) - observed_r)^2 on field 0 (the
  * density of the Euler laws); points are dim doubles each. */
 int dgp_adjoint_set_receivers(dgp_solver s, int n, const double* points, const double* observed);
@@ -360,6 +364,11 @@ int dgp_receiver_values(dgp_solver s, double* rho, double* J);
  * segment; every == 0: keep all 3 * nsteps stage states in device memory, the
  * backward pass recomputes nothing (DGP_ERR_NOMEM when they do not fit). */
 int dgp_forward_checkpointed(dgp_solver s, double t0, double dt, int nsteps, int every, double* J);
+/* on = 1: later forward passes (every == 0, the same nsteps) apply the Barth
+ * slope factors recorded by the last such pass instead of computing them, i.e.
+ * run the frozen map whose transpose the backward pass applies (a check of the
+ * gradient by finite differences); on = 0 computes them again */
+int dgp_adjoint_freeze_limiter(dgp_solver s, int on);
 /* dJ/du0 (host, file order [cell][field][mode]) of the last forward pass; the
  * seed dJ/du_T is dJ_duT when not NULL, else the receiver objective's */
 int dgp_backward(dgp_solver s, const double* dJ_duT, double* dJ_du0);

@@ -206,3 +206,72 @@ def test_adjoint_matches_cpu_fp64_directional_derivative(tmp_path):
         fd = (J_cpu(u0 + eps * d) - J_cpu(u0 - eps * d)) / (2 * eps)
         ad = float(np.sum(g * d))
         assert abs(fd - ad) <= 1e-6 * max(abs(fd), abs(ad)), (fd, ad)
+
+
+def _barth_solver(tmp_path, order=2, beta=5.0):
+    """The vortex on a coarse mesh, Barth limiter after every stage (the
+    vortex core spans a few cells, so the limiter acts)."""
+    msh = _mesh(tmp_path, 10, (0.0, 10.0), 2)
+    prm = VORTEX.copy()
+    prm[8] = beta
+    s = dgp.Solver(dgp.Mesh.from_msh(msh), dgp.Law(dgp.LAW_EULER2D, dgp.FLUX_ROE, dgp.FIELD_VORTEX, prm), order,
+                   dgp.FP64, dgp.LIMITER_BARTH)
+    s.project(0.0)
+    return s
+
+
+def test_adjoint_frozen_barth_limiter_matches_fd_of_the_frozen_map(tmp_path):
+    """With the Barth limiter the adjoint linearises the limiter with its
+    active set frozen (the recorded slope factors as a fixed linear map).  Its
+    gradient equals central differences of exactly that map: forward passes
+    that replay the recorded factors (dgp_adjoint_freeze_limiter)."""
+    nsteps = 12
+    so = _barth_solver(tmp_path, beta=5.5)
+    pts = _receivers(np.random.default_rng(4), 48, 1.0, 9.0)
+    dt = 0.5 * so.cfl_dt(0.1)
+    so.set_receivers(pts, np.zeros(len(pts)))
+    so.forward_checkpointed(0.0, dt, nsteps, 0)
+    obs, _ = so.receiver_values()
+    s = _barth_solver(tmp_path)
+    s.set_receivers(pts, obs)
+    u0 = s.get_state()
+    J0 = s.forward_checkpointed(0.0, dt, nsteps, 0)
+    assert s.limiter_triggers().any()  # the limiter acted in the last pass
+    g = s.backward()
+    assert J0 > 0 and np.isfinite(g).all()
+    # the same gradient when the backward pass recomputes segments
+    s.set_state(u0)
+    assert s.forward_checkpointed(0.0, dt, nsteps, 4) == J0
+    assert np.array_equal(s.backward(), g)
+    # central differences of the frozen map
+    s.set_state(u0)
+    s.forward_checkpointed(0.0, dt, nsteps, 0)  # records the factors again
+    s.adjoint_freeze_limiter(True)
+    with pytest.raises(dgp.DGPError):
+        s.forward_checkpointed(0.0, dt, nsteps, 4)  # replay needs a recorded pass
+    rng = np.random.default_rng(5)
+    eps = 1e-6
+    for _ in range(4):
+        d = rng.standard_normal(u0.shape)
+        s.set_state(u0 + eps * d)
+        jp = s.forward_checkpointed(0.0, dt, nsteps, 0)
+        s.set_state(u0 - eps * d)
+        jm = s.forward_checkpointed(0.0, dt, nsteps, 0)
+        fd = (jp - jm) / (2 * eps)
+        ad = float(np.sum(g * d))
+        assert abs(fd - ad) <= 1e-6 * max(abs(fd), abs(ad)), (fd, ad)
+    s.adjoint_freeze_limiter(False)
+    # frozen and unfrozen forward passes agree at the recorded state itself
+    s.set_state(u0)
+    assert s.forward_checkpointed(0.0, dt, nsteps, 0) == J0
+
+
+def test_adjoint_moment_limiter_refused(tmp_path):
+    msh = _mesh(tmp_path, 6, (0.0, 1.0), 1)
+    s = dgp.Solver(dgp.Mesh.from_msh(msh), dgp.Law(dgp.LAW_BURGERS2D, dgp.FLUX_LLF, dgp.FIELD_SINE,
+                                                   params(amplitude=0.25)), 2, dgp.FP64, dgp.LIMITER_MOMENT)
+    with pytest.raises(dgp.DGPError) as ei:
+        s.forward_checkpointed(0.0, 1e-3, 2, 1)
+    assert ei.value.code == -3
+    with pytest.raises(dgp.DGPError):
+        s.adjoint_freeze_limiter(True)
