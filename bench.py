@@ -633,6 +633,8 @@ def configs_bench(steps=200):
       s = 0.01) on the unit square cut into 32x32x2 = 2048 jittered triangles
       (seed 1), P2, upwind, exact-solution inflow, CFL 0.1, 200 steps; also
       DG-Parallel's pthreads path on all host cores and on one.
+    llf: the vortex workload (131072 triangles, P3) with the local
+      Lax-Friedrichs flux, to t = 2 for the density error.
     maxwell: 3D Maxwell (eps = mu = 1), upwind flux, PEC walls, TM110 cavity
       mode on the unit cube cut into 48^3 x 6 = 663552 jittered tets (seed 3),
       P2, CFL 0.1; `steps` timed steps, then one full period (T = sqrt 2) for
@@ -734,6 +736,12 @@ def configs_bench(steps=200):
     # the workload's stated quadrature: 11-point volume, 6-point face rules
     out["maxwell3d_p2_663552tet_11pt"] = measure(mesh3, law3, 2, 6, 10, 4 * 6, 3, 2, t_full=np.sqrt(2.0),
                                                  rule=dgp.RULE_WORKLOAD)
+    # the vortex workload with the local Lax-Friedrichs flux (to t = 2 for the
+    # density error)
+    m2 = make_mesh()
+    mesh2 = dgp.Mesh.from_arrays(2, m2.vertices, m2.cells, 100, m2.bfaces, m2.btags)
+    law2 = dgp.Law(dgp.LAW_EULER2D, dgp.FLUX_LLF, dgp.FIELD_VORTEX, vortex_params())
+    out["euler2d_p3_vortex256_llf"] = measure(mesh2, law2, 3, 4, 10, 3 * 4, 2, 0, t_full=2.0)
     return out
 
 
