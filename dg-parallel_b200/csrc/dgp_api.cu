@@ -1026,12 +1026,25 @@ int dgp_checkpoint_read(dgp_solver s, const char* path, double* t, int* iter) {
   return DGP_OK;
 }
 
+// the face-point traces after the state was set from outside the stages:
+// the separate face kernel reads them at once; the fused stage kernel keeps
+// none, so they are only marked stale (refreshed by whatever reads them next:
+// local time stepping, a switch to the separate form)
+static void traces_after_state_change(dgp_solver s) {
+  if (s->fused && !s->lts.on) {
+    s->tr_stale = true;
+    return;
+  }
+  s->ops.trace(s->b, nullptr, s->stream);
+  s->tr_stale = false;
+}
+
 int dgp_set_state(dgp_solver s, const double* host_state) {
   if (!s || !host_state) return fail(DGP_ERR_INVALID, "null argument");
   DGP_CUDA(cudaSetDevice(s->device));
   DGP_CUDA(cudaStreamSynchronize(s->stream));
   if (int rc = host_to_state(s, host_state, s->b.C)) return rc;
-  s->ops.trace(s->b, nullptr, s->stream);
+  traces_after_state_change(s);
   DGP_CUDA(cudaGetLastError());
   DGP_CUDA(cudaStreamSynchronize(s->stream));
   return DGP_OK;
@@ -1052,7 +1065,7 @@ int dgp_set_state_device(dgp_solver s, const double* dev_state) {
   const int grid = static_cast<int>((n + 255) / 256);
   gather_cells<double, double><<<grid, 256, 0, s->stream>>>(dev_state, static_cast<double*>(s->b.C),
                                                             s->d_i2f, s->b.E, mnp);
-  s->ops.trace(s->b, nullptr, s->stream);
+  traces_after_state_change(s);
   DGP_CUDA(cudaGetLastError());
   DGP_CUDA(cudaStreamSynchronize(s->stream));
   return DGP_OK;
