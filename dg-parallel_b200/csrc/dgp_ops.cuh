@@ -11,11 +11,13 @@
 
 namespace dgp {
 
-// the discrete adjoint covers the laws whose numerical fluxes are closed-form
-// (the exact Riemann solver's Newton iteration is not differentiated)
+// the discrete adjoint covers every law and flux (the exact Riemann solver is
+// differentiated through its Newton iteration:
+// dual numbers carry the derivative of every iterate, which converges with
+// the iterate to the derivative of the solution)
 template <class K>
 constexpr bool adjoint_built() {
-  return K::FLUX != DGP_FLUX_GODUNOV;
+  return true;
 }
 
 constexpr size_t kSmemPerCta = 227 * 1024;

@@ -348,8 +348,9 @@ int dgp_ensemble_launches_per_step(dgp_ensemble e, int* n);
  * SSP-RK3 steps of fixed size dt, by checkpoint (every `every` steps) and
  * recompute.  The backward pass runs the transposed linearised operator
  * (transposed volume contraction and lift, Jacobians of the numerical and
- * boundary fluxes, reversed stage combination) on the device.  Built for the
- * closed-form fluxes (not the exact Riemann solver).  With the Barth limiter
+ * boundary fluxes, reversed stage combination) on the device.  Built for every
+ * flux (the exact Riemann solver differentiated through its Newton
+ * iteration); meshes with periodic edges are refused.  With the Barth limiter
  * the limiter is linearised with its active set frozen: the forward pass
  * records each pass's slope factors per (cell, field), and the backward pass
  * applies that fixed linear map (degree 1 scaled, degrees >= 2 dropped below

@@ -12,7 +12,7 @@ import pytest
 
 import dgp
 from dgp import meshgen
-from cases import SCALAR2D, TM110, VORTEX, params, rel
+from cases import PULSE3D, SCALAR2D, TM110, VORTEX, params, rel
 
 pytestmark = pytest.mark.gpu
 
@@ -166,11 +166,33 @@ def test_adjoint_mixed_form_close_to_fp64(tmp_path):
 
 
 def test_adjoint_refused_where_not_built(tmp_path):
-    msh = _mesh(tmp_path, 6, (0.0, 10.0), 2)
-    mesh = dgp.Mesh.from_msh(msh)
-    s = dgp.Solver(mesh, dgp.Law(dgp.LAW_EULER2D, dgp.FLUX_GODUNOV, dgp.FIELD_VORTEX, VORTEX), 2)
-    with pytest.raises(dgp.DGPError):
+    """Periodic edges: the partner's cotangent would leave the slot layout."""
+    m = meshgen.tri_square(5, 4, -1.0, 1.0, -1.0, 1.0, jitter=0.15, seed=7, side_tags=(610, 510, 610, 510))
+    p = str(tmp_path / "periodic.msh")
+    meshgen.write_msh_v1(m, p)
+    s = dgp.Solver(dgp.Mesh.from_msh(p), dgp.Law(dgp.LAW_SCALAR, dgp.FLUX_UPWIND, dgp.FIELD_GAUSS, SCALAR2D), 2)
+    with pytest.raises(dgp.DGPError) as ei:
         s.forward_checkpointed(0.0, 1e-3, 2, 1)
+    assert ei.value.code == -3
+
+
+def test_adjoint_euler_exact_godunov_matches_fd(tmp_path):
+    """The exact Riemann solver differentiated through its Newton iteration."""
+    msh = _mesh(tmp_path, 12, (0.0, 10.0), 2)
+    pts = _receivers(np.random.default_rng(4), 64, 1.0, 9.0)
+    obs_prm = VORTEX.copy()
+    obs_prm[8] = 5.5
+    s, dt = _setup(msh, dgp.LAW_EULER2D, dgp.FLUX_GODUNOV, dgp.FIELD_VORTEX, 2, VORTEX, obs_prm, pts, 16, 5)
+    _fd_check(s, dt, 16, 5, 4, 1e-6, 1e-6)
+
+
+def test_adjoint_euler3d_exact_godunov_matches_fd(tmp_path):
+    msh = _mesh(tmp_path, 3, (0.0, 1.0), 3, dim=3)
+    pts = _receivers(np.random.default_rng(4), 16, 0.2, 0.8, dim=3)
+    obs_prm = PULSE3D.copy()
+    obs_prm[6] = 0.06
+    s, dt = _setup(msh, dgp.LAW_EULER3D, dgp.FLUX_GODUNOV, dgp.FIELD_PULSE3D, 1, PULSE3D, obs_prm, pts, 8, 3)
+    _fd_check(s, dt, 8, 3, 3, 1e-6, 1e-6)
 
 
 def test_adjoint_matches_cpu_fp64_directional_derivative(tmp_path):
