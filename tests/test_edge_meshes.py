@@ -87,3 +87,35 @@ def test_gpu_edge_mesh_matches_oracle(tmp_path, cid, kind, box, law, flux, field
     to, no = o.run(t, 0.0, 0.1, 5)
     assert ng == no == 5 and abs(tg - to) <= 1e-14 * to
     assert rel(s.get_state(), o.state()) < 1e-11
+
+
+@pytest.mark.gpu
+def test_gpu_switching_stage_forms_mid_run_matches_oracle(tmp_path):
+    """Steps alternating between the fused and the separate stage form (with a
+    state set from the host in between) give the oracle's states: the switch
+    refreshes the face-point traces that only the separate form reads."""
+    msh = _tri(tmp_path, 9, 7, 10.0, seed=2)
+    o = Oracle(msh, dgp.LAW_EULER2D, dgp.FLUX_ROE, 3, dgp.FIELD_VORTEX, VORTEX)
+    s = dgp.Solver(dgp.Mesh.from_msh(msh), dgp.Law(dgp.LAW_EULER2D, dgp.FLUX_ROE, dgp.FIELD_VORTEX, VORTEX), 3,
+                   dgp.FP64)
+    assert s.fused
+    t = 0.0
+    for k, form in enumerate((True, True, False, False, True, False)):
+        s.set_fused(form)
+        if k == 3:
+            s.set_state(o.state())  # set while separate
+        if k == 4:
+            s.set_state(o.state())  # set while fused, stepped fused
+        dt = o.cfl_dt(0.1)
+        s.step(t, dt)
+        o.step(t, dt)
+        t += dt
+        assert rel(s.get_state(), o.state()) < 1e-12, k
+    # a state set in the fused form, then the switch before the first step
+    s.set_fused(True)
+    s.set_state(o.state())
+    s.set_fused(False)
+    dt = o.cfl_dt(0.1)
+    s.step(t, dt)
+    o.step(t, dt)
+    assert rel(s.get_state(), o.state()) < 1e-12
