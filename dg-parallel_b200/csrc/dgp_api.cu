@@ -275,9 +275,10 @@ static std::vector<int> morton_order(const HostMesh& m) {
 // Face records and halos of the fused stage kernel's tiles (TileMesh): for
 // tile t, every face with a side among its cells, in face order, with both
 // sides as local rows (own cells first, then the halo in order of first use)
-// and the face's FP64 normal and measure.  The fused kernel is left off (the
-// stages use the face and element kernels) if a tile's halo would not fit in
-// shared memory.
+// and the face's FP64 normal and measure.  The fused kernel is built for the
+// solver (fused_ok) when every tile's halo fits in shared memory; whether the
+// stages then use it or the face and element kernels is tuned_fused's choice
+// (dgp_set_fused switches).
 static int build_tiles(dgp_solver s, int Etot, const std::vector<int>& fel, const std::vector<int>& fcode,
                        const std::vector<double>& fnrm, const std::vector<double>& fj, const std::vector<int>& bpart,
                        const std::vector<int>& cface) {
