@@ -92,6 +92,14 @@ def aggregate_rate(units_per_rank: float, seconds_max: float) -> float:
     return units_per_rank / seconds_max
 
 
+def select_device(index: int):
+    """The rank's GPU for torch (events, collectives) and for the library."""
+    import torch
+    import dgp
+    torch.cuda.set_device(index)
+    dgp.set_device(index)
+
+
 def load_peaks():
     try:
         with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as fh:
@@ -282,32 +290,27 @@ def main():
     if args.profile_case:
         return profile_case(args)
     if args.adjoint:
-        import torch
-        torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+        select_device(int(os.environ.get("LOCAL_RANK", "0")))
         print(json.dumps({"adjoint": adjoint_bench()}))
         return 0
     if args.ensemble:
-        import torch
         ranks = Ranks("nccl")
-        torch.cuda.set_device(ranks.local)
+        select_device(ranks.local)
         out = ensemble_bench(tend=args.ensemble_tend, ranks=ranks)
         if ranks.rank == 0:
             print(json.dumps({"ensemble": out}))
         ranks.close()
         return 0
     if args.decompose:
-        import torch
-        torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+        select_device(int(os.environ.get("LOCAL_RANK", "0")))
         print(json.dumps({"decompose": decompose_bench()}))
         return 0
     if args.configs:
-        import torch
-        torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+        select_device(int(os.environ.get("LOCAL_RANK", "0")))
         print(json.dumps({"configs": configs_bench()}))
         return 0
     if args.lts:
-        import torch
-        torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+        select_device(int(os.environ.get("LOCAL_RANK", "0")))
         print(json.dumps({"lts": lts_bench(steps=args.steps if args.steps != 300 else 16)}))
         return 0
 
@@ -317,7 +320,7 @@ def main():
 
     ranks = Ranks("nccl")
     world, rank, local = ranks.world, ranks.rank, ranks.local
-    torch.cuda.set_device(local)
+    select_device(local)
 
     mesh_np = make_mesh()
     prm = vortex_params()

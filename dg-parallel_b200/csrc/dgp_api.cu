@@ -688,6 +688,14 @@ extern "C" {
 const char* dgp_last_error(void) { return g_err.c_str(); }
 int dgp_version(void) { return 1; }
 
+int dgp_set_device(int device) {
+  int n = 0;
+  if (cudaGetDeviceCount(&n) != cudaSuccess || device < 0 || device >= n)
+    return fail(DGP_ERR_INVALID, "no CUDA device " + std::to_string(device));
+  DGP_CUDA(cudaSetDevice(device));
+  return DGP_OK;
+}
+
 int dgp_mesh_from_msh(const char* path, dgp_mesh* out) { return dgp_mesh_from_msh_ex(path, 0, out); }
 
 int dgp_mesh_from_msh_ex(const char* path, int gpu_faces, dgp_mesh* out) {

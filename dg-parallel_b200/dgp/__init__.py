@@ -51,6 +51,7 @@ def lib() -> ctypes.CDLL:
     pP = ctypes.POINTER(ctypes.c_void_p)
     sig = {
         "dgp_last_error": ([], ctypes.c_char_p),
+        "dgp_set_device": ([I], I),
         "dgp_version": ([], I),
         "dgp_mesh_from_msh": ([ctypes.c_char_p, pP], I),
         "dgp_mesh_from_arrays": ([I, I, pD, pI, I, pI, I, I, pI, pI, pP], I),
@@ -507,6 +508,11 @@ class Probe:
             self.close()
         except Exception:
             pass
+
+
+def set_device(device: int):
+    """CUDA device of the calling thread for the solvers created afterwards."""
+    check(lib().dgp_set_device(int(device)))
 
 
 def line_points(p1, p2, n: int) -> np.ndarray:

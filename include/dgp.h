@@ -85,6 +85,9 @@ typedef struct dgp_probe_s* dgp_probe;
 
 const char* dgp_last_error(void);
 int dgp_version(void);
+/* the CUDA device of the calling thread for the solvers, meshes and ensembles
+ * it creates afterwards (one process per GPU: each rank selects its own) */
+int dgp_set_device(int device);
 
 /* ---- mesh: replaces mImportExport::import (mImportExport.cc:57-170) and
  * mMesh::createCellBoundaries/createConnections (mMesh.cc:321-378) */
