@@ -136,3 +136,30 @@ def test_autotune_ensemble_groups(tmp_path):
     ens = dgp.Ensemble(meshes, laws, orders, dgp.FP64, dgp.LIMITER_MOMENT)
     for g in set(ens.groups):
         assert ens.group_block(g)[0] in (64, 128, 256)
+
+
+def test_ensemble_fused_form_equals_single_solvers(tmp_path):
+    """Euler (Roe) instances at P1-P3, which run the fused stage kernel by
+    default: the ensemble instantiation of that kernel (per-instance time
+    controls, the finalize per instance) gives the single solvers' states."""
+    from cases import VORTEX
+    specs = [(6, 21, 1), (9, 22, 2), (7, 23, 3), (8, 24, 2), (5, 25, 3)]
+    paths, laws, orders = [], [], []
+    for n, seed, order in specs:
+        m = meshgen.tri_square(n, n, 0.0, 10.0, 0.0, 10.0, jitter=0.15, seed=seed)
+        p = str(tmp_path / f"ensv_{n}_{seed}.msh")
+        meshgen.write_msh_v1(m, p)
+        paths.append(p)
+        laws.append(dgp.Law(dgp.LAW_EULER2D, dgp.FLUX_ROE, dgp.FIELD_VORTEX, VORTEX))
+        orders.append(order)
+    meshes = [dgp.Mesh.from_msh(p) for p in paths]
+    ens = dgp.Ensemble(meshes, laws, orders, dgp.FP64, dgp.LIMITER_NONE)
+    ens.project(0.0)
+    t, steps, ms, total = ens.run(0.0, 0.05, 0.1)
+    for i, p in enumerate(paths):
+        s = dgp.Solver(dgp.Mesh.from_msh(p), laws[i], orders[i], dgp.FP64)
+        assert s.fused
+        s.project(0.0)
+        ts, ns = s.run(0.0, 0.05, 0.1)
+        assert ns == steps[i] and abs(ts - t[i]) < 1e-14
+        assert rel(ens.get_state(i), s.get_state()) == 0.0
