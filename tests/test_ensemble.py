@@ -141,7 +141,10 @@ def test_autotune_ensemble_groups(tmp_path):
 def test_ensemble_fused_form_equals_single_solvers(tmp_path):
     """Euler (Roe) instances at P1-P3, which run the fused stage kernel by
     default: the ensemble instantiation of that kernel (per-instance time
-    controls, the finalize per instance) gives the single solvers' states."""
+    controls, the finalize per instance) takes the single solvers' steps to the
+    same times and gives their states to the last rounding (the two
+    instantiations are compiled separately and may contract a multiply-add
+    differently)."""
     from cases import VORTEX
     specs = [(6, 21, 1), (9, 22, 2), (7, 23, 3), (8, 24, 2), (5, 25, 3)]
     paths, laws, orders = [], [], []
@@ -162,4 +165,4 @@ def test_ensemble_fused_form_equals_single_solvers(tmp_path):
         s.project(0.0)
         ts, ns = s.run(0.0, 0.05, 0.1)
         assert ns == steps[i] and abs(ts - t[i]) < 1e-14
-        assert rel(ens.get_state(i), s.get_state()) == 0.0
+        assert rel(ens.get_state(i), s.get_state()) < 1e-15
