@@ -84,7 +84,10 @@ extern "C" int dgp_rhs_noalloc(dgp_solver s, const double* dev_state, double t, 
   // length up to 16 bytes and must stay inside the region
   const size_t state_b = round256(s->state_count() * 8 + 256);
   const size_t ntiles = (static_cast<size_t>(E) + s->ops.TE - 1) / s->ops.TE;
-  const size_t slot_b = round256(ntiles * s->ops.TE * s->tab.nlf * s->tab.nqf * s->b.M * tsize);
+  // the fused stage kernel keeps face data in shared memory: state and RHS
+  // only; the separate kernels also need the face slots and traces
+  const size_t slot_b =
+      s->fused ? 0 : round256(ntiles * s->ops.TE * s->tab.nlf * s->tab.nqf * s->b.M * tsize);
   const size_t need = 2 * state_b + 2 * slot_b;
   if (need > kScratchBytes)
     return fail(DGP_ERR_INVALID, "dgp_rhs_noalloc: this mesh needs " + std::to_string(need) +
@@ -94,7 +97,10 @@ extern "C" int dgp_rhs_noalloc(dgp_solver s, const double* dev_state, double t, 
   if (int rc = scratch_address(s->device, &base)) return rc;
   unsigned char* p = static_cast<unsigned char*>(base);
   dgp::DeviceBuffers b = s->b;  // geometry and tables of the solver, intermediates in scratch
-  b.p0 = 0;  // the P0 fallback's second pass would zero modes of the caller's state
+  // the separate form's P0 second pass would zero modes of the state copy in
+  // place before the element kernel reads it, which the fused kernel does in
+  // shared memory only: the fallback applies in the fused form
+  if (!s->fused) b.p0 = 0;
   b.C = p;
   b.slots = p + state_b;
   b.rhs = p + state_b + slot_b;
@@ -108,9 +114,14 @@ extern "C" int dgp_rhs_noalloc(dgp_solver s, const double* dev_state, double t, 
   c.dtmin_bits = 0x7FF0000000000000ull;
   s->h_ctl[0] = c;
   DGP_CUDA(cudaMemcpyAsync(s->b.ctl, &s->h_ctl[0], sizeof(dgp::TimeCtl), cudaMemcpyHostToDevice, s->stream));
-  s->ops.trace(b, nullptr, s->stream);
-  s->ops.face(b, 0, 0.0, s->stream);
-  s->ops.elem(b, 0, 0, s->stream);
+  if (s->fused) {
+    const double* C = static_cast<const double*>(b.C);
+    s->ops.fused(b, C, C, static_cast<double*>(b.rhs), nullptr, 0, 0.0, 0, s->stream);
+  } else {
+    s->ops.trace(b, nullptr, s->stream);
+    s->ops.face(b, 0, 0.0, s->stream);
+    s->ops.elem(b, 0, 0, s->stream);
+  }
   permute_rows<double, double><<<grid, 256, 0, s->stream>>>(static_cast<const double*>(b.rhs), dev_rhs,
                                                              s->d_f2i, E, mnp);
   DGP_CUDA(cudaGetLastError());

@@ -310,8 +310,11 @@ int dgp_set_fused(dgp_solver s, int on);
  * (device memory owned by another allocator, or no tolerance for the
  * synchronisation an allocation implies).  dev_state and dev_rhs are device
  * buffers, FP64 [cell][field][mode] in file order, like dgp_rhs's output.  The
- * intermediates live in a 32 MiB static device array that every GPU loading
- * the library holds until exit; meshes that need more return DGP_ERR_INVALID.
+ * intermediates (a state and a RHS copy in internal order; with the separate
+ * stage form also the face slots and traces) live in a 32 MiB static device
+ * array that every GPU loading the library holds until exit; meshes that need
+ * more return DGP_ERR_INVALID.  The P0 fallback applies in the fused form (as
+ * in dgp_rhs) and not in the separate form.
  * Calls share that array: calls that overlap on the GPU race.  The first call
  * on a device looks up the array's device address (host-side setup), so make
  * it before any stream capture.  Like dgp_rhs, the call resets the solver's

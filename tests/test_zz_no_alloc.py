@@ -41,9 +41,11 @@ def rel(a, b):
     return float(np.abs(a - b).max() / np.abs(b).max())
 
 
-def test_rhs_noalloc_matches_rhs_on_consecutive_calls(tmp_path):
+@pytest.mark.parametrize("fused", [True, False])
+def test_rhs_noalloc_matches_rhs_on_consecutive_calls(tmp_path, fused):
     torch = pytest.importorskip("torch")
     s = vortex_solver(str(tmp_path / "v12.msh"), 12)
+    s.set_fused(fused)
     s.run(0.0, 0.0, 0.1, 3)  # a non-trivial state
     for t in (0.02, 0.31):   # two calls in a row, different states and times
         state = s.get_state()
@@ -58,9 +60,13 @@ def test_rhs_noalloc_matches_rhs_on_consecutive_calls(tmp_path):
         s.step(t, 1e-3)  # move to another state for the second call
 
 
-def test_rhs_noalloc_refuses_meshes_beyond_the_scratch(tmp_path):
+@pytest.mark.parametrize("fused,n", [(False, 136), (True, 170)])
+def test_rhs_noalloc_refuses_meshes_beyond_the_scratch(tmp_path, fused, n):
+    """Separate form: 36992 cells need ~36 MiB of intermediates (state, RHS,
+    slots, traces); fused form: 57800 cells need ~37 MiB (state and RHS)."""
     torch = pytest.importorskip("torch")
-    s = vortex_solver(str(tmp_path / "v136.msh"), 136)  # 36992 cells: ~36 MiB of intermediates
+    s = vortex_solver(str(tmp_path / f"v{n}.msh"), n)
+    s.set_fused(fused)
     n = int(np.prod(s.shape))
     dev_state = torch.zeros(n, dtype=torch.float64, device="cuda")
     dev_out = torch.zeros_like(dev_state)
