@@ -275,7 +275,7 @@ def main():
     ap.add_argument("--lts", action="store_true",
                     help="only the local time stepping measurement (Euler vortex P3 on 256x256x2 graded "
                          "triangles, 4 size bins, against SSP-RK3 on the same mesh, ~1 min)")
-    ap.add_argument("--profile-case", choices=["fp64", "mixed", "maxwell", "limiter", "lts"], default=None,
+    ap.add_argument("--profile-case", choices=["fp64", "mixed", "maxwell", "limiter", "lts", "adjoint"], default=None,
                     help="only set up the workload and run --warmup + --steps steps (for ncu)")
     ap.add_argument("--tensor-cores", action="store_true",
                     help="--profile-case mixed: the volume contraction on the tensor cores")
@@ -957,6 +957,23 @@ def profile_case(args):
         t, n = s.run(0.0, 0.0, 0.1, args.warmup + args.steps)
         s.synchronize()
         print(f"profile case limiter: {n} steps, t = {t:.6e}")
+        return 0
+    if args.profile_case == "adjoint":
+        # the adjoint bench's mesh and law: --steps recorded steps (every = 0)
+        # and one backward pass, FP64
+        import numpy as np
+        from dgp import meshgen
+        m = meshgen.tri_square(128, 128, 0.0, 10.0, 0.0, 10.0, jitter=0.15, seed=2)
+        mesh = dgp.Mesh.from_arrays(2, m.vertices, m.cells, m.domain_tag, m.bfaces, m.btags)
+        law = dgp.Law(dgp.LAW_EULER2D, dgp.FLUX_ROE, dgp.FIELD_VORTEX, vortex_params())
+        s = dgp.Solver(mesh, law, 2, dgp.FP64)
+        s.project(0.0)
+        s.set_receivers(np.random.default_rng(4).uniform(0.5, 9.5, size=(64, 2)), np.zeros(64))
+        dt = 0.5 * s.cfl_dt(0.1)
+        J = s.forward_checkpointed(0.0, dt, args.steps, 0)
+        g = s.backward()
+        s.synchronize()
+        print(f"profile case adjoint: {args.steps} steps, J = {J:.6e}, |g|max = {np.abs(g).max():.6e}")
         return 0
     if args.profile_case == "lts":
         # lts_bench's workload: local time stepping steps only
